@@ -1,0 +1,142 @@
+/*
+ * ostc.h -- C ABI of the B200 OpenSTC right-hand-side + SSP-RK3 library (libostc_b200.so).
+ *
+ * The reference solver has no plugin/FFI layer: its seam is the set of C++ template calls made by
+ * RK3<mix,turb>() in RK.cuh:112-174 (compute_inviscid_flux, compute_viscous_flux, compute_source,
+ * local_time_step/global_time_step, update_cv_and_bv_rk, apply_boundary_conditions,
+ * data_communication, update_physical_properties) over the DZone/DParameter/Parameter data built
+ * from input/setup.txt and the grid/boundary files.  Each entry point below names the reference
+ * interface it replaces.  Conventions:
+ *   - every function returns OSTC_OK (0) or a negative OSTC_E* code; ostc_last_error() gives text;
+ *   - no exceptions cross the boundary, no torch or CUDA types appear in the signatures;
+ *   - a context owns all device memory and one CUDA stream on the device given to ostc_create;
+ *     one host thread uses a context at a time;
+ *   - host arrays are SoA with the i index fastest: a[l][k][j][i] for l < n_var (or 6, or n_scalar),
+ *     over the interior nodes of one block (mx*my*mz per variable).
+ */
+#ifndef OSTC_H
+#define OSTC_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OSTC_OK 0
+#define OSTC_EINVAL (-1)     /* bad argument or unsupported configuration */
+#define OSTC_EIO (-2)        /* input file missing or malformed */
+#define OSTC_ECUDA (-3)      /* CUDA runtime error */
+#define OSTC_ESTATE (-4)     /* call out of order (e.g. stepping before a state was set) */
+#define OSTC_ENOMEM (-5)     /* device allocation failed */
+#define OSTC_ENUMERIC (-6)   /* a device error flag was raised (see ostc_error_flags) */
+
+/* ostc_set_state / ostc_get_state / ostc_rhs pointer kinds */
+#define OSTC_HOST 0
+#define OSTC_DEVICE 1
+
+/* ostc_set_precision modes */
+#define OSTC_PREC_FP64 0   /* every operation in FP64, as the reference */
+#define OSTC_PREC_MIXED 1  /* reconstruction, Riemann, viscous flux in FP32; RK3 state, EOS in FP64 */
+
+/* ostc_rhs term mask (the order of evaluation follows RK.cuh:116-139) */
+#define OSTC_TERM_INVISCID 1u
+#define OSTC_TERM_VISCOUS 2u
+#define OSTC_TERM_SOURCE 4u
+#define OSTC_TERM_ALL 7u
+
+/* device error flags (ostc_error_flags) */
+#define OSTC_FLAG_NONPOSITIVE 1u   /* rho, p or T not positive after an RK stage */
+#define OSTC_FLAG_NAN 2u           /* NaN in the conservative state */
+
+typedef struct ostc_ctx ostc_ctx;
+
+/* Raw device views of one block, zero-copy (replaces reading DZone, Field.h:12-90).  Arrays are
+ * ghost-padded SoA: element (i,j,k,l) of a field sits at base[l*plane + (k+gz)*sy*pitch +
+ * (j+g)*pitch + (i+g)].  In 2-D (mz == 1) gz is 0: the reference's copied k-ghost layers
+ * (eliminate_k_gradient, FieldOperation.cu:42-67) are implicit. */
+typedef struct {
+  int mx, my, mz, ngg, gz;
+  int pitch, sy, sz;       /* padded extents in i (row pitch), j, k */
+  long long plane;         /* elements per variable plane */
+  double *cv, *bv, *mul;   /* current state: cv[n_var], bv[6] (rho,u,v,w,p,T), mu */
+  double *metric, *jac;    /* metric[9] planes ((r-1)*3+(c-1)), Jacobian */
+} ostc_zone_view;
+
+/* Build a context from a reference-format case directory: reads <input_dir>/setup.txt (or the file
+ * given by setup_txt), the binary grid "grid/grid   0.dat" and "boundary_condition/boundary   0.txt" /
+ * "inner   0.txt" below input_dir, computes ghost grids, metrics and Jacobians, and allocates the
+ * device state on `device`.  Replaces Parameter(&argc,&argv) + Mesh(parameter) + Driver ctor
+ * (Parameter.cpp:10-23, Mesh.cpp:592-641, Driver.cu:12-113). */
+int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_ctx **out);
+
+/* Free every resource of the context. */
+void ostc_destroy(ostc_ctx *ctx);
+
+/* Text of the last error raised on this context (or of the last failed ostc_create when ctx is NULL). */
+const char *ostc_last_error(const ostc_ctx *ctx);
+
+/* Number of blocks and the size of block b: dims = {mx, my, mz, ngg}. */
+int ostc_n_blocks(const ostc_ctx *ctx, int *n_block);
+int ostc_block_dims(const ostc_ctx *ctx, int block, int dims[4]);
+/* n_var (5 + transported scalars) and n_scalar (Parameter::deduce_sim_info, Parameter.cpp:589-653). */
+int ostc_n_var(const ostc_ctx *ctx, int *n_var, int *n_scalar);
+
+/* Arithmetic of the flux path (see OSTC_PREC_*). */
+int ostc_set_precision(ostc_ctx *ctx, int mode);
+
+/* Set the interior primitive state of one block: bv[6][N] (rho,u,v,w,p,T), sv[n_scalar][N] (NULL
+ * when n_scalar == 0).  After the last block is set, the next ostc_rhs/ostc_rk3_step first runs
+ * the reference initialisation (2-D k-copy, boundary conditions, interfaces, properties,
+ * cv <- bv; Driver.cu:115-199, RK.cuh:37-45). Replaces Field::initialize_basic_variables. */
+int ostc_set_state(ostc_ctx *ctx, int block, const double *bv, const double *sv, int ptr_kind);
+
+/* Copy the interior state of one block out: cv[n_var][N], bv[6][N], sv[n_scalar][N] (any pointer
+ * may be NULL).  Synchronises the context stream.  Replaces Field::copy_data_from_device. */
+int ostc_get_state(ostc_ctx *ctx, int block, double *cv, double *bv, double *sv, int ptr_kind);
+
+/* Right-hand side dq[n_var][N] of the current state for one block, terms selected by mask
+ * (compute_inviscid_flux + compute_viscous_flux + compute_source, SchemeSelector.cuh:24-67,
+ * SourceTerm.cuh:11-35).  dq has the reference's sign: d(cv)/dt = dq / jac. */
+int ostc_rhs(ostc_ctx *ctx, int block, unsigned term_mask, double *dq, int ptr_kind);
+
+/* Advance n_steps full SSP-RK3 steps (the loop body of RK3<mix,turb>, RK.cuh:85-185), all stream
+ * ordered and replayed from a CUDA graph.  dt_last (nullable) receives the last step's dt (CFL
+ * minimum over all blocks, TimeAdvanceFunc.cu:39-64, or the fixed dt); reading it synchronises. */
+int ostc_rk3_step(ostc_ctx *ctx, int n_steps, double *dt_last);
+
+/* Physical time advanced so far (RK.cuh:175-176).  Synchronises. */
+int ostc_physical_time(ostc_ctx *ctx, double *t);
+
+/* Snapshot the current state as the residual reference (store_last_step, TimeAdvanceFunc.cu:6-19). */
+int ostc_store_residual_reference(ostc_ctx *ctx);
+/* RMS change of rho, |V|, p, T since the snapshot (compute_residual, Residual.cuh:74-190):
+ * res[l] = sqrt(sum over all interior nodes of (change)^2 / total node count). Synchronises. */
+int ostc_residual(ostc_ctx *ctx, double res[4]);
+
+/* Device error flags (OSTC_FLAG_*) accumulated since the last call, then cleared.  Synchronises. */
+int ostc_error_flags(ostc_ctx *ctx, unsigned *flags);
+
+/* Zero-copy device view of block b (valid until ostc_destroy). */
+int ostc_device_view(ostc_ctx *ctx, int block, ostc_zone_view *out);
+
+/* Kernel timing for measurement: runs n_steps steps launch by launch (no graph) with CUDA events
+ * around every kernel on the context stream and returns, per kernel family, the number of launches
+ * and the summed device milliseconds.  names[i] points to static strings. Returns the number of
+ * families written (<= max). */
+int ostc_profile_steps(ostc_ctx *ctx, int n_steps, int max, const char **names, int *launches, double *ms);
+
+/* Number of interior nodes over all blocks (the unit of cell-steps/s). */
+int ostc_total_nodes(const ostc_ctx *ctx, long long *n);
+
+/* Host-only parse of a case directory (no device is touched): runs the setup/grid/boundary readers
+ * and writes out[0..13] = ngg, inviscid_type, n_var, n_scalar, n_block, dimension, mx, my, mz of
+ * block 0, number of boundary faces of block 0, reconstruction, inviscid_scheme, viscous_order,
+ * number of boundary-face applications per stage.  On failure msg receives the reason
+ * (Parameter::deduce_known_info / Mesh::Mesh checks, Parameter.cpp:187-437, Mesh.cpp:592-641). */
+int ostc_probe_case(const char *setup_txt, const char *input_dir, int out[16], char *msg, int msg_len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,693 @@
+// host.cpp -- setup.txt parsing, derived parameters, grid/boundary file reading, ghost grids,
+// metrics and boundary registration.  All of it restates the reference's host-side set-up so that
+// the device path sees exactly the values the reference computes.
+#include "host.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+
+namespace ostc {
+
+// ------------------------------------------------------------------------------------ setup.txt
+
+void Setup::set_defaults() {
+  ints["problem_type"] = 0;
+  ints["mesh_file_type"] = 0;
+  ints["gridIsBinary"] = 0;
+  reals["gridScale"] = 1.0;
+  bools["steady"] = true;
+  ints["implicit_method"] = 0;
+  ints["temporal_scheme"] = 3;
+  bools["fixed_time_step"] = false;
+  reals["dt"] = 1e-8;
+  ints["inviscid_scheme"] = 3;
+  ints["reconstruction"] = 2;
+  ints["limiter"] = 0;
+  reals["entropy_fix_factor"] = 0.125;
+  ints["viscous_order"] = 2;
+  bools["gradPInDiffusionFlux"] = false;
+  bools["positive_preserving"] = false;
+  ints["species"] = 0;
+  ints["reaction"] = 0;
+  strings["therm_file"] = "chemistry/therm.dat";
+  strings["transport_file"] = "chemistry/tran.dat";
+  ints["chemSrcMethod"] = 0;
+  bools["turbulence"] = false;
+  ints["turbulence_method"] = 1;
+  ints["RANS_model"] = 2;
+  ints["n_ps"] = 0;
+  reals["schmidt_number"] = 0.5;
+  reals["prandtl_number"] = 0.72;
+  reals["turbulent_prandtl_number"] = 0.9;
+  reals["turbulent_schmidt_number"] = 0.9;
+  bools["limit_flow"] = false;
+  bools["sponge_layer"] = false;
+  reals["cfl"] = 1.0;
+  ints["total_step"] = 1;
+  ints["output_screen"] = 100;
+  string_arrays["boundary_conditions"] = {};
+}
+
+namespace {
+// Reads tokens of one line into arr until "}" (returns false: array finished) or "//" / end of
+// line (returns true: continue on the next line).  Parameter::read_line_to_array, Parameter.cpp:136-160.
+template <typename T>
+bool read_line_to_array(std::istringstream &line, std::vector<T> &arr) {
+  std::string tok;
+  while (line >> tok) {
+    if (tok == "}") return false;
+    if (tok == "//") break;
+    if constexpr (std::is_same_v<T, double>) arr.push_back(std::stod(tok));
+    else if constexpr (std::is_same_v<T, int>) arr.push_back(std::stoi(tok));
+    else arr.push_back(tok);
+  }
+  return true;
+}
+
+void next_line(std::ifstream &f, std::string &input, std::istringstream &line) {
+  if (!std::getline(f, input)) input.clear();
+  const auto s = input.find_first_not_of(" \t");
+  input = s == std::string::npos ? std::string() : input.substr(s);
+  line.clear();
+  line.str(input);
+}
+
+template <typename T>
+void read_array(std::ifstream &f, std::string &input, std::istringstream &line, std::vector<T> &arr) {
+  while (read_line_to_array(line, arr)) {
+    if (!f) break;
+    next_line(f, input, line);
+    if (!f && input.empty()) break;
+  }
+}
+}  // namespace
+
+bool Setup::read_file(const std::string &path, std::string &err) {
+  std::ifstream f(path);
+  if (!f) {
+    err = "cannot open setup file " + path;
+    return false;
+  }
+  std::string input, type, key, temp;
+  std::istringstream line;
+  try {
+    while (std::getline(f, input)) {
+      if (input.rfind("//", 0) == 0 || input.rfind("!", 0) == 0 || input.empty()) continue;
+      line.clear();
+      line.str(input);
+      type.clear();
+      key.clear();
+      temp.clear();
+      line >> type;
+      line >> key >> temp;
+      if (type == "int") {
+        int v{};
+        line >> v;
+        ints[key] = v;
+      } else if (type == "real") {
+        double v{};
+        line >> v;
+        reals[key] = v;
+      } else if (type == "bool") {
+        bool v{};
+        line >> v;
+        bools[key] = v;
+      } else if (type == "string") {
+        std::string v;
+        line >> v;
+        strings[key] = v;
+      } else if (type == "array") {
+        const std::string name = temp;
+        line >> temp >> temp;  // "= {" or "{" plus the first value (reference behaviour)
+        if (key == "int") {
+          std::vector<int> a;
+          read_array(f, input, line, a);
+          int_arrays[name] = a;
+        } else if (key == "real") {
+          std::vector<double> a;
+          read_array(f, input, line, a);
+          real_arrays[name] = a;
+        } else if (key == "string") {
+          std::vector<std::string> a;
+          read_array(f, input, line, a);
+          string_arrays[name] = a;
+        }
+      } else if (type == "struct") {
+        std::map<std::string, StructVal> st;
+        while (true) {
+          next_line(f, input, line);
+          if (!f && input.empty()) break;
+          std::string k2, name, eq;
+          line >> k2;
+          if (k2 == "}") break;
+          if (k2 == "string") {
+            std::string v;
+            line >> name >> eq >> v;
+            st.emplace(name, v);
+          } else if (k2 == "int") {
+            int v{};
+            line >> name >> eq >> v;
+            st.emplace(name, v);
+          } else if (k2 == "real") {
+            double v{};
+            line >> name >> eq >> v;
+            st.emplace(name, v);
+          }
+        }
+        structs[key] = st;
+      } else if (type == "range") {
+        const std::string name = temp;
+        line >> temp >> temp;
+        if (key == "real") {
+          std::vector<double> a;
+          read_array(f, input, line, a);
+          if (a.size() != 2 && a.size() != 4 && a.size() != 6) {
+            err = "range " + name + ": expected 2, 4 or 6 values";
+            return false;
+          }
+          real_ranges[name] = a;
+        } else if (key == "int") {
+          std::vector<int> a;
+          read_array(f, input, line, a);
+          if (a.size() != 2 && a.size() != 4 && a.size() != 6) {
+            err = "range " + name + ": expected 2, 4 or 6 values";
+            return false;
+          }
+          int_ranges[name] = a;
+        }
+      }
+    }
+  } catch (const std::exception &e) {
+    err = std::string("setup parse error: ") + e.what();
+    return false;
+  }
+  return true;
+}
+
+int Setup::get_int(const std::string &k) const {
+  auto it = ints.find(k);
+  return it == ints.end() ? 0 : it->second;
+}
+double Setup::get_real(const std::string &k) const {
+  auto it = reals.find(k);
+  return it == reals.end() ? 0.0 : it->second;
+}
+bool Setup::get_bool(const std::string &k) const {
+  auto it = bools.find(k);
+  return it == bools.end() ? false : it->second;
+}
+
+bool derive(const Setup &s, Derived &d, std::string &err) {
+  d.reconstruction = s.get_int("reconstruction");
+  d.inviscid_scheme = s.get_int("inviscid_scheme");
+  d.viscous_order = s.get_int("viscous_order");
+  // ghost layers (Parameter.cpp:194-242)
+  int ngg = 2;
+  if (d.reconstruction == 4) ngg = 3;
+  else if (d.reconstruction == 5) ngg = 4;
+  const int is = d.inviscid_scheme;
+  if (is == 51 || is == 52 || is == 6) ngg = 3;
+  if (is == 71 || is == 72) ngg = 4;
+  d.ngg = ngg;
+  // inviscid_type (Parameter.cpp:264-278)
+  int it = 0;
+  if (is == 2) it = 2;
+  if (d.reconstruction == 4 || d.reconstruction == 5) it = 1;
+  if (is == 51 || is == 52 || is == 71 || is == 72) it = 3;
+  if (is == 6) it = 4;
+  d.inviscid_type = it;
+  d.steady = s.get_bool("steady");
+  d.temporal_scheme = s.get_int("temporal_scheme");
+  d.fixed_time_step = s.get_bool("fixed_time_step");
+  d.dt = s.get_real("dt");
+  d.cfl = s.get_real("cfl");
+  d.prandtl = s.get_real("prandtl_number");
+  d.grid_scale = s.get_real("gridScale");
+  d.species = s.get_int("species");
+  d.n_spec = 0;
+  d.n_scalar = 0;
+  d.n_var = 5;
+  if (d.species != 0) {
+    err = "species != 0 (multi-component mixtures) is not supported by this build of the library";
+    return false;
+  }
+  if (s.get_bool("turbulence")) {
+    err = "turbulence models are outside this library's path (laminar/DNS only)";
+    return false;
+  }
+  if (d.steady || d.temporal_scheme != 3) {
+    err = "only unsteady SSP-RK3 (steady = 0, temporal_scheme = 3) is on this library's path";
+    return false;
+  }
+  if (d.inviscid_type != 1) {
+    err = "for air this library implements the AWENO path (reconstruction = 4 or 5); got inviscid_type " +
+          std::to_string(d.inviscid_type);
+    return false;
+  }
+  if (d.inviscid_scheme != 3 && d.inviscid_scheme != 4) {
+    err = "AWENO supports inviscid_scheme 3 (AUSM+) or 4 (HLLC) on this path";
+    return false;
+  }
+  if (d.viscous_order != 0 && d.viscous_order != 2) {
+    err = "viscous_order must be 0 or 2";
+    return false;
+  }
+  if (s.get_bool("limit_flow") || s.get_bool("sponge_layer")) {
+    err = "limit_flow / sponge_layer are not on this library's path";
+    return false;
+  }
+  if (s.get_int("n_ps") != 0) {
+    err = "passive scalars (n_ps) are not on this library's path";
+    return false;
+  }
+  return true;
+}
+
+// ------------------------------------------------------------------------------------ mesh
+
+namespace {
+
+// Boundary::register_boundary (Mesh.cpp:14-32)
+void register_boundary(BcFace &b, int ngg, int dim) {
+  b.face = 0;
+  b.direction = 1;
+  for (int i = 0; i < dim; ++i) {
+    if (b.rs[i] == b.re[i]) {
+      b.face = i;
+      if (b.rs[i] == 0) b.direction = -1;
+      break;
+    }
+  }
+  for (int i = 0; i < dim; ++i) {
+    if (i == b.face) continue;
+    if (b.re[i] < b.rs[i]) std::swap(b.re[i], b.rs[i]);
+    b.rs[i] -= ngg;
+    b.re[i] += ngg;
+  }
+  if (dim == 2) {
+    b.rs[2] = -ngg;
+    b.re[2] = ngg;
+  }
+}
+
+// Mesh::init_ghost_grid for one block without interfaces (Mesh.cpp:893-1043)
+void ghost_grid(HostBlock &B, int dimension) {
+  const int mx = B.mx, my = B.my, mz = B.mz, ngg = B.ngg;
+  std::array<std::vector<double> *, 3> C{&B.x, &B.y, &B.z};
+  auto at = [&](int q, int i, int j, int k) -> double & { return (*C[q])[B.cidx(i, j, k)]; };
+  for (int q = 0; q < 3; ++q)
+    for (int k = 0; k < mz; ++k)
+      for (int j = 0; j < my; ++j) {
+        for (int i = -1; i >= -ngg - 1; --i) at(q, i, j, k) = 2 * at(q, 0, j, k) - at(q, -i, j, k);
+        for (int i = mx; i < mx + ngg + 1; ++i) at(q, i, j, k) = 2 * at(q, mx - 1, j, k) - at(q, 2 * (mx - 1) - i, j, k);
+      }
+  for (int q = 0; q < 3; ++q)
+    for (int k = 0; k < mz; ++k)
+      for (int i = 0; i < mx; ++i) {
+        for (int j = -1; j >= -ngg - 1; --j) at(q, i, j, k) = 2 * at(q, i, 0, k) - at(q, i, -j, k);
+        for (int j = my; j < my + ngg + 1; ++j) at(q, i, j, k) = 2 * at(q, i, my - 1, k) - at(q, i, 2 * (my - 1) - j, k);
+      }
+  if (dimension == 3) {
+    for (int q = 0; q < 3; ++q)
+      for (int j = 0; j < my; ++j)
+        for (int i = 0; i < mx; ++i) {
+          for (int k = -1; k >= -ngg - 1; --k) at(q, i, j, k) = 2 * at(q, i, j, 0) - at(q, i, j, -k);
+          for (int k = mz; k < mz + ngg + 1; ++k) at(q, i, j, k) = 2 * at(q, i, j, mz - 1) - at(q, i, j, 2 * (mz - 1) - k);
+        }
+  } else {
+    for (int j = 0; j < my; ++j)
+      for (int i = 0; i < mx; ++i) {
+        for (int k = -1; k >= -ngg - 1; --k) {
+          at(0, i, j, k) = at(0, i, j, 0);
+          at(1, i, j, k) = at(1, i, j, 0);
+          at(2, i, j, k) = at(2, i, j, 0) + k;
+        }
+        for (int k = mz; k < mz + ngg + 1; ++k) {
+          at(0, i, j, k) = at(0, i, j, mz - 1);
+          at(1, i, j, k) = at(1, i, j, mz - 1);
+          at(2, i, j, k) = at(2, i, j, mz - 1) + k - mz + 1;
+        }
+      }
+  }
+  for (int i = 1; i <= ngg + 1; ++i)
+    for (int j = 1; j <= ngg + 1; ++j)
+      for (int k = 0; k < mz; ++k) {
+        const int i1 = -i, j1 = -j, i2 = mx - 1 + i, j2 = my - 1 + j;
+        for (int q = 0; q < 3; ++q) {
+          at(q, i1, j1, k) = at(q, i1, 0, k) + at(q, 0, j1, k) - at(q, 0, 0, k);
+          at(q, i2, j2, k) = at(q, i2, my - 1, k) + at(q, mx - 1, j2, k) - at(q, mx - 1, my - 1, k);
+          at(q, i1, j2, k) = at(q, i1, my - 1, k) + at(q, 0, j2, k) - at(q, 0, my - 1, k);
+          at(q, i2, j1, k) = at(q, i2, 0, k) + at(q, mx - 1, j1, k) - at(q, mx - 1, 0, k);
+        }
+      }
+  for (int i = 1; i <= ngg + 1; ++i)
+    for (int j = 0; j < my; ++j)
+      for (int k = 1; k <= ngg + 1; ++k) {
+        const int i1 = -i, k1 = -k, i2 = mx - 1 + i, k2 = mz - 1 + k;
+        for (int q = 0; q < 3; ++q) {
+          at(q, i1, j, k1) = at(q, i1, j, 0) + at(q, 0, j, k1) - at(q, 0, j, 0);
+          at(q, i2, j, k2) = at(q, i2, j, mz - 1) + at(q, mx - 1, j, k2) - at(q, mx - 1, j, mz - 1);
+          at(q, i1, j, k2) = at(q, i1, j, mz - 1) + at(q, 0, j, k2) - at(q, 0, j, mz - 1);
+          at(q, i2, j, k1) = at(q, i2, j, 0) + at(q, mx - 1, j, k1) - at(q, mx - 1, j, 0);
+        }
+      }
+  for (int i = -ngg - 1; i <= mx + ngg; ++i)
+    for (int j = 1; j <= ngg + 1; ++j)
+      for (int k = 1; k <= ngg + 1; ++k) {
+        const int j1 = -j, k1 = -k, j2 = my - 1 + j, k2 = mz - 1 + k;
+        for (int q = 0; q < 3; ++q) {
+          at(q, i, j1, k1) = at(q, i, j1, 0) + at(q, i, 0, k1) - at(q, i, 0, 0);
+          at(q, i, j2, k2) = at(q, i, j2, mz - 1) + at(q, i, my - 1, k2) - at(q, i, my - 1, mz - 1);
+          at(q, i, j1, k2) = at(q, i, j1, mz - 1) + at(q, i, 0, k2) - at(q, i, 0, mz - 1);
+          at(q, i, j2, k1) = at(q, i, j2, 0) + at(q, i, my - 1, k1) - at(q, i, my - 1, 0);
+        }
+      }
+}
+
+// One node of Block::compute_jac_metric (Mesh.cpp:241-503)
+void metric_node(HostBlock &B, int i, int j, int k, int fi, int fj, int fk) {
+  auto X = [&](int a, int b, int c) { return B.x[B.cidx(a, b, c)]; };
+  auto Y = [&](int a, int b, int c) { return B.y[B.cidx(a, b, c)]; };
+  auto Z = [&](int a, int b, int c) { return B.z[B.cidx(a, b, c)]; };
+  const double dxd1 = (X(i + 1, j, k) - X(i - 1, j, k)) * 0.5, dyd1 = (Y(i + 1, j, k) - Y(i - 1, j, k)) * 0.5,
+               dzd1 = (Z(i + 1, j, k) - Z(i - 1, j, k)) * 0.5;
+  const double dxd2 = (X(i, j + 1, k) - X(i, j - 1, k)) * 0.5, dyd2 = (Y(i, j + 1, k) - Y(i, j - 1, k)) * 0.5,
+               dzd2 = (Z(i, j + 1, k) - Z(i, j - 1, k)) * 0.5;
+  const double dxd3 = (X(i, j, k + 1) - X(i, j, k - 1)) * 0.5, dyd3 = (Y(i, j, k + 1) - Y(i, j, k - 1)) * 0.5,
+               dzd3 = (Z(i, j, k + 1) - Z(i, j, k - 1)) * 0.5;
+  const double jac = dxd1 * dyd2 * dzd3 + dxd2 * dyd3 * dzd1 + dxd3 * dyd1 * dzd2 - dxd1 * dyd3 * dzd2 -
+                     dxd2 * dyd1 * dzd3 - dxd3 * dyd2 * dzd1;
+  const long P = B.padded(), p = B.gidx(i, j, k);
+  if (jac <= 0) {
+    const long q = B.gidx(fi, fj, fk);
+    B.jac[p] = B.jac[q];
+    for (int r = 0; r < 9; ++r) B.metric[r * P + p] = B.metric[r * P + q];
+    return;
+  }
+  B.jac[p] = jac;
+  double *m = B.metric.data();
+  m[0 * P + p] = (dyd2 * dzd3 - dyd3 * dzd2) / jac;
+  m[1 * P + p] = (dxd3 * dzd2 - dxd2 * dzd3) / jac;
+  m[2 * P + p] = (dxd2 * dyd3 - dxd3 * dyd2) / jac;
+  m[3 * P + p] = (dyd3 * dzd1 - dyd1 * dzd3) / jac;
+  m[4 * P + p] = (dxd1 * dzd3 - dxd3 * dzd1) / jac;
+  m[5 * P + p] = (dxd3 * dyd1 - dxd1 * dyd3) / jac;
+  m[6 * P + p] = (dyd1 * dzd2 - dyd2 * dzd1) / jac;
+  m[7 * P + p] = (dxd2 * dzd1 - dxd1 * dzd2) / jac;
+  m[8 * P + p] = (dxd1 * dyd2 - dxd2 * dyd1) / jac;
+}
+
+void compute_jac_metric(HostBlock &B) {
+  const int mx = B.mx, my = B.my, mz = B.mz, ngg = B.ngg;
+  for (int i = 1; i < mx - 1; ++i)
+    for (int j = 1; j < my - 1; ++j) {
+      int k0 = 1, k1 = mz - 1;
+      if (mz == 1) {
+        k0 = 0;
+        k1 = 1;
+      }
+      for (int k = k0; k < k1; ++k) metric_node(B, i, j, k, i, j, k);
+    }
+  for (int i = 1; i < mx - 1; ++i)
+    for (int j = 1; j < my - 1; ++j)
+      for (int k = 0; k >= -ngg; --k) metric_node(B, i, j, k, i, j, k + 1);
+  for (int i = 1; i < mx - 1; ++i)
+    for (int j = 1; j < my - 1; ++j)
+      for (int k = mz - 1; k < mz + ngg; ++k) metric_node(B, i, j, k, i, j, k - 1);
+  for (int i = 1; i < mx - 1; ++i)
+    for (int j = 0; j >= -ngg; --j)
+      for (int k = -ngg; k < mz + ngg; ++k) metric_node(B, i, j, k, i, j + 1, k);
+  for (int i = 1; i < mx - 1; ++i)
+    for (int j = my - 1; j < my + ngg; ++j)
+      for (int k = -ngg; k < mz + ngg; ++k) metric_node(B, i, j, k, i, j - 1, k);
+  for (int i = 0; i >= -ngg; --i)
+    for (int j = -ngg; j < my + ngg; ++j)
+      for (int k = -ngg; k < mz + ngg; ++k) metric_node(B, i, j, k, i + 1, j, k);
+  for (int i = mx - 1; i < mx + ngg; ++i)
+    for (int j = -ngg; j < my + ngg; ++j)
+      for (int k = -ngg; k < mz + ngg; ++k) metric_node(B, i, j, k, i - 1, j, k);
+}
+
+}  // namespace
+
+bool read_mesh(const std::string &dir, const Derived &d, HostMesh &mesh, std::string &err) {
+  const std::string gpath = dir + "/grid/grid   0.dat";
+  FILE *fp = std::fopen(gpath.c_str(), "rb");
+  if (!fp) {
+    err = "cannot open grid file " + gpath + " (binary grid, gridIsBinary = 1, is expected)";
+    return false;
+  }
+  int nblk = 0;
+  if (std::fread(&nblk, sizeof(int), 1, fp) != 1 || nblk <= 0 || nblk > 4096) {
+    std::fclose(fp);
+    err = "grid file: bad block count";
+    return false;
+  }
+  mesh.blocks.assign(nblk, HostBlock{});
+  for (auto &B : mesh.blocks) {
+    int dims[3];
+    if (std::fread(dims, sizeof(int), 3, fp) != 3 || dims[0] < 2 || dims[1] < 2 || dims[2] < 1) {
+      std::fclose(fp);
+      err = "grid file: bad block dimensions";
+      return false;
+    }
+    B.mx = dims[0];
+    B.my = dims[1];
+    B.mz = dims[2];
+    B.ngg = d.ngg;
+  }
+  mesh.dimension = mesh.blocks[0].mz == 1 ? 2 : 3;
+  for (auto &B : mesh.blocks) {
+    const int g = B.ngg + 1;
+    const long n = (long)(B.mx + 2 * g) * (B.my + 2 * g) * (B.mz + 2 * g);
+    B.x.assign(n, 0.0);
+    B.y.assign(n, 0.0);
+    B.z.assign(n, 0.0);
+    const long N = (long)B.mx * B.my * B.mz;
+    std::vector<double> buf(N);
+    std::vector<double> *dst[3] = {&B.x, &B.y, &B.z};
+    for (int q = 0; q < 3; ++q) {
+      if (std::fread(buf.data(), sizeof(double), N, fp) != (size_t)N) {
+        std::fclose(fp);
+        err = "grid file: truncated coordinates";
+        return false;
+      }
+      for (int k = 0; k < B.mz; ++k)
+        for (int j = 0; j < B.my; ++j)
+          for (int i = 0; i < B.mx; ++i) (*dst[q])[B.cidx(i, j, k)] = buf[((long)k * B.my + j) * B.mx + i];
+    }
+  }
+  std::fclose(fp);
+
+  // boundary file (Mesh.cpp:790-810)
+  {
+    const std::string bpath = dir + "/boundary_condition/boundary   0.txt";
+    std::ifstream bf(bpath);
+    if (!bf) {
+      err = "cannot open " + bpath;
+      return false;
+    }
+    std::string input;
+    for (auto &B : mesh.blocks) {
+      if (!std::getline(bf, input)) {
+        err = "boundary file: missing face count";
+        return false;
+      }
+      const int n = std::stoi(input);
+      for (int f = 0; f < n; ++f) {
+        std::getline(bf, input);
+        std::istringstream line(input);
+        BcFace b;
+        line >> b.rs[0] >> b.re[0] >> b.rs[1] >> b.re[1] >> b.rs[2] >> b.re[2] >> b.label;
+        if (!line) {
+          err = "boundary file: malformed face line";
+          return false;
+        }
+        // every device access of a face kernel derives from these ranges: reject anything that
+        // is not a whole-face or sub-face range of this block's nodes
+        const int ext[3] = {B.mx, B.my, B.mz};
+        bool ok = false;
+        for (int q = 0; q < mesh.dimension; ++q) {
+          const int lo = std::min(b.rs[q], b.re[q]), hi = std::max(b.rs[q], b.re[q]);
+          if (lo < 0 || hi > ext[q] - 1) {
+            err = "boundary file: face range outside the block";
+            return false;
+          }
+          if (b.rs[q] == b.re[q] && (b.rs[q] == 0 || b.rs[q] == ext[q] - 1)) ok = true;
+        }
+        if (!ok || (mesh.dimension == 2 && (b.rs[2] != 0 || b.re[2] != 0))) {
+          err = "boundary file: a face must lie on a block side (one index fixed at 0 or m-1)";
+          return false;
+        }
+        for (int q = 0; q < 3; ++q)
+          if (ext[q] <= B.ngg + 1 && !(mesh.dimension == 2 && q == 2)) {
+            err = "block too small for the stencil (every extent must exceed ngg + 1)";
+            return false;
+          }
+        register_boundary(b, B.ngg, mesh.dimension);
+        B.faces.push_back(b);
+      }
+    }
+  }
+  // inner-face file (Mesh.cpp:812-844)
+  {
+    const std::string ipath = dir + "/boundary_condition/inner   0.txt";
+    std::ifstream inf(ipath);
+    if (inf) {
+      std::string input;
+      std::getline(inf, input);
+      for (size_t b = 0; b < mesh.blocks.size(); ++b) {
+        int n = 0;
+        inf >> n;
+        if (n != 0) {
+          err = "block interfaces (inner faces) are not supported by this build of the library";
+          return false;
+        }
+      }
+    }
+  }
+  // scale (Mesh.cpp:613-619, 877-891)
+  if (std::abs(d.grid_scale - 1.0) > 1e-15) {
+    for (auto &B : mesh.blocks) {
+      for (auto &v : B.x) v *= d.grid_scale;
+      for (auto &v : B.y) v *= d.grid_scale;
+      for (auto &v : B.z) v *= d.grid_scale;
+    }
+  }
+  for (auto &B : mesh.blocks) {
+    ghost_grid(B, mesh.dimension);
+    B.jac.assign(B.padded(), 0.0);
+    B.metric.assign(9 * B.padded(), 0.0);
+    compute_jac_metric(B);
+    for (int k = 0; k < B.mz; ++k)
+      for (int j = 0; j < B.my; ++j)
+        for (int i = 0; i < B.mx; ++i)
+          if (!(B.jac[B.gidx(i, j, k)] > 0)) {
+            err = "negative Jacobian at interior node (" + std::to_string(i) + "," + std::to_string(j) + "," +
+                  std::to_string(k) + ")";
+            return false;
+          }
+  }
+  return true;
+}
+
+namespace {
+double struct_real(const std::map<std::string, Setup::StructVal> &st, const char *k, double def) {
+  auto it = st.find(k);
+  if (it == st.end()) return def;
+  if (auto p = std::get_if<double>(&it->second)) return *p;
+  if (auto q = std::get_if<int>(&it->second)) return *q;
+  return def;
+}
+double sutherland_host(double t) { return 1.7894e-5 * std::pow(t / 288.16, 1.5) * (288.16 + 110) / (t + 110); }
+}  // namespace
+
+bool resolve_boundaries(const Setup &s, const Derived &, HostMesh &mesh, std::string &err) {
+  // label -> (type, struct name) from the setup's boundary_conditions structs, then default labels
+  std::map<int, std::pair<int, std::string>> lab;
+  static const std::map<std::string, int> tname{{"wall", kWall},          {"inflow", kInflow},
+                                                {"outflow", kOutflow},    {"symmetry", kSymmetry},
+                                                {"farfield", kFarfield},  {"subsonic_inflow", kSubsonicInflow},
+                                                {"back_pressure", kBackPressure}, {"periodic", kPeriodic}};
+  auto bcs = s.string_arrays.find("boundary_conditions");
+  if (bcs != s.string_arrays.end()) {
+    for (const auto &name : bcs->second) {
+      auto st = s.structs.find(name);
+      if (st == s.structs.end()) continue;
+      auto l = st->second.find("label");
+      auto t = st->second.find("type");
+      if (l == st->second.end() || t == st->second.end()) continue;
+      const int label = std::get<int>(l->second);
+      auto tt = tname.find(std::get<std::string>(t->second));
+      if (tt != tname.end() && !lab.count(label)) lab[label] = {tt->second, name};
+    }
+  }
+  for (auto &B : mesh.blocks)
+    for (auto &f : B.faces) {
+      auto it = lab.find(f.label);
+      f.type = it != lab.end() ? it->second.first : f.label;
+      if (f.type != kSymmetry && f.type != kFarfield && f.type != kOutflow && f.type != kPeriodic) {
+        err = "boundary label " + std::to_string(f.label) +
+              " maps to a type outside this path (supported: symmetry 3, farfield 4, outflow 6, periodic 8)";
+        return false;
+      }
+      if (f.type == kFarfield) {
+        if (it == lab.end()) {
+          err = "farfield label " + std::to_string(f.label) + " needs a struct in boundary_conditions";
+          return false;
+        }
+        const auto &st = s.structs.at(it->second.second);
+        // FarField::FarField (BoundCond.cpp:586-669), air
+        double mach = struct_real(st, "mach", -1), pressure = struct_real(st, "pressure", -1),
+               temperature = struct_real(st, "temperature", -1), velocity = struct_real(st, "velocity", 0),
+               density = struct_real(st, "density", -1), u = struct_real(st, "u", 1), v = struct_real(st, "v", 0),
+               w = struct_real(st, "w", 0), re = struct_real(st, "reynolds_number", -1);
+        const double mw = kMwAir, gamma = kGammaAir;
+        if (temperature < 0) temperature = pressure * mw / (density * kRu);
+        const double viscosity = sutherland_host(temperature);
+        const double c = std::sqrt(gamma * kRu / mw * temperature);
+        if (mach < 0) mach = velocity / c;
+        else velocity = mach * c;
+        u *= velocity;
+        v *= velocity;
+        w *= velocity;
+        if (pressure < 0) {
+          density = viscosity * re / velocity;
+          pressure = density * temperature * kRu / mw;
+        }
+        if (density < 0) density = pressure * mw / (kRu * temperature);
+        f.density = density;
+        f.u = u;
+        f.v = v;
+        f.w = w;
+        f.pressure = pressure;
+        f.temperature = temperature;
+        f.acoustic_speed = c;
+        f.gamma = gamma;
+        f.entropy = pressure / std::pow(density, gamma);
+        f.mw = mw;
+      }
+    }
+  return true;
+}
+
+std::vector<std::pair<int, int>> bc_order(const Setup &s, const HostMesh &mesh) {
+  // label order per type: first the labels named in boundary_conditions (in that order), then the
+  // remaining labels in order of first appearance (BoundCond.cu:163-258)
+  std::vector<int> seen;
+  for (const auto &B : mesh.blocks)
+    for (const auto &f : B.faces)
+      if (std::find(seen.begin(), seen.end(), f.label) == seen.end()) seen.push_back(f.label);
+  std::vector<int> ordered;
+  auto bcs = s.string_arrays.find("boundary_conditions");
+  if (bcs != s.string_arrays.end())
+    for (const auto &name : bcs->second) {
+      auto st = s.structs.find(name);
+      if (st == s.structs.end()) continue;
+      auto l = st->second.find("label");
+      if (l == st->second.end()) continue;
+      const int label = std::get<int>(l->second);
+      auto it = std::find(seen.begin(), seen.end(), label);
+      if (it != seen.end()) {
+        ordered.push_back(label);
+        seen.erase(it);
+      }
+    }
+  for (int l : seen) ordered.push_back(l);
+  static const int prio[] = {kFarfield, kOutflow, kBackPressure, kInflow, kSubsonicInflow, kSymmetry, kWall, kPeriodic};
+  std::vector<std::pair<int, int>> out;
+  for (size_t b = 0; b < mesh.blocks.size(); ++b) {
+    const auto &B = mesh.blocks[b];
+    for (int t : prio)
+      for (int label : ordered)
+        for (size_t f = 0; f < B.faces.size(); ++f)
+          if (B.faces[f].label == label && B.faces[f].type == t) out.emplace_back((int)b, (int)f);
+  }
+  return out;
+}
+
+}  // namespace ostc

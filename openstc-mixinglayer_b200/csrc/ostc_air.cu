@@ -1,0 +1,1316 @@
+// ostc_air.cu -- sm_100a kernels of the calorically-perfect-air RHS + SSP-RK3 path and the C ABI
+// (include/ostc.h) that drives them.
+//
+// Per RK stage the device work is (reference order in brackets, RK.cuh:112-174):
+//   k_cfl_dt           [local_time_step + min_of_arr x2 + D2H + update_dt_global] first stage only:
+//                      spectral radius, warp-shuffle min, one 64-bit atomicMin into a device scalar
+//   k_flux_x           [compute_convective_term_aweno_1D + CDSPart1D, x]: staged row tile, one face per thread
+//   k_flux_march<1|2>  [same, y and z]: each thread marches one column, coalesced across i, with a
+//                      per-thread ring of 2*ngg+1 nodes in shared memory (no halo re-reads)
+//   k_visc_update      [viscous_flux_fv/gv/hv + update_cv_and_bv_rk + update_physical_properties]
+//                      3-D tile, face fluxes staged in shared memory, RK combine and EOS fused
+//   k_bc_face          [apply_farfield/outflow/symmetry/periodic, in the reference priority order]
+// The three RK stages ping-pong over three state buffers (A -> B -> C -> A) so no stage overwrites
+// data another block still reads; buffer A doubles as q^n (RK.cuh:99-102 needs no copy).
+#include "air_math.cuh"
+#include "host.h"
+#include "ostc.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace ostc {
+
+struct DevBlock {
+  int mx, my, mz, g, gz, pitch, sy, sz;
+  long long plane, off0, n;
+  const double *met, *jac;
+  __host__ __device__ __forceinline__ long long id(int i, int j, int k) const {
+    return off0 + ((long long)k * sy + j) * pitch + i;
+  }
+  __host__ __device__ __forceinline__ long long iq(int i, int j, int k) const {
+    return ((long long)k * my + j) * mx + i;
+  }
+};
+
+struct DevState {
+  double *cv, *bv, *mul;
+};
+
+struct DevFace {
+  int type, face, direction, rs[3], re[3];
+  double density, u, v, w, pressure, temperature, acoustic_speed, gamma, entropy;
+};
+
+__device__ __forceinline__ void cv_from_bv_node(const DevBlock &b, DevState s, long long p) {
+  // compute_cv_from_bv_1_point + compute_total_energy<Air> (FieldOperation.cuh:17-38,78-105)
+  const long long P = b.plane;
+  const double rho = s.bv[p], u = s.bv[P + p], v = s.bv[2 * P + p], w = s.bv[3 * P + p];
+  s.cv[p] = rho;
+  s.cv[P + p] = rho * u;
+  s.cv[2 * P + p] = rho * v;
+  s.cv[3 * P + p] = rho * w;
+  const double V2 = u * u + v * v + w * w;
+  double te = 0.5 * V2;
+  te *= rho;
+  te += s.bv[4 * P + p] / (kGamma - 1);
+  s.cv[4 * P + p] = te;
+}
+
+// ------------------------------------------------------------------------------ time step
+
+__global__ void k_dt_reset(unsigned long long *dtbits) { *dtbits = (unsigned long long)__double_as_longlong(1e6); }
+
+// local_time_step<Air, Laminar> (TimeAdvanceFunc.cuh:28-83) fused with the global minimum of
+// global_time_step (TimeAdvanceFunc.cu:39-64).  Positive doubles order like their bit patterns, so
+// the minimum is one 64-bit atomicMin per block after a warp-shuffle reduction.
+__global__ void __launch_bounds__(256) k_cfl_dt(DevBlock b, DevState s, double cfl, double prandtl, int dim3,
+                                                unsigned long long *dtbits) {
+  double local = 1e6;
+  const long long P = b.plane;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % b.mx);
+    const long long r = n / b.mx;
+    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const long long p = b.id(i, j, k);
+    double m[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) m[q] = b.met[q * P + p];
+    const double gx = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+    const double ge = sqrt(m[3] * m[3] + m[4] * m[4] + m[5] * m[5]);
+    const double gz = sqrt(m[6] * m[6] + m[7] * m[7] + m[8] * m[8]);
+    const double u = s.bv[P + p], v = s.bv[2 * P + p], w = s.bv[3 * P + p];
+    const double U = u * m[0] + v * m[1] + w * m[2];
+    const double V = u * m[3] + v * m[4] + w * m[5];
+    const double W = u * m[6] + v * m[7] + w * m[8];
+    const double a = sqrt(kGamma * kRuD * s.bv[5 * P + p] / kMwD);
+    const double s0 = fabs(U) + a * gx, s1 = fabs(V) + a * ge;
+    const double s2 = dim3 ? fabs(W) + a * gz : 0.0;
+    const double sinv = s0 + s1 + s2;
+    const double c1 = fmax(kGamma, 4.0 / 3.0) / s.bv[p];
+    const double c2 = s.mul[p] / prandtl;
+    double sv = gx * gx + ge * ge;
+    if (dim3) sv += gz * gz;
+    sv *= c1 * c2;
+    local = fmin(local, cfl / (sinv + sv));
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) local = fmin(local, __shfl_xor_sync(0xffffffffu, local, off));
+  __shared__ double wmin[8];
+  if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = local;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = wmin[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmin(m, wmin[w]);
+    atomicMin(dtbits, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+// ------------------------------------------------------------------------------ inviscid flux
+
+// x sweep.  A block of 128 threads stages 127 + 2*NG nodes of one (j,k) row in shared memory
+// (coalesced along i), computes the 128 faces i0-1/2 .. i0+126+1/2 (one per thread) and finalises
+// the 127 nodes between them: dq = -(fc(i+1/2) - fc(i-1/2)) + central correction.
+template <int NG, int RS, typename T>
+__global__ void __launch_bounds__(128) k_flux_x(DevBlock b, DevState s, double *__restrict__ dq) {
+  constexpr int L = 127;
+  constexpr int NP = L + 2 * NG;
+  __shared__ T sq[6][NP];
+  __shared__ T sf[5][NP];
+  __shared__ T sm[4][NP];
+  __shared__ T sfc[5][128];
+  const int t = threadIdx.x;
+  const int i0 = blockIdx.x * L;
+  const int j = blockIdx.y, k = blockIdx.z;
+  const long long P = b.plane;
+  const long long base = b.id(0, j, k);
+  for (int n = t; n < NP; n += 128) {
+    const int i = i0 - NG + n;
+    if (i < b.mx + NG) {
+      const long long p = base + i;
+      T bb[5], kk[3];
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        sq[l][n] = (T)s.cv[l * P + p];
+        bb[l] = (T)s.bv[l * P + p];
+      }
+      sq[5][n] = bb[4];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        kk[c] = (T)b.met[c * P + p];
+        sm[c][n] = kk[c];
+      }
+      const T jj = (T)b.jac[p];
+      sm[3][n] = jj;
+      T f[5];
+      node_flux<T>(bb, (T)s.cv[4 * P + p], kk, jj, f);
+#pragma unroll
+      for (int l = 0; l < 5; ++l) sf[l][n] = f[l];
+    }
+  }
+  __syncthreads();
+  const int face = i0 - 1 + t;
+  if (face < b.mx) {
+    auto q = [&](int st, int v) -> T { return sq[v][t + st]; };
+    const T mt0[3] = {sm[0][t + NG - 1], sm[1][t + NG - 1], sm[2][t + NG - 1]};
+    const T mt1[3] = {sm[0][t + NG], sm[1][t + NG], sm[2][t + NG]};
+    T fc[5];
+    aweno_face_flux<NG, RS, T>(q, mt0, mt1, sm[3][t + NG - 1], sm[3][t + NG], fc);
+#pragma unroll
+    for (int l = 0; l < 5; ++l) sfc[l][t] = fc[l];
+  }
+  __syncthreads();
+  const int i = i0 - 1 + t;
+  if (t >= 1 && i < b.mx) {
+    const long long qi = b.iq(i, j, k);
+    const int c = t - 1 + NG;  // staged index of node i
+    auto f = [&](int m, int l) -> T { return sf[l][c + m]; };
+    const bool cds = i < b.mx - 2 * NG;
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+      double d = 0.0;
+      d -= (double)(sfc[l][t] - sfc[l][t - 1]);
+      if (cds) d += (double)cds_correction<NG, T>(f, l);
+      dq[l * b.n + qi] = d;
+    }
+  }
+}
+
+// y (DIR = 1) or z (DIR = 2) sweep.  Thread (i, o) marches nodes c = s0..s1-1 of its column (o is
+// k for y, j for z); warps are contiguous in i, so every load of a new node is coalesced.  The
+// per-thread ring in shared memory keeps the last 2*NG+1 nodes: cv(5), p, node flux(5), metric
+// row(3), Jacobian.  Segments of `seg` nodes split long columns across blocks.
+template <int DIR, int NG, int RS, typename T>
+__global__ void __launch_bounds__(64) k_flux_march(DevBlock b, DevState s, double *__restrict__ dq, int seg) {
+  constexpr int W = 2 * NG + 1;
+  constexpr int NV = 15;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T *ring = reinterpret_cast<T *>(smraw);
+  const int nthr = blockDim.x * blockDim.y;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int o = blockIdx.y * blockDim.y + threadIdx.y;
+  const int n_dir = DIR == 1 ? b.my : b.mz;
+  const int n_o = DIR == 1 ? b.mz : b.my;
+  if (i >= b.mx || o >= n_o) return;
+  const int s0 = blockIdx.z * seg;
+  if (s0 >= n_dir) return;
+  const int s1 = min(s0 + seg, n_dir);
+  const long long P = b.plane;
+  const long long stride = DIR == 1 ? (long long)b.pitch : (long long)b.pitch * b.sy;
+  const long long base = DIR == 1 ? b.id(i, 0, o) : b.id(i, o, 0);
+  auto R = [&](int slot, int v) -> T & { return ring[(slot * NV + v) * nthr + tid]; };
+  auto load = [&](int n) {
+    const long long p = base + (long long)n * stride;
+    const int slot = (n + NG) % W;
+    T bb[5], kk[3];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+      R(slot, l) = (T)s.cv[l * P + p];
+      bb[l] = (T)s.bv[l * P + p];
+    }
+    R(slot, 5) = bb[4];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      kk[c] = (T)b.met[(DIR * 3 + c) * P + p];
+      R(slot, 11 + c) = kk[c];
+    }
+    const T jj = (T)b.jac[p];
+    R(slot, 14) = jj;
+    T f[5];
+    node_flux<T>(bb, (T)s.cv[4 * P + p], kk, jj, f);
+#pragma unroll
+    for (int l = 0; l < 5; ++l) R(slot, 6 + l) = f[l];
+  };
+  for (int n = s0 - NG; n <= s0 + NG - 2; ++n) load(n);
+  T fprev[5] = {T(0), T(0), T(0), T(0), T(0)};
+  for (int c = s0 - 1; c < s1; ++c) {
+    load(c + NG);
+    const int b0 = (c + 1) % W;
+    auto q = [&](int st, int v) -> T {
+      int sl = b0 + st;
+      sl = sl >= W ? sl - W : sl;
+      return R(sl, v);
+    };
+    const int sc = (c + NG) % W, sc1 = (c + 1 + NG) % W;
+    const T mt0[3] = {R(sc, 11), R(sc, 12), R(sc, 13)};
+    const T mt1[3] = {R(sc1, 11), R(sc1, 12), R(sc1, 13)};
+    T fc[5];
+    aweno_face_flux<NG, RS, T>(q, mt0, mt1, R(sc, 14), R(sc1, 14), fc);
+    if (c >= s0) {
+      const long long qi = DIR == 1 ? b.iq(i, c, o) : b.iq(i, o, c);
+      const bool cds = c < n_dir - 2 * NG;
+      auto f = [&](int m, int l) -> T { return R((c + m + NG + W) % W, 6 + l); };
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        double d = dq[l * b.n + qi];
+        d -= (double)(fc[l] - fprev[l]);
+        if (cds) d += (double)cds_correction<NG, T>(f, l);
+        dq[l * b.n + qi] = d;
+      }
+    }
+#pragma unroll
+    for (int l = 0; l < 5; ++l) fprev[l] = fc[l];
+  }
+}
+
+// ------------------------------------------------------------------------------ viscous + update
+
+// compute_fv/gv/hv_2nd_order<Air, Laminar> (ViscousScheme.cuh:24-911): viscous flux through the face
+// between node (i,j,k) and its neighbour in direction d; fv[0..3] = components 1..4 (component 0 is 0).
+template <typename T, bool DIM3>
+__device__ __forceinline__ void viscous_face(const DevBlock &b, const DevState &s, double prandtl, int i, int j,
+                                             int k, int d, T *fv) {
+  const long long P = b.plane;
+  const long long st[3] = {1, b.pitch, (long long)b.pitch * b.sy};
+  const long long p0 = b.id(i, j, k), p1 = p0 + st[d];
+  T m[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) m[r] = T(0.5) * ((T)b.met[r * P + p0] + (T)b.met[r * P + p1]);
+  const int vars[4] = {1, 2, 3, 5};
+  T gx[4], gy[4], gz[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const double *B = s.bv + vars[q] * P;
+    T g[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (c == d) {
+        g[c] = (T)B[p1] - (T)B[p0];
+      } else if (c == 2 && !DIM3) {
+        g[c] = T(0);
+      } else {
+        const long long sc = st[c];
+        g[c] = T(0.25) * ((T)B[p0 + sc] - (T)B[p0 - sc] + (T)B[p1 + sc] - (T)B[p1 - sc]);
+      }
+    }
+    gx[q] = g[0] * m[0] + g[1] * m[3] + g[2] * m[6];
+    gy[q] = g[0] * m[1] + g[1] * m[4] + g[2] * m[7];
+    gz[q] = g[0] * m[2] + g[1] * m[5] + g[2] * m[8];
+  }
+  const T u_x = gx[0], u_y = gy[0], u_z = gz[0];
+  const T v_x = gx[1], v_y = gy[1], v_z = gz[1];
+  const T w_x = gx[2], w_y = gy[2], w_z = gz[2];
+  const T mul = T(0.5) * ((T)s.mul[p0] + (T)s.mul[p1]);
+  const T txx = mul * (T(4) * u_x - T(2) * v_y - T(2) * w_z) / T(3.0);
+  const T tyy = mul * (T(4) * v_y - T(2) * u_x - T(2) * w_z) / T(3.0);
+  const T tzz = mul * (T(4) * w_z - T(2) * u_x - T(2) * v_y) / T(3.0);
+  const T txy = mul * (u_y + v_x);
+  const T txz = mul * (u_z + w_x);
+  const T tyz = mul * (v_z + w_y);
+  const T j0 = (T)b.jac[p0], j1 = (T)b.jac[p1];
+  const T nx = T(0.5) * ((T)b.met[(d * 3 + 0) * P + p0] * j0 + (T)b.met[(d * 3 + 0) * P + p1] * j1);
+  const T ny = T(0.5) * ((T)b.met[(d * 3 + 1) * P + p0] * j0 + (T)b.met[(d * 3 + 1) * P + p1] * j1);
+  const T nz = T(0.5) * ((T)b.met[(d * 3 + 2) * P + p0] * j0 + (T)b.met[(d * 3 + 2) * P + p1] * j1);
+  fv[0] = nx * txx + ny * txy + nz * txz;
+  fv[1] = nx * txy + ny * tyy + nz * tyz;
+  fv[2] = nx * txz + ny * tyz + nz * tzz;
+  const T um = T(0.5) * ((T)s.bv[P + p0] + (T)s.bv[P + p1]);
+  const T vm = T(0.5) * ((T)s.bv[2 * P + p0] + (T)s.bv[2 * P + p1]);
+  const T wm = T(0.5) * ((T)s.bv[3 * P + p0] + (T)s.bv[3 * P + p1]);
+  const T cp = T(kGamma * kRuD / kMwD / (kGamma - 1));
+  const T cond = (mul / (T)prandtl) * cp;
+  fv[3] = um * fv[0] + vm * fv[1] + wm * fv[2] + cond * (nx * gx[3] + ny * gy[3] + nz * gz[3]);
+}
+
+struct StageArgs {
+  DevState in, qn, out;
+  double a, bcoef, c;
+  const double *dt;
+  double prandtl;
+  int viscous, update;
+  unsigned *flags;
+};
+
+// Viscous fluxes of all directions (viscous_flux_fv/gv/hv, SchemeSelector.cuh:69-154), then the
+// SSP-RK3 combine, EOS and Sutherland viscosity of the new state (update_cv_and_bv_rk, RK.cuh:230-284;
+// update_physical_properties<Air>, FieldOperation.cuh:107-140).  Tile TX x TY x TZ; every face flux
+// is computed once into shared memory.
+template <typename T, bool DIM3, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(TX *TY *TZ) k_visc_update(DevBlock b, StageArgs a, double *__restrict__ dq) {
+  __shared__ T fx[TZ][TY][TX + 1][4];
+  __shared__ T fy[TZ][TY + 1][TX][4];
+  __shared__ T fz[DIM3 ? TZ + 1 : 1][TY][TX][4];
+  const int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
+  const int i = blockIdx.x * TX + tx, j = blockIdx.y * TY + ty, k = blockIdx.z * TZ + tz;
+  const bool inside = i < b.mx && j < b.my && k < b.mz;
+  if (a.viscous && inside) {
+    viscous_face<T, DIM3>(b, a.in, a.prandtl, i - 1, j, k, 0, fx[tz][ty][tx]);
+    if (tx == TX - 1 || i == b.mx - 1) viscous_face<T, DIM3>(b, a.in, a.prandtl, i, j, k, 0, fx[tz][ty][tx + 1]);
+    viscous_face<T, DIM3>(b, a.in, a.prandtl, i, j - 1, k, 1, fy[tz][ty][tx]);
+    if (ty == TY - 1 || j == b.my - 1) viscous_face<T, DIM3>(b, a.in, a.prandtl, i, j, k, 1, fy[tz][ty + 1][tx]);
+    if constexpr (DIM3) {
+      viscous_face<T, DIM3>(b, a.in, a.prandtl, i, j, k - 1, 2, fz[tz][ty][tx]);
+      if (tz == TZ - 1 || k == b.mz - 1) viscous_face<T, DIM3>(b, a.in, a.prandtl, i, j, k, 2, fz[tz + 1][ty][tx]);
+    }
+  }
+  __syncthreads();
+  if (!inside) return;
+  const long long qi = b.iq(i, j, k);
+  double d[5];
+#pragma unroll
+  for (int l = 0; l < 5; ++l) d[l] = dq[l * b.n + qi];
+  if (a.viscous) {
+#pragma unroll
+    for (int l = 1; l < 5; ++l) d[l] += (double)(fx[tz][ty][tx + 1][l - 1] - fx[tz][ty][tx][l - 1]);
+#pragma unroll
+    for (int l = 1; l < 5; ++l) d[l] += (double)(fy[tz][ty + 1][tx][l - 1] - fy[tz][ty][tx][l - 1]);
+    if constexpr (DIM3) {
+#pragma unroll
+      for (int l = 1; l < 5; ++l) d[l] += (double)(fz[tz + 1][ty][tx][l - 1] - fz[tz][ty][tx][l - 1]);
+    }
+  }
+  if (!a.update) {
+#pragma unroll
+    for (int l = 0; l < 5; ++l) dq[l * b.n + qi] = d[l];
+    return;
+  }
+  const long long P = b.plane, p = b.id(i, j, k);
+  const double dt = *a.dt;
+  const double dtj = dt / b.jac[p];
+  double cv[5];
+#pragma unroll
+  for (int l = 0; l < 5; ++l) cv[l] = a.a * a.qn.cv[l * P + p] + a.bcoef * a.in.cv[l * P + p] + a.c * dtj * d[l];
+  if (!DIM3) cv[3] = 0;
+  const double rho = cv[0];
+  const double di = 1.0 / cv[0];
+  const double u = cv[1] * di, v = cv[2] * di, w = cv[3] * di;
+  const double V2 = u * u + v * v + w * w;
+  const double pr = (kGamma - 1) * (cv[4] - 0.5 * rho * V2);
+  const double tt = pr * kMwD * di / kRuD;
+#pragma unroll
+  for (int l = 0; l < 5; ++l) a.out.cv[l * P + p] = cv[l];
+  a.out.bv[p] = rho;
+  a.out.bv[P + p] = u;
+  a.out.bv[2 * P + p] = v;
+  a.out.bv[3 * P + p] = w;
+  a.out.bv[4 * P + p] = pr;
+  a.out.bv[5 * P + p] = tt;
+  a.out.mul[p] = sutherland(tt);
+  if (!(rho > 0.0) || !(pr > 0.0) || !(tt > 0.0)) atomicOr(a.flags, (unsigned)OSTC_FLAG_NONPOSITIVE);
+  if (isnan(cv[0]) || isnan(cv[1]) || isnan(cv[2]) || isnan(cv[3]) || isnan(cv[4]))
+    atomicOr(a.flags, (unsigned)OSTC_FLAG_NAN);
+}
+
+// ------------------------------------------------------------------------------ boundaries
+
+__device__ __forceinline__ void copy_bv(const DevBlock &b, DevState s, long long dst, long long src) {
+#pragma unroll
+  for (int l = 0; l < 6; ++l) s.bv[l * b.plane + dst] = s.bv[l * b.plane + src];
+}
+
+__device__ __forceinline__ void finish_node(const DevBlock &b, DevState s, long long p) {
+  cv_from_bv_node(b, s, p);
+  s.mul[p] = sutherland(s.bv[5 * b.plane + p]);
+}
+
+// One boundary face: apply_symmetry / apply_outflow / apply_periodic / apply_farfield<Air>
+// (BoundCond.cuh:137-233, 755-1022, 1443-1486).  Threads cover the two tangential index ranges,
+// which include ngg ghost layers on each side (Mesh.cpp:14-32).
+__global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace f) {
+  const int t0 = f.face == 0 ? 1 : 0;
+  const int t1 = f.face == 2 ? 1 : 2;
+  const int n0 = f.re[t0] - f.rs[t0] + 1, n1 = f.re[t1] - f.rs[t1] + 1;
+  const long long nn = (long long)n0 * n1;
+  const long long P = b.plane;
+  const long long st[3] = {1, b.pitch, (long long)b.pitch * b.sy};
+  int dir[3] = {0, 0, 0};
+  dir[f.face] = f.direction;
+  const long long dstep = dir[0] * st[0] + dir[1] * st[1] + dir[2] * st[2];
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += (long long)gridDim.x * blockDim.x) {
+    int idx[3];
+    idx[f.face] = f.rs[f.face];
+    idx[t0] = f.rs[t0] + (int)(n % n0);
+    idx[t1] = f.rs[t1] + (int)(n / n0);
+    const long long pb = b.id(idx[0], idx[1], idx[2]);
+    if (f.type == kSymmetry) {
+      const long long pin = pb - dstep;
+      double kx = b.met[(f.face * 3 + 0) * P + pb], ky = b.met[(f.face * 3 + 1) * P + pb],
+             kz = b.met[(f.face * 3 + 2) * P + pb];
+      const double km = sqrt(kx * kx + ky * ky + kz * kz);
+      kx /= km;
+      ky /= km;
+      kz /= km;
+      const double u1 = s.bv[P + pin], v1 = s.bv[2 * P + pin], w1 = s.bv[3 * P + pin];
+      double uk = kx * u1 + ky * v1 + kz * w1;
+      s.bv[P + pb] = u1 - kx * uk;
+      s.bv[2 * P + pb] = v1 - ky * uk;
+      s.bv[3 * P + pb] = w1 - kz * uk;
+      s.bv[pb] = s.bv[pin];
+      s.bv[4 * P + pb] = s.bv[4 * P + pin];
+      s.bv[5 * P + pb] = s.bv[5 * P + pin];
+      s.mul[pb] = sutherland(s.bv[5 * P + pb]);
+      for (int g = 1; g <= b.g; ++g) {
+        const long long pg = pb + g * dstep, pi = pb - g * dstep;
+        s.bv[pg] = s.bv[pi];
+        const double u = s.bv[P + pi], v = s.bv[2 * P + pi], w = s.bv[3 * P + pi];
+        uk = kx * u + ky * v + kz * w;
+        s.bv[P + pg] = u - 2 * uk * kx;
+        s.bv[2 * P + pg] = v - 2 * uk * ky;
+        s.bv[3 * P + pg] = w - 2 * uk * kz;
+        s.bv[4 * P + pg] = s.bv[4 * P + pi];
+        s.bv[5 * P + pg] = s.bv[5 * P + pi];
+        finish_node(b, s, pg);
+      }
+    } else if (f.type == kOutflow) {
+      for (int g = 1; g <= b.g; ++g) {
+        const long long pg = pb + g * dstep;
+        copy_bv(b, s, pg, pb);
+        finish_node(b, s, pg);
+      }
+    } else if (f.type == kPeriodic) {
+      const int ext[3] = {b.mx, b.my, b.mz};
+      int other[3] = {idx[0], idx[1], idx[2]};
+      other[f.face] = f.direction < 0 ? ext[f.face] - 1 : 0;
+      const long long po = b.id(other[0], other[1], other[2]);
+      for (int g = 1; g <= b.g; ++g) {
+        const long long pg = pb + g * dstep, ps = po + g * dstep;
+        copy_bv(b, s, pg, ps);
+        finish_node(b, s, pg);
+      }
+    } else if (f.type == kFarfield) {
+      double nx = b.met[(f.face * 3 + 0) * P + pb], ny = b.met[(f.face * 3 + 1) * P + pb],
+             nz = b.met[(f.face * 3 + 2) * P + pb];
+      const double gni = f.direction / sqrt(nx * nx + ny * ny + nz * nz);
+      nx *= gni;
+      ny *= gni;
+      nz *= gni;
+      const double ub = s.bv[P + pb], vb = s.bv[2 * P + pb], wb = s.bv[3 * P + pb];
+      const double uf = nx * ub + ny * vb + nz * wb;
+      const double pbv = s.bv[4 * P + pb], rb = s.bv[pb];
+      const double ab = sqrt(kGamma * pbv / rb);
+      const double mb = uf / ab;
+      double vals[6];
+      if (mb <= -1) {
+        vals[0] = f.density; vals[1] = f.u; vals[2] = f.v; vals[3] = f.w; vals[4] = f.pressure; vals[5] = f.temperature;
+      } else if (mb >= 1) {
+        for (int g = 1; g <= b.g; ++g) {
+          const long long pg = pb + g * dstep;
+          copy_bv(b, s, pg, pb);
+          finish_node(b, s, pg);
+        }
+        continue;
+      } else {
+        const double rpos = uf + 2 * ab / (kGamma - 1);
+        const double uinf = f.u * nx + f.v * ny + f.w * nz;
+        const double rneg = uinf - 2 * f.acoustic_speed / (f.gamma - 1);
+        const double Un = 0.5 * (rpos + rneg);
+        const double cb = 0.25 * (kGamma - 1) * (rpos - rneg);
+        double sb;
+        if (mb <= 0) {
+          sb = f.entropy;
+          vals[1] = f.u + (Un - uinf) * nx;
+          vals[2] = f.v + (Un - uinf) * ny;
+          vals[3] = f.w + (Un - uinf) * nz;
+        } else {
+          sb = pbv / pow(rb, kGamma);
+          vals[1] = ub + (Un - uf) * nx;
+          vals[2] = vb + (Un - uf) * ny;
+          vals[3] = wb + (Un - uf) * nz;
+        }
+        vals[0] = pow(cb * cb / (kGamma * sb), 1 / (kGamma - 1));
+        vals[4] = vals[0] * cb * cb / kGamma;
+        vals[5] = vals[4] * kMwD / (vals[0] * kRuD);
+      }
+#pragma unroll
+      for (int l = 0; l < 6; ++l) s.bv[l * P + pb] = vals[l];
+      finish_node(b, s, pb);
+      for (int g = 1; g <= b.g; ++g) {
+        const long long pg = pb + g * dstep;
+#pragma unroll
+        for (int l = 0; l < 6; ++l) s.bv[l * P + pg] = vals[l];
+        finish_node(b, s, pg);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------ set-up kernels
+
+// interior [nv][N] (i fastest) <-> padded planes
+__global__ void k_scatter(DevBlock b, const double *__restrict__ src, double *__restrict__ dst, int nv) {
+  const long long tot = b.n * nv;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < tot; n += (long long)gridDim.x * blockDim.x) {
+    const int l = (int)(n / b.n);
+    const long long r = n - (long long)l * b.n;
+    const int i = (int)(r % b.mx);
+    const long long r2 = r / b.mx;
+    const int j = (int)(r2 % b.my), k = (int)(r2 / b.my);
+    dst[l * b.plane + b.id(i, j, k)] = src[n];
+  }
+}
+
+__global__ void k_gather(DevBlock b, const double *__restrict__ src, double *__restrict__ dst, int nv) {
+  const long long tot = b.n * nv;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < tot; n += (long long)gridDim.x * blockDim.x) {
+    const int l = (int)(n / b.n);
+    const long long r = n - (long long)l * b.n;
+    const int i = (int)(r % b.mx);
+    const long long r2 = r / b.mx;
+    const int j = (int)(r2 % b.my), k = (int)(r2 / b.my);
+    dst[n] = src[l * b.plane + b.id(i, j, k)];
+  }
+}
+
+// cv <- bv and mu <- Sutherland(T) over the whole padded block (update_physical_properties and
+// compute_cv_from_bv over ghosts, Driver.cu:186-191, RK.cuh:37-45)
+__global__ void k_init_fields(DevBlock b, DevState s) {
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < b.plane; p += (long long)gridDim.x * blockDim.x) {
+    finish_node(b, s, p);
+  }
+}
+
+// residual snapshot and squared differences (store_last_step, compute_square_of_dbv,
+// TimeAdvanceFunc.cu:6-37) reduced with warp shuffles into 4 sums.
+__global__ void k_store_last(DevBlock b, DevState s, double *last) {
+  const long long P = b.plane;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % b.mx);
+    const long long r = n / b.mx;
+    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const long long p = b.id(i, j, k);
+    const double u = s.bv[P + p], v = s.bv[2 * P + p], w = s.bv[3 * P + p];
+    last[n] = s.bv[p];
+    last[b.n + n] = sqrt(u * u + v * v + w * w);
+    last[2 * b.n + n] = s.bv[4 * P + p];
+    last[3 * b.n + n] = s.bv[5 * P + p];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_residual(DevBlock b, DevState s, const double *last, double *sums) {
+  const long long P = b.plane;
+  double acc[4] = {0, 0, 0, 0};
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % b.mx);
+    const long long r = n / b.mx;
+    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const long long p = b.id(i, j, k);
+    const double u = s.bv[P + p], v = s.bv[2 * P + p], w = s.bv[3 * P + p];
+    const double d0 = s.bv[p] - last[n];
+    const double d1 = sqrt(u * u + v * v + w * w) - last[b.n + n];
+    const double d2 = s.bv[4 * P + p] - last[2 * b.n + n];
+    const double d3 = s.bv[5 * P + p] - last[3 * b.n + n];
+    acc[0] += d0 * d0;
+    acc[1] += d1 * d1;
+    acc[2] += d2 * d2;
+    acc[3] += d3 * d3;
+  }
+  __shared__ double red[8][4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+  if ((threadIdx.x & 31) == 0)
+    for (int q = 0; q < 4; ++q) red[threadIdx.x >> 5][q] = acc[q];
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w][threadIdx.x];
+    atomicAdd(&sums[threadIdx.x], t);
+  }
+}
+
+__global__ void k_step_end(double *t, const double *dt, long long *step) {
+  *t += *dt;
+  *step += 1;
+}
+
+__global__ void k_dt_decode(const unsigned long long *bits, double *dt) { *dt = __longlong_as_double((long long)*bits); }
+
+}  // namespace ostc
+
+// ================================================================================= C ABI
+
+using namespace ostc;
+
+struct BlockRes {
+  DevBlock db{};
+  double *met = nullptr, *jac = nullptr;
+  double *cv[3]{}, *bv[3]{}, *mul[3]{};
+  double *dq = nullptr;
+  double *last = nullptr;
+  std::vector<DevFace> faces;  // file order
+};
+
+struct ostc_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Setup setup;
+  Derived der;
+  HostMesh mesh;
+  std::vector<BlockRes> blk;
+  std::vector<std::pair<int, int>> order;
+  int precision = OSTC_PREC_FP64;
+  bool state_set = false, initialised = false;
+  std::vector<char> block_set;
+  unsigned long long *d_dtbits = nullptr;
+  double *d_dt = nullptr, *d_time = nullptr, *d_sums = nullptr, *d_staging = nullptr;
+  long long *d_step = nullptr;
+  unsigned *d_flags = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int graph_precision = -1;
+  std::string err;
+  int sm_count = 148;
+  // timing (ostc_profile_steps)
+  bool timing = false;
+  struct Fam {
+    const char *name;
+    int launches;
+    double ms;
+  };
+  std::vector<Fam> fams;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+  std::vector<std::pair<int, size_t>> ev_used;
+};
+
+static std::string g_create_error;
+
+#define CK(call)                                                                                         \
+  do {                                                                                                   \
+    cudaError_t e_ = (call);                                                                             \
+    if (e_ != cudaSuccess) {                                                                             \
+      ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);                                      \
+      return OSTC_ECUDA;                                                                                 \
+    }                                                                                                    \
+  } while (0)
+
+namespace {
+
+int fam_index(ostc_ctx *ctx, const char *name) {
+  for (size_t i = 0; i < ctx->fams.size(); ++i)
+    if (std::strcmp(ctx->fams[i].name, name) == 0) return (int)i;
+  ctx->fams.push_back({name, 0, 0.0});
+  return (int)ctx->fams.size() - 1;
+}
+
+// Records a begin event for a kernel family when timing is on; returns a token for end_t.
+long begin_t(ostc_ctx *ctx, const char *name) {
+  if (!ctx->timing) return -1;
+  const size_t slot = ctx->ev_used.size();
+  if (slot >= ctx->ev_pool.size()) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    ctx->ev_pool.emplace_back(a, b);
+  }
+  ctx->ev_used.emplace_back(fam_index(ctx, name), slot);
+  cudaEventRecord(ctx->ev_pool[slot].first, ctx->stream);
+  return (long)slot;
+}
+void end_t(ostc_ctx *ctx, long tok) {
+  if (tok < 0) return;
+  cudaEventRecord(ctx->ev_pool[tok].second, ctx->stream);
+}
+
+int grid_for(ostc_ctx *ctx, long long n, int tpb) {
+  long long g = (n + tpb - 1) / tpb;
+  const long long cap = (long long)ctx->sm_count * 16;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+// inviscid sweep of one block
+template <typename T>
+int launch_flux(ostc_ctx *ctx, BlockRes &B, DevState in) {
+  const DevBlock &b = B.db;
+  const int ng = ctx->der.ngg, rs = ctx->der.inviscid_scheme;
+  const bool is3d = b.mz > 1;
+  // x
+  {
+    dim3 grid((b.mx + 126) / 127, b.my, b.mz);
+    long tok = begin_t(ctx, "flux_x");
+    if (ng == 3 && rs == 3) k_flux_x<3, 3, T><<<grid, 128, 0, ctx->stream>>>(b, in, B.dq);
+    else if (ng == 3) k_flux_x<3, 4, T><<<grid, 128, 0, ctx->stream>>>(b, in, B.dq);
+    else if (rs == 3) k_flux_x<4, 3, T><<<grid, 128, 0, ctx->stream>>>(b, in, B.dq);
+    else k_flux_x<4, 4, T><<<grid, 128, 0, ctx->stream>>>(b, in, B.dq);
+    end_t(ctx, tok);
+  }
+  // y and z
+  for (int dir = 1; dir <= (is3d ? 2 : 1); ++dir) {
+    const int n_dir = dir == 1 ? b.my : b.mz, n_o = dir == 1 ? b.mz : b.my;
+    // split columns into segments so that the grid fills the GPU at least ~4 waves deep
+    const long long cols = (long long)((b.mx + 31) / 32) * ((n_o + 1) / 2);
+    int nseg = (int)std::max<long long>(1, (ctx->sm_count * 12 + cols - 1) / cols);
+    int seg = std::max(2 * ng, (n_dir + nseg - 1) / nseg);
+    nseg = (n_dir + seg - 1) / seg;
+    dim3 grid((b.mx + 31) / 32, (n_o + 1) / 2, nseg);
+    dim3 block(32, 2, 1);
+    const size_t smem = (size_t)(2 * ng + 1) * 15 * 64 * sizeof(T);
+    long tok = begin_t(ctx, dir == 1 ? "flux_y" : "flux_z");
+#define OSTC_MARCH(D, N, R) k_flux_march<D, N, R, T><<<grid, block, smem, ctx->stream>>>(b, in, B.dq, seg)
+    if (dir == 1) {
+      if (ng == 3 && rs == 3) OSTC_MARCH(1, 3, 3);
+      else if (ng == 3) OSTC_MARCH(1, 3, 4);
+      else if (rs == 3) OSTC_MARCH(1, 4, 3);
+      else OSTC_MARCH(1, 4, 4);
+    } else {
+      if (ng == 3 && rs == 3) OSTC_MARCH(2, 3, 3);
+      else if (ng == 3) OSTC_MARCH(2, 3, 4);
+      else if (rs == 3) OSTC_MARCH(2, 4, 3);
+      else OSTC_MARCH(2, 4, 4);
+    }
+#undef OSTC_MARCH
+    end_t(ctx, tok);
+  }
+  return OSTC_OK;
+}
+
+template <typename T>
+void launch_visc(ostc_ctx *ctx, BlockRes &B, const StageArgs &a) {
+  const DevBlock &b = B.db;
+  long tok = begin_t(ctx, "visc_update");
+  if (b.mz > 1) {
+    dim3 grid((b.mx + 31) / 32, (b.my + 3) / 4, (b.mz + 1) / 2);
+    k_visc_update<T, true, 32, 4, 2><<<grid, dim3(32, 4, 2), 0, ctx->stream>>>(b, a, B.dq);
+  } else {
+    dim3 grid((b.mx + 31) / 32, (b.my + 7) / 8, 1);
+    k_visc_update<T, false, 32, 8, 1><<<grid, dim3(32, 8, 1), 0, ctx->stream>>>(b, a, B.dq);
+  }
+  end_t(ctx, tok);
+}
+
+void launch_bcs(ostc_ctx *ctx, int block, DevState out) {
+  for (const auto &bf : ctx->order) {
+    if (bf.first != block) continue;
+    BlockRes &B = ctx->blk[block];
+    const DevFace &f = B.faces[bf.second];
+    const int t0 = f.face == 0 ? 1 : 0, t1 = f.face == 2 ? 1 : 2;
+    const long long nn = (long long)(f.re[t0] - f.rs[t0] + 1) * (f.re[t1] - f.rs[t1] + 1);
+    long tok = begin_t(ctx, "bc_face");
+    k_bc_face<<<grid_for(ctx, nn, 128), 128, 0, ctx->stream>>>(B.db, out, f);
+    end_t(ctx, tok);
+  }
+}
+
+DevState state_of(BlockRes &B, int s) { return DevState{B.cv[s], B.bv[s], B.mul[s]}; }
+
+// The march kernels stage up to 2*ngg+1 nodes x 15 values x 64 threads in dynamic shared memory
+// (up to 69 KB in FP64); raise the per-kernel limit once, outside any stream capture.
+template <typename T>
+bool set_march_attrs() {
+  bool ok = true;
+  auto set = [&](const void *fn, int ng) {
+    const int bytes = (2 * ng + 1) * 15 * 64 * (int)sizeof(T);
+    ok = ok && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+  };
+  set((const void *)k_flux_march<1, 3, 3, T>, 3);
+  set((const void *)k_flux_march<1, 3, 4, T>, 3);
+  set((const void *)k_flux_march<1, 4, 3, T>, 4);
+  set((const void *)k_flux_march<1, 4, 4, T>, 4);
+  set((const void *)k_flux_march<2, 3, 3, T>, 3);
+  set((const void *)k_flux_march<2, 3, 4, T>, 3);
+  set((const void *)k_flux_march<2, 4, 3, T>, 4);
+  set((const void *)k_flux_march<2, 4, 4, T>, 4);
+  return ok;
+}
+
+int initialise(ostc_ctx *ctx) {
+  // Driver::initialize_computation (Driver.cu:115-199): BCs, properties, then cv <- bv (RK.cuh:37-45)
+  for (size_t b = 0; b < ctx->blk.size(); ++b) launch_bcs(ctx, (int)b, state_of(ctx->blk[b], 0));
+  for (auto &B : ctx->blk)
+    k_init_fields<<<grid_for(ctx, B.db.plane, 256), 256, 0, ctx->stream>>>(B.db, state_of(B, 0));
+  CK(cudaGetLastError());
+  ctx->initialised = true;
+  return OSTC_OK;
+}
+
+// One SSP-RK3 step over all blocks (RK.cuh:85-185).
+template <typename T>
+int enqueue_step(ostc_ctx *ctx) {
+  static const double A[3] = {1.0, 0.75, 1.0 / 3.0}, Bc[3] = {0.0, 0.25, 2.0 / 3.0}, C[3] = {1.0, 0.25, 2.0 / 3.0};
+  const bool fixed = ctx->der.fixed_time_step;
+  for (int rk = 0; rk < 3; ++rk) {
+    const int sin = rk, sout = (rk + 1) % 3;
+    if (rk == 0 && !fixed) {
+      long tok = begin_t(ctx, "cfl_dt");
+      k_dt_reset<<<1, 1, 0, ctx->stream>>>(ctx->d_dtbits);
+      for (auto &B : ctx->blk)
+        k_cfl_dt<<<grid_for(ctx, B.db.n, 256), 256, 0, ctx->stream>>>(B.db, state_of(B, sin), ctx->der.cfl,
+                                                                     ctx->der.prandtl, B.db.mz > 1, ctx->d_dtbits);
+      k_dt_decode<<<1, 1, 0, ctx->stream>>>(ctx->d_dtbits, ctx->d_dt);
+      end_t(ctx, tok);
+    }
+    for (size_t bi = 0; bi < ctx->blk.size(); ++bi) {
+      BlockRes &B = ctx->blk[bi];
+      launch_flux<T>(ctx, B, state_of(B, sin));
+      StageArgs a{};
+      a.in = state_of(B, sin);
+      a.qn = state_of(B, 0);
+      a.out = state_of(B, sout);
+      a.a = A[rk];
+      a.bcoef = Bc[rk];
+      a.c = C[rk];
+      a.dt = ctx->d_dt;
+      a.prandtl = ctx->der.prandtl;
+      a.viscous = ctx->der.viscous_order != 0;
+      a.update = 1;
+      a.flags = ctx->d_flags;
+      launch_visc<T>(ctx, B, a);
+      launch_bcs(ctx, (int)bi, state_of(B, sout));
+    }
+  }
+  k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->d_time, ctx->d_dt, ctx->d_step);
+  return OSTC_OK;
+}
+
+int enqueue_step_any(ostc_ctx *ctx) {
+  return ctx->precision == OSTC_PREC_MIXED ? enqueue_step<float>(ctx) : enqueue_step<double>(ctx);
+}
+
+int check_ready(ostc_ctx *ctx) {
+  if (!ctx->state_set) {
+    ctx->err = "no state: call ostc_set_state for every block first";
+    return OSTC_ESTATE;
+  }
+  for (char c : ctx->block_set)
+    if (!c) {
+      ctx->err = "ostc_set_state was not called for every block";
+      return OSTC_ESTATE;
+    }
+  if (!ctx->initialised) return initialise(ctx);
+  return OSTC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_ctx **out) {
+  if (!out || !input_dir) {
+    g_create_error = "ostc_create: null argument";
+    return OSTC_EINVAL;
+  }
+  *out = nullptr;
+  auto ctx = std::make_unique<ostc_ctx>();
+  ctx->device = device;
+  ctx->setup.set_defaults();
+  std::string err;
+  const std::string dir(input_dir);
+  const std::string sp = setup_txt && *setup_txt ? std::string(setup_txt) : dir + "/setup.txt";
+  if (!ctx->setup.read_file(sp, err) || !derive(ctx->setup, ctx->der, err) ||
+      !read_mesh(dir, ctx->der, ctx->mesh, err) || !resolve_boundaries(ctx->setup, ctx->der, ctx->mesh, err)) {
+    g_create_error = err;
+    return err.find("cannot open") != std::string::npos || err.find("grid file") != std::string::npos ||
+                   err.find("file:") != std::string::npos
+               ? OSTC_EIO
+               : OSTC_EINVAL;
+  }
+  ctx->order = bc_order(ctx->setup, ctx->mesh);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    g_create_error = "no CUDA device " + std::to_string(device) + " available";
+    return OSTC_ECUDA;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) {
+    g_create_error = "cudaSetDevice failed";
+    return OSTC_ECUDA;
+  }
+  cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (!set_march_attrs<double>() || !set_march_attrs<float>()) {
+    g_create_error = "cudaFuncSetAttribute (dynamic shared memory) failed";
+    return OSTC_ECUDA;
+  }
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    g_create_error = "cudaStreamCreate failed";
+    return OSTC_ECUDA;
+  }
+  const bool is3d = ctx->mesh.dimension == 3;
+  size_t max_n = 0;
+  for (auto &HB : ctx->mesh.blocks) {
+    BlockRes R;
+    DevBlock &b = R.db;
+    b.mx = HB.mx;
+    b.my = HB.my;
+    b.mz = HB.mz;
+    b.g = HB.ngg;
+    b.gz = is3d ? HB.ngg : 0;
+    b.pitch = ((HB.mx + 2 * b.g) + 7) / 8 * 8;
+    b.sy = HB.my + 2 * b.g;
+    b.sz = HB.mz + 2 * b.gz;
+    b.plane = (long long)b.pitch * b.sy * b.sz;
+    b.off0 = ((long long)b.gz * b.sy + b.g) * b.pitch + b.g;
+    b.n = (long long)HB.mx * HB.my * HB.mz;
+    max_n = std::max<size_t>(max_n, (size_t)b.n);
+    auto alloc = [&](double **p, size_t n) -> bool {
+      if (cudaMalloc(p, n * sizeof(double)) != cudaSuccess) return false;
+      return cudaMemset(*p, 0, n * sizeof(double)) == cudaSuccess;
+    };
+    bool ok = alloc(&R.met, 9 * b.plane) && alloc(&R.jac, b.plane) && alloc(&R.dq, 5 * b.n) && alloc(&R.last, 4 * b.n);
+    for (int s = 0; s < 3 && ok; ++s) ok = alloc(&R.cv[s], 5 * b.plane) && alloc(&R.bv[s], 6 * b.plane) && alloc(&R.mul[s], b.plane);
+    if (!ok) {
+      g_create_error = "device allocation failed";
+      ctx->blk.push_back(R);
+      ostc_destroy(ctx.release());
+      return OSTC_ENOMEM;
+    }
+    // metric/Jacobian: host arrays have ngg ghosts in every direction; copy the device part
+    std::vector<double> hm(9 * b.plane, 0.0), hj(b.plane, 0.0);
+    const long HP = HB.padded();
+    for (int k = -b.gz; k < b.mz + b.gz; ++k)
+      for (int j = -b.g; j < b.my + b.g; ++j)
+        for (int i = -b.g; i < b.mx + b.g; ++i) {
+          const long long d = b.id(i, j, k);
+          const long h = HB.gidx(i, j, k);
+          hj[d] = HB.jac[h];
+          for (int r = 0; r < 9; ++r) hm[r * b.plane + d] = HB.metric[r * HP + h];
+        }
+    cudaMemcpy(R.met, hm.data(), hm.size() * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(R.jac, hj.data(), hj.size() * sizeof(double), cudaMemcpyHostToDevice);
+    b.met = R.met;
+    b.jac = R.jac;
+    for (auto &hf : HB.faces) {
+      DevFace f{};
+      f.type = hf.type;
+      f.face = hf.face;
+      f.direction = hf.direction;
+      for (int q = 0; q < 3; ++q) {
+        f.rs[q] = hf.rs[q];
+        f.re[q] = hf.re[q];
+      }
+      if (!is3d) {
+        f.rs[2] = 0;
+        f.re[2] = 0;
+      }
+      f.density = hf.density;
+      f.u = hf.u;
+      f.v = hf.v;
+      f.w = hf.w;
+      f.pressure = hf.pressure;
+      f.temperature = hf.temperature;
+      f.acoustic_speed = hf.acoustic_speed;
+      f.gamma = hf.gamma;
+      f.entropy = hf.entropy;
+      R.faces.push_back(f);
+    }
+    ctx->blk.push_back(R);
+  }
+  ctx->block_set.assign(ctx->blk.size(), 0);
+  bool ok = cudaMalloc(&ctx->d_dtbits, sizeof(unsigned long long)) == cudaSuccess &&
+            cudaMalloc(&ctx->d_dt, sizeof(double)) == cudaSuccess && cudaMalloc(&ctx->d_time, sizeof(double)) == cudaSuccess &&
+            cudaMalloc(&ctx->d_sums, 4 * sizeof(double)) == cudaSuccess &&
+            cudaMalloc(&ctx->d_step, sizeof(long long)) == cudaSuccess &&
+            cudaMalloc(&ctx->d_flags, sizeof(unsigned)) == cudaSuccess &&
+            cudaMalloc(&ctx->d_staging, 6 * max_n * sizeof(double)) == cudaSuccess;
+  if (!ok) {
+    g_create_error = "device allocation failed";
+    ostc_destroy(ctx.release());
+    return OSTC_ENOMEM;
+  }
+  const double dt0 = ctx->der.fixed_time_step ? ctx->der.dt : 1e6;
+  cudaMemcpy(ctx->d_dt, &dt0, sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemset(ctx->d_time, 0, sizeof(double));
+  cudaMemset(ctx->d_step, 0, sizeof(long long));
+  cudaMemset(ctx->d_flags, 0, sizeof(unsigned));
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    g_create_error = "device set-up failed";
+    ostc_destroy(ctx.release());
+    return OSTC_ECUDA;
+  }
+  *out = ctx.release();
+  return OSTC_OK;
+}
+
+void ostc_destroy(ostc_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+  for (auto &B : ctx->blk) {
+    cudaFree(B.met);
+    cudaFree(B.jac);
+    cudaFree(B.dq);
+    cudaFree(B.last);
+    for (int s = 0; s < 3; ++s) {
+      cudaFree(B.cv[s]);
+      cudaFree(B.bv[s]);
+      cudaFree(B.mul[s]);
+    }
+  }
+  cudaFree(ctx->d_dtbits);
+  cudaFree(ctx->d_dt);
+  cudaFree(ctx->d_time);
+  cudaFree(ctx->d_sums);
+  cudaFree(ctx->d_step);
+  cudaFree(ctx->d_flags);
+  cudaFree(ctx->d_staging);
+  for (auto &e : ctx->ev_pool) {
+    cudaEventDestroy(e.first);
+    cudaEventDestroy(e.second);
+  }
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char *ostc_last_error(const ostc_ctx *ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+int ostc_n_blocks(const ostc_ctx *ctx, int *n) {
+  if (!ctx || !n) return OSTC_EINVAL;
+  *n = (int)ctx->blk.size();
+  return OSTC_OK;
+}
+
+int ostc_block_dims(const ostc_ctx *ctx, int block, int dims[4]) {
+  if (!ctx || !dims || block < 0 || block >= (int)ctx->blk.size()) return OSTC_EINVAL;
+  const DevBlock &b = ctx->blk[block].db;
+  dims[0] = b.mx;
+  dims[1] = b.my;
+  dims[2] = b.mz;
+  dims[3] = b.g;
+  return OSTC_OK;
+}
+
+int ostc_n_var(const ostc_ctx *ctx, int *n_var, int *n_scalar) {
+  if (!ctx) return OSTC_EINVAL;
+  if (n_var) *n_var = ctx->der.n_var;
+  if (n_scalar) *n_scalar = ctx->der.n_scalar;
+  return OSTC_OK;
+}
+
+int ostc_total_nodes(const ostc_ctx *ctx, long long *n) {
+  if (!ctx || !n) return OSTC_EINVAL;
+  long long t = 0;
+  for (auto &B : ctx->blk) t += B.db.n;
+  *n = t;
+  return OSTC_OK;
+}
+
+int ostc_set_precision(ostc_ctx *ctx, int mode) {
+  if (!ctx) return OSTC_EINVAL;
+  if (mode != OSTC_PREC_FP64 && mode != OSTC_PREC_MIXED) {
+    ctx->err = "unknown precision mode";
+    return OSTC_EINVAL;
+  }
+  ctx->precision = mode;
+  return OSTC_OK;
+}
+
+int ostc_set_state(ostc_ctx *ctx, int block, const double *bv, const double *sv, int ptr_kind) {
+  if (!ctx || !bv || block < 0 || block >= (int)ctx->blk.size()) return OSTC_EINVAL;
+  (void)sv;
+  cudaSetDevice(ctx->device);
+  BlockRes &B = ctx->blk[block];
+  const size_t bytes = 6 * (size_t)B.db.n * sizeof(double);
+  CK(cudaMemcpyAsync(ctx->d_staging, bv, bytes, ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                     ctx->stream));
+  for (int s = 0; s < 3; ++s) {
+    CK(cudaMemsetAsync(B.bv[s], 0, 6 * B.db.plane * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(B.cv[s], 0, 5 * B.db.plane * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(B.mul[s], 0, B.db.plane * sizeof(double), ctx->stream));
+  }
+  k_scatter<<<grid_for(ctx, 6 * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, ctx->d_staging, B.bv[0], 6);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->block_set[block] = 1;
+  ctx->state_set = true;
+  ctx->initialised = false;
+  CK(cudaMemsetAsync(ctx->d_time, 0, sizeof(double), ctx->stream));
+  return OSTC_OK;
+}
+
+int ostc_get_state(ostc_ctx *ctx, int block, double *cv, double *bv, double *sv, int ptr_kind) {
+  if (!ctx || block < 0 || block >= (int)ctx->blk.size()) return OSTC_EINVAL;
+  (void)sv;
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  BlockRes &B = ctx->blk[block];
+  const auto kind = ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (cv) {
+    k_gather<<<grid_for(ctx, 5 * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, B.cv[0], ctx->d_staging, 5);
+    CK(cudaMemcpyAsync(cv, ctx->d_staging, 5 * B.db.n * sizeof(double), kind, ctx->stream));
+  }
+  if (bv) {
+    k_gather<<<grid_for(ctx, 6 * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, B.bv[0], ctx->d_staging, 6);
+    CK(cudaMemcpyAsync(bv, ctx->d_staging, 6 * B.db.n * sizeof(double), kind, ctx->stream));
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  return OSTC_OK;
+}
+
+int ostc_rhs(ostc_ctx *ctx, int block, unsigned mask, double *dq, int ptr_kind) {
+  if (!ctx || !dq || block < 0 || block >= (int)ctx->blk.size()) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  BlockRes &B = ctx->blk[block];
+  CK(cudaMemsetAsync(B.dq, 0, 5 * B.db.n * sizeof(double), ctx->stream));
+  const bool mixed = ctx->precision == OSTC_PREC_MIXED;
+  if (mask & OSTC_TERM_INVISCID) {
+    if (mixed) launch_flux<float>(ctx, B, state_of(B, 0));
+    else launch_flux<double>(ctx, B, state_of(B, 0));
+  }
+  if ((mask & OSTC_TERM_VISCOUS) && ctx->der.viscous_order != 0) {
+    StageArgs a{};
+    a.in = state_of(B, 0);
+    a.qn = a.in;
+    a.out = a.in;
+    a.prandtl = ctx->der.prandtl;
+    a.viscous = 1;
+    a.update = 0;
+    a.flags = ctx->d_flags;
+    a.dt = ctx->d_dt;
+    if (mixed) launch_visc<float>(ctx, B, a);
+    else launch_visc<double>(ctx, B, a);
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(dq, B.dq, 5 * B.db.n * sizeof(double),
+                     ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return OSTC_OK;
+}
+
+int ostc_rk3_step(ostc_ctx *ctx, int n_steps, double *dt_last) {
+  if (!ctx || n_steps < 0) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  if (!ctx->graph || ctx->graph_precision != ctx->precision) {
+    if (ctx->graph) {
+      cudaGraphExecDestroy(ctx->graph);
+      ctx->graph = nullptr;
+    }
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_step_any(ctx);
+    CK(cudaStreamEndCapture(ctx->stream, &g));
+    CK(cudaGraphInstantiate(&ctx->graph, g, 0));
+    cudaGraphDestroy(g);
+    ctx->graph_precision = ctx->precision;
+  }
+  for (int s = 0; s < n_steps; ++s) CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+  if (dt_last) {
+    CK(cudaMemcpyAsync(dt_last, ctx->d_dt, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  return OSTC_OK;
+}
+
+int ostc_physical_time(ostc_ctx *ctx, double *t) {
+  if (!ctx || !t) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  CK(cudaMemcpyAsync(t, ctx->d_time, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return OSTC_OK;
+}
+
+int ostc_store_residual_reference(ostc_ctx *ctx) {
+  if (!ctx) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  for (auto &B : ctx->blk)
+    k_store_last<<<grid_for(ctx, B.db.n, 256), 256, 0, ctx->stream>>>(B.db, state_of(B, 0), B.last);
+  CK(cudaGetLastError());
+  return OSTC_OK;
+}
+
+int ostc_residual(ostc_ctx *ctx, double res[4]) {
+  if (!ctx || !res) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  CK(cudaMemsetAsync(ctx->d_sums, 0, 4 * sizeof(double), ctx->stream));
+  long long tot = 0;
+  for (auto &B : ctx->blk) {
+    k_residual<<<grid_for(ctx, B.db.n, 256), 256, 0, ctx->stream>>>(B.db, state_of(B, 0), B.last, ctx->d_sums);
+    tot += B.db.n;
+  }
+  CK(cudaGetLastError());
+  double h[4];
+  CK(cudaMemcpyAsync(h, ctx->d_sums, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int l = 0; l < 4; ++l) res[l] = std::sqrt(h[l] / (double)tot);
+  return OSTC_OK;
+}
+
+int ostc_error_flags(ostc_ctx *ctx, unsigned *flags) {
+  if (!ctx || !flags) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  CK(cudaMemcpyAsync(flags, ctx->d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_flags, 0, sizeof(unsigned), ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return OSTC_OK;
+}
+
+int ostc_device_view(ostc_ctx *ctx, int block, ostc_zone_view *v) {
+  if (!ctx || !v || block < 0 || block >= (int)ctx->blk.size()) return OSTC_EINVAL;
+  BlockRes &B = ctx->blk[block];
+  const DevBlock &b = B.db;
+  v->mx = b.mx;
+  v->my = b.my;
+  v->mz = b.mz;
+  v->ngg = b.g;
+  v->gz = b.gz;
+  v->pitch = b.pitch;
+  v->sy = b.sy;
+  v->sz = b.sz;
+  v->plane = b.plane;
+  v->cv = B.cv[0];
+  v->bv = B.bv[0];
+  v->mul = B.mul[0];
+  v->metric = B.met;
+  v->jac = B.jac;
+  return OSTC_OK;
+}
+
+int ostc_probe_case(const char *setup_txt, const char *input_dir, int out[16], char *msg, int msg_len) {
+  if (!input_dir || !out) return OSTC_EINVAL;
+  Setup setup;
+  setup.set_defaults();
+  Derived der;
+  HostMesh mesh;
+  std::string err;
+  const std::string dir(input_dir);
+  const std::string sp = setup_txt && *setup_txt ? std::string(setup_txt) : dir + "/setup.txt";
+  int rc = OSTC_OK;
+  if (!setup.read_file(sp, err)) rc = OSTC_EIO;
+  else if (!derive(setup, der, err)) rc = OSTC_EINVAL;
+  else if (!read_mesh(dir, der, mesh, err)) rc = err.find("cannot open") != std::string::npos ? OSTC_EIO : OSTC_EINVAL;
+  else if (!resolve_boundaries(setup, der, mesh, err)) rc = OSTC_EINVAL;
+  if (rc != OSTC_OK) {
+    if (msg && msg_len > 0) {
+      std::strncpy(msg, err.c_str(), (size_t)msg_len - 1);
+      msg[msg_len - 1] = 0;
+    }
+    return rc;
+  }
+  const auto order = bc_order(setup, mesh);
+  const HostBlock &B = mesh.blocks[0];
+  const int vals[14] = {der.ngg, der.inviscid_type, der.n_var, der.n_scalar, (int)mesh.blocks.size(), mesh.dimension,
+                        B.mx, B.my, B.mz, (int)B.faces.size(), der.reconstruction, der.inviscid_scheme,
+                        der.viscous_order, (int)order.size()};
+  for (int i = 0; i < 14; ++i) out[i] = vals[i];
+  return OSTC_OK;
+}
+
+int ostc_profile_steps(ostc_ctx *ctx, int n_steps, int max, const char **names, int *launches, double *ms) {
+  if (!ctx || n_steps < 0) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  ctx->fams.clear();
+  ctx->ev_used.clear();
+  ctx->timing = true;
+  for (int s = 0; s < n_steps; ++s) enqueue_step_any(ctx);
+  ctx->timing = false;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (auto &u : ctx->ev_used) {
+    float t = 0;
+    cudaEventElapsedTime(&t, ctx->ev_pool[u.second].first, ctx->ev_pool[u.second].second);
+    ctx->fams[u.first].ms += t;
+    ctx->fams[u.first].launches += 1;
+  }
+  const int n = std::min<int>(max, (int)ctx->fams.size());
+  for (int i = 0; i < n; ++i) {
+    if (names) names[i] = ctx->fams[i].name;
+    if (launches) launches[i] = ctx->fams[i].launches;
+    if (ms) ms[i] = ctx->fams[i].ms;
+  }
+  return n;
+}
+
+}  // extern "C"

@@ -1,0 +1,210 @@
+"""ctypes binding of libostc_b200.so (include/ostc.h).
+
+This is the Python face of the C ABI for test harnesses and benchmarks; the library itself is C++ and
+CUDA.  Loading fails loudly when the shared library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent.parent
+LIB_PATH = PKG_DIR / "libostc_b200.so"
+
+OSTC_HOST, OSTC_DEVICE = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+TERM_INVISCID, TERM_VISCOUS, TERM_SOURCE, TERM_ALL = 1, 2, 4, 7
+FLAG_NONPOSITIVE, FLAG_NAN = 1, 2
+
+EXPORTS = [
+    "ostc_create", "ostc_destroy", "ostc_last_error", "ostc_n_blocks", "ostc_block_dims", "ostc_n_var",
+    "ostc_set_precision", "ostc_set_state", "ostc_get_state", "ostc_rhs", "ostc_rk3_step",
+    "ostc_physical_time", "ostc_store_residual_reference", "ostc_residual", "ostc_error_flags",
+    "ostc_device_view", "ostc_profile_steps", "ostc_total_nodes", "ostc_probe_case",
+]
+
+
+class OstcError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"ostc error {code}: {msg}")
+        self.code = code
+
+
+class ZoneView(ctypes.Structure):
+    _fields_ = [("mx", ctypes.c_int), ("my", ctypes.c_int), ("mz", ctypes.c_int), ("ngg", ctypes.c_int),
+                ("gz", ctypes.c_int), ("pitch", ctypes.c_int), ("sy", ctypes.c_int), ("sz", ctypes.c_int),
+                ("plane", ctypes.c_longlong), ("cv", ctypes.c_void_p), ("bv", ctypes.c_void_p),
+                ("mul", ctypes.c_void_p), ("metric", ctypes.c_void_p), ("jac", ctypes.c_void_p)]
+
+
+_lib = None
+
+
+def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
+    """Load libostc_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise OstcError(-100, f"{p} not built: run __graft_entry__.build() (nvcc for sm_100a)")
+    lib = ctypes.CDLL(str(p))
+    vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)
+    lib.ostc_create.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ip, ctypes.POINTER(vp)]
+    lib.ostc_destroy.argtypes = [vp]
+    lib.ostc_destroy.restype = None
+    lib.ostc_last_error.argtypes = [vp]
+    lib.ostc_last_error.restype = ctypes.c_char_p
+    lib.ostc_n_blocks.argtypes = [vp, ctypes.POINTER(ip)]
+    lib.ostc_block_dims.argtypes = [vp, ip, ctypes.POINTER(ip)]
+    lib.ostc_n_var.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
+    lib.ostc_set_precision.argtypes = [vp, ip]
+    lib.ostc_set_state.argtypes = [vp, ip, vp, vp, ip]
+    lib.ostc_get_state.argtypes = [vp, ip, vp, vp, vp, ip]
+    lib.ostc_rhs.argtypes = [vp, ip, ctypes.c_uint, vp, ip]
+    lib.ostc_rk3_step.argtypes = [vp, ip, dp]
+    lib.ostc_physical_time.argtypes = [vp, dp]
+    lib.ostc_store_residual_reference.argtypes = [vp]
+    lib.ostc_residual.argtypes = [vp, dp]
+    lib.ostc_error_flags.argtypes = [vp, ctypes.POINTER(ctypes.c_uint)]
+    lib.ostc_device_view.argtypes = [vp, ip, ctypes.POINTER(ZoneView)]
+    lib.ostc_profile_steps.argtypes = [vp, ip, ip, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ip), dp]
+    lib.ostc_total_nodes.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    lib.ostc_probe_case.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(ip), ctypes.c_char_p, ip]
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def probe_case(input_dir: str, setup: str | None = None) -> dict:
+    """Parse a case directory on the host only (no GPU): derived values the reference computes."""
+    lib = load_library()
+    out = (ctypes.c_int * 16)()
+    msg = ctypes.create_string_buffer(512)
+    rc = lib.ostc_probe_case((setup or "").encode(), str(input_dir).encode(), out, msg, 512)
+    if rc != 0:
+        raise OstcError(rc, msg.value.decode())
+    keys = ["ngg", "inviscid_type", "n_var", "n_scalar", "n_block", "dimension", "mx", "my", "mz",
+            "n_faces", "reconstruction", "inviscid_scheme", "viscous_order", "n_bc_launches"]
+    return {k: out[i] for i, k in enumerate(keys)}
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Solver:
+    """One library context on one GPU (RHS + SSP-RK3 for a reference-format case directory)."""
+
+    def __init__(self, input_dir: str, setup: str | None = None, device: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.ostc_create((setup or "").encode(), str(input_dir).encode(), device, ctypes.byref(h))
+        if rc != 0:
+            raise OstcError(rc, self.lib.ostc_last_error(None).decode())
+        self.h = h
+        n = ctypes.c_int()
+        self._check(self.lib.ostc_n_blocks(self.h, ctypes.byref(n)))
+        self.n_block = n.value
+        self.dims = []
+        for b in range(self.n_block):
+            d = (ctypes.c_int * 4)()
+            self._check(self.lib.ostc_block_dims(self.h, b, d))
+            self.dims.append(tuple(d))
+        nv, ns = ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.ostc_n_var(self.h, ctypes.byref(nv), ctypes.byref(ns)))
+        self.n_var, self.n_scalar = nv.value, ns.value
+
+    def _check(self, rc: int):
+        if rc < 0:
+            raise OstcError(rc, self.lib.ostc_last_error(self.h).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ostc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def shape(self, block: int = 0):
+        mx, my, mz, _ = self.dims[block]
+        return (mz, my, mx)
+
+    def set_precision(self, mode: int):
+        self._check(self.lib.ostc_set_precision(self.h, mode))
+
+    def set_state(self, bv: np.ndarray, block: int = 0, sv: np.ndarray | None = None):
+        bv = np.ascontiguousarray(bv, dtype=np.float64)
+        assert bv.shape == (6,) + self.shape(block), bv.shape
+        self._check(self.lib.ostc_set_state(self.h, block, _ptr(bv), None if sv is None else _ptr(sv), OSTC_HOST))
+
+    def set_state_ptr(self, bv_ptr: int, block: int = 0, kind: int = OSTC_HOST):
+        self._check(self.lib.ostc_set_state(self.h, block, ctypes.c_void_p(bv_ptr), None, kind))
+
+    def get_state(self, block: int = 0):
+        sh = self.shape(block)
+        cv = np.empty((self.n_var,) + sh)
+        bv = np.empty((6,) + sh)
+        self._check(self.lib.ostc_get_state(self.h, block, _ptr(cv), _ptr(bv), None, OSTC_HOST))
+        return cv, bv
+
+    def get_state_ptr(self, cv_ptr: int, bv_ptr: int, block: int = 0, kind: int = OSTC_HOST):
+        self._check(self.lib.ostc_get_state(self.h, block, ctypes.c_void_p(cv_ptr) if cv_ptr else None,
+                                            ctypes.c_void_p(bv_ptr) if bv_ptr else None, None, kind))
+
+    def rhs(self, mask: int = TERM_ALL, block: int = 0) -> np.ndarray:
+        dq = np.empty((self.n_var,) + self.shape(block))
+        self._check(self.lib.ostc_rhs(self.h, block, mask, _ptr(dq), OSTC_HOST))
+        return dq
+
+    def step(self, n: int = 1) -> float:
+        dt = ctypes.c_double()
+        self._check(self.lib.ostc_rk3_step(self.h, n, ctypes.byref(dt)))
+        return dt.value
+
+    def step_async(self, n: int = 1):
+        self._check(self.lib.ostc_rk3_step(self.h, n, None))
+
+    def time(self) -> float:
+        t = ctypes.c_double()
+        self._check(self.lib.ostc_physical_time(self.h, ctypes.byref(t)))
+        return t.value
+
+    def store_residual_reference(self):
+        self._check(self.lib.ostc_store_residual_reference(self.h))
+
+    def residual(self) -> np.ndarray:
+        r = (ctypes.c_double * 4)()
+        self._check(self.lib.ostc_residual(self.h, r))
+        return np.array(r[:])
+
+    def error_flags(self) -> int:
+        f = ctypes.c_uint()
+        self._check(self.lib.ostc_error_flags(self.h, ctypes.byref(f)))
+        return f.value
+
+    def device_view(self, block: int = 0) -> ZoneView:
+        v = ZoneView()
+        self._check(self.lib.ostc_device_view(self.h, block, ctypes.byref(v)))
+        return v
+
+    def total_nodes(self) -> int:
+        n = ctypes.c_longlong()
+        self._check(self.lib.ostc_total_nodes(self.h, ctypes.byref(n)))
+        return n.value
+
+    def profile(self, n_steps: int) -> dict:
+        mx = 32
+        names = (ctypes.c_char_p * mx)()
+        launches = (ctypes.c_int * mx)()
+        ms = (ctypes.c_double * mx)()
+        k = self._check(self.lib.ostc_profile_steps(self.h, n_steps, mx, names, launches, ms))
+        return {names[i].decode(): (launches[i], ms[i]) for i in range(k)}

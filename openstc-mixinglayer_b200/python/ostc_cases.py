@@ -1,0 +1,240 @@
+"""Synthetic mixing-layer cases in the reference's input format.
+
+A case is a single-block grid, a list of boundary faces, a setup.txt and a seeded initial primitive
+state.  `write_case` lays them out exactly as the reference reads them:
+  <dir>/setup.txt                                  (Parameter::read_one_file grammar)
+  <dir>/grid/grid   0.dat                          (binary: nblk, mx my mz, x[] y[] z[]; Mesh.cpp:663-697)
+  <dir>/boundary_condition/boundary   0.txt        (face count, then "x1 x2 y1 y2 z1 z2 label"; Mesh.cpp:790-810)
+  <dir>/boundary_condition/inner   0.txt           (no interfaces)
+The named workloads follow the benchmark configurations: a 2-D temporal mixing layer (256 x 128
+cells, WENO5-Z + AUSM+, periodic x, slip walls in y) and a 3-D one (512 x 256 x 128, WENO7-Z + HLLC,
+periodic x and z, far-field y).  All inputs are synthetic and seeded.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import os
+from pathlib import Path
+
+import numpy as np
+
+GAMMA = 1.4
+R_U = 8314.462618
+MW_AIR = 28.9647
+R_AIR = R_U / MW_AIR
+
+
+def sutherland(t):
+    return 1.7894e-5 * (t / 288.16) ** 1.5 * (288.16 + 110) / (t + 110)
+
+
+@dataclasses.dataclass
+class Face:
+    raw: tuple  # x1 x2 y1 y2 z1 z2 (0-based node indices)
+    label: int
+
+
+@dataclasses.dataclass
+class Case:
+    name: str
+    mx: int
+    my: int
+    mz: int
+    x: np.ndarray  # [mz, my, mx] grid units
+    y: np.ndarray
+    z: np.ndarray
+    grid_scale: float
+    faces: list
+    bc_structs: dict  # name -> {key: (type, value)}
+    scheme: dict      # reconstruction, inviscid_scheme, viscous_order, cfl, prandtl_number
+    bv: np.ndarray    # [6, mz, my, mx] initial primitive state
+    steps: int = 100
+
+    @property
+    def nodes(self) -> int:
+        return self.mx * self.my * self.mz
+
+    def setup_text(self) -> str:
+        s = self.scheme
+        lines = [
+            "// synthetic temporal mixing layer",
+            "bool parallel = 0",
+            "int problem_type = 0",
+            "int mesh_file_type = 0",
+            "int gridIsBinary = 1",
+            f"real gridScale = {self.grid_scale!r}",
+            "int initial = 1",
+            f"int total_step = {self.steps}",
+            "int output_file = 1000000",
+            "int output_screen = 1000000",
+            "bool steady = 0",
+            "int temporal_scheme = 3",
+            f"real cfl = {s['cfl']!r}",
+            "bool fixed_time_step = 0",
+            "real dt = 1e-8",
+            f"int reconstruction = {s['reconstruction']}",
+            f"int inviscid_scheme = {s['inviscid_scheme']}",
+            f"int viscous_order = {s['viscous_order']}",
+            f"real prandtl_number = {s['prandtl_number']!r}",
+            "int species = 0",
+            "int reaction = 0",
+            "bool turbulence = 0",
+            "bool limit_flow = 0",
+            "array string boundary_conditions {",
+            "    " + " ".join(self.bc_structs.keys()),
+            "}",
+        ]
+        for name, st in self.bc_structs.items():
+            lines.append(f"struct {name} = {{")
+            for k, (t, v) in st.items():
+                lines.append(f"    {t} {k} = {v!r}" if t == "real" else f"    {t} {k} = {v}")
+            lines.append("}")
+        return "\n".join(lines) + "\n"
+
+    def farfield_states(self):
+        """FarField ctor for air (BoundCond.cpp:586-669): label -> state dict."""
+        out = {}
+        for name, st in self.bc_structs.items():
+            if st.get("type", (None, None))[1] != "farfield":
+                continue
+            g = {k: v for k, (t, v) in st.items()}
+            mach, p, t = g.get("mach", -1.0), g.get("pressure", -1.0), g.get("temperature", -1.0)
+            u, v, w = g.get("u", 1.0), g.get("v", 0.0), g.get("w", 0.0)
+            c = math.sqrt(GAMMA * R_U / MW_AIR * t)
+            vel = mach * c
+            rho = p * MW_AIR / (R_U * t)
+            out[g["label"]] = dict(density=rho, u=u * vel, v=v * vel, w=w * vel, pressure=p, temperature=t,
+                                   acoustic_speed=c, gamma=GAMMA, entropy=p / rho ** GAMMA, mw=MW_AIR)
+        return out
+
+    def label_types(self):
+        types = {"symmetry": 3, "farfield": 4, "outflow": 6, "periodic": 8}
+        m = {}
+        for st in self.bc_structs.values():
+            m[st["label"][1]] = types[st["type"][1]]
+        return m
+
+
+def write_case(case: Case, directory: os.PathLike) -> Path:
+    d = Path(directory)
+    (d / "grid").mkdir(parents=True, exist_ok=True)
+    (d / "boundary_condition").mkdir(parents=True, exist_ok=True)
+    (d / "setup.txt").write_text(case.setup_text())
+    with open(d / "grid" / "grid   0.dat", "wb") as f:
+        np.array([1, case.mx, case.my, case.mz], dtype=np.int32).tofile(f)
+        for a in (case.x, case.y, case.z):
+            np.ascontiguousarray(a, dtype=np.float64).tofile(f)
+    with open(d / "boundary_condition" / "boundary   0.txt", "w") as f:
+        f.write(f"{len(case.faces):7d}\n")
+        for fc in case.faces:
+            f.write("".join(f"{v:7d}" for v in fc.raw) + f"{fc.label:7d}\n")
+    with open(d / "boundary_condition" / "inner   0.txt", "w") as f:
+        f.write("        1        0\n        0\niMin  iMax  jMin  jMax  kMin  kMax   id\n")
+    return d
+
+
+def _box_faces(mx, my, mz, xlab, ylab_lo, ylab_hi, zlab):
+    f = [Face((0, 0, 0, my - 1, 0, mz - 1), xlab), Face((mx - 1, mx - 1, 0, my - 1, 0, mz - 1), xlab),
+         Face((0, mx - 1, 0, 0, 0, mz - 1), ylab_lo), Face((0, mx - 1, my - 1, my - 1, 0, mz - 1), ylab_hi)]
+    if mz > 1:
+        f += [Face((0, mx - 1, 0, my - 1, 0, 0), zlab), Face((0, mx - 1, 0, my - 1, mz - 1, mz - 1), zlab)]
+    return f
+
+
+def mixing_layer_2d(mx=257, my=129, seed=0, steps=100, mc=0.4, re=1000.0, t0=300.0, delta0=1e-3,
+                    reconstruction=4, inviscid_scheme=3, cfl=0.5) -> Case:
+    """2-D temporal mixing layer: 256 x 128 cells on 2*pi x pi (node-coincident periodic x, mx = 257),
+    u = dU/2 tanh(2y/delta0), Mc = dU/(2c), Re = rho dU delta0 / mu(T) , T and p uniform, and
+    v' = 1e-3 dU sum_{m=1..8} a_m cos(m x + phi_m) exp(-(y/delta0)^2), a_m = 1/8, phi_m ~ U[0,2pi)."""
+    rng = np.random.default_rng(seed)
+    xs = np.linspace(0.0, 2 * math.pi, mx)
+    ys = np.linspace(-math.pi / 2, math.pi / 2, my)
+    Y, X = np.meshgrid(ys, xs, indexing="ij")
+    x = X[None].copy()
+    y = Y[None].copy()
+    z = np.zeros_like(x)
+    c0 = math.sqrt(GAMMA * R_AIR * t0)
+    du = 2 * mc * c0
+    rho0 = re * sutherland(t0) / (du * delta0)
+    p0 = rho0 * R_AIR * t0
+    phi = rng.uniform(0, 2 * math.pi, 8)
+    a = np.full(8, 1 / 8)
+    yy = y  # grid units = y / delta0
+    vprime = 1e-3 * du * sum(a[m] * np.cos((m + 1) * x + phi[m]) for m in range(8)) * np.exp(-yy ** 2)
+    bv = np.empty((6, 1, my, mx))
+    bv[0] = rho0
+    bv[1] = 0.5 * du * np.tanh(2 * yy)
+    bv[2] = vprime
+    bv[3] = 0.0
+    bv[4] = p0
+    bv[5] = t0
+    faces = _box_faces(mx, my, 1, 8, 3, 3, 8)
+    structs = {"slipwall": {"type": ("string", "symmetry"), "label": ("int", 3)},
+               "periodic": {"type": ("string", "periodic"), "label": ("int", 8)}}
+    scheme = dict(reconstruction=reconstruction, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=cfl,
+                  prandtl_number=0.72)
+    return Case("mixing_layer_2d", mx, my, 1, x, y, z, delta0, faces, structs, scheme, bv, steps)
+
+
+def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0, t0=300.0, delta0=1e-3,
+                    h=0.125, reconstruction=5, inviscid_scheme=4, cfl=0.5, ybc="farfield") -> Case:
+    """3-D temporal mixing layer: uniform spacing h*delta0, periodic x and z (node-coincident),
+    far-field (Riemann-invariant, label 4/41) or outflow (label 6) y faces; u = dU/2 tanh(2y/delta0),
+    Mc = 0.7, plus 1e-2 dU N(0,1) exp(-(y/delta0)^2) seeded white noise in u, v, w."""
+    rng = np.random.default_rng(seed)
+    xs = np.arange(mx) * h
+    ys = (np.arange(my) - (my - 1) / 2) * h
+    zs = np.arange(mz) * h
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    c0 = math.sqrt(GAMMA * R_AIR * t0)
+    du = 2 * mc * c0
+    rho0 = re * sutherland(t0) / (du * delta0)
+    p0 = rho0 * R_AIR * t0
+    env = np.exp(-Y ** 2)
+    bv = np.empty((6, mz, my, mx))
+    bv[0] = rho0
+    bv[1] = 0.5 * du * np.tanh(2 * Y) + 1e-2 * du * rng.standard_normal(X.shape) * env
+    bv[2] = 1e-2 * du * rng.standard_normal(X.shape) * env
+    bv[3] = 1e-2 * du * rng.standard_normal(X.shape) * env
+    bv[4] = p0
+    bv[5] = t0
+    if ybc == "farfield":
+        faces = _box_faces(mx, my, mz, 8, 41, 4, 8)
+        structs = {"periodic": {"type": ("string", "periodic"), "label": ("int", 8)},
+                   "farfield_upper": {"type": ("string", "farfield"), "label": ("int", 4), "mach": ("real", mc),
+                                      "pressure": ("real", p0), "temperature": ("real", t0), "u": ("real", 1.0),
+                                      "v": ("real", 0.0), "w": ("real", 0.0)},
+                   "farfield_lower": {"type": ("string", "farfield"), "label": ("int", 41), "mach": ("real", mc),
+                                      "pressure": ("real", p0), "temperature": ("real", t0), "u": ("real", -1.0),
+                                      "v": ("real", 0.0), "w": ("real", 0.0)}}
+    else:
+        faces = _box_faces(mx, my, mz, 8, 6, 6, 8)
+        structs = {"periodic": {"type": ("string", "periodic"), "label": ("int", 8)},
+                   "outflow": {"type": ("string", "outflow"), "label": ("int", 6)}}
+    scheme = dict(reconstruction=reconstruction, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=cfl,
+                  prandtl_number=0.72)
+    return Case("mixing_layer_3d", mx, my, mz, X, Y, Z, delta0, faces, structs, scheme, bv, steps)
+
+
+def relative_errors(a: np.ndarray, b: np.ndarray, momentum_group: bool = True):
+    """Per conserved variable (rho, rho u, rho v, rho w, rho E): (max-abs error / scale, L2 error / L2 scale).
+
+    The scale of a scalar variable is its own max-abs (or L2 norm).  With momentum_group, the three
+    momentum components share one scale, the momentum vector's max-abs (L2) magnitude: a transverse
+    component that is only a small perturbation (rho v in a shear layer) is then measured against the
+    momentum it is part of, not against its own near-zero size."""
+    out = []
+    mom = slice(1, 4)
+    mom_max = float(np.max(np.sqrt(np.sum(b[mom] ** 2, axis=0))))
+    mom_l2 = float(np.linalg.norm(b[mom]))
+    for l in range(a.shape[0]):
+        if momentum_group and 1 <= l <= 3:
+            smax, sl2 = mom_max, mom_l2
+        else:
+            smax, sl2 = float(np.max(np.abs(b[l]))), float(np.linalg.norm(b[l]))
+        d = a[l] - b[l]
+        mx = float(np.max(np.abs(d)) / smax) if smax > 0 else float(np.max(np.abs(d)))
+        l2 = float(np.linalg.norm(d) / sl2) if sl2 > 0 else float(np.linalg.norm(d))
+        out.append((mx, l2))
+    return out

@@ -1,0 +1,141 @@
+"""ctypes binding of the CPU oracle (oracle/ostc_oracle.c).
+
+TEST INFRASTRUCTURE: used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg only, as the
+checker or the timed CPU baseline.  The oracle restates the reference OpenSTC RHS + SSP-RK3 path for
+calorically perfect air in serial FP64 C; each routine cites the reference file:line it follows.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "libostc_oracle.so"
+
+
+class OrcFace(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("raw", ctypes.c_int * 6)] + [
+        (n, ctypes.c_double) for n in ("density", "u", "v", "w", "pressure", "temperature", "acoustic_speed",
+                                       "gamma", "entropy", "mw")]
+
+
+class OrcCase(ctypes.Structure):
+    _fields_ = [("mx", ctypes.c_int), ("my", ctypes.c_int), ("mz", ctypes.c_int), ("reconstruction", ctypes.c_int),
+                ("inviscid_scheme", ctypes.c_int), ("viscous_order", ctypes.c_int), ("cfl", ctypes.c_double),
+                ("prandtl", ctypes.c_double), ("fixed_time_step", ctypes.c_int), ("dt", ctypes.c_double),
+                ("n_face", ctypes.c_int), ("face", OrcFace * 16)]
+
+
+def build() -> Path:
+    subprocess.run(["make", "-C", str(HERE)], check=True, capture_output=True)
+    return LIB
+
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        lib = ctypes.CDLL(str(LIB))
+        vp, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)
+        lib.orc_create.argtypes = [ctypes.POINTER(OrcCase), dp, dp, dp]
+        lib.orc_create.restype = vp
+        lib.orc_destroy.argtypes = [vp]
+        lib.orc_ngg.argtypes = [vp]
+        lib.orc_set_state.argtypes = [vp, dp]
+        lib.orc_get_state.argtypes = [vp, dp, dp, dp]
+        lib.orc_get_metric.argtypes = [vp, dp, dp]
+        lib.orc_rhs.argtypes = [vp, ctypes.c_uint, dp]
+        lib.orc_step.argtypes = [vp, ctypes.c_int]
+        lib.orc_step.restype = ctypes.c_double
+        lib.orc_time.argtypes = [vp]
+        lib.orc_time.restype = ctypes.c_double
+        lib.orc_dt.argtypes = [vp]
+        lib.orc_dt.restype = ctypes.c_double
+        _lib = lib
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Oracle:
+    """CPU restatement of one single-block case (see ostc_cases.Case)."""
+
+    def __init__(self, case):
+        self.lib = load()
+        c = OrcCase()
+        c.mx, c.my, c.mz = case.mx, case.my, case.mz
+        s = case.scheme
+        c.reconstruction, c.inviscid_scheme, c.viscous_order = s["reconstruction"], s["inviscid_scheme"], s["viscous_order"]
+        c.cfl, c.prandtl = s["cfl"], s["prandtl_number"]
+        c.fixed_time_step, c.dt = 0, 1e-8
+        types = case.label_types()
+        ff = case.farfield_states()
+        c.n_face = len(case.faces)
+        for n, f in enumerate(case.faces):
+            c.face[n].type = types[f.label]
+            for q in range(6):
+                c.face[n].raw[q] = f.raw[q]
+            if f.label in ff:
+                for k, v in ff[f.label].items():
+                    setattr(c.face[n], k, v)
+        self.case = case
+        self.shape = (case.mz, case.my, case.mx)
+        x = np.ascontiguousarray(case.x * case.grid_scale, dtype=np.float64)
+        y = np.ascontiguousarray(case.y * case.grid_scale, dtype=np.float64)
+        z = np.ascontiguousarray(case.z * case.grid_scale, dtype=np.float64)
+        if case.mz == 1:
+            # 2-D: the reference scales z too, but builds k ghosts at unit spacing after scaling
+            z = np.ascontiguousarray(case.z * case.grid_scale, dtype=np.float64)
+        self._c = c
+        self.h = self.lib.orc_create(ctypes.byref(c), _dp(x), _dp(y), _dp(z))
+
+    def close(self):
+        if self.h:
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, bv: np.ndarray):
+        bv = np.ascontiguousarray(bv, dtype=np.float64)
+        self.lib.orc_set_state(self.h, _dp(bv))
+
+    def get_state(self):
+        cv = np.empty((5,) + self.shape)
+        bv = np.empty((6,) + self.shape)
+        mul = np.empty(self.shape)
+        self.lib.orc_get_state(self.h, _dp(cv), _dp(bv), _dp(mul))
+        return cv, bv, mul
+
+    def metric(self):
+        m = np.empty((9,) + self.shape)
+        j = np.empty(self.shape)
+        self.lib.orc_get_metric(self.h, _dp(m), _dp(j))
+        return m, j
+
+    def rhs(self, mask: int = 3) -> np.ndarray:
+        dq = np.empty((5,) + self.shape)
+        self.lib.orc_rhs(self.h, mask, _dp(dq))
+        return dq
+
+    def step(self, n: int = 1) -> float:
+        return self.lib.orc_step(self.h, n)
+
+    def time(self) -> float:
+        return self.lib.orc_time(self.h)
+
+    def dt(self) -> float:
+        return self.lib.orc_dt(self.h)
