@@ -105,6 +105,13 @@ int ostc_rhs(ostc_ctx *ctx, int block, unsigned term_mask, double *dq, int ptr_k
  * minimum over all blocks, TimeAdvanceFunc.cu:39-64, or the fixed dt); reading it synchronises. */
 int ostc_rk3_step(ostc_ctx *ctx, int n_steps, double *dt_last);
 
+/* Same as ostc_rk3_step without the dt read-back, bracketed by CUDA events recorded on the context
+ * stream: *ms receives the device time of the n_steps steps.  Synchronises. */
+int ostc_timed_steps(ostc_ctx *ctx, int n_steps, double *ms);
+
+/* Number of kernels one step launches (kernel nodes of the captured step graph). */
+int ostc_step_kernel_count(ostc_ctx *ctx, int *n_kernels);
+
 /* Physical time advanced so far (RK.cuh:175-176).  Synchronises. */
 int ostc_physical_time(ostc_ctx *ctx, double *t);
 

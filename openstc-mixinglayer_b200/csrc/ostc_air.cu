@@ -656,6 +656,7 @@ struct ostc_ctx {
   unsigned *d_flags = nullptr;
   cudaGraphExec_t graph = nullptr;
   int graph_precision = -1;
+  int graph_kernels = 0;
   std::string err;
   int sm_count = 148;
   // timing (ostc_profile_steps)
@@ -1100,11 +1101,10 @@ int ostc_set_state(ostc_ctx *ctx, int block, const double *bv, const double *sv,
   const size_t bytes = 6 * (size_t)B.db.n * sizeof(double);
   CK(cudaMemcpyAsync(ctx->d_staging, bv, bytes, ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                      ctx->stream));
-  for (int s = 0; s < 3; ++s) {
-    CK(cudaMemsetAsync(B.bv[s], 0, 6 * B.db.plane * sizeof(double), ctx->stream));
-    CK(cudaMemsetAsync(B.cv[s], 0, 5 * B.db.plane * sizeof(double), ctx->stream));
-    CK(cudaMemsetAsync(B.mul[s], 0, B.db.plane * sizeof(double), ctx->stream));
-  }
+  // buffer A holds the new state; every ghost node is rewritten by the boundary faces before use
+  CK(cudaMemsetAsync(B.bv[0], 0, 6 * B.db.plane * sizeof(double), ctx->stream));
+  CK(cudaMemsetAsync(B.cv[0], 0, 5 * B.db.plane * sizeof(double), ctx->stream));
+  CK(cudaMemsetAsync(B.mul[0], 0, B.db.plane * sizeof(double), ctx->stream));
   k_scatter<<<grid_for(ctx, 6 * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, ctx->d_staging, B.bv[0], 6);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
@@ -1166,10 +1166,7 @@ int ostc_rhs(ostc_ctx *ctx, int block, unsigned mask, double *dq, int ptr_kind) 
   return OSTC_OK;
 }
 
-int ostc_rk3_step(ostc_ctx *ctx, int n_steps, double *dt_last) {
-  if (!ctx || n_steps < 0) return OSTC_EINVAL;
-  cudaSetDevice(ctx->device);
-  if (int r = check_ready(ctx)) return r;
+static int ensure_graph(ostc_ctx *ctx) {
   if (!ctx->graph || ctx->graph_precision != ctx->precision) {
     if (ctx->graph) {
       cudaGraphExecDestroy(ctx->graph);
@@ -1180,14 +1177,61 @@ int ostc_rk3_step(ostc_ctx *ctx, int n_steps, double *dt_last) {
     enqueue_step_any(ctx);
     CK(cudaStreamEndCapture(ctx->stream, &g));
     CK(cudaGraphInstantiate(&ctx->graph, g, 0));
+    size_t nodes = 0;
+    CK(cudaGraphGetNodes(g, nullptr, &nodes));
+    std::vector<cudaGraphNode_t> nv(nodes);
+    CK(cudaGraphGetNodes(g, nv.data(), &nodes));
+    int nk = 0;
+    for (auto nd : nv) {
+      cudaGraphNodeType t;
+      if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++nk;
+    }
+    ctx->graph_kernels = nk;
     cudaGraphDestroy(g);
     ctx->graph_precision = ctx->precision;
   }
+  return OSTC_OK;
+}
+
+int ostc_rk3_step(ostc_ctx *ctx, int n_steps, double *dt_last) {
+  if (!ctx || n_steps < 0) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  if (int r = ensure_graph(ctx)) return r;
   for (int s = 0; s < n_steps; ++s) CK(cudaGraphLaunch(ctx->graph, ctx->stream));
   if (dt_last) {
     CK(cudaMemcpyAsync(dt_last, ctx->d_dt, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
   }
+  return OSTC_OK;
+}
+
+int ostc_timed_steps(ostc_ctx *ctx, int n_steps, double *ms) {
+  if (!ctx || n_steps < 0 || !ms) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  if (int r = ensure_graph(ctx)) return r;
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  CK(cudaEventRecord(a, ctx->stream));
+  for (int s = 0; s < n_steps; ++s) CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+  CK(cudaEventRecord(b, ctx->stream));
+  CK(cudaEventSynchronize(b));
+  float t = 0;
+  CK(cudaEventElapsedTime(&t, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = t;
+  return OSTC_OK;
+}
+
+int ostc_step_kernel_count(ostc_ctx *ctx, int *n) {
+  if (!ctx || !n) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  if (int r = ensure_graph(ctx)) return r;
+  *n = ctx->graph_kernels;
   return OSTC_OK;
 }
 

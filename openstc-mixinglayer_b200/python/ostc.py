@@ -23,7 +23,8 @@ EXPORTS = [
     "ostc_create", "ostc_destroy", "ostc_last_error", "ostc_n_blocks", "ostc_block_dims", "ostc_n_var",
     "ostc_set_precision", "ostc_set_state", "ostc_get_state", "ostc_rhs", "ostc_rk3_step",
     "ostc_physical_time", "ostc_store_residual_reference", "ostc_residual", "ostc_error_flags",
-    "ostc_device_view", "ostc_profile_steps", "ostc_total_nodes", "ostc_probe_case",
+    "ostc_device_view", "ostc_profile_steps", "ostc_total_nodes", "ostc_probe_case", "ostc_timed_steps",
+    "ostc_step_kernel_count",
 ]
 
 
@@ -73,6 +74,8 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.ostc_device_view.argtypes = [vp, ip, ctypes.POINTER(ZoneView)]
     lib.ostc_profile_steps.argtypes = [vp, ip, ip, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ip), dp]
     lib.ostc_total_nodes.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    lib.ostc_timed_steps.argtypes = [vp, ip, dp]
+    lib.ostc_step_kernel_count.argtypes = [vp, ctypes.POINTER(ip)]
     lib.ostc_probe_case.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(ip), ctypes.c_char_p, ip]
     if path is None:
         _lib = lib
@@ -172,6 +175,17 @@ class Solver:
 
     def step_async(self, n: int = 1):
         self._check(self.lib.ostc_rk3_step(self.h, n, None))
+
+    def timed_steps(self, n: int) -> float:
+        """Advance n steps; device milliseconds between events on the library's stream."""
+        ms = ctypes.c_double()
+        self._check(self.lib.ostc_timed_steps(self.h, n, ctypes.byref(ms)))
+        return ms.value
+
+    def step_kernel_count(self) -> int:
+        k = ctypes.c_int()
+        self._check(self.lib.ostc_step_kernel_count(self.h, ctypes.byref(k)))
+        return k.value
 
     def time(self) -> float:
         t = ctypes.c_double()

@@ -81,3 +81,40 @@ def test_rk3_trajectory(built, tmp_path, dims, recon, rs, steps):
     assert all(m < TOL and l2 < TOL for m, l2 in err), err
     assert abs(s.time() - o.time()) / o.time() < 1e-12
     assert s.error_flags() == 0
+
+
+def test_mixed_precision_accuracy(built, tmp_path):
+    """Mixed path (FP32 reconstruction/Riemann/viscous arithmetic, FP64 state and EOS) against the
+    FP64 path after 100 steps: relative L2 error of the conserved variables <= 1e-6."""
+    case = oc.mixing_layer_3d(mx=48, my=32, mz=24)
+    d = oc.write_case(case, tmp_path / "mixed")
+    a = ostc.Solver(str(d))
+    a.set_state(case.bv)
+    b = ostc.Solver(str(d))
+    b.set_precision(ostc.PREC_MIXED)
+    b.set_state(case.bv)
+    a.step(100)
+    b.step(100)
+    ca, _ = a.get_state()
+    cb, _ = b.get_state()
+    err = oc.relative_errors(cb, ca)
+    assert b.error_flags() == 0
+    assert all(l2 <= 1e-6 for _, l2 in err), err
+
+
+def test_device_flags_clean_and_residual(built, tmp_path):
+    case = oc.mixing_layer_2d(mx=65, my=33)
+    d = oc.write_case(case, tmp_path / "res")
+    s = ostc.Solver(str(d))
+    s.set_state(case.bv)
+    s.store_residual_reference()
+    _, b0 = s.get_state()
+    s.step(3)
+    _, b1 = s.get_state()
+    res = s.residual()
+    v0 = np.sqrt(b0[1] ** 2 + b0[2] ** 2 + b0[3] ** 2)
+    v1 = np.sqrt(b1[1] ** 2 + b1[2] ** 2 + b1[3] ** 2)
+    ref = np.sqrt([np.mean((b1[0] - b0[0]) ** 2), np.mean((v1 - v0) ** 2), np.mean((b1[4] - b0[4]) ** 2),
+                   np.mean((b1[5] - b0[5]) ** 2)])
+    assert np.allclose(res, ref, rtol=1e-10, atol=0)
+    assert s.error_flags() == 0
