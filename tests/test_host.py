@@ -1,0 +1,98 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports every declared symbol, the
+setup/grid/boundary readers derive what the reference derives, and bad inputs are rejected on the
+host (so no kernel ever sees an out-of-range face)."""
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import ostc
+import ostc_cases as oc
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def test_exports_every_declared_symbol(built):
+    lib = ostc.load_library()
+    header = (ROOT / "include" / "ostc.h").read_text()
+    declared = set(re.findall(r"^\s*(?:int|void|const char \*)\s*(ostc_\w+)\s*\(", header, re.M))
+    assert len(declared) >= 20
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert declared == set(ostc.EXPORTS), declared ^ set(ostc.EXPORTS)
+
+
+@pytest.mark.parametrize("recon,rs,ngg", [(4, 3, 3), (5, 4, 4), (4, 4, 3), (5, 3, 4)])
+def test_probe_2d(built, tmp_path, recon, rs, ngg):
+    case = oc.mixing_layer_2d(mx=33, my=17, reconstruction=recon, inviscid_scheme=rs)
+    d = oc.write_case(case, tmp_path / "c")
+    p = ostc.probe_case(str(d))
+    assert p["ngg"] == ngg and p["inviscid_type"] == 1 and p["n_var"] == 5 and p["dimension"] == 2
+    assert (p["mx"], p["my"], p["mz"]) == (33, 17, 1)
+    assert p["n_faces"] == 4 and p["n_bc_launches"] == 4
+
+
+def test_probe_3d_farfield(built, tmp_path):
+    case = oc.mixing_layer_3d(mx=24, my=20, mz=16)
+    d = oc.write_case(case, tmp_path / "c")
+    p = ostc.probe_case(str(d))
+    assert p["dimension"] == 3 and p["n_faces"] == 6 and p["ngg"] == 4
+    assert p["reconstruction"] == 5 and p["inviscid_scheme"] == 4
+
+
+def _case_dir(tmp_path, **kw):
+    case = oc.mixing_layer_2d(mx=33, my=17, **kw)
+    return case, oc.write_case(case, tmp_path / "c")
+
+
+def test_missing_grid_is_io_error(built, tmp_path):
+    _, d = _case_dir(tmp_path)
+    (d / "grid" / "grid   0.dat").unlink()
+    with pytest.raises(ostc.OstcError) as e:
+        ostc.probe_case(str(d))
+    assert e.value.code == -2
+
+
+def test_unsupported_species_rejected(built, tmp_path):
+    _, d = _case_dir(tmp_path)
+    s = (d / "setup.txt").read_text().replace("int species = 0", "int species = 1")
+    (d / "setup.txt").write_text(s)
+    with pytest.raises(ostc.OstcError, match="species"):
+        ostc.probe_case(str(d))
+
+
+def test_face_outside_block_rejected(built, tmp_path):
+    case, _ = _case_dir(tmp_path)
+    case.faces[2] = oc.Face((0, 40, 0, 0, 0, 0), 3)
+    d = oc.write_case(case, tmp_path / "bad")
+    with pytest.raises(ostc.OstcError, match="outside"):
+        ostc.probe_case(str(d))
+
+
+def test_face_not_on_a_side_rejected(built, tmp_path):
+    case, _ = _case_dir(tmp_path)
+    case.faces[2] = oc.Face((0, 32, 5, 5, 0, 0), 3)
+    d = oc.write_case(case, tmp_path / "bad")
+    with pytest.raises(ostc.OstcError, match="side"):
+        ostc.probe_case(str(d))
+
+
+def test_setup_grammar(built, tmp_path):
+    """Comments, '//' continuation inside arrays, structs and later overrides (Parameter.cpp:39-185)."""
+    _, d = _case_dir(tmp_path)
+    s = (d / "setup.txt").read_text()
+    s = s.replace("int reconstruction = 4", "int reconstruction = 5 // overridden below\n"
+                  "! a bang comment\n\nint reconstruction = 4")
+    s += "array real some_values = { 1 2 // next line\n  3 4 }\nrange real core = {\n 0 1\n -1 1\n}\n"
+    (d / "setup.txt").write_text(s)
+    p = ostc.probe_case(str(d))
+    assert p["ngg"] == 3 and p["reconstruction"] == 4
+
+
+def test_unknown_boundary_type_rejected(built, tmp_path):
+    case, _ = _case_dir(tmp_path)
+    case.faces[0] = oc.Face(case.faces[0].raw, 2)  # label 2 = wall, not on this path
+    d = oc.write_case(case, tmp_path / "bad")
+    with pytest.raises(ostc.OstcError, match="label 2"):
+        ostc.probe_case(str(d))
