@@ -143,6 +143,31 @@ int ostc_total_nodes(const ostc_ctx *ctx, long long *n);
  * (Parameter::deduce_known_info / Mesh::Mesh checks, Parameter.cpp:187-437, Mesh.cpp:592-641). */
 int ostc_probe_case(const char *setup_txt, const char *input_dir, int out[16], char *msg, int msg_len);
 
+/* Limits of ostc_residual_noalloc: its static scratch holds one partial sum set per block of
+ * 256 threads x 64 nodes, for at most OSTC_NOALLOC_MAX_BLOCKS blocks (128 KB of device memory). */
+#define OSTC_NOALLOC_NODES_PER_THREAD 64
+#define OSTC_NOALLOC_MAX_BLOCKS 4096
+#define OSTC_NOALLOC_MAX_NODES (256LL * OSTC_NOALLOC_NODES_PER_THREAD * OSTC_NOALLOC_MAX_BLOCKS)
+
+/* Residual norms without any device allocation.  No counterpart in the reference: it exists for
+ * callers that cannot call cudaMalloc - hosts whose device memory is planned up front and handed out
+ * by their own pool, loops that must not take an allocation's implicit synchronisation, code that
+ * runs while another thread captures a CUDA graph in global mode.
+ * bv_new, bv_old: caller-owned device arrays of interior primitive states, [6][n_nodes]
+ * (rho,u,v,w,p,T), e.g. the output of ostc_get_state(..., OSTC_DEVICE).  res: host array that
+ * receives the RMS changes of rho, |V|, p and T (the same quantities as ostc_residual).  stream:
+ * cudaStream_t to run on (NULL = legacy default stream); the call synchronises it.
+ * n_nodes above OSTC_NOALLOC_MAX_NODES (67,108,864) is rejected with OSTC_EINVAL; the message is
+ * available from ostc_last_error(NULL).
+ * Scratch lives in one file-scope __device__ array (per GPU, held until the process exits), shared
+ * by every call: calls that overlap on the GPU (different streams, or host threads on the same
+ * device) race on it and must be serialised by the caller.  Each call writes every partial it
+ * reads, so nothing in the array has to start at zero.  The first call on a device resolves the
+ * array's device address (cudaGetSymbolAddress) and caches it; make that first call before any
+ * stream capture. */
+int ostc_residual_noalloc(const double *bv_new, const double *bv_old, long long n_nodes, double res[4],
+                          void *stream);
+
 #ifdef __cplusplus
 }
 #endif

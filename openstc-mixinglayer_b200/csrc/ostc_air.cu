@@ -673,6 +673,12 @@ struct ostc_ctx {
 
 static std::string g_create_error;
 
+namespace ostc {
+// Error text of the context-free entry points (ostc_create failures, ostc_residual_noalloc),
+// reported by ostc_last_error(NULL).
+void set_free_error(const std::string &msg) { g_create_error = msg; }
+}  // namespace ostc
+
 #define CK(call)                                                                                         \
   do {                                                                                                   \
     cudaError_t e_ = (call);                                                                             \

@@ -24,7 +24,7 @@ EXPORTS = [
     "ostc_set_precision", "ostc_set_state", "ostc_get_state", "ostc_rhs", "ostc_rk3_step",
     "ostc_physical_time", "ostc_store_residual_reference", "ostc_residual", "ostc_error_flags",
     "ostc_device_view", "ostc_profile_steps", "ostc_total_nodes", "ostc_probe_case", "ostc_timed_steps",
-    "ostc_step_kernel_count",
+    "ostc_step_kernel_count", "ostc_residual_noalloc",
 ]
 
 
@@ -76,6 +76,7 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.ostc_total_nodes.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     lib.ostc_timed_steps.argtypes = [vp, ip, dp]
     lib.ostc_step_kernel_count.argtypes = [vp, ctypes.POINTER(ip)]
+    lib.ostc_residual_noalloc.argtypes = [vp, vp, ctypes.c_longlong, dp, vp]
     lib.ostc_probe_case.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(ip), ctypes.c_char_p, ip]
     if path is None:
         _lib = lib
@@ -93,6 +94,18 @@ def probe_case(input_dir: str, setup: str | None = None) -> dict:
     keys = ["ngg", "inviscid_type", "n_var", "n_scalar", "n_block", "dimension", "mx", "my", "mz",
             "n_faces", "reconstruction", "inviscid_scheme", "viscous_order", "n_bc_launches"]
     return {k: out[i] for i, k in enumerate(keys)}
+
+
+def residual_noalloc(bv_new_ptr: int, bv_old_ptr: int, n_nodes: int, stream: int = 0) -> np.ndarray:
+    """RMS changes of rho, |V|, p, T between two device states [6][n_nodes] without any device
+    allocation (ostc_residual_noalloc)."""
+    lib = load_library()
+    r = (ctypes.c_double * 4)()
+    rc = lib.ostc_residual_noalloc(ctypes.c_void_p(bv_new_ptr), ctypes.c_void_p(bv_old_ptr), n_nodes, r,
+                                   ctypes.c_void_p(stream) if stream else None)
+    if rc != 0:
+        raise OstcError(rc, lib.ostc_last_error(None).decode())
+    return np.array(r[:])
 
 
 def _ptr(a: np.ndarray) -> ctypes.c_void_p:
