@@ -115,11 +115,16 @@ __global__ void __launch_bounds__(256) k_cfl_dt(DevBlock b, DevState s, double c
 
 // ------------------------------------------------------------------------------ inviscid flux
 
+// Resident blocks per SM the x sweep is compiled for (register budget 65536 / (128 * this)).
+#ifndef OSTC_FLUXX_MINB
+#define OSTC_FLUXX_MINB 2
+#endif
+
 // x sweep.  A block of 128 threads stages 127 + 2*NG nodes of one (j,k) row in shared memory
 // (coalesced along i), computes the 128 faces i0-1/2 .. i0+126+1/2 (one per thread) and finalises
 // the 127 nodes between them: dq = -(fc(i+1/2) - fc(i-1/2)) + central correction.
 template <int NG, int RS, typename T>
-__global__ void __launch_bounds__(128) k_flux_x(DevBlock b, DevState s, double *__restrict__ dq) {
+__global__ void __launch_bounds__(128, OSTC_FLUXX_MINB) k_flux_x(DevBlock b, DevState s, double *__restrict__ dq) {
   constexpr int L = 127;
   constexpr int NP = L + 2 * NG;
   __shared__ T sq[6][NP];
@@ -184,13 +189,14 @@ __global__ void __launch_bounds__(128) k_flux_x(DevBlock b, DevState s, double *
 }
 
 // y (DIR = 1) or z (DIR = 2) sweep.  Thread (i, o) marches nodes c = s0..s1-1 of its column (o is
-// k for y, j for z); warps are contiguous in i, so every load of a new node is coalesced.  The
-// per-thread ring in shared memory keeps the last 2*NG+1 nodes: cv(5), p, node flux(5), metric
-// row(3), Jacobian.  Segments of `seg` nodes split long columns across blocks.
+// k for y, j for z); warps are contiguous in i, so every load of a new node is coalesced.  A
+// per-thread ring in shared memory keeps the last 2*NG+1 nodes' cv(5), p and node flux(5); the
+// metric row and Jacobian of the face's two nodes travel in registers (node c+1 is re-read, an L1/L2
+// hit, when its face comes up).  Segments of `seg` nodes split long columns across blocks.
 template <int DIR, int NG, int RS, typename T>
-__global__ void __launch_bounds__(64) k_flux_march(DevBlock b, DevState s, double *__restrict__ dq, int seg) {
+__global__ void __launch_bounds__(64, 4) k_flux_march(DevBlock b, DevState s, double *__restrict__ dq, int seg) {
   constexpr int W = 2 * NG + 1;
-  constexpr int NV = 15;
+  constexpr int NV = 11;
   extern __shared__ __align__(16) unsigned char smraw[];
   T *ring = reinterpret_cast<T *>(smraw);
   const int nthr = blockDim.x * blockDim.y;
@@ -206,6 +212,7 @@ __global__ void __launch_bounds__(64) k_flux_march(DevBlock b, DevState s, doubl
   const long long P = b.plane;
   const long long stride = DIR == 1 ? (long long)b.pitch : (long long)b.pitch * b.sy;
   const long long base = DIR == 1 ? b.id(i, 0, o) : b.id(i, o, 0);
+  const double *__restrict__ mrow = b.met + (long long)DIR * 3 * P;
   auto R = [&](int slot, int v) -> T & { return ring[(slot * NV + v) * nthr + tid]; };
   auto load = [&](int n) {
     const long long p = base + (long long)n * stride;
@@ -218,36 +225,39 @@ __global__ void __launch_bounds__(64) k_flux_march(DevBlock b, DevState s, doubl
     }
     R(slot, 5) = bb[4];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      kk[c] = (T)b.met[(DIR * 3 + c) * P + p];
-      R(slot, 11 + c) = kk[c];
-    }
-    const T jj = (T)b.jac[p];
-    R(slot, 14) = jj;
+    for (int c = 0; c < 3; ++c) kk[c] = (T)mrow[c * P + p];
     T f[5];
-    node_flux<T>(bb, (T)s.cv[4 * P + p], kk, jj, f);
+    node_flux<T>(bb, (T)s.cv[4 * P + p], kk, (T)b.jac[p], f);
 #pragma unroll
     for (int l = 0; l < 5; ++l) R(slot, 6 + l) = f[l];
   };
   for (int n = s0 - NG; n <= s0 + NG - 2; ++n) load(n);
   T fprev[5] = {T(0), T(0), T(0), T(0), T(0)};
+  long long pc = base + (long long)(s0 - 1) * stride;
+  T mt0[3] = {(T)mrow[pc], (T)mrow[P + pc], (T)mrow[2 * P + pc]};
+  T j0 = (T)b.jac[pc];
   for (int c = s0 - 1; c < s1; ++c) {
     load(c + NG);
+    const long long pn = pc + stride;
+    const T mt1[3] = {(T)mrow[pn], (T)mrow[P + pn], (T)mrow[2 * P + pn]};
+    const T j1 = (T)b.jac[pn];
     const int b0 = (c + 1) % W;
     auto q = [&](int st, int v) -> T {
       int sl = b0 + st;
       sl = sl >= W ? sl - W : sl;
       return R(sl, v);
     };
-    const int sc = (c + NG) % W, sc1 = (c + 1 + NG) % W;
-    const T mt0[3] = {R(sc, 11), R(sc, 12), R(sc, 13)};
-    const T mt1[3] = {R(sc1, 11), R(sc1, 12), R(sc1, 13)};
     T fc[5];
-    aweno_face_flux<NG, RS, T>(q, mt0, mt1, R(sc, 14), R(sc1, 14), fc);
+    aweno_face_flux<NG, RS, T>(q, mt0, mt1, j0, j1, fc);
     if (c >= s0) {
       const long long qi = DIR == 1 ? b.iq(i, c, o) : b.iq(i, o, c);
       const bool cds = c < n_dir - 2 * NG;
-      auto f = [&](int m, int l) -> T { return R((c + m + NG + W) % W, 6 + l); };
+      const int bc = c % W;  // slot of node c - NG
+      auto f = [&](int m, int l) -> T {
+        int sl = bc + NG + m;
+        sl = sl >= W ? sl - W : sl;
+        return R(sl, 6 + l);
+      };
 #pragma unroll
       for (int l = 0; l < 5; ++l) {
         double d = dq[l * b.n + qi];
@@ -258,6 +268,10 @@ __global__ void __launch_bounds__(64) k_flux_march(DevBlock b, DevState s, doubl
     }
 #pragma unroll
     for (int l = 0; l < 5; ++l) fprev[l] = fc[l];
+    pc = pn;
+#pragma unroll
+    for (int q3 = 0; q3 < 3; ++q3) mt0[q3] = mt1[q3];
+    j0 = j1;
   }
 }
 
@@ -750,7 +764,7 @@ int launch_flux(ostc_ctx *ctx, BlockRes &B, DevState in) {
     nseg = (n_dir + seg - 1) / seg;
     dim3 grid((b.mx + 31) / 32, (n_o + 1) / 2, nseg);
     dim3 block(32, 2, 1);
-    const size_t smem = (size_t)(2 * ng + 1) * 15 * 64 * sizeof(T);
+    const size_t smem = (size_t)(2 * ng + 1) * 11 * 64 * sizeof(T);
     long tok = begin_t(ctx, dir == 1 ? "flux_y" : "flux_z");
 #define OSTC_MARCH(D, N, R) k_flux_march<D, N, R, T><<<grid, block, smem, ctx->stream>>>(b, in, B.dq, seg)
     if (dir == 1) {
@@ -799,13 +813,13 @@ void launch_bcs(ostc_ctx *ctx, int block, DevState out) {
 
 DevState state_of(BlockRes &B, int s) { return DevState{B.cv[s], B.bv[s], B.mul[s]}; }
 
-// The march kernels stage up to 2*ngg+1 nodes x 15 values x 64 threads in dynamic shared memory
-// (up to 69 KB in FP64); raise the per-kernel limit once, outside any stream capture.
+// The march kernels stage 2*ngg+1 nodes x 11 values x 64 threads in dynamic shared memory (up to
+// 51 KB in FP64); raise the per-kernel limit once, outside any stream capture.
 template <typename T>
 bool set_march_attrs() {
   bool ok = true;
   auto set = [&](const void *fn, int ng) {
-    const int bytes = (2 * ng + 1) * 15 * 64 * (int)sizeof(T);
+    const int bytes = (2 * ng + 1) * 11 * 64 * (int)sizeof(T);
     ok = ok && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
   };
   set((const void *)k_flux_march<1, 3, 3, T>, 3);
