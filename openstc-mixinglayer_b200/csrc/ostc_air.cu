@@ -24,6 +24,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace ostc {
@@ -278,31 +279,30 @@ __global__ void __launch_bounds__(64, 4) k_flux_march(DevBlock b, DevState s, do
 // ------------------------------------------------------------------------------ viscous + update
 
 // compute_fv/gv/hv_2nd_order<Air, Laminar> (ViscousScheme.cuh:24-911): viscous flux through the face
-// between node (i,j,k) and its neighbour in direction d; fv[0..3] = components 1..4 (component 0 is 0).
-template <typename T, bool DIM3>
-__device__ __forceinline__ void viscous_face(const DevBlock &b, const DevState &s, double prandtl, int i, int j,
-                                             int k, int d, T *fv) {
-  const long long P = b.plane;
-  const long long st[3] = {1, b.pitch, (long long)b.pitch * b.sy};
-  const long long p0 = b.id(i, j, k), p1 = p0 + st[d];
+// between a node and its neighbour in direction d; fv[0..3] = flux components 1..4 (component 0 is 0).
+// V(q, di, dj, dk): q = u, v, w, T, mu of the node at offset (di,dj,dk) from the face's first node,
+// u, v, w, T possibly as deviations from a reference whose velocity part is vref (0 in FP64);
+// Mt(r, s): metric entry r (0..8, (row-1)*3+col-1) or Jacobian (r = 9) of face node s (0 or 1).
+template <typename T, bool DIM3, class VA, class MA>
+__device__ __forceinline__ void viscous_face(int d, const VA &V, const MA &Mt, T iprandtl, const T *vref, T *fv) {
+  const int e[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
   T m[9];
 #pragma unroll
-  for (int r = 0; r < 9; ++r) m[r] = T(0.5) * ((T)b.met[r * P + p0] + (T)b.met[r * P + p1]);
-  const int vars[4] = {1, 2, 3, 5};
+  for (int r = 0; r < 9; ++r) m[r] = T(0.5) * (Mt(r, 0) + Mt(r, 1));
   T gx[4], gy[4], gz[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    const double *B = s.bv + vars[q] * P;
     T g[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       if (c == d) {
-        g[c] = (T)B[p1] - (T)B[p0];
+        g[c] = V(q, e[d][0], e[d][1], e[d][2]) - V(q, 0, 0, 0);
       } else if (c == 2 && !DIM3) {
         g[c] = T(0);
       } else {
-        const long long sc = st[c];
-        g[c] = T(0.25) * ((T)B[p0 + sc] - (T)B[p0 - sc] + (T)B[p1 + sc] - (T)B[p1 - sc]);
+        const int a0 = e[c][0], a1 = e[c][1], a2 = e[c][2];
+        g[c] = T(0.25) * (V(q, a0, a1, a2) - V(q, -a0, -a1, -a2) + V(q, e[d][0] + a0, e[d][1] + a1, e[d][2] + a2) -
+                          V(q, e[d][0] - a0, e[d][1] - a1, e[d][2] - a2));
       }
     }
     gx[q] = g[0] * m[0] + g[1] * m[3] + g[2] * m[6];
@@ -312,25 +312,26 @@ __device__ __forceinline__ void viscous_face(const DevBlock &b, const DevState &
   const T u_x = gx[0], u_y = gy[0], u_z = gz[0];
   const T v_x = gx[1], v_y = gy[1], v_z = gz[1];
   const T w_x = gx[2], w_y = gy[2], w_z = gz[2];
-  const T mul = T(0.5) * ((T)s.mul[p0] + (T)s.mul[p1]);
-  const T txx = mul * (T(4) * u_x - T(2) * v_y - T(2) * w_z) / T(3.0);
-  const T tyy = mul * (T(4) * v_y - T(2) * u_x - T(2) * w_z) / T(3.0);
-  const T tzz = mul * (T(4) * w_z - T(2) * u_x - T(2) * v_y) / T(3.0);
+  const T mul = T(0.5) * (V(4, 0, 0, 0) + V(4, e[d][0], e[d][1], e[d][2]));
+  const T third = T(1.0 / 3.0);
+  const T txx = mul * (T(4) * u_x - T(2) * v_y - T(2) * w_z) * third;
+  const T tyy = mul * (T(4) * v_y - T(2) * u_x - T(2) * w_z) * third;
+  const T tzz = mul * (T(4) * w_z - T(2) * u_x - T(2) * v_y) * third;
   const T txy = mul * (u_y + v_x);
   const T txz = mul * (u_z + w_x);
   const T tyz = mul * (v_z + w_y);
-  const T j0 = (T)b.jac[p0], j1 = (T)b.jac[p1];
-  const T nx = T(0.5) * ((T)b.met[(d * 3 + 0) * P + p0] * j0 + (T)b.met[(d * 3 + 0) * P + p1] * j1);
-  const T ny = T(0.5) * ((T)b.met[(d * 3 + 1) * P + p0] * j0 + (T)b.met[(d * 3 + 1) * P + p1] * j1);
-  const T nz = T(0.5) * ((T)b.met[(d * 3 + 2) * P + p0] * j0 + (T)b.met[(d * 3 + 2) * P + p1] * j1);
+  const T j0 = Mt(9, 0), j1 = Mt(9, 1);
+  const T nx = T(0.5) * (Mt(d * 3 + 0, 0) * j0 + Mt(d * 3 + 0, 1) * j1);
+  const T ny = T(0.5) * (Mt(d * 3 + 1, 0) * j0 + Mt(d * 3 + 1, 1) * j1);
+  const T nz = T(0.5) * (Mt(d * 3 + 2, 0) * j0 + Mt(d * 3 + 2, 1) * j1);
   fv[0] = nx * txx + ny * txy + nz * txz;
   fv[1] = nx * txy + ny * tyy + nz * tyz;
   fv[2] = nx * txz + ny * tyz + nz * tzz;
-  const T um = T(0.5) * ((T)s.bv[P + p0] + (T)s.bv[P + p1]);
-  const T vm = T(0.5) * ((T)s.bv[2 * P + p0] + (T)s.bv[2 * P + p1]);
-  const T wm = T(0.5) * ((T)s.bv[3 * P + p0] + (T)s.bv[3 * P + p1]);
+  const T um = vref[0] + T(0.5) * (V(0, 0, 0, 0) + V(0, e[d][0], e[d][1], e[d][2]));
+  const T vm = vref[1] + T(0.5) * (V(1, 0, 0, 0) + V(1, e[d][0], e[d][1], e[d][2]));
+  const T wm = vref[2] + T(0.5) * (V(2, 0, 0, 0) + V(2, e[d][0], e[d][1], e[d][2]));
   const T cp = T(kGamma * kRuD / kMwD / (kGamma - 1));
-  const T cond = (mul / (T)prandtl) * cp;
+  const T cond = mul * iprandtl * cp;
   fv[3] = um * fv[0] + vm * fv[1] + wm * fv[2] + cond * (nx * gx[3] + ny * gy[3] + nz * gz[3]);
 }
 
@@ -345,72 +346,152 @@ struct StageArgs {
 
 // Viscous fluxes of all directions (viscous_flux_fv/gv/hv, SchemeSelector.cuh:69-154), then the
 // SSP-RK3 combine, EOS and Sutherland viscosity of the new state (update_cv_and_bv_rk, RK.cuh:230-284;
-// update_physical_properties<Air>, FieldOperation.cuh:107-140).  Tile TX x TY x TZ; every face flux
-// is computed once into shared memory.
-template <typename T, bool DIM3, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(TX *TY *TZ) k_visc_update(DevBlock b, StageArgs a, double *__restrict__ dq) {
-  __shared__ T fx[TZ][TY][TX + 1][4];
-  __shared__ T fy[TZ][TY + 1][TX][4];
-  __shared__ T fz[DIM3 ? TZ + 1 : 1][TY][TX][4];
-  const int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
-  const int i = blockIdx.x * TX + tx, j = blockIdx.y * TY + ty, k = blockIdx.z * TZ + tz;
-  const bool inside = i < b.mx && j < b.my && k < b.mz;
-  if (a.viscous && inside) {
-    viscous_face<T, DIM3>(b, a.in, a.prandtl, i - 1, j, k, 0, fx[tz][ty][tx]);
-    if (tx == TX - 1 || i == b.mx - 1) viscous_face<T, DIM3>(b, a.in, a.prandtl, i, j, k, 0, fx[tz][ty][tx + 1]);
-    viscous_face<T, DIM3>(b, a.in, a.prandtl, i, j - 1, k, 1, fy[tz][ty][tx]);
-    if (ty == TY - 1 || j == b.my - 1) viscous_face<T, DIM3>(b, a.in, a.prandtl, i, j, k, 1, fy[tz][ty + 1][tx]);
-    if constexpr (DIM3) {
-      viscous_face<T, DIM3>(b, a.in, a.prandtl, i, j, k - 1, 2, fz[tz][ty][tx]);
-      if (tz == TZ - 1 || k == b.mz - 1) viscous_face<T, DIM3>(b, a.in, a.prandtl, i, j, k, 2, fz[tz + 1][ty][tx]);
-    }
+// update_physical_properties<Air>, FieldOperation.cuh:107-140).
+// A block owns a TX x TY column of nodes and marches k through [k0, k1).  Shared memory keeps a ring
+// of three k planes (k-1, k, k+1) of u, v, w, T, mu and of the metric + Jacobian, each with a one-node
+// halo in i and j, loaded once (coalesced along i).  Every face flux is computed once: x and y faces
+// of plane k into shared memory, the z face k+1/2 in registers (carried to the next plane as k-1/2).
+template <typename T, bool DIM3, int TX, int TY>
+constexpr size_t visc_smem_bytes() {
+  return sizeof(T) * ((DIM3 ? 3 : 1) * 15 * (TY + 2) * (TX + 2) + TY * (TX + 1) * 4 + (TY + 1) * TX * 4);
+}
+
+template <typename T, bool DIM3, int TX, int TY>
+__global__ void __launch_bounds__(TX *TY, 3) k_visc_update(DevBlock b, StageArgs a, double *__restrict__ dq,
+                                                                      int kseg) {
+  constexpr int NP = DIM3 ? 3 : 1;  // planes in the ring
+  constexpr int SX = TX + 2, SY = TY + 2;
+  extern __shared__ __align__(16) unsigned char vsm_raw[];
+  auto sv = reinterpret_cast<T(*)[5][SY][SX]>(vsm_raw);
+  auto sm = reinterpret_cast<T(*)[10][SY][SX]>(vsm_raw + sizeof(T) * NP * 5 * SY * SX);
+  auto fxs = reinterpret_cast<T(*)[TX + 1][4]>(vsm_raw + sizeof(T) * NP * 15 * SY * SX);
+  auto fys = reinterpret_cast<T(*)[TX][4]>(vsm_raw + sizeof(T) * (NP * 15 * SY * SX + TY * (TX + 1) * 4));
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * TX + tx;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int k0 = blockIdx.z * kseg;
+  const int k1 = min(k0 + kseg, b.mz);
+  const bool inside = i < b.mx && j < b.my;
+  const long long P = b.plane;
+  const T ipr = T(1.0 / a.prandtl);
+  // FP32 staging: u, v, w, T are stored as deviations from one reference node of the block, formed
+  // in FP64, so that neighbour differences keep their digits (T ~ 300 K varies by mK across a node);
+  // the FP64 instantiation stores the values themselves (reference 0).
+  double ref[4] = {0.0, 0.0, 0.0, 0.0};
+  if constexpr (!std::is_same_v<T, double>) {
+    const long long pr0 = b.id(min(i0, b.mx - 1), min(j0, b.my - 1), k0);
+    ref[0] = a.in.bv[P + pr0];
+    ref[1] = a.in.bv[2 * P + pr0];
+    ref[2] = a.in.bv[3 * P + pr0];
+    ref[3] = a.in.bv[5 * P + pr0];
   }
-  __syncthreads();
-  if (!inside) return;
-  const long long qi = b.iq(i, j, k);
-  double d[5];
+  const T tref[3] = {(T)ref[0], (T)ref[1], (T)ref[2]};
+  auto load_plane = [&](int kk) {
+    const int slot = DIM3 ? (kk + 3) % 3 : 0;
+    for (int n = tid; n < SX * SY; n += TX * TY) {
+      const int ii = i0 - 1 + n % SX, jj = j0 - 1 + n / SX;
+      if (ii >= b.mx + b.g || jj >= b.my + b.g) continue;
+      const long long p = b.id(ii, jj, kk);
+      const int x = n % SX, y = n / SX;
+      sv[slot][0][y][x] = (T)(a.in.bv[P + p] - ref[0]);
+      sv[slot][1][y][x] = (T)(a.in.bv[2 * P + p] - ref[1]);
+      sv[slot][2][y][x] = (T)(a.in.bv[3 * P + p] - ref[2]);
+      sv[slot][3][y][x] = (T)(a.in.bv[5 * P + p] - ref[3]);
+      sv[slot][4][y][x] = (T)a.in.mul[p];
 #pragma unroll
-  for (int l = 0; l < 5; ++l) d[l] = dq[l * b.n + qi];
+      for (int r = 0; r < 9; ++r) sm[slot][r][y][x] = (T)b.met[r * P + p];
+      sm[slot][9][y][x] = (T)b.jac[p];
+    }
+  };
+  // face whose first node is tile node (x, y) of plane kk, direction d
+  auto face = [&](int d, int x, int y, int kk, T *fv) {
+    const int s0 = DIM3 ? (kk + 3) % 3 : 0;
+    auto V = [&](int q, int di, int dj, int dk) -> T {
+      const int sl = DIM3 ? (s0 + dk + 3) % 3 : 0;
+      return sv[sl][q][y + dj][x + di];
+    };
+    auto Mt = [&](int r, int sd) -> T {
+      if (sd == 0) return sm[s0][r][y][x];
+      if (d == 0) return sm[s0][r][y][x + 1];
+      if (d == 1) return sm[s0][r][y + 1][x];
+      return sm[DIM3 ? (s0 + 1) % 3 : 0][r][y][x];
+    };
+    viscous_face<T, DIM3>(d, V, Mt, ipr, tref, fv);
+  };
+  T fz_prev[4] = {T(0), T(0), T(0), T(0)};
   if (a.viscous) {
-#pragma unroll
-    for (int l = 1; l < 5; ++l) d[l] += (double)(fx[tz][ty][tx + 1][l - 1] - fx[tz][ty][tx][l - 1]);
-#pragma unroll
-    for (int l = 1; l < 5; ++l) d[l] += (double)(fy[tz][ty + 1][tx][l - 1] - fy[tz][ty][tx][l - 1]);
-    if constexpr (DIM3) {
-#pragma unroll
-      for (int l = 1; l < 5; ++l) d[l] += (double)(fz[tz + 1][ty][tx][l - 1] - fz[tz][ty][tx][l - 1]);
+    if (DIM3) {
+      load_plane(k0 - 1);
+      load_plane(k0);
+      __syncthreads();
+      if (inside) face(2, tx + 1, ty + 1, k0 - 1, fz_prev);
     }
   }
-  if (!a.update) {
+  const double dt = a.update ? *a.dt : 0.0;
+  for (int k = k0; k < k1; ++k) {
+    T fz_next[4] = {T(0), T(0), T(0), T(0)};
+    if (a.viscous) {
+      if (DIM3) load_plane(k + 1);
+      else load_plane(k);
+      __syncthreads();
+      if (inside) {
+        face(0, tx, ty + 1, k, fxs[ty][tx]);
+        if (tx == TX - 1 || i == b.mx - 1) face(0, tx + 1, ty + 1, k, fxs[ty][tx + 1]);
+        face(1, tx + 1, ty, k, fys[ty][tx]);
+        if (ty == TY - 1 || j == b.my - 1) face(1, tx + 1, ty + 1, k, fys[ty + 1][tx]);
+        if (DIM3) face(2, tx + 1, ty + 1, k, fz_next);
+      }
+      __syncthreads();
+    }
+    if (inside) {
+      const long long qi = b.iq(i, j, k);
+      double d[5];
 #pragma unroll
-    for (int l = 0; l < 5; ++l) dq[l * b.n + qi] = d[l];
-    return;
+      for (int l = 0; l < 5; ++l) d[l] = dq[l * b.n + qi];
+      if (a.viscous) {
+#pragma unroll
+        for (int l = 1; l < 5; ++l) d[l] += (double)(fxs[ty][tx + 1][l - 1] - fxs[ty][tx][l - 1]);
+#pragma unroll
+        for (int l = 1; l < 5; ++l) d[l] += (double)(fys[ty + 1][tx][l - 1] - fys[ty][tx][l - 1]);
+        if (DIM3) {
+#pragma unroll
+          for (int l = 1; l < 5; ++l) d[l] += (double)(fz_next[l - 1] - fz_prev[l - 1]);
+        }
+      }
+      if (!a.update) {
+#pragma unroll
+        for (int l = 0; l < 5; ++l) dq[l * b.n + qi] = d[l];
+      } else {
+        const long long p = b.id(i, j, k);
+        const double dtj = dt / b.jac[p];
+        double cv[5];
+#pragma unroll
+        for (int l = 0; l < 5; ++l) cv[l] = a.a * a.qn.cv[l * P + p] + a.bcoef * a.in.cv[l * P + p] + a.c * dtj * d[l];
+        if (!DIM3) cv[3] = 0;
+        const double rho = cv[0];
+        const double di = 1.0 / cv[0];
+        const double u = cv[1] * di, v = cv[2] * di, w = cv[3] * di;
+        const double V2 = u * u + v * v + w * w;
+        const double pr = (kGamma - 1) * (cv[4] - 0.5 * rho * V2);
+        const double tt = pr * kMwD * di / kRuD;
+#pragma unroll
+        for (int l = 0; l < 5; ++l) a.out.cv[l * P + p] = cv[l];
+        a.out.bv[p] = rho;
+        a.out.bv[P + p] = u;
+        a.out.bv[2 * P + p] = v;
+        a.out.bv[3 * P + p] = w;
+        a.out.bv[4 * P + p] = pr;
+        a.out.bv[5 * P + p] = tt;
+        a.out.mul[p] = sutherland(tt);
+        if (!(rho > 0.0) || !(pr > 0.0) || !(tt > 0.0)) atomicOr(a.flags, (unsigned)OSTC_FLAG_NONPOSITIVE);
+        if (isnan(cv[0]) || isnan(cv[1]) || isnan(cv[2]) || isnan(cv[3]) || isnan(cv[4]))
+          atomicOr(a.flags, (unsigned)OSTC_FLAG_NAN);
+      }
+    }
+#pragma unroll
+    for (int l = 0; l < 4; ++l) fz_prev[l] = fz_next[l];
   }
-  const long long P = b.plane, p = b.id(i, j, k);
-  const double dt = *a.dt;
-  const double dtj = dt / b.jac[p];
-  double cv[5];
-#pragma unroll
-  for (int l = 0; l < 5; ++l) cv[l] = a.a * a.qn.cv[l * P + p] + a.bcoef * a.in.cv[l * P + p] + a.c * dtj * d[l];
-  if (!DIM3) cv[3] = 0;
-  const double rho = cv[0];
-  const double di = 1.0 / cv[0];
-  const double u = cv[1] * di, v = cv[2] * di, w = cv[3] * di;
-  const double V2 = u * u + v * v + w * w;
-  const double pr = (kGamma - 1) * (cv[4] - 0.5 * rho * V2);
-  const double tt = pr * kMwD * di / kRuD;
-#pragma unroll
-  for (int l = 0; l < 5; ++l) a.out.cv[l * P + p] = cv[l];
-  a.out.bv[p] = rho;
-  a.out.bv[P + p] = u;
-  a.out.bv[2 * P + p] = v;
-  a.out.bv[3 * P + p] = w;
-  a.out.bv[4 * P + p] = pr;
-  a.out.bv[5 * P + p] = tt;
-  a.out.mul[p] = sutherland(tt);
-  if (!(rho > 0.0) || !(pr > 0.0) || !(tt > 0.0)) atomicOr(a.flags, (unsigned)OSTC_FLAG_NONPOSITIVE);
-  if (isnan(cv[0]) || isnan(cv[1]) || isnan(cv[2]) || isnan(cv[3]) || isnan(cv[4]))
-    atomicOr(a.flags, (unsigned)OSTC_FLAG_NAN);
 }
 
 // ------------------------------------------------------------------------------ boundaries
@@ -789,11 +870,19 @@ void launch_visc(ostc_ctx *ctx, BlockRes &B, const StageArgs &a) {
   const DevBlock &b = B.db;
   long tok = begin_t(ctx, "visc_update");
   if (b.mz > 1) {
-    dim3 grid((b.mx + 31) / 32, (b.my + 3) / 4, (b.mz + 1) / 2);
-    k_visc_update<T, true, 32, 4, 2><<<grid, dim3(32, 4, 2), 0, ctx->stream>>>(b, a, B.dq);
+    constexpr int TX = 32, TY = 4;
+    const long long cols = (long long)((b.mx + TX - 1) / TX) * ((b.my + TY - 1) / TY);
+    int nseg = (int)std::max<long long>(1, (ctx->sm_count * 8 + cols - 1) / cols);
+    int kseg = std::max(4, (b.mz + nseg - 1) / nseg);
+    nseg = (b.mz + kseg - 1) / kseg;
+    dim3 grid((b.mx + TX - 1) / TX, (b.my + TY - 1) / TY, nseg);
+    k_visc_update<T, true, TX, TY>
+        <<<grid, dim3(TX, TY, 1), visc_smem_bytes<T, true, TX, TY>(), ctx->stream>>>(b, a, B.dq, kseg);
   } else {
-    dim3 grid((b.mx + 31) / 32, (b.my + 7) / 8, 1);
-    k_visc_update<T, false, 32, 8, 1><<<grid, dim3(32, 8, 1), 0, ctx->stream>>>(b, a, B.dq);
+    constexpr int TX = 32, TY = 4;
+    dim3 grid((b.mx + TX - 1) / TX, (b.my + TY - 1) / TY, 1);
+    k_visc_update<T, false, TX, TY>
+        <<<grid, dim3(TX, TY, 1), visc_smem_bytes<T, false, TX, TY>(), ctx->stream>>>(b, a, B.dq, 1);
   }
   end_t(ctx, tok);
 }
@@ -830,6 +919,10 @@ bool set_march_attrs() {
   set((const void *)k_flux_march<2, 3, 4, T>, 3);
   set((const void *)k_flux_march<2, 4, 3, T>, 4);
   set((const void *)k_flux_march<2, 4, 4, T>, 4);
+  ok = ok && cudaFuncSetAttribute((const void *)k_visc_update<T, true, 32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)visc_smem_bytes<T, true, 32, 4>()) == cudaSuccess;
+  ok = ok && cudaFuncSetAttribute((const void *)k_visc_update<T, false, 32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)visc_smem_bytes<T, false, 32, 4>()) == cudaSuccess;
   return ok;
 }
 

@@ -86,7 +86,7 @@ def test_rk3_trajectory(built, tmp_path, dims, recon, rs, steps):
 def test_mixed_precision_accuracy(built, tmp_path):
     """Mixed path (FP32 reconstruction/Riemann/viscous arithmetic, FP64 state and EOS) against the
     FP64 path after 100 steps: relative L2 error of the conserved variables <= 1e-6."""
-    case = oc.mixing_layer_3d(mx=48, my=32, mz=24)
+    case = oc.mixing_layer_3d(mx=96, my=64, mz=48)
     d = oc.write_case(case, tmp_path / "mixed")
     a = ostc.Solver(str(d))
     a.set_state(case.bv)
