@@ -117,15 +117,14 @@ __global__ void __launch_bounds__(256) k_cfl_dt(DevBlock b, DevState s, double c
 // ------------------------------------------------------------------------------ inviscid flux
 
 // Resident blocks per SM the x sweep is compiled for (register budget 65536 / (128 * this)).
-#ifndef OSTC_FLUXX_MINB
-#define OSTC_FLUXX_MINB 2
-#endif
+template <typename T> struct FluxXOcc { static constexpr int blocks = 2; };
+template <> struct FluxXOcc<float> { static constexpr int blocks = 4; };
 
 // x sweep.  A block of 128 threads stages 127 + 2*NG nodes of one (j,k) row in shared memory
 // (coalesced along i), computes the 128 faces i0-1/2 .. i0+126+1/2 (one per thread) and finalises
 // the 127 nodes between them: dq = -(fc(i+1/2) - fc(i-1/2)) + central correction.
 template <int NG, int RS, typename T>
-__global__ void __launch_bounds__(128, OSTC_FLUXX_MINB) k_flux_x(DevBlock b, DevState s, double *__restrict__ dq) {
+__global__ void __launch_bounds__(128, FluxXOcc<T>::blocks) k_flux_x(DevBlock b, DevState s, double *__restrict__ dq) {
   constexpr int L = 127;
   constexpr int NP = L + 2 * NG;
   __shared__ T sq[6][NP];
@@ -189,18 +188,42 @@ __global__ void __launch_bounds__(128, OSTC_FLUXX_MINB) k_flux_x(DevBlock b, Dev
   }
 }
 
+// Asynchronous global -> shared copies (cp.async, Ampere and later, plain non-bulk form).
+__device__ __forceinline__ void cp_async8(void *smem_dst, const void *gsrc) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Resident 64-thread blocks per SM the march kernel is compiled for.
+template <typename T> struct MarchOcc { static constexpr int blocks = 4; };
+template <> struct MarchOcc<float> { static constexpr int blocks = 6; };
+
 // y (DIR = 1) or z (DIR = 2) sweep.  Thread (i, o) marches nodes c = s0..s1-1 of its column (o is
 // k for y, j for z); warps are contiguous in i, so every load of a new node is coalesced.  A
 // per-thread ring in shared memory keeps the last 2*NG+1 nodes' cv(5), p and node flux(5); the
-// metric row and Jacobian of the face's two nodes travel in registers (node c+1 is re-read, an L1/L2
-// hit, when its face comes up).  Segments of `seg` nodes split long columns across blocks.
+// metric row and Jacobian of the face's two nodes travel in registers.
+// FP32 instantiation: the raw FP64 data of the next node (cv 5, rho/u/v/w/p 5, metric row 3,
+// Jacobian 1) and the metric row + Jacobian of the face's right node are prefetched with cp.async
+// one iteration ahead (double-buffered) so their latency hides behind the face computation
+// (measured 1.18x).  FP64 instantiation: plain loads - the prefetch buffers would cut it from 4 to 3
+// resident blocks, which costs more than the latency it hides (measured 0.79x).  Segments of `seg`
+// nodes split long columns across blocks.
 template <int DIR, int NG, int RS, typename T>
-__global__ void __launch_bounds__(64, 4) k_flux_march(DevBlock b, DevState s, double *__restrict__ dq, int seg) {
+__global__ void __launch_bounds__(64, MarchOcc<T>::blocks) k_flux_march(DevBlock b, DevState s,
+                                                                         double *__restrict__ dq, int seg) {
   constexpr int W = 2 * NG + 1;
   constexpr int NV = 11;
+  constexpr int NRAW = 14;
+  constexpr bool PIPE = std::is_same_v<T, float>;
   extern __shared__ __align__(16) unsigned char smraw[];
-  T *ring = reinterpret_cast<T *>(smraw);
   const int nthr = blockDim.x * blockDim.y;
+  T *ring = reinterpret_cast<T *>(smraw);
+  // prefetch buffers (FP32 only): raw [2][NRAW][nthr], metric [2][4][nthr], 16-byte aligned
+  double *raw = reinterpret_cast<double *>(
+      (reinterpret_cast<size_t>(smraw) + (size_t)W * NV * nthr * sizeof(T) + 15) & ~(size_t)15);
+  double *mraw = raw + 2 * NRAW * nthr;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int o = blockIdx.y * blockDim.y + threadIdx.y;
@@ -215,33 +238,95 @@ __global__ void __launch_bounds__(64, 4) k_flux_march(DevBlock b, DevState s, do
   const long long base = DIR == 1 ? b.id(i, 0, o) : b.id(i, o, 0);
   const double *__restrict__ mrow = b.met + (long long)DIR * 3 * P;
   auto R = [&](int slot, int v) -> T & { return ring[(slot * NV + v) * nthr + tid]; };
-  auto load = [&](int n) {
+  auto Raw = [&](int sl, int v) -> double & { return raw[(sl * NRAW + v) * nthr + tid]; };
+  auto Mraw = [&](int sl, int v) -> double & { return mraw[(sl * 4 + v) * nthr + tid]; };
+  auto prefetch_node = [&](int n, int sl) {
     const long long p = base + (long long)n * stride;
+#pragma unroll
+    for (int l = 0; l < 5; ++l) cp_async8(&Raw(sl, l), s.cv + l * P + p);
+#pragma unroll
+    for (int l = 0; l < 5; ++l) cp_async8(&Raw(sl, 5 + l), s.bv + l * P + p);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) cp_async8(&Raw(sl, 10 + c), mrow + c * P + p);
+    cp_async8(&Raw(sl, 13), b.jac + p);
+  };
+  auto prefetch_metric = [&](int n, int sl) {
+    const long long p = base + (long long)n * stride;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) cp_async8(&Mraw(sl, c), mrow + c * P + p);
+    cp_async8(&Mraw(sl, 3), b.jac + p);
+  };
+  // node n from its raw FP64 values into the ring
+  auto commit_node = [&](int n, const double *cv, const double *bv, const double *km, double jac) {
     const int slot = (n + NG) % W;
     T bb[5], kk[3];
 #pragma unroll
     for (int l = 0; l < 5; ++l) {
-      R(slot, l) = (T)s.cv[l * P + p];
-      bb[l] = (T)s.bv[l * P + p];
+      R(slot, l) = (T)cv[l];
+      bb[l] = (T)bv[l];
     }
     R(slot, 5) = bb[4];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) kk[c] = (T)mrow[c * P + p];
+    for (int c = 0; c < 3; ++c) kk[c] = (T)km[c];
     T f[5];
-    node_flux<T>(bb, (T)s.cv[4 * P + p], kk, (T)b.jac[p], f);
+    node_flux<T>(bb, (T)cv[4], kk, (T)jac, f);
 #pragma unroll
     for (int l = 0; l < 5; ++l) R(slot, 6 + l) = f[l];
   };
-  for (int n = s0 - NG; n <= s0 + NG - 2; ++n) load(n);
+  auto load_direct = [&](int n) {
+    const long long p = base + (long long)n * stride;
+    double cv[5], bv[5], km[3];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+      cv[l] = s.cv[l * P + p];
+      bv[l] = s.bv[l * P + p];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) km[c] = mrow[c * P + p];
+    commit_node(n, cv, bv, km, b.jac[p]);
+  };
+  for (int n = s0 - NG; n <= s0 + NG - 2; ++n) load_direct(n);
+  if constexpr (PIPE) {
+    // first stage: node s0-1+NG and the right-node metric of face s0-1/2 (node s0)
+    prefetch_node(s0 - 1 + NG, 0);
+    prefetch_metric(s0, 0);
+    cp_async_commit();
+  }
   T fprev[5] = {T(0), T(0), T(0), T(0), T(0)};
   long long pc = base + (long long)(s0 - 1) * stride;
   T mt0[3] = {(T)mrow[pc], (T)mrow[P + pc], (T)mrow[2 * P + pc]};
   T j0 = (T)b.jac[pc];
   for (int c = s0 - 1; c < s1; ++c) {
-    load(c + NG);
-    const long long pn = pc + stride;
-    const T mt1[3] = {(T)mrow[pn], (T)mrow[P + pn], (T)mrow[2 * P + pn]};
-    const T j1 = (T)b.jac[pn];
+    T mt1[3], j1;
+    if constexpr (PIPE) {
+      cp_async_wait_all();
+      // both prefetch buffers alternate slots, so a copy never targets the slot just read
+      const int ms = (c - s0 + 1) & 1;
+      double cv[5], bv[5], km[3];
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        cv[l] = Raw(ms, l);
+        bv[l] = Raw(ms, 5 + l);
+      }
+#pragma unroll
+      for (int q3 = 0; q3 < 3; ++q3) km[q3] = Raw(ms, 10 + q3);
+      commit_node(c + NG, cv, bv, km, Raw(ms, 13));
+#pragma unroll
+      for (int q3 = 0; q3 < 3; ++q3) mt1[q3] = (T)Mraw(ms, q3);
+      j1 = (T)Mraw(ms, 3);
+      if (c + 1 < s1) {
+        prefetch_node(c + 1 + NG, ms ^ 1);
+        prefetch_metric(c + 2, ms ^ 1);
+        cp_async_commit();
+      }
+    } else {
+      load_direct(c + NG);
+      const long long pn = pc + stride;
+#pragma unroll
+      for (int q3 = 0; q3 < 3; ++q3) mt1[q3] = (T)mrow[q3 * P + pn];
+      j1 = (T)b.jac[pn];
+      pc = pn;
+    }
     const int b0 = (c + 1) % W;
     auto q = [&](int st, int v) -> T {
       int sl = b0 + st;
@@ -269,11 +354,18 @@ __global__ void __launch_bounds__(64, 4) k_flux_march(DevBlock b, DevState s, do
     }
 #pragma unroll
     for (int l = 0; l < 5; ++l) fprev[l] = fc[l];
-    pc = pn;
 #pragma unroll
     for (int q3 = 0; q3 < 3; ++q3) mt0[q3] = mt1[q3];
     j0 = j1;
   }
+  if constexpr (PIPE) cp_async_wait_all();
+}
+
+// Dynamic shared memory of one 64-thread march block: the ring, plus the prefetch buffers in FP32.
+template <typename T>
+constexpr size_t march_smem_bytes(int ng) {
+  return (size_t)(2 * ng + 1) * 11 * 64 * sizeof(T) +
+         (std::is_same_v<T, float> ? 16 + (2 * 14 + 8) * 64 * sizeof(double) : 0);
 }
 
 // ------------------------------------------------------------------------------ viscous + update
@@ -845,7 +937,7 @@ int launch_flux(ostc_ctx *ctx, BlockRes &B, DevState in) {
     nseg = (n_dir + seg - 1) / seg;
     dim3 grid((b.mx + 31) / 32, (n_o + 1) / 2, nseg);
     dim3 block(32, 2, 1);
-    const size_t smem = (size_t)(2 * ng + 1) * 11 * 64 * sizeof(T);
+    const size_t smem = march_smem_bytes<T>(ng);
     long tok = begin_t(ctx, dir == 1 ? "flux_y" : "flux_z");
 #define OSTC_MARCH(D, N, R) k_flux_march<D, N, R, T><<<grid, block, smem, ctx->stream>>>(b, in, B.dq, seg)
     if (dir == 1) {
@@ -902,13 +994,13 @@ void launch_bcs(ostc_ctx *ctx, int block, DevState out) {
 
 DevState state_of(BlockRes &B, int s) { return DevState{B.cv[s], B.bv[s], B.mul[s]}; }
 
-// The march kernels stage 2*ngg+1 nodes x 11 values x 64 threads in dynamic shared memory (up to
-// 51 KB in FP64); raise the per-kernel limit once, outside any stream capture.
+// The march kernels stage 2*ngg+1 nodes x 11 values x 64 threads (plus the FP32 prefetch buffers)
+// in dynamic shared memory (up to 51 KB); raise the per-kernel limit once, outside any stream capture.
 template <typename T>
 bool set_march_attrs() {
   bool ok = true;
   auto set = [&](const void *fn, int ng) {
-    const int bytes = (2 * ng + 1) * 11 * 64 * (int)sizeof(T);
+    const int bytes = (int)march_smem_bytes<T>(ng);
     ok = ok && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
   };
   set((const void *)k_flux_march<1, 3, 3, T>, 3);

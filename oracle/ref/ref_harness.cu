@@ -1,0 +1,118 @@
+// ref_harness.cu -- runs the reference solver's own RK3 path on a case directory for parity checks.
+// TEST INFRASTRUCTURE ONLY (built by oracle/ref/build_ref.sh into oracle/_ref/ref_harness).
+//
+// Usage (cwd = case directory holding ./input/setup.txt, grid and boundary files):
+//   ref_harness state_in.bin state_out.bin
+// It builds cfd::Parameter, cfd::Mesh and cfd::Driver<Air, Laminar> as the reference's main() does
+// (main.cu:8-136), replaces the freshly initialised interior primitive variables with the ones in
+// state_in.bin ([block][6][mz][my][mx] doubles), runs the reference's
+// Driver::initialize_computation() and RK3() (RK.cuh:19-228) for total_step steps, and writes the
+// interior cv[5] and bv[6] of every block, then the physical time, to state_out.bin.
+#include <cstdio>
+#include <exception>
+#include <vector>
+
+#include "Parameter.h"
+#include "Mesh.h"
+#include "Driver.cuh"
+#include "Simulate.cuh"
+#include "SST.cuh"
+
+namespace {
+// element (i,j,k) of variable l of a VectorField3D with ngg ghosts (gxl_lib/Array.cuh:209-230)
+long long padded_index(int mx, int my, int mz, int ngg, int i, int j, int k, int l) {
+  const long long disp2 = mx + 2 * ngg;
+  const long long disp1 = (my + 2 * ngg) * disp2;
+  const long long dispt = (disp1 + disp2 + 1) * ngg;
+  const long long sz = (long long)(mx + 2 * ngg) * (my + 2 * ngg) * (mz + 2 * ngg);
+  return k * disp1 + j * disp2 + i + dispt + l * sz;
+}
+
+const char *g_stage = "start";
+}  // namespace
+
+int run(const char *fin, const char *fout, int *argc, char ***argv) {
+  g_stage = "Parameter";
+  cfd::Parameter parameter(argc, argv);
+  // the reference reads total_simulation_time without a default (Simulate.cuh:62, RK.cuh:64); the run
+  // is bounded by total_step instead
+  parameter.update_parameter("total_simulation_time", 1e30);
+  g_stage = "Mesh";
+  cfd::Mesh mesh(parameter);
+  if (!parameter.get_bool("turbulence")) parameter.update_parameter("turbulence_method", 0);
+  g_stage = "Driver";
+  cfd::Driver<MixtureModel::Air, cfd::Laminar> driver(parameter, mesh);
+
+  g_stage = "state_in";
+  std::FILE *f = std::fopen(fin, "rb");
+  if (!f) {
+    std::fprintf(stderr, "cannot open %s\n", fin);
+    return 2;
+  }
+  for (int b = 0; b < mesh.n_block; ++b) {
+    const int mx = mesh[b].mx, my = mesh[b].my, mz = mesh[b].mz, ngg = mesh[b].ngg;
+    const long long n = (long long)mx * my * mz;
+    const long long sz = (long long)(mx + 2 * ngg) * (my + 2 * ngg) * (mz + 2 * ngg);
+    std::vector<double> in(6 * n), pad(6 * sz);
+    if (std::fread(in.data(), sizeof(double), in.size(), f) != in.size()) {
+      std::fprintf(stderr, "short state file\n");
+      return 2;
+    }
+    cudaMemcpy(pad.data(), driver.field[b].h_ptr->bv.data(), pad.size() * sizeof(double), cudaMemcpyDeviceToHost);
+    for (int l = 0; l < 6; ++l)
+      for (int k = 0; k < mz; ++k)
+        for (int j = 0; j < my; ++j)
+          for (int i = 0; i < mx; ++i)
+            pad[padded_index(mx, my, mz, ngg, i, j, k, l)] = in[l * n + ((long long)k * my + j) * mx + i];
+    cudaMemcpy(driver.field[b].h_ptr->bv.data(), pad.data(), pad.size() * sizeof(double), cudaMemcpyHostToDevice);
+  }
+  std::fclose(f);
+
+  g_stage = "initialize_computation";
+  driver.initialize_computation();
+  g_stage = "RK3";
+  cfd::RK3<MixtureModel::Air, cfd::Laminar>(driver);
+  cudaDeviceSynchronize();
+
+  g_stage = "state_out";
+  f = std::fopen(fout, "wb");
+  for (int b = 0; b < mesh.n_block; ++b) {
+    const int mx = mesh[b].mx, my = mesh[b].my, mz = mesh[b].mz, ngg = mesh[b].ngg;
+    const long long n = (long long)mx * my * mz;
+    const long long sz = (long long)(mx + 2 * ngg) * (my + 2 * ngg) * (mz + 2 * ngg);
+    std::vector<double> cv(5 * sz), bv(6 * sz), out(11 * n);
+    cudaMemcpy(cv.data(), driver.field[b].h_ptr->cv.data(), cv.size() * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaMemcpy(bv.data(), driver.field[b].h_ptr->bv.data(), bv.size() * sizeof(double), cudaMemcpyDeviceToHost);
+    for (int l = 0; l < 11; ++l)
+      for (int k = 0; k < mz; ++k)
+        for (int j = 0; j < my; ++j)
+          for (int i = 0; i < mx; ++i) {
+            const double v = l < 5 ? cv[padded_index(mx, my, mz, ngg, i, j, k, l)]
+                                   : bv[padded_index(mx, my, mz, ngg, i, j, k, l - 5)];
+            out[l * n + ((long long)k * my + j) * mx + i] = v;
+          }
+    std::fwrite(out.data(), sizeof(double), out.size(), f);
+  }
+  const double t = parameter.get_real("solution_time");
+  std::fwrite(&t, sizeof(double), 1, f);
+  std::fclose(f);
+  const cudaError_t e = cudaGetLastError();
+  std::printf("ref_harness: done (%s), t = %.17g\n", cudaGetErrorString(e), t);
+  return e == cudaSuccess ? 0 : 1;
+}
+
+int main(int argc, char *argv[]) {
+  if (argc < 3) {
+    std::fprintf(stderr, "usage: ref_harness state_in.bin state_out.bin\n");
+    return 2;
+  }
+  std::setvbuf(stdout, nullptr, _IONBF, 0);
+  int one = 1;
+  char **av = argv;
+  try {
+    return run(argv[1], argv[2], &one, &av);
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "ref_harness: exception in stage %s: %s\n", g_stage, e.what());
+    return 5;
+  }
+}

@@ -1,0 +1,100 @@
+"""Runs the reference solver's own RK3 path (oracle/_ref/ref_harness, built by oracle/ref/build_ref.sh
+from the reference sources) on a synthetic case.  TEST INFRASTRUCTURE: used only to generate the
+golden fixtures under tests/golden/ that pin the CPU oracle and the CUDA path to the reference.
+
+The case directory gets the same setup.txt, grid and boundary files the library reads, plus the
+keys the reference's Driver needs for a plain (non-mixing-layer) start: a `freestream` inflow struct
+for its default initialisation and reference state, and neutral values for statistics / sponge /
+digital-filter keys it reads without defaults.  The harness then overwrites the interior primitive
+state with the case's seeded state and runs Driver::initialize_computation() + RK3() for `steps`
+steps on GPU 0.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+HARNESS = HERE / "_ref" / "ref_harness"
+
+EXTRA = """
+// keys the reference reads without defaults (parity runs only)
+int initial = 0
+string reference_state = freestream
+string default_init = freestream
+int output_file = 100000000
+int output_screen = 100000000
+int slice_frequency = 100000000
+real cfl_steady = 1
+bool rho_p_correlation = 0
+bool stat_tke_budget = 0
+bool stat_species_velocity_correlation = 0
+bool stat_species_dissipation_rate = 0
+real spongeCoefficient = 1e-8
+string mesh_prefix = grid
+string result_file = none
+int reynolds_stress_supplier = 0
+real delta_omega = 1e-3
+real total_simulation_time = 1e30
+bool use_df = 0
+array real sc_passive_scalar {
+    0.5
+}
+array real sct_passive_scalar {
+    1.0
+}
+array string stat_rey_1st {
+    u
+}
+array string stat_species {
+    all
+}
+struct freestream = {
+    string type = inflow
+    int label = 5
+    real mach = @MACH@
+    real pressure = @P@
+    real temperature = @T@
+    real u = 1.0
+    real v = 0.0
+    real w = 0.0
+}
+"""
+
+
+def write_reference_case(case, steps: int, directory: os.PathLike) -> Path:
+    import ostc_cases as oc
+
+    d = Path(directory)
+    inp = d / "input"
+    oc.write_case(case, inp)
+    setup = (inp / "setup.txt").read_text()
+    setup = setup.replace(f"int total_step = {case.steps}", f"int total_step = {steps}")
+    setup = setup.replace("int initial = 1\n", "")
+    p0 = float(case.bv[4].flat[0])
+    t0 = float(case.bv[5].flat[0])
+    setup += EXTRA.replace("@MACH@", "0.5").replace("@P@", repr(p0)).replace("@T@", repr(t0))
+    (inp / "setup.txt").write_text(setup)
+    np.ascontiguousarray(case.bv, dtype=np.float64).tofile(d / "state_in.bin")
+    (d / "output" / "message").mkdir(parents=True, exist_ok=True)
+    return d
+
+
+def run_reference(case, steps: int, workdir: os.PathLike | None = None, timeout: int = 1800):
+    """Returns (cv[5,mz,my,mx], bv[6,mz,my,mx], physical time) after `steps` reference RK3 steps."""
+    if not HARNESS.exists():
+        raise FileNotFoundError(f"{HARNESS} not built (oracle/ref/build_ref.sh)")
+    d = Path(workdir) if workdir else Path(tempfile.mkdtemp(prefix="ostc_ref_"))
+    write_reference_case(case, steps, d)
+    r = subprocess.run([str(HARNESS), "state_in.bin", "state_out.bin"], cwd=d, capture_output=True, text=True,
+                       timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference harness failed ({r.returncode}):\n{r.stdout[-4000:]}\n{r.stderr[-3000:]}")
+    raw = np.fromfile(d / "state_out.bin", dtype=np.float64)
+    n = case.nodes
+    out = raw[: 11 * n].reshape((11,) + case.bv.shape[1:])
+    return out[:5].copy(), out[5:].copy(), float(raw[11 * n])
