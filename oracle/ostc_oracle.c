@@ -3,9 +3,11 @@
  * calorically perfect air.  TEST INFRASTRUCTURE: only tests/, the smoke check and bench.py's CPU
  * baseline use it, and only as the checker / timed CPU baseline.
  *
- * Parity unpinned: the reference ships no tests or golden vectors for this path, and its code runs
- * only as CUDA device code.  The restatement is checked against known-answer properties
- * (tests/test_oracle.py); pinning it against the reference's own FP64 CUDA build is pending.
+ * Parity pin: the reference ships no tests or golden vectors for this path and runs only as CUDA, so
+ * its own FP64 build (oracle/ref/build_ref.sh: the reference sources compiled for sm_100a with a
+ * single-rank MPI subset, driven through its Driver and RK3 by oracle/ref/ref_harness.cu) produced
+ * the fixtures in tests/golden/ (tests/golden/make_golden.py).  This restatement matches them to
+ * ~1e-14 relative after 20-100 SSP-RK3 steps (tests/test_golden.py).
  *
  * Build (see oracle/Makefile): gcc -O2 -ffp-contract=off -fPIC -shared.  Contraction is disabled so
  * that every product/sum is rounded exactly as written, like the reference's source order.
