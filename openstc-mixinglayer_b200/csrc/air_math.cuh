@@ -394,6 +394,163 @@ __device__ __forceinline__ void hllc(const T *pl, const T *pr, const T *mt0, con
   fc[4] = Q * q[5] * irk + pc * jac * (sk * pm * sm * gradK - sm * q[4] * Uk);
 }
 
+// riemannSolver_laxFriedrich<Air> (RiemannSolver.cuh:420-460): face-averaged metric, the larger
+// spectral radius of the two sides.
+template <typename T>
+__device__ __forceinline__ void lax_friedrichs(const T *pl, const T *pr, const T *mt0, const T *mt1, T j0, T j1,
+                                               T *fc) {
+  const T kx = T(0.5) * (mt0[0] + mt1[0]);
+  const T ky = T(0.5) * (mt0[1] + mt1[1]);
+  const T kz = T(0.5) * (mt0[2] + mt1[2]);
+  const T gradK = tsqrt(kx * kx + ky * ky + kz * kz);
+  const T Ukl = pl[1] * kx + pl[2] * ky + pl[3] * kz;
+  const T Ukr = pr[1] * kx + pr[2] * ky + pr[3] * kz;
+  const T cl = tsqrt(T(kGamma) * pl[4] / pl[0]);
+  const T cr = tsqrt(T(kGamma) * pr[4] / pr[0]);
+  const T sr = tmax(tabs(Ukl) + cl * gradK, tabs(Ukr) + cr * gradK);
+  const T hj = T(0.25) * (j0 + j1);
+  const T rUl = pl[0] * Ukl, rUr = pr[0] * Ukr;
+  fc[0] = (rUl + rUr - sr * (pr[0] - pl[0])) * hj;
+  fc[1] = (rUl * pl[1] + rUr * pr[1] + kx * (pl[4] + pr[4]) - sr * (pr[1] * pr[0] - pl[1] * pl[0])) * hj;
+  fc[2] = (rUl * pl[2] + rUr * pr[2] + ky * (pl[4] + pr[4]) - sr * (pr[2] * pr[0] - pl[2] * pl[0])) * hj;
+  fc[3] = (rUl * pl[3] + rUr * pr[3] + kz * (pl[4] + pr[4]) - sr * (pr[3] * pr[0] - pl[3] * pl[0])) * hj;
+  fc[4] = ((pl[5] + pl[4]) * Ukl + (pr[5] + pr[4]) * Ukr - sr * (pr[5] - pl[5])) * hj;
+}
+
+// Harten entropy-fix threshold of one node (compute_entropy_fix_delta<Air>, InviscidScheme.cu:417-456):
+// factor * (|U| + |V| (+ |W|) + c * mean |grad xi|).  m: the 9 metric entries of the node, b: rho..p.
+template <typename T>
+__device__ __forceinline__ T entropy_fix_delta(const T *m, const T *b, T factor, bool dim3) {
+  const T U = tabs(b[1] * m[0] + b[2] * m[1] + b[3] * m[2]);
+  const T V = tabs(b[1] * m[3] + b[2] * m[4] + b[3] * m[5]);
+  const T W = tabs(b[1] * m[6] + b[2] * m[7] + b[3] * m[8]);
+  const T kx = tsqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+  const T ky = tsqrt(m[3] * m[3] + m[4] * m[4] + m[5] * m[5]);
+  const T kz = tsqrt(m[6] * m[6] + m[7] * m[7] + m[8] * m[8]);
+  const T c = tsqrt(T(kGamma) * b[4] / b[0]);
+  if (!dim3) return factor * (U + V + c * T(0.5) * (kx + ky));
+  return factor * (U + V + W + c * (kx + ky + kz) / T(3));
+}
+
+// riemannSolver_Roe<Air> (RiemannSolver.cuh:279-417): the half sum of the two sides' physical fluxes
+// (each with its own node's metric and Jacobian, compute_half_sum_left_right_flux :232-277) plus
+// the Roe dissipation with Harten's entropy fix on |lambda| below the face-averaged threshold.
+template <typename T>
+__device__ __forceinline__ void roe(const T *pl, const T *pr, const T *mt0, const T *mt1, T j0, T j1, T d0, T d1,
+                                    T *fc) {
+  {
+    const T jx = j0 * mt0[0], jy = j0 * mt0[1], jz = j0 * mt0[2];
+    const T Uk = pl[1] * jx + pl[2] * jy + pl[3] * jz;
+    const T co = Uk * pl[0];
+    fc[0] = T(0.5) * co;
+    fc[1] = T(0.5) * (co * pl[1] + pl[4] * jx);
+    fc[2] = T(0.5) * (co * pl[2] + pl[4] * jy);
+    fc[3] = T(0.5) * (co * pl[3] + pl[4] * jz);
+    fc[4] = T(0.5) * Uk * (pl[4] + pl[5]);
+  }
+  {
+    const T jx = j1 * mt1[0], jy = j1 * mt1[1], jz = j1 * mt1[2];
+    const T Uk = pr[1] * jx + pr[2] * jy + pr[3] * jz;
+    const T co = Uk * pr[0];
+    fc[0] += T(0.5) * co;
+    fc[1] += T(0.5) * (co * pr[1] + pr[4] * jx);
+    fc[2] += T(0.5) * (co * pr[2] + pr[4] * jy);
+    fc[3] += T(0.5) * (co * pr[3] + pr[4] * jz);
+    fc[4] += T(0.5) * Uk * (pr[4] + pr[5]);
+  }
+  const T dl = tsqrt(pl[0]), dr = tsqrt(pr[0]);
+  const T inv = T(1) / (dl + dr);
+  const T u = (dl * pl[1] + dr * pr[1]) * inv;
+  const T v = (dl * pl[2] + dr * pr[2]) * inv;
+  const T w = (dl * pl[3] + dr * pr[3]) * inv;
+  const T ek = T(0.5) * (u * u + v * v + w * w);
+  const T hl = (pl[5] + pl[4]) / pl[0];
+  const T hr = (pr[5] + pr[4]) / pr[0];
+  const T h = (dl * hl + dr * hr) * inv;
+  const T gm1 = T(kGamma - 1);
+  const T c = tsqrt(gm1 * (h - ek));
+  T kx = T(0.5) * (mt0[0] + mt1[0]);
+  T ky = T(0.5) * (mt0[1] + mt1[1]);
+  T kz = T(0.5) * (mt0[2] + mt1[2]);
+  const T gradK = tsqrt(kx * kx + ky * ky + kz * kz);
+  T Uk = kx * u + ky * v + kz * w;
+  T ch[3] = {Uk - gradK * c, Uk, Uk + gradK * c};
+  const T da = T(0.5) * (d0 + d1);
+#pragma unroll
+  for (int n = 0; n < 3; ++n) {
+    ch[n] = tabs(ch[n]);
+    if (ch[n] < da) ch[n] = T(0.5) * (ch[n] * ch[n] / da + da);
+  }
+  const T igk = T(1) / gradK;
+  kx *= igk;
+  ky *= igk;
+  kz *= igk;
+  Uk *= igk;
+  const T ja = T(0.5) * (j0 + j1);
+  const T q0 = ja * (pr[0] - pl[0]);
+  const T q1 = ja * (pr[0] * pr[1] - pl[0] * pl[1]);
+  const T q2 = ja * (pr[0] * pr[2] - pl[0] * pl[2]);
+  const T q3 = ja * (pr[0] * pr[3] - pl[0] * pl[3]);
+  const T q4 = ja * (pr[5] - pl[5]);
+  const T ic = T(1) / c;
+  T c1 = gm1 * (ek * q0 - u * q1 - v * q2 - w * q3 + q4) * ic * ic;
+  T c2 = (kx * q1 + ky * q2 + kz * q3 - Uk * q0) * ic;
+  const T c3 = q0 - c1;
+  const T L0 = T(0.5) * (c1 - c2);
+  const T L1 = kx * c3 - ((kz * v - ky * w) * q0 - kz * q2 + ky * q3) * ic;
+  const T L2 = ky * c3 - ((kx * w - kz * u) * q0 - kx * q3 + kz * q1) * ic;
+  const T L3 = kz * c3 - ((ky * u - kx * v) * q0 - ky * q1 + kx * q2) * ic;
+  const T L4 = T(0.5) * (c1 + c2);
+  const T b0 = -ch[0] * L0, b1 = -ch[1] * L1, b2 = -ch[1] * L2, b3 = -ch[1] * L3, b4 = -ch[2] * L4;
+  const T c0 = kx * b1 + ky * b2 + kz * b3;
+  c1 = c0 + b0 + b4;
+  c2 = c * (b4 - b0);
+  fc[0] += T(0.5) * c1;
+  fc[1] += T(0.5) * (u * c1 + kx * c2 - c * (kz * b2 - ky * b3));
+  fc[2] += T(0.5) * (v * c1 + ky * c2 - c * (kx * b3 - kz * b1));
+  fc[3] += T(0.5) * (w * c1 + kz * c2 - c * (ky * b1 - kx * b2));
+  fc[4] += T(0.5) * (h * c1 + Uk * c2 - c * c * c0 / gm1 +
+                     c * ((kz * v - ky * w) * b1 + (kx * w - kz * u) * b2 + (ky * u - kx * v) * b3));
+}
+
+// ------------------------------------------------------------------ primitive reconstruction
+
+// minmod with the reference's sign convention sgn(0) = +1 (Limiter.cuh:13-16, gxl_lib/Math.hpp:13-15).
+template <typename T>
+__device__ __forceinline__ T minmod(T a, T b) {
+  const T sa = a < T(0) ? T(-1) : T(1), sb = b < T(0) ? T(-1) : T(1);
+  return T(0.5) * (sa + sb) * tmin(tabs(a), tabs(b));
+}
+
+// Left/right primitive states at i+1/2 from nodes i-1, i, i+1, i+2 (v(m, l), m = -1..2), then the total
+// energy of each side (reconstruction<Air>, InviscidScheme.cu:163-215; first_order_reconstruct,
+// MUSCL_reconstruct (kappa = 1/3), NND2_reconstruct, Reconstruction.cu:5-45).
+template <typename T, class V>
+__device__ __forceinline__ void pv_reconstruct(const V &v, int recon, T *pl, T *pr) {
+#pragma unroll
+  for (int l = 0; l < 5; ++l) {
+    const T a = v(0, l), bq = v(1, l);
+    if (recon == 2 || recon == 3) {
+      const T di = a - v(-1, l), di1 = bq - a, di2 = v(2, l) - bq;
+      if (recon == 2) {
+        const T k1 = T(1) - T(1.0 / 3.0), k2 = T(1) + T(1.0 / 3.0);
+        pl[l] = a + T(0.25) * (k1 * minmod(di, di1) + k2 * minmod(di1, di));
+        pr[l] = bq - T(0.25) * (k1 * minmod(di2, di1) + k2 * minmod(di1, di2));
+      } else {
+        pl[l] = a + T(0.5) * minmod(di, di1);
+        pr[l] = bq - T(0.5) * minmod(di1, di2);
+      }
+    } else {
+      pl[l] = a;
+      pr[l] = bq;
+    }
+  }
+  const T el = T(0.5) * (pl[1] * pl[1] + pl[2] * pl[2] + pl[3] * pl[3]);
+  const T er = T(0.5) * (pr[1] * pr[1] + pr[2] * pr[2] + pr[3] * pr[3]);
+  pl[5] = el * pl[0] + pl[4] / T(kGamma - 1);
+  pr[5] = er * pr[0] + pr[4] / T(kGamma - 1);
+}
+
 // Whole AWENO face flux: interpolation then the selected Riemann solver (InviscidScheme.cu:333-345).
 template <int NG, int RS, typename T, class Q>
 __device__ __forceinline__ void aweno_face_flux(const Q &q, const T *mt0, const T *mt1, T j0, T j1, T *fc) {
@@ -401,6 +558,8 @@ __device__ __forceinline__ void aweno_face_flux(const Q &q, const T *mt0, const 
   aweno_interp<NG, T>(q, mt0, mt1, pl, pr);
   if constexpr (RS == 4) {
     hllc<T>(pl, pr, mt0, mt1, j0, j1, fc);
+  } else if constexpr (RS == 1) {
+    lax_friedrichs<T>(pl, pr, mt0, mt1, j0, j1, fc);
   } else {
     ausm_plus<T>(pl, pr, mt0, mt1, j0, j1, fc);
   }

@@ -243,15 +243,30 @@ bool derive(const Setup &s, Derived &d, std::string &err) {
     err = "only unsteady SSP-RK3 (steady = 0, temporal_scheme = 3) is on this library's path";
     return false;
   }
-  if (d.inviscid_type != 1) {
-    err = "for air this library implements the AWENO path (reconstruction = 4 or 5); got inviscid_type " +
-          std::to_string(d.inviscid_type);
+  if (d.inviscid_type == 3 || d.inviscid_type == 4) {
+    err = "inviscid_scheme " + std::to_string(is) +
+          " (characteristic FVS WENO / energy-preserving) is not on this library's path for air";
     return false;
   }
-  if (d.inviscid_scheme != 3 && d.inviscid_scheme != 4) {
-    err = "AWENO supports inviscid_scheme 3 (AUSM+) or 4 (HLLC) on this path";
+  if (d.inviscid_type == 0 || d.inviscid_type == 2) {
+    // primitive reconstruction (Reconstruction.cu:5-45): 1 first order, 2 MUSCL, 3 NND2
+    if (d.reconstruction < 1 || d.reconstruction > 3) {
+      err = "reconstruction must be 1 (1st order), 2 (MUSCL), 3 (NND2), 4 (AWENO5) or 5 (AWENO7); got " +
+            std::to_string(d.reconstruction);
+      return false;
+    }
+  }
+  d.limiter = s.get_int("limiter");
+  if (d.limiter != 0 && d.limiter != 1) {
+    // apply_limiter<0, 1> has no case for other values (Limiter.cuh:24-41) and returns an undefined value
+    err = "limiter must be 0 or 1 (minmod); got " + std::to_string(d.limiter);
     return false;
   }
+  d.entropy_fix_factor = s.get_real("entropy_fix_factor");
+  if (d.inviscid_type == 2) d.riemann = 2;
+  else if (is == 1) d.riemann = 1;
+  else if (is == 4) d.riemann = 4;
+  else d.riemann = 3;
   if (d.viscous_order != 0 && d.viscous_order != 2) {
     err = "viscous_order must be 0 or 2";
     return false;

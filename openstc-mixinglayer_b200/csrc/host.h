@@ -52,6 +52,12 @@ struct Derived {
   int n_spec = 0;
   int reconstruction = 2;
   int inviscid_scheme = 3;
+  // Riemann solver the face flux actually uses: 1 Lax-Friedrichs, 2 Roe, 3 AUSM+, 4 HLLC.  The
+  // reference's switches fall back to AUSM+ for any other inviscid_scheme (InviscidScheme.cu:145-159,
+  // 345-359), and AWENO with inviscid_scheme 2 lands there too (inviscid_type 1 takes precedence).
+  int riemann = 3;
+  int limiter = 0;                  // 0 and 1 are both minmod (Limiter.cuh:8-17)
+  double entropy_fix_factor = 0.125;
   int viscous_order = 2;
   double cfl = 1.0;
   double prandtl = 0.72;

@@ -368,6 +368,146 @@ constexpr size_t march_smem_bytes(int ng) {
          (std::is_same_v<T, float> ? 16 + (2 * 14 + 8) * 64 * sizeof(double) : 0);
 }
 
+// ------------------------------------------------------- primitive reconstruction + Riemann
+
+// Scheme constants of the primitive-reconstruction sweeps (inviscid_type 0 and 2).
+struct PvArgs {
+  int recon;       // 1 first order, 2 MUSCL, 3 NND2
+  double efix;     // entropy_fix_factor (Roe)
+  int is3d;
+};
+
+// Face flux between nodes n and n+1 of one sweep.  v(m, l): primitive l (rho,u,v,w,p) of node n+m,
+// m = -1..2; mt0/mt1, j0/j1: metric row and Jacobian of nodes n, n+1; d0/d1: their entropy-fix
+// thresholds (Roe only).
+template <int RS, typename T, class V>
+__device__ __forceinline__ void pv_face_flux(const V &v, int recon, const T *mt0, const T *mt1, T j0, T j1, T d0,
+                                             T d1, T *fc) {
+  T pl[6], pr[6];
+  pv_reconstruct<T>(v, recon, pl, pr);
+  if constexpr (RS == 2) roe<T>(pl, pr, mt0, mt1, j0, j1, d0, d1, fc);
+  else if constexpr (RS == 1) lax_friedrichs<T>(pl, pr, mt0, mt1, j0, j1, fc);
+  else if constexpr (RS == 4) hllc<T>(pl, pr, mt0, mt1, j0, j1, fc);
+  else ausm_plus<T>(pl, pr, mt0, mt1, j0, j1, fc);
+}
+
+template <typename T>
+__device__ __forceinline__ T node_efix(const DevBlock &b, const DevState &s, long long p, T factor, bool dim3) {
+  const long long P = b.plane;
+  T m[9], bb[5];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) m[r] = (T)__ldg(b.met + r * P + p);
+#pragma unroll
+  for (int l = 0; l < 5; ++l) bb[l] = (T)__ldg(s.bv + l * P + p);
+  return entropy_fix_delta<T>(m, bb, factor, dim3);
+}
+
+// x sweep of the primitive-reconstruction schemes (compute_convective_term_pv_1D and
+// Roe_compute_inviscid_flux_1D, InviscidScheme.cu:52-161, 459-548).  Each warp owns 31 nodes of one
+// (j,k) row: lane l computes the face between nodes i0-1+l and i0+l from its 4-node stencil (read
+// through the read-only cache, neighbouring lanes share lines), and lanes 1..31 finalise node
+// i0-1+l with the left face taken from lane l-1 by a shuffle.  dq is written (first sweep).
+template <int RS, typename T>
+__global__ void __launch_bounds__(128) k_flux_pv_x(DevBlock b, DevState s, PvArgs a, double *__restrict__ dq) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int i0 = (blockIdx.x * 4 + warp) * 31;
+  const int j = blockIdx.y, k = blockIdx.z;
+  const int n = i0 - 1 + lane;  // left node of this lane's face
+  const long long P = b.plane;
+  T fc[5] = {T(0), T(0), T(0), T(0), T(0)};
+  if (n < b.mx) {
+    const long long p = b.id(n, j, k);
+    T st[4][5];
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+      for (int l = 0; l < 5; ++l) st[m][l] = (T)__ldg(s.bv + l * P + p + m - 1);
+    T mt0[3], mt1[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      mt0[c] = (T)__ldg(b.met + c * P + p);
+      mt1[c] = (T)__ldg(b.met + c * P + p + 1);
+    }
+    const T j0 = (T)__ldg(b.jac + p), j1 = (T)__ldg(b.jac + p + 1);
+    T d0 = T(0), d1 = T(0);
+    if constexpr (RS == 2) {
+      d0 = node_efix<T>(b, s, p, (T)a.efix, a.is3d);
+      d1 = node_efix<T>(b, s, p + 1, (T)a.efix, a.is3d);
+    }
+    auto v = [&](int m, int l) -> T { return st[m + 1][l]; };
+    pv_face_flux<RS, T>(v, a.recon, mt0, mt1, j0, j1, d0, d1, fc);
+  }
+  T left[5];
+#pragma unroll
+  for (int l = 0; l < 5; ++l) left[l] = __shfl_up_sync(0xffffffffu, fc[l], 1);
+  const int i = n;  // node finalised by this lane: between faces (lane-1) and (lane)
+  if (lane >= 1 && i < b.mx) {
+    const long long q = b.iq(i, j, k);
+#pragma unroll
+    for (int l = 0; l < 5; ++l) dq[l * b.n + q] = -(double)(fc[l] - left[l]);
+  }
+}
+
+// y / z sweep of the primitive-reconstruction schemes: each thread marches one column over a
+// segment [d0, d1) of the sweep direction, keeping the 4-node stencil, the two face nodes' metric
+// rows, Jacobians and entropy-fix thresholds in registers, so every node is read once per segment
+// and every face flux is computed once.  Consecutive threads are consecutive i (coalesced).
+template <int DIR, int RS, typename T>
+__global__ void __launch_bounds__(128) k_flux_pv_march(DevBlock b, DevState s, PvArgs a, double *__restrict__ dq,
+                                                        int seg) {
+  const int i = blockIdx.x * 128 + threadIdx.x;
+  const int o = blockIdx.y;  // k for the y sweep, j for the z sweep
+  const int nd = DIR == 1 ? b.my : b.mz;
+  const int d0 = blockIdx.z * seg;
+  const int d1 = min(d0 + seg, nd);
+  if (i >= b.mx || d0 >= nd) return;
+  const long long P = b.plane;
+  auto pid = [&](int d) -> long long { return DIR == 1 ? b.id(i, d, o) : b.id(i, o, d); };
+  T st[4][5];
+  auto load_node = [&](int slot, int d) {
+    const long long p = pid(d);
+#pragma unroll
+    for (int l = 0; l < 5; ++l) st[slot][l] = (T)__ldg(s.bv + l * P + p);
+  };
+  T mt0[3], mt1[3], j0, j1, e0 = T(0), e1 = T(0);
+  auto load_face_node = [&](T *mt, T &jj, T &ee, int d) {
+    const long long p = pid(d);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) mt[c] = (T)__ldg(b.met + (DIR * 3 + c) * P + p);
+    jj = (T)__ldg(b.jac + p);
+    if constexpr (RS == 2) ee = node_efix<T>(b, s, p, (T)a.efix, a.is3d);
+  };
+  // stencil of the face (d0-1, d0): nodes d0-2 .. d0+1
+#pragma unroll
+  for (int m = 0; m < 4; ++m) load_node(m, d0 - 2 + m);
+  load_face_node(mt0, j0, e0, d0 - 1);
+  load_face_node(mt1, j1, e1, d0);
+  auto v = [&](int m, int l) -> T { return st[m + 1][l]; };
+  T fl[5];
+  pv_face_flux<RS, T>(v, a.recon, mt0, mt1, j0, j1, e0, e1, fl);
+  for (int d = d0; d < d1; ++d) {
+    // shift the stencil to nodes d-1 .. d+2 and the face nodes to d, d+1
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+      for (int l = 0; l < 5; ++l) st[m][l] = st[m + 1][l];
+    load_node(3, d + 2);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) mt0[c] = mt1[c];
+    j0 = j1;
+    e0 = e1;
+    load_face_node(mt1, j1, e1, d + 1);
+    T fr[5];
+    pv_face_flux<RS, T>(v, a.recon, mt0, mt1, j0, j1, e0, e1, fr);
+    const long long q = DIR == 1 ? b.iq(i, d, o) : b.iq(i, o, d);
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+      dq[l * b.n + q] -= (double)(fr[l] - fl[l]);
+      fl[l] = fr[l];
+    }
+  }
+}
+
 // ------------------------------------------------------------------------------ viscous + update
 
 // compute_fv/gv/hv_2nd_order<Air, Laminar> (ViscousScheme.cuh:24-911): viscous flux through the face
@@ -911,20 +1051,68 @@ int grid_for(ostc_ctx *ctx, long long n, int tpb) {
   return (int)g;
 }
 
+// inviscid sweeps of one block with a primitive reconstruction (inviscid_type 0: MUSCL/NND/1st order
+// + LF/AUSM+/HLLC, InviscidScheme.cu:12-50; inviscid_type 2: Roe, :369-415)
+template <int RS, typename T>
+void launch_flux_pv_rs(ostc_ctx *ctx, BlockRes &B, DevState in) {
+  const DevBlock &b = B.db;
+  const bool is3d = b.mz > 1;
+  const PvArgs a{ctx->der.reconstruction, ctx->der.entropy_fix_factor, is3d ? 1 : 0};
+  {
+    dim3 grid((b.mx + 123) / 124, b.my, b.mz);
+    long tok = begin_t(ctx, "flux_x");
+    k_flux_pv_x<RS, T><<<grid, 128, 0, ctx->stream>>>(b, in, a, B.dq);
+    end_t(ctx, tok);
+  }
+  for (int dir = 1; dir <= (is3d ? 2 : 1); ++dir) {
+    const int n_dir = dir == 1 ? b.my : b.mz, n_o = dir == 1 ? b.mz : b.my;
+    const long long cols = (long long)((b.mx + 127) / 128) * n_o;
+    int nseg = (int)std::max<long long>(1, (ctx->sm_count * 16 + cols - 1) / cols);
+    int seg = std::max(8, (n_dir + nseg - 1) / nseg);
+    nseg = (n_dir + seg - 1) / seg;
+    dim3 grid((b.mx + 127) / 128, n_o, nseg);
+    long tok = begin_t(ctx, dir == 1 ? "flux_y" : "flux_z");
+    if (dir == 1) k_flux_pv_march<1, RS, T><<<grid, 128, 0, ctx->stream>>>(b, in, a, B.dq, seg);
+    else k_flux_pv_march<2, RS, T><<<grid, 128, 0, ctx->stream>>>(b, in, a, B.dq, seg);
+    end_t(ctx, tok);
+  }
+}
+
+template <typename T>
+void launch_flux_pv(ostc_ctx *ctx, BlockRes &B, DevState in) {
+  switch (ctx->der.riemann) {
+    case 1: launch_flux_pv_rs<1, T>(ctx, B, in); break;
+    case 2: launch_flux_pv_rs<2, T>(ctx, B, in); break;
+    case 4: launch_flux_pv_rs<4, T>(ctx, B, in); break;
+    default: launch_flux_pv_rs<3, T>(ctx, B, in); break;
+  }
+}
+
 // inviscid sweep of one block
 template <typename T>
 int launch_flux(ostc_ctx *ctx, BlockRes &B, DevState in) {
+  if (ctx->der.inviscid_type != 1) {
+    launch_flux_pv<T>(ctx, B, in);
+    return OSTC_OK;
+  }
   const DevBlock &b = B.db;
-  const int ng = ctx->der.ngg, rs = ctx->der.inviscid_scheme;
+  const int ng = ctx->der.ngg, rs = ctx->der.riemann;
   const bool is3d = b.mz > 1;
   // x
   {
     dim3 grid((b.mx + 126) / 127, b.my, b.mz);
     long tok = begin_t(ctx, "flux_x");
-    if (ng == 3 && rs == 3) k_flux_x<3, 3, T><<<grid, 128, 0, ctx->stream>>>(b, in, B.dq);
-    else if (ng == 3) k_flux_x<3, 4, T><<<grid, 128, 0, ctx->stream>>>(b, in, B.dq);
-    else if (rs == 3) k_flux_x<4, 3, T><<<grid, 128, 0, ctx->stream>>>(b, in, B.dq);
-    else k_flux_x<4, 4, T><<<grid, 128, 0, ctx->stream>>>(b, in, B.dq);
+#define OSTC_FX(N, R) k_flux_x<N, R, T><<<grid, 128, 0, ctx->stream>>>(b, in, B.dq)
+    if (ng == 3) {
+      if (rs == 4) OSTC_FX(3, 4);
+      else if (rs == 1) OSTC_FX(3, 1);
+      else OSTC_FX(3, 3);
+    } else {
+      if (rs == 4) OSTC_FX(4, 4);
+      else if (rs == 1) OSTC_FX(4, 1);
+      else OSTC_FX(4, 3);
+    }
+#undef OSTC_FX
     end_t(ctx, tok);
   }
   // y and z
@@ -940,17 +1128,22 @@ int launch_flux(ostc_ctx *ctx, BlockRes &B, DevState in) {
     const size_t smem = march_smem_bytes<T>(ng);
     long tok = begin_t(ctx, dir == 1 ? "flux_y" : "flux_z");
 #define OSTC_MARCH(D, N, R) k_flux_march<D, N, R, T><<<grid, block, smem, ctx->stream>>>(b, in, B.dq, seg)
+#define OSTC_MARCH_NR(D)                  \
+  if (ng == 3) {                           \
+    if (rs == 4) OSTC_MARCH(D, 3, 4);      \
+    else if (rs == 1) OSTC_MARCH(D, 3, 1); \
+    else OSTC_MARCH(D, 3, 3);              \
+  } else {                                 \
+    if (rs == 4) OSTC_MARCH(D, 4, 4);      \
+    else if (rs == 1) OSTC_MARCH(D, 4, 1); \
+    else OSTC_MARCH(D, 4, 3);              \
+  }
     if (dir == 1) {
-      if (ng == 3 && rs == 3) OSTC_MARCH(1, 3, 3);
-      else if (ng == 3) OSTC_MARCH(1, 3, 4);
-      else if (rs == 3) OSTC_MARCH(1, 4, 3);
-      else OSTC_MARCH(1, 4, 4);
+      OSTC_MARCH_NR(1)
     } else {
-      if (ng == 3 && rs == 3) OSTC_MARCH(2, 3, 3);
-      else if (ng == 3) OSTC_MARCH(2, 3, 4);
-      else if (rs == 3) OSTC_MARCH(2, 4, 3);
-      else OSTC_MARCH(2, 4, 4);
+      OSTC_MARCH_NR(2)
     }
+#undef OSTC_MARCH_NR
 #undef OSTC_MARCH
     end_t(ctx, tok);
   }
@@ -1003,12 +1196,16 @@ bool set_march_attrs() {
     const int bytes = (int)march_smem_bytes<T>(ng);
     ok = ok && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
   };
+  set((const void *)k_flux_march<1, 3, 1, T>, 3);
   set((const void *)k_flux_march<1, 3, 3, T>, 3);
   set((const void *)k_flux_march<1, 3, 4, T>, 3);
+  set((const void *)k_flux_march<1, 4, 1, T>, 4);
   set((const void *)k_flux_march<1, 4, 3, T>, 4);
   set((const void *)k_flux_march<1, 4, 4, T>, 4);
+  set((const void *)k_flux_march<2, 3, 1, T>, 3);
   set((const void *)k_flux_march<2, 3, 3, T>, 3);
   set((const void *)k_flux_march<2, 3, 4, T>, 3);
+  set((const void *)k_flux_march<2, 4, 1, T>, 4);
   set((const void *)k_flux_march<2, 4, 3, T>, 4);
   set((const void *)k_flux_march<2, 4, 4, T>, 4);
   ok = ok && cudaFuncSetAttribute((const void *)k_visc_update<T, true, 32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -77,6 +77,8 @@ class Case:
             f"int inviscid_scheme = {s['inviscid_scheme']}",
             f"int viscous_order = {s['viscous_order']}",
             f"real prandtl_number = {s['prandtl_number']!r}",
+            f"int limiter = {s.get('limiter', 0)}",
+            f"real entropy_fix_factor = {s.get('entropy_fix_factor', 0.125)!r}",
             "int species = 0",
             "int reaction = 0",
             "bool turbulence = 0",
@@ -143,7 +145,7 @@ def _box_faces(mx, my, mz, xlab, ylab_lo, ylab_hi, zlab):
 
 
 def mixing_layer_2d(mx=257, my=129, seed=0, steps=100, mc=0.4, re=1000.0, t0=300.0, delta0=1e-3,
-                    reconstruction=4, inviscid_scheme=3, cfl=0.5) -> Case:
+                    reconstruction=4, inviscid_scheme=3, cfl=0.5, entropy_fix_factor=0.125) -> Case:
     """2-D temporal mixing layer: 256 x 128 cells on 2*pi x pi (node-coincident periodic x, mx = 257),
     u = dU/2 tanh(2y/delta0), Mc = dU/(2c), Re = rho dU delta0 / mu(T) , T and p uniform, and
     v' = 1e-3 dU sum_{m=1..8} a_m cos(m x + phi_m) exp(-(y/delta0)^2), a_m = 1/8, phi_m ~ U[0,2pi)."""
@@ -173,12 +175,13 @@ def mixing_layer_2d(mx=257, my=129, seed=0, steps=100, mc=0.4, re=1000.0, t0=300
     structs = {"slipwall": {"type": ("string", "symmetry"), "label": ("int", 3)},
                "periodic": {"type": ("string", "periodic"), "label": ("int", 8)}}
     scheme = dict(reconstruction=reconstruction, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=cfl,
-                  prandtl_number=0.72)
+                  prandtl_number=0.72, limiter=0, entropy_fix_factor=entropy_fix_factor)
     return Case("mixing_layer_2d", mx, my, 1, x, y, z, delta0, faces, structs, scheme, bv, steps)
 
 
 def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0, t0=300.0, delta0=1e-3,
-                    h=0.125, reconstruction=5, inviscid_scheme=4, cfl=0.5, ybc="farfield") -> Case:
+                    h=0.125, reconstruction=5, inviscid_scheme=4, cfl=0.5, ybc="farfield",
+                    entropy_fix_factor=0.125) -> Case:
     """3-D temporal mixing layer: uniform spacing h*delta0, periodic x and z (node-coincident),
     far-field (Riemann-invariant, label 4/41) or outflow (label 6) y faces; u = dU/2 tanh(2y/delta0),
     Mc = 0.7, plus 1e-2 dU N(0,1) exp(-(y/delta0)^2) seeded white noise in u, v, w."""
@@ -213,7 +216,7 @@ def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0
         structs = {"periodic": {"type": ("string", "periodic"), "label": ("int", 8)},
                    "outflow": {"type": ("string", "outflow"), "label": ("int", 6)}}
     scheme = dict(reconstruction=reconstruction, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=cfl,
-                  prandtl_number=0.72)
+                  prandtl_number=0.72, limiter=0, entropy_fix_factor=entropy_fix_factor)
     return Case("mixing_layer_3d", mx, my, mz, X, Y, Z, delta0, faces, structs, scheme, bv, steps)
 
 

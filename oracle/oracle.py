@@ -24,9 +24,19 @@ class OrcFace(ctypes.Structure):
 
 class OrcCase(ctypes.Structure):
     _fields_ = [("mx", ctypes.c_int), ("my", ctypes.c_int), ("mz", ctypes.c_int), ("reconstruction", ctypes.c_int),
-                ("inviscid_scheme", ctypes.c_int), ("viscous_order", ctypes.c_int), ("cfl", ctypes.c_double),
+                ("inviscid_scheme", ctypes.c_int), ("riemann", ctypes.c_int), ("entropy_fix_factor", ctypes.c_double),
+                ("viscous_order", ctypes.c_int), ("cfl", ctypes.c_double),
                 ("prandtl", ctypes.c_double), ("fixed_time_step", ctypes.c_int), ("dt", ctypes.c_double),
                 ("n_face", ctypes.c_int), ("face", OrcFace * 16)]
+
+
+def riemann_of(reconstruction: int, inviscid_scheme: int) -> int:
+    """Riemann solver the reference's switches select: 1 LF, 2 Roe, 3 AUSM+, 4 HLLC.  Roe only with a
+    primitive reconstruction (inviscid_type 2, Parameter.cpp:264-278); every unlisted scheme falls to
+    AUSM+ (InviscidScheme.cu:145-159, 345-359)."""
+    if inviscid_scheme == 2 and reconstruction in (1, 2, 3):
+        return 2
+    return inviscid_scheme if inviscid_scheme in (1, 4) else 3
 
 
 def build() -> Path:
@@ -75,6 +85,8 @@ class Oracle:
         c.mx, c.my, c.mz = case.mx, case.my, case.mz
         s = case.scheme
         c.reconstruction, c.inviscid_scheme, c.viscous_order = s["reconstruction"], s["inviscid_scheme"], s["viscous_order"]
+        c.riemann = riemann_of(s["reconstruction"], s["inviscid_scheme"])
+        c.entropy_fix_factor = s.get("entropy_fix_factor", 0.125)
         c.cfl, c.prandtl = s["cfl"], s["prandtl_number"]
         c.fixed_time_step, c.dt = 0, 1e-8
         types = case.label_types()

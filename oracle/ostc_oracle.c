@@ -565,6 +565,195 @@ static void hllc(const double pl[6], const double pr[6], const double mt[2][3], 
   }
 }
 
+/* riemannSolver_laxFriedrich<Air> (RiemannSolver.cuh:420-460). */
+static void lax_friedrichs(const double pl[6], const double pr[6], const double mt[2][3], const double jc[2],
+                           double fc[5]) {
+  const double kx = 0.5 * (mt[0][0] + mt[1][0]);
+  const double ky = 0.5 * (mt[0][1] + mt[1][1]);
+  const double kz = 0.5 * (mt[0][2] + mt[1][2]);
+  const double gradK = sqrt(kx * kx + ky * ky + kz * kz);
+  const double Ukl = pl[1] * kx + pl[2] * ky + pl[3] * kz;
+  const double Ukr = pr[1] * kx + pr[2] * ky + pr[3] * kz;
+  const double cl = sqrt(GAMMA_AIR * pl[4] / pl[0]);
+  const double cr = sqrt(GAMMA_AIR * pr[4] / pr[0]);
+  const double sr = fmax(fabs(Ukl) + cl * gradK, fabs(Ukr) + cr * gradK);
+  const double hj = 0.5 * 0.5 * (jc[0] + jc[1]);
+  const double rUl = pl[0] * Ukl, rUr = pr[0] * Ukr;
+  fc[0] = (rUl + rUr - sr * (pr[0] - pl[0])) * hj;
+  fc[1] = (rUl * pl[1] + rUr * pr[1] + kx * (pl[4] + pr[4]) - sr * (pr[1] * pr[0] - pl[1] * pl[0])) * hj;
+  fc[2] = (rUl * pl[2] + rUr * pr[2] + ky * (pl[4] + pr[4]) - sr * (pr[2] * pr[0] - pl[2] * pl[0])) * hj;
+  fc[3] = (rUl * pl[3] + rUr * pr[3] + kz * (pl[4] + pr[4]) - sr * (pr[3] * pr[0] - pl[3] * pl[0])) * hj;
+  fc[4] = ((pl[5] + pl[4]) * Ukl + (pr[5] + pr[4]) * Ukr - sr * (pr[5] - pl[5])) * hj;
+}
+
+/* compute_entropy_fix_delta<Air> (InviscidScheme.cu:417-456) at padded index p. */
+static double entropy_fix_delta(const orc_ctx *o, long p) {
+  const long P = o->P;
+  const double u = o->bv[P + p], v = o->bv[2 * P + p], w = o->bv[3 * P + p];
+  const double U = fabs(u * M(o, 1, 1, p) + v * M(o, 1, 2, p) + w * M(o, 1, 3, p));
+  const double V = fabs(u * M(o, 2, 1, p) + v * M(o, 2, 2, p) + w * M(o, 2, 3, p));
+  const double W = fabs(u * M(o, 3, 1, p) + v * M(o, 3, 2, p) + w * M(o, 3, 3, p));
+  const double kx = sqrt(M(o, 1, 1, p) * M(o, 1, 1, p) + M(o, 1, 2, p) * M(o, 1, 2, p) + M(o, 1, 3, p) * M(o, 1, 3, p));
+  const double ky = sqrt(M(o, 2, 1, p) * M(o, 2, 1, p) + M(o, 2, 2, p) * M(o, 2, 2, p) + M(o, 2, 3, p) * M(o, 2, 3, p));
+  const double kz = sqrt(M(o, 3, 1, p) * M(o, 3, 1, p) + M(o, 3, 2, p) * M(o, 3, 2, p) + M(o, 3, 3, p) * M(o, 3, 3, p));
+  const double c = sqrt(GAMMA_AIR * o->bv[4 * P + p] / o->bv[p]);
+  if (o->dim == 2) return o->c.entropy_fix_factor * (U + V + c * 0.5 * (kx + ky));
+  return o->c.entropy_fix_factor * (U + V + W + c * (kx + ky + kz) / 3.0);
+}
+
+/* riemannSolver_Roe<Air> (RiemannSolver.cuh:279-417) with compute_half_sum_left_right_flux
+ * (:232-277): central part from each side's own metric and Jacobian, Roe dissipation with Harten's
+ * entropy fix.  dl/dr: entropy-fix thresholds of the two face nodes. */
+static void roe(const double pl[6], const double pr[6], const double mt[2][3], const double jc[2], double d0,
+                double d1, double fc[5]) {
+  double jx = jc[0] * mt[0][0], jy = jc[0] * mt[0][1], jz = jc[0] * mt[0][2];
+  double Uk = pl[1] * jx + pl[2] * jy + pl[3] * jz;
+  double co = Uk * pl[0];
+  fc[0] = 0.5 * co;
+  fc[1] = 0.5 * (co * pl[1] + pl[4] * jx);
+  fc[2] = 0.5 * (co * pl[2] + pl[4] * jy);
+  fc[3] = 0.5 * (co * pl[3] + pl[4] * jz);
+  fc[4] = 0.5 * Uk * (pl[4] + pl[5]);
+  jx = jc[1] * mt[1][0], jy = jc[1] * mt[1][1], jz = jc[1] * mt[1][2];
+  Uk = pr[1] * jx + pr[2] * jy + pr[3] * jz;
+  co = Uk * pr[0];
+  fc[0] += 0.5 * co;
+  fc[1] += 0.5 * (co * pr[1] + pr[4] * jx);
+  fc[2] += 0.5 * (co * pr[2] + pr[4] * jy);
+  fc[3] += 0.5 * (co * pr[3] + pr[4] * jz);
+  fc[4] += 0.5 * Uk * (pr[4] + pr[5]);
+
+  const double dl = sqrt(pl[0]), dr = sqrt(pr[0]);
+  const double inv = 1.0 / (dl + dr);
+  const double u = (dl * pl[1] + dr * pr[1]) * inv;
+  const double v = (dl * pl[2] + dr * pr[2]) * inv;
+  const double w = (dl * pl[3] + dr * pr[3]) * inv;
+  const double ek = 0.5 * (u * u + v * v + w * w);
+  const double hl = (pl[5] + pl[4]) / pl[0];
+  const double hr = (pr[5] + pr[4]) / pr[0];
+  const double h = (dl * hl + dr * hr) * inv;
+  const double gamma = GAMMA_AIR;
+  const double c = sqrt((gamma - 1) * (h - ek));
+  double kx = 0.5 * (mt[0][0] + mt[1][0]);
+  double ky = 0.5 * (mt[0][1] + mt[1][1]);
+  double kz = 0.5 * (mt[0][2] + mt[1][2]);
+  const double gradK = sqrt(kx * kx + ky * ky + kz * kz);
+  Uk = kx * u + ky * v + kz * w;
+  double ch[3] = {Uk - gradK * c, Uk, Uk + gradK * c};
+  const double da = 0.5 * (d0 + d1);
+  for (int n = 0; n < 3; ++n) {
+    ch[n] = fabs(ch[n]);
+    if (ch[n] < da) ch[n] = 0.5 * (ch[n] * ch[n] / da + da);
+  }
+  kx /= gradK;
+  ky /= gradK;
+  kz /= gradK;
+  Uk /= gradK;
+  const double ja = 0.5 * (jc[0] + jc[1]);
+  double dq[5];
+  dq[0] = ja * (pr[0] - pl[0]);
+  for (int l = 1; l < 5; ++l) dq[l] = ja * (pr[0] * pr[l] - pl[0] * pl[l]);
+  dq[4] = ja * (pr[5] - pl[5]);
+  double c1 = (gamma - 1) * (ek * dq[0] - u * dq[1] - v * dq[2] - w * dq[3] + dq[4]) / (c * c);
+  double c2 = (kx * dq[1] + ky * dq[2] + kz * dq[3] - Uk * dq[0]) / c;
+  double c3 = dq[0] - c1;
+  double L[5];
+  L[0] = 0.5 * (c1 - c2);
+  L[1] = kx * c3 - ((kz * v - ky * w) * dq[0] - kz * dq[2] + ky * dq[3]) / c;
+  L[2] = ky * c3 - ((kx * w - kz * u) * dq[0] - kx * dq[3] + kz * dq[1]) / c;
+  L[3] = kz * c3 - ((ky * u - kx * v) * dq[0] - ky * dq[1] + kx * dq[2]) / c;
+  L[4] = 0.5 * (c1 + c2);
+  double b[5];
+  b[0] = -ch[0] * L[0];
+  for (int l = 1; l < 5; ++l) b[l] = -ch[1] * L[l];
+  b[4] = -ch[2] * L[4];
+  const double c0 = kx * b[1] + ky * b[2] + kz * b[3];
+  c1 = c0 + b[0] + b[4];
+  c2 = c * (b[4] - b[0]);
+  c3 = 0;
+  fc[0] += 0.5 * c1;
+  fc[1] += 0.5 * (u * c1 + kx * c2 - c * (kz * b[2] - ky * b[3]));
+  fc[2] += 0.5 * (v * c1 + ky * c2 - c * (kx * b[3] - kz * b[1]));
+  fc[3] += 0.5 * (w * c1 + kz * c2 - c * (ky * b[1] - kx * b[2]));
+  fc[4] += 0.5 * (h * c1 + Uk * c2 - c * c * c0 / (gamma - 1) +
+                  c * ((kz * v - ky * w) * b[1] + (kx * w - kz * u) * b[2] + (ky * u - kx * v) * b[3]) + c3);
+}
+
+/* minmod limiter, sgn(0) = +1 (Limiter.cuh:13-16, gxl_lib/Math.hpp:13-15). */
+static double minmod(double a, double b) {
+  const int sa = a < 0 ? -1 : 1, sb = b < 0 ? -1 : 1;
+  return 0.5 * (sa + sb) * fmin(fabs(a), fabs(b));
+}
+
+/* reconstruction<Air> (InviscidScheme.cu:163-215) with first_order_reconstruct, MUSCL_reconstruct and
+ * NND2_reconstruct (Reconstruction.cu:5-45).  st[m][l]: primitive l of nodes i-1, i, i+1, i+2. */
+static void pv_reconstruct(const double st[4][5], int recon, double pl[6], double pr[6]) {
+  const double kappa = 1.0 / 3.0;
+  for (int l = 0; l < 5; ++l) {
+    const double di = st[1][l] - st[0][l], di1 = st[2][l] - st[1][l], di2 = st[3][l] - st[2][l];
+    if (recon == 2) {
+      const double dnl = minmod(di, di1), dpl = minmod(di1, di);
+      const double dnr = minmod(di1, di2), dpr = minmod(di2, di1);
+      pl[l] = st[1][l] + 0.25 * ((1 - kappa) * dnl + (1 + kappa) * dpl);
+      pr[l] = st[2][l] - 0.25 * ((1 - kappa) * dpr + (1 + kappa) * dnr);
+    } else if (recon == 3) {
+      pl[l] = st[1][l] + 0.5 * minmod(di, di1);
+      pr[l] = st[2][l] - 0.5 * minmod(di1, di2);
+    } else {
+      pl[l] = st[1][l];
+      pr[l] = st[2][l];
+    }
+  }
+  const double el = 0.5 * (pl[1] * pl[1] + pl[2] * pl[2] + pl[3] * pl[3]);
+  const double er = 0.5 * (pr[1] * pr[1] + pr[2] * pr[2] + pr[3] * pr[3]);
+  pl[5] = el * pl[0] + pl[4] / (GAMMA_AIR - 1);
+  pr[5] = er * pr[0] + pr[4] / (GAMMA_AIR - 1);
+}
+
+/* compute_convective_term_pv_1D (InviscidScheme.cu:52-161) and Roe_compute_inviscid_flux_1D
+ * (:459-548) for one direction: faces at idx+1/2, idx = -1 .. n-1, then dq -= fc(i+1/2) - fc(i-1/2). */
+static void pv_direction(orc_ctx *o, int dir) {
+  const int ext[3] = {o->mx, o->my, o->mz};
+  const long P = o->P, N = (long)o->mx * o->my * o->mz;
+  int e[3] = {0, 0, 0};
+  e[dir] = 1;
+  const int n = ext[dir];
+  int hi[3] = {o->mx, o->my, o->mz};
+  hi[dir] = 1;
+  double *fc = (double *)malloc(sizeof(double) * 5 * (n + 1));
+  for (int a = 0; a < hi[0]; ++a)
+    for (int b = 0; b < hi[1]; ++b)
+      for (int cc = 0; cc < hi[2]; ++cc) {
+        for (int idx = -1; idx < n; ++idx) {
+          double st[4][5], mt[2][3], jc[2], ed[2] = {0, 0};
+          for (int m = 0; m < 4; ++m) {
+            const long p = ID(o, a + (idx - 1 + m) * e[0], b + (idx - 1 + m) * e[1], cc + (idx - 1 + m) * e[2]);
+            for (int l = 0; l < 5; ++l) st[m][l] = o->bv[l * P + p];
+          }
+          for (int s = 0; s < 2; ++s) {
+            const long p = ID(o, a + (idx + s) * e[0], b + (idx + s) * e[1], cc + (idx + s) * e[2]);
+            for (int q = 0; q < 3; ++q) mt[s][q] = o->met[(long)(dir * 3 + q) * P + p];
+            jc[s] = o->jac[p];
+            if (o->c.riemann == 2) ed[s] = entropy_fix_delta(o, p);
+          }
+          double pl[6], pr[6];
+          pv_reconstruct(st, o->c.reconstruction, pl, pr);
+          double *f = &fc[5 * (idx + 1)];
+          switch (o->c.riemann) {
+            case 1: lax_friedrichs(pl, pr, mt, jc, f); break;
+            case 2: roe(pl, pr, mt, jc, ed[0], ed[1], f); break;
+            case 4: hllc(pl, pr, mt, jc, f); break;
+            default: ausm_plus(pl, pr, mt, jc, f); break;
+          }
+        }
+        for (int idx = 0; idx < n; ++idx) {
+          const long q = IQ(o, a + idx * e[0], b + idx * e[1], cc + idx * e[2]);
+          for (int l = 0; l < 5; ++l) o->dq[l * N + q] -= fc[5 * (idx + 1) + l] - fc[5 * idx + l];
+        }
+      }
+  free(fc);
+}
+
 /* Physical flux of one node for the central-difference correction (AWENO.cu:307-321). */
 static void node_flux(const orc_ctx *o, long p, int dir, double f[5]) {
   const long P = o->P;
@@ -616,7 +805,8 @@ static void aweno_direction(orc_ctx *o, int dir) {
           double pl[6], pr[6];
           aweno_interp(st, ngg, o->c.reconstruction, mt, pl, pr);
           double *f = &fc[5 * (idx + 1)];
-          if (o->c.inviscid_scheme == 4) hllc(pl, pr, mt, jc, f);
+          if (o->c.riemann == 4) hllc(pl, pr, mt, jc, f);
+          else if (o->c.riemann == 1) lax_friedrichs(pl, pr, mt, jc, f);
           else ausm_plus(pl, pr, mt, jc, f);
         }
         for (int idx = 0; idx < n; ++idx) {
@@ -984,7 +1174,7 @@ orc_ctx *orc_create(const orc_case *c, const double *x, const double *y, const d
   o->my = c->my;
   o->mz = c->mz;
   o->dim = c->mz == 1 ? 2 : 3;
-  o->g = c->reconstruction == 5 ? 4 : 3; /* Parameter.cpp:194-209 */
+  o->g = c->reconstruction == 5 ? 4 : c->reconstruction == 4 ? 3 : 2; /* Parameter.cpp:194-209 */
   o->sx = o->mx + 2 * o->g;
   o->sy = o->my + 2 * o->g;
   o->sz = o->mz + 2 * o->g;
@@ -1075,7 +1265,10 @@ void orc_rhs(orc_ctx *o, unsigned mask, double *dq) {
   const long N = (long)o->mx * o->my * o->mz;
   memset(o->dq, 0, sizeof(double) * 5 * N);
   if (mask & 1u)
-    for (int d = 0; d < o->dim; ++d) aweno_direction(o, d);
+    for (int d = 0; d < o->dim; ++d) {
+      if (o->c.reconstruction == 4 || o->c.reconstruction == 5) aweno_direction(o, d);
+      else pv_direction(o, d);
+    }
   if ((mask & 2u) && o->c.viscous_order != 0) viscous(o);
   if (dq) memcpy(dq, o->dq, sizeof(double) * 5 * N);
 }

@@ -27,8 +27,12 @@ typedef struct {
 
 typedef struct {
   int mx, my, mz;            /* grid nodes of the block */
-  int reconstruction;        /* 4 = AWENO5, 5 = AWENO7 (Parameter.cpp:203-209) */
-  int inviscid_scheme;       /* 3 = AUSM+, 4 = HLLC (InviscidScheme.cu:333-345) */
+  int reconstruction;        /* 1 = 1st order, 2 = MUSCL, 3 = NND2, 4 = AWENO5, 5 = AWENO7 (Parameter.cpp:195-209) */
+  int inviscid_scheme;       /* as in setup.txt (informational; the solver is `riemann`) */
+  int riemann;               /* 1 = Lax-Friedrichs, 2 = Roe, 3 = AUSM+, 4 = HLLC: the solver the
+                                reference's switches select (InviscidScheme.cu:145-159, 345-359,
+                                SchemeSelector.cuh:24-45) */
+  double entropy_fix_factor; /* Roe entropy fix (Parameter.cpp:474) */
   int viscous_order;         /* 0 = inviscid, 2 = 2nd-order central (SchemeSelector.cuh:47-67) */
   double cfl, prandtl;
   int fixed_time_step;
@@ -49,7 +53,8 @@ void orc_set_state(orc_ctx *o, const double *bv);
 void orc_get_state(const orc_ctx *o, double *cv, double *bv, double *mul);
 /* Metric (9 entries, row-major 1-based (r,c) -> (r-1)*3+c-1) and Jacobian on the interior nodes. */
 void orc_get_metric(const orc_ctx *o, double *metric9, double *jac);
-/* Right-hand side dq[5][N] of the current state.  mask: 1 = inviscid (AWENO + Riemann + CDS),
+/* Right-hand side dq[5][N] of the current state.  mask: 1 = inviscid (AWENO + Riemann + CDS, or a
+ * primitive reconstruction + Riemann),
  * 2 = viscous; the reference evaluates them in that order (RK.cuh:138-139). */
 void orc_rhs(orc_ctx *o, unsigned mask, double *dq);
 /* n full SSP-RK3 steps (RK.cuh:85-185).  Returns the last dt. */

@@ -7,7 +7,9 @@
 // (main.cu:8-136), replaces the freshly initialised interior primitive variables with the ones in
 // state_in.bin ([block][6][mz][my][mx] doubles), runs the reference's
 // Driver::initialize_computation() and RK3() (RK.cuh:19-228) for total_step steps, and writes the
-// interior cv[5] and bv[6] of every block, then the physical time, to state_out.bin.
+// interior cv[5] and bv[6] of every block, then the physical time, to state_out.bin.  It prints the
+// wall time of the RK3 call (steps, per-step output checks and the final flow-field file included).
+#include <chrono>
 #include <cstdio>
 #include <exception>
 #include <vector>
@@ -71,8 +73,12 @@ int run(const char *fin, const char *fout, int *argc, char ***argv) {
   g_stage = "initialize_computation";
   driver.initialize_computation();
   g_stage = "RK3";
+  cudaDeviceSynchronize();
+  const auto t_begin = std::chrono::steady_clock::now();
   cfd::RK3<MixtureModel::Air, cfd::Laminar>(driver);
   cudaDeviceSynchronize();
+  const double rk3_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_begin).count();
+  std::printf("ref_harness: rk3_seconds = %.6f\n", rk3_seconds);
 
   g_stage = "state_out";
   f = std::fopen(fout, "wb");

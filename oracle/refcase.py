@@ -84,8 +84,10 @@ def write_reference_case(case, steps: int, directory: os.PathLike) -> Path:
     return d
 
 
-def run_reference(case, steps: int, workdir: os.PathLike | None = None, timeout: int = 1800):
-    """Returns (cv[5,mz,my,mx], bv[6,mz,my,mx], physical time) after `steps` reference RK3 steps."""
+def run_reference(case, steps: int, workdir: os.PathLike | None = None, timeout: int = 1800,
+                  with_seconds: bool = False):
+    """Returns (cv[5,mz,my,mx], bv[6,mz,my,mx], physical time) after `steps` reference RK3 steps, and
+    with_seconds the wall time of the reference's RK3 call."""
     if not HARNESS.exists():
         raise FileNotFoundError(f"{HARNESS} not built (oracle/ref/build_ref.sh)")
     d = Path(workdir) if workdir else Path(tempfile.mkdtemp(prefix="ostc_ref_"))
@@ -97,4 +99,8 @@ def run_reference(case, steps: int, workdir: os.PathLike | None = None, timeout:
     raw = np.fromfile(d / "state_out.bin", dtype=np.float64)
     n = case.nodes
     out = raw[: 11 * n].reshape((11,) + case.bv.shape[1:])
-    return out[:5].copy(), out[5:].copy(), float(raw[11 * n])
+    res = (out[:5].copy(), out[5:].copy(), float(raw[11 * n]))
+    if with_seconds:
+        sec = [float(l.split("=")[1]) for l in r.stdout.splitlines() if "rk3_seconds" in l]
+        return res + (sec[0] if sec else float("nan"),)
+    return res

@@ -32,6 +32,16 @@ CASES = [
      dict(mx=32, my=20, mz=16, reconstruction=5, inviscid_scheme=4), 20),
     ("ml3d_weno5_ausm_outflow", "mixing_layer_3d",
      dict(mx=32, my=20, mz=16, reconstruction=4, inviscid_scheme=3, ybc="outflow"), 20),
+    # primitive reconstructions (inviscid_type 0 and 2) and AWENO with Lax-Friedrichs
+    ("ml2d_muscl_roe", "mixing_layer_2d", dict(mx=65, my=33, reconstruction=2, inviscid_scheme=2), 100),
+    ("ml2d_nnd_hllc", "mixing_layer_2d", dict(mx=65, my=33, reconstruction=3, inviscid_scheme=4), 100),
+    ("ml2d_weno5_lf", "mixing_layer_2d", dict(mx=65, my=33, reconstruction=4, inviscid_scheme=1), 50),
+    ("ml3d_first_ausm_outflow", "mixing_layer_3d",
+     dict(mx=32, my=20, mz=16, reconstruction=1, inviscid_scheme=3, ybc="outflow"), 20),
+    ("ml3d_muscl_lf_farfield", "mixing_layer_3d",
+     dict(mx=32, my=20, mz=16, reconstruction=2, inviscid_scheme=1), 20),
+    ("ml3d_nnd_roe_farfield", "mixing_layer_3d",
+     dict(mx=32, my=20, mz=16, reconstruction=3, inviscid_scheme=2), 20),
 ]
 
 
