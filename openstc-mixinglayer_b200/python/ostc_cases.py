@@ -50,6 +50,13 @@ class Case:
     scheme: dict      # reconstruction, inviscid_scheme, viscous_order, cfl, prandtl_number
     bv: np.ndarray    # [6, mz, my, mx] initial primitive state
     steps: int = 100
+    # multi-component mixtures: sv [n_spec, mz, my, mx] mass fractions; mixture = dict(tables (an
+    # object with names, mw, ... as oracle/chem.py builds), finite_rate, chem_dir (directory holding
+    # the CHEMKIN files), mechanism, therm, tran); freestream = reference state (mach, pressure,
+    # temperature, Y {name: value}) written as the inflow struct "freestream"
+    sv: np.ndarray | None = None
+    mixture: dict | None = None
+    freestream: dict | None = None
 
     @property
     def nodes(self) -> int:
@@ -79,14 +86,26 @@ class Case:
             f"real prandtl_number = {s['prandtl_number']!r}",
             f"int limiter = {s.get('limiter', 0)}",
             f"real entropy_fix_factor = {s.get('entropy_fix_factor', 0.125)!r}",
-            "int species = 0",
-            "int reaction = 0",
+            f"int species = {1 if self.mixture else 0}",
+            f"int reaction = {1 if self.mixture and self.mixture['finite_rate'] else 0}",
             "bool turbulence = 0",
             "bool limit_flow = 0",
             "array string boundary_conditions {",
             "    " + " ".join(self.bc_structs.keys()),
             "}",
         ]
+        if self.mixture:
+            m = self.mixture
+            lines += [f"string mechanism_file = chemistry/{m['mechanism']}", f"string therm_file = chemistry/{m['therm']}",
+                      f"string transport_file = chemistry/{m['tran']}"]
+        if self.freestream:
+            f = self.freestream
+            lines += ["string reference_state = freestream", "struct freestream = {", "    string type = inflow",
+                      "    int label = 5", f"    real mach = {f['mach']!r}", f"    real pressure = {f['pressure']!r}",
+                      f"    real temperature = {f['temperature']!r}", "    real u = 1.0", "    real v = 0.0",
+                      "    real w = 0.0"]
+            lines += [f"    real {k} = {v!r}" for k, v in f.get("Y", {}).items()]
+            lines.append("}")
         for name, st in self.bc_structs.items():
             lines.append(f"struct {name} = {{")
             for k, (t, v) in st.items():
@@ -110,6 +129,36 @@ class Case:
                                    acoustic_speed=c, gamma=GAMMA, entropy=p / rho ** GAMMA, mw=MW_AIR)
         return out
 
+    def reference_scales(self):
+        """(rho_inf^2 v_inf^2, v_inf) of the reference state as the reference's Inflow ctor computes
+        them (BoundCond.cpp:157-214, 299-305); (0, 0) without one."""
+        f = self.freestream
+        if not f:
+            return 0.0, 0.0
+        t, p, mach = f["temperature"], f["pressure"], f["mach"]
+        if self.mixture:
+            tb = self.mixture["tables"]
+            y = np.zeros(tb.n_spec)
+            for k, v in f.get("Y", {}).items():
+                y[tb.names.index(k)] = v
+            mw = 0.0
+            for i in range(tb.n_spec):
+                mw += y[i] / tb.mw[i]
+            mw = 1 / mw
+            cpi = species_cp(tb, t)
+            cp = cv = 0.0
+            for i in range(tb.n_spec):
+                cp += y[i] * cpi[i]
+                cv += y[i] * (cpi[i] - R_U / tb.mw[i])
+            gamma = cp / cv
+        else:
+            mw, gamma = MW_AIR, GAMMA
+        c = math.sqrt(gamma * R_U / mw * t)
+        vel = mach * c
+        rho = p * mw / (R_U * t)
+        v_inf = c if abs(vel) < 1 else vel
+        return rho * vel * rho * vel if abs(vel) >= 1 else rho * c * rho * c, v_inf
+
     def label_types(self):
         types = {"symmetry": 3, "farfield": 4, "outflow": 6, "periodic": 8}
         m = {}
@@ -118,9 +167,36 @@ class Case:
         return m
 
 
+def species_cp(tb, t):
+    """Species::compute_cp (ChemData.cpp:148-171): cp_k(T) in J/(kg K), constant below t_low."""
+    out = np.empty(tb.n_spec)
+    for i in range(tb.n_spec):
+        tt = t
+        if t < tb.t_low[i]:
+            tt = tb.t_low[i]
+            a = tb.low[i]
+            tt2 = tt * tt
+            tt3 = tt2 * tt
+            tt4 = tt3 * tt
+            out[i] = a[0] + a[1] * tt + a[2] * tt2 + a[3] * tt3 + a[4] * tt4
+        else:
+            a = tb.low[i] if tt < tb.t_mid[i] else tb.high[i]
+            t2 = t * t
+            t3 = t2 * t
+            t4 = t3 * t
+            out[i] = a[0] + a[1] * tt + a[2] * t2 + a[3] * t3 + a[4] * t4
+        out[i] *= R_U / tb.mw[i]
+    return out
+
+
 def write_case(case: Case, directory: os.PathLike) -> Path:
     d = Path(directory)
     (d / "grid").mkdir(parents=True, exist_ok=True)
+    if case.mixture:
+        import shutil
+        (d / "chemistry").mkdir(parents=True, exist_ok=True)
+        for k in ("mechanism", "therm", "tran"):
+            shutil.copyfile(Path(case.mixture["chem_dir"]) / case.mixture[k], d / "chemistry" / case.mixture[k])
     (d / "boundary_condition").mkdir(parents=True, exist_ok=True)
     (d / "setup.txt").write_text(case.setup_text())
     with open(d / "grid" / "grid   0.dat", "wb") as f:
@@ -218,6 +294,72 @@ def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0
     scheme = dict(reconstruction=reconstruction, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=cfl,
                   prandtl_number=0.72, limiter=0, entropy_fix_factor=entropy_fix_factor)
     return Case("mixing_layer_3d", mx, my, mz, X, Y, Z, delta0, faces, structs, scheme, bv, steps)
+
+
+CHEM_FIXTURE = Path(__file__).resolve().parents[2] / "tests" / "golden" / "chem"
+
+
+def reacting_mixing_layer_3d(mx=384, my=192, mz=96, seed=0, steps=100, h=0.125, delta0=1e-3, mc=0.4,
+                             p0=101325.0, inviscid_scheme=72, finite_rate=True, ybc="outflow",
+                             chem_dir=None, fuel=None, oxidiser=None) -> Case:
+    """Reacting H2/air temporal mixing layer (9 species, 19 reactions after merging duplicates):
+    fuel Y_H2 = 0.05 in N2 at 300 K (y > 0) over vitiated air at 1500 K (y < 0): Y_O2 = 0.20, Y_H2O = 0.10,
+    radicals Y_OH = 1e-3, Y_O = 1e-4, Y_H = 1e-5, Y_HO2 = 1e-6, Y_H2O2 = 1e-7 (so that every reaction
+    runs from the first step), N2 the rest; T and Y blended by (1 + tanh(2y/delta0))/2, uniform p0, u = dU/2 tanh(2y/delta0)
+    with dU = 2 Mc (c_fuel + c_ox)/2 and 1e-2 dU N(0,1) exp(-(y/delta0)^2) seeded noise in u, v, w;
+    periodic x and z, outflow y; flux-split characteristic WENO7-Z (inviscid_scheme 72)."""
+    import sys
+    sys.path.insert(0, str(Path(__file__).resolve().parents[2] / "oracle"))
+    import chem as chemreader
+
+    chem_dir = Path(chem_dir) if chem_dir else CHEM_FIXTURE
+    tb = chemreader.read(chem_dir, "H2_mech.inp", "therm.dat", "tran.dat", reactions=finite_rate)
+    ns = tb.n_spec
+    fuel = fuel or {"H2": 0.05, "N2": 0.95}
+    oxidiser = oxidiser or {"O2": 0.20, "H2O": 0.10, "OH": 1e-3, "O": 1e-4, "H": 1e-5, "HO2": 1e-6, "H2O2": 1e-7,
+                            "N2": 0.70 - 1e-3 - 1e-4 - 1e-5 - 1e-6 - 1e-7}
+    yf, yo = np.zeros(ns), np.zeros(ns)
+    for k, v in fuel.items():
+        yf[tb.names.index(k)] = v
+    for k, v in oxidiser.items():
+        yo[tb.names.index(k)] = v
+    tf, to = 300.0, 1500.0
+    rng = np.random.default_rng(seed)
+    xs = np.arange(mx) * h
+    ys = (np.arange(my) - (my - 1) / 2) * h
+    zs = np.arange(mz) * h
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    mwf = 1 / np.sum(yf / tb.mw)
+    mwo = 1 / np.sum(yo / tb.mw)
+    cf = math.sqrt(GAMMA * R_U / mwf * tf)
+    co = math.sqrt(GAMMA * R_U / mwo * to)
+    du = mc * (cf + co)
+    f = 0.5 * (1 + np.tanh(2 * Y))
+    sv = np.empty((ns,) + X.shape)
+    for l in range(ns):
+        sv[l] = f * yf[l] + (1 - f) * yo[l]
+    T = f * tf + (1 - f) * to
+    mw = 1 / np.einsum("l...,l->...", sv, 1 / tb.mw)
+    env = np.exp(-Y ** 2)
+    bv = np.empty((6,) + X.shape)
+    bv[0] = p0 * mw / (R_U * T)
+    bv[1] = 0.5 * du * np.tanh(2 * Y) + 1e-2 * du * rng.standard_normal(X.shape) * env
+    bv[2] = 1e-2 * du * rng.standard_normal(X.shape) * env
+    bv[3] = 1e-2 * du * rng.standard_normal(X.shape) * env
+    bv[4] = p0
+    bv[5] = T
+    if ybc != "outflow":
+        raise ValueError("the reacting case uses outflow y faces")
+    faces = _box_faces(mx, my, mz, 8, 6, 6, 8)
+    structs = {"periodic": {"type": ("string", "periodic"), "label": ("int", 8)},
+               "outflow": {"type": ("string", "outflow"), "label": ("int", 6)}}
+    scheme = dict(reconstruction=2, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=0.5, prandtl_number=0.72,
+                  limiter=0, entropy_fix_factor=0.125)
+    mixture = dict(tables=tb, finite_rate=finite_rate, chem_dir=str(chem_dir), mechanism="H2_mech.inp",
+                   therm="therm.dat", tran="tran.dat")
+    freestream = dict(mach=0.5, pressure=p0, temperature=to, Y=dict(oxidiser))
+    return Case("reacting_mixing_layer_3d", mx, my, mz, X, Y, Z, delta0, faces, structs, scheme, bv, steps,
+                sv=sv, mixture=mixture, freestream=freestream)
 
 
 def relative_errors(a: np.ndarray, b: np.ndarray, momentum_group: bool = True):

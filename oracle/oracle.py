@@ -22,12 +22,44 @@ class OrcFace(ctypes.Structure):
                                        "gamma", "entropy", "mw")]
 
 
+MAXS, MAXR = 16, 64
+
+
+class OrcChem(ctypes.Structure):
+    D, I = ctypes.c_double, ctypes.c_int
+    _fields_ = [("n_spec", I), ("n_reac", I), ("mw", D * MAXS), ("t_low", D * MAXS), ("t_mid", D * MAXS),
+                ("low", D * (MAXS * 7)), ("high", D * (MAXS * 7)), ("lj_potent_inv", D * MAXS),
+                ("vis_coeff", D * MAXS), ("wj_div_wi_1_4", D * (MAXS * MAXS)), ("sqrt_wiwj_8", D * (MAXS * MAXS)),
+                ("binary_diff", D * (MAXS * MAXS)), ("kb_over_eps_jk", D * (MAXS * MAXS)), ("label", I * MAXR),
+                ("rev_type", I * MAXR), ("order", I * MAXR), ("stoi_f", I * (MAXR * MAXS)),
+                ("stoi_b", I * (MAXR * MAXS)), ("A", D * MAXR), ("b", D * MAXR), ("Ea", D * MAXR), ("A2", D * MAXR),
+                ("b2", D * MAXR), ("Ea2", D * MAXR), ("third_body", D * (MAXR * MAXS)), ("troe_alpha", D * MAXR),
+                ("troe_t3", D * MAXR), ("troe_t1", D * MAXR), ("troe_t2", D * MAXR)]
+
+
+def chem_struct(t) -> OrcChem:
+    """ctypes copy of oracle/chem.py tables (row-major, first n_spec / n_reac entries used)."""
+    c = OrcChem()
+    c.n_spec, c.n_reac = t.n_spec, t.n_reac
+    for name, _ in OrcChem._fields_[2:]:
+        v = getattr(t, name, None)
+        if v is None:
+            continue
+        flat = np.asarray(v).ravel()
+        arr = getattr(c, name)
+        for i, x in enumerate(flat):
+            arr[i] = x
+    return c
+
+
 class OrcCase(ctypes.Structure):
     _fields_ = [("mx", ctypes.c_int), ("my", ctypes.c_int), ("mz", ctypes.c_int), ("reconstruction", ctypes.c_int),
                 ("inviscid_scheme", ctypes.c_int), ("riemann", ctypes.c_int), ("entropy_fix_factor", ctypes.c_double),
                 ("viscous_order", ctypes.c_int), ("cfl", ctypes.c_double),
                 ("prandtl", ctypes.c_double), ("fixed_time_step", ctypes.c_int), ("dt", ctypes.c_double),
-                ("n_face", ctypes.c_int), ("face", OrcFace * 16)]
+                ("n_face", ctypes.c_int), ("face", OrcFace * 16), ("n_spec", ctypes.c_int),
+                ("finite_rate", ctypes.c_int), ("chem", ctypes.POINTER(OrcChem)), ("weno_eps_scale", ctypes.c_double),
+                ("v_ref", ctypes.c_double)]
 
 
 def riemann_of(reconstruction: int, inviscid_scheme: int) -> int:
@@ -59,6 +91,8 @@ def load():
         lib.orc_destroy.argtypes = [vp]
         lib.orc_ngg.argtypes = [vp]
         lib.orc_set_state.argtypes = [vp, dp]
+        lib.orc_set_state_sv.argtypes = [vp, dp, dp]
+        lib.orc_get_mixture.argtypes = [vp, dp, dp, dp, dp, dp]
         lib.orc_get_state.argtypes = [vp, dp, dp, dp]
         lib.orc_get_metric.argtypes = [vp, dp, dp]
         lib.orc_rhs.argtypes = [vp, ctypes.c_uint, dp]
@@ -99,6 +133,14 @@ class Oracle:
             if f.label in ff:
                 for k, v in ff[f.label].items():
                     setattr(c.face[n], k, v)
+        self.n_spec = 0
+        mix = getattr(case, "mixture", None)
+        if mix is not None:
+            self._chem = chem_struct(mix["tables"])
+            c.chem = ctypes.pointer(self._chem)
+            c.n_spec = self.n_spec = mix["tables"].n_spec
+            c.finite_rate = 1 if mix["finite_rate"] else 0
+        c.weno_eps_scale, c.v_ref = case.reference_scales()
         self.case = case
         self.shape = (case.mz, case.my, case.mx)
         x = np.ascontiguousarray(case.x * case.grid_scale, dtype=np.float64)
@@ -121,12 +163,26 @@ class Oracle:
         except Exception:
             pass
 
-    def set_state(self, bv: np.ndarray):
+    def set_state(self, bv: np.ndarray, sv: np.ndarray | None = None):
         bv = np.ascontiguousarray(bv, dtype=np.float64)
-        self.lib.orc_set_state(self.h, _dp(bv))
+        if sv is None and getattr(self.case, "sv", None) is not None and self.n_spec:
+            sv = self.case.sv
+        if self.n_spec:
+            sv = np.ascontiguousarray(sv, dtype=np.float64)
+            self.lib.orc_set_state_sv(self.h, _dp(bv), _dp(sv))
+        else:
+            self.lib.orc_set_state(self.h, _dp(bv))
+
+    def mixture(self):
+        """Interior Y_k, conductivity, rho D_k, acoustic speed, gamma."""
+        sv = np.empty((self.n_spec,) + self.shape)
+        rd = np.empty((self.n_spec,) + self.shape)
+        cond, ac, ga = np.empty(self.shape), np.empty(self.shape), np.empty(self.shape)
+        self.lib.orc_get_mixture(self.h, _dp(sv), _dp(cond), _dp(rd), _dp(ac), _dp(ga))
+        return dict(sv=sv, cond=cond, rho_d=rd, acoustic=ac, gamma=ga)
 
     def get_state(self):
-        cv = np.empty((5,) + self.shape)
+        cv = np.empty((5 + self.n_spec,) + self.shape)
         bv = np.empty((6,) + self.shape)
         mul = np.empty(self.shape)
         self.lib.orc_get_state(self.h, _dp(cv), _dp(bv), _dp(mul))
@@ -139,7 +195,7 @@ class Oracle:
         return m, j
 
     def rhs(self, mask: int = 3) -> np.ndarray:
-        dq = np.empty((5,) + self.shape)
+        dq = np.empty((5 + self.n_spec,) + self.shape)
         self.lib.orc_rhs(self.h, mask, _dp(dq))
         return dq
 

@@ -39,6 +39,10 @@ struct orc_ctx {
   double *x, *y, *z;
   double *jac, *met; /* met: 9 SoA planes of P */
   double *cv, *bv, *mul, *qn, *dq, *dtl;
+  /* mixtures: ns species, nv = 5 + ns conservative variables; per-node properties over the padded
+   * block (update_physical_properties, FieldOperation.cuh:107-140) */
+  int ns, nv;
+  double *sv, *cond, *rhod, *cpm, *gam, *acs;
   face_t f[16];
   int nf;
   double t;
@@ -255,6 +259,8 @@ static void register_face(orc_ctx *o, const orc_face_in *in, face_t *f) {
 /* ---------------------------------------------------------------- pointwise helpers */
 
 /* compute_cv_from_bv_1_point + compute_total_energy<Air> (FieldOperation.cuh:17-38,78-105). */
+static void mix_h_cp(const orc_chem *ch, double t, double *h, double *cp);
+
 static void cv_from_bv(orc_ctx *o, long p) {
   const long P = o->P;
   const double rho = o->bv[p];
@@ -265,8 +271,20 @@ static void cv_from_bv(orc_ctx *o, long p) {
   const double u = o->bv[P + p], v = o->bv[2 * P + p], w = o->bv[3 * P + p];
   const double V2 = u * u + v * v + w * w;
   double te = 0.5 * V2;
-  te *= rho;
-  te += o->bv[4 * P + p] / (GAMMA_AIR - 1);
+  if (o->ns) {
+    /* compute_total_energy<mixture> (FieldOperation.cuh:17-32): rho (sum h_k Y_k + V^2/2) - p */
+    double h[ORC_MAX_SPEC];
+    mix_h_cp(o->c.chem, o->bv[5 * P + p], h, NULL);
+    for (int l = 0; l < o->ns; ++l) {
+      o->cv[(5 + l) * P + p] = rho * o->sv[l * P + p];
+      te += h[l] * o->sv[l * P + p];
+    }
+    te *= rho;
+    te -= o->bv[4 * P + p];
+  } else {
+    te *= rho;
+    te += o->bv[4 * P + p] / (GAMMA_AIR - 1);
+  }
   o->cv[4 * P + p] = te;
 }
 
@@ -839,11 +857,560 @@ static void aweno_direction(orc_ctx *o, int dir) {
   free(fp);
 }
 
+/* ---------------------------------------------------------------- mixtures: thermodynamics */
+
+/* compute_enthalpy_and_cp / compute_enthalpy / compute_cp (Thermo.cu:136-192, two-range NASA-7 with
+ * linear extrapolation of h below t_low).  Either output may be NULL. */
+static void mix_h_cp(const orc_chem *ch, double t, double *h, double *cp) {
+  const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t5 = t4 * t;
+  for (int i = 0; i < ch->n_spec; ++i) {
+    double hh, cc;
+    if (t < ch->t_low[i]) {
+      const double tt = ch->t_low[i], tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tt5 = tt4 * tt;
+      const double *a = &ch->low[i * 7];
+      hh = a[0] * tt + 0.5 * a[1] * tt2 + a[2] * tt3 / 3 + 0.25 * a[3] * tt4 + 0.2 * a[4] * tt5 + a[5];
+      cc = a[0] + a[1] * tt + a[2] * tt2 + a[3] * tt3 + a[4] * tt4;
+      hh += cc * (t - tt);
+    } else {
+      const double *a = t < ch->t_mid[i] ? &ch->low[i * 7] : &ch->high[i * 7];
+      hh = a[0] * t + 0.5 * a[1] * t2 + a[2] * t3 / 3 + 0.25 * a[3] * t4 + 0.2 * a[4] * t5 + a[5];
+      cc = a[0] + a[1] * t + a[2] * t2 + a[3] * t3 + a[4] * t4;
+    }
+    if (h) h[i] = hh * (R_U / ch->mw[i]);
+    if (cp) cp[i] = cc * (R_U / ch->mw[i]);
+  }
+}
+
+/* compute_gibbs_div_rt (Thermo.cu:194-210): g_k / (R_u T) */
+static void mix_gibbs_rt(const orc_chem *ch, double t, double *g) {
+  const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, ti = 1 / t, lt = log(t);
+  for (int i = 0; i < ch->n_spec; ++i) {
+    if (t < ch->t_low[i]) {
+      const double tt = ch->t_low[i], tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tti = 1 / tt, ltt = log(tt);
+      const double *a = &ch->low[i * 7];
+      g[i] = a[0] * (1.0 - ltt) - 0.5 * a[1] * tt - a[2] * tt2 / 6.0 - a[3] * tt3 / 12.0 - a[4] * tt4 * 0.05 +
+             a[5] * tti - a[6];
+    } else {
+      const double *a = t < ch->t_mid[i] ? &ch->low[i * 7] : &ch->high[i * 7];
+      g[i] = a[0] * (1.0 - lt) - 0.5 * a[1] * t - a[2] * t2 / 6.0 - a[3] * t3 / 12.0 - a[4] * t4 * 0.05 + a[5] * ti -
+             a[6];
+    }
+  }
+}
+
+/* compute_Omega_D (Transport.cu:168-170) */
+static double omega_d(double tr) { return 1.0 / pow(tr, 0.145) + 1.0 / ((tr + 0.5) * (tr + 0.5)); }
+
+/* update_physical_properties<mixture> (FieldOperation.cuh:116-134) with compute_transport_property
+ * (Transport.cu:43-136): cp, gamma, c, Wilke viscosity, Eucken-type conductivity, mixture-averaged
+ * rho*D_k. */
+static void mix_properties_node(orc_ctx *o, long p) {
+  const orc_chem *ch = o->c.chem;
+  const int ns = o->ns;
+  const long P = o->P;
+  const double t = o->bv[5 * P + p];
+  double cp[ORC_MAX_SPEC];
+  mix_h_cp(ch, t, NULL, cp);
+  double mw = 0, cpt = 0, cvt = 0;
+  for (int l = 0; l < ns; ++l) {
+    const double y = o->sv[l * P + p];
+    mw += y / ch->mw[l];
+    cpt += y * cp[l];
+    cvt += y * (cp[l] - R_U / ch->mw[l]);
+  }
+  mw = 1 / mw;
+  o->cpm[p] = cpt;
+  o->gam[p] = cpt / cvt;
+  o->acs[p] = sqrt(o->gam[p] * R_U * t / mw);
+  double X[ORC_MAX_SPEC], vis[ORC_MAX_SPEC], dij[ORC_MAX_SPEC * ORC_MAX_SPEC];
+  for (int l = 0; l < ns; ++l) {
+    X[l] = o->sv[l * P + p] * mw / ch->mw[l];
+    const double tdl = t * ch->lj_potent_inv[l];
+    const double ci = 1.147 * pow(tdl, -0.145) + pow(tdl + 0.5, -2);
+    vis[l] = ch->vis_coeff[l] * sqrt(t) / ci;
+  }
+  const double t32p = t * sqrt(t) / o->bv[4 * P + p];
+  for (int m = 0; m < ns; ++m)
+    for (int n = m; n < ns; ++n) {
+      const double tr = t * ch->kb_over_eps_jk[m * ns + n];
+      dij[m * ns + n] = ch->binary_diff[m * ns + n] * t32p / omega_d(tr);
+      if (m != n) dij[n * ns + m] = dij[m * ns + n];
+    }
+  double visc = 0, cond = 0;
+  for (int m = 0; m < ns; ++m) {
+    double vt = 0;
+    for (int n = 0; n < ns; ++n) {
+      double pf = 1.0;
+      if (m != n) {
+        const double num = 1 + sqrt(vis[m] / vis[n]) * ch->wj_div_wi_1_4[m * ns + n];
+        pf = num * num * ch->sqrt_wiwj_8[m * ns + n];
+      }
+      vt += pf * X[n];
+    }
+    const double ct = 1.065 * vt - 0.065 * X[m];
+    visc += vis[m] * X[m] / vt;
+    const double lam = vis[m] * (cp[m] + 1.25 * R_U / ch->mw[m]);
+    cond += lam * X[m] / ct;
+  }
+  o->mul[p] = visc;
+  o->cond[p] = cond;
+  const double eps = 1e-12;
+  for (int l = 0; l < ns; ++l) {
+    double num = 0, den = 0;
+    for (int n = 0; n < ns; ++n)
+      if (l != n) {
+        num += (X[n] + eps) * ch->mw[n];
+        den += (X[n] + eps) / dij[l * ns + n];
+      }
+    o->rhod[l * P + p] = o->bv[p] * num / (den * mw);
+  }
+}
+
+/* compute_temperature_and_pressure (FieldOperation.cu:3-40): Newton on e(T) from the current T,
+ * relative tolerance 1e-3, at most 1000 iterations; p = rho R T. */
+static void mix_t_and_p(orc_ctx *o, long p, double total_energy) {
+  const orc_chem *ch = o->c.chem;
+  const long P = o->P;
+  double mw = 0;
+  for (int l = 0; l < o->ns; ++l) mw += o->sv[l * P + p] / ch->mw[l];
+  mw = 1 / mw;
+  const double gc = R_U / mw;
+  const double u = o->bv[P + p], v = o->bv[2 * P + p], w = o->bv[3 * P + p];
+  const double e = total_energy / o->bv[p] - 0.5 * (u * u + v * v + w * w);
+  double err = 1, t = o->bv[5 * P + p];
+  int iter = 0;
+  double h[ORC_MAX_SPEC], cp[ORC_MAX_SPEC];
+  while (err > 1e-3 && iter++ < 1000) {
+    mix_h_cp(ch, t, h, cp);
+    double cpt = 0, hm = 0;
+    for (int l = 0; l < o->ns; ++l) {
+      cpt += cp[l] * o->sv[l * P + p];
+      hm += h[l] * o->sv[l * P + p];
+    }
+    const double et = hm - gc * t;
+    const double cv = cpt - gc;
+    const double t1 = t - (et - e) / cv;
+    err = fabs(1 - t1 / t);
+    t = t1;
+  }
+  o->bv[5 * P + p] = t;
+  o->bv[4 * P + p] = o->bv[p] * t * gc;
+}
+
+/* ---------------------------------------------------------------- mixtures: chemistry */
+
+static double arrhenius(double t, double A, double b, double Ea) { return A * pow(t, b) * exp(-Ea / t); }
+
+/* finite_rate_chemistry (FiniteRateChem.cu:7-58) with forward_reaction_rate (:60-102),
+ * backward_reaction_rate (:108-150), rate_of_progress (:152-177), chemical_source (:179-195):
+ * dq[5+l] += jac * omega_l at interior node (i,j,k). */
+static void chemistry_node(orc_ctx *o, int i, int j, int k) {
+  const orc_chem *ch = o->c.chem;
+  const int ns = ch->n_spec, nr = ch->n_reac;
+  const long P = o->P, N = (long)o->mx * o->my * o->mz;
+  const long p = ID(o, i, j, k), q = IQ(o, i, j, k);
+  double c[ORC_MAX_SPEC];
+  const double rho = o->bv[p];
+  for (int l = 0; l < ns; ++l) c[l] = rho * o->sv[l * P + p] / ch->mw[l] * 1e-3;
+  const double t = o->bv[5 * P + p];
+  double kf[ORC_MAX_REAC], kb[ORC_MAX_REAC];
+  for (int r = 0; r < nr; ++r) {
+    kb[r] = 0;
+    kf[r] = arrhenius(t, ch->A[r], ch->b[r], ch->Ea[r]);
+    const int ty = ch->label[r];
+    if (ty == 3) {
+      kf[r] += arrhenius(t, ch->A2[r], ch->b2[r], ch->Ea2[r]);
+    } else if (ty > 3) {
+      double cc = 0;
+      for (int l = 0; l < ns; ++l) cc += c[l] * ch->third_body[r * ns + l];
+      if (ty == 4) {
+        kf[r] *= cc;
+      } else {
+        const double klow = arrhenius(t, ch->A2[r], ch->b2[r], ch->Ea2[r]);
+        const double khigh = kf[r];
+        const double pr = klow * cc / khigh;
+        double F = 1.0;
+        if (ty > 5) {
+          double fc = (1 - ch->troe_alpha[r]) * exp(-t / ch->troe_t3[r]) + ch->troe_alpha[r] * exp(-t / ch->troe_t1[r]);
+          if (ty == 7) fc += exp(-ch->troe_t2[r] / t);
+          const double lfc = log10(fc);
+          const double cq = -0.4 - 0.67 * lfc;
+          const double nq = 0.75 - 1.27 * lfc;
+          const double lpr = log10(pr);
+          const double tmp = (lpr + cq) / (nq - 0.14 * (lpr + cq));
+          const double pw = lfc / (1.0 + tmp * tmp);
+          F = pow(10, pw);
+        }
+        kf[r] = khigh * pr / (1.0 + pr) * F;
+      }
+    }
+  }
+  int n_gibbs = nr;
+  for (int r = 0; r < nr; ++r) {
+    if (ch->label[r] == 0) {
+      kb[r] = 0;
+      --n_gibbs;
+    } else if (ch->rev_type[r] == 1) {
+      kb[r] = arrhenius(t, ch->A2[r], ch->b2[r], ch->Ea2[r]);
+      if (ch->label[r] == 4) {
+        double cc = 0;
+        for (int l = 0; l < ns; ++l) cc += c[l] * ch->third_body[r * ns + l];
+        kb[r] *= cc;
+      }
+      --n_gibbs;
+    }
+  }
+  if (n_gibbs >= 1) {
+    double g[ORC_MAX_SPEC];
+    mix_gibbs_rt(ch, t, g);
+    const double temp_p = 101325.0 / R_U * 1e-3;
+    const double temp_t = temp_p / t;
+    for (int r = 0; r < nr; ++r) {
+      if (ch->label[r] != 2 && ch->label[r] != 0) {
+        double dg = 0;
+        for (int l = 0; l < ns; ++l) dg += g[l] * (ch->stoi_b[r * ns + l] - ch->stoi_f[r * ns + l]);
+        const double kc = pow(temp_t, ch->order[r]) * exp(-dg);
+        kb[r] = kf[r] / kc;
+      }
+    }
+  }
+  double q1[ORC_MAX_REAC], q2[ORC_MAX_REAC];
+  for (int r = 0; r < nr; ++r) {
+    q1[r] = 1.0;
+    q2[r] = ch->label[r] != 0 ? 1.0 : 0.0;
+    for (int l = 0; l < ns; ++l) q1[r] *= pow(c[l], ch->stoi_f[r * ns + l]);
+    if (ch->label[r] != 0)
+      for (int l = 0; l < ns; ++l) q2[r] *= pow(c[l], ch->stoi_b[r * ns + l]);
+    q1[r] *= kf[r];
+    if (ch->label[r] != 0) q2[r] *= kb[r];
+  }
+  const double jac = o->jac[p];
+  for (int l = 0; l < ns; ++l) {
+    double cre = 0, des = 0;
+    for (int r = 0; r < nr; ++r) {
+      cre += q2[r] * ch->stoi_f[r * ns + l] + q1[r] * ch->stoi_b[r * ns + l];
+      des += q1[r] * ch->stoi_f[r * ns + l] + q2[r] * ch->stoi_b[r * ns + l];
+    }
+    cre *= ch->mw[l] * 1e+3;
+    des *= ch->mw[l] * 1e+3;
+    o->dq[(5 + l) * N + q] += jac * (cre - des);
+  }
+}
+
+/* ---------------------------------------------------------------- flux-split WENO (51/52/71/72) */
+
+/* WENO7 of the flux-split path (WENO.cu:1619-1693): Z-type weights with tau = |b0 - b3|, linear
+ * weights 1/35, 12/35, 18/35, 4/35; returns f+ + f-. */
+static double fvs_beta7(double s1, double s2, double s3) {
+  return s1 * s1 + 13.0 / 12.0 * s2 * s2 + 1043.0 / 960 * s3 * s3 + 1.0 / 12 * s1 * s3;
+}
+
+static double fvs_weno7(const double *vp, const double *vm, double eps) {
+  const double one6th = 1.0 / 6, one12th = 1.0 / 12;
+  const double c0 = 1.0 / 35, c1 = 12.0 / 35, c2 = 18.0 / 35, c3 = 4.0 / 35;
+  double s1 = one6th * (-2 * vp[0] + 9 * vp[1] - 18 * vp[2] + 11 * vp[3]);
+  double s2 = -vp[0] + 4 * vp[1] - 5 * vp[2] + 2 * vp[3];
+  double s3 = -vp[0] + 3 * vp[1] - 3 * vp[2] + vp[3];
+  double b0 = fvs_beta7(s1, s2, s3);
+  s1 = one6th * (vp[1] - 6 * vp[2] + 3 * vp[3] + 2 * vp[4]);
+  s2 = vp[2] - 2 * vp[3] + vp[4];
+  s3 = -vp[1] + 3 * vp[2] - 3 * vp[3] + vp[4];
+  double b1 = fvs_beta7(s1, s2, s3);
+  s1 = one6th * (-2 * vp[2] - 3 * vp[3] + 6 * vp[4] - vp[5]);
+  s3 = -vp[2] + 3 * vp[3] - 3 * vp[4] + vp[5];
+  double b2 = fvs_beta7(s1, s2, s3);
+  s1 = one6th * (-11 * vp[3] + 18 * vp[4] - 9 * vp[5] + 2 * vp[6]);
+  s2 = 2 * vp[3] - 5 * vp[4] + 4 * vp[5] - vp[6];
+  s3 = -vp[3] + 3 * vp[4] - 3 * vp[5] + vp[6];
+  double b3 = fvs_beta7(s1, s2, s3);
+  double tau = (b0 - b3) * (b0 - b3);
+  double a0 = c0 + c0 * tau / ((eps + b0) * (eps + b0));
+  double a1 = c1 + c1 * tau / ((eps + b1) * (eps + b1));
+  double a2 = c2 + c2 * tau / ((eps + b2) * (eps + b2));
+  double a3 = c3 + c3 * tau / ((eps + b3) * (eps + b3));
+  double v0 = one12th * (-3 * vp[0] + 13 * vp[1] - 23 * vp[2] + 25 * vp[3]);
+  double v1 = one12th * (vp[1] - 5 * vp[2] + 13 * vp[3] + 3 * vp[4]);
+  double v2 = one12th * (-vp[2] + 7 * vp[3] + 7 * vp[4] - vp[5]);
+  double v3 = one12th * (3 * vp[3] + 13 * vp[4] - 5 * vp[5] + vp[6]);
+  const double fp = (a0 * v0 + a1 * v1 + a2 * v2 + a3 * v3) / (a0 + a1 + a2 + a3);
+  s1 = one6th * (-2 * vm[6] + 9 * vm[5] - 18 * vm[4] + 11 * vm[3]);
+  s2 = -vm[6] + 4 * vm[5] - 5 * vm[4] + 2 * vm[3];
+  s3 = -vm[6] + 3 * vm[5] - 3 * vm[4] + vm[3];
+  b0 = fvs_beta7(s1, s2, s3);
+  s1 = one6th * (vm[5] - 6 * vm[4] + 3 * vm[3] + 2 * vm[2]);
+  s2 = vm[4] - 2 * vm[3] + vm[2];
+  s3 = -vm[5] + 3 * vm[4] - 3 * vm[3] + vm[2];
+  b1 = fvs_beta7(s1, s2, s3);
+  s1 = one6th * (-2 * vm[4] - 3 * vm[3] + 6 * vm[2] - vm[1]);
+  s3 = -vm[4] + 3 * vm[3] - 3 * vm[2] + vm[1];
+  b2 = fvs_beta7(s1, s2, s3);
+  s1 = one6th * (-11 * vm[3] + 18 * vm[2] - 9 * vm[1] + 2 * vm[0]);
+  s2 = 2 * vm[3] - 5 * vm[2] + 4 * vm[1] - vm[0];
+  s3 = -vm[3] + 3 * vm[2] - 3 * vm[1] + vm[0];
+  b3 = fvs_beta7(s1, s2, s3);
+  tau = (b0 - b3) * (b0 - b3);
+  a0 = c0 + c0 * tau / ((eps + b0) * (eps + b0));
+  a1 = c1 + c1 * tau / ((eps + b1) * (eps + b1));
+  a2 = c2 + c2 * tau / ((eps + b2) * (eps + b2));
+  a3 = c3 + c3 * tau / ((eps + b3) * (eps + b3));
+  v0 = one12th * (-3 * vm[6] + 13 * vm[5] - 23 * vm[4] + 25 * vm[3]);
+  v1 = one12th * (vm[5] - 5 * vm[4] + 13 * vm[3] + 3 * vm[2]);
+  v2 = one12th * (-vm[4] + 7 * vm[3] + 7 * vm[2] - vm[1]);
+  v3 = one12th * (3 * vm[3] + 13 * vm[2] - 5 * vm[1] + vm[0]);
+  const double fm = (a0 * v0 + a1 * v1 + a2 * v2 + a3 * v3) / (a0 + a1 + a2 + a3);
+  return fp + fm;
+}
+
+/* compute_flux (WENO.cu:697-720): Lax-Friedrichs split F+- of one node with lambda0 = |U_k| + c|grad k|.
+ * Q: cv[nv], then p, then c. */
+static void fvs_node_flux(const double *Q, int nv, const double *k, double jac, double *Fp, double *Fm) {
+  const double Uk = (Q[1] * k[0] + Q[2] * k[1] + Q[3] * k[2]) / Q[0];
+  const double pk = Q[nv];
+  const double cg = Q[nv + 1] * sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]);
+  const double l0 = fabs(Uk) + cg;
+  Fp[0] = 0.5 * jac * (Uk * Q[0] + l0 * Q[0]);
+  Fp[1] = 0.5 * jac * (Uk * Q[1] + pk * k[0] + l0 * Q[1]);
+  Fp[2] = 0.5 * jac * (Uk * Q[2] + pk * k[1] + l0 * Q[2]);
+  Fp[3] = 0.5 * jac * (Uk * Q[3] + pk * k[2] + l0 * Q[3]);
+  Fp[4] = 0.5 * jac * (Uk * (Q[4] + pk) + l0 * Q[4]);
+  Fm[0] = 0.5 * jac * (Uk * Q[0] - l0 * Q[0]);
+  Fm[1] = 0.5 * jac * (Uk * Q[1] + pk * k[0] - l0 * Q[1]);
+  Fm[2] = 0.5 * jac * (Uk * Q[2] + pk * k[1] - l0 * Q[2]);
+  Fm[3] = 0.5 * jac * (Uk * Q[3] + pk * k[2] - l0 * Q[3]);
+  Fm[4] = 0.5 * jac * (Uk * (Q[4] + pk) - l0 * Q[4]);
+  for (int l = 5; l < nv; ++l) {
+    Fp[l] = 0.5 * jac * (Uk * Q[l] + l0 * Q[l]);
+    Fm[l] = 0.5 * jac * (Uk * Q[l] - l0 * Q[l]);
+  }
+}
+
+#define FVS_MAXV (5 + ORC_MAX_SPEC)
+
+/* compute_weno_flux_ch<mixture> for inviscid_scheme 72 (WENO.cu:722-758, 899-965, 1119-1142):
+ * Roe-averaged mixture eigensystem at the face, characteristic projection of the split fluxes of
+ * 7 nodes each side, WENO7-Z per field, back-projection.  Q[s]: node idx-3+s (s = 0..7), each
+ * cv[nv], p, c; mt/jc: metric row and Jacobian of the same nodes. */
+static void fvs_char_face(const orc_ctx *o, double Q[8][FVS_MAXV + 2], double mt[8][3], const double jc[8],
+                          double *fc) {
+  const orc_chem *ch = o->c.chem;
+  const int nv = o->nv, ns = o->ns;
+  double Fp[8][FVS_MAXV], Fm[8][FVS_MAXV];
+  for (int s = 0; s < 8; ++s) fvs_node_flux(Q[s], nv, mt[s], jc[s], Fp[s], Fm[s]);
+  const double *cvl = Q[3], *cvr = Q[4];
+  const double *m_l = mt[3], *m_r = mt[4];
+  const double rli = 1.0 / cvl[0], rri = 1.0 / cvr[0];
+  const double rlc = sqrt(cvl[0]) / (sqrt(cvl[0]) + sqrt(cvr[0]));
+  const double rrc = sqrt(cvr[0]) / (sqrt(cvl[0]) + sqrt(cvr[0]));
+  const double um = rlc * cvl[1] * rli + rrc * cvr[1] * rri;
+  const double vm = rlc * cvl[2] * rli + rrc * cvr[2] * rri;
+  const double wm = rlc * cvl[3] * rli + rrc * cvr[3] * rri;
+  const double ekm = 0.5 * (um * um + vm * vm + wm * wm);
+  const double hl = (cvl[4] + cvl[nv]) * rli;
+  const double hr = (cvr[4] + cvr[nv]) * rri;
+  const double hm = rlc * hl + rrc * hr;
+  double svm[ORC_MAX_SPEC];
+  for (int l = 0; l < ns; ++l) svm[l] = rlc * cvl[l + 5] * rli + rrc * cvr[l + 5] * rri;
+  double mw_inv = 0;
+  for (int l = 0; l < ns; ++l) mw_inv += svm[l] / ch->mw[l];
+  const double tl = cvl[nv] * rli, tr = cvr[nv] * rri;
+  const double tm = (rlc * tl + rrc * tr) / (R_U * mw_inv);
+  double cpi[ORC_MAX_SPEC], hi[ORC_MAX_SPEC];
+  mix_h_cp(ch, tm, hi, cpi);
+  double cp = 0, cvt = 0;
+  for (int l = 0; l < ns; ++l) {
+    cp += svm[l] * cpi[l];
+    cvt += svm[l] * (cpi[l] - R_U / ch->mw[l]);
+  }
+  const double gamma = cp / cvt;
+  const double cm = sqrt(gamma * R_U * mw_inv * tm);
+  const double gm1 = gamma - 1;
+  const double jl = jc[3], jr = jc[4];
+  const double kxJ = m_l[0] * jl + m_r[0] * jr, kyJ = m_l[1] * jl + m_r[1] * jr, kzJ = m_l[2] * jl + m_r[2] * jr;
+  double kx = kxJ / (jl + jr), ky = kyJ / (jl + jr), kz = kzJ / (jl + jr);
+  const double gradK = sqrt(kx * kx + ky * ky + kz * kz);
+  kx /= gradK;
+  ky /= gradK;
+  kz /= gradK;
+  const double Ukb = kx * um + ky * vm + kz * wm;
+  const double alpha = gm1 * ekm;
+  const double c2i = 1.0 / (cm * cm);
+  const double eps = 1e-40 * o->c.weno_eps_scale * 0.25 * (kxJ * kxJ + kyJ * kyJ + kzJ * kzJ);
+  double al[ORC_MAX_SPEC];
+  for (int l = 0; l < ns; ++l) {
+    al[l] = gamma * R_U / ch->mw[l] * tm - (gamma - 1) * hi[l];
+    al[l] *= c2i;
+  }
+  double fch[FVS_MAXV];
+  for (int l = 0; l < 5; ++l) {
+    double cs = 0.5, L[5];
+    switch (l) {
+      case 0:
+        L[0] = (alpha + Ukb * cm) * c2i * 0.5;
+        L[1] = -(gm1 * um + kx * cm) * c2i * 0.5;
+        L[2] = -(gm1 * vm + ky * cm) * c2i * 0.5;
+        L[3] = -(gm1 * wm + kz * cm) * c2i * 0.5;
+        L[4] = gm1 * c2i * 0.5;
+        break;
+      case 1:
+        cs = -kx;
+        L[0] = kx * (1 - alpha * c2i) - (kz * vm - ky * wm) / cm;
+        L[1] = kx * gm1 * um * c2i;
+        L[2] = (kx * gm1 * vm + kz * cm) * c2i;
+        L[3] = (kx * gm1 * wm - ky * cm) * c2i;
+        L[4] = -kx * gm1 * c2i;
+        break;
+      case 2:
+        cs = -ky;
+        L[0] = ky * (1 - alpha * c2i) - (kx * wm - kz * um) / cm;
+        L[1] = (ky * gm1 * um - kz * cm) * c2i;
+        L[2] = ky * gm1 * vm * c2i;
+        L[3] = (ky * gm1 * wm + kx * cm) * c2i;
+        L[4] = -ky * gm1 * c2i;
+        break;
+      case 3:
+        cs = -kz;
+        L[0] = kz * (1 - alpha * c2i) - (ky * um - kx * vm) / cm;
+        L[1] = (kz * gm1 * um + ky * cm) * c2i;
+        L[2] = (kz * gm1 * vm - kx * cm) * c2i;
+        L[3] = kz * gm1 * wm * c2i;
+        L[4] = -kz * gm1 * c2i;
+        break;
+      default:
+        L[0] = (alpha - Ukb * cm) * c2i * 0.5;
+        L[1] = -(gm1 * um - kx * cm) * c2i * 0.5;
+        L[2] = -(gm1 * vm - ky * cm) * c2i * 0.5;
+        L[3] = -(gm1 * wm - kz * cm) * c2i * 0.5;
+        L[4] = gm1 * c2i * 0.5;
+        break;
+    }
+    double vp[7] = {0}, vmn[7] = {0};
+    for (int m = 0; m < 7; ++m) {
+      for (int n = 0; n < 5; ++n) {
+        vp[m] += L[n] * Fp[m][n];
+        vmn[m] += L[n] * Fm[m + 1][n];
+      }
+      for (int n = 0; n < ns; ++n) {
+        vp[m] += cs * al[n] * Fp[m][5 + n];
+        vmn[m] += cs * al[n] * Fm[m + 1][5 + n];
+      }
+    }
+    fch[l] = fvs_weno7(vp, vmn, eps);
+  }
+  for (int l = 0; l < ns; ++l) {
+    double vp[7], vmn[7];
+    for (int m = 0; m < 7; ++m) {
+      vp[m] = -svm[l] * Fp[m][0] + Fp[m][5 + l];
+      vmn[m] = -svm[l] * Fm[m + 1][0] + Fm[m + 1][5 + l];
+    }
+    fch[5 + l] = fvs_weno7(vp, vmn, eps);
+  }
+  fc[0] = fch[0] + kx * fch[1] + ky * fch[2] + kz * fch[3] + fch[4];
+  fc[1] = (um - kx * cm) * fch[0] + kx * um * fch[1] + (ky * um - kz * cm) * fch[2] + (kz * um + ky * cm) * fch[3] +
+          (um + kx * cm) * fch[4];
+  fc[2] = (vm - ky * cm) * fch[0] + (kx * vm + kz * cm) * fch[1] + ky * vm * fch[2] + (kz * vm - kx * cm) * fch[3] +
+          (vm + ky * cm) * fch[4];
+  fc[3] = (wm - kz * cm) * fch[0] + (kx * wm - ky * cm) * fch[1] + (ky * wm + kx * cm) * fch[2] + kz * wm * fch[3] +
+          (wm + kz * cm) * fch[4];
+  fc[4] = (hm - Ukb * cm) * fch[0] + (kx * (hm - cm * cm / gm1) + (kz * vm - ky * wm) * cm) * fch[1] +
+          (ky * (hm - cm * cm / gm1) + (kx * wm - kz * um) * cm) * fch[2] +
+          (kz * (hm - cm * cm / gm1) + (ky * um - kx * vm) * cm) * fch[3] + (hm + Ukb * cm) * fch[4];
+  double add = 0;
+  const double ca = fch[0] + kx * fch[1] + ky * fch[2] + kz * fch[3] + fch[4];
+  for (int l = 0; l < ns; ++l) {
+    fc[5 + l] = svm[l] * ca + fch[l + 5];
+    add += al[l] * fch[l + 5];
+  }
+  fc[4] -= add * cm * cm / gm1;
+}
+
+/* compute_weno_flux_cp for inviscid_scheme 71 (WENO.cu:1455-1536): component-wise WENO7-Z of F+-
+ * with eps scaled by the face metric and the reference velocity per equation group. */
+static void fvs_cp_face(const orc_ctx *o, double Q[8][FVS_MAXV + 2], double mt[8][3], const double jc[8],
+                        double *fc) {
+  const int nv = o->nv;
+  double Fp[8][FVS_MAXV], Fm[8][FVS_MAXV];
+  for (int s = 0; s < 8; ++s) fvs_node_flux(Q[s], nv, mt[s], jc[s], Fp[s], Fm[s]);
+  const double j1 = jc[3], j2 = jc[4];
+  const double a0 = mt[3][0] * j1 + mt[4][0] * j2, a1 = mt[3][1] * j1 + mt[4][1] * j2, a2 = mt[3][2] * j1 + mt[4][2] * j2;
+  const double eps_ref = 1e-20 * o->c.weno_eps_scale * 0.25 * (a0 * a0 + a1 * a1 + a2 * a2);
+  double es[3];
+  es[0] = eps_ref;
+  es[1] = eps_ref * o->c.v_ref * o->c.v_ref;
+  es[2] = es[1] * o->c.v_ref * o->c.v_ref;
+  for (int l = 0; l < nv; ++l) {
+    const double e = (l >= 1 && l <= 3) ? es[1] : (l == 4 ? es[2] : es[0]);
+    double vp[7], vmn[7];
+    for (int m = 0; m < 7; ++m) {
+      vp[m] = Fp[m][l];
+      vmn[m] = Fm[m + 1][l];
+    }
+    fc[l] = fvs_weno7(vp, vmn, e);
+  }
+}
+
+/* compute_convective_term_weno_x/_y/_z (WENO.cu:8-461) for scheme 71 or 72 in direction dir: faces
+ * idx+1/2 for idx = -1..n-1, dq -= fc(i+1/2) - fc(i-1/2). */
+static void fvs_direction(orc_ctx *o, int dir) {
+  const int ext[3] = {o->mx, o->my, o->mz};
+  const int nv = o->nv;
+  const long P = o->P, N = (long)o->mx * o->my * o->mz;
+  int e[3] = {0, 0, 0};
+  e[dir] = 1;
+  const int n = ext[dir];
+  int hi[3] = {o->mx, o->my, o->mz};
+  hi[dir] = 1;
+  double *fc = (double *)malloc(sizeof(double) * nv * (n + 1));
+  for (int a = 0; a < hi[0]; ++a)
+    for (int b = 0; b < hi[1]; ++b)
+      for (int cc = 0; cc < hi[2]; ++cc) {
+        for (int idx = -1; idx < n; ++idx) {
+          double Q[8][FVS_MAXV + 2], mt[8][3], jc[8];
+          for (int s = 0; s < 8; ++s) {
+            const int off = idx - 3 + s;
+            const long p = ID(o, a + off * e[0], b + off * e[1], cc + off * e[2]);
+            for (int l = 0; l < nv; ++l) Q[s][l] = o->cv[l * P + p];
+            Q[s][nv] = o->bv[4 * P + p];
+            Q[s][nv + 1] = o->ns ? o->acs[p] : sqrt(GAMMA_AIR * (R_U / MW_AIR) * o->bv[5 * P + p]);
+            for (int q = 0; q < 3; ++q) mt[s][q] = o->met[(long)(dir * 3 + q) * P + p];
+            jc[s] = o->jac[p];
+          }
+          if (o->c.inviscid_scheme == 72) fvs_char_face(o, Q, mt, jc, &fc[nv * (idx + 1)]);
+          else fvs_cp_face(o, Q, mt, jc, &fc[nv * (idx + 1)]);
+        }
+        for (int idx = 0; idx < n; ++idx) {
+          const long q = IQ(o, a + idx * e[0], b + idx * e[1], cc + idx * e[2]);
+          for (int l = 0; l < nv; ++l) o->dq[l * N + q] -= fc[nv * (idx + 1) + l] - fc[nv * idx + l];
+        }
+      }
+  free(fc);
+}
+
 /* ---------------------------------------------------------------- viscous flux */
 
 /* compute_fv/gv/hv_2nd_order<Air, Laminar> (ViscousScheme.cuh:24-318, 321-616, 619-911): face flux
  * between node (i,j,k) and its neighbour in direction d. */
-static void viscous_face(const orc_ctx *o, int i, int j, int k, int d, double fv[5]) {
+/* Gradient (x, y, z) at the face between (i,j,k) and its d-neighbour of the padded plane B: 2-point
+ * normal difference, 4-point averages across, chain rule with the face-averaged metric m. */
+static void face_grad(const orc_ctx *o, const double *B, int i, int j, int k, int d, const double m[9], double out[3]) {
+  int e[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  const long p0 = ID(o, i, j, k), p1 = ID(o, i + e[d][0], j + e[d][1], k + e[d][2]);
+  double g[3];
+  for (int c = 0; c < 3; ++c) {
+    if (c == d) {
+      g[c] = B[p1] - B[p0];
+    } else {
+      const int a0 = e[c][0], a1 = e[c][1], a2 = e[c][2];
+      g[c] = 0.25 * (B[ID(o, i + a0, j + a1, k + a2)] - B[ID(o, i - a0, j - a1, k - a2)] +
+                     B[ID(o, i + e[d][0] + a0, j + e[d][1] + a1, k + e[d][2] + a2)] -
+                     B[ID(o, i + e[d][0] - a0, j + e[d][1] - a1, k + e[d][2] - a2)]);
+    }
+  }
+  out[0] = g[0] * m[0] + g[1] * m[3] + g[2] * m[6];
+  out[1] = g[0] * m[1] + g[1] * m[4] + g[2] * m[7];
+  out[2] = g[0] * m[2] + g[1] * m[5] + g[2] * m[8];
+}
+
+static void viscous_face(const orc_ctx *o, int i, int j, int k, int d, double *fv) {
   const long P = o->P;
   int e[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
   const long p0 = ID(o, i, j, k), p1 = ID(o, i + e[d][0], j + e[d][1], k + e[d][2]);
@@ -894,9 +1461,44 @@ static void viscous_face(const orc_ctx *o, int i, int j, int k, int d, double fv
   const double um = 0.5 * (bv[P + p0] + bv[P + p1]);
   const double vm = 0.5 * (bv[2 * P + p0] + bv[2 * P + p1]);
   const double wm = 0.5 * (bv[3 * P + p0] + bv[3 * P + p1]);
-  const double cp = GAMMA_AIR * R_U / MW_AIR / (GAMMA_AIR - 1);
-  const double cond = (mul / o->c.prandtl + 0.0 / 0.9) * cp;
+  double cond;
+  if (o->ns) {
+    cond = 0.5 * (o->cond[p0] + o->cond[p1]);
+  } else {
+    const double cp = GAMMA_AIR * R_U / MW_AIR / (GAMMA_AIR - 1);
+    cond = (mul / o->c.prandtl + 0.0 / 0.9) * cp;
+  }
   fv[4] = um * fv[1] + vm * fv[2] + wm * fv[3] + cond * (nx * dx[3] + ny * dy[3] + nz * dz[3]);
+  if (o->ns) {
+    /* species diffusion, mixture-averaged with the correction velocity (ViscousScheme.cuh:126-206,
+     * gradPInDiffusionFlux off) */
+    const orc_chem *ch = o->c.chem;
+    const int ns = o->ns;
+    double dif[ORC_MAX_SPEC], yk[ORC_MAX_SPEC], ddf[ORC_MAX_SPEC];
+    double sgw = 0, srdy = 0, corr = 0, mwt = 0;
+    for (int l = 0; l < ns; ++l) {
+      const double *Y = o->sv + (long)l * P;
+      yk[l] = 0.5 * (Y[p0] + Y[p1]);
+      dif[l] = 0.5 * (o->rhod[l * P + p0] + o->rhod[l * P + p1]) + 0.0;
+      double gy[3];
+      face_grad(o, Y, i, j, k, d, m, gy);
+      const double gdy = nx * gy[0] + ny * gy[1] + nz * gy[2];
+      ddf[l] = gdy;
+      corr += dif[l] * gdy;
+      sgw += gdy / ch->mw[l];
+      mwt += yk[l] / ch->mw[l];
+      srdy += dif[l] * yk[l];
+    }
+    mwt = 1.0 / mwt;
+    corr -= mwt * srdy * sgw;
+    double h[ORC_MAX_SPEC];
+    mix_h_cp(ch, 0.5 * (bv[5 * P + p0] + bv[5 * P + p1]), h, NULL);
+    for (int l = 0; l < ns; ++l) {
+      const double flux = dif[l] * (ddf[l] - mwt * yk[l] * sgw) - yk[l] * corr;
+      fv[5 + l] = flux;
+      fv[4] += h[l] * flux;
+    }
+  }
 }
 
 /* viscous_flux_fv/gv/hv (SchemeSelector.cuh:69-154) */
@@ -908,13 +1510,13 @@ static void viscous(orc_ctx *o) {
       for (int j = 0; j < o->my; ++j)
         for (int i = 0; i < o->mx; ++i) {
           const int c[3] = {i, j, k};
-          double fl[5], fr[5];
+          double fl[FVS_MAXV], fr[FVS_MAXV];
           viscous_face(o, i - (d == 0), j - (d == 1), k - (d == 2), d, fl);
           viscous_face(o, i, j, k, d, fr);
           (void)c;
           (void)ext;
           const long q = IQ(o, i, j, k);
-          for (int l = 0; l < 5; ++l) o->dq[l * N + q] += fr[l] - fl[l];
+          for (int l = 0; l < o->nv; ++l) o->dq[l * N + q] += fr[l] - fl[l];
         }
   }
 }
@@ -923,6 +1525,7 @@ static void viscous(orc_ctx *o) {
 
 static void copy_node(orc_ctx *o, long dst, long src) {
   for (int l = 0; l < 6; ++l) o->bv[l * o->P + dst] = o->bv[l * o->P + src];
+  for (int l = 0; l < o->ns; ++l) o->sv[l * o->P + dst] = o->sv[l * o->P + src];
 }
 
 /* apply_symmetry (BoundCond.cuh:137-203) */
@@ -948,6 +1551,7 @@ static void bc_symmetry(orc_ctx *o, const face_t *f) {
         o->bv[pb] = o->bv[pin];
         o->bv[4 * P + pb] = o->bv[4 * P + pin];
         o->bv[5 * P + pb] = o->bv[5 * P + pin];
+        for (int l = 0; l < o->ns; ++l) o->sv[l * P + pb] = o->sv[l * P + pin];
         for (int g = 1; g <= o->g; ++g) {
           const long pg = ID(o, i + g * dir[0], j + g * dir[1], k + g * dir[2]);
           const long pi = ID(o, i - g * dir[0], j - g * dir[1], k - g * dir[2]);
@@ -959,6 +1563,7 @@ static void bc_symmetry(orc_ctx *o, const face_t *f) {
           o->bv[3 * P + pg] = w - 2 * uk * kz;
           o->bv[4 * P + pg] = o->bv[4 * P + pi];
           o->bv[5 * P + pg] = o->bv[5 * P + pi];
+          for (int l = 0; l < o->ns; ++l) o->sv[l * P + pg] = o->sv[l * P + pi];
           cv_from_bv(o, pg);
         }
       }
@@ -1089,7 +1694,11 @@ static void eliminate_k(orc_ctx *o) {
           o->bv[l * P + pp] = o->bv[l * P + p0];
           o->bv[l * P + pm] = o->bv[l * P + p0];
         }
-        for (int l = 0; l < 5; ++l) {
+        for (int l = 0; l < o->ns; ++l) {
+          o->sv[l * P + pp] = o->sv[l * P + p0];
+          o->sv[l * P + pm] = o->sv[l * P + p0];
+        }
+        for (int l = 0; l < o->nv; ++l) {
           o->cv[l * P + pp] = o->cv[l * P + p0];
           o->cv[l * P + pm] = o->cv[l * P + p0];
         }
@@ -1097,7 +1706,12 @@ static void eliminate_k(orc_ctx *o) {
 }
 
 /* update_physical_properties<Air> (FieldOperation.cuh:107-140): mu over the padded block */
+static void mix_properties_node(orc_ctx *o, long p);
 static void properties(orc_ctx *o) {
+  if (o->ns) {
+    for (long p = 0; p < o->P; ++p) mix_properties_node(o, p);
+    return;
+  }
   for (long p = 0; p < o->P; ++p) o->mul[p] = sutherland(o->bv[5 * o->P + p]);
 }
 
@@ -1119,11 +1733,11 @@ double orc_dt(orc_ctx *o) {
         const double U = u * m[0] + v * m[1] + w * m[2];
         const double V = u * m[3] + v * m[4] + w * m[5];
         const double W = u * m[6] + v * m[7] + w * m[8];
-        const double a = sqrt(GAMMA_AIR * R_U * o->bv[5 * P + p] / MW_AIR);
+        const double a = o->ns ? o->acs[p] : sqrt(GAMMA_AIR * R_U * o->bv[5 * P + p] / MW_AIR);
         const double s0 = fabs(U) + a * gx, s1 = fabs(V) + a * ge;
         const double s2 = o->dim == 3 ? fabs(W) + a * gz : 0;
         const double sinv = s0 + s1 + s2;
-        const double c1 = fmax(GAMMA_AIR, 4.0 / 3.0) / o->bv[p];
+        const double c1 = fmax(o->ns ? o->gam[p] : GAMMA_AIR, 4.0 / 3.0) / o->bv[p];
         const double c2 = o->mul[p] / o->c.prandtl;
         double sv = gx * gx + ge * ge;
         if (o->dim == 3) sv += gz * gz;
@@ -1144,7 +1758,7 @@ static void rk_update(orc_ctx *o, double dt, int rk) {
       for (int i = 0; i < o->mx; ++i) {
         const long p = ID(o, i, j, k), q = IQ(o, i, j, k);
         const double dtj = dt / o->jac[p];
-        for (int l = 0; l < 5; ++l)
+        for (int l = 0; l < o->nv; ++l)
           o->cv[l * P + p] = A[rk] * o->qn[l * P + p] + B[rk] * o->cv[l * P + p] + C[rk] * dtj * o->dq[l * N + q];
         if (o->mz == 1) o->cv[3 * P + p] = 0;
         o->bv[p] = o->cv[p];
@@ -1154,8 +1768,13 @@ static void rk_update(orc_ctx *o, double dt, int rk) {
         o->bv[3 * P + p] = o->cv[3 * P + p] * di;
         const double V2 = o->bv[P + p] * o->bv[P + p] + o->bv[2 * P + p] * o->bv[2 * P + p] +
                           o->bv[3 * P + p] * o->bv[3 * P + p];
-        o->bv[4 * P + p] = (GAMMA_AIR - 1) * (o->cv[4 * P + p] - 0.5 * o->bv[p] * V2);
-        o->bv[5 * P + p] = o->bv[4 * P + p] * MW_AIR * di / R_U;
+        if (o->ns) {
+          for (int l = 0; l < o->ns; ++l) o->sv[l * P + p] = o->cv[(5 + l) * P + p] * di;
+          mix_t_and_p(o, p, o->cv[4 * P + p]);
+        } else {
+          o->bv[4 * P + p] = (GAMMA_AIR - 1) * (o->cv[4 * P + p] - 0.5 * o->bv[p] * V2);
+          o->bv[5 * P + p] = o->bv[4 * P + p] * MW_AIR * di / R_U;
+        }
       }
 }
 
@@ -1174,7 +1793,10 @@ orc_ctx *orc_create(const orc_case *c, const double *x, const double *y, const d
   o->my = c->my;
   o->mz = c->mz;
   o->dim = c->mz == 1 ? 2 : 3;
-  o->g = c->reconstruction == 5 ? 4 : c->reconstruction == 4 ? 3 : 2; /* Parameter.cpp:194-209 */
+  o->g = c->reconstruction == 5 ? 4 : c->reconstruction == 4 ? 3 : 2; /* Parameter.cpp:194-248 */
+  if (c->inviscid_scheme == 71 || c->inviscid_scheme == 72) o->g = 4;
+  o->ns = c->n_spec;
+  o->nv = 5 + c->n_spec;
   o->sx = o->mx + 2 * o->g;
   o->sy = o->my + 2 * o->g;
   o->sz = o->mz + 2 * o->g;
@@ -1199,11 +1821,17 @@ orc_ctx *orc_create(const orc_case *c, const double *x, const double *y, const d
   ghost_grid(o);
   compute_metric(o);
   const long N = (long)o->mx * o->my * o->mz;
-  o->cv = (double *)calloc(5 * o->P, sizeof(double));
-  o->qn = (double *)calloc(5 * o->P, sizeof(double));
+  o->cv = (double *)calloc(o->nv * o->P, sizeof(double));
+  o->qn = (double *)calloc(o->nv * o->P, sizeof(double));
   o->bv = (double *)calloc(6 * o->P, sizeof(double));
   o->mul = (double *)calloc(o->P, sizeof(double));
-  o->dq = (double *)calloc(5 * N, sizeof(double));
+  o->dq = (double *)calloc(o->nv * N, sizeof(double));
+  o->sv = (double *)calloc(o->ns * o->P + 1, sizeof(double));
+  o->rhod = (double *)calloc(o->ns * o->P + 1, sizeof(double));
+  o->cond = (double *)calloc(o->P, sizeof(double));
+  o->cpm = (double *)calloc(o->P, sizeof(double));
+  o->gam = (double *)calloc(o->P, sizeof(double));
+  o->acs = (double *)calloc(o->P, sizeof(double));
   o->dtl = (double *)calloc(N, sizeof(double));
   o->nf = c->n_face;
   for (int n = 0; n < c->n_face; ++n) register_face(o, &c->face[n], &o->f[n]);
@@ -1214,6 +1842,7 @@ void orc_destroy(orc_ctx *o) {
   if (!o) return;
   free(o->x); free(o->y); free(o->z); free(o->jac); free(o->met);
   free(o->cv); free(o->qn); free(o->bv); free(o->mul); free(o->dq); free(o->dtl);
+  free(o->sv); free(o->rhod); free(o->cond); free(o->cpm); free(o->gam); free(o->acs);
   free(o);
 }
 
@@ -1223,14 +1852,21 @@ double orc_time(const orc_ctx *o) { return o->t; }
 
 /* Initialisation: Driver::initialize_computation (Driver.cu:115-199) then compute_cv_from_bv over
  * the padded block at the start of RK3 (RK.cuh:37-45). */
-void orc_set_state(orc_ctx *o, const double *bv) {
+void orc_set_state(orc_ctx *o, const double *bv) { orc_set_state_sv(o, bv, NULL); }
+
+void orc_set_state_sv(orc_ctx *o, const double *bv, const double *sv) {
   const long P = o->P, N = (long)o->mx * o->my * o->mz;
   memset(o->bv, 0, sizeof(double) * 6 * P);
-  memset(o->cv, 0, sizeof(double) * 5 * P);
+  memset(o->cv, 0, sizeof(double) * o->nv * P);
+  if (o->ns) memset(o->sv, 0, sizeof(double) * o->ns * P);
   for (int l = 0; l < 6; ++l)
     for (int k = 0; k < o->mz; ++k)
       for (int j = 0; j < o->my; ++j)
         for (int i = 0; i < o->mx; ++i) o->bv[l * P + ID(o, i, j, k)] = bv[l * N + IQ(o, i, j, k)];
+  for (int l = 0; l < o->ns && sv; ++l)
+    for (int k = 0; k < o->mz; ++k)
+      for (int j = 0; j < o->my; ++j)
+        for (int i = 0; i < o->mx; ++i) o->sv[l * P + ID(o, i, j, k)] = sv[l * N + IQ(o, i, j, k)];
   if (o->dim == 2) eliminate_k(o);
   apply_bcs(o);
   properties(o);
@@ -1244,7 +1880,7 @@ void orc_get_state(const orc_ctx *o, double *cv, double *bv, double *mul) {
     for (int j = 0; j < o->my; ++j)
       for (int i = 0; i < o->mx; ++i) {
         const long p = ID(o, i, j, k), q = IQ(o, i, j, k);
-        if (cv) for (int l = 0; l < 5; ++l) cv[l * N + q] = o->cv[l * P + p];
+        if (cv) for (int l = 0; l < o->nv; ++l) cv[l * N + q] = o->cv[l * P + p];
         if (bv) for (int l = 0; l < 6; ++l) bv[l * N + q] = o->bv[l * P + p];
         if (mul) mul[q] = o->mul[p];
       }
@@ -1261,26 +1897,48 @@ void orc_get_metric(const orc_ctx *o, double *metric9, double *jac) {
       }
 }
 
+void orc_get_mixture(const orc_ctx *o, double *sv, double *cond, double *rho_d, double *acoustic, double *gamma) {
+  const long P = o->P, N = (long)o->mx * o->my * o->mz;
+  for (int k = 0; k < o->mz; ++k)
+    for (int j = 0; j < o->my; ++j)
+      for (int i = 0; i < o->mx; ++i) {
+        const long p = ID(o, i, j, k), q = IQ(o, i, j, k);
+        for (int l = 0; l < o->ns; ++l) {
+          if (sv) sv[l * N + q] = o->sv[l * P + p];
+          if (rho_d) rho_d[l * N + q] = o->rhod[l * P + p];
+        }
+        if (cond) cond[q] = o->cond[p];
+        if (acoustic) acoustic[q] = o->acs[p];
+        if (gamma) gamma[q] = o->gam[p];
+      }
+}
+
 void orc_rhs(orc_ctx *o, unsigned mask, double *dq) {
   const long N = (long)o->mx * o->my * o->mz;
-  memset(o->dq, 0, sizeof(double) * 5 * N);
+  memset(o->dq, 0, sizeof(double) * o->nv * N);
+  if ((mask & 4u) && o->ns && o->c.finite_rate)
+    for (int k = 0; k < o->mz; ++k)
+      for (int j = 0; j < o->my; ++j)
+        for (int i = 0; i < o->mx; ++i) chemistry_node(o, i, j, k);
   if (mask & 1u)
     for (int d = 0; d < o->dim; ++d) {
-      if (o->c.reconstruction == 4 || o->c.reconstruction == 5) aweno_direction(o, d);
+      const int is = o->c.inviscid_scheme;
+      if (is == 71 || is == 72) fvs_direction(o, d);
+      else if (o->c.reconstruction == 4 || o->c.reconstruction == 5) aweno_direction(o, d);
       else pv_direction(o, d);
     }
   if ((mask & 2u) && o->c.viscous_order != 0) viscous(o);
-  if (dq) memcpy(dq, o->dq, sizeof(double) * 5 * N);
+  if (dq) memcpy(dq, o->dq, sizeof(double) * o->nv * N);
 }
 
-/* RK3<Air, Laminar> time loop body (RK.cuh:85-185) */
+/* RK3<mixture model, Laminar> time loop body (RK.cuh:85-185) */
 double orc_step(orc_ctx *o, int n) {
   double dt = o->c.fixed_time_step ? o->c.dt : 1e6;
   for (int s = 0; s < n; ++s) {
-    memcpy(o->qn, o->cv, sizeof(double) * 5 * o->P);
+    memcpy(o->qn, o->cv, sizeof(double) * o->nv * o->P);
     for (int rk = 0; rk < 3; ++rk) {
       if (!o->c.fixed_time_step && rk == 0) dt = orc_dt(o);
-      orc_rhs(o, 3u, NULL);
+      orc_rhs(o, 7u, NULL);
       rk_update(o, dt, rk);
       fill_ghosts(o);
     }

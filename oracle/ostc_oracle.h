@@ -25,6 +25,23 @@ typedef struct {
   double density, u, v, w, pressure, temperature, acoustic_speed, gamma, entropy, mw;
 } orc_face_in;
 
+/* Mixture tables (Species / Reaction, ChemData.cpp; DParameter.cu:57-155), row-major [i][j]. */
+#define ORC_MAX_SPEC 16
+#define ORC_MAX_REAC 64
+typedef struct {
+  int n_spec, n_reac;
+  double mw[ORC_MAX_SPEC], t_low[ORC_MAX_SPEC], t_mid[ORC_MAX_SPEC];
+  double low[ORC_MAX_SPEC * 7], high[ORC_MAX_SPEC * 7];
+  double lj_potent_inv[ORC_MAX_SPEC], vis_coeff[ORC_MAX_SPEC];
+  double wj_div_wi_1_4[ORC_MAX_SPEC * ORC_MAX_SPEC], sqrt_wiwj_8[ORC_MAX_SPEC * ORC_MAX_SPEC];
+  double binary_diff[ORC_MAX_SPEC * ORC_MAX_SPEC], kb_over_eps_jk[ORC_MAX_SPEC * ORC_MAX_SPEC];
+  int label[ORC_MAX_REAC], rev_type[ORC_MAX_REAC], order[ORC_MAX_REAC];
+  int stoi_f[ORC_MAX_REAC * ORC_MAX_SPEC], stoi_b[ORC_MAX_REAC * ORC_MAX_SPEC];
+  double A[ORC_MAX_REAC], b[ORC_MAX_REAC], Ea[ORC_MAX_REAC], A2[ORC_MAX_REAC], b2[ORC_MAX_REAC], Ea2[ORC_MAX_REAC];
+  double third_body[ORC_MAX_REAC * ORC_MAX_SPEC];
+  double troe_alpha[ORC_MAX_REAC], troe_t3[ORC_MAX_REAC], troe_t1[ORC_MAX_REAC], troe_t2[ORC_MAX_REAC];
+} orc_chem;
+
 typedef struct {
   int mx, my, mz;            /* grid nodes of the block */
   int reconstruction;        /* 1 = 1st order, 2 = MUSCL, 3 = NND2, 4 = AWENO5, 5 = AWENO7 (Parameter.cpp:195-209) */
@@ -39,6 +56,13 @@ typedef struct {
   double dt;                 /* used when fixed_time_step != 0 */
   int n_face;
   orc_face_in face[16];      /* in the order of the boundary file */
+  /* multi-component mixture (species = 1): n_spec > 0 and chem set; finite_rate = 1 adds the
+   * chemical source (reaction = 1, MixtureModel::FR) */
+  int n_spec;
+  int finite_rate;
+  const orc_chem *chem;
+  double weno_eps_scale;     /* rho_inf^2 v_inf^2 of the reference state (DParameter.cu:26-29) */
+  double v_ref;              /* v_inf (component-wise WENO eps scaling, WENO.cu:1471-1473) */
 } orc_case;
 
 typedef struct orc_ctx orc_ctx;
@@ -49,12 +73,18 @@ void orc_destroy(orc_ctx *o);
 int orc_ngg(const orc_ctx *o);
 /* bv: [6][mz][my][mx] interior (rho, u, v, w, p, T).  Runs the reference initialisation sequence. */
 void orc_set_state(orc_ctx *o, const double *bv);
-/* Interior copies of cv[5][N], bv[6][N] and mul[N] (any pointer may be NULL). */
+/* Same with the species mass fractions sv: [n_spec][mz][my][mx] (mixtures). */
+void orc_set_state_sv(orc_ctx *o, const double *bv, const double *sv);
+/* Interior copies of cv[n_var][N], bv[6][N] and mul[N] (any pointer may be NULL); n_var = 5 + n_spec. */
 void orc_get_state(const orc_ctx *o, double *cv, double *bv, double *mul);
+/* Interior mass fractions sv[n_spec][N] and, when non-NULL, thermal conductivity, rho*D[n_spec][N],
+ * acoustic speed and gamma (mixtures). */
+void orc_get_mixture(const orc_ctx *o, double *sv, double *cond, double *rho_d, double *acoustic, double *gamma);
 /* Metric (9 entries, row-major 1-based (r,c) -> (r-1)*3+c-1) and Jacobian on the interior nodes. */
 void orc_get_metric(const orc_ctx *o, double *metric9, double *jac);
-/* Right-hand side dq[5][N] of the current state.  mask: 1 = inviscid (AWENO + Riemann + CDS, or a
- * primitive reconstruction + Riemann),
+/* Right-hand side dq[n_var][N] of the current state.  mask: 4 = chemical source (evaluated first,
+ * RK.cuh:116), 1 = inviscid (AWENO + Riemann + CDS, a primitive reconstruction + Riemann, or the
+ * flux-split WENO of inviscid_scheme 51/52/71/72),
  * 2 = viscous; the reference evaluates them in that order (RK.cuh:138-139). */
 void orc_rhs(orc_ctx *o, unsigned mask, double *dq);
 /* n full SSP-RK3 steps (RK.cuh:85-185).  Returns the last dt. */

@@ -3,11 +3,12 @@
 //
 // Usage (cwd = case directory holding ./input/setup.txt, grid and boundary files):
 //   ref_harness state_in.bin state_out.bin
-// It builds cfd::Parameter, cfd::Mesh and cfd::Driver<Air, Laminar> as the reference's main() does
-// (main.cu:8-136), replaces the freshly initialised interior primitive variables with the ones in
-// state_in.bin ([block][6][mz][my][mx] doubles), runs the reference's
+// It builds cfd::Parameter, cfd::Mesh and cfd::Driver<model, Laminar> as the reference's main() does
+// (main.cu:8-136; model Air, Mixture or FR from the species/reaction keys), replaces the freshly
+// initialised interior primitive variables with the ones in state_in.bin ([block][6 + n_spec][mz][my][mx]
+// doubles: rho u v w p T, then the mass fractions), runs the reference's
 // Driver::initialize_computation() and RK3() (RK.cuh:19-228) for total_step steps, and writes the
-// interior cv[5] and bv[6] of every block, then the physical time, to state_out.bin.  It prints the
+// interior cv[n_var], bv[6] and sv[n_spec] of every block, then the physical time, to state_out.bin.  It prints the
 // wall time of the RK3 call (steps, per-step output checks and the final flow-field file included).
 #include <chrono>
 #include <cstdio>
@@ -33,17 +34,11 @@ long long padded_index(int mx, int my, int mz, int ngg, int i, int j, int k, int
 const char *g_stage = "start";
 }  // namespace
 
-int run(const char *fin, const char *fout, int *argc, char ***argv) {
-  g_stage = "Parameter";
-  cfd::Parameter parameter(argc, argv);
-  // the reference reads total_simulation_time without a default (Simulate.cuh:62, RK.cuh:64); the run
-  // is bounded by total_step instead
-  parameter.update_parameter("total_simulation_time", 1e30);
-  g_stage = "Mesh";
-  cfd::Mesh mesh(parameter);
-  if (!parameter.get_bool("turbulence")) parameter.update_parameter("turbulence_method", 0);
+template <MixtureModel M>
+int run_model(cfd::Parameter &parameter, cfd::Mesh &mesh, const char *fin, const char *fout) {
   g_stage = "Driver";
-  cfd::Driver<MixtureModel::Air, cfd::Laminar> driver(parameter, mesh);
+  cfd::Driver<M, cfd::Laminar> driver(parameter, mesh);
+  const int n_var = parameter.get_int("n_var"), n_spec = parameter.get_int("n_spec");
 
   g_stage = "state_in";
   std::FILE *f = std::fopen(fin, "rb");
@@ -55,7 +50,7 @@ int run(const char *fin, const char *fout, int *argc, char ***argv) {
     const int mx = mesh[b].mx, my = mesh[b].my, mz = mesh[b].mz, ngg = mesh[b].ngg;
     const long long n = (long long)mx * my * mz;
     const long long sz = (long long)(mx + 2 * ngg) * (my + 2 * ngg) * (mz + 2 * ngg);
-    std::vector<double> in(6 * n), pad(6 * sz);
+    std::vector<double> in((6 + n_spec) * n), pad(6 * sz), spad(n_spec > 0 ? n_spec * sz : 1);
     if (std::fread(in.data(), sizeof(double), in.size(), f) != in.size()) {
       std::fprintf(stderr, "short state file\n");
       return 2;
@@ -67,6 +62,15 @@ int run(const char *fin, const char *fout, int *argc, char ***argv) {
           for (int i = 0; i < mx; ++i)
             pad[padded_index(mx, my, mz, ngg, i, j, k, l)] = in[l * n + ((long long)k * my + j) * mx + i];
     cudaMemcpy(driver.field[b].h_ptr->bv.data(), pad.data(), pad.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (n_spec > 0) {
+      cudaMemcpy(spad.data(), driver.field[b].h_ptr->sv.data(), spad.size() * sizeof(double), cudaMemcpyDeviceToHost);
+      for (int l = 0; l < n_spec; ++l)
+        for (int k = 0; k < mz; ++k)
+          for (int j = 0; j < my; ++j)
+            for (int i = 0; i < mx; ++i)
+              spad[padded_index(mx, my, mz, ngg, i, j, k, l)] = in[(6 + l) * n + ((long long)k * my + j) * mx + i];
+      cudaMemcpy(driver.field[b].h_ptr->sv.data(), spad.data(), spad.size() * sizeof(double), cudaMemcpyHostToDevice);
+    }
   }
   std::fclose(f);
 
@@ -75,7 +79,7 @@ int run(const char *fin, const char *fout, int *argc, char ***argv) {
   g_stage = "RK3";
   cudaDeviceSynchronize();
   const auto t_begin = std::chrono::steady_clock::now();
-  cfd::RK3<MixtureModel::Air, cfd::Laminar>(driver);
+  cfd::RK3<M, cfd::Laminar>(driver);
   cudaDeviceSynchronize();
   const double rk3_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_begin).count();
   std::printf("ref_harness: rk3_seconds = %.6f\n", rk3_seconds);
@@ -86,15 +90,20 @@ int run(const char *fin, const char *fout, int *argc, char ***argv) {
     const int mx = mesh[b].mx, my = mesh[b].my, mz = mesh[b].mz, ngg = mesh[b].ngg;
     const long long n = (long long)mx * my * mz;
     const long long sz = (long long)(mx + 2 * ngg) * (my + 2 * ngg) * (mz + 2 * ngg);
-    std::vector<double> cv(5 * sz), bv(6 * sz), out(11 * n);
+    const int nout = n_var + 6 + n_spec;
+    std::vector<double> cv(n_var * sz), bv(6 * sz), sv(n_spec > 0 ? n_spec * sz : 1), out(nout * n);
     cudaMemcpy(cv.data(), driver.field[b].h_ptr->cv.data(), cv.size() * sizeof(double), cudaMemcpyDeviceToHost);
     cudaMemcpy(bv.data(), driver.field[b].h_ptr->bv.data(), bv.size() * sizeof(double), cudaMemcpyDeviceToHost);
-    for (int l = 0; l < 11; ++l)
+    if (n_spec > 0)
+      cudaMemcpy(sv.data(), driver.field[b].h_ptr->sv.data(), sv.size() * sizeof(double), cudaMemcpyDeviceToHost);
+    for (int l = 0; l < nout; ++l)
       for (int k = 0; k < mz; ++k)
         for (int j = 0; j < my; ++j)
           for (int i = 0; i < mx; ++i) {
-            const double v = l < 5 ? cv[padded_index(mx, my, mz, ngg, i, j, k, l)]
-                                   : bv[padded_index(mx, my, mz, ngg, i, j, k, l - 5)];
+            double v;
+            if (l < n_var) v = cv[padded_index(mx, my, mz, ngg, i, j, k, l)];
+            else if (l < n_var + 6) v = bv[padded_index(mx, my, mz, ngg, i, j, k, l - n_var)];
+            else v = sv[padded_index(mx, my, mz, ngg, i, j, k, l - n_var - 6)];
             out[l * n + ((long long)k * my + j) * mx + i] = v;
           }
     std::fwrite(out.data(), sizeof(double), out.size(), f);
@@ -105,6 +114,23 @@ int run(const char *fin, const char *fout, int *argc, char ***argv) {
   const cudaError_t e = cudaGetLastError();
   std::printf("ref_harness: done (%s), t = %.17g\n", cudaGetErrorString(e), t);
   return e == cudaSuccess ? 0 : 1;
+}
+
+int run(const char *fin, const char *fout, int *argc, char ***argv) {
+  g_stage = "Parameter";
+  cfd::Parameter parameter(argc, argv);
+  // the reference reads total_simulation_time without a default (Simulate.cuh:62, RK.cuh:64); the run
+  // is bounded by total_step instead
+  parameter.update_parameter("total_simulation_time", 1e30);
+  g_stage = "Mesh";
+  cfd::Mesh mesh(parameter);
+  if (!parameter.get_bool("turbulence")) parameter.update_parameter("turbulence_method", 0);
+  // model selection as main.cu:60-71 (laminar): species 1 with reaction 1 -> FR, else Mixture
+  if (parameter.get_int("species") == 1) {
+    if (parameter.get_int("reaction") == 1) return run_model<MixtureModel::FR>(parameter, mesh, fin, fout);
+    return run_model<MixtureModel::Mixture>(parameter, mesh, fin, fout);
+  }
+  return run_model<MixtureModel::Air>(parameter, mesh, fin, fout);
 }
 
 int main(int argc, char *argv[]) {

@@ -24,7 +24,6 @@ HARNESS = HERE / "_ref" / "ref_harness"
 EXTRA = """
 // keys the reference reads without defaults (parity runs only)
 int initial = 0
-string reference_state = freestream
 string default_init = freestream
 int output_file = 100000000
 int output_screen = 100000000
@@ -53,7 +52,9 @@ array string stat_rey_1st {
 array string stat_species {
     all
 }
-struct freestream = {
+"""
+
+FREESTREAM = """struct freestream = {
     string type = inflow
     int label = 5
     real mach = @MACH@
@@ -77,17 +78,25 @@ def write_reference_case(case, steps: int, directory: os.PathLike) -> Path:
     setup = setup.replace("int initial = 1\n", "")
     p0 = float(case.bv[4].flat[0])
     t0 = float(case.bv[5].flat[0])
-    setup += EXTRA.replace("@MACH@", "0.5").replace("@P@", repr(p0)).replace("@T@", repr(t0))
+    setup += EXTRA
+    if not case.freestream:
+        setup += FREESTREAM.replace("@MACH@", "0.5").replace("@P@", repr(p0)).replace("@T@", repr(t0))
     (inp / "setup.txt").write_text(setup)
-    np.ascontiguousarray(case.bv, dtype=np.float64).tofile(d / "state_in.bin")
+    if not case.freestream:
+        setup += "string reference_state = freestream\n"
+        (inp / "setup.txt").write_text(setup)
+    with open(d / "state_in.bin", "wb") as f:
+        np.ascontiguousarray(case.bv, dtype=np.float64).tofile(f)
+        if case.sv is not None:
+            np.ascontiguousarray(case.sv, dtype=np.float64).tofile(f)
     (d / "output" / "message").mkdir(parents=True, exist_ok=True)
     return d
 
 
 def run_reference(case, steps: int, workdir: os.PathLike | None = None, timeout: int = 1800,
                   with_seconds: bool = False):
-    """Returns (cv[5,mz,my,mx], bv[6,mz,my,mx], physical time) after `steps` reference RK3 steps, and
-    with_seconds the wall time of the reference's RK3 call."""
+    """Returns (cv[n_var,mz,my,mx], bv[6,mz,my,mx], physical time[, sv[n_spec,...] for mixtures]) after
+    `steps` reference RK3 steps, and with_seconds the wall time of the reference's RK3 call."""
     if not HARNESS.exists():
         raise FileNotFoundError(f"{HARNESS} not built (oracle/ref/build_ref.sh)")
     d = Path(workdir) if workdir else Path(tempfile.mkdtemp(prefix="ostc_ref_"))
@@ -98,8 +107,12 @@ def run_reference(case, steps: int, workdir: os.PathLike | None = None, timeout:
         raise RuntimeError(f"reference harness failed ({r.returncode}):\n{r.stdout[-4000:]}\n{r.stderr[-3000:]}")
     raw = np.fromfile(d / "state_out.bin", dtype=np.float64)
     n = case.nodes
-    out = raw[: 11 * n].reshape((11,) + case.bv.shape[1:])
-    res = (out[:5].copy(), out[5:].copy(), float(raw[11 * n]))
+    ns = 0 if case.sv is None else case.sv.shape[0]
+    nv = 5 + ns
+    out = raw[: (nv + 6 + ns) * n].reshape((nv + 6 + ns,) + case.bv.shape[1:])
+    res = (out[:nv].copy(), out[nv:nv + 6].copy(), float(raw[(nv + 6 + ns) * n]))
+    if ns:
+        res = res + (out[nv + 6:].copy(),)
     if with_seconds:
         sec = [float(l.split("=")[1]) for l in r.stdout.splitlines() if "rk3_seconds" in l]
         return res + (sec[0] if sec else float("nan"),)
