@@ -8,7 +8,7 @@ from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
-SOURCES = ["csrc/host.cpp", "csrc/ostc_air.cu", "csrc/ostc_noalloc.cu"]
+SOURCES = ["csrc/host.cpp", "csrc/chem.cpp", "csrc/ostc_air.cu", "csrc/ostc_noalloc.cu"]
 HEADERS = ["csrc/host.h", "csrc/air_math.cuh"]
 OUT = PKG / "libostc_b200.so"
 

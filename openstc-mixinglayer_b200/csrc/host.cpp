@@ -231,8 +231,13 @@ bool derive(const Setup &s, Derived &d, std::string &err) {
   d.n_spec = 0;
   d.n_scalar = 0;
   d.n_var = 5;
-  if (d.species != 0) {
-    err = "species != 0 (multi-component mixtures) is not supported by this build of the library";
+  d.reaction = s.get_int("reaction");
+  if (d.species != 0 && d.species != 1) {
+    err = "species = " + std::to_string(d.species) + " (mixture-fraction / flamelet models) is not on this library's path";
+    return false;
+  }
+  if (d.species == 1 && d.reaction != 0 && d.reaction != 1) {
+    err = "reaction = " + std::to_string(d.reaction) + " (flamelet) is not on this library's path";
     return false;
   }
   if (s.get_bool("turbulence")) {
@@ -243,9 +248,20 @@ bool derive(const Setup &s, Derived &d, std::string &err) {
     err = "only unsteady SSP-RK3 (steady = 0, temporal_scheme = 3) is on this library's path";
     return false;
   }
-  if (d.inviscid_type == 3 || d.inviscid_type == 4) {
-    err = "inviscid_scheme " + std::to_string(is) +
-          " (characteristic FVS WENO / energy-preserving) is not on this library's path for air";
+  if (d.inviscid_type == 4) {
+    err = "inviscid_scheme 6 (energy-preserving) is not on this library's path";
+    return false;
+  }
+  if (d.inviscid_type == 3 && is != 71 && !(is == 72 && d.species == 1)) {
+    // 51 / 52 stencils read outside the loaded points for the first face of every tile
+    // (WENO.cu:855-856: i_shared - 3 with ngg = 3), and 72 for air runs a 5x5 loop over 7 rows
+    // (WENO.cu:1319-1328): neither defines a result to match
+    err = "inviscid_scheme " + std::to_string(is) + (d.species ? "" : " for air") +
+          " is not supported (reference reads outside its stencil); use 71 or, for mixtures, 72";
+    return false;
+  }
+  if (d.species == 1 && d.inviscid_type != 3) {
+    err = "for mixtures this library implements the flux-split WENO7 path (inviscid_scheme 71 or 72)";
     return false;
   }
   if (d.inviscid_type == 0 || d.inviscid_type == 2) {
@@ -601,7 +617,60 @@ double struct_real(const std::map<std::string, Setup::StructVal> &st, const char
 double sutherland_host(double t) { return 1.7894e-5 * std::pow(t / 288.16, 1.5) * (288.16 + 110) / (t + 110); }
 }  // namespace
 
-bool resolve_boundaries(const Setup &s, const Derived &, HostMesh &mesh, std::string &err) {
+bool reference_scales(const Setup &s, const ChemTables *chem, double &eps_scale, double &v_ref, std::string &err) {
+  eps_scale = 0;
+  v_ref = 0;
+  auto rs = s.strings.find("reference_state");
+  if (rs == s.strings.end()) return true;
+  auto it = s.structs.find(rs->second);
+  if (it == s.structs.end()) {
+    err = "reference_state names struct '" + rs->second + "', which the setup does not define";
+    return false;
+  }
+  const auto &st = it->second;
+  // Inflow::Inflow for a plain inflow struct (BoundCond.cpp:157-214) and the reference state it sets
+  // (:299-305): density from p, T and the mixture weight, velocity = Mach * c (c when |V| < 1).
+  const double mach = struct_real(st, "mach", -1), pressure = struct_real(st, "pressure", -1);
+  const double temperature = struct_real(st, "temperature", -1);
+  double mw = kMwAir, gamma = kGammaAir;
+  if (chem && chem->n_spec > 0) {
+    std::vector<double> y(chem->n_spec, 0.0), cp(chem->n_spec), h(chem->n_spec);
+    for (int i = 0; i < chem->n_spec; ++i) y[i] = struct_real(st, chem->names[i].c_str(), 0.0);
+    mw = 0;
+    for (int i = 0; i < chem->n_spec; ++i) mw += y[i] / chem->mw[i];
+    mw = 1 / mw;
+    // Species::compute_cp (ChemData.cpp:148-171): cp frozen at t_low below it
+    const double t = temperature, t2 = t * t, t3 = t2 * t, t4 = t3 * t;
+    double cpt = 0, cvt = 0;
+    for (int i = 0; i < chem->n_spec; ++i) {
+      double c;
+      if (t < chem->t_low[i]) {
+        const double tt = chem->t_low[i], tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt;
+        const double *a = &chem->low[i * 7];
+        c = a[0] + a[1] * tt + a[2] * tt2 + a[3] * tt3 + a[4] * tt4;
+      } else {
+        const double *a = t < chem->t_mid[i] ? &chem->low[i * 7] : &chem->high[i * 7];
+        c = a[0] + a[1] * t + a[2] * t2 + a[3] * t3 + a[4] * t4;
+      }
+      c *= kRu / chem->mw[i];
+      cpt += y[i] * c;
+      cvt += y[i] * (c - kRu / chem->mw[i]);
+    }
+    gamma = cpt / cvt;
+  }
+  if (mach < 0 || pressure < 0 || temperature < 0) {
+    err = "reference_state struct '" + rs->second + "' needs mach, pressure and temperature on this path";
+    return false;
+  }
+  const double c = std::sqrt(gamma * kRu / mw * temperature);
+  const double velocity = mach * c;
+  const double density = pressure * mw / (kRu * temperature);
+  v_ref = std::abs(velocity) < 1 ? c : velocity;
+  eps_scale = density * v_ref * density * v_ref;
+  return true;
+}
+
+bool resolve_boundaries(const Setup &s, const Derived &d, HostMesh &mesh, std::string &err) {
   // label -> (type, struct name) from the setup's boundary_conditions structs, then default labels
   std::map<int, std::pair<int, std::string>> lab;
   static const std::map<std::string, int> tname{{"wall", kWall},          {"inflow", kInflow},
@@ -628,6 +697,11 @@ bool resolve_boundaries(const Setup &s, const Derived &, HostMesh &mesh, std::st
       if (f.type != kSymmetry && f.type != kFarfield && f.type != kOutflow && f.type != kPeriodic) {
         err = "boundary label " + std::to_string(f.label) +
               " maps to a type outside this path (supported: symmetry 3, farfield 4, outflow 6, periodic 8)";
+        return false;
+      }
+      if (f.type == kFarfield && d.species != 0) {
+        err = "far-field faces (label " + std::to_string(f.label) +
+              ") are implemented for air; mixtures use symmetry, outflow or periodic faces";
         return false;
       }
       if (f.type == kFarfield) {

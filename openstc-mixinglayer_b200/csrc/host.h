@@ -9,6 +9,8 @@
 #include <variant>
 #include <vector>
 
+#include "chem.h"
+
 namespace ostc {
 
 // Physical constants (Constants.h:18,26,31-35 of the reference).
@@ -67,6 +69,7 @@ struct Derived {
   double dt = 1e-8;
   double grid_scale = 1.0;
   int species = 0;
+  int reaction = 0;
 };
 
 bool derive(const Setup &s, Derived &d, std::string &err);
@@ -126,6 +129,9 @@ bool read_mesh(const std::string &input_dir, const Derived &d, HostMesh &mesh, s
 // Attaches types and far-field states to the faces from the setup's boundary structs
 // (DBoundCond::initialize_bc_on_GPU, BoundCond.cu:162-258).
 bool resolve_boundaries(const Setup &s, const Derived &d, HostMesh &mesh, std::string &err);
+// rho_inf^2 v_inf^2 and v_inf of the struct named by reference_state (0, 0 without one): the scales of
+// the flux-split WENO epsilon (DParameter.cu:26-29, WENO.cu:1466-1473).
+bool reference_scales(const Setup &s, const ChemTables *chem, double &eps_scale, double &v_ref, std::string &err);
 // Order in which faces are applied each stage (BoundCond.cuh:1488-1679): a list of (block, face).
 std::vector<std::pair<int, int>> bc_order(const Setup &s, const HostMesh &mesh);
 

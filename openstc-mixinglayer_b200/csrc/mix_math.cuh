@@ -1,0 +1,298 @@
+// mix_math.cuh -- device arithmetic of the multi-component (species = 1) path: NASA-7 thermodynamics,
+// mixture transport, the temperature Newton iteration, finite-rate chemistry and the flux-split
+// characteristic WENO7-Z face flux.  The species and reaction tables sit in constant memory: every
+// thread of a warp reads the same coefficient at the same time, which the constant cache broadcasts.
+#pragma once
+
+#include "air_math.cuh"
+
+namespace ostc {
+
+constexpr int kMS = 16;  // species capacity of the device tables
+constexpr int kMR = 64;  // reaction capacity
+constexpr int kMV = 5 + kMS;
+constexpr double kPatmD = 101325.0;
+
+struct MixTables {
+  int ns, nr;
+  int use_gibbs;  // some reaction takes kb from the equilibrium constant (backward_reaction_rate's n_gibbs)
+  double weno_eps_scale, v_ref;
+  double mw[kMS], imw[kMS], ru_mw[kMS], t_low[kMS], t_mid[kMS];
+  double low[kMS][7], high[kMS][7];
+  double lj_potent_inv[kMS], vis_coeff[kMS];
+  double wj_div_wi_1_4[kMS][kMS], sqrt_wiwj_8[kMS][kMS], binary_diff[kMS][kMS], kb_over_eps[kMS][kMS];
+  int label[kMR], rev_type[kMR], order[kMR];
+  signed char stoi_f[kMR][kMS], stoi_b[kMR][kMS];
+  double A[kMR], b[kMR], Ea[kMR], A2[kMR], b2[kMR], Ea2[kMR], third_body[kMR][kMS];
+  double troe_alpha[kMR], troe_t3[kMR], troe_t1[kMR], troe_t2[kMR];
+};
+
+// the tables of the bound context (one translation unit includes this header)
+__constant__ MixTables c_mix;
+
+// compute_enthalpy_and_cp (Thermo.cu:136-192): h_k and cp_k in J/kg, linear h extrapolation below
+// t_low.  Either output may be null (compute_enthalpy / compute_cp).
+__device__ __forceinline__ void mix_h_cp(double t, double *h, double *cp) {
+  const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t5 = t4 * t;
+  for (int i = 0; i < c_mix.ns; ++i) {
+    double hh, cc;
+    if (t < c_mix.t_low[i]) {
+      const double tt = c_mix.t_low[i], tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tt5 = tt4 * tt;
+      const double *a = c_mix.low[i];
+      hh = a[0] * tt + 0.5 * a[1] * tt2 + a[2] * tt3 / 3 + 0.25 * a[3] * tt4 + 0.2 * a[4] * tt5 + a[5];
+      cc = a[0] + a[1] * tt + a[2] * tt2 + a[3] * tt3 + a[4] * tt4;
+      hh += cc * (t - tt);
+    } else {
+      const double *a = t < c_mix.t_mid[i] ? c_mix.low[i] : c_mix.high[i];
+      hh = a[0] * t + 0.5 * a[1] * t2 + a[2] * t3 / 3 + 0.25 * a[3] * t4 + 0.2 * a[4] * t5 + a[5];
+      cc = a[0] + a[1] * t + a[2] * t2 + a[3] * t3 + a[4] * t4;
+    }
+    if (h) h[i] = hh * c_mix.ru_mw[i];
+    if (cp) cp[i] = cc * c_mix.ru_mw[i];
+  }
+}
+
+// compute_gibbs_div_rt (Thermo.cu:194-210)
+__device__ __forceinline__ void mix_gibbs_rt(double t, double *g) {
+  const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, ti = 1 / t, lt = log(t);
+  for (int i = 0; i < c_mix.ns; ++i) {
+    if (t < c_mix.t_low[i]) {
+      const double tt = c_mix.t_low[i], tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tti = 1 / tt, ltt = log(tt);
+      const double *a = c_mix.low[i];
+      g[i] = a[0] * (1.0 - ltt) - 0.5 * a[1] * tt - a[2] * tt2 / 6.0 - a[3] * tt3 / 12.0 - a[4] * tt4 * 0.05 +
+             a[5] * tti - a[6];
+    } else {
+      const double *a = t < c_mix.t_mid[i] ? c_mix.low[i] : c_mix.high[i];
+      g[i] = a[0] * (1.0 - lt) - 0.5 * a[1] * t - a[2] * t2 / 6.0 - a[3] * t3 / 12.0 - a[4] * t4 * 0.05 + a[5] * ti -
+             a[6];
+    }
+  }
+}
+
+// Node properties of update_physical_properties<mixture> (FieldOperation.cuh:116-134) with
+// compute_transport_property (Transport.cu:43-136): cp, gamma, acoustic speed, Wilke viscosity,
+// Eucken-type conductivity and mixture-averaged rho*D_k (outputs written through the pointers).
+__device__ __forceinline__ void mix_properties(double rho, double p, double t, const double *y, double &gamma,
+                                               double &acoustic, double &mu, double &cond, double *rhod) {
+  const int ns = c_mix.ns;
+  double cp[kMS];
+  mix_h_cp(t, nullptr, cp);
+  double mw = 0, cpt = 0, cvt = 0;
+  for (int l = 0; l < ns; ++l) {
+    mw += y[l] * c_mix.imw[l];
+    cpt += y[l] * cp[l];
+    cvt += y[l] * (cp[l] - c_mix.ru_mw[l]);
+  }
+  mw = 1 / mw;
+  gamma = cpt / cvt;
+  acoustic = sqrt(gamma * kRuD * t / mw);
+  double X[kMS], vis[kMS];
+  const double st = sqrt(t);
+  for (int l = 0; l < ns; ++l) {
+    X[l] = y[l] * mw * c_mix.imw[l];
+    const double tdl = t * c_mix.lj_potent_inv[l];
+    const double ci = 1.147 * pow(tdl, -0.145) + pow(tdl + 0.5, -2);
+    vis[l] = c_mix.vis_coeff[l] * st / ci;
+  }
+  double visc = 0, cd = 0;
+  for (int m = 0; m < ns; ++m) {
+    double vt = 0;
+    for (int n = 0; n < ns; ++n) {
+      double pf = 1.0;
+      if (m != n) {
+        const double num = 1 + sqrt(vis[m] / vis[n]) * c_mix.wj_div_wi_1_4[m][n];
+        pf = num * num * c_mix.sqrt_wiwj_8[m][n];
+      }
+      vt += pf * X[n];
+    }
+    const double ct = 1.065 * vt - 0.065 * X[m];
+    visc += vis[m] * X[m] / vt;
+    const double lam = vis[m] * (cp[m] + 1.25 * c_mix.ru_mw[m]);
+    cd += lam * X[m] / ct;
+  }
+  mu = visc;
+  cond = cd;
+  // mixture-averaged diffusion with the binary coefficients D_ln = coeff T^1.5 / (p Omega_D(T*))
+  const double t32p = t * st / p;
+  const double eps = 1e-12;
+  for (int l = 0; l < ns; ++l) {
+    double num = 0, den = 0;
+    for (int n = 0; n < ns; ++n) {
+      if (l == n) continue;
+      const double tr = t * c_mix.kb_over_eps[l][n];
+      const double om = 1.0 / pow(tr, 0.145) + 1.0 / ((tr + 0.5) * (tr + 0.5));
+      const double dln = c_mix.binary_diff[l][n] * t32p / om;
+      num += (X[n] + eps) * c_mix.mw[n];
+      den += (X[n] + eps) / dln;
+    }
+    rhod[l] = rho * num / (den * mw);
+  }
+}
+
+// compute_temperature_and_pressure (FieldOperation.cu:3-40): Newton on e(T) starting from t, relative
+// tolerance 1e-3, at most 1000 iterations.  Returns T; p = rho R T through pout.
+__device__ __forceinline__ double mix_temperature(double rho, double e, double t, const double *y, double &pout) {
+  const int ns = c_mix.ns;
+  double mw = 0;
+  for (int l = 0; l < ns; ++l) mw += y[l] * c_mix.imw[l];
+  mw = 1 / mw;
+  const double gc = kRuD / mw;
+  double err = 1;
+  int iter = 0;
+  double h[kMS], cp[kMS];
+  while (err > 1e-3 && iter++ < 1000) {
+    mix_h_cp(t, h, cp);
+    double cpt = 0, hm = 0;
+    for (int l = 0; l < ns; ++l) {
+      cpt += cp[l] * y[l];
+      hm += h[l] * y[l];
+    }
+    const double t1 = t - (hm - gc * t - e) / (cpt - gc);
+    err = fabs(1 - t1 / t);
+    t = t1;
+  }
+  pout = rho * t * gc;
+  return t;
+}
+
+__device__ __forceinline__ double arrhenius(double t, double A, double b, double Ea) {
+  return A * pow(t, b) * exp(-Ea / t);
+}
+
+// finite_rate_chemistry (FiniteRateChem.cu:7-58, rates :60-195): omega_k in kg/(m^3 s) at one node.
+__device__ __forceinline__ void mix_chemistry(double rho, double t, const double *y, double *omega) {
+  const int ns = c_mix.ns, nr = c_mix.nr;
+  double c[kMS];
+  for (int l = 0; l < ns; ++l) c[l] = rho * y[l] * c_mix.imw[l] * 1e-3;
+  double g[kMS];
+  bool gibbs = false;
+  for (int l = 0; l < ns; ++l) omega[l] = 0;
+  double cre[kMS], des[kMS];
+  for (int l = 0; l < ns; ++l) cre[l] = des[l] = 0;
+  for (int r = 0; r < nr; ++r) {
+    const int ty = c_mix.label[r];
+    double cc = 0;
+    if (ty >= 4)
+      for (int l = 0; l < ns; ++l) cc += c[l] * c_mix.third_body[r][l];
+    double kf = arrhenius(t, c_mix.A[r], c_mix.b[r], c_mix.Ea[r]);
+    if (ty == 3) {
+      kf += arrhenius(t, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
+    } else if (ty == 4) {
+      kf *= cc;
+    } else if (ty > 4) {
+      const double klow = arrhenius(t, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
+      const double pr = klow * cc / kf;
+      double F = 1.0;
+      if (ty > 5) {
+        double fc = (1 - c_mix.troe_alpha[r]) * exp(-t / c_mix.troe_t3[r]) +
+                    c_mix.troe_alpha[r] * exp(-t / c_mix.troe_t1[r]);
+        if (ty == 7) fc += exp(-c_mix.troe_t2[r] / t);
+        const double lfc = log10(fc);
+        const double cq = -0.4 - 0.67 * lfc, nq = 0.75 - 1.27 * lfc;
+        const double lpr = log10(pr);
+        const double tmp = (lpr + cq) / (nq - 0.14 * (lpr + cq));
+        F = pow(10.0, lfc / (1.0 + tmp * tmp));
+      }
+      kf = kf * pr / (1.0 + pr) * F;
+    }
+    // backward_reaction_rate (FiniteRateChem.cu:108-150): irreversible 0; the equilibrium constant
+    // for every other type but 2 when any reaction needs it (it also overwrites REV coefficients);
+    // else the REV Arrhenius coefficients (times the third-body sum for type 4)
+    double kb = 0;
+    if (ty == 0) {
+      kb = 0;
+    } else if (ty != 2 && c_mix.use_gibbs) {
+      if (!gibbs) {
+        mix_gibbs_rt(t, g);
+        gibbs = true;
+      }
+      double dg = 0;
+      for (int l = 0; l < ns; ++l) dg += g[l] * (c_mix.stoi_b[r][l] - c_mix.stoi_f[r][l]);
+      const double temp_t = kPatmD / kRuD * 1e-3 / t;
+      const double kc = pow(temp_t, (double)c_mix.order[r]) * exp(-dg);
+      kb = kf / kc;
+    } else if (c_mix.rev_type[r] == 1) {
+      kb = arrhenius(t, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
+      if (ty == 4) kb *= cc;
+    }
+    double q1 = 1.0, q2 = ty != 0 ? 1.0 : 0.0;
+    for (int l = 0; l < ns; ++l) {
+      if (c_mix.stoi_f[r][l]) q1 *= pow(c[l], (double)c_mix.stoi_f[r][l]);
+    }
+    if (ty != 0)
+      for (int l = 0; l < ns; ++l)
+        if (c_mix.stoi_b[r][l]) q2 *= pow(c[l], (double)c_mix.stoi_b[r][l]);
+    q1 *= kf;
+    if (ty != 0) q2 *= kb;
+    for (int l = 0; l < ns; ++l) {
+      cre[l] += q2 * c_mix.stoi_f[r][l] + q1 * c_mix.stoi_b[r][l];
+      des[l] += q1 * c_mix.stoi_f[r][l] + q2 * c_mix.stoi_b[r][l];
+    }
+  }
+  for (int l = 0; l < ns; ++l) omega[l] = cre[l] * (c_mix.mw[l] * 1e+3) - des[l] * (c_mix.mw[l] * 1e+3);
+}
+
+// ---------------------------------------------------------------- flux-split WENO7 (71 / 72)
+
+__device__ __forceinline__ double fvs_beta7(double s1, double s2, double s3) {
+  return s1 * s1 + 13.0 / 12.0 * s2 * s2 + 1043.0 / 960 * s3 * s3 + 1.0 / 12 * s1 * s3;
+}
+
+// WENO7 of the flux-split path (WENO.cu:1619-1693): returns f+ + f-.
+__device__ __forceinline__ double fvs_weno7(const double *vp, const double *vm, double eps) {
+  const double one6th = 1.0 / 6, one12th = 1.0 / 12;
+  const double c0 = 1.0 / 35, c1 = 12.0 / 35, c2 = 18.0 / 35, c3 = 4.0 / 35;
+  double s1 = one6th * (-2 * vp[0] + 9 * vp[1] - 18 * vp[2] + 11 * vp[3]);
+  double s2 = -vp[0] + 4 * vp[1] - 5 * vp[2] + 2 * vp[3];
+  double s3 = -vp[0] + 3 * vp[1] - 3 * vp[2] + vp[3];
+  double b0 = fvs_beta7(s1, s2, s3);
+  s1 = one6th * (vp[1] - 6 * vp[2] + 3 * vp[3] + 2 * vp[4]);
+  s2 = vp[2] - 2 * vp[3] + vp[4];
+  s3 = -vp[1] + 3 * vp[2] - 3 * vp[3] + vp[4];
+  double b1 = fvs_beta7(s1, s2, s3);
+  s1 = one6th * (-2 * vp[2] - 3 * vp[3] + 6 * vp[4] - vp[5]);
+  s3 = -vp[2] + 3 * vp[3] - 3 * vp[4] + vp[5];
+  double b2 = fvs_beta7(s1, s2, s3);
+  s1 = one6th * (-11 * vp[3] + 18 * vp[4] - 9 * vp[5] + 2 * vp[6]);
+  s2 = 2 * vp[3] - 5 * vp[4] + 4 * vp[5] - vp[6];
+  s3 = -vp[3] + 3 * vp[4] - 3 * vp[5] + vp[6];
+  double b3 = fvs_beta7(s1, s2, s3);
+  double tau = (b0 - b3) * (b0 - b3);
+  double a0 = c0 + c0 * tau / ((eps + b0) * (eps + b0));
+  double a1 = c1 + c1 * tau / ((eps + b1) * (eps + b1));
+  double a2 = c2 + c2 * tau / ((eps + b2) * (eps + b2));
+  double a3 = c3 + c3 * tau / ((eps + b3) * (eps + b3));
+  double v0 = one12th * (-3 * vp[0] + 13 * vp[1] - 23 * vp[2] + 25 * vp[3]);
+  double v1 = one12th * (vp[1] - 5 * vp[2] + 13 * vp[3] + 3 * vp[4]);
+  double v2 = one12th * (-vp[2] + 7 * vp[3] + 7 * vp[4] - vp[5]);
+  double v3 = one12th * (3 * vp[3] + 13 * vp[4] - 5 * vp[5] + vp[6]);
+  const double fp = (a0 * v0 + a1 * v1 + a2 * v2 + a3 * v3) / (a0 + a1 + a2 + a3);
+  s1 = one6th * (-2 * vm[6] + 9 * vm[5] - 18 * vm[4] + 11 * vm[3]);
+  s2 = -vm[6] + 4 * vm[5] - 5 * vm[4] + 2 * vm[3];
+  s3 = -vm[6] + 3 * vm[5] - 3 * vm[4] + vm[3];
+  b0 = fvs_beta7(s1, s2, s3);
+  s1 = one6th * (vm[5] - 6 * vm[4] + 3 * vm[3] + 2 * vm[2]);
+  s2 = vm[4] - 2 * vm[3] + vm[2];
+  s3 = -vm[5] + 3 * vm[4] - 3 * vm[3] + vm[2];
+  b1 = fvs_beta7(s1, s2, s3);
+  s1 = one6th * (-2 * vm[4] - 3 * vm[3] + 6 * vm[2] - vm[1]);
+  s3 = -vm[4] + 3 * vm[3] - 3 * vm[2] + vm[1];
+  b2 = fvs_beta7(s1, s2, s3);
+  s1 = one6th * (-11 * vm[3] + 18 * vm[2] - 9 * vm[1] + 2 * vm[0]);
+  s2 = 2 * vm[3] - 5 * vm[2] + 4 * vm[1] - vm[0];
+  s3 = -vm[3] + 3 * vm[2] - 3 * vm[1] + vm[0];
+  b3 = fvs_beta7(s1, s2, s3);
+  tau = (b0 - b3) * (b0 - b3);
+  a0 = c0 + c0 * tau / ((eps + b0) * (eps + b0));
+  a1 = c1 + c1 * tau / ((eps + b1) * (eps + b1));
+  a2 = c2 + c2 * tau / ((eps + b2) * (eps + b2));
+  a3 = c3 + c3 * tau / ((eps + b3) * (eps + b3));
+  v0 = one12th * (-3 * vm[6] + 13 * vm[5] - 23 * vm[4] + 25 * vm[3]);
+  v1 = one12th * (vm[5] - 5 * vm[4] + 13 * vm[3] + 3 * vm[2]);
+  v2 = one12th * (-vm[4] + 7 * vm[3] + 7 * vm[2] - vm[1]);
+  v3 = one12th * (3 * vm[3] + 13 * vm[2] - 5 * vm[1] + vm[0]);
+  const double fm = (a0 * v0 + a1 * v1 + a2 * v2 + a3 * v3) / (a0 + a1 + a2 + a3);
+  return fp + fm;
+}
+
+}  // namespace ostc

@@ -43,6 +43,8 @@ struct DevBlock {
 
 struct DevState {
   double *cv, *bv, *mul;
+  // mixtures (null on the air path): mass fractions, conductivity, rho*D_k, gamma, acoustic speed
+  double *sv = nullptr, *cond = nullptr, *rhod = nullptr, *gam = nullptr, *acs = nullptr;
 };
 
 struct DevFace {
@@ -64,6 +66,12 @@ __device__ __forceinline__ void cv_from_bv_node(const DevBlock &b, DevState s, l
   te += s.bv[4 * P + p] / (kGamma - 1);
   s.cv[4 * P + p] = te;
 }
+
+}  // namespace ostc
+
+#include "ostc_mix.cuh"
+
+namespace ostc {
 
 // ------------------------------------------------------------------------------ time step
 
@@ -91,11 +99,11 @@ __global__ void __launch_bounds__(256) k_cfl_dt(DevBlock b, DevState s, double c
     const double U = u * m[0] + v * m[1] + w * m[2];
     const double V = u * m[3] + v * m[4] + w * m[5];
     const double W = u * m[6] + v * m[7] + w * m[8];
-    const double a = sqrt(kGamma * kRuD * s.bv[5 * P + p] / kMwD);
+    const double a = s.acs ? s.acs[p] : sqrt(kGamma * kRuD * s.bv[5 * P + p] / kMwD);
     const double s0 = fabs(U) + a * gx, s1 = fabs(V) + a * ge;
     const double s2 = dim3 ? fabs(W) + a * gz : 0.0;
     const double sinv = s0 + s1 + s2;
-    const double c1 = fmax(kGamma, 4.0 / 3.0) / s.bv[p];
+    const double c1 = fmax(s.gam ? s.gam[p] : kGamma, 4.0 / 3.0) / s.bv[p];
     const double c2 = s.mul[p] / prandtl;
     double sv = gx * gx + ge * ge;
     if (dim3) sv += gz * gz;
@@ -731,9 +739,16 @@ __global__ void __launch_bounds__(TX *TY, 3) k_visc_update(DevBlock b, StageArgs
 __device__ __forceinline__ void copy_bv(const DevBlock &b, DevState s, long long dst, long long src) {
 #pragma unroll
   for (int l = 0; l < 6; ++l) s.bv[l * b.plane + dst] = s.bv[l * b.plane + src];
+  if (s.sv)
+    for (int l = 0; l < c_mix.ns; ++l) s.sv[l * b.plane + dst] = s.sv[l * b.plane + src];
 }
 
 __device__ __forceinline__ void finish_node(const DevBlock &b, DevState s, long long p) {
+  if (s.sv) {
+    // mixtures: properties of the ghost come from the properties sweep over the padded block
+    mix_cv_from_bv_node(b, s, p);
+    return;
+  }
   cv_from_bv_node(b, s, p);
   s.mul[p] = sutherland(s.bv[5 * b.plane + p]);
 }
@@ -773,7 +788,11 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
       s.bv[pb] = s.bv[pin];
       s.bv[4 * P + pb] = s.bv[4 * P + pin];
       s.bv[5 * P + pb] = s.bv[5 * P + pin];
-      s.mul[pb] = sutherland(s.bv[5 * P + pb]);
+      if (s.sv) {
+        for (int l = 0; l < c_mix.ns; ++l) s.sv[l * P + pb] = s.sv[l * P + pin];
+      } else {
+        s.mul[pb] = sutherland(s.bv[5 * P + pb]);
+      }
       for (int g = 1; g <= b.g; ++g) {
         const long long pg = pb + g * dstep, pi = pb - g * dstep;
         s.bv[pg] = s.bv[pi];
@@ -784,6 +803,8 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
         s.bv[3 * P + pg] = w - 2 * uk * kz;
         s.bv[4 * P + pg] = s.bv[4 * P + pi];
         s.bv[5 * P + pg] = s.bv[5 * P + pi];
+        if (s.sv)
+          for (int l = 0; l < c_mix.ns; ++l) s.sv[l * P + pg] = s.sv[l * P + pi];
         finish_node(b, s, pg);
       }
     } else if (f.type == kOutflow) {
@@ -961,6 +982,7 @@ struct BlockRes {
   DevBlock db{};
   double *met = nullptr, *jac = nullptr;
   double *cv[3]{}, *bv[3]{}, *mul[3]{};
+  double *sv[3]{}, *cond[3]{}, *rhod[3]{}, *gam[3]{}, *acs[3]{};  // mixtures only
   double *dq = nullptr;
   double *last = nullptr;
   std::vector<DevFace> faces;  // file order
@@ -968,6 +990,12 @@ struct BlockRes {
 
 struct ostc_ctx {
   int device = 0;
+  // multi-component mixture (species = 1): tables, device copy in constant memory, n_var = 5 + n_spec
+  bool mixture = false;
+  bool tables = false;  // constant tables in use (mixtures, or the flux-split path's epsilon scales)
+  int nv = 5;
+  ChemTables chem;
+  MixTables mixtab{};
   cudaStream_t stream = nullptr;
   Setup setup;
   Derived der;
@@ -999,6 +1027,17 @@ struct ostc_ctx {
 };
 
 static std::string g_create_error;
+
+// The constant-memory tables belong to one context at a time; a context (re)binds them before its
+// first launch, outside any stream capture.
+static const ostc_ctx *g_mix_owner = nullptr;
+static int bind_tables(ostc_ctx *ctx) {
+  if (!ctx->tables || g_mix_owner == ctx) return 0;
+  if (g_mix_owner && cudaDeviceSynchronize() != cudaSuccess) return -1;  // the previous owner's work
+  if (cudaMemcpyToSymbol(c_mix, &ctx->mixtab, sizeof(MixTables)) != cudaSuccess) return -1;
+  g_mix_owner = ctx;
+  return 0;
+}
 
 namespace ostc {
 // Error text of the context-free entry points (ostc_create failures, ostc_residual_noalloc),
@@ -1088,9 +1127,67 @@ void launch_flux_pv(ostc_ctx *ctx, BlockRes &B, DevState in) {
   }
 }
 
+// flux-split WENO7 sweeps (inviscid_type 3, schemes 71 / 72), accumulating into dq
+void launch_fvs(ostc_ctx *ctx, BlockRes &B, DevState in) {
+  const DevBlock &b = B.db;
+  const int nv = ctx->nv, sch = ctx->der.inviscid_scheme;
+  {
+    long tok = begin_t(ctx, "flux_x");
+    dim3 grid((b.mx + FvsTile<0>::TD - 2) / (FvsTile<0>::TD - 1), b.my, b.mz);
+    k_fvs<0><<<grid, FvsTile<0>::TD, fvs_smem_bytes<0>(nv), ctx->stream>>>(b, in, B.dq, nv, sch);
+    end_t(ctx, tok);
+  }
+  {
+    long tok = begin_t(ctx, "flux_y");
+    dim3 grid((b.mx + FvsTile<1>::TXL - 1) / FvsTile<1>::TXL, (b.my + FvsTile<1>::TD - 2) / (FvsTile<1>::TD - 1), b.mz);
+    k_fvs<1><<<grid, dim3(FvsTile<1>::TXL, FvsTile<1>::TD), fvs_smem_bytes<1>(nv), ctx->stream>>>(b, in, B.dq, nv, sch);
+    end_t(ctx, tok);
+  }
+  if (b.mz > 1) {
+    long tok = begin_t(ctx, "flux_z");
+    dim3 grid((b.mx + FvsTile<2>::TXL - 1) / FvsTile<2>::TXL, (b.mz + FvsTile<2>::TD - 2) / (FvsTile<2>::TD - 1), b.my);
+    k_fvs<2><<<grid, dim3(FvsTile<2>::TXL, FvsTile<2>::TD), fvs_smem_bytes<2>(nv), ctx->stream>>>(b, in, B.dq, nv, sch);
+    end_t(ctx, tok);
+  }
+}
+
+// mixture viscous sweeps, accumulating into dq
+void launch_mix_visc(ostc_ctx *ctx, BlockRes &B, DevState in) {
+  const DevBlock &b = B.db;
+  const int nv = ctx->nv;
+  const bool is3d = b.mz > 1;
+  long tok = begin_t(ctx, "visc");
+  {
+    dim3 grid((b.mx + FvsTile<0>::TD - 2) / (FvsTile<0>::TD - 1), b.my, b.mz);
+    const size_t sm = (size_t)FvsTile<0>::TD * nv * sizeof(double);
+    if (is3d) k_mix_visc<0, true><<<grid, FvsTile<0>::TD, sm, ctx->stream>>>(b, in, B.dq, nv);
+    else k_mix_visc<0, false><<<grid, FvsTile<0>::TD, sm, ctx->stream>>>(b, in, B.dq, nv);
+  }
+  {
+    dim3 grid((b.mx + FvsTile<1>::TXL - 1) / FvsTile<1>::TXL, (b.my + FvsTile<1>::TD - 2) / (FvsTile<1>::TD - 1), b.mz);
+    const size_t sm = (size_t)FvsTile<1>::TD * FvsTile<1>::TXL * nv * sizeof(double);
+    dim3 blk(FvsTile<1>::TXL, FvsTile<1>::TD);
+    if (is3d) k_mix_visc<1, true><<<grid, blk, sm, ctx->stream>>>(b, in, B.dq, nv);
+    else k_mix_visc<1, false><<<grid, blk, sm, ctx->stream>>>(b, in, B.dq, nv);
+  }
+  if (is3d) {
+    dim3 grid((b.mx + FvsTile<2>::TXL - 1) / FvsTile<2>::TXL, (b.mz + FvsTile<2>::TD - 2) / (FvsTile<2>::TD - 1), b.my);
+    const size_t sm = (size_t)FvsTile<2>::TD * FvsTile<2>::TXL * nv * sizeof(double);
+    k_mix_visc<2, true><<<grid, dim3(FvsTile<2>::TXL, FvsTile<2>::TD), sm, ctx->stream>>>(b, in, B.dq, nv);
+  }
+  end_t(ctx, tok);
+}
+
 // inviscid sweep of one block
 template <typename T>
 int launch_flux(ostc_ctx *ctx, BlockRes &B, DevState in) {
+  if (ctx->der.inviscid_type == 3) {
+    // the flux-split sweeps accumulate: the air path starts dq from zero here (mixtures start it with
+    // the chemical source)
+    if (!ctx->mixture) cudaMemsetAsync(B.dq, 0, (size_t)ctx->nv * B.db.n * sizeof(double), ctx->stream);
+    launch_fvs(ctx, B, in);
+    return OSTC_OK;
+  }
   if (ctx->der.inviscid_type != 1) {
     launch_flux_pv<T>(ctx, B, in);
     return OSTC_OK;
@@ -1185,7 +1282,15 @@ void launch_bcs(ostc_ctx *ctx, int block, DevState out) {
   }
 }
 
-DevState state_of(BlockRes &B, int s) { return DevState{B.cv[s], B.bv[s], B.mul[s]}; }
+DevState state_of(BlockRes &B, int s) {
+  DevState d{B.cv[s], B.bv[s], B.mul[s]};
+  d.sv = B.sv[s];
+  d.cond = B.cond[s];
+  d.rhod = B.rhod[s];
+  d.gam = B.gam[s];
+  d.acs = B.acs[s];
+  return d;
+}
 
 // The march kernels stage 2*ngg+1 nodes x 11 values x 64 threads (plus the FP32 prefetch buffers)
 // in dynamic shared memory (up to 51 KB); raise the per-kernel limit once, outside any stream capture.
@@ -1215,11 +1320,29 @@ bool set_march_attrs() {
   return ok;
 }
 
+// dynamic shared memory of the flux-split and mixture viscous sweeps (up to ~45 KB at n_var 14)
+bool set_mix_attrs(int nv) {
+  bool ok = true;
+  auto set = [&](const void *fn, size_t bytes) {
+    ok = ok && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess;
+  };
+  set((const void *)k_fvs<0>, fvs_smem_bytes<0>(nv));
+  set((const void *)k_fvs<1>, fvs_smem_bytes<1>(nv));
+  set((const void *)k_fvs<2>, fvs_smem_bytes<2>(nv));
+  return ok;
+}
+
 int initialise(ostc_ctx *ctx) {
   // Driver::initialize_computation (Driver.cu:115-199): BCs, properties, then cv <- bv (RK.cuh:37-45)
   for (size_t b = 0; b < ctx->blk.size(); ++b) launch_bcs(ctx, (int)b, state_of(ctx->blk[b], 0));
-  for (auto &B : ctx->blk)
-    k_init_fields<<<grid_for(ctx, B.db.plane, 256), 256, 0, ctx->stream>>>(B.db, state_of(B, 0));
+  for (auto &B : ctx->blk) {
+    if (ctx->mixture) {
+      k_mix_props<<<grid_for(ctx, B.db.plane, 128), 128, 0, ctx->stream>>>(B.db, state_of(B, 0));
+      k_mix_init_cv<<<grid_for(ctx, B.db.plane, 128), 128, 0, ctx->stream>>>(B.db, state_of(B, 0));
+    } else {
+      k_init_fields<<<grid_for(ctx, B.db.plane, 256), 256, 0, ctx->stream>>>(B.db, state_of(B, 0));
+    }
+  }
   CK(cudaGetLastError());
   ctx->initialised = true;
   return OSTC_OK;
@@ -1264,7 +1387,54 @@ int enqueue_step(ostc_ctx *ctx) {
   return OSTC_OK;
 }
 
+// One SSP-RK3 step of a mixture (RK.cuh:85-185 with MixtureModel Mixture / FR): source, flux-split
+// WENO7, viscous, update + temperature Newton, boundary faces, properties.
+int enqueue_step_mix(ostc_ctx *ctx) {
+  static const double A[3] = {1.0, 0.75, 1.0 / 3.0}, Bc[3] = {0.0, 0.25, 2.0 / 3.0}, C[3] = {1.0, 0.25, 2.0 / 3.0};
+  const bool fixed = ctx->der.fixed_time_step;
+  const int nv = ctx->nv;
+  for (int rk = 0; rk < 3; ++rk) {
+    const int sin = rk, sout = (rk + 1) % 3;
+    if (rk == 0 && !fixed) {
+      long tok = begin_t(ctx, "cfl_dt");
+      k_dt_reset<<<1, 1, 0, ctx->stream>>>(ctx->d_dtbits);
+      for (auto &B : ctx->blk)
+        k_cfl_dt<<<grid_for(ctx, B.db.n, 256), 256, 0, ctx->stream>>>(B.db, state_of(B, sin), ctx->der.cfl,
+                                                                     ctx->der.prandtl, B.db.mz > 1, ctx->d_dtbits);
+      k_dt_decode<<<1, 1, 0, ctx->stream>>>(ctx->d_dtbits, ctx->d_dt);
+      end_t(ctx, tok);
+    }
+    for (size_t bi = 0; bi < ctx->blk.size(); ++bi) {
+      BlockRes &B = ctx->blk[bi];
+      const DevState in = state_of(B, sin);
+      {
+        long tok = begin_t(ctx, "source");
+        k_mix_source<<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, in, B.dq, nv, ctx->der.reaction == 1);
+        end_t(ctx, tok);
+      }
+      launch_fvs(ctx, B, in);
+      if (ctx->der.viscous_order != 0) launch_mix_visc(ctx, B, in);
+      {
+        long tok = begin_t(ctx, "update");
+        k_mix_update<<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, in, state_of(B, 0), state_of(B, sout),
+                                                                          B.dq, ctx->d_dt, A[rk], Bc[rk], C[rk], nv,
+                                                                          ctx->d_flags);
+        end_t(ctx, tok);
+      }
+      launch_bcs(ctx, (int)bi, state_of(B, sout));
+      {
+        long tok = begin_t(ctx, "properties");
+        k_mix_props<<<grid_for(ctx, B.db.plane, 128), 128, 0, ctx->stream>>>(B.db, state_of(B, sout));
+        end_t(ctx, tok);
+      }
+    }
+  }
+  k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->d_time, ctx->d_dt, ctx->d_step);
+  return OSTC_OK;
+}
+
 int enqueue_step_any(ostc_ctx *ctx) {
+  if (ctx->mixture) return enqueue_step_mix(ctx);
   return ctx->precision == OSTC_PREC_MIXED ? enqueue_step<float>(ctx) : enqueue_step<double>(ctx);
 }
 
@@ -1278,6 +1448,10 @@ int check_ready(ostc_ctx *ctx) {
       ctx->err = "ostc_set_state was not called for every block";
       return OSTC_ESTATE;
     }
+  if (bind_tables(ctx) != 0) {
+    ctx->err = "upload of the species / reaction tables to constant memory failed";
+    return OSTC_ECUDA;
+  }
   if (!ctx->initialised) return initialise(ctx);
   return OSTC_OK;
 }
@@ -1307,6 +1481,80 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
                : OSTC_EINVAL;
   }
   ctx->order = bc_order(ctx->setup, ctx->mesh);
+  if (ctx->der.species == 1) {
+    auto str = [&](const char *k) {
+      auto it = ctx->setup.strings.find(k);
+      return it == ctx->setup.strings.end() ? std::string() : it->second;
+    };
+    if (!read_chemistry(dir, str("mechanism_file"), str("therm_file"), str("transport_file"), ctx->der.reaction == 1,
+                        ctx->chem, err)) {
+      g_create_error = err;
+      return err.find("cannot open") != std::string::npos ? OSTC_EIO : OSTC_EINVAL;
+    }
+    const ChemTables &c = ctx->chem;
+    MixTables &m = ctx->mixtab;
+    m.ns = c.n_spec;
+    m.nr = c.n_reac;
+    for (int i = 0; i < c.n_spec; ++i) {
+      m.mw[i] = c.mw[i];
+      m.imw[i] = 1.0 / c.mw[i];
+      m.ru_mw[i] = kRu / c.mw[i];
+      m.t_low[i] = c.t_low[i];
+      m.t_mid[i] = c.t_mid[i];
+      for (int q = 0; q < 7; ++q) {
+        m.low[i][q] = c.low[i * 7 + q];
+        m.high[i][q] = c.high[i * 7 + q];
+      }
+      m.lj_potent_inv[i] = c.lj_potent_inv[i];
+      m.vis_coeff[i] = c.vis_coeff[i];
+      for (int j = 0; j < c.n_spec; ++j) {
+        m.wj_div_wi_1_4[i][j] = c.wj_div_wi_1_4[i * c.n_spec + j];
+        m.sqrt_wiwj_8[i][j] = c.sqrt_wiwj_8[i * c.n_spec + j];
+        m.binary_diff[i][j] = c.binary_diff[i * c.n_spec + j];
+        m.kb_over_eps[i][j] = c.kb_over_eps_jk[i * c.n_spec + j];
+      }
+    }
+    m.use_gibbs = 0;
+    for (int r = 0; r < c.n_reac; ++r) {
+      m.label[r] = c.label[r];
+      m.rev_type[r] = c.rev_type[r];
+      m.order[r] = c.order[r];
+      if (c.label[r] != 0 && c.rev_type[r] != 1) m.use_gibbs = 1;
+      m.A[r] = c.A[r];
+      m.b[r] = c.b[r];
+      m.Ea[r] = c.Ea[r];
+      m.A2[r] = c.A2[r];
+      m.b2[r] = c.b2[r];
+      m.Ea2[r] = c.Ea2[r];
+      m.troe_alpha[r] = c.troe_alpha[r];
+      m.troe_t3[r] = c.troe_t3[r];
+      m.troe_t1[r] = c.troe_t1[r];
+      m.troe_t2[r] = c.troe_t2[r];
+      for (int i = 0; i < c.n_spec; ++i) {
+        m.stoi_f[r][i] = (signed char)c.stoi_f[r * c.n_spec + i];
+        m.stoi_b[r][i] = (signed char)c.stoi_b[r * c.n_spec + i];
+        m.third_body[r][i] = c.third_body[r * c.n_spec + i];
+      }
+    }
+    ctx->mixture = true;
+    ctx->nv = 5 + c.n_spec;
+    ctx->der.n_spec = c.n_spec;
+    ctx->der.n_scalar = c.n_spec;
+    ctx->der.n_var = ctx->nv;
+  }
+  if (ctx->der.inviscid_type == 3) {
+    if (!reference_scales(ctx->setup, ctx->mixture ? &ctx->chem : nullptr, ctx->mixtab.weno_eps_scale,
+                          ctx->mixtab.v_ref, err)) {
+      g_create_error = err;
+      return OSTC_EINVAL;
+    }
+    if (!ctx->mixture) {
+      // air on the flux-split path: the tables carry only the epsilon scales
+      ctx->mixtab.ns = 0;
+      ctx->mixtab.nr = 0;
+    }
+  }
+  ctx->tables = ctx->mixture || ctx->der.inviscid_type == 3;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
     g_create_error = "no CUDA device " + std::to_string(device) + " available";
@@ -1317,7 +1565,7 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
     return OSTC_ECUDA;
   }
   cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
-  if (!set_march_attrs<double>() || !set_march_attrs<float>()) {
+  if (!set_march_attrs<double>() || !set_march_attrs<float>() || !set_mix_attrs(ctx->nv)) {
     g_create_error = "cudaFuncSetAttribute (dynamic shared memory) failed";
     return OSTC_ECUDA;
   }
@@ -1346,8 +1594,15 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
       if (cudaMalloc(p, n * sizeof(double)) != cudaSuccess) return false;
       return cudaMemset(*p, 0, n * sizeof(double)) == cudaSuccess;
     };
-    bool ok = alloc(&R.met, 9 * b.plane) && alloc(&R.jac, b.plane) && alloc(&R.dq, 5 * b.n) && alloc(&R.last, 4 * b.n);
-    for (int s = 0; s < 3 && ok; ++s) ok = alloc(&R.cv[s], 5 * b.plane) && alloc(&R.bv[s], 6 * b.plane) && alloc(&R.mul[s], b.plane);
+    const int nv = ctx->nv, ns = ctx->der.n_spec;
+    bool ok = alloc(&R.met, 9 * b.plane) && alloc(&R.jac, b.plane) && alloc(&R.dq, (size_t)nv * b.n) &&
+              alloc(&R.last, 4 * b.n);
+    for (int s = 0; s < 3 && ok; ++s) {
+      ok = alloc(&R.cv[s], (size_t)nv * b.plane) && alloc(&R.bv[s], 6 * b.plane) && alloc(&R.mul[s], b.plane);
+      if (ok && ctx->mixture)
+        ok = alloc(&R.sv[s], (size_t)ns * b.plane) && alloc(&R.rhod[s], (size_t)ns * b.plane) &&
+             alloc(&R.cond[s], b.plane) && alloc(&R.gam[s], b.plane) && alloc(&R.acs[s], b.plane);
+    }
     if (!ok) {
       g_create_error = "device allocation failed";
       ctx->blk.push_back(R);
@@ -1401,7 +1656,7 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
             cudaMalloc(&ctx->d_sums, 4 * sizeof(double)) == cudaSuccess &&
             cudaMalloc(&ctx->d_step, sizeof(long long)) == cudaSuccess &&
             cudaMalloc(&ctx->d_flags, sizeof(unsigned)) == cudaSuccess &&
-            cudaMalloc(&ctx->d_staging, 6 * max_n * sizeof(double)) == cudaSuccess;
+            cudaMalloc(&ctx->d_staging, (size_t)std::max(6, ctx->nv) * max_n * sizeof(double)) == cudaSuccess;
   if (!ok) {
     g_create_error = "device allocation failed";
     ostc_destroy(ctx.release());
@@ -1423,6 +1678,7 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
 
 void ostc_destroy(ostc_ctx *ctx) {
   if (!ctx) return;
+  if (g_mix_owner == ctx) g_mix_owner = nullptr;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
@@ -1435,6 +1691,11 @@ void ostc_destroy(ostc_ctx *ctx) {
       cudaFree(B.cv[s]);
       cudaFree(B.bv[s]);
       cudaFree(B.mul[s]);
+      cudaFree(B.sv[s]);
+      cudaFree(B.cond[s]);
+      cudaFree(B.rhod[s]);
+      cudaFree(B.gam[s]);
+      cudaFree(B.acs[s]);
     }
   }
   cudaFree(ctx->d_dtbits);
@@ -1491,23 +1752,37 @@ int ostc_set_precision(ostc_ctx *ctx, int mode) {
     ctx->err = "unknown precision mode";
     return OSTC_EINVAL;
   }
+  if (mode == OSTC_PREC_MIXED && ctx->der.inviscid_type == 3) {
+    ctx->err = "the mixed-precision path covers the AWENO and primitive-reconstruction schemes; the flux-split "
+               "WENO7 path (inviscid_scheme 71/72, mixtures) runs in FP64";
+    return OSTC_EINVAL;
+  }
   ctx->precision = mode;
   return OSTC_OK;
 }
 
 int ostc_set_state(ostc_ctx *ctx, int block, const double *bv, const double *sv, int ptr_kind) {
   if (!ctx || !bv || block < 0 || block >= (int)ctx->blk.size()) return OSTC_EINVAL;
-  (void)sv;
+  if (ctx->mixture && !sv) {
+    ctx->err = "ostc_set_state: a mixture case needs the mass fractions sv[n_spec][N]";
+    return OSTC_EINVAL;
+  }
   cudaSetDevice(ctx->device);
   BlockRes &B = ctx->blk[block];
+  const auto kind = ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   const size_t bytes = 6 * (size_t)B.db.n * sizeof(double);
-  CK(cudaMemcpyAsync(ctx->d_staging, bv, bytes, ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                     ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_staging, bv, bytes, kind, ctx->stream));
   // buffer A holds the new state; every ghost node is rewritten by the boundary faces before use
   CK(cudaMemsetAsync(B.bv[0], 0, 6 * B.db.plane * sizeof(double), ctx->stream));
-  CK(cudaMemsetAsync(B.cv[0], 0, 5 * B.db.plane * sizeof(double), ctx->stream));
+  CK(cudaMemsetAsync(B.cv[0], 0, (size_t)ctx->nv * B.db.plane * sizeof(double), ctx->stream));
   CK(cudaMemsetAsync(B.mul[0], 0, B.db.plane * sizeof(double), ctx->stream));
   k_scatter<<<grid_for(ctx, 6 * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, ctx->d_staging, B.bv[0], 6);
+  if (ctx->mixture) {
+    const int ns = ctx->der.n_spec;
+    CK(cudaMemsetAsync(B.sv[0], 0, (size_t)ns * B.db.plane * sizeof(double), ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_staging, sv, (size_t)ns * B.db.n * sizeof(double), kind, ctx->stream));
+    k_scatter<<<grid_for(ctx, ns * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, ctx->d_staging, B.sv[0], ns);
+  }
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->block_set[block] = 1;
@@ -1519,14 +1794,20 @@ int ostc_set_state(ostc_ctx *ctx, int block, const double *bv, const double *sv,
 
 int ostc_get_state(ostc_ctx *ctx, int block, double *cv, double *bv, double *sv, int ptr_kind) {
   if (!ctx || block < 0 || block >= (int)ctx->blk.size()) return OSTC_EINVAL;
-  (void)sv;
   cudaSetDevice(ctx->device);
   if (int r = check_ready(ctx)) return r;
   BlockRes &B = ctx->blk[block];
   const auto kind = ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  const int nv = ctx->nv;
   if (cv) {
-    k_gather<<<grid_for(ctx, 5 * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, B.cv[0], ctx->d_staging, 5);
-    CK(cudaMemcpyAsync(cv, ctx->d_staging, 5 * B.db.n * sizeof(double), kind, ctx->stream));
+    k_gather<<<grid_for(ctx, nv * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, B.cv[0], ctx->d_staging, nv);
+    CK(cudaMemcpyAsync(cv, ctx->d_staging, (size_t)nv * B.db.n * sizeof(double), kind, ctx->stream));
+  }
+  if (sv && ctx->mixture) {
+    const int ns = ctx->der.n_spec;
+    CK(cudaStreamSynchronize(ctx->stream));
+    k_gather<<<grid_for(ctx, ns * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, B.sv[0], ctx->d_staging, ns);
+    CK(cudaMemcpyAsync(sv, ctx->d_staging, (size_t)ns * B.db.n * sizeof(double), kind, ctx->stream));
   }
   if (bv) {
     k_gather<<<grid_for(ctx, 6 * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, B.bv[0], ctx->d_staging, 6);
@@ -1542,7 +1823,21 @@ int ostc_rhs(ostc_ctx *ctx, int block, unsigned mask, double *dq, int ptr_kind) 
   cudaSetDevice(ctx->device);
   if (int r = check_ready(ctx)) return r;
   BlockRes &B = ctx->blk[block];
-  CK(cudaMemsetAsync(B.dq, 0, 5 * B.db.n * sizeof(double), ctx->stream));
+  const int nv = ctx->nv;
+  CK(cudaMemsetAsync(B.dq, 0, (size_t)nv * B.db.n * sizeof(double), ctx->stream));
+  if (ctx->mixture) {
+    // source (dq initialised by it, RK.cuh:116), flux-split WENO7, viscous
+    const DevState in = state_of(B, 0);
+    k_mix_source<<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, in, B.dq, nv,
+                                                                      (mask & OSTC_TERM_SOURCE) && ctx->der.reaction == 1);
+    if (mask & OSTC_TERM_INVISCID) launch_fvs(ctx, B, in);
+    if ((mask & OSTC_TERM_VISCOUS) && ctx->der.viscous_order != 0) launch_mix_visc(ctx, B, in);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dq, B.dq, (size_t)nv * B.db.n * sizeof(double),
+                       ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return OSTC_OK;
+  }
   const bool mixed = ctx->precision == OSTC_PREC_MIXED;
   if (mask & OSTC_TERM_INVISCID) {
     if (mixed) launch_flux<float>(ctx, B, state_of(B, 0));
@@ -1717,6 +2012,21 @@ int ostc_probe_case(const char *setup_txt, const char *input_dir, int out[16], c
   else if (!derive(setup, der, err)) rc = OSTC_EINVAL;
   else if (!read_mesh(dir, der, mesh, err)) rc = err.find("cannot open") != std::string::npos ? OSTC_EIO : OSTC_EINVAL;
   else if (!resolve_boundaries(setup, der, mesh, err)) rc = OSTC_EINVAL;
+  if (rc == OSTC_OK && der.species == 1) {
+    // the species count comes from the mechanism (Species ctor, ChemData.cpp:11-75)
+    ChemTables chem;
+    auto str = [&](const char *k) {
+      auto it = setup.strings.find(k);
+      return it == setup.strings.end() ? std::string() : it->second;
+    };
+    if (!read_chemistry(dir, str("mechanism_file"), str("therm_file"), str("transport_file"), der.reaction == 1, chem,
+                        err)) {
+      rc = err.find("cannot open") != std::string::npos ? OSTC_EIO : OSTC_EINVAL;
+    } else {
+      der.n_spec = der.n_scalar = chem.n_spec;
+      der.n_var = 5 + chem.n_spec;
+    }
+  }
   if (rc != OSTC_OK) {
     if (msg && msg_len > 0) {
       std::strncpy(msg, err.c_str(), (size_t)msg_len - 1);

@@ -1,0 +1,485 @@
+// ostc_mix.cuh -- kernels of the multi-component path (species = 1; included by ostc_air.cu after
+// DevBlock/DevState).  Per RK stage (RK.cuh:112-172): the chemical source initialises dq, the
+// flux-split WENO7 sweeps and the viscous sweeps accumulate into it, the update kernel combines the
+// stage and solves the temperature, the boundary faces fill the ghosts, and the properties kernel
+// recomputes gamma, c, mu, lambda and rho*D over the padded block.
+#pragma once
+
+#include "mix_math.cuh"
+
+namespace ostc {
+
+// compute_cv_from_bv_1_point<mixture> (FieldOperation.cuh:78-105, total energy :17-32)
+__device__ __forceinline__ void mix_cv_from_bv_node(const DevBlock &b, const DevState &s, long long p) {
+  const long long P = b.plane;
+  const int ns = c_mix.ns;
+  const double rho = s.bv[p], u = s.bv[P + p], v = s.bv[2 * P + p], w = s.bv[3 * P + p];
+  s.cv[p] = rho;
+  s.cv[P + p] = rho * u;
+  s.cv[2 * P + p] = rho * v;
+  s.cv[3 * P + p] = rho * w;
+  double h[kMS];
+  mix_h_cp(s.bv[5 * P + p], h, nullptr);
+  double te = 0.5 * (u * u + v * v + w * w);
+  for (int l = 0; l < ns; ++l) {
+    const double y = s.sv[l * P + p];
+    s.cv[(5 + l) * P + p] = rho * y;
+    te += h[l] * y;
+  }
+  te *= rho;
+  te -= s.bv[4 * P + p];
+  s.cv[4 * P + p] = te;
+}
+
+// update_physical_properties<mixture> over every padded node (FieldOperation.cuh:107-134)
+__global__ void __launch_bounds__(128) k_mix_props(DevBlock b, DevState s) {
+  const long long P = b.plane;
+  const int ns = c_mix.ns;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
+    const double rho = s.bv[p];
+    if (!(rho > 0)) continue;  // padding columns of the row pitch carry no state
+    double y[kMS], rd[kMS];
+    for (int l = 0; l < ns; ++l) y[l] = s.sv[l * P + p];
+    double g, a, mu, cd;
+    mix_properties(rho, s.bv[4 * P + p], s.bv[5 * P + p], y, g, a, mu, cd, rd);
+    s.gam[p] = g;
+    s.acs[p] = a;
+    s.mul[p] = mu;
+    s.cond[p] = cd;
+    for (int l = 0; l < ns; ++l) s.rhod[l * P + p] = rd[l];
+  }
+}
+
+// conservative variables from bv and sv over the padded block (initialisation, RK.cuh:37-45)
+__global__ void k_mix_init_cv(DevBlock b, DevState s) {
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < b.plane; p += (long long)gridDim.x * blockDim.x)
+    if (s.bv[p] > 0) mix_cv_from_bv_node(b, s, p);
+}
+
+// compute_source<FR> (SourceTerm.cuh:11-35) as the first contribution to dq: dq[5+l] = J omega_l
+// (finite rate) or 0, dq[0..4] = 0.
+__global__ void __launch_bounds__(128) k_mix_source(DevBlock b, DevState s, double *__restrict__ dq, int nv,
+                                                     int finite_rate) {
+  const long long P = b.plane;
+  const int ns = c_mix.ns;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % b.mx);
+    const long long r = n / b.mx;
+    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const long long p = b.id(i, j, k);
+    for (int l = 0; l < 5; ++l) dq[l * b.n + n] = 0.0;
+    if (finite_rate) {
+      double y[kMS], om[kMS];
+      for (int l = 0; l < ns; ++l) y[l] = s.sv[l * P + p];
+      mix_chemistry(s.bv[p], s.bv[5 * P + p], y, om);
+      const double jac = b.jac[p];
+      for (int l = 0; l < ns; ++l) dq[(5 + l) * b.n + n] = jac * om[l];
+    } else {
+      for (int l = 5; l < nv; ++l) dq[l * b.n + n] = 0.0;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ flux-split WENO7 sweeps
+
+// Tile geometry of the sweeps: TD faces along the sweep direction (TD-1 nodes finalised per tile),
+// and for the y / z sweeps TXL consecutive i per tile (coalesced rows).
+template <int DIR> struct FvsTile {
+  static constexpr int TXL = DIR == 0 ? 1 : 8;
+  static constexpr int TD = DIR == 0 ? 128 : 16;
+  static constexpr int NS = TD + 7;  // staged nodes: stencils of 8 nodes around TD faces
+};
+
+template <int DIR>
+__host__ __device__ constexpr size_t fvs_smem_bytes(int nv) {
+  return (size_t)FvsTile<DIR>::NS * FvsTile<DIR>::TXL * nv * 2 * sizeof(double);
+}
+
+// compute_convective_term_weno_x/_y/_z (WENO.cu:8-461) for inviscid_scheme 72 (characteristic,
+// compute_weno_flux_ch method 1, WENO.cu:722-758, 899-965, 1119-1142) or 71 (component-wise,
+// compute_weno_flux_cp, :1455-1536).  Every node's split fluxes F+- (compute_flux, :697-720) are
+// computed once into shared memory; each thread then forms one face flux from the 8-node stencil,
+// and after a barrier the node threads difference neighbouring faces into dq.
+template <int DIR>
+__global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_fvs(DevBlock b, DevState s,
+                                                                               double *__restrict__ dq, int nv,
+                                                                               int scheme) {
+  constexpr int TXL = FvsTile<DIR>::TXL, TD = FvsTile<DIR>::TD, NS = FvsTile<DIR>::NS;
+  extern __shared__ double fsm[];
+  double *Fp = fsm;                       // [NS][TXL][nv]
+  double *Fm = fsm + NS * TXL * nv;       // [NS][TXL][nv]
+  const int lane = DIR == 0 ? 0 : (int)threadIdx.x;
+  const int t = DIR == 0 ? (int)threadIdx.x : (int)threadIdx.y;
+  const int ns = c_mix.ns;
+  const long long P = b.plane;
+  const int nd = DIR == 0 ? b.mx : DIR == 1 ? b.my : b.mz;
+  const int start = (DIR == 0 ? blockIdx.x : blockIdx.y) * (TD - 1);
+  int i0, j0, k0;  // coordinates of this lane's line
+  if (DIR == 0) {
+    i0 = 0; j0 = blockIdx.y; k0 = blockIdx.z;
+  } else if (DIR == 1) {
+    i0 = blockIdx.x * TXL + lane; j0 = 0; k0 = blockIdx.z;
+  } else {
+    i0 = blockIdx.x * TXL + lane; j0 = blockIdx.z; k0 = 0;
+  }
+  const bool lane_ok = i0 < b.mx;
+  auto pid = [&](int n) -> long long {
+    return DIR == 0 ? b.id(n, j0, k0) : DIR == 1 ? b.id(i0, n, k0) : b.id(i0, j0, n);
+  };
+  // stage split fluxes of nodes start-4 .. start+TD+2
+  if (lane_ok) {
+    for (int st = t; st < NS; st += TD) {
+      const int n = start - 4 + st;
+      if (n > nd + 3) continue;
+      const long long p = pid(n);
+      double Q[kMV];
+      for (int l = 0; l < nv; ++l) Q[l] = s.cv[l * P + p];
+      const double pk = s.bv[4 * P + p];
+      const double c = s.acs ? s.acs[p] : sqrt(kGamma * (kRuD / kMwD) * s.bv[5 * P + p]);
+      const double k0m = b.met[(DIR * 3 + 0) * P + p], k1m = b.met[(DIR * 3 + 1) * P + p],
+                   k2m = b.met[(DIR * 3 + 2) * P + p];
+      const double jac = b.jac[p];
+      const double Uk = (Q[1] * k0m + Q[2] * k1m + Q[3] * k2m) / Q[0];
+      const double cg = c * sqrt(k0m * k0m + k1m * k1m + k2m * k2m);
+      const double l0 = fabs(Uk) + cg;
+      double *fp = Fp + ((long long)st * TXL + lane) * nv, *fm = Fm + ((long long)st * TXL + lane) * nv;
+      fp[0] = 0.5 * jac * (Uk * Q[0] + l0 * Q[0]);
+      fp[1] = 0.5 * jac * (Uk * Q[1] + pk * k0m + l0 * Q[1]);
+      fp[2] = 0.5 * jac * (Uk * Q[2] + pk * k1m + l0 * Q[2]);
+      fp[3] = 0.5 * jac * (Uk * Q[3] + pk * k2m + l0 * Q[3]);
+      fp[4] = 0.5 * jac * (Uk * (Q[4] + pk) + l0 * Q[4]);
+      fm[0] = 0.5 * jac * (Uk * Q[0] - l0 * Q[0]);
+      fm[1] = 0.5 * jac * (Uk * Q[1] + pk * k0m - l0 * Q[1]);
+      fm[2] = 0.5 * jac * (Uk * Q[2] + pk * k1m - l0 * Q[2]);
+      fm[3] = 0.5 * jac * (Uk * Q[3] + pk * k2m - l0 * Q[3]);
+      fm[4] = 0.5 * jac * (Uk * (Q[4] + pk) - l0 * Q[4]);
+      for (int l = 5; l < nv; ++l) {
+        fp[l] = 0.5 * jac * (Uk * Q[l] + l0 * Q[l]);
+        fm[l] = 0.5 * jac * (Uk * Q[l] - l0 * Q[l]);
+      }
+    }
+  }
+  __syncthreads();
+  const int n = start - 1 + t;  // left node of this thread's face
+  const bool face_ok = lane_ok && n < nd;
+  double fc[kMV];
+  for (int l = 0; l < kMV; ++l) fc[l] = 0.0;
+  auto FP = [&](int m, int l) -> double { return Fp[((long long)(t + m) * TXL + lane) * nv + l]; };
+  auto FM = [&](int m, int l) -> double { return Fm[((long long)(t + m) * TXL + lane) * nv + l]; };
+  if (face_ok && scheme == 71) {
+    const long long pl = pid(n), pr = pid(n + 1);
+    const double j1 = b.jac[pl], j2 = b.jac[pr];
+    double a[3];
+    for (int q = 0; q < 3; ++q) a[q] = b.met[(DIR * 3 + q) * P + pl] * j1 + b.met[(DIR * 3 + q) * P + pr] * j2;
+    const double eps_ref = 1e-20 * c_mix.weno_eps_scale * 0.25 * (a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    const double e1 = eps_ref * c_mix.v_ref * c_mix.v_ref;
+    const double e2 = e1 * c_mix.v_ref * c_mix.v_ref;
+    for (int l = 0; l < nv; ++l) {
+      const double e = (l >= 1 && l <= 3) ? e1 : (l == 4 ? e2 : eps_ref);
+      double vp[7], vm[7];
+      for (int m = 0; m < 7; ++m) {
+        vp[m] = FP(m, l);
+        vm[m] = FM(m + 1, l);
+      }
+      fc[l] = fvs_weno7(vp, vm, e);
+    }
+  } else if (face_ok) {
+    // Roe-averaged mixture eigensystem at the face (WENO.cu:747-821)
+    const long long pl = pid(n), pr = pid(n + 1);
+    double cvl[kMV], cvr[kMV];
+    for (int l = 0; l < nv; ++l) {
+      cvl[l] = s.cv[l * P + pl];
+      cvr[l] = s.cv[l * P + pr];
+    }
+    const double p_l = s.bv[4 * P + pl], p_r = s.bv[4 * P + pr];
+    const double rli = 1.0 / cvl[0], rri = 1.0 / cvr[0];
+    const double sl = sqrt(cvl[0]), sr = sqrt(cvr[0]);
+    const double rlc = sl / (sl + sr), rrc = sr / (sl + sr);
+    const double um = rlc * cvl[1] * rli + rrc * cvr[1] * rri;
+    const double vm_ = rlc * cvl[2] * rli + rrc * cvr[2] * rri;
+    const double wm = rlc * cvl[3] * rli + rrc * cvr[3] * rri;
+    const double ekm = 0.5 * (um * um + vm_ * vm_ + wm * wm);
+    const double hm = rlc * ((cvl[4] + p_l) * rli) + rrc * ((cvr[4] + p_r) * rri);
+    double svm[kMS], hi[kMS], cpi[kMS], al[kMS];
+    double mw_inv = 0;
+    for (int l = 0; l < ns; ++l) {
+      svm[l] = rlc * cvl[l + 5] * rli + rrc * cvr[l + 5] * rri;
+      mw_inv += svm[l] / c_mix.mw[l];
+    }
+    const double tm = (rlc * (p_l * rli) + rrc * (p_r * rri)) / (kRuD * mw_inv);
+    mix_h_cp(tm, hi, cpi);
+    double cp = 0, cvt = 0;
+    for (int l = 0; l < ns; ++l) {
+      cp += svm[l] * cpi[l];
+      cvt += svm[l] * (cpi[l] - c_mix.ru_mw[l]);
+    }
+    const double gamma = cp / cvt;
+    const double cm = sqrt(gamma * kRuD * mw_inv * tm);
+    const double gm1 = gamma - 1;
+    const double jl = b.jac[pl], jr = b.jac[pr];
+    const double kxJ = b.met[(DIR * 3 + 0) * P + pl] * jl + b.met[(DIR * 3 + 0) * P + pr] * jr;
+    const double kyJ = b.met[(DIR * 3 + 1) * P + pl] * jl + b.met[(DIR * 3 + 1) * P + pr] * jr;
+    const double kzJ = b.met[(DIR * 3 + 2) * P + pl] * jl + b.met[(DIR * 3 + 2) * P + pr] * jr;
+    double kx = kxJ / (jl + jr), ky = kyJ / (jl + jr), kz = kzJ / (jl + jr);
+    const double gradK = sqrt(kx * kx + ky * ky + kz * kz);
+    kx /= gradK;
+    ky /= gradK;
+    kz /= gradK;
+    const double Ukb = kx * um + ky * vm_ + kz * wm;
+    const double alpha = gm1 * ekm;
+    const double c2i = 1.0 / (cm * cm);
+    const double eps = 1e-40 * c_mix.weno_eps_scale * 0.25 * (kxJ * kxJ + kyJ * kyJ + kzJ * kzJ);
+    for (int l = 0; l < ns; ++l) {
+      al[l] = gamma * kRuD / c_mix.mw[l] * tm - (gamma - 1) * hi[l];
+      al[l] *= c2i;
+    }
+    double fch[kMV];
+    for (int l = 0; l < 5; ++l) {
+      double cs = 0.5, L[5];
+      if (l == 0) {
+        L[0] = (alpha + Ukb * cm) * c2i * 0.5;
+        L[1] = -(gm1 * um + kx * cm) * c2i * 0.5;
+        L[2] = -(gm1 * vm_ + ky * cm) * c2i * 0.5;
+        L[3] = -(gm1 * wm + kz * cm) * c2i * 0.5;
+        L[4] = gm1 * c2i * 0.5;
+      } else if (l == 1) {
+        cs = -kx;
+        L[0] = kx * (1 - alpha * c2i) - (kz * vm_ - ky * wm) / cm;
+        L[1] = kx * gm1 * um * c2i;
+        L[2] = (kx * gm1 * vm_ + kz * cm) * c2i;
+        L[3] = (kx * gm1 * wm - ky * cm) * c2i;
+        L[4] = -kx * gm1 * c2i;
+      } else if (l == 2) {
+        cs = -ky;
+        L[0] = ky * (1 - alpha * c2i) - (kx * wm - kz * um) / cm;
+        L[1] = (ky * gm1 * um - kz * cm) * c2i;
+        L[2] = ky * gm1 * vm_ * c2i;
+        L[3] = (ky * gm1 * wm + kx * cm) * c2i;
+        L[4] = -ky * gm1 * c2i;
+      } else if (l == 3) {
+        cs = -kz;
+        L[0] = kz * (1 - alpha * c2i) - (ky * um - kx * vm_) / cm;
+        L[1] = (kz * gm1 * um + ky * cm) * c2i;
+        L[2] = (kz * gm1 * vm_ - kx * cm) * c2i;
+        L[3] = kz * gm1 * wm * c2i;
+        L[4] = -kz * gm1 * c2i;
+      } else {
+        L[0] = (alpha - Ukb * cm) * c2i * 0.5;
+        L[1] = -(gm1 * um - kx * cm) * c2i * 0.5;
+        L[2] = -(gm1 * vm_ - ky * cm) * c2i * 0.5;
+        L[3] = -(gm1 * wm - kz * cm) * c2i * 0.5;
+        L[4] = gm1 * c2i * 0.5;
+      }
+      double vp[7], vmn[7];
+      for (int m = 0; m < 7; ++m) {
+        double a = 0, bq = 0;
+        for (int q = 0; q < 5; ++q) {
+          a += L[q] * FP(m, q);
+          bq += L[q] * FM(m + 1, q);
+        }
+        for (int q = 0; q < ns; ++q) {
+          a += cs * al[q] * FP(m, 5 + q);
+          bq += cs * al[q] * FM(m + 1, 5 + q);
+        }
+        vp[m] = a;
+        vmn[m] = bq;
+      }
+      fch[l] = fvs_weno7(vp, vmn, eps);
+    }
+    for (int l = 0; l < ns; ++l) {
+      double vp[7], vmn[7];
+      for (int m = 0; m < 7; ++m) {
+        vp[m] = -svm[l] * FP(m, 0) + FP(m, 5 + l);
+        vmn[m] = -svm[l] * FM(m + 1, 0) + FM(m + 1, 5 + l);
+      }
+      fch[5 + l] = fvs_weno7(vp, vmn, eps);
+    }
+    fc[0] = fch[0] + kx * fch[1] + ky * fch[2] + kz * fch[3] + fch[4];
+    fc[1] = (um - kx * cm) * fch[0] + kx * um * fch[1] + (ky * um - kz * cm) * fch[2] + (kz * um + ky * cm) * fch[3] +
+            (um + kx * cm) * fch[4];
+    fc[2] = (vm_ - ky * cm) * fch[0] + (kx * vm_ + kz * cm) * fch[1] + ky * vm_ * fch[2] +
+            (kz * vm_ - kx * cm) * fch[3] + (vm_ + ky * cm) * fch[4];
+    fc[3] = (wm - kz * cm) * fch[0] + (kx * wm - ky * cm) * fch[1] + (ky * wm + kx * cm) * fch[2] + kz * wm * fch[3] +
+            (wm + kz * cm) * fch[4];
+    const double hc = hm - cm * cm / gm1;
+    fc[4] = (hm - Ukb * cm) * fch[0] + (kx * hc + (kz * vm_ - ky * wm) * cm) * fch[1] +
+            (ky * hc + (kx * wm - kz * um) * cm) * fch[2] + (kz * hc + (ky * um - kx * vm_) * cm) * fch[3] +
+            (hm + Ukb * cm) * fch[4];
+    double add = 0;
+    const double ca = fch[0] + kx * fch[1] + ky * fch[2] + kz * fch[3] + fch[4];
+    for (int l = 0; l < ns; ++l) {
+      fc[5 + l] = svm[l] * ca + fch[l + 5];
+      add += al[l] * fch[l + 5];
+    }
+    fc[4] -= add * cm * cm / gm1;
+  }
+  __syncthreads();  // every thread is done with the staged fluxes: reuse them for the face fluxes
+  double *fcs = fsm;  // [TD][TXL][nv]
+  for (int l = 0; l < nv; ++l) fcs[((long long)t * TXL + lane) * nv + l] = fc[l];
+  __syncthreads();
+  if (face_ok && t >= 1) {
+    const long long q = DIR == 0 ? b.iq(n, j0, k0) : DIR == 1 ? b.iq(i0, n, k0) : b.iq(i0, j0, n);
+    for (int l = 0; l < nv; ++l)
+      dq[l * b.n + q] -= fc[l] - fcs[((long long)(t - 1) * TXL + lane) * nv + l];
+  }
+}
+
+// ------------------------------------------------------------------ viscous sweeps (mixtures)
+
+// compute_fv/gv/hv_2nd_order<mixture, Laminar> (ViscousScheme.cuh:24-318 and its y / z twins) at the
+// face between node p0 and its neighbour p0 + e[d]: stress, Fourier conduction with the mixture
+// conductivity, mixture-averaged species diffusion with the correction velocity and its enthalpy flux.
+template <bool DIM3>
+__device__ __forceinline__ void mix_visc_face(const DevBlock &b, const DevState &s, long long p0, int d, int nv,
+                                              double *fv) {
+  const long long P = b.plane;
+  const long long st[3] = {1, b.pitch, (long long)b.pitch * b.sy};
+  const long long p1 = p0 + st[d];
+  double m[9];
+  for (int r = 0; r < 9; ++r) m[r] = 0.5 * (b.met[r * P + p0] + b.met[r * P + p1]);
+  // gradient of plane B at the face: 2-point normal difference, 4-point averages across
+  auto grad = [&](const double *B, double *out) {
+    double g[3];
+    for (int c = 0; c < 3; ++c) {
+      if (c == d) {
+        g[c] = B[p1] - B[p0];
+      } else if (c == 2 && !DIM3) {
+        g[c] = 0.0;
+      } else {
+        const long long a = st[c];
+        g[c] = 0.25 * (B[p0 + a] - B[p0 - a] + B[p1 + a] - B[p1 - a]);
+      }
+    }
+    out[0] = g[0] * m[0] + g[1] * m[3] + g[2] * m[6];
+    out[1] = g[0] * m[1] + g[1] * m[4] + g[2] * m[7];
+    out[2] = g[0] * m[2] + g[1] * m[5] + g[2] * m[8];
+  };
+  double gu[3], gv[3], gw[3], gt[3];
+  grad(s.bv + P, gu);
+  grad(s.bv + 2 * P, gv);
+  grad(s.bv + 3 * P, gw);
+  grad(s.bv + 5 * P, gt);
+  const double mul = 0.5 * (s.mul[p0] + s.mul[p1]);
+  const double txx = mul * (4 * gu[0] - 2 * gv[1] - 2 * gw[2]) / 3.0;
+  const double tyy = mul * (4 * gv[1] - 2 * gu[0] - 2 * gw[2]) / 3.0;
+  const double tzz = mul * (4 * gw[2] - 2 * gu[0] - 2 * gv[1]) / 3.0;
+  const double txy = mul * (gu[1] + gv[0]);
+  const double txz = mul * (gu[2] + gw[0]);
+  const double tyz = mul * (gv[2] + gw[1]);
+  const double j0 = b.jac[p0], j1 = b.jac[p1];
+  const double nx = 0.5 * (b.met[(d * 3 + 0) * P + p0] * j0 + b.met[(d * 3 + 0) * P + p1] * j1);
+  const double ny = 0.5 * (b.met[(d * 3 + 1) * P + p0] * j0 + b.met[(d * 3 + 1) * P + p1] * j1);
+  const double nz = 0.5 * (b.met[(d * 3 + 2) * P + p0] * j0 + b.met[(d * 3 + 2) * P + p1] * j1);
+  fv[0] = 0;
+  fv[1] = nx * txx + ny * txy + nz * txz;
+  fv[2] = nx * txy + ny * tyy + nz * tyz;
+  fv[3] = nx * txz + ny * tyz + nz * tzz;
+  const double um = 0.5 * (s.bv[P + p0] + s.bv[P + p1]);
+  const double vm = 0.5 * (s.bv[2 * P + p0] + s.bv[2 * P + p1]);
+  const double wm = 0.5 * (s.bv[3 * P + p0] + s.bv[3 * P + p1]);
+  const double cond = 0.5 * (s.cond[p0] + s.cond[p1]);
+  fv[4] = um * fv[1] + vm * fv[2] + wm * fv[3] + cond * (nx * gt[0] + ny * gt[1] + nz * gt[2]);
+  const int ns = c_mix.ns;
+  double dif[kMS], yk[kMS], ddf[kMS];
+  double sgw = 0, srdy = 0, corr = 0, mwt = 0;
+  for (int l = 0; l < ns; ++l) {
+    const double *Y = s.sv + (long long)l * P;
+    yk[l] = 0.5 * (Y[p0] + Y[p1]);
+    dif[l] = 0.5 * (s.rhod[l * P + p0] + s.rhod[l * P + p1]);
+    double gy[3];
+    grad(Y, gy);
+    const double gdy = nx * gy[0] + ny * gy[1] + nz * gy[2];
+    ddf[l] = gdy;
+    corr += dif[l] * gdy;
+    sgw += gdy / c_mix.mw[l];
+    mwt += yk[l] / c_mix.mw[l];
+    srdy += dif[l] * yk[l];
+  }
+  mwt = 1.0 / mwt;
+  corr -= mwt * srdy * sgw;
+  double h[kMS];
+  mix_h_cp(0.5 * (s.bv[5 * P + p0] + s.bv[5 * P + p1]), h, nullptr);
+  for (int l = 0; l < ns; ++l) {
+    const double flux = dif[l] * (ddf[l] - mwt * yk[l] * sgw) - yk[l] * corr;
+    fv[5 + l] = flux;
+    fv[4] += h[l] * flux;
+  }
+}
+
+// viscous_flux_fv/gv/hv (SchemeSelector.cuh:69-154) for mixtures: one thread per face of the tile,
+// then dq += fv(i+1/2) - fv(i-1/2) through shared memory; tiles as the flux-split sweeps.
+template <int DIR, bool DIM3>
+__global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_mix_visc(DevBlock b, DevState s,
+                                                                                    double *__restrict__ dq, int nv) {
+  constexpr int TXL = FvsTile<DIR>::TXL, TD = FvsTile<DIR>::TD;
+  extern __shared__ double fsm[];
+  const int lane = DIR == 0 ? 0 : (int)threadIdx.x;
+  const int t = DIR == 0 ? (int)threadIdx.x : (int)threadIdx.y;
+  const int nd = DIR == 0 ? b.mx : DIR == 1 ? b.my : b.mz;
+  const int start = (DIR == 0 ? blockIdx.x : blockIdx.y) * (TD - 1);
+  int i0, j0, k0;
+  if (DIR == 0) {
+    i0 = 0; j0 = blockIdx.y; k0 = blockIdx.z;
+  } else if (DIR == 1) {
+    i0 = blockIdx.x * TXL + lane; j0 = 0; k0 = blockIdx.z;
+  } else {
+    i0 = blockIdx.x * TXL + lane; j0 = blockIdx.z; k0 = 0;
+  }
+  const int n = start - 1 + t;
+  const bool face_ok = i0 < b.mx && n < nd;
+  double fv[kMV];
+  for (int l = 0; l < kMV; ++l) fv[l] = 0.0;
+  if (face_ok) {
+    const long long p0 = DIR == 0 ? b.id(n, j0, k0) : DIR == 1 ? b.id(i0, n, k0) : b.id(i0, j0, n);
+    mix_visc_face<DIM3>(b, s, p0, DIR, nv, fv);
+  }
+  for (int l = 0; l < nv; ++l) fsm[((long long)t * TXL + lane) * nv + l] = fv[l];
+  __syncthreads();
+  if (face_ok && t >= 1) {
+    const long long q = DIR == 0 ? b.iq(n, j0, k0) : DIR == 1 ? b.iq(i0, n, k0) : b.iq(i0, j0, n);
+    for (int l = 0; l < nv; ++l) dq[l * b.n + q] += fv[l] - fsm[((long long)(t - 1) * TXL + lane) * nv + l];
+  }
+}
+
+// update_cv_and_bv_rk<mixture> (RK.cuh:230-284) with compute_temperature_and_pressure
+// (FieldOperation.cu:3-40): the Newton iteration starts from the stage-input temperature.
+__global__ void __launch_bounds__(128) k_mix_update(DevBlock b, DevState in, DevState qn, DevState out,
+                                                     const double *__restrict__ dq, const double *dtp, double ca,
+                                                     double cb, double cc, int nv, unsigned *flags) {
+  const long long P = b.plane;
+  const int ns = c_mix.ns;
+  const double dt = *dtp;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % b.mx);
+    const long long r = n / b.mx;
+    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const long long p = b.id(i, j, k);
+    const double dtj = dt / b.jac[p];
+    double c[kMV];
+    for (int l = 0; l < nv; ++l) {
+      c[l] = ca * qn.cv[l * P + p] + cb * in.cv[l * P + p] + cc * dtj * dq[l * b.n + n];
+    }
+    if (b.mz == 1) c[3] = 0;
+    for (int l = 0; l < nv; ++l) out.cv[l * P + p] = c[l];
+    const double rho = c[0];
+    const double di = 1.0 / rho;
+    const double u = c[1] * di, v = c[2] * di, w = c[3] * di;
+    out.bv[p] = rho;
+    out.bv[P + p] = u;
+    out.bv[2 * P + p] = v;
+    out.bv[3 * P + p] = w;
+    double y[kMS];
+    for (int l = 0; l < ns; ++l) {
+      y[l] = c[5 + l] * di;
+      out.sv[l * P + p] = y[l];
+    }
+    const double e = c[4] / rho - 0.5 * (u * u + v * v + w * w);
+    double pr;
+    const double t = mix_temperature(rho, e, in.bv[5 * P + p], y, pr);
+    out.bv[4 * P + p] = pr;
+    out.bv[5 * P + p] = t;
+    if (!(rho > 0) || !(pr > 0) || !(t > 0)) atomicOr(flags, (rho != rho || pr != pr || t != t) ? 2u : 1u);
+  }
+}
+
+}  // namespace ostc

@@ -158,8 +158,12 @@ class Solver:
         self._check(self.lib.ostc_set_precision(self.h, mode))
 
     def set_state(self, bv: np.ndarray, block: int = 0, sv: np.ndarray | None = None):
+        """bv [6][mz][my][mx] (rho, u, v, w, p, T); sv [n_spec][mz][my][mx] mass fractions for mixtures."""
         bv = np.ascontiguousarray(bv, dtype=np.float64)
         assert bv.shape == (6,) + self.shape(block), bv.shape
+        if sv is not None:
+            sv = np.ascontiguousarray(sv, dtype=np.float64)
+            assert sv.shape == (self.n_scalar,) + self.shape(block), sv.shape
         self._check(self.lib.ostc_set_state(self.h, block, _ptr(bv), None if sv is None else _ptr(sv), OSTC_HOST))
 
     def set_state_ptr(self, bv_ptr: int, block: int = 0, kind: int = OSTC_HOST):
@@ -171,6 +175,12 @@ class Solver:
         bv = np.empty((6,) + sh)
         self._check(self.lib.ostc_get_state(self.h, block, _ptr(cv), _ptr(bv), None, OSTC_HOST))
         return cv, bv
+
+    def get_species(self, block: int = 0) -> np.ndarray:
+        """Mass fractions sv [n_spec][mz][my][mx] of a mixture case."""
+        sv = np.empty((self.n_scalar,) + self.shape(block))
+        self._check(self.lib.ostc_get_state(self.h, block, None, None, _ptr(sv), OSTC_HOST))
+        return sv
 
     def get_state_ptr(self, cv_ptr: int, bv_ptr: int, block: int = 0, kind: int = OSTC_HOST):
         self._check(self.lib.ostc_get_state(self.h, block, ctypes.c_void_p(cv_ptr) if cv_ptr else None,

@@ -42,6 +42,10 @@ CASES = [
      dict(mx=32, my=20, mz=16, reconstruction=2, inviscid_scheme=1), 20),
     ("ml3d_nnd_roe_farfield", "mixing_layer_3d",
      dict(mx=32, my=20, mz=16, reconstruction=3, inviscid_scheme=2), 20),
+    # 9-species H2/air mixtures: finite-rate (FR) and non-reacting (Mixture) models, flux-split WENO7
+    ("rml3d_fr72", "reacting_mixing_layer_3d", dict(mx=32, my=20, mz=16, inviscid_scheme=72), 10),
+    ("rml3d_mix71", "reacting_mixing_layer_3d", dict(mx=32, my=20, mz=16, inviscid_scheme=71, finite_rate=False), 10),
+    ("rml2d_fr72", "reacting_mixing_layer_3d", dict(mx=48, my=24, mz=1, inviscid_scheme=72), 20),
 ]
 
 
@@ -55,7 +59,7 @@ def main(outdir: Path, only=None):
         if only and name not in only:
             continue
         case = make_case(gen, kw)
-        cv, bv, t = refcase.run_reference(case, steps)
+        cv, bv, t = refcase.run_reference(case, steps)[:3]
         np.savez_compressed(outdir / f"golden_{name}.npz", cv=cv, t=t, steps=steps,
                             case=json.dumps({"generator": gen, "kwargs": kw}),
                             bv0_sum=float(np.sum(case.bv)))

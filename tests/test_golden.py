@@ -53,7 +53,7 @@ def test_gpu_matches_reference(built, tmp_path, path):
     case, steps, cv_ref, t_ref = _load(path)
     d = oc.write_case(case, tmp_path / "case")
     s = ostc.Solver(str(d))
-    s.set_state(case.bv)
+    s.set_state(case.bv, sv=case.sv)
     s.step(steps)
     cv, _ = s.get_state()
     err = oc.relative_errors(cv, cv_ref)
