@@ -56,10 +56,30 @@ def test_missing_grid_is_io_error(built, tmp_path):
 
 def test_unsupported_species_rejected(built, tmp_path):
     _, d = _case_dir(tmp_path)
-    s = (d / "setup.txt").read_text().replace("int species = 0", "int species = 1")
-    (d / "setup.txt").write_text(s)
-    with pytest.raises(ostc.OstcError, match="species"):
+    s = (d / "setup.txt").read_text()
+    (d / "setup.txt").write_text(s.replace("int species = 0", "int species = 2"))
+    with pytest.raises(ostc.OstcError, match="species = 2"):
         ostc.probe_case(str(d))
+    # species = 1 with an AWENO scheme: mixtures run the flux-split WENO7 path only
+    (d / "setup.txt").write_text(s.replace("int species = 0", "int species = 1"))
+    with pytest.raises(ostc.OstcError, match="flux-split"):
+        ostc.probe_case(str(d))
+
+
+def test_mixture_probe_and_errors(built, tmp_path):
+    case = oc.reacting_mixing_layer_3d(mx=12, my=10, mz=8)
+    d = oc.write_case(case, tmp_path / "mix")
+    info = ostc.probe_case(str(d))
+    assert info["n_var"] == 14 and info["n_scalar"] == 9 and info["ngg"] == 4 and info["inviscid_type"] == 3
+    setup = (d / "setup.txt").read_text()
+    # the reference's 52 reads outside its stencil: rejected with the reason
+    (d / "setup.txt").write_text(setup.replace("int inviscid_scheme = 72", "int inviscid_scheme = 52"))
+    with pytest.raises(ostc.OstcError, match="outside its stencil"):
+        ostc.probe_case(str(d))
+    (d / "setup.txt").write_text(setup.replace("chemistry/H2_mech.inp", "chemistry/missing.inp"))
+    with pytest.raises(ostc.OstcError, match="cannot open") as e:
+        ostc.probe_case(str(d))
+    assert e.value.code == -2  # OSTC_EIO
 
 
 def test_face_outside_block_rejected(built, tmp_path):
