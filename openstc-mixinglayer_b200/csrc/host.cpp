@@ -325,7 +325,7 @@ void register_boundary(BcFace &b, int ngg, int dim) {
   }
 }
 
-// Mesh::init_ghost_grid for one block without interfaces (Mesh.cpp:893-1043)
+// Face layers of the ghost grid by point reflection (Mesh.cpp:893-960).
 void ghost_grid(HostBlock &B, int dimension) {
   const int mx = B.mx, my = B.my, mz = B.mz, ngg = B.ngg;
   std::array<std::vector<double> *, 3> C{&B.x, &B.y, &B.z};
@@ -364,6 +364,14 @@ void ghost_grid(HostBlock &B, int dimension) {
         }
       }
   }
+}
+
+// Edges and corners of the ghost grid by the parallelogram rule (Mesh.cpp:968-1041), after the face
+// layers and the interface layers are in place.
+void ghost_grid_edges(HostBlock &B) {
+  const int mx = B.mx, my = B.my, mz = B.mz, ngg = B.ngg;
+  std::array<std::vector<double> *, 3> C{&B.x, &B.y, &B.z};
+  auto at = [&](int q, int i, int j, int k) -> double & { return (*C[q])[B.cidx(i, j, k)]; };
   for (int i = 1; i <= ngg + 1; ++i)
     for (int j = 1; j <= ngg + 1; ++j)
       for (int k = 0; k < mz; ++k) {
@@ -463,6 +471,114 @@ void compute_jac_metric(HostBlock &B) {
       for (int k = -ngg; k < mz + ngg; ++k) metric_node(B, i, j, k, i - 1, j, k);
 }
 
+}  // namespace
+
+namespace {
+int sgn(int a) { return a < 0 ? -1 : 1; }  // gxl::sgn: sgn(0) = +1 (gxl_lib/Math.hpp:13-15)
+
+// InnerFace::register_boundary (Mesh.cpp:38-141).  Input: the two 1-based index ranges of the file,
+// signs marking the first tangential direction (3-D); output: the written range (face + ngg ghost
+// layers, tangential extent of the face), the target start, the index map and loop directions.
+void register_inner(InnerFace &f, int ngg, int dim) {
+  for (int i = 0; i < dim; ++i)
+    if (f.rs[i] == f.re[i]) {
+      f.face = i;
+      if (f.rs[i] == 1) f.direction = -1;
+      f.rs[i] -= 1;
+      f.re[i] -= 1;
+      break;
+    }
+  for (int i = 0; i < dim; ++i)
+    if (f.ts[i] == f.te[i]) {
+      f.target_face = i;
+      if (f.ts[i] == 1) f.target_direction = -1;
+      f.ts[i] -= 1;
+      f.te[i] -= 1;
+      break;
+    }
+  f.src_tar[f.target_face] = -(f.direction * f.target_direction) * (f.face + 1);
+  if (dim == 2) {
+    const int nf = 1 - f.face, tnf = 1 - f.target_face;
+    f.rs[nf] = std::abs(f.rs[nf]) - 1;
+    f.re[nf] = std::abs(f.re[nf]) - 1;
+    f.ts[tnf] = std::abs(f.ts[tnf]) - 1;
+    f.te[tnf] = std::abs(f.te[tnf]) - 1;
+    f.src_tar[tnf] = sgn((f.te[tnf] - f.ts[tnf]) * (f.re[nf] - f.rs[nf])) * (nf + 1);
+    f.src_tar[2] = 3;
+    f.rs[2] = f.re[2] = f.ts[2] = f.te[2] = 0;
+  } else {
+    int nf = 0, tnf = 0;
+    for (int i = 0; i < dim; ++i)
+      if (f.rs[i] < 0) {
+        nf = i;
+        f.rs[i] = -f.rs[i] - 1;
+        f.re[i] = -f.re[i] - 1;
+        break;
+      }
+    for (int i = 0; i < dim; ++i)
+      if (f.ts[i] < 0) {
+        tnf = i;
+        f.ts[i] = -f.ts[i] - 1;
+        f.te[i] = -f.te[i] - 1;
+        break;
+      }
+    f.src_tar[tnf] = sgn((f.te[tnf] - f.ts[tnf]) * (f.re[nf] - f.rs[nf])) * (nf + 1);
+    nf = 3 - f.face - nf;
+    tnf = 3 - f.target_face - tnf;
+    f.rs[nf] -= 1;
+    f.re[nf] -= 1;
+    f.ts[tnf] -= 1;
+    f.te[tnf] -= 1;
+    f.src_tar[tnf] = sgn((f.te[tnf] - f.ts[tnf]) * (f.re[nf] - f.rs[nf])) * (nf + 1);
+  }
+  f.rs[f.face] = f.direction < 0 ? -ngg : f.re[f.face];
+  f.re[f.face] = f.direction < 0 ? 0 : f.re[f.face] + ngg;
+  const int st = sgn(f.src_tar[f.target_face]);
+  if (f.target_direction > 0) f.ts[f.target_face] = st > 0 ? f.te[f.target_face] - ngg : f.te[f.target_face];
+  else f.ts[f.target_face] = st > 0 ? 0 : ngg;
+  for (int i = 0; i < 3; ++i) {
+    f.loop_dir[i] = f.rs[i] <= f.re[i] ? 1 : -1;
+    f.target_loop_dir[i] = sgn(f.src_tar[i]);
+    f.src_tar[i] = std::abs(f.src_tar[i]) - 1;
+  }
+  for (int i = 0; i < 3; ++i) f.n_point[i] = std::abs(f.rs[i] - f.re[i]) + 1;
+}
+
+// Mesh::init_inner_ghost_grid (Mesh.cpp:1049-1097): ghost coordinates across an interface are the
+// neighbour's interior coordinates (ngg + 1 layers).
+void inner_ghost_grid(HostMesh &mesh) {
+  for (auto &B : mesh.blocks)
+    for (const auto &fc : B.inner) {
+      HostBlock &nB = mesh.blocks[fc.target_block];
+      int mn[3] = {fc.rs[0], fc.rs[1], fc.rs[2]}, mx_[3] = {fc.re[0], fc.re[1], fc.re[2]};
+      int mt[3] = {fc.ts[0], fc.ts[1], fc.ts[2]};
+      if (fc.direction < 0) {
+        mn[fc.face] -= 1;
+        mx_[fc.face] -= 1;
+      } else {
+        mn[fc.face] += 1;
+        mx_[fc.face] += 1;
+      }
+      mt[fc.target_face] += fc.target_direction > 0 ? -1 : 1;
+      const int d1[3] = {fc.loop_dir[0], fc.loop_dir[1], fc.loop_dir[2]};
+      int di[3];
+      for (int i1 = mn[0]; d1[0] * (i1 - mx_[0]) != 1; i1 += d1[0]) {
+        di[0] = i1 - mn[0];
+        for (int j1 = mn[1]; d1[1] * (j1 - mx_[1]) != 1; j1 += d1[1]) {
+          di[1] = j1 - mn[1];
+          for (int k1 = mn[2]; d1[2] * (k1 - mx_[2]) != 1; k1 += d1[2]) {
+            di[2] = k1 - mn[2];
+            const int i2 = mt[0] + fc.target_loop_dir[0] * di[fc.src_tar[0]];
+            const int j2 = mt[1] + fc.target_loop_dir[1] * di[fc.src_tar[1]];
+            const int k2 = mt[2] + fc.target_loop_dir[2] * di[fc.src_tar[2]];
+            B.x[B.cidx(i1, j1, k1)] = nB.x[nB.cidx(i2, j2, k2)];
+            B.y[B.cidx(i1, j1, k1)] = nB.y[nB.cidx(i2, j2, k2)];
+            B.z[B.cidx(i1, j1, k1)] = nB.z[nB.cidx(i2, j2, k2)];
+          }
+        }
+      }
+    }
+}
 }  // namespace
 
 bool read_mesh(const std::string &dir, const Derived &d, HostMesh &mesh, std::string &err) {
@@ -569,14 +685,54 @@ bool read_mesh(const std::string &dir, const Derived &d, HostMesh &mesh, std::st
     const std::string ipath = dir + "/boundary_condition/inner   0.txt";
     std::ifstream inf(ipath);
     if (inf) {
+      // Mesh::read_inner_interface (Mesh.cpp:812-844): a header line, the face count of every block,
+      // a column-title line, then per face two lines: this block's 1-based range and the target's
+      // range followed by the target block id.
       std::string input;
       std::getline(inf, input);
-      for (size_t b = 0; b < mesh.blocks.size(); ++b) {
-        int n = 0;
-        inf >> n;
-        if (n != 0) {
-          err = "block interfaces (inner faces) are not supported by this build of the library";
-          return false;
+      std::vector<int> nface(mesh.blocks.size(), 0);
+      for (auto &n : nface) inf >> n;
+      std::getline(inf, input);
+      std::getline(inf, input);
+      const int nb = (int)mesh.blocks.size();
+      for (int b = 0; b < nb; ++b) {
+        HostBlock &B = mesh.blocks[b];
+        for (int l = 0; l < nface[b]; ++l) {
+          InnerFace f;
+          int i7 = 0, j7 = 0;
+          std::getline(inf, input);
+          std::istringstream l1(input);
+          l1 >> f.rs[0] >> f.re[0] >> f.rs[1] >> f.re[1] >> f.rs[2] >> f.re[2] >> i7;
+          std::getline(inf, input);
+          std::istringstream l2(input);
+          l2 >> f.ts[0] >> f.te[0] >> f.ts[1] >> f.te[1] >> f.ts[2] >> f.te[2] >> j7;
+          if (!l1 || !l2 || j7 < 1 || j7 > nb) {
+            err = "inner face file: malformed face of block " + std::to_string(b + 1);
+            return false;
+          }
+          f.target_block = j7 - 1;
+          register_inner(f, B.ngg, mesh.dimension);
+          // every device index of the exchange derives from these ranges: check them against both blocks
+          const HostBlock &T = mesh.blocks[f.target_block];
+          const int ext[3] = {B.mx, B.my, B.mz}, text[3] = {T.mx, T.my, T.mz};
+          bool ok = true;
+          for (int q = 0; q < 3; ++q) {
+            const int lo = std::min(f.rs[q], f.re[q]), hi = std::max(f.rs[q], f.re[q]);
+            const int g = q == f.face ? B.ngg : 0;
+            if (lo < -g || hi > ext[q] - 1 + g) ok = false;
+          }
+          for (int q = 0; q < 3 && ok; ++q) {
+            // the target index of the last point along each source axis
+            const int dmax = f.n_point[f.src_tar[q]] - 1;
+            const int a = f.ts[q], bq = f.ts[q] + f.target_loop_dir[q] * f.loop_dir[f.src_tar[q]] * dmax;
+            if (std::min(a, bq) < 0 || std::max(a, bq) > text[q] - 1) ok = false;
+          }
+          if (!ok) {
+            err = "inner face file: interface " + std::to_string(l + 1) + " of block " + std::to_string(b + 1) +
+                  " reaches outside a block";
+            return false;
+          }
+          B.inner.push_back(f);
         }
       }
     }
@@ -589,8 +745,10 @@ bool read_mesh(const std::string &dir, const Derived &d, HostMesh &mesh, std::st
       for (auto &v : B.z) v *= d.grid_scale;
     }
   }
+  for (auto &B : mesh.blocks) ghost_grid(B, mesh.dimension);
+  inner_ghost_grid(mesh);
   for (auto &B : mesh.blocks) {
-    ghost_grid(B, mesh.dimension);
+    ghost_grid_edges(B);
     B.jac.assign(B.padded(), 0.0);
     B.metric.assign(9 * B.padded(), 0.0);
     compute_jac_metric(B);
@@ -617,24 +775,28 @@ double struct_real(const std::map<std::string, Setup::StructVal> &st, const char
 double sutherland_host(double t) { return 1.7894e-5 * std::pow(t / 288.16, 1.5) * (288.16 + 110) / (t + 110); }
 }  // namespace
 
-bool reference_scales(const Setup &s, const ChemTables *chem, double &eps_scale, double &v_ref, std::string &err) {
-  eps_scale = 0;
-  v_ref = 0;
-  auto rs = s.strings.find("reference_state");
-  if (rs == s.strings.end()) return true;
-  auto it = s.structs.find(rs->second);
+// State of a plain inflow struct (Inflow::Inflow, BoundCond.cpp:157-214): density from p, T and the
+// mixture weight, velocity = Mach * c along (u, v, w).  Returns false with err set when the struct
+// lacks mach, pressure or temperature.
+bool inflow_state(const Setup &s, const std::string &name, const ChemTables *chem, double bv[6],
+                  std::vector<double> &y, double &c, std::string &err) {
+  auto it = s.structs.find(name);
   if (it == s.structs.end()) {
-    err = "reference_state names struct '" + rs->second + "', which the setup does not define";
+    err = "struct '" + name + "' is not defined in the setup";
     return false;
   }
   const auto &st = it->second;
-  // Inflow::Inflow for a plain inflow struct (BoundCond.cpp:157-214) and the reference state it sets
-  // (:299-305): density from p, T and the mixture weight, velocity = Mach * c (c when |V| < 1).
   const double mach = struct_real(st, "mach", -1), pressure = struct_real(st, "pressure", -1);
   const double temperature = struct_real(st, "temperature", -1);
+  if (mach < 0 || pressure < 0 || temperature < 0) {
+    err = "struct '" + name + "' needs mach, pressure and temperature on this path";
+    return false;
+  }
   double mw = kMwAir, gamma = kGammaAir;
+  y.clear();
   if (chem && chem->n_spec > 0) {
-    std::vector<double> y(chem->n_spec, 0.0), cp(chem->n_spec), h(chem->n_spec);
+    y.assign(chem->n_spec, 0.0);
+    std::vector<double> cp(chem->n_spec);
     for (int i = 0; i < chem->n_spec; ++i) y[i] = struct_real(st, chem->names[i].c_str(), 0.0);
     mw = 0;
     for (int i = 0; i < chem->n_spec; ++i) mw += y[i] / chem->mw[i];
@@ -643,30 +805,50 @@ bool reference_scales(const Setup &s, const ChemTables *chem, double &eps_scale,
     const double t = temperature, t2 = t * t, t3 = t2 * t, t4 = t3 * t;
     double cpt = 0, cvt = 0;
     for (int i = 0; i < chem->n_spec; ++i) {
-      double c;
+      double cc;
       if (t < chem->t_low[i]) {
         const double tt = chem->t_low[i], tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt;
         const double *a = &chem->low[i * 7];
-        c = a[0] + a[1] * tt + a[2] * tt2 + a[3] * tt3 + a[4] * tt4;
+        cc = a[0] + a[1] * tt + a[2] * tt2 + a[3] * tt3 + a[4] * tt4;
       } else {
         const double *a = t < chem->t_mid[i] ? &chem->low[i * 7] : &chem->high[i * 7];
-        c = a[0] + a[1] * t + a[2] * t2 + a[3] * t3 + a[4] * t4;
+        cc = a[0] + a[1] * t + a[2] * t2 + a[3] * t3 + a[4] * t4;
       }
-      c *= kRu / chem->mw[i];
-      cpt += y[i] * c;
-      cvt += y[i] * (c - kRu / chem->mw[i]);
+      cc *= kRu / chem->mw[i];
+      cpt += y[i] * cc;
+      cvt += y[i] * (cc - kRu / chem->mw[i]);
     }
     gamma = cpt / cvt;
   }
-  if (mach < 0 || pressure < 0 || temperature < 0) {
-    err = "reference_state struct '" + rs->second + "' needs mach, pressure and temperature on this path";
+  c = std::sqrt(gamma * kRu / mw * temperature);
+  const double velocity = mach * c;
+  bv[0] = pressure * mw / (kRu * temperature);
+  bv[1] = struct_real(st, "u", 1.0) * velocity;
+  bv[2] = struct_real(st, "v", 0.0) * velocity;
+  bv[3] = struct_real(st, "w", 0.0) * velocity;
+  bv[4] = pressure;
+  bv[5] = temperature;
+  return true;
+}
+
+bool reference_scales(const Setup &s, const ChemTables *chem, double &eps_scale, double &v_ref, std::string &err) {
+  eps_scale = 0;
+  v_ref = 0;
+  auto rs = s.strings.find("reference_state");
+  if (rs == s.strings.end()) return true;
+  double bv[6], c;
+  std::vector<double> y;
+  if (!inflow_state(s, rs->second, chem, bv, y, c, err)) {
+    err = "reference_state: " + err;
     return false;
   }
-  const double c = std::sqrt(gamma * kRu / mw * temperature);
-  const double velocity = mach * c;
-  const double density = pressure * mw / (kRu * temperature);
-  v_ref = std::abs(velocity) < 1 ? c : velocity;
-  eps_scale = density * v_ref * density * v_ref;
+  // the reference state (BoundCond.cpp:299-305): v_inf = |V|, or c when |V| < 1
+  const double velocity = std::sqrt(bv[1] * bv[1] + bv[2] * bv[2] + bv[3] * bv[3]);
+  const auto &st = s.structs.at(rs->second);
+  const double vmag = struct_real(st, "mach", -1) * c;  // Inflow's `velocity` member
+  (void)velocity;
+  v_ref = std::abs(vmag) < 1 ? c : vmag;
+  eps_scale = bv[0] * v_ref * bv[0] * v_ref;
   return true;
 }
 

@@ -90,7 +90,9 @@ struct BcFace {
   double acoustic_speed = 0, gamma = kGammaAir, entropy = 0, mw = kMwAir;
 };
 
-// One 1:1 block interface after InnerFace::register_boundary (Mesh.cpp:34-176).
+// One 1:1 block interface after InnerFace::register_boundary (Mesh.cpp:34-176): the node range of
+// this block it writes (the coincident face plus ngg ghost layers), the matching start in the target
+// block, and the index map src_tar / loop directions between the two.
 struct InnerFace {
   int rs[3]{}, re[3]{};
   int face = 0, direction = 1;
@@ -98,6 +100,7 @@ struct InnerFace {
   int target_block = 0, target_face = 0, target_direction = 1;
   int src_tar[3]{};
   int loop_dir[3]{1, 1, 1}, target_loop_dir[3]{1, 1, 1};
+  int n_point[3]{1, 1, 1};
 };
 
 struct HostBlock {
@@ -132,6 +135,10 @@ bool resolve_boundaries(const Setup &s, const Derived &d, HostMesh &mesh, std::s
 // rho_inf^2 v_inf^2 and v_inf of the struct named by reference_state (0, 0 without one): the scales of
 // the flux-split WENO epsilon (DParameter.cu:26-29, WENO.cu:1466-1473).
 bool reference_scales(const Setup &s, const ChemTables *chem, double &eps_scale, double &v_ref, std::string &err);
+// The state (rho, u, v, w, p, T; mass fractions y, acoustic speed c) of a plain inflow struct, as the
+// reference's default initialisation fills every node of a block with it (Field.cu:316-345).
+bool inflow_state(const Setup &s, const std::string &name, const ChemTables *chem, double bv[6],
+                  std::vector<double> &y, double &c, std::string &err);
 // Order in which faces are applied each stage (BoundCond.cuh:1488-1679): a list of (block, face).
 std::vector<std::pair<int, int>> bc_order(const Setup &s, const HostMesh &mesh);
 

@@ -13,6 +13,13 @@ constexpr int kMR = 64;  // reaction capacity
 constexpr int kMV = 5 + kMS;
 constexpr double kPatmD = 101325.0;
 
+// Species count as a compile-time constant: NS > 0 instantiates for exactly NS species (arrays in
+// registers, loops unrolled); NS = 0 is the generic build that reads the count from the tables.
+template <int NS> struct Spec {
+  static constexpr int A = NS > 0 ? NS : kMS;  // array extent
+};
+#define OSTC_NS (NS > 0 ? NS : c_mix.ns)
+
 struct MixTables {
   int ns, nr;
   int use_gibbs;  // some reaction takes kb from the equilibrium constant (backward_reaction_rate's n_gibbs)
@@ -32,9 +39,11 @@ __constant__ MixTables c_mix;
 
 // compute_enthalpy_and_cp (Thermo.cu:136-192): h_k and cp_k in J/kg, linear h extrapolation below
 // t_low.  Either output may be null (compute_enthalpy / compute_cp).
+template <int NS>
 __device__ __forceinline__ void mix_h_cp(double t, double *h, double *cp) {
   const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t5 = t4 * t;
-  for (int i = 0; i < c_mix.ns; ++i) {
+#pragma unroll
+  for (int i = 0; i < OSTC_NS; ++i) {
     double hh, cc;
     if (t < c_mix.t_low[i]) {
       const double tt = c_mix.t_low[i], tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tt5 = tt4 * tt;
@@ -53,9 +62,11 @@ __device__ __forceinline__ void mix_h_cp(double t, double *h, double *cp) {
 }
 
 // compute_gibbs_div_rt (Thermo.cu:194-210)
+template <int NS>
 __device__ __forceinline__ void mix_gibbs_rt(double t, double *g) {
   const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, ti = 1 / t, lt = log(t);
-  for (int i = 0; i < c_mix.ns; ++i) {
+#pragma unroll
+  for (int i = 0; i < OSTC_NS; ++i) {
     if (t < c_mix.t_low[i]) {
       const double tt = c_mix.t_low[i], tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tti = 1 / tt, ltt = log(tt);
       const double *a = c_mix.low[i];
@@ -72,11 +83,12 @@ __device__ __forceinline__ void mix_gibbs_rt(double t, double *g) {
 // Node properties of update_physical_properties<mixture> (FieldOperation.cuh:116-134) with
 // compute_transport_property (Transport.cu:43-136): cp, gamma, acoustic speed, Wilke viscosity,
 // Eucken-type conductivity and mixture-averaged rho*D_k (outputs written through the pointers).
+template <int NS>
 __device__ __forceinline__ void mix_properties(double rho, double p, double t, const double *y, double &gamma,
                                                double &acoustic, double &mu, double &cond, double *rhod) {
-  const int ns = c_mix.ns;
-  double cp[kMS];
-  mix_h_cp(t, nullptr, cp);
+  const int ns = OSTC_NS;
+  double cp[Spec<NS>::A];
+  mix_h_cp<NS>(t, nullptr, cp);
   double mw = 0, cpt = 0, cvt = 0;
   for (int l = 0; l < ns; ++l) {
     mw += y[l] * c_mix.imw[l];
@@ -86,7 +98,7 @@ __device__ __forceinline__ void mix_properties(double rho, double p, double t, c
   mw = 1 / mw;
   gamma = cpt / cvt;
   acoustic = sqrt(gamma * kRuD * t / mw);
-  double X[kMS], vis[kMS];
+  double X[Spec<NS>::A], vis[Spec<NS>::A];
   const double st = sqrt(t);
   for (int l = 0; l < ns; ++l) {
     X[l] = y[l] * mw * c_mix.imw[l];
@@ -131,17 +143,18 @@ __device__ __forceinline__ void mix_properties(double rho, double p, double t, c
 
 // compute_temperature_and_pressure (FieldOperation.cu:3-40): Newton on e(T) starting from t, relative
 // tolerance 1e-3, at most 1000 iterations.  Returns T; p = rho R T through pout.
+template <int NS>
 __device__ __forceinline__ double mix_temperature(double rho, double e, double t, const double *y, double &pout) {
-  const int ns = c_mix.ns;
+  const int ns = OSTC_NS;
   double mw = 0;
   for (int l = 0; l < ns; ++l) mw += y[l] * c_mix.imw[l];
   mw = 1 / mw;
   const double gc = kRuD / mw;
   double err = 1;
   int iter = 0;
-  double h[kMS], cp[kMS];
+  double h[Spec<NS>::A], cp[Spec<NS>::A];
   while (err > 1e-3 && iter++ < 1000) {
-    mix_h_cp(t, h, cp);
+    mix_h_cp<NS>(t, h, cp);
     double cpt = 0, hm = 0;
     for (int l = 0; l < ns; ++l) {
       cpt += cp[l] * y[l];
@@ -156,18 +169,20 @@ __device__ __forceinline__ double mix_temperature(double rho, double e, double t
 }
 
 __device__ __forceinline__ double arrhenius(double t, double A, double b, double Ea) {
-  return A * pow(t, b) * exp(-Ea / t);
+  // pow(t, 0) is exactly 1: temperature-independent prefactors skip the pow
+  return A * (b == 0.0 ? 1.0 : pow(t, b)) * exp(-Ea / t);
 }
 
 // finite_rate_chemistry (FiniteRateChem.cu:7-58, rates :60-195): omega_k in kg/(m^3 s) at one node.
+template <int NS>
 __device__ __forceinline__ void mix_chemistry(double rho, double t, const double *y, double *omega) {
-  const int ns = c_mix.ns, nr = c_mix.nr;
-  double c[kMS];
+  const int ns = OSTC_NS, nr = c_mix.nr;
+  double c[Spec<NS>::A];
   for (int l = 0; l < ns; ++l) c[l] = rho * y[l] * c_mix.imw[l] * 1e-3;
-  double g[kMS];
+  double g[Spec<NS>::A];
   bool gibbs = false;
   for (int l = 0; l < ns; ++l) omega[l] = 0;
-  double cre[kMS], des[kMS];
+  double cre[Spec<NS>::A], des[Spec<NS>::A];
   for (int l = 0; l < ns; ++l) cre[l] = des[l] = 0;
   for (int r = 0; r < nr; ++r) {
     const int ty = c_mix.label[r];
@@ -203,7 +218,7 @@ __device__ __forceinline__ void mix_chemistry(double rho, double t, const double
       kb = 0;
     } else if (ty != 2 && c_mix.use_gibbs) {
       if (!gibbs) {
-        mix_gibbs_rt(t, g);
+        mix_gibbs_rt<NS>(t, g);
         gibbs = true;
       }
       double dg = 0;
@@ -215,13 +230,25 @@ __device__ __forceinline__ void mix_chemistry(double rho, double t, const double
       kb = arrhenius(t, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
       if (ty == 4) kb *= cc;
     }
+    // concentration products: integer powers as products (pow(c, 1) = c, pow(c, 2) = c*c to within
+    // the rounding of pow itself), pow only for higher orders
     double q1 = 1.0, q2 = ty != 0 ? 1.0 : 0.0;
+#pragma unroll
     for (int l = 0; l < ns; ++l) {
-      if (c_mix.stoi_f[r][l]) q1 *= pow(c[l], (double)c_mix.stoi_f[r][l]);
+      const int nf = c_mix.stoi_f[r][l];
+      if (nf == 1) q1 *= c[l];
+      else if (nf == 2) q1 *= c[l] * c[l];
+      else if (nf) q1 *= pow(c[l], (double)nf);
     }
-    if (ty != 0)
-      for (int l = 0; l < ns; ++l)
-        if (c_mix.stoi_b[r][l]) q2 *= pow(c[l], (double)c_mix.stoi_b[r][l]);
+    if (ty != 0) {
+#pragma unroll
+      for (int l = 0; l < ns; ++l) {
+        const int nb = c_mix.stoi_b[r][l];
+        if (nb == 1) q2 *= c[l];
+        else if (nb == 2) q2 *= c[l] * c[l];
+        else if (nb) q2 *= pow(c[l], (double)nb);
+      }
+    }
     q1 *= kf;
     if (ty != 0) q2 *= kb;
     for (int l = 0; l < ns; ++l) {

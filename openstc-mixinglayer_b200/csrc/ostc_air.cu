@@ -52,6 +52,16 @@ struct DevFace {
   double density, u, v, w, pressure, temperature, acoustic_speed, gamma, entropy;
 };
 
+struct FillVals {
+  double val[16];
+};
+
+// One block interface (InnerFace after register_boundary, Mesh.cpp:38-141).
+struct DevInner {
+  int rs[3], ts[3], loop_dir[3], target_loop_dir[3], src_tar[3], n_point[3];
+  int face, direction, face_index;  // face_index: the coincident node layer along `face`
+};
+
 __device__ __forceinline__ void cv_from_bv_node(const DevBlock &b, DevState s, long long p) {
   // compute_cv_from_bv_1_point + compute_total_energy<Air> (FieldOperation.cuh:17-38,78-105)
   const long long P = b.plane;
@@ -746,7 +756,7 @@ __device__ __forceinline__ void copy_bv(const DevBlock &b, DevState s, long long
 __device__ __forceinline__ void finish_node(const DevBlock &b, DevState s, long long p) {
   if (s.sv) {
     // mixtures: properties of the ghost come from the properties sweep over the padded block
-    mix_cv_from_bv_node(b, s, p);
+    mix_cv_from_bv_node<0>(b, s, p);
     return;
   }
   cv_from_bv_node(b, s, p);
@@ -880,7 +890,74 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
   }
 }
 
+// inner_communication (DataCommunication.cuh:60-105): on the coincident face layer both blocks take
+// the average of their values; the ngg layers beyond it take the neighbour's interior values; every
+// written node gets its conservative variables (and, for air, its viscosity) again.
+__global__ void __launch_bounds__(128) k_inner_face(DevBlock b, DevState s, DevBlock tb, DevState ts, DevInner f) {
+  const long long tot = (long long)f.n_point[0] * f.n_point[1] * f.n_point[2];
+  const long long P = b.plane, TP = tb.plane;
+  const int ns = s.sv ? c_mix.ns : 0;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < tot; n += (long long)gridDim.x * blockDim.x) {
+    const int n0 = (int)(n % f.n_point[0]);
+    const long long r = n / f.n_point[0];
+    const int n1 = (int)(r % f.n_point[1]), n2 = (int)(r / f.n_point[1]);
+    const int d_idx[3] = {f.loop_dir[0] * n0, f.loop_dir[1] * n1, f.loop_dir[2] * n2};
+    const int idx[3] = {f.rs[0] + d_idx[0], f.rs[1] + d_idx[1], f.rs[2] + d_idx[2]};
+    int it[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) it[q] = f.ts[q] + f.target_loop_dir[q] * d_idx[f.src_tar[q]];
+    const long long p = b.id(idx[0], idx[1], idx[2]);
+    const long long pt = tb.id(it[0], it[1], it[2]);
+    if (idx[f.face] == f.face_index) {
+#pragma unroll
+      for (int l = 0; l < 6; ++l) {
+        const double ave = 0.5 * (ts.bv[l * TP + pt] + s.bv[l * P + p]);
+        s.bv[l * P + p] = ave;
+        ts.bv[l * TP + pt] = ave;
+      }
+      for (int l = 0; l < ns; ++l) {
+        const double ave = 0.5 * (ts.sv[l * TP + pt] + s.sv[l * P + p]);
+        s.sv[l * P + p] = ave;
+        ts.sv[l * TP + pt] = ave;
+      }
+    } else {
+#pragma unroll
+      for (int l = 0; l < 6; ++l) s.bv[l * P + p] = ts.bv[l * TP + pt];
+      for (int l = 0; l < ns; ++l) s.sv[l * P + p] = ts.sv[l * TP + pt];
+    }
+    finish_node(b, s, p);
+  }
+}
+
+// The reference updates one state in place, so when a stage's boundary faces run, the ghost layers an
+// interface fills still hold the previous stage's exchanged values, and faces that reach into them
+// (tangential ranges include the ghost layers) read those.  Stages here write a fresh buffer: carry
+// the interface ghost layers (not the coincident face, which the update rewrote) from the stage input.
+__global__ void __launch_bounds__(128) k_inner_carry(DevBlock b, DevState in, DevState out, DevInner f) {
+  const long long tot = (long long)f.n_point[0] * f.n_point[1] * f.n_point[2];
+  const long long P = b.plane;
+  const int ns = out.sv ? c_mix.ns : 0;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < tot; n += (long long)gridDim.x * blockDim.x) {
+    const int n0 = (int)(n % f.n_point[0]);
+    const long long r = n / f.n_point[0];
+    const int n1 = (int)(r % f.n_point[1]), n2 = (int)(r / f.n_point[1]);
+    const int idx[3] = {f.rs[0] + f.loop_dir[0] * n0, f.rs[1] + f.loop_dir[1] * n1, f.rs[2] + f.loop_dir[2] * n2};
+    if (idx[f.face] == f.face_index) continue;
+    const long long p = b.id(idx[0], idx[1], idx[2]);
+#pragma unroll
+    for (int l = 0; l < 6; ++l) out.bv[l * P + p] = in.bv[l * P + p];
+    for (int l = 0; l < ns; ++l) out.sv[l * P + p] = in.sv[l * P + p];
+  }
+}
+
 // ------------------------------------------------------------------------------ set-up kernels
+
+// every padded node of planes dst[0..nv) set to val[l]
+__global__ void k_fill_planes(long long plane, double *__restrict__ dst, int nv, FillVals v) {
+  const long long tot = plane * nv;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < tot; n += (long long)gridDim.x * blockDim.x)
+    dst[n] = v.val[n / plane];
+}
 
 // interior [nv][N] (i fastest) <-> padded planes
 __global__ void k_scatter(DevBlock b, const double *__restrict__ src, double *__restrict__ dst, int nv) {
@@ -986,6 +1063,8 @@ struct BlockRes {
   double *dq = nullptr;
   double *last = nullptr;
   std::vector<DevFace> faces;  // file order
+  std::vector<DevInner> inner;  // interfaces of this block, file order
+  std::vector<int> inner_target;
 };
 
 struct ostc_ctx {
@@ -996,6 +1075,11 @@ struct ostc_ctx {
   int nv = 5;
   ChemTables chem;
   MixTables mixtab{};
+  // default initialisation of every node (ghosts included) before the interior state is set
+  // (Field::initialize_basic_variables with the default_init struct, Field.cu:316-345, 388-470)
+  bool has_init = false;
+  double init_bv[6]{};
+  std::vector<double> init_sv;
   cudaStream_t stream = nullptr;
   Setup setup;
   Derived der;
@@ -1128,31 +1212,33 @@ void launch_flux_pv(ostc_ctx *ctx, BlockRes &B, DevState in) {
 }
 
 // flux-split WENO7 sweeps (inviscid_type 3, schemes 71 / 72), accumulating into dq
-void launch_fvs(ostc_ctx *ctx, BlockRes &B, DevState in) {
+template <int NS>
+void launch_fvs_t(ostc_ctx *ctx, BlockRes &B, DevState in) {
   const DevBlock &b = B.db;
   const int nv = ctx->nv, sch = ctx->der.inviscid_scheme;
   {
     long tok = begin_t(ctx, "flux_x");
     dim3 grid((b.mx + FvsTile<0>::TD - 2) / (FvsTile<0>::TD - 1), b.my, b.mz);
-    k_fvs<0><<<grid, FvsTile<0>::TD, fvs_smem_bytes<0>(nv), ctx->stream>>>(b, in, B.dq, nv, sch);
+    k_fvs<0, NS><<<grid, FvsTile<0>::TD, fvs_smem_bytes<0>(nv), ctx->stream>>>(b, in, B.dq, nv, sch);
     end_t(ctx, tok);
   }
   {
     long tok = begin_t(ctx, "flux_y");
     dim3 grid((b.mx + FvsTile<1>::TXL - 1) / FvsTile<1>::TXL, (b.my + FvsTile<1>::TD - 2) / (FvsTile<1>::TD - 1), b.mz);
-    k_fvs<1><<<grid, dim3(FvsTile<1>::TXL, FvsTile<1>::TD), fvs_smem_bytes<1>(nv), ctx->stream>>>(b, in, B.dq, nv, sch);
+    k_fvs<1, NS><<<grid, dim3(FvsTile<1>::TXL, FvsTile<1>::TD), fvs_smem_bytes<1>(nv), ctx->stream>>>(b, in, B.dq, nv, sch);
     end_t(ctx, tok);
   }
   if (b.mz > 1) {
     long tok = begin_t(ctx, "flux_z");
     dim3 grid((b.mx + FvsTile<2>::TXL - 1) / FvsTile<2>::TXL, (b.mz + FvsTile<2>::TD - 2) / (FvsTile<2>::TD - 1), b.my);
-    k_fvs<2><<<grid, dim3(FvsTile<2>::TXL, FvsTile<2>::TD), fvs_smem_bytes<2>(nv), ctx->stream>>>(b, in, B.dq, nv, sch);
+    k_fvs<2, NS><<<grid, dim3(FvsTile<2>::TXL, FvsTile<2>::TD), fvs_smem_bytes<2>(nv), ctx->stream>>>(b, in, B.dq, nv, sch);
     end_t(ctx, tok);
   }
 }
 
 // mixture viscous sweeps, accumulating into dq
-void launch_mix_visc(ostc_ctx *ctx, BlockRes &B, DevState in) {
+template <int NS>
+void launch_mix_visc_t(ostc_ctx *ctx, BlockRes &B, DevState in) {
   const DevBlock &b = B.db;
   const int nv = ctx->nv;
   const bool is3d = b.mz > 1;
@@ -1160,22 +1246,47 @@ void launch_mix_visc(ostc_ctx *ctx, BlockRes &B, DevState in) {
   {
     dim3 grid((b.mx + FvsTile<0>::TD - 2) / (FvsTile<0>::TD - 1), b.my, b.mz);
     const size_t sm = (size_t)FvsTile<0>::TD * nv * sizeof(double);
-    if (is3d) k_mix_visc<0, true><<<grid, FvsTile<0>::TD, sm, ctx->stream>>>(b, in, B.dq, nv);
-    else k_mix_visc<0, false><<<grid, FvsTile<0>::TD, sm, ctx->stream>>>(b, in, B.dq, nv);
+    if (is3d) k_mix_visc<0, true, NS><<<grid, FvsTile<0>::TD, sm, ctx->stream>>>(b, in, B.dq, nv);
+    else k_mix_visc<0, false, NS><<<grid, FvsTile<0>::TD, sm, ctx->stream>>>(b, in, B.dq, nv);
   }
   {
     dim3 grid((b.mx + FvsTile<1>::TXL - 1) / FvsTile<1>::TXL, (b.my + FvsTile<1>::TD - 2) / (FvsTile<1>::TD - 1), b.mz);
     const size_t sm = (size_t)FvsTile<1>::TD * FvsTile<1>::TXL * nv * sizeof(double);
     dim3 blk(FvsTile<1>::TXL, FvsTile<1>::TD);
-    if (is3d) k_mix_visc<1, true><<<grid, blk, sm, ctx->stream>>>(b, in, B.dq, nv);
-    else k_mix_visc<1, false><<<grid, blk, sm, ctx->stream>>>(b, in, B.dq, nv);
+    if (is3d) k_mix_visc<1, true, NS><<<grid, blk, sm, ctx->stream>>>(b, in, B.dq, nv);
+    else k_mix_visc<1, false, NS><<<grid, blk, sm, ctx->stream>>>(b, in, B.dq, nv);
   }
   if (is3d) {
     dim3 grid((b.mx + FvsTile<2>::TXL - 1) / FvsTile<2>::TXL, (b.mz + FvsTile<2>::TD - 2) / (FvsTile<2>::TD - 1), b.my);
     const size_t sm = (size_t)FvsTile<2>::TD * FvsTile<2>::TXL * nv * sizeof(double);
-    k_mix_visc<2, true><<<grid, dim3(FvsTile<2>::TXL, FvsTile<2>::TD), sm, ctx->stream>>>(b, in, B.dq, nv);
+    k_mix_visc<2, true, NS><<<grid, dim3(FvsTile<2>::TXL, FvsTile<2>::TD), sm, ctx->stream>>>(b, in, B.dq, nv);
   }
   end_t(ctx, tok);
+}
+
+// The H2/air mechanism's 9 species get a dedicated instantiation; other counts the generic one.
+constexpr int kFixedNS = 9;
+void launch_fvs(ostc_ctx *ctx, BlockRes &B, DevState in) {
+  if (ctx->der.n_spec == kFixedNS) launch_fvs_t<kFixedNS>(ctx, B, in);
+  else launch_fvs_t<0>(ctx, B, in);
+}
+void launch_mix_visc(ostc_ctx *ctx, BlockRes &B, DevState in) {
+  if (ctx->der.n_spec == kFixedNS) launch_mix_visc_t<kFixedNS>(ctx, B, in);
+  else launch_mix_visc_t<0>(ctx, B, in);
+}
+template <int NS>
+void launch_mix_source_t(ostc_ctx *ctx, BlockRes &B, DevState in, bool chem) {
+  k_mix_source<NS><<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, in, B.dq, ctx->nv, chem ? 1 : 0);
+}
+void launch_mix_source(ostc_ctx *ctx, BlockRes &B, DevState in, bool chem) {
+  if (ctx->der.n_spec == kFixedNS) launch_mix_source_t<kFixedNS>(ctx, B, in, chem);
+  else launch_mix_source_t<0>(ctx, B, in, chem);
+}
+void launch_mix_props(ostc_ctx *ctx, BlockRes &B, DevState st) {
+  if (ctx->der.n_spec == kFixedNS)
+    k_mix_props<kFixedNS><<<grid_for(ctx, B.db.plane, 128), 128, 0, ctx->stream>>>(B.db, st);
+  else
+    k_mix_props<0><<<grid_for(ctx, B.db.plane, 128), 128, 0, ctx->stream>>>(B.db, st);
 }
 
 // inviscid sweep of one block
@@ -1269,6 +1380,13 @@ void launch_visc(ostc_ctx *ctx, BlockRes &B, const StageArgs &a) {
   end_t(ctx, tok);
 }
 
+void launch_carry(ostc_ctx *ctx, BlockRes &B, DevState in, DevState out) {
+  for (const auto &fi : B.inner) {
+    const long long tot = (long long)fi.n_point[0] * fi.n_point[1] * fi.n_point[2];
+    k_inner_carry<<<grid_for(ctx, tot, 128), 128, 0, ctx->stream>>>(B.db, in, out, fi);
+  }
+}
+
 void launch_bcs(ostc_ctx *ctx, int block, DevState out) {
   for (const auto &bf : ctx->order) {
     if (bf.first != block) continue;
@@ -1280,6 +1398,21 @@ void launch_bcs(ostc_ctx *ctx, int block, DevState out) {
     k_bc_face<<<grid_for(ctx, nn, 128), 128, 0, ctx->stream>>>(B.db, out, f);
     end_t(ctx, tok);
   }
+}
+
+DevState state_of(BlockRes &B, int s);
+
+// data_communication (DataCommunication.cuh:29-58): every interface of every block in file order.
+void launch_interfaces(ostc_ctx *ctx, int slot) {
+  for (auto &B : ctx->blk)
+    for (size_t f = 0; f < B.inner.size(); ++f) {
+      BlockRes &T = ctx->blk[B.inner_target[f]];
+      const DevInner &fi = B.inner[f];
+      const long long tot = (long long)fi.n_point[0] * fi.n_point[1] * fi.n_point[2];
+      long tok = begin_t(ctx, "interface");
+      k_inner_face<<<grid_for(ctx, tot, 128), 128, 0, ctx->stream>>>(B.db, state_of(B, slot), T.db, state_of(T, slot), fi);
+      end_t(ctx, tok);
+    }
 }
 
 DevState state_of(BlockRes &B, int s) {
@@ -1326,19 +1459,23 @@ bool set_mix_attrs(int nv) {
   auto set = [&](const void *fn, size_t bytes) {
     ok = ok && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess;
   };
-  set((const void *)k_fvs<0>, fvs_smem_bytes<0>(nv));
-  set((const void *)k_fvs<1>, fvs_smem_bytes<1>(nv));
-  set((const void *)k_fvs<2>, fvs_smem_bytes<2>(nv));
+  set((const void *)k_fvs<0, 0>, fvs_smem_bytes<0>(nv));
+  set((const void *)k_fvs<1, 0>, fvs_smem_bytes<1>(nv));
+  set((const void *)k_fvs<2, 0>, fvs_smem_bytes<2>(nv));
+  set((const void *)k_fvs<0, kFixedNS>, fvs_smem_bytes<0>(nv));
+  set((const void *)k_fvs<1, kFixedNS>, fvs_smem_bytes<1>(nv));
+  set((const void *)k_fvs<2, kFixedNS>, fvs_smem_bytes<2>(nv));
   return ok;
 }
 
 int initialise(ostc_ctx *ctx) {
   // Driver::initialize_computation (Driver.cu:115-199): BCs, properties, then cv <- bv (RK.cuh:37-45)
   for (size_t b = 0; b < ctx->blk.size(); ++b) launch_bcs(ctx, (int)b, state_of(ctx->blk[b], 0));
+  launch_interfaces(ctx, 0);
   for (auto &B : ctx->blk) {
     if (ctx->mixture) {
-      k_mix_props<<<grid_for(ctx, B.db.plane, 128), 128, 0, ctx->stream>>>(B.db, state_of(B, 0));
-      k_mix_init_cv<<<grid_for(ctx, B.db.plane, 128), 128, 0, ctx->stream>>>(B.db, state_of(B, 0));
+      launch_mix_props(ctx, B, state_of(B, 0));
+      k_mix_init_cv<0><<<grid_for(ctx, B.db.plane, 128), 128, 0, ctx->stream>>>(B.db, state_of(B, 0));
     } else {
       k_init_fields<<<grid_for(ctx, B.db.plane, 256), 256, 0, ctx->stream>>>(B.db, state_of(B, 0));
     }
@@ -1380,8 +1517,10 @@ int enqueue_step(ostc_ctx *ctx) {
       a.update = 1;
       a.flags = ctx->d_flags;
       launch_visc<T>(ctx, B, a);
+      launch_carry(ctx, B, state_of(B, sin), state_of(B, sout));
       launch_bcs(ctx, (int)bi, state_of(B, sout));
     }
+    launch_interfaces(ctx, sout);
   }
   k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->d_time, ctx->d_dt, ctx->d_step);
   return OSTC_OK;
@@ -1409,24 +1548,29 @@ int enqueue_step_mix(ostc_ctx *ctx) {
       const DevState in = state_of(B, sin);
       {
         long tok = begin_t(ctx, "source");
-        k_mix_source<<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, in, B.dq, nv, ctx->der.reaction == 1);
+        launch_mix_source(ctx, B, in, ctx->der.reaction == 1);
         end_t(ctx, tok);
       }
       launch_fvs(ctx, B, in);
       if (ctx->der.viscous_order != 0) launch_mix_visc(ctx, B, in);
       {
         long tok = begin_t(ctx, "update");
-        k_mix_update<<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, in, state_of(B, 0), state_of(B, sout),
-                                                                          B.dq, ctx->d_dt, A[rk], Bc[rk], C[rk], nv,
-                                                                          ctx->d_flags);
+        if (ctx->der.n_spec == kFixedNS)
+          k_mix_update<kFixedNS><<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(
+              B.db, in, state_of(B, 0), state_of(B, sout), B.dq, ctx->d_dt, A[rk], Bc[rk], C[rk], nv, ctx->d_flags);
+        else
+          k_mix_update<0><<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(
+              B.db, in, state_of(B, 0), state_of(B, sout), B.dq, ctx->d_dt, A[rk], Bc[rk], C[rk], nv, ctx->d_flags);
         end_t(ctx, tok);
       }
+      launch_carry(ctx, B, in, state_of(B, sout));
       launch_bcs(ctx, (int)bi, state_of(B, sout));
-      {
-        long tok = begin_t(ctx, "properties");
-        k_mix_props<<<grid_for(ctx, B.db.plane, 128), 128, 0, ctx->stream>>>(B.db, state_of(B, sout));
-        end_t(ctx, tok);
-      }
+    }
+    launch_interfaces(ctx, sout);
+    for (auto &B : ctx->blk) {
+      long tok = begin_t(ctx, "properties");
+      launch_mix_props(ctx, B, state_of(B, sout));
+      end_t(ctx, tok);
     }
   }
   k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->d_time, ctx->d_dt, ctx->d_step);
@@ -1555,6 +1699,15 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
     }
   }
   ctx->tables = ctx->mixture || ctx->der.inviscid_type == 3;
+  {
+    auto di = ctx->setup.strings.find("default_init");
+    if (di != ctx->setup.strings.end() && ctx->setup.structs.count(di->second)) {
+      double c;
+      std::string e2;
+      ctx->has_init = inflow_state(ctx->setup, di->second, ctx->mixture ? &ctx->chem : nullptr, ctx->init_bv,
+                                   ctx->init_sv, c, e2);
+    }
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
     g_create_error = "no CUDA device " + std::to_string(device) + " available";
@@ -1647,6 +1800,23 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
       f.gamma = hf.gamma;
       f.entropy = hf.entropy;
       R.faces.push_back(f);
+    }
+    for (auto &hi : HB.inner) {
+      DevInner fi{};
+      for (int q = 0; q < 3; ++q) {
+        fi.rs[q] = hi.rs[q];
+        fi.ts[q] = hi.ts[q];
+        fi.loop_dir[q] = hi.loop_dir[q];
+        fi.target_loop_dir[q] = hi.target_loop_dir[q];
+        fi.src_tar[q] = hi.src_tar[q];
+        fi.n_point[q] = hi.n_point[q];
+      }
+      fi.face = hi.face;
+      fi.direction = hi.direction;
+      // the coincident layer: the start of a high-side range, the end of a low-side one
+      fi.face_index = hi.direction > 0 ? hi.rs[hi.face] : hi.re[hi.face];
+      R.inner.push_back(fi);
+      R.inner_target.push_back(hi.target_block);
     }
     ctx->blk.push_back(R);
   }
@@ -1772,14 +1942,27 @@ int ostc_set_state(ostc_ctx *ctx, int block, const double *bv, const double *sv,
   const auto kind = ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   const size_t bytes = 6 * (size_t)B.db.n * sizeof(double);
   CK(cudaMemcpyAsync(ctx->d_staging, bv, bytes, kind, ctx->stream));
-  // buffer A holds the new state; every ghost node is rewritten by the boundary faces before use
-  CK(cudaMemsetAsync(B.bv[0], 0, 6 * B.db.plane * sizeof(double), ctx->stream));
+  // buffer A holds the new state; ghost nodes start from the default initialisation (or zero) and
+  // are rewritten by the boundary faces and interfaces
+  if (ctx->has_init) {
+    FillVals fv{};
+    for (int l = 0; l < 6; ++l) fv.val[l] = ctx->init_bv[l];
+    k_fill_planes<<<grid_for(ctx, 6 * B.db.plane, 256), 256, 0, ctx->stream>>>(B.db.plane, B.bv[0], 6, fv);
+  } else {
+    CK(cudaMemsetAsync(B.bv[0], 0, 6 * B.db.plane * sizeof(double), ctx->stream));
+  }
   CK(cudaMemsetAsync(B.cv[0], 0, (size_t)ctx->nv * B.db.plane * sizeof(double), ctx->stream));
   CK(cudaMemsetAsync(B.mul[0], 0, B.db.plane * sizeof(double), ctx->stream));
   k_scatter<<<grid_for(ctx, 6 * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, ctx->d_staging, B.bv[0], 6);
   if (ctx->mixture) {
     const int ns = ctx->der.n_spec;
-    CK(cudaMemsetAsync(B.sv[0], 0, (size_t)ns * B.db.plane * sizeof(double), ctx->stream));
+    if (ctx->has_init && (int)ctx->init_sv.size() == ns && ns <= 16) {
+      FillVals fv{};
+      for (int l = 0; l < ns; ++l) fv.val[l] = ctx->init_sv[l];
+      k_fill_planes<<<grid_for(ctx, ns * B.db.plane, 256), 256, 0, ctx->stream>>>(B.db.plane, B.sv[0], ns, fv);
+    } else {
+      CK(cudaMemsetAsync(B.sv[0], 0, (size_t)ns * B.db.plane * sizeof(double), ctx->stream));
+    }
     CK(cudaMemcpyAsync(ctx->d_staging, sv, (size_t)ns * B.db.n * sizeof(double), kind, ctx->stream));
     k_scatter<<<grid_for(ctx, ns * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, ctx->d_staging, B.sv[0], ns);
   }
@@ -1828,8 +2011,7 @@ int ostc_rhs(ostc_ctx *ctx, int block, unsigned mask, double *dq, int ptr_kind) 
   if (ctx->mixture) {
     // source (dq initialised by it, RK.cuh:116), flux-split WENO7, viscous
     const DevState in = state_of(B, 0);
-    k_mix_source<<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, in, B.dq, nv,
-                                                                      (mask & OSTC_TERM_SOURCE) && ctx->der.reaction == 1);
+    launch_mix_source(ctx, B, in, (mask & OSTC_TERM_SOURCE) && ctx->der.reaction == 1);
     if (mask & OSTC_TERM_INVISCID) launch_fvs(ctx, B, in);
     if ((mask & OSTC_TERM_VISCOUS) && ctx->der.viscous_order != 0) launch_mix_visc(ctx, B, in);
     CK(cudaGetLastError());

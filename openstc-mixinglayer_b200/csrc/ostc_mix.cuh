@@ -10,16 +10,17 @@
 namespace ostc {
 
 // compute_cv_from_bv_1_point<mixture> (FieldOperation.cuh:78-105, total energy :17-32)
+template <int NS>
 __device__ __forceinline__ void mix_cv_from_bv_node(const DevBlock &b, const DevState &s, long long p) {
   const long long P = b.plane;
-  const int ns = c_mix.ns;
+  const int ns = OSTC_NS;
   const double rho = s.bv[p], u = s.bv[P + p], v = s.bv[2 * P + p], w = s.bv[3 * P + p];
   s.cv[p] = rho;
   s.cv[P + p] = rho * u;
   s.cv[2 * P + p] = rho * v;
   s.cv[3 * P + p] = rho * w;
-  double h[kMS];
-  mix_h_cp(s.bv[5 * P + p], h, nullptr);
+  double h[Spec<NS>::A];
+  mix_h_cp<NS>(s.bv[5 * P + p], h, nullptr);
   double te = 0.5 * (u * u + v * v + w * w);
   for (int l = 0; l < ns; ++l) {
     const double y = s.sv[l * P + p];
@@ -32,16 +33,17 @@ __device__ __forceinline__ void mix_cv_from_bv_node(const DevBlock &b, const Dev
 }
 
 // update_physical_properties<mixture> over every padded node (FieldOperation.cuh:107-134)
+template <int NS>
 __global__ void __launch_bounds__(128) k_mix_props(DevBlock b, DevState s) {
   const long long P = b.plane;
-  const int ns = c_mix.ns;
+  const int ns = OSTC_NS;
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
     const double rho = s.bv[p];
     if (!(rho > 0)) continue;  // padding columns of the row pitch carry no state
-    double y[kMS], rd[kMS];
+    double y[Spec<NS>::A], rd[Spec<NS>::A];
     for (int l = 0; l < ns; ++l) y[l] = s.sv[l * P + p];
     double g, a, mu, cd;
-    mix_properties(rho, s.bv[4 * P + p], s.bv[5 * P + p], y, g, a, mu, cd, rd);
+    mix_properties<NS>(rho, s.bv[4 * P + p], s.bv[5 * P + p], y, g, a, mu, cd, rd);
     s.gam[p] = g;
     s.acs[p] = a;
     s.mul[p] = mu;
@@ -51,17 +53,20 @@ __global__ void __launch_bounds__(128) k_mix_props(DevBlock b, DevState s) {
 }
 
 // conservative variables from bv and sv over the padded block (initialisation, RK.cuh:37-45)
+template <int NS>
 __global__ void k_mix_init_cv(DevBlock b, DevState s) {
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < b.plane; p += (long long)gridDim.x * blockDim.x)
-    if (s.bv[p] > 0) mix_cv_from_bv_node(b, s, p);
+    if (s.bv[p] > 0) mix_cv_from_bv_node<NS>(b, s, p);
 }
 
 // compute_source<FR> (SourceTerm.cuh:11-35) as the first contribution to dq: dq[5+l] = J omega_l
 // (finite rate) or 0, dq[0..4] = 0.
+template <int NS>
 __global__ void __launch_bounds__(128) k_mix_source(DevBlock b, DevState s, double *__restrict__ dq, int nv,
                                                      int finite_rate) {
+  if (NS > 0) nv = 5 + NS;
   const long long P = b.plane;
-  const int ns = c_mix.ns;
+  const int ns = OSTC_NS;
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(n % b.mx);
     const long long r = n / b.mx;
@@ -69,9 +74,9 @@ __global__ void __launch_bounds__(128) k_mix_source(DevBlock b, DevState s, doub
     const long long p = b.id(i, j, k);
     for (int l = 0; l < 5; ++l) dq[l * b.n + n] = 0.0;
     if (finite_rate) {
-      double y[kMS], om[kMS];
+      double y[Spec<NS>::A], om[Spec<NS>::A];
       for (int l = 0; l < ns; ++l) y[l] = s.sv[l * P + p];
-      mix_chemistry(s.bv[p], s.bv[5 * P + p], y, om);
+      mix_chemistry<NS>(s.bv[p], s.bv[5 * P + p], y, om);
       const double jac = b.jac[p];
       for (int l = 0; l < ns; ++l) dq[(5 + l) * b.n + n] = jac * om[l];
     } else {
@@ -87,12 +92,12 @@ __global__ void __launch_bounds__(128) k_mix_source(DevBlock b, DevState s, doub
 template <int DIR> struct FvsTile {
   static constexpr int TXL = DIR == 0 ? 1 : 8;
   static constexpr int TD = DIR == 0 ? 128 : 16;
-  static constexpr int NS = TD + 7;  // staged nodes: stencils of 8 nodes around TD faces
+  static constexpr int NST = TD + 7;  // staged nodes: stencils of 8 nodes around TD faces
 };
 
 template <int DIR>
 __host__ __device__ constexpr size_t fvs_smem_bytes(int nv) {
-  return (size_t)FvsTile<DIR>::NS * FvsTile<DIR>::TXL * nv * 2 * sizeof(double);
+  return (size_t)FvsTile<DIR>::NST * FvsTile<DIR>::TXL * nv * 2 * sizeof(double);
 }
 
 // compute_convective_term_weno_x/_y/_z (WENO.cu:8-461) for inviscid_scheme 72 (characteristic,
@@ -100,17 +105,18 @@ __host__ __device__ constexpr size_t fvs_smem_bytes(int nv) {
 // compute_weno_flux_cp, :1455-1536).  Every node's split fluxes F+- (compute_flux, :697-720) are
 // computed once into shared memory; each thread then forms one face flux from the 8-node stencil,
 // and after a barrier the node threads difference neighbouring faces into dq.
-template <int DIR>
+template <int DIR, int NS>
 __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_fvs(DevBlock b, DevState s,
                                                                                double *__restrict__ dq, int nv,
                                                                                int scheme) {
-  constexpr int TXL = FvsTile<DIR>::TXL, TD = FvsTile<DIR>::TD, NS = FvsTile<DIR>::NS;
+  constexpr int TXL = FvsTile<DIR>::TXL, TD = FvsTile<DIR>::TD, NST = FvsTile<DIR>::NST;
   extern __shared__ double fsm[];
-  double *Fp = fsm;                       // [NS][TXL][nv]
-  double *Fm = fsm + NS * TXL * nv;       // [NS][TXL][nv]
+  double *Fp = fsm;                        // [NST][TXL][nv]
+  double *Fm = fsm + NST * TXL * nv;       // [NST][TXL][nv]
   const int lane = DIR == 0 ? 0 : (int)threadIdx.x;
   const int t = DIR == 0 ? (int)threadIdx.x : (int)threadIdx.y;
-  const int ns = c_mix.ns;
+  const int ns = OSTC_NS;
+  if (NS > 0) nv = 5 + NS;
   const long long P = b.plane;
   const int nd = DIR == 0 ? b.mx : DIR == 1 ? b.my : b.mz;
   const int start = (DIR == 0 ? blockIdx.x : blockIdx.y) * (TD - 1);
@@ -128,11 +134,11 @@ __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_fvs(De
   };
   // stage split fluxes of nodes start-4 .. start+TD+2
   if (lane_ok) {
-    for (int st = t; st < NS; st += TD) {
+    for (int st = t; st < NST; st += TD) {
       const int n = start - 4 + st;
       if (n > nd + 3) continue;
       const long long p = pid(n);
-      double Q[kMV];
+      double Q[Spec<NS>::A + 5];
       for (int l = 0; l < nv; ++l) Q[l] = s.cv[l * P + p];
       const double pk = s.bv[4 * P + p];
       const double c = s.acs ? s.acs[p] : sqrt(kGamma * (kRuD / kMwD) * s.bv[5 * P + p]);
@@ -162,7 +168,7 @@ __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_fvs(De
   __syncthreads();
   const int n = start - 1 + t;  // left node of this thread's face
   const bool face_ok = lane_ok && n < nd;
-  double fc[kMV];
+  double fc[Spec<NS>::A + 5];
   for (int l = 0; l < kMV; ++l) fc[l] = 0.0;
   auto FP = [&](int m, int l) -> double { return Fp[((long long)(t + m) * TXL + lane) * nv + l]; };
   auto FM = [&](int m, int l) -> double { return Fm[((long long)(t + m) * TXL + lane) * nv + l]; };
@@ -186,7 +192,7 @@ __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_fvs(De
   } else if (face_ok) {
     // Roe-averaged mixture eigensystem at the face (WENO.cu:747-821)
     const long long pl = pid(n), pr = pid(n + 1);
-    double cvl[kMV], cvr[kMV];
+    double cvl[Spec<NS>::A + 5], cvr[Spec<NS>::A + 5];
     for (int l = 0; l < nv; ++l) {
       cvl[l] = s.cv[l * P + pl];
       cvr[l] = s.cv[l * P + pr];
@@ -200,14 +206,14 @@ __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_fvs(De
     const double wm = rlc * cvl[3] * rli + rrc * cvr[3] * rri;
     const double ekm = 0.5 * (um * um + vm_ * vm_ + wm * wm);
     const double hm = rlc * ((cvl[4] + p_l) * rli) + rrc * ((cvr[4] + p_r) * rri);
-    double svm[kMS], hi[kMS], cpi[kMS], al[kMS];
+    double svm[Spec<NS>::A], hi[Spec<NS>::A], cpi[Spec<NS>::A], al[Spec<NS>::A];
     double mw_inv = 0;
     for (int l = 0; l < ns; ++l) {
       svm[l] = rlc * cvl[l + 5] * rli + rrc * cvr[l + 5] * rri;
       mw_inv += svm[l] / c_mix.mw[l];
     }
     const double tm = (rlc * (p_l * rli) + rrc * (p_r * rri)) / (kRuD * mw_inv);
-    mix_h_cp(tm, hi, cpi);
+    mix_h_cp<NS>(tm, hi, cpi);
     double cp = 0, cvt = 0;
     for (int l = 0; l < ns; ++l) {
       cp += svm[l] * cpi[l];
@@ -233,7 +239,7 @@ __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_fvs(De
       al[l] = gamma * kRuD / c_mix.mw[l] * tm - (gamma - 1) * hi[l];
       al[l] *= c2i;
     }
-    double fch[kMV];
+    double fch[Spec<NS>::A + 5];
     for (int l = 0; l < 5; ++l) {
       double cs = 0.5, L[5];
       if (l == 0) {
@@ -329,7 +335,7 @@ __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_fvs(De
 // compute_fv/gv/hv_2nd_order<mixture, Laminar> (ViscousScheme.cuh:24-318 and its y / z twins) at the
 // face between node p0 and its neighbour p0 + e[d]: stress, Fourier conduction with the mixture
 // conductivity, mixture-averaged species diffusion with the correction velocity and its enthalpy flux.
-template <bool DIM3>
+template <bool DIM3, int NS>
 __device__ __forceinline__ void mix_visc_face(const DevBlock &b, const DevState &s, long long p0, int d, int nv,
                                               double *fv) {
   const long long P = b.plane;
@@ -379,8 +385,8 @@ __device__ __forceinline__ void mix_visc_face(const DevBlock &b, const DevState 
   const double wm = 0.5 * (s.bv[3 * P + p0] + s.bv[3 * P + p1]);
   const double cond = 0.5 * (s.cond[p0] + s.cond[p1]);
   fv[4] = um * fv[1] + vm * fv[2] + wm * fv[3] + cond * (nx * gt[0] + ny * gt[1] + nz * gt[2]);
-  const int ns = c_mix.ns;
-  double dif[kMS], yk[kMS], ddf[kMS];
+  const int ns = OSTC_NS;
+  double dif[Spec<NS>::A], yk[Spec<NS>::A], ddf[Spec<NS>::A];
   double sgw = 0, srdy = 0, corr = 0, mwt = 0;
   for (int l = 0; l < ns; ++l) {
     const double *Y = s.sv + (long long)l * P;
@@ -397,8 +403,8 @@ __device__ __forceinline__ void mix_visc_face(const DevBlock &b, const DevState 
   }
   mwt = 1.0 / mwt;
   corr -= mwt * srdy * sgw;
-  double h[kMS];
-  mix_h_cp(0.5 * (s.bv[5 * P + p0] + s.bv[5 * P + p1]), h, nullptr);
+  double h[Spec<NS>::A];
+  mix_h_cp<NS>(0.5 * (s.bv[5 * P + p0] + s.bv[5 * P + p1]), h, nullptr);
   for (int l = 0; l < ns; ++l) {
     const double flux = dif[l] * (ddf[l] - mwt * yk[l] * sgw) - yk[l] * corr;
     fv[5 + l] = flux;
@@ -408,9 +414,10 @@ __device__ __forceinline__ void mix_visc_face(const DevBlock &b, const DevState 
 
 // viscous_flux_fv/gv/hv (SchemeSelector.cuh:69-154) for mixtures: one thread per face of the tile,
 // then dq += fv(i+1/2) - fv(i-1/2) through shared memory; tiles as the flux-split sweeps.
-template <int DIR, bool DIM3>
+template <int DIR, bool DIM3, int NS>
 __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_mix_visc(DevBlock b, DevState s,
                                                                                     double *__restrict__ dq, int nv) {
+  if (NS > 0) nv = 5 + NS;
   constexpr int TXL = FvsTile<DIR>::TXL, TD = FvsTile<DIR>::TD;
   extern __shared__ double fsm[];
   const int lane = DIR == 0 ? 0 : (int)threadIdx.x;
@@ -427,11 +434,11 @@ __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_mix_vi
   }
   const int n = start - 1 + t;
   const bool face_ok = i0 < b.mx && n < nd;
-  double fv[kMV];
+  double fv[Spec<NS>::A + 5];
   for (int l = 0; l < kMV; ++l) fv[l] = 0.0;
   if (face_ok) {
     const long long p0 = DIR == 0 ? b.id(n, j0, k0) : DIR == 1 ? b.id(i0, n, k0) : b.id(i0, j0, n);
-    mix_visc_face<DIM3>(b, s, p0, DIR, nv, fv);
+    mix_visc_face<DIM3, NS>(b, s, p0, DIR, nv, fv);
   }
   for (int l = 0; l < nv; ++l) fsm[((long long)t * TXL + lane) * nv + l] = fv[l];
   __syncthreads();
@@ -443,11 +450,13 @@ __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_mix_vi
 
 // update_cv_and_bv_rk<mixture> (RK.cuh:230-284) with compute_temperature_and_pressure
 // (FieldOperation.cu:3-40): the Newton iteration starts from the stage-input temperature.
+template <int NS>
 __global__ void __launch_bounds__(128) k_mix_update(DevBlock b, DevState in, DevState qn, DevState out,
                                                      const double *__restrict__ dq, const double *dtp, double ca,
                                                      double cb, double cc, int nv, unsigned *flags) {
+  if (NS > 0) nv = 5 + NS;
   const long long P = b.plane;
-  const int ns = c_mix.ns;
+  const int ns = OSTC_NS;
   const double dt = *dtp;
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(n % b.mx);
@@ -455,7 +464,7 @@ __global__ void __launch_bounds__(128) k_mix_update(DevBlock b, DevState in, Dev
     const int j = (int)(r % b.my), k = (int)(r / b.my);
     const long long p = b.id(i, j, k);
     const double dtj = dt / b.jac[p];
-    double c[kMV];
+    double c[Spec<NS>::A + 5];
     for (int l = 0; l < nv; ++l) {
       c[l] = ca * qn.cv[l * P + p] + cb * in.cv[l * P + p] + cc * dtj * dq[l * b.n + n];
     }
@@ -468,14 +477,14 @@ __global__ void __launch_bounds__(128) k_mix_update(DevBlock b, DevState in, Dev
     out.bv[P + p] = u;
     out.bv[2 * P + p] = v;
     out.bv[3 * P + p] = w;
-    double y[kMS];
+    double y[Spec<NS>::A];
     for (int l = 0; l < ns; ++l) {
       y[l] = c[5 + l] * di;
       out.sv[l * P + p] = y[l];
     }
     const double e = c[4] / rho - 0.5 * (u * u + v * v + w * w);
     double pr;
-    const double t = mix_temperature(rho, e, in.bv[5 * P + p], y, pr);
+    const double t = mix_temperature<NS>(rho, e, in.bv[5 * P + p], y, pr);
     out.bv[4 * P + p] = pr;
     out.bv[5 * P + p] = t;
     if (!(rho > 0) || !(pr > 0) || !(t > 0)) atomicOr(flags, (rho != rho || pr != pr || t != t) ? 2u : 1u);

@@ -100,7 +100,8 @@ class Case:
                       f"string transport_file = chemistry/{m['tran']}"]
         if self.freestream:
             f = self.freestream
-            lines += ["string reference_state = freestream", "struct freestream = {", "    string type = inflow",
+            lines += ["string reference_state = freestream", "string default_init = freestream",
+                      "struct freestream = {", "    string type = inflow",
                       "    int label = 5", f"    real mach = {f['mach']!r}", f"    real pressure = {f['pressure']!r}",
                       f"    real temperature = {f['temperature']!r}", "    real u = 1.0", "    real v = 0.0",
                       "    real w = 0.0"]
@@ -128,6 +129,34 @@ class Case:
             out[g["label"]] = dict(density=rho, u=u * vel, v=v * vel, w=w * vel, pressure=p, temperature=t,
                                    acoustic_speed=c, gamma=GAMMA, entropy=p / rho ** GAMMA, mw=MW_AIR)
         return out
+
+    def default_state(self):
+        """(bv[6], Y) of the default initialisation (the freestream struct), or None."""
+        f = self.freestream
+        if not f:
+            return None
+        t, p, mach = f["temperature"], f["pressure"], f["mach"]
+        y = []
+        if self.mixture:
+            tb = self.mixture["tables"]
+            y = [0.0] * tb.n_spec
+            for k, v in f.get("Y", {}).items():
+                y[tb.names.index(k)] = v
+            mw = 0.0
+            for i in range(tb.n_spec):
+                mw += y[i] / tb.mw[i]
+            mw = 1 / mw
+            cpi = species_cp(tb, t)
+            cp = cv = 0.0
+            for i in range(tb.n_spec):
+                cp += y[i] * cpi[i]
+                cv += y[i] * (cpi[i] - R_U / tb.mw[i])
+            gamma = cp / cv
+        else:
+            mw, gamma = MW_AIR, GAMMA
+        c = math.sqrt(gamma * R_U / mw * t)
+        vel = mach * c
+        return [p * mw / (R_U * t), 1.0 * vel, 0.0 * vel, 0.0 * vel, p, t], y
 
     def reference_scales(self):
         """(rho_inf^2 v_inf^2, v_inf) of the reference state as the reference's Inflow ctor computes
@@ -189,7 +218,59 @@ def species_cp(tb, t):
     return out
 
 
-def write_case(case: Case, directory: os.PathLike) -> Path:
+@dataclasses.dataclass
+class Block:
+    mx: int
+    my: int
+    mz: int
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    faces: list
+    bv: np.ndarray
+    inner: list = dataclasses.field(default_factory=list)  # (this 7 ints, target 7 ints), 1-based
+    sv: np.ndarray | None = None
+
+    @property
+    def nodes(self) -> int:
+        return self.mx * self.my * self.mz
+
+
+@dataclasses.dataclass
+class MultiCase:
+    """Several blocks joined by 1:1 interfaces (inner-face file), with one setup."""
+    name: str
+    blocks: list
+    grid_scale: float
+    bc_structs: dict
+    scheme: dict
+    steps: int = 100
+    mixture: dict | None = None
+    freestream: dict | None = None
+
+    @property
+    def nodes(self) -> int:
+        return sum(b.nodes for b in self.blocks)
+
+    def setup_text(self) -> str:
+        return Case.setup_text(self)
+
+    def farfield_states(self):
+        return Case.farfield_states(self)
+
+    def label_types(self):
+        return Case.label_types(self)
+
+    def reference_scales(self):
+        return Case.reference_scales(self)
+
+    def default_state(self):
+        return Case.default_state(self)
+
+
+def write_case(case, directory: os.PathLike) -> Path:
+    if isinstance(case, MultiCase):
+        return _write_multi(case, directory)
     d = Path(directory)
     (d / "grid").mkdir(parents=True, exist_ok=True)
     if case.mixture:
@@ -210,6 +291,100 @@ def write_case(case: Case, directory: os.PathLike) -> Path:
     with open(d / "boundary_condition" / "inner   0.txt", "w") as f:
         f.write("        1        0\n        0\niMin  iMax  jMin  jMax  kMin  kMax   id\n")
     return d
+
+
+def _write_multi(case: MultiCase, directory: os.PathLike) -> Path:
+    d = Path(directory)
+    (d / "grid").mkdir(parents=True, exist_ok=True)
+    (d / "boundary_condition").mkdir(parents=True, exist_ok=True)
+    (d / "setup.txt").write_text(case.setup_text())
+    with open(d / "grid" / "grid   0.dat", "wb") as f:
+        np.array([len(case.blocks)], dtype=np.int32).tofile(f)
+        for b in case.blocks:
+            np.array([b.mx, b.my, b.mz], dtype=np.int32).tofile(f)
+        for b in case.blocks:
+            for a in (b.x, b.y, b.z):
+                np.ascontiguousarray(a, dtype=np.float64).tofile(f)
+    with open(d / "boundary_condition" / "boundary   0.txt", "w") as f:
+        for b in case.blocks:
+            f.write(f"{len(b.faces):7d}\n")
+            for fc in b.faces:
+                f.write("".join(f"{v:7d}" for v in fc.raw) + f"{fc.label:7d}\n")
+    with open(d / "boundary_condition" / "inner   0.txt", "w") as f:
+        f.write(f"{len(case.blocks):9d}{0:9d}\n")
+        f.write("".join(f"{len(b.inner):9d}" for b in case.blocks) + "\n")
+        f.write("iMin  iMax  jMin  jMax  kMin  kMax   id\n")
+        for b in case.blocks:
+            for src, tar in b.inner:
+                f.write("".join(f"{v:7d}" for v in src) + "\n")
+                f.write("".join(f"{v:7d}" for v in tar) + "\n")
+    if case.mixture:
+        import shutil
+        (d / "chemistry").mkdir(parents=True, exist_ok=True)
+        for k in ("mechanism", "therm", "tran"):
+            shutil.copyfile(Path(case.mixture["chem_dir"]) / case.mixture[k], d / "chemistry" / case.mixture[k])
+    return d
+
+
+def multiblock_mixing_layer_3d(nb=12, lo=32, hi=256, my=64, mz=32, seed=0, steps=100, mc=0.5, re=1000.0,
+                               t0=300.0, delta0=1e-3, h=0.125, reconstruction=5, inviscid_scheme=4, cfl=0.5,
+                               dims=None) -> MultiCase:
+    """nb blocks chained along x with seeded uneven i extents (uniform in [lo, hi]; `dims` overrides),
+    common j / k extents, joined by 1:1 interfaces (block b's i-max face on block b+1's i-min face,
+    coincident nodes).  Outflow at the two x ends, far-field y, periodic z within every block.  Shear
+    layer u = dU/2 tanh(2y/delta0), Mc = 0.5, with 1e-2 dU N(0,1) exp(-(y/delta0)^2) seeded noise in u, v, w."""
+    rng = np.random.default_rng(seed)
+    mxs = list(dims) if dims is not None else [int(v) for v in rng.integers(lo, hi + 1, nb)]
+    nb = len(mxs)
+    c0 = math.sqrt(GAMMA * R_AIR * t0)
+    du = 2 * mc * c0
+    rho0 = re * sutherland(t0) / (du * delta0)
+    p0 = rho0 * R_AIR * t0
+    two_d = mz == 1
+    blocks = []
+    x0 = 0.0
+    for b, mx in enumerate(mxs):
+        xs = x0 + np.arange(mx) * h
+        ys = (np.arange(my) - (my - 1) / 2) * h
+        zs = np.arange(mz) * h
+        Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+        x0 = xs[-1]
+        env = np.exp(-Y ** 2)
+        bv = np.empty((6, mz, my, mx))
+        bv[0] = rho0
+        bv[1] = 0.5 * du * np.tanh(2 * Y) + 1e-2 * du * rng.standard_normal(X.shape) * env
+        bv[2] = 1e-2 * du * rng.standard_normal(X.shape) * env
+        bv[3] = 0.0 if two_d else 1e-2 * du * rng.standard_normal(X.shape) * env
+        bv[4] = p0
+        bv[5] = t0
+        faces = []
+        if b == 0:
+            faces.append(Face((0, 0, 0, my - 1, 0, mz - 1), 6))
+        if b == nb - 1:
+            faces.append(Face((mx - 1, mx - 1, 0, my - 1, 0, mz - 1), 6))
+        faces += [Face((0, mx - 1, 0, 0, 0, mz - 1), 41), Face((0, mx - 1, my - 1, my - 1, 0, mz - 1), 4)]
+        if not two_d:
+            faces += [Face((0, mx - 1, 0, my - 1, 0, 0), 8), Face((0, mx - 1, 0, my - 1, mz - 1, mz - 1), 8)]
+        inner = []
+        if b > 0:
+            pm = mxs[b - 1]
+            inner.append(([1, 1, -1, -my, 1, mz, b + 1], [pm, pm, -1, -my, 1, mz, b]))
+        if b < nb - 1:
+            inner.append(([mx, mx, -1, -my, 1, mz, b + 1], [1, 1, -1, -my, 1, mz, b + 2]))
+        blocks.append(Block(mx, my, mz, X, Y, Z, faces, bv, inner))
+    structs = {"outflow": {"type": ("string", "outflow"), "label": ("int", 6)},
+               "farfield_upper": {"type": ("string", "farfield"), "label": ("int", 4), "mach": ("real", mc),
+                                  "pressure": ("real", p0), "temperature": ("real", t0), "u": ("real", 1.0),
+                                  "v": ("real", 0.0), "w": ("real", 0.0)},
+               "farfield_lower": {"type": ("string", "farfield"), "label": ("int", 41), "mach": ("real", mc),
+                                  "pressure": ("real", p0), "temperature": ("real", t0), "u": ("real", -1.0),
+                                  "v": ("real", 0.0), "w": ("real", 0.0)}}
+    if not two_d:
+        structs["periodic"] = {"type": ("string", "periodic"), "label": ("int", 8)}
+    scheme = dict(reconstruction=reconstruction, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=cfl,
+                  prandtl_number=0.72, limiter=0, entropy_fix_factor=0.125)
+    return MultiCase("multiblock_mixing_layer", blocks, delta0, structs, scheme, steps,
+                     freestream=dict(mach=mc, pressure=p0, temperature=t0))
 
 
 def _box_faces(mx, my, mz, xlab, ylab_lo, ylab_hi, zlab):

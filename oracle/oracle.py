@@ -37,6 +37,10 @@ class OrcChem(ctypes.Structure):
                 ("troe_t3", D * MAXR), ("troe_t1", D * MAXR), ("troe_t2", D * MAXR)]
 
 
+class OrcInner(ctypes.Structure):
+    _fields_ = [("raw", ctypes.c_int * 7), ("traw", ctypes.c_int * 7)]
+
+
 def chem_struct(t) -> OrcChem:
     """ctypes copy of oracle/chem.py tables (row-major, first n_spec / n_reac entries used)."""
     c = OrcChem()
@@ -59,7 +63,8 @@ class OrcCase(ctypes.Structure):
                 ("prandtl", ctypes.c_double), ("fixed_time_step", ctypes.c_int), ("dt", ctypes.c_double),
                 ("n_face", ctypes.c_int), ("face", OrcFace * 16), ("n_spec", ctypes.c_int),
                 ("finite_rate", ctypes.c_int), ("chem", ctypes.POINTER(OrcChem)), ("weno_eps_scale", ctypes.c_double),
-                ("v_ref", ctypes.c_double)]
+                ("v_ref", ctypes.c_double), ("has_init", ctypes.c_int), ("init_bv", ctypes.c_double * 6),
+                ("init_sv", ctypes.c_double * MAXS)]
 
 
 def riemann_of(reconstruction: int, inviscid_scheme: int) -> int:
@@ -69,6 +74,17 @@ def riemann_of(reconstruction: int, inviscid_scheme: int) -> int:
     if inviscid_scheme == 2 and reconstruction in (1, 2, 3):
         return 2
     return inviscid_scheme if inviscid_scheme in (1, 4) else 3
+
+
+def _set_init(c, case):
+    st = case.default_state() if hasattr(case, "default_state") else None
+    if st is not None:
+        bv, y = st
+        c.has_init = 1
+        for q in range(6):
+            c.init_bv[q] = bv[q]
+        for q, v in enumerate(y):
+            c.init_sv[q] = v
 
 
 def build() -> Path:
@@ -102,12 +118,25 @@ def load():
         lib.orc_time.restype = ctypes.c_double
         lib.orc_dt.argtypes = [vp]
         lib.orc_dt.restype = ctypes.c_double
+        lib.orc_multi_create.argtypes = [ctypes.c_int, ctypes.POINTER(OrcCase), ctypes.POINTER(dp),
+                                         ctypes.POINTER(dp), ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(OrcInner)]
+        lib.orc_multi_create.restype = vp
+        lib.orc_multi_destroy.argtypes = [vp]
+        lib.orc_multi_block.argtypes = [vp, ctypes.c_int]
+        lib.orc_multi_block.restype = vp
+        lib.orc_multi_set_state.argtypes = [vp, ctypes.POINTER(dp), ctypes.POINTER(dp)]
+        lib.orc_multi_step.argtypes = [vp, ctypes.c_int]
+        lib.orc_multi_step.restype = ctypes.c_double
         _lib = lib
     return _lib
 
 
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+dp_arr = ctypes.POINTER(ctypes.c_double)
 
 
 class Oracle:
@@ -141,6 +170,7 @@ class Oracle:
             c.n_spec = self.n_spec = mix["tables"].n_spec
             c.finite_rate = 1 if mix["finite_rate"] else 0
         c.weno_eps_scale, c.v_ref = case.reference_scales()
+        _set_init(c, case)
         self.case = case
         self.shape = (case.mz, case.my, case.mx)
         x = np.ascontiguousarray(case.x * case.grid_scale, dtype=np.float64)
@@ -207,3 +237,86 @@ class Oracle:
 
     def dt(self) -> float:
         return self.lib.orc_dt(self.h)
+
+
+class _BlockView:
+    """Per-block accessor of a multi-block oracle (state, metric) sharing the Oracle methods."""
+
+    def __init__(self, lib, h, shape, n_spec):
+        self.lib, self.h, self.shape, self.n_spec = lib, h, shape, n_spec
+
+    get_state = Oracle.get_state
+    metric = Oracle.metric
+    mixture = Oracle.mixture
+    time = Oracle.time
+
+
+class MultiOracle:
+    """CPU restatement of a multi-block case (ostc_cases.MultiCase): per-block contexts joined by the
+    interface exchange of the reference (orc_multi_*)."""
+
+    def __init__(self, case):
+        self.lib = load()
+        nb = len(case.blocks)
+        cases = (OrcCase * nb)()
+        types = case.label_types()
+        ff = case.farfield_states()
+        self._keep = []
+        xs, ys, zs = (dp_arr * nb)(), (dp_arr * nb)(), (dp_arr * nb)()
+        for b, blk in enumerate(case.blocks):
+            c = cases[b]
+            c.mx, c.my, c.mz = blk.mx, blk.my, blk.mz
+            sch = case.scheme
+            c.reconstruction, c.inviscid_scheme, c.viscous_order = sch["reconstruction"], sch["inviscid_scheme"], sch["viscous_order"]
+            c.riemann = riemann_of(sch["reconstruction"], sch["inviscid_scheme"])
+            c.entropy_fix_factor = sch.get("entropy_fix_factor", 0.125)
+            c.cfl, c.prandtl = sch["cfl"], sch["prandtl_number"]
+            c.fixed_time_step, c.dt = 0, 1e-8
+            c.n_face = len(blk.faces)
+            for n, f in enumerate(blk.faces):
+                c.face[n].type = types[f.label]
+                for q in range(6):
+                    c.face[n].raw[q] = f.raw[q]
+                if f.label in ff:
+                    for k, v in ff[f.label].items():
+                        setattr(c.face[n], k, v)
+            c.weno_eps_scale, c.v_ref = case.reference_scales()
+            _set_init(c, case)
+            for arr, src in ((xs, blk.x), (ys, blk.y), (zs, blk.z)):
+                a = np.ascontiguousarray(src * case.grid_scale, dtype=np.float64)
+                self._keep.append(a)
+                arr[b] = _dp(a)
+        nin = (ctypes.c_int * nb)(*[len(b.inner) for b in case.blocks])
+        allf = [f for b in case.blocks for f in b.inner]
+        inner = (OrcInner * max(1, len(allf)))()
+        for i, (src, tar) in enumerate(allf):
+            for q in range(7):
+                inner[i].raw[q], inner[i].traw[q] = src[q], tar[q]
+        self.h = self.lib.orc_multi_create(nb, cases, xs, ys, zs, nin, inner)
+        self.case = case
+        self.blocks = [_BlockView(self.lib, self.lib.orc_multi_block(self.h, b), (blk.mz, blk.my, blk.mx), 0)
+                       for b, blk in enumerate(case.blocks)]
+
+    def close(self):
+        if self.h:
+            self.lib.orc_multi_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self):
+        nb = len(self.case.blocks)
+        bvs = [np.ascontiguousarray(b.bv, dtype=np.float64) for b in self.case.blocks]
+        self._state = bvs
+        arr = (dp_arr * nb)(*[_dp(a) for a in bvs])
+        self.lib.orc_multi_set_state(self.h, arr, None)
+
+    def step(self, n: int = 1) -> float:
+        return self.lib.orc_multi_step(self.h, n)
+
+    def time(self) -> float:
+        return self.blocks[0].time()

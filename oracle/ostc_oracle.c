@@ -121,8 +121,17 @@ static void ghost_grid(orc_ctx *o) {
         }
       }
   }
-  /* edges and corners by the parallelogram rule (Mesh.cpp:968-1036) */
-  for (int i = 1; i <= ngg + 1; ++i)
+}
+
+/* edges and corners by the parallelogram rule (Mesh.cpp:968-1036), after the face layers and the
+ * interface layers (Mesh.cpp:962-967) */
+static void ghost_grid_edges(orc_ctx *o) {
+  const int mx = o->mx, my = o->my, mz = o->mz, ngg = o->g;
+  double *X = o->x, *Y = o->y, *Z = o->z;
+#define XX(i, j, k) X[IC(o, i, j, k)]
+#define YY(i, j, k) Y[IC(o, i, j, k)]
+#define ZZ(i, j, k) Z[IC(o, i, j, k)]
+    for (int i = 1; i <= ngg + 1; ++i)
     for (int j = 1; j <= ngg + 1; ++j)
       for (int k = 0; k < mz; ++k) {
         const int i1 = -i, j1 = -j, i2 = mx - 1 + i, j2 = my - 1 + j;
@@ -1786,7 +1795,15 @@ static void fill_ghosts(orc_ctx *o) {
 
 /* ---------------------------------------------------------------- public entry points */
 
+static orc_ctx *create_block(const orc_case *c, const double *x, const double *y, const double *z, int finish);
+
 orc_ctx *orc_create(const orc_case *c, const double *x, const double *y, const double *z) {
+  return create_block(c, x, y, z, 1);
+}
+
+/* finish = 0 leaves the edge / corner ghost coordinates and the metric to the caller, which first
+ * copies the interface ghost layers from the neighbours (multi-block). */
+static orc_ctx *create_block(const orc_case *c, const double *x, const double *y, const double *z, int finish) {
   orc_ctx *o = (orc_ctx *)calloc(1, sizeof(orc_ctx));
   o->c = *c;
   o->mx = c->mx;
@@ -1819,7 +1836,10 @@ orc_ctx *orc_create(const orc_case *c, const double *x, const double *y, const d
   o->jac = (double *)calloc(o->P, sizeof(double));
   o->met = (double *)calloc(9 * o->P, sizeof(double));
   ghost_grid(o);
-  compute_metric(o);
+  if (finish) {
+    ghost_grid_edges(o);
+    compute_metric(o);
+  }
   const long N = (long)o->mx * o->my * o->mz;
   o->cv = (double *)calloc(o->nv * o->P, sizeof(double));
   o->qn = (double *)calloc(o->nv * o->P, sizeof(double));
@@ -1854,11 +1874,28 @@ double orc_time(const orc_ctx *o) { return o->t; }
  * the padded block at the start of RK3 (RK.cuh:37-45). */
 void orc_set_state(orc_ctx *o, const double *bv) { orc_set_state_sv(o, bv, NULL); }
 
+static void load_state(orc_ctx *o, const double *bv, const double *sv);
+
 void orc_set_state_sv(orc_ctx *o, const double *bv, const double *sv) {
+  load_state(o, bv, sv);
+  if (o->dim == 2) eliminate_k(o);
+  apply_bcs(o);
+  properties(o);
+  for (long p = 0; p < o->P; ++p) cv_from_bv(o, p);
+  o->t = 0;
+}
+
+static void load_state(orc_ctx *o, const double *bv, const double *sv) {
   const long P = o->P, N = (long)o->mx * o->my * o->mz;
   memset(o->bv, 0, sizeof(double) * 6 * P);
   memset(o->cv, 0, sizeof(double) * o->nv * P);
   if (o->ns) memset(o->sv, 0, sizeof(double) * o->ns * P);
+  if (o->c.has_init) {
+    for (int l = 0; l < 6; ++l)
+      for (long p = 0; p < P; ++p) o->bv[l * P + p] = o->c.init_bv[l];
+    for (int l = 0; l < o->ns; ++l)
+      for (long p = 0; p < P; ++p) o->sv[l * P + p] = o->c.init_sv[l];
+  }
   for (int l = 0; l < 6; ++l)
     for (int k = 0; k < o->mz; ++k)
       for (int j = 0; j < o->my; ++j)
@@ -1867,11 +1904,6 @@ void orc_set_state_sv(orc_ctx *o, const double *bv, const double *sv) {
     for (int k = 0; k < o->mz; ++k)
       for (int j = 0; j < o->my; ++j)
         for (int i = 0; i < o->mx; ++i) o->sv[l * P + ID(o, i, j, k)] = sv[l * N + IQ(o, i, j, k)];
-  if (o->dim == 2) eliminate_k(o);
-  apply_bcs(o);
-  properties(o);
-  for (long p = 0; p < P; ++p) cv_from_bv(o, p);
-  o->t = 0;
 }
 
 void orc_get_state(const orc_ctx *o, double *cv, double *bv, double *mul) {
@@ -1943,6 +1975,255 @@ double orc_step(orc_ctx *o, int n) {
       fill_ghosts(o);
     }
     o->t += dt;
+  }
+  return dt;
+}
+
+/* ---------------------------------------------------------------- multi-block (interfaces) */
+
+typedef struct {
+  int rs[3], re[3], ts[3], te[3];
+  int face, direction, target_face, target_direction;
+  int src_tar[3], loop_dir[3], target_loop_dir[3], n_point[3];
+  int target;
+} inner_t;
+
+struct orc_multi {
+  int nb;
+  orc_ctx **b;
+  int *nf;
+  inner_t **f;
+};
+
+static int isgn(int a) { return a < 0 ? -1 : 1; } /* gxl::sgn, sgn(0) = +1 (gxl_lib/Math.hpp:13-15) */
+
+/* InnerFace::register_boundary (Mesh.cpp:38-141) */
+static void register_inner(inner_t *f, int ngg, int dim) {
+  f->direction = f->target_direction = 1;
+  f->face = f->target_face = 0;
+  for (int i = 0; i < 3; ++i) f->src_tar[i] = 0;
+  for (int i = 0; i < dim; ++i)
+    if (f->rs[i] == f->re[i]) {
+      f->face = i;
+      if (f->rs[i] == 1) f->direction = -1;
+      f->rs[i] -= 1;
+      f->re[i] -= 1;
+      break;
+    }
+  for (int i = 0; i < dim; ++i)
+    if (f->ts[i] == f->te[i]) {
+      f->target_face = i;
+      if (f->ts[i] == 1) f->target_direction = -1;
+      f->ts[i] -= 1;
+      f->te[i] -= 1;
+      break;
+    }
+  f->src_tar[f->target_face] = -(f->direction * f->target_direction) * (f->face + 1);
+  if (dim == 2) {
+    const int nf = 1 - f->face, tnf = 1 - f->target_face;
+    f->rs[nf] = abs(f->rs[nf]) - 1;
+    f->re[nf] = abs(f->re[nf]) - 1;
+    f->ts[tnf] = abs(f->ts[tnf]) - 1;
+    f->te[tnf] = abs(f->te[tnf]) - 1;
+    f->src_tar[tnf] = isgn((f->te[tnf] - f->ts[tnf]) * (f->re[nf] - f->rs[nf])) * (nf + 1);
+    f->src_tar[2] = 3;
+    f->rs[2] = f->re[2] = f->ts[2] = f->te[2] = 0;
+  } else {
+    int nf = 0, tnf = 0;
+    for (int i = 0; i < dim; ++i)
+      if (f->rs[i] < 0) {
+        nf = i;
+        f->rs[i] = -f->rs[i] - 1;
+        f->re[i] = -f->re[i] - 1;
+        break;
+      }
+    for (int i = 0; i < dim; ++i)
+      if (f->ts[i] < 0) {
+        tnf = i;
+        f->ts[i] = -f->ts[i] - 1;
+        f->te[i] = -f->te[i] - 1;
+        break;
+      }
+    f->src_tar[tnf] = isgn((f->te[tnf] - f->ts[tnf]) * (f->re[nf] - f->rs[nf])) * (nf + 1);
+    nf = 3 - f->face - nf;
+    tnf = 3 - f->target_face - tnf;
+    f->rs[nf] -= 1;
+    f->re[nf] -= 1;
+    f->ts[tnf] -= 1;
+    f->te[tnf] -= 1;
+    f->src_tar[tnf] = isgn((f->te[tnf] - f->ts[tnf]) * (f->re[nf] - f->rs[nf])) * (nf + 1);
+  }
+  f->rs[f->face] = f->direction < 0 ? -ngg : f->re[f->face];
+  f->re[f->face] = f->direction < 0 ? 0 : f->re[f->face] + ngg;
+  const int st = isgn(f->src_tar[f->target_face]);
+  if (f->target_direction > 0) f->ts[f->target_face] = st > 0 ? f->te[f->target_face] - ngg : f->te[f->target_face];
+  else f->ts[f->target_face] = st > 0 ? 0 : ngg;
+  for (int i = 0; i < 3; ++i) {
+    f->loop_dir[i] = f->rs[i] <= f->re[i] ? 1 : -1;
+    f->target_loop_dir[i] = isgn(f->src_tar[i]);
+    f->src_tar[i] = abs(f->src_tar[i]) - 1;
+    f->n_point[i] = abs(f->rs[i] - f->re[i]) + 1;
+  }
+}
+
+/* Mesh::init_inner_ghost_grid (Mesh.cpp:1049-1097) */
+static void inner_ghost_grid(orc_multi *m) {
+  for (int bb = 0; bb < m->nb; ++bb) {
+    orc_ctx *B = m->b[bb];
+    for (int n = 0; n < m->nf[bb]; ++n) {
+      const inner_t *fc = &m->f[bb][n];
+      orc_ctx *T = m->b[fc->target];
+      int mn[3] = {fc->rs[0], fc->rs[1], fc->rs[2]}, mx[3] = {fc->re[0], fc->re[1], fc->re[2]};
+      int mt[3] = {fc->ts[0], fc->ts[1], fc->ts[2]};
+      const int sh = fc->direction < 0 ? -1 : 1;
+      mn[fc->face] += sh;
+      mx[fc->face] += sh;
+      mt[fc->target_face] += fc->target_direction > 0 ? -1 : 1;
+      int di[3];
+      for (int i1 = mn[0]; fc->loop_dir[0] * (i1 - mx[0]) != 1; i1 += fc->loop_dir[0]) {
+        di[0] = i1 - mn[0];
+        for (int j1 = mn[1]; fc->loop_dir[1] * (j1 - mx[1]) != 1; j1 += fc->loop_dir[1]) {
+          di[1] = j1 - mn[1];
+          for (int k1 = mn[2]; fc->loop_dir[2] * (k1 - mx[2]) != 1; k1 += fc->loop_dir[2]) {
+            di[2] = k1 - mn[2];
+            const int i2 = mt[0] + fc->target_loop_dir[0] * di[fc->src_tar[0]];
+            const int j2 = mt[1] + fc->target_loop_dir[1] * di[fc->src_tar[1]];
+            const int k2 = mt[2] + fc->target_loop_dir[2] * di[fc->src_tar[2]];
+            B->x[IC(B, i1, j1, k1)] = T->x[IC(T, i2, j2, k2)];
+            B->y[IC(B, i1, j1, k1)] = T->y[IC(T, i2, j2, k2)];
+            B->z[IC(B, i1, j1, k1)] = T->z[IC(T, i2, j2, k2)];
+          }
+        }
+      }
+    }
+  }
+}
+
+/* data_communication / inner_communication (DataCommunication.cuh:29-105) */
+static void exchange(orc_multi *m) {
+  for (int bb = 0; bb < m->nb; ++bb) {
+    orc_ctx *o = m->b[bb];
+    for (int n = 0; n < m->nf[bb]; ++n) {
+      const inner_t *f = &m->f[bb][n];
+      orc_ctx *t = m->b[f->target];
+      const int face_dir = f->direction > 0 ? f->rs[f->face] : f->re[f->face];
+      for (int n2 = 0; n2 < f->n_point[2]; ++n2)
+        for (int n1 = 0; n1 < f->n_point[1]; ++n1)
+          for (int n0 = 0; n0 < f->n_point[0]; ++n0) {
+            const int d[3] = {f->loop_dir[0] * n0, f->loop_dir[1] * n1, f->loop_dir[2] * n2};
+            const int idx[3] = {f->rs[0] + d[0], f->rs[1] + d[1], f->rs[2] + d[2]};
+            int it[3];
+            for (int q = 0; q < 3; ++q) it[q] = f->ts[q] + f->target_loop_dir[q] * d[f->src_tar[q]];
+            const long p = ID(o, idx[0], idx[1], idx[2]), pt = ID(t, it[0], it[1], it[2]);
+            if (idx[f->face] == face_dir) {
+              for (int l = 0; l < 6; ++l) {
+                const double ave = 0.5 * (t->bv[l * t->P + pt] + o->bv[l * o->P + p]);
+                o->bv[l * o->P + p] = ave;
+                t->bv[l * t->P + pt] = ave;
+              }
+              for (int l = 0; l < o->ns; ++l) {
+                const double ave = 0.5 * (t->sv[l * t->P + pt] + o->sv[l * o->P + p]);
+                o->sv[l * o->P + p] = ave;
+                t->sv[l * t->P + pt] = ave;
+              }
+            } else {
+              for (int l = 0; l < 6; ++l) o->bv[l * o->P + p] = t->bv[l * t->P + pt];
+              for (int l = 0; l < o->ns; ++l) o->sv[l * o->P + p] = t->sv[l * t->P + pt];
+            }
+            cv_from_bv(o, p);
+          }
+    }
+  }
+}
+
+orc_multi *orc_multi_create(int nb, const orc_case *cases, const double *const *x, const double *const *y,
+                            const double *const *z, const int *n_inner, const orc_inner_in *inner) {
+  orc_multi *m = (orc_multi *)calloc(1, sizeof(orc_multi));
+  m->nb = nb;
+  m->b = (orc_ctx **)calloc(nb, sizeof(orc_ctx *));
+  m->nf = (int *)calloc(nb, sizeof(int));
+  m->f = (inner_t **)calloc(nb, sizeof(inner_t *));
+  for (int b = 0; b < nb; ++b) m->b[b] = create_block(&cases[b], x[b], y[b], z[b], 0);
+  int off = 0;
+  for (int b = 0; b < nb; ++b) {
+    m->nf[b] = n_inner[b];
+    m->f[b] = (inner_t *)calloc(n_inner[b] + 1, sizeof(inner_t));
+    for (int n = 0; n < n_inner[b]; ++n) {
+      const orc_inner_in *in = &inner[off++];
+      inner_t *f = &m->f[b][n];
+      for (int q = 0; q < 3; ++q) {
+        f->rs[q] = in->raw[2 * q];
+        f->re[q] = in->raw[2 * q + 1];
+        f->ts[q] = in->traw[2 * q];
+        f->te[q] = in->traw[2 * q + 1];
+      }
+      f->target = in->traw[6] - 1;
+      register_inner(f, m->b[b]->g, m->b[b]->dim);
+    }
+  }
+  inner_ghost_grid(m);
+  for (int b = 0; b < nb; ++b) {
+    ghost_grid_edges(m->b[b]);
+    compute_metric(m->b[b]);
+  }
+  return m;
+}
+
+void orc_multi_destroy(orc_multi *m) {
+  if (!m) return;
+  for (int b = 0; b < m->nb; ++b) {
+    orc_destroy(m->b[b]);
+    free(m->f[b]);
+  }
+  free(m->b);
+  free(m->f);
+  free(m->nf);
+  free(m);
+}
+
+orc_ctx *orc_multi_block(orc_multi *m, int b) { return m->b[b]; }
+
+/* Driver::initialize_computation (Driver.cu:115-199) over all blocks, then cv <- bv (RK.cuh:37-45) */
+void orc_multi_set_state(orc_multi *m, const double *const *bv, const double *const *sv) {
+  for (int b = 0; b < m->nb; ++b) {
+    load_state(m->b[b], bv[b], sv ? sv[b] : NULL);
+    if (m->b[b]->dim == 2) eliminate_k(m->b[b]);
+  }
+  for (int b = 0; b < m->nb; ++b) apply_bcs(m->b[b]);
+  exchange(m);
+  for (int b = 0; b < m->nb; ++b) {
+    properties(m->b[b]);
+    for (long p = 0; p < m->b[b]->P; ++p) cv_from_bv(m->b[b], p);
+    m->b[b]->t = 0;
+  }
+}
+
+/* RK3 over all blocks (RK.cuh:85-185): one dt (minimum over the blocks), per stage every block's RHS,
+ * update and boundary faces, then the interfaces, then the k copies (2-D) and the properties. */
+double orc_multi_step(orc_multi *m, int n) {
+  double dt = m->b[0]->c.fixed_time_step ? m->b[0]->c.dt : 1e6;
+  for (int s = 0; s < n; ++s) {
+    for (int b = 0; b < m->nb; ++b) memcpy(m->b[b]->qn, m->b[b]->cv, sizeof(double) * m->b[b]->nv * m->b[b]->P);
+    for (int rk = 0; rk < 3; ++rk) {
+      if (!m->b[0]->c.fixed_time_step && rk == 0) {
+        dt = 1e6;
+        for (int b = 0; b < m->nb; ++b) {
+          const double d = orc_dt(m->b[b]);
+          if (d < dt) dt = d;
+        }
+      }
+      for (int b = 0; b < m->nb; ++b) {
+        orc_rhs(m->b[b], 7u, NULL);
+        rk_update(m->b[b], dt, rk);
+        apply_bcs(m->b[b]);
+      }
+      exchange(m);
+      for (int b = 0; b < m->nb; ++b) {
+        if (m->b[b]->dim == 2) eliminate_k(m->b[b]);
+        properties(m->b[b]);
+      }
+    }
+    for (int b = 0; b < m->nb; ++b) m->b[b]->t += dt;
   }
   return dt;
 }

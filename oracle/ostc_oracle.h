@@ -63,6 +63,11 @@ typedef struct {
   const orc_chem *chem;
   double weno_eps_scale;     /* rho_inf^2 v_inf^2 of the reference state (DParameter.cu:26-29) */
   double v_ref;              /* v_inf (component-wise WENO eps scaling, WENO.cu:1471-1473) */
+  /* default initialisation of every node, ghosts included (Field.cu:316-345): has_init, then
+   * rho u v w p T and the mass fractions */
+  int has_init;
+  double init_bv[6];
+  double init_sv[ORC_MAX_SPEC];
 } orc_case;
 
 typedef struct orc_ctx orc_ctx;
@@ -92,6 +97,24 @@ double orc_step(orc_ctx *o, int n);
 double orc_time(const orc_ctx *o);
 /* Local CFL time step of the current state and its minimum (TimeAdvanceFunc.cuh:28-83). */
 double orc_dt(orc_ctx *o);
+
+/* Multi-block: one context per block plus the 1:1 interfaces of the inner-face file
+ * ("inner   0.txt", Mesh.cpp:812-844), each as its two lines: this block's 1-based range with the
+ * reference's signs (x1 x2 y1 y2 z1 z2, seventh value unused) and the target's range + block id. */
+typedef struct {
+  int raw[7];
+  int traw[7];
+} orc_inner_in;
+
+typedef struct orc_multi orc_multi;
+/* n_inner[b] faces of block b, concatenated in `inner` in block order. */
+orc_multi *orc_multi_create(int nb, const orc_case *cases, const double *const *x, const double *const *y,
+                            const double *const *z, const int *n_inner, const orc_inner_in *inner);
+void orc_multi_destroy(orc_multi *m);
+orc_ctx *orc_multi_block(orc_multi *m, int b);
+/* bv[b]: [6][N_b] interior state of block b; sv[b] its mass fractions (NULL for air). */
+void orc_multi_set_state(orc_multi *m, const double *const *bv, const double *const *sv);
+double orc_multi_step(orc_multi *m, int n);
 
 #ifdef __cplusplus
 }

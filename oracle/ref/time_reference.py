@@ -6,7 +6,7 @@ reference's per-run fixed costs (its final flow-field write, first-launch overhe
 n1 and n2 steps are taken and the per-step time is the difference quotient, so those fixed costs
 cancel:  ms/step = (t(n2) - t(n1)) / (n2 - n1).
 
-Usage: python oracle/ref/time_reference.py [mx my mz] [--steps n1 n2]
+Usage: python oracle/ref/time_reference.py [mx my mz] [--steps n1 n2] [--case reacting_mixing_layer_3d]
 Prints one JSON line: grid, steps, per-run seconds, ms/step and cell-steps/s.
 """
 from __future__ import annotations
@@ -26,12 +26,13 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("dims", nargs="*", type=int, default=[512, 256, 128])
     ap.add_argument("--steps", nargs=2, type=int, default=[4, 24])
+    ap.add_argument("--case", default="mixing_layer_3d", choices=["mixing_layer_3d", "reacting_mixing_layer_3d"])
     a = ap.parse_args()
     import ostc_cases as oc
     import refcase
 
     mx, my, mz = a.dims
-    case = oc.mixing_layer_3d(mx=mx, my=my, mz=mz)
+    case = getattr(oc, a.case)(mx=mx, my=my, mz=mz)
     secs = []
     for n in a.steps:
         *_, s = refcase.run_reference(case, n, with_seconds=True)
@@ -40,7 +41,7 @@ def main():
     ms = (secs[1] - secs[0]) / (n2 - n1) * 1e3
     print(json.dumps({"impl": "reference FP64 CUDA build", "grid": [mx, my, mz], "steps": a.steps,
                       "rk3_seconds": secs, "ms_per_step": ms, "cell_steps_per_s": case.nodes / ms * 1e3,
-                      "workload": "3-D mixing layer, AWENO7 + HLLC, viscous, far-field y, periodic x/z"}))
+                      "workload": a.case}))
 
 
 if __name__ == "__main__":

@@ -76,8 +76,9 @@ def write_reference_case(case, steps: int, directory: os.PathLike) -> Path:
     setup = (inp / "setup.txt").read_text()
     setup = setup.replace(f"int total_step = {case.steps}", f"int total_step = {steps}")
     setup = setup.replace("int initial = 1\n", "")
-    p0 = float(case.bv[4].flat[0])
-    t0 = float(case.bv[5].flat[0])
+    bv0 = case.blocks[0].bv if hasattr(case, "blocks") else case.bv
+    p0 = float(bv0[4].flat[0])
+    t0 = float(bv0[5].flat[0])
     setup += EXTRA
     if not case.freestream:
         setup += FREESTREAM.replace("@MACH@", "0.5").replace("@P@", repr(p0)).replace("@T@", repr(t0))
@@ -86,9 +87,10 @@ def write_reference_case(case, steps: int, directory: os.PathLike) -> Path:
         setup += "string reference_state = freestream\n"
         (inp / "setup.txt").write_text(setup)
     with open(d / "state_in.bin", "wb") as f:
-        np.ascontiguousarray(case.bv, dtype=np.float64).tofile(f)
-        if case.sv is not None:
-            np.ascontiguousarray(case.sv, dtype=np.float64).tofile(f)
+        for blk in (case.blocks if hasattr(case, "blocks") else [case]):
+            np.ascontiguousarray(blk.bv, dtype=np.float64).tofile(f)
+            if blk.sv is not None:
+                np.ascontiguousarray(blk.sv, dtype=np.float64).tofile(f)
     (d / "output" / "message").mkdir(parents=True, exist_ok=True)
     return d
 
@@ -106,6 +108,19 @@ def run_reference(case, steps: int, workdir: os.PathLike | None = None, timeout:
     if r.returncode != 0:
         raise RuntimeError(f"reference harness failed ({r.returncode}):\n{r.stdout[-4000:]}\n{r.stderr[-3000:]}")
     raw = np.fromfile(d / "state_out.bin", dtype=np.float64)
+    if hasattr(case, "blocks"):
+        # multi-block: per block [cv(5), bv(6)] interior, then the time
+        out, off = [], 0
+        for blk in case.blocks:
+            nn = blk.nodes
+            a = raw[off: off + 11 * nn].reshape((11,) + blk.bv.shape[1:])
+            out.append((a[:5].copy(), a[5:].copy()))
+            off += 11 * nn
+        res = ([o[0] for o in out], [o[1] for o in out], float(raw[off]))
+        if with_seconds:
+            sec = [float(l.split("=")[1]) for l in r.stdout.splitlines() if "rk3_seconds" in l]
+            return res + (sec[0] if sec else float("nan"),)
+        return res
     n = case.nodes
     ns = 0 if case.sv is None else case.sv.shape[0]
     nv = 5 + ns

@@ -46,6 +46,10 @@ CASES = [
     ("rml3d_fr72", "reacting_mixing_layer_3d", dict(mx=32, my=20, mz=16, inviscid_scheme=72), 10),
     ("rml3d_mix71", "reacting_mixing_layer_3d", dict(mx=32, my=20, mz=16, inviscid_scheme=71, finite_rate=False), 10),
     ("rml2d_fr72", "reacting_mixing_layer_3d", dict(mx=48, my=24, mz=1, inviscid_scheme=72), 20),
+    # multi-block chains joined by 1:1 interfaces (inner-face file)
+    ("mb3d_awe7_hllc", "multiblock_mixing_layer_3d", dict(dims=[20, 17, 23], my=16, mz=10), 10),
+    ("mb2d_awe5_ausm", "multiblock_mixing_layer_3d",
+     dict(dims=[30, 21, 26, 18], my=24, mz=1, reconstruction=4, inviscid_scheme=3), 20),
 ]
 
 
@@ -60,8 +64,14 @@ def main(outdir: Path, only=None):
             continue
         case = make_case(gen, kw)
         cv, bv, t = refcase.run_reference(case, steps)[:3]
-        np.savez_compressed(outdir / f"golden_{name}.npz", cv=cv, t=t, steps=steps,
-                            case=json.dumps({"generator": gen, "kwargs": kw}),
+        meta = json.dumps({"generator": gen, "kwargs": kw})
+        if hasattr(case, "blocks"):
+            arrays = {f"cv_{b}": c for b, c in enumerate(cv)}
+            np.savez_compressed(outdir / f"golden_{name}.npz", t=t, steps=steps, case=meta, n_block=len(cv),
+                                bv0_sum=float(sum(np.sum(b.bv) for b in case.blocks)), **arrays)
+            print(name, "t =", t, "blocks", len(cv), flush=True)
+            continue
+        np.savez_compressed(outdir / f"golden_{name}.npz", cv=cv, t=t, steps=steps, case=meta,
                             bv0_sum=float(np.sum(case.bv)))
         print(name, "t =", t, "rho range", float(bv[0].min()), float(bv[0].max()), flush=True)
 
