@@ -85,6 +85,15 @@ int ostc_n_var(const ostc_ctx *ctx, int *n_var, int *n_scalar);
 /* Arithmetic of the flux path (see OSTC_PREC_*). */
 int ostc_set_precision(ostc_ctx *ctx, int mode);
 
+/* Treatment of the finite-rate chemical source in RK3 (mixtures with reaction = 1).
+ * OSTC_CHEM_EXPLICIT: the reference's RK3 path (chemSrcMethod forced to 0, Parameter.cpp:280-283).
+ * OSTC_CHEM_POINT_IMPLICIT: extension -- the species part of dq is replaced by the solution of
+ * (I - dt J_chem) x = dq_species per cell (EPI + solve_chem_system, FiniteRateChem.cu:197-254,
+ * 302-357, with the step's global dt), batched over all cells in one launch per stage. */
+#define OSTC_CHEM_EXPLICIT 0
+#define OSTC_CHEM_POINT_IMPLICIT 1
+int ostc_set_chem_mode(ostc_ctx *ctx, int mode);
+
 /* Set the interior primitive state of one block: bv[6][N] (rho,u,v,w,p,T), sv[n_scalar][N] (NULL
  * when n_scalar == 0).  After the last block is set, the next ostc_rhs/ostc_rk3_step first runs
  * the reference initialisation (2-D k-copy, boundary conditions, interfaces, properties,

@@ -174,8 +174,11 @@ __device__ __forceinline__ double arrhenius(double t, double A, double b, double
 }
 
 // finite_rate_chemistry (FiniteRateChem.cu:7-58, rates :60-195): omega_k in kg/(m^3 s) at one node.
+// With jac non-null also the chemical source Jacobian of compute_chem_src_jacobian
+// (FiniteRateChem.cu:197-217), [ns][ns] row-major, in 1/s.
 template <int NS>
-__device__ __forceinline__ void mix_chemistry(double rho, double t, const double *y, double *omega) {
+__device__ __forceinline__ void mix_chemistry(double rho, double t, const double *y, double *omega,
+                                              double *jac = nullptr) {
   const int ns = OSTC_NS, nr = c_mix.nr;
   double c[Spec<NS>::A];
   for (int l = 0; l < ns; ++l) c[l] = rho * y[l] * c_mix.imw[l] * 1e-3;
@@ -251,12 +254,72 @@ __device__ __forceinline__ void mix_chemistry(double rho, double t, const double
     }
     q1 *= kf;
     if (ty != 0) q2 *= kb;
+    if (jac) {
+      // sum over reactions in order, per (m, n): (nu_b,m - nu_f,m)(nu_f,n q1 - nu_b,n q2)
+#pragma unroll
+      for (int m = 0; m < ns; ++m) {
+        const int dm = c_mix.stoi_b[r][m] - c_mix.stoi_f[r][m];
+        if (dm == 0) continue;
+#pragma unroll
+        for (int n = 0; n < ns; ++n)
+          jac[m * ns + n] += dm * (c_mix.stoi_f[r][n] * q1 - c_mix.stoi_b[r][n] * q2);
+      }
+    }
     for (int l = 0; l < ns; ++l) {
       cre[l] += q2 * c_mix.stoi_f[r][l] + q1 * c_mix.stoi_b[r][l];
       des[l] += q1 * c_mix.stoi_f[r][l] + q2 * c_mix.stoi_b[r][l];
     }
   }
   for (int l = 0; l < ns; ++l) omega[l] = cre[l] * (c_mix.mw[l] * 1e+3) - des[l] * (c_mix.mw[l] * 1e+3);
+  if (jac) {
+#pragma unroll
+    for (int n = 0; n < ns; ++n) {
+      const bool live = y[n] > 1e-25;
+      const double inv = live ? 1.0 / (rho * y[n]) : 0.0;
+#pragma unroll
+      for (int m = 0; m < ns; ++m) jac[m * ns + n] = c_mix.mw[m] * (live ? jac[m * ns + n] * inv : 0.0) * 1e+3;
+    }
+  }
+}
+
+// solve_chem_system (FiniteRateChem.cu:302-357): column-pivoted LU of the ns x ns matrix lhs in place,
+// then forward / back substitution of b (length ns) in place.
+template <int NS>
+__device__ __forceinline__ void mix_lu_solve(double *lhs, double *b) {
+  const int dim = OSTC_NS;
+  int ipiv[Spec<NS>::A];
+  for (int n = 0; n < dim; ++n) {
+    int ik = n;
+    for (int m = n; m < dim; ++m) {
+      for (int t = 0; t < n; ++t) lhs[m * dim + n] -= lhs[m * dim + t] * lhs[t * dim + n];
+      if (fabs(lhs[m * dim + n]) > fabs(lhs[ik * dim + n])) ik = m;
+    }
+    ipiv[n] = ik;
+    if (ik != n)
+      for (int t = 0; t < dim; ++t) {
+        const double mid = lhs[ik * dim + t];
+        lhs[ik * dim + t] = lhs[n * dim + t];
+        lhs[n * dim + t] = mid;
+      }
+    for (int p = n + 1; p < dim; ++p)
+      for (int t = 0; t < n; ++t) lhs[n * dim + p] -= lhs[n * dim + t] * lhs[t * dim + p];
+    for (int m = n + 1; m < dim; ++m) lhs[m * dim + n] /= lhs[n * dim + n];
+  }
+  for (int m = 0; m < dim; ++m) {
+    const int t = ipiv[m];
+    if (t != m) {
+      const double mid = b[t];
+      b[t] = b[m];
+      b[m] = mid;
+    }
+  }
+  for (int m = 1; m < dim; ++m)
+    for (int t = 0; t < m; ++t) b[m] -= lhs[m * dim + t] * b[t];
+  b[dim - 1] /= lhs[dim * dim - 1];
+  for (int m = dim - 2; m >= 0; --m) {
+    for (int t = m + 1; t < dim; ++t) b[m] -= lhs[m * dim + t] * b[t];
+    b[m] /= lhs[m * dim + m];
+  }
 }
 
 // ---------------------------------------------------------------- flux-split WENO7 (71 / 72)

@@ -1077,6 +1077,7 @@ struct ostc_ctx {
   MixTables mixtab{};
   // default initialisation of every node (ghosts included) before the interior state is set
   // (Field::initialize_basic_variables with the default_init struct, Field.cu:316-345, 388-470)
+  int chem_mode = OSTC_CHEM_EXPLICIT;
   bool has_init = false;
   double init_bv[6]{};
   std::vector<double> init_sv;
@@ -1282,6 +1283,15 @@ void launch_mix_source(ostc_ctx *ctx, BlockRes &B, DevState in, bool chem) {
   if (ctx->der.n_spec == kFixedNS) launch_mix_source_t<kFixedNS>(ctx, B, in, chem);
   else launch_mix_source_t<0>(ctx, B, in, chem);
 }
+void launch_chem_epi(ostc_ctx *ctx, BlockRes &B, DevState in) {
+  long tok = begin_t(ctx, "chem_implicit");
+  if (ctx->der.n_spec == kFixedNS)
+    k_mix_chem_epi<kFixedNS><<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, in, B.dq, ctx->d_dt);
+  else
+    k_mix_chem_epi<0><<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, in, B.dq, ctx->d_dt);
+  end_t(ctx, tok);
+}
+
 void launch_mix_props(ostc_ctx *ctx, BlockRes &B, DevState st) {
   if (ctx->der.n_spec == kFixedNS)
     k_mix_props<kFixedNS><<<grid_for(ctx, B.db.plane, 128), 128, 0, ctx->stream>>>(B.db, st);
@@ -1546,13 +1556,15 @@ int enqueue_step_mix(ostc_ctx *ctx) {
     for (size_t bi = 0; bi < ctx->blk.size(); ++bi) {
       BlockRes &B = ctx->blk[bi];
       const DevState in = state_of(B, sin);
+      const bool chem = ctx->der.reaction == 1, implicit = chem && ctx->chem_mode == OSTC_CHEM_POINT_IMPLICIT;
       {
         long tok = begin_t(ctx, "source");
-        launch_mix_source(ctx, B, in, ctx->der.reaction == 1);
+        launch_mix_source(ctx, B, in, chem && !implicit);
         end_t(ctx, tok);
       }
       launch_fvs(ctx, B, in);
       if (ctx->der.viscous_order != 0) launch_mix_visc(ctx, B, in);
+      if (implicit) launch_chem_epi(ctx, B, in);
       {
         long tok = begin_t(ctx, "update");
         if (ctx->der.n_spec == kFixedNS)
@@ -1931,6 +1943,24 @@ int ostc_set_precision(ostc_ctx *ctx, int mode) {
   return OSTC_OK;
 }
 
+int ostc_set_chem_mode(ostc_ctx *ctx, int mode) {
+  if (!ctx) return OSTC_EINVAL;
+  if (mode != OSTC_CHEM_EXPLICIT && mode != OSTC_CHEM_POINT_IMPLICIT) {
+    ctx->err = "unknown chemistry mode";
+    return OSTC_EINVAL;
+  }
+  if (mode == OSTC_CHEM_POINT_IMPLICIT && !(ctx->mixture && ctx->der.reaction == 1)) {
+    ctx->err = "point-implicit chemistry needs a finite-rate mixture (species = 1, reaction = 1)";
+    return OSTC_EINVAL;
+  }
+  if (ctx->graph && ctx->chem_mode != mode) {
+    cudaGraphExecDestroy(ctx->graph);
+    ctx->graph = nullptr;
+  }
+  ctx->chem_mode = mode;
+  return OSTC_OK;
+}
+
 int ostc_set_state(ostc_ctx *ctx, int block, const double *bv, const double *sv, int ptr_kind) {
   if (!ctx || !bv || block < 0 || block >= (int)ctx->blk.size()) return OSTC_EINVAL;
   if (ctx->mixture && !sv) {
@@ -2011,9 +2041,12 @@ int ostc_rhs(ostc_ctx *ctx, int block, unsigned mask, double *dq, int ptr_kind) 
   if (ctx->mixture) {
     // source (dq initialised by it, RK.cuh:116), flux-split WENO7, viscous
     const DevState in = state_of(B, 0);
-    launch_mix_source(ctx, B, in, (mask & OSTC_TERM_SOURCE) && ctx->der.reaction == 1);
+    const bool chem = (mask & OSTC_TERM_SOURCE) && ctx->der.reaction == 1;
+    const bool implicit = chem && ctx->chem_mode == OSTC_CHEM_POINT_IMPLICIT;
+    launch_mix_source(ctx, B, in, chem && !implicit);
     if (mask & OSTC_TERM_INVISCID) launch_fvs(ctx, B, in);
     if ((mask & OSTC_TERM_VISCOUS) && ctx->der.viscous_order != 0) launch_mix_visc(ctx, B, in);
+    if (implicit) launch_chem_epi(ctx, B, in);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(dq, B.dq, (size_t)nv * B.db.n * sizeof(double),
                        ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));

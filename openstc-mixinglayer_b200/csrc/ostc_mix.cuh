@@ -85,6 +85,34 @@ __global__ void __launch_bounds__(128) k_mix_source(DevBlock b, DevState s, doub
   }
 }
 
+// Point-implicit chemistry (chem mode 1, an extension of the RK3 path): after the fluxes, add the
+// chemical source J omega to dq and replace the species part by the solution of
+// (I - dt J_chem) x = dq_species (EPI + solve_chem_system, FiniteRateChem.cu:233-254, 302-357, with the
+// stage's global dt), one cell per thread, every cell of the block in one launch.
+template <int NS>
+__global__ void __launch_bounds__(128) k_mix_chem_epi(DevBlock b, DevState s, double *__restrict__ dq,
+                                                       const double *dtp) {
+  const long long P = b.plane;
+  const int ns = OSTC_NS;
+  const double dt = *dtp;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % b.mx);
+    const long long r = n / b.mx;
+    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const long long p = b.id(i, j, k);
+    double y[Spec<NS>::A], om[Spec<NS>::A], jc[Spec<NS>::A * Spec<NS>::A], rhs[Spec<NS>::A];
+    for (int l = 0; l < ns; ++l) y[l] = s.sv[l * P + p];
+    for (int l = 0; l < ns * ns; ++l) jc[l] = 0.0;
+    mix_chemistry<NS>(s.bv[p], s.bv[5 * P + p], y, om, jc);
+    const double jac = b.jac[p];
+    for (int l = 0; l < ns; ++l) rhs[l] = dq[(5 + l) * b.n + n] + jac * om[l];
+    for (int m = 0; m < ns; ++m)
+      for (int q = 0; q < ns; ++q) jc[m * ns + q] = (m == q ? 1.0 : 0.0) - dt * jc[m * ns + q];
+    mix_lu_solve<NS>(jc, rhs);
+    for (int l = 0; l < ns; ++l) dq[(5 + l) * b.n + n] = rhs[l];
+  }
+}
+
 // ------------------------------------------------------------------ flux-split WENO7 sweeps
 
 // Tile geometry of the sweeps: TD faces along the sweep direction (TD-1 nodes finalised per tile),

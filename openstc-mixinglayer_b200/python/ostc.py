@@ -18,13 +18,14 @@ OSTC_HOST, OSTC_DEVICE = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 TERM_INVISCID, TERM_VISCOUS, TERM_SOURCE, TERM_ALL = 1, 2, 4, 7
 FLAG_NONPOSITIVE, FLAG_NAN = 1, 2
+CHEM_EXPLICIT, CHEM_POINT_IMPLICIT = 0, 1
 
 EXPORTS = [
     "ostc_create", "ostc_destroy", "ostc_last_error", "ostc_n_blocks", "ostc_block_dims", "ostc_n_var",
     "ostc_set_precision", "ostc_set_state", "ostc_get_state", "ostc_rhs", "ostc_rk3_step",
     "ostc_physical_time", "ostc_store_residual_reference", "ostc_residual", "ostc_error_flags",
     "ostc_device_view", "ostc_profile_steps", "ostc_total_nodes", "ostc_probe_case", "ostc_timed_steps",
-    "ostc_step_kernel_count", "ostc_residual_noalloc",
+    "ostc_step_kernel_count", "ostc_residual_noalloc", "ostc_set_chem_mode",
 ]
 
 
@@ -63,6 +64,7 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.ostc_block_dims.argtypes = [vp, ip, ctypes.POINTER(ip)]
     lib.ostc_n_var.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
     lib.ostc_set_precision.argtypes = [vp, ip]
+    lib.ostc_set_chem_mode.argtypes = [vp, ip]
     lib.ostc_set_state.argtypes = [vp, ip, vp, vp, ip]
     lib.ostc_get_state.argtypes = [vp, ip, vp, vp, vp, ip]
     lib.ostc_rhs.argtypes = [vp, ip, ctypes.c_uint, vp, ip]
@@ -156,6 +158,9 @@ class Solver:
 
     def set_precision(self, mode: int):
         self._check(self.lib.ostc_set_precision(self.h, mode))
+
+    def set_chem_mode(self, mode: int):
+        self._check(self.lib.ostc_set_chem_mode(self.h, mode))
 
     def set_state(self, bv: np.ndarray, block: int = 0, sv: np.ndarray | None = None):
         """bv [6][mz][my][mx] (rho, u, v, w, p, T); sv [n_spec][mz][my][mx] mass fractions for mixtures."""

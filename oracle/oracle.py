@@ -64,7 +64,7 @@ class OrcCase(ctypes.Structure):
                 ("n_face", ctypes.c_int), ("face", OrcFace * 16), ("n_spec", ctypes.c_int),
                 ("finite_rate", ctypes.c_int), ("chem", ctypes.POINTER(OrcChem)), ("weno_eps_scale", ctypes.c_double),
                 ("v_ref", ctypes.c_double), ("has_init", ctypes.c_int), ("init_bv", ctypes.c_double * 6),
-                ("init_sv", ctypes.c_double * MAXS)]
+                ("init_sv", ctypes.c_double * MAXS), ("chem_mode", ctypes.c_int)]
 
 
 def riemann_of(reconstruction: int, inviscid_scheme: int) -> int:
@@ -142,9 +142,10 @@ dp_arr = ctypes.POINTER(ctypes.c_double)
 class Oracle:
     """CPU restatement of one single-block case (see ostc_cases.Case)."""
 
-    def __init__(self, case):
+    def __init__(self, case, chem_mode: int = 0):
         self.lib = load()
         c = OrcCase()
+        c.chem_mode = chem_mode
         c.mx, c.my, c.mz = case.mx, case.my, case.mz
         s = case.scheme
         c.reconstruction, c.inviscid_scheme, c.viscous_order = s["reconstruction"], s["inviscid_scheme"], s["viscous_order"]

@@ -43,6 +43,7 @@ struct orc_ctx {
    * block (update_physical_properties, FieldOperation.cuh:107-140) */
   int ns, nv;
   double *sv, *cond, *rhod, *cpm, *gam, *acs;
+  double dt_cur; /* dt of the current step (point-implicit chemistry) */
   face_t f[16];
   int nf;
   double t;
@@ -1013,7 +1014,49 @@ static double arrhenius(double t, double A, double b, double Ea) { return A * po
 /* finite_rate_chemistry (FiniteRateChem.cu:7-58) with forward_reaction_rate (:60-102),
  * backward_reaction_rate (:108-150), rate_of_progress (:152-177), chemical_source (:179-195):
  * dq[5+l] += jac * omega_l at interior node (i,j,k). */
-static void chemistry_node(orc_ctx *o, int i, int j, int k) {
+static void chemistry_node_jac(orc_ctx *o, int i, int j, int k, int implicit);
+static void chemistry_node(orc_ctx *o, int i, int j, int k) { chemistry_node_jac(o, i, j, k, 0); }
+
+/* solve_chem_system (FiniteRateChem.cu:302-357): column-pivoted LU in place, then substitution. */
+static void lu_solve(double *lhs, double *b, int dim) {
+  int ipiv[ORC_MAX_SPEC] = {0};
+  for (int n = 0; n < dim; ++n) {
+    int ik = n;
+    for (int m = n; m < dim; ++m) {
+      for (int t = 0; t < n; ++t) lhs[m * dim + n] -= lhs[m * dim + t] * lhs[t * dim + n];
+      if (fabs(lhs[m * dim + n]) > fabs(lhs[ik * dim + n])) ik = m;
+    }
+    ipiv[n] = ik;
+    if (ik != n)
+      for (int t = 0; t < dim; ++t) {
+        const double mid = lhs[ik * dim + t];
+        lhs[ik * dim + t] = lhs[n * dim + t];
+        lhs[n * dim + t] = mid;
+      }
+    for (int p = n + 1; p < dim; ++p)
+      for (int t = 0; t < n; ++t) lhs[n * dim + p] -= lhs[n * dim + t] * lhs[t * dim + p];
+    for (int m = n + 1; m < dim; ++m) lhs[m * dim + n] /= lhs[n * dim + n];
+  }
+  for (int m = 0; m < dim; ++m) {
+    const int t = ipiv[m];
+    if (t != m) {
+      const double mid = b[t];
+      b[t] = b[m];
+      b[m] = mid;
+    }
+  }
+  for (int m = 1; m < dim; ++m)
+    for (int t = 0; t < m; ++t) b[m] -= lhs[m * dim + t] * b[t];
+  b[dim - 1] /= lhs[dim * dim - 1];
+  for (int m = dim - 2; m >= 0; --m) {
+    for (int t = m + 1; t < dim; ++t) b[m] -= lhs[m * dim + t] * b[t];
+    b[m] /= lhs[m * dim + m];
+  }
+}
+
+/* implicit = 1: also compute_chem_src_jacobian (FiniteRateChem.cu:197-217) and replace the species dq
+ * by the EPI solution (FiniteRateChem.cu:233-254) with dt_cur. */
+static void chemistry_node_jac(orc_ctx *o, int i, int j, int k, int implicit) {
   const orc_chem *ch = o->c.chem;
   const int ns = ch->n_spec, nr = ch->n_reac;
   const long P = o->P, N = (long)o->mx * o->my * o->mz;
@@ -1104,6 +1147,24 @@ static void chemistry_node(orc_ctx *o, int i, int j, int k) {
     des *= ch->mw[l] * 1e+3;
     o->dq[(5 + l) * N + q] += jac * (cre - des);
   }
+  if (!implicit) return;
+  double lhs[ORC_MAX_SPEC * ORC_MAX_SPEC], b[ORC_MAX_SPEC];
+  for (int m = 0; m < ns; ++m)
+    for (int n = 0; n < ns; ++n) {
+      double zz = 0;
+      const double yn = o->sv[n * P + p];
+      if (yn > 1e-25) {
+        for (int r = 0; r < nr; ++r)
+          zz += (ch->stoi_b[r * ns + m] - ch->stoi_f[r * ns + m]) *
+                (ch->stoi_f[r * ns + n] * q1[r] - ch->stoi_b[r * ns + n] * q2[r]);
+        zz /= rho * yn;
+      }
+      const double jm = ch->mw[m] * zz * 1e+3;
+      lhs[m * ns + n] = (m == n ? 1.0 : 0.0) - o->dt_cur * jm;
+    }
+  for (int l = 0; l < ns; ++l) b[l] = o->dq[(5 + l) * N + q];
+  lu_solve(lhs, b, ns);
+  for (int l = 0; l < ns; ++l) o->dq[(5 + l) * N + q] = b[l];
 }
 
 /* ---------------------------------------------------------------- flux-split WENO (51/52/71/72) */
@@ -1948,7 +2009,7 @@ void orc_get_mixture(const orc_ctx *o, double *sv, double *cond, double *rho_d, 
 void orc_rhs(orc_ctx *o, unsigned mask, double *dq) {
   const long N = (long)o->mx * o->my * o->mz;
   memset(o->dq, 0, sizeof(double) * o->nv * N);
-  if ((mask & 4u) && o->ns && o->c.finite_rate)
+  if ((mask & 4u) && o->ns && o->c.finite_rate && !o->c.chem_mode)
     for (int k = 0; k < o->mz; ++k)
       for (int j = 0; j < o->my; ++j)
         for (int i = 0; i < o->mx; ++i) chemistry_node(o, i, j, k);
@@ -1960,6 +2021,10 @@ void orc_rhs(orc_ctx *o, unsigned mask, double *dq) {
       else pv_direction(o, d);
     }
   if ((mask & 2u) && o->c.viscous_order != 0) viscous(o);
+  if ((mask & 4u) && o->ns && o->c.finite_rate && o->c.chem_mode)
+    for (int k = 0; k < o->mz; ++k)
+      for (int j = 0; j < o->my; ++j)
+        for (int i = 0; i < o->mx; ++i) chemistry_node_jac(o, i, j, k, 1);
   if (dq) memcpy(dq, o->dq, sizeof(double) * o->nv * N);
 }
 
@@ -1970,6 +2035,7 @@ double orc_step(orc_ctx *o, int n) {
     memcpy(o->qn, o->cv, sizeof(double) * o->nv * o->P);
     for (int rk = 0; rk < 3; ++rk) {
       if (!o->c.fixed_time_step && rk == 0) dt = orc_dt(o);
+      o->dt_cur = dt;
       orc_rhs(o, 7u, NULL);
       rk_update(o, dt, rk);
       fill_ghosts(o);
@@ -2213,6 +2279,7 @@ double orc_multi_step(orc_multi *m, int n) {
         }
       }
       for (int b = 0; b < m->nb; ++b) {
+        m->b[b]->dt_cur = dt;
         orc_rhs(m->b[b], 7u, NULL);
         rk_update(m->b[b], dt, rk);
         apply_bcs(m->b[b]);

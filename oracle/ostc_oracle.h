@@ -68,6 +68,10 @@ typedef struct {
   int has_init;
   double init_bv[6];
   double init_sv[ORC_MAX_SPEC];
+  /* 0: explicit chemistry (the reference's RK3); 1: point-implicit -- after the fluxes the species
+   * part of dq is replaced by the solution of (I - dt J_chem) x = dq_s (EPI, solve_chem_system,
+   * FiniteRateChem.cu:197-254, 302-357) with the step's dt */
+  int chem_mode;
 } orc_case;
 
 typedef struct orc_ctx orc_ctx;

@@ -1,0 +1,42 @@
+"""Host-side checks of the chemistry restatements (no GPU): the CHEMKIN readers agree, the
+point-implicit treatment tends to the explicit one as dt -> 0, and the reacting case conserves
+element mass through the chemical source."""
+import numpy as np
+import pytest
+
+import ostc_cases as oc
+from oracle import Oracle
+
+
+def test_h2_mechanism_tables(built):
+    case = oc.reacting_mixing_layer_3d(mx=8, my=8, mz=6)
+    t = case.mixture["tables"]
+    assert t.n_spec == 9 and t.n_reac == 19  # 21 reactions, two DUPLICATE pairs merged
+    assert t.names == ["H", "H2", "H2O", "H2O2", "HO2", "O", "O2", "OH", "N2"]
+    # Troe fall-off reactions (label 6) and third-body reactions (label 4) of the mechanism
+    assert int(np.sum(t.label == 6)) == 2 and int(np.sum(t.label == 4)) == 4 and int(np.sum(t.label == 3)) == 2
+    # molecular weights from the element table
+    assert abs(t.mw[t.names.index("H2O")] - (2 * 1.008 + 15.999)) < 1e-12
+
+
+def test_chemical_source_conserves_mass(built):
+    """sum_k omega_k = 0: the source moves mass between species and creates none."""
+    case = oc.reacting_mixing_layer_3d(mx=10, my=12, mz=6)
+    o = Oracle(case)
+    o.set_state(case.bv)
+    dq = o.rhs(4)
+    s = dq[5:].sum(axis=0)
+    assert np.max(np.abs(s)) <= 1e-9 * np.max(np.abs(dq[5:]))
+
+
+def test_point_implicit_reduces_to_explicit(built):
+    """Before any step the oracle's step size is 0, so (I - dt J) is the identity and the
+    point-implicit RHS (source added after the fluxes) equals the explicit one to rounding."""
+    case = oc.reacting_mixing_layer_3d(mx=10, my=12, mz=6)
+    oe = Oracle(case)
+    oe.set_state(case.bv)
+    oi = Oracle(case, chem_mode=1)
+    oi.set_state(case.bv)
+    de = oe.rhs(7)
+    di = oi.rhs(7)
+    assert np.allclose(di, de, rtol=1e-12, atol=1e-12 * np.max(np.abs(de)))
