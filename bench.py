@@ -15,6 +15,11 @@ inviscid + viscous RHS, update, boundaries).  One cell-step = one interior node 
            (ostc_get_state)
   roofline dominant kernel (by device time), algorithmic bytes per launch / average launch time
   cpu_baseline  the serial C restatement of the same path (oracle/) on a sub-grid sample
+  reacting the 9-species H2/air mixing layer, 384 x 192 x 96, flux-split characteristic WENO7,
+           finite-rate chemistry (explicit, and the point-implicit batched 9x9 LU extension), FP64
+  multiblock  12 blocks of seeded uneven i extents (j, k extents shared by the chain) joined by 1:1
+           interfaces, about 40 M nodes, AWENO7 + HLLC, FP64; every block's sweeps, update,
+           boundary faces and interface exchange are one CUDA graph per step
 
 --impl reference times that C restatement on all host cores (independent sub-grid replicas, one
 process per core): the reference's own implementation of this path exists only as CUDA device code.
@@ -50,6 +55,11 @@ FALLBACK_HBM_GBS = 6650.0
 #               cv(5) + bv(6) + mu written                                                    = 42 x 8
 #   cfl_dt      metric(9) + rho,u,v,w,T(5) + mu read                                          = 15 x 8
 ALGO_BYTES_PER_NODE = {"flux_x": 152, "flux_y": 192, "flux_z": 192, "visc_update": 336, "cfl_dt": 120}
+# DRAM bytes per node measured by one ncu capture of the kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum over the nodes of the launch, 256x128x64 case of the same workload; traffic
+# grows with the node count, so a full-size launch moves this figure times its nodes):
+# profiles/k_flux_march_fp64_awe7_256x128x64.md (y sweep) and profiles/k_flux_march_z_fp64_awe7_256x128x64.md.
+MEASURED_TRAFFIC_PER_NODE = {"flux_y": 209.8}
 # Whole fused stage (three state passes + metric): 8 (3 n_var + 10) bytes per cell-stage, n_var = 5
 STAGE_BYTES = 8 * (3 * 5 + 10)
 
@@ -65,6 +75,8 @@ def parse():
     p.add_argument("--no-mixed", action="store_true")
     p.add_argument("--cpu-sample", type=int, nargs=3, default=[96, 64, 48])
     p.add_argument("--cpu-steps", type=int, default=3)
+    p.add_argument("--no-extra", action="store_true",
+                   help="skip the reacting (9-species) and uneven multi-block workloads")
     return p.parse_args()
 
 
@@ -199,6 +211,23 @@ def run_reference(args):
 
 # ------------------------------------------------------------------------------- GPU leg
 
+def reduce_max(x: float, dist, device) -> float:
+    """Max over ranks of a per-rank device time (every rank calls it; identity without a group)."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, nodes_per_rank: int, steps: int, ms_max: float) -> float:
+    """Cell-steps/s of the whole job: every rank advances its own replica of nodes_per_rank nodes by
+    `steps` steps; the job takes as long as its slowest rank."""
+    return world * nodes_per_rank * steps / (ms_max / 1e3)
+
+
 def run_ours(args):
     world, rank, local = dist_env()
     import torch
@@ -216,11 +245,7 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     def allmax(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, "cuda")
 
     import ostc
     import ostc_cases as oc
@@ -248,7 +273,7 @@ def run_ours(args):
     barrier()
     ms_max = allmax(ms)
     nodes = s.total_nodes()
-    value = world * nodes * K / (ms_max / 1e3)
+    value = whole_job_rate(world, nodes, K, ms_max)
     launches_per_step = s.step_kernel_count()
     cv64, _ = s.get_state()
     flags = s.error_flags()
@@ -283,11 +308,8 @@ def run_ours(args):
     algo = ALGO_BYTES_PER_NODE[dom] * nodes
     achieved = algo / (avg_ms / 1e3) / 1e9
     traffic = None
-    tfile = ROOT / "profiles" / "traffic_per_node.json"
-    if tfile.exists():
-        tb = json.loads(tfile.read_text()).get(dom)
-        if tb:
-            traffic = tb * nodes
+    if dom in MEASURED_TRAFFIC_PER_NODE:
+        traffic = MEASURED_TRAFFIC_PER_NODE[dom] * nodes
     step_ms = ms_max / K
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": traffic, "algorithmic_bytes_per_launch": algo,
@@ -325,6 +347,10 @@ def run_ours(args):
         se.close()
     s.close()
 
+    extra = {}
+    if not args.no_extra:
+        extra = run_extra(args, local, barrier, allmax, world)
+
     cpu = None
     if rank == 0 and world == 1:
         ensure_oracle_built()
@@ -340,11 +366,58 @@ def run_ours(args):
                 "dtype": "f64", "data": "synthetic (seeded tanh shear layer + white noise; no dataset)",
                 "config": config_dict(args), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "mixed": mixed, "clocks": clocks, "gpu_launches": launches_per_step * K,
-                "error_flags": flags}
+                "error_flags": flags, **extra}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_extra(args, local, barrier, allmax, world):
+    """The reacting (C3-shaped) and multi-block (C4-shaped) workloads: device-timed cell-steps/s, the
+    per-kernel split, and their settings.  Warm-up 2 steps, 5 timed steps each."""
+    import ostc
+    import ostc_cases as oc
+
+    out = {}
+    # reacting 9-species H2/air
+    rc = oc.reacting_mixing_layer_3d(mx=384, my=192, mz=96, seed=0)
+    tmp = tempfile.mkdtemp(prefix="ostc_bench_react_")
+    oc.write_case(rc, tmp)
+    react = {"workload": "reacting H2/air mixing layer 384x192x96, 9 species / 19 reactions, WENO7-Z "
+                         "characteristic flux splitting (inviscid_scheme 72), mixture-averaged transport, FP64",
+             "nodes": rc.nodes}
+    for mode, key in ((ostc.CHEM_EXPLICIT, "explicit"), (ostc.CHEM_POINT_IMPLICIT, "point_implicit")):
+        s = ostc.Solver(tmp, device=local)
+        s.set_chem_mode(mode)
+        s.set_state(rc.bv, sv=rc.sv)
+        s.step(2)
+        barrier()
+        ms = allmax(s.timed_steps(5))
+        prof = s.profile(1)
+        react[key] = {"value": world * rc.nodes * 5 / (ms / 1e3), "ms_per_step": ms / 5,
+                      "kernels_ms_per_step": {k: v[1] for k, v in prof.items()}, "flags": s.error_flags()}
+        s.close()
+    react["value"] = react["explicit"]["value"]
+    out["reacting"] = react
+    # uneven multi-block chain
+    mc = oc.multiblock_mixing_layer_3d(nb=12, lo=32, hi=256, seed=0)
+    tmp = tempfile.mkdtemp(prefix="ostc_bench_mb_")
+    oc.write_case(mc, tmp)
+    s = ostc.Solver(tmp, device=local)
+    for b, blk in enumerate(mc.blocks):
+        s.set_state(blk.bv, block=b)
+    s.step(2)
+    barrier()
+    ms = allmax(s.timed_steps(5))
+    prof = s.profile(1)
+    out["multiblock"] = {"workload": f"{len(mc.blocks)} blocks, i extents {[b.mx for b in mc.blocks]}, "
+                                     f"j x k {mc.blocks[0].my} x {mc.blocks[0].mz}, 1:1 interfaces, AWENO7 + HLLC, FP64",
+                         "nodes": mc.nodes, "value": world * mc.nodes * 5 / (ms / 1e3), "ms_per_step": ms / 5,
+                         "kernels_per_step": s.step_kernel_count(),
+                         "kernels_ms_per_step": {k: v[1] for k, v in prof.items()}, "flags": s.error_flags()}
+    s.close()
+    return out
 
 
 def main():

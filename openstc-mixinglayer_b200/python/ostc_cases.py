@@ -326,15 +326,20 @@ def _write_multi(case: MultiCase, directory: os.PathLike) -> Path:
     return d
 
 
-def multiblock_mixing_layer_3d(nb=12, lo=32, hi=256, my=64, mz=32, seed=0, steps=100, mc=0.5, re=1000.0,
+def multiblock_mixing_layer_3d(nb=12, lo=32, hi=256, my=None, mz=None, seed=0, steps=100, mc=0.5, re=1000.0,
                                t0=300.0, delta0=1e-3, h=0.125, reconstruction=5, inviscid_scheme=4, cfl=0.5,
                                dims=None) -> MultiCase:
     """nb blocks chained along x with seeded uneven i extents (uniform in [lo, hi]; `dims` overrides),
-    common j / k extents, joined by 1:1 interfaces (block b's i-max face on block b+1's i-min face,
+    common j / k extents (drawn once in [lo, hi] unless given), joined by 1:1 interfaces (block b's i-max face on block b+1's i-min face,
     coincident nodes).  Outflow at the two x ends, far-field y, periodic z within every block.  Shear
     layer u = dU/2 tanh(2y/delta0), Mc = 0.5, with 1e-2 dU N(0,1) exp(-(y/delta0)^2) seeded noise in u, v, w."""
     rng = np.random.default_rng(seed)
     mxs = list(dims) if dims is not None else [int(v) for v in rng.integers(lo, hi + 1, nb)]
+    # the chain shares its j and k extents (1:1 faces); unless given they are drawn once from the seed
+    if my is None:
+        my = int(rng.integers(lo, hi + 1))
+    if mz is None:
+        mz = int(rng.integers(lo, hi + 1))
     nb = len(mxs)
     c0 = math.sqrt(GAMMA * R_AIR * t0)
     du = 2 * mc * c0
