@@ -379,6 +379,97 @@ __global__ void __launch_bounds__(64, MarchOcc<T>::blocks) k_flux_march(DevBlock
   if constexpr (PIPE) cp_async_wait_all();
 }
 
+// y / z sweep as a tile: a block of TXL consecutive i (coalesced rows) x TD threads along the sweep
+// direction stages TF - 1 + 2*NG nodes per lane in shared memory (cv, p, node flux, metric row,
+// Jacobian), computes FPT faces per thread and finalises TF - 1 nodes per lane, as the x sweep does
+// for rows.  Against the column march it trades (TF - 1 + 2 NG) / (TF - 1) node loads per node for
+// independent faces with no serial dependence along the column; the autotuner picks between them.
+// TF = TD * FPT faces per tile along the sweep (TF - 1 nodes finalised), FPT faces per thread.
+template <int NG, int TXL, int TF, typename T>
+constexpr size_t tile_smem_bytes() {
+  return (size_t)(15 * (TF - 1 + 2 * NG) + 5 * TF) * TXL * sizeof(T);
+}
+
+template <int DIR, int NG, int RS, typename T, int TXL, int TD, int FPT>
+__global__ void __launch_bounds__(TXL * TD) k_flux_tile(DevBlock b, DevState s, double *__restrict__ dq) {
+  constexpr int TF = TD * FPT;
+  constexpr int L = TF - 1;
+  constexpr int NP = L + 2 * NG;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T *sq = reinterpret_cast<T *>(smraw);  // [6][NP][TXL]  cv 0..4, p
+  T *sf = sq + 6 * NP * TXL;             // [5][NP][TXL]  node flux
+  T *smt = sf + 5 * NP * TXL;            // [4][NP][TXL]  metric row, Jacobian
+  T *sfc = smt + 4 * NP * TXL;           // [5][TF][TXL]  face flux
+  const int lane = threadIdx.x;
+  const int i = blockIdx.x * TXL + lane;
+  const int d0 = blockIdx.y * L;
+  const int o = blockIdx.z;
+  const int nd = DIR == 1 ? b.my : b.mz;
+  const bool lane_ok = i < b.mx;
+  const long long P = b.plane;
+  const long long stride = DIR == 1 ? (long long)b.pitch : (long long)b.pitch * b.sy;
+  const long long base = DIR == 1 ? b.id(i < b.mx ? i : 0, 0, o) : b.id(i < b.mx ? i : 0, o, 0);
+  const double *__restrict__ mrow = b.met + (long long)DIR * 3 * P;
+  auto at = [&](T *a, int v, int n) -> T & { return a[(v * NP + n) * TXL + lane]; };
+  if (lane_ok) {
+    for (int n = threadIdx.y; n < NP; n += TD) {
+      const int d = d0 - NG + n;
+      if (d >= nd + NG) continue;
+      const long long p = base + (long long)d * stride;
+      T bb[5], kk[3];
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        at(sq, l, n) = (T)s.cv[l * P + p];
+        bb[l] = (T)s.bv[l * P + p];
+      }
+      at(sq, 5, n) = bb[4];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        kk[c] = (T)mrow[c * P + p];
+        at(smt, c, n) = kk[c];
+      }
+      const T jj = (T)b.jac[p];
+      at(smt, 3, n) = jj;
+      T f[5];
+      node_flux<T>(bb, (T)s.cv[4 * P + p], kk, jj, f);
+#pragma unroll
+      for (int l = 0; l < 5; ++l) at(sf, l, n) = f[l];
+    }
+  }
+  __syncthreads();
+  for (int r = 0; r < FPT; ++r) {
+    const int t = threadIdx.y + r * TD;
+    const int face = d0 - 1 + t;  // left node of this face
+    if (lane_ok && face < nd) {
+      auto q = [&](int st, int v) -> T { return at(sq, v, t + st); };
+      const T mt0[3] = {at(smt, 0, t + NG - 1), at(smt, 1, t + NG - 1), at(smt, 2, t + NG - 1)};
+      const T mt1[3] = {at(smt, 0, t + NG), at(smt, 1, t + NG), at(smt, 2, t + NG)};
+      T fc[5];
+      aweno_face_flux<NG, RS, T>(q, mt0, mt1, at(smt, 3, t + NG - 1), at(smt, 3, t + NG), fc);
+#pragma unroll
+      for (int l = 0; l < 5; ++l) sfc[(l * TF + t) * TXL + lane] = fc[l];
+    }
+  }
+  __syncthreads();
+  for (int r = 0; r < FPT; ++r) {
+    const int t = threadIdx.y + r * TD;
+    const int d = d0 - 1 + t;
+    if (lane_ok && t >= 1 && d < nd) {
+      const long long qi = DIR == 1 ? b.iq(i, d, o) : b.iq(i, o, d);
+      const int c = t - 1 + NG;
+      auto f = [&](int m, int l) -> T { return at(sf, l, c + m); };
+      const bool cds = d < nd - 2 * NG;
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        double v = dq[l * b.n + qi];
+        v -= (double)(sfc[(l * TF + t) * TXL + lane] - sfc[(l * TF + t - 1) * TXL + lane]);
+        if (cds) v += (double)cds_correction<NG, T>(f, l);
+        dq[l * b.n + qi] = v;
+      }
+    }
+  }
+}
+
 // Dynamic shared memory of one 64-thread march block: the ring, plus the prefetch buffers in FP32.
 template <typename T>
 constexpr size_t march_smem_bytes(int ng) {
@@ -1064,6 +1155,7 @@ struct BlockRes {
   double *last = nullptr;
   std::vector<DevFace> faces;  // file order
   std::vector<DevInner> inner;  // interfaces of this block, file order
+  int yz_var[2][2] = {{-1, -1}, {-1, -1}};  // autotuned y / z sweep variant [FP64, mixed][y, z]
   std::vector<int> inner_target;
 };
 
@@ -1096,6 +1188,7 @@ struct ostc_ctx {
   unsigned *d_flags = nullptr;
   cudaGraphExec_t graph = nullptr;
   int graph_precision = -1;
+  bool tuned[2] = {false, false};  // y / z sweep autotuning done [FP64, mixed]
   int graph_kernels = 0;
   std::string err;
   int sm_count = 148;
@@ -1299,6 +1392,103 @@ void launch_mix_props(ostc_ctx *ctx, BlockRes &B, DevState st) {
     k_mix_props<0><<<grid_for(ctx, B.db.plane, 128), 128, 0, ctx->stream>>>(B.db, st);
 }
 
+DevState state_of(BlockRes &B, int s);
+
+// y / z sweep variants: 0 = column march, 1..3 = tiles of the shapes below (per precision: rows
+// of 128 bytes, and a block small enough for the register budget of the FP64 face arithmetic).
+template <typename T> struct YzShapes;
+// {lanes, threads along the sweep, faces per thread} of tile variants 1..3
+template <> struct YzShapes<float> {
+  static constexpr int X1 = 32, D1 = 16, F1 = 1, X2 = 32, D2 = 8, F2 = 2, X3 = 32, D3 = 4, F3 = 4;
+};
+template <> struct YzShapes<double> {
+  static constexpr int X1 = 16, D1 = 16, F1 = 1, X2 = 16, D2 = 8, F2 = 2, X3 = 32, D3 = 4, F3 = 4;
+};
+constexpr int kYzVariants = 4;
+
+template <typename T, int D, int N, int R>
+void launch_yz_v(ostc_ctx *ctx, BlockRes &B, DevState in, int variant) {
+  const DevBlock &b = B.db;
+  const int n_dir = D == 1 ? b.my : b.mz, n_o = D == 1 ? b.mz : b.my;
+  if (variant >= 1 && variant <= 3) {
+    using S = YzShapes<T>;
+#define OSTC_TILE(X, DD, F)                                                                             \
+  {                                                                                                   \
+    constexpr int TF = DD * F;                                                                        \
+    dim3 grid((b.mx + X - 1) / X, (n_dir + TF - 2) / (TF - 1), n_o);                                   \
+    k_flux_tile<D, N, R, T, X, DD, F><<<grid, dim3(X, DD), tile_smem_bytes<N, X, TF, T>(), ctx->stream>>>( \
+        b, in, B.dq);                                                                                 \
+  }
+    if (variant == 1) OSTC_TILE(S::X1, S::D1, S::F1)
+    else if (variant == 2) OSTC_TILE(S::X2, S::D2, S::F2)
+    else OSTC_TILE(S::X3, S::D3, S::F3)
+#undef OSTC_TILE
+    return;
+  }
+  // split columns into segments so that the grid fills the GPU at least ~4 waves deep
+  const long long cols = (long long)((b.mx + 31) / 32) * ((n_o + 1) / 2);
+  int nseg = (int)std::max<long long>(1, (ctx->sm_count * 12 + cols - 1) / cols);
+  int seg = std::max(2 * N, (n_dir + nseg - 1) / nseg);
+  nseg = (n_dir + seg - 1) / seg;
+  dim3 grid((b.mx + 31) / 32, (n_o + 1) / 2, nseg);
+  k_flux_march<D, N, R, T><<<grid, dim3(32, 2, 1), march_smem_bytes<T>(N), ctx->stream>>>(b, in, B.dq, seg);
+}
+
+template <typename T, int D>
+void launch_yz(ostc_ctx *ctx, BlockRes &B, DevState in, int variant) {
+  const int ng = ctx->der.ngg, rs = ctx->der.riemann;
+  if (ng == 3) {
+    if (rs == 4) launch_yz_v<T, D, 3, 4>(ctx, B, in, variant);
+    else if (rs == 1) launch_yz_v<T, D, 3, 1>(ctx, B, in, variant);
+    else launch_yz_v<T, D, 3, 3>(ctx, B, in, variant);
+  } else {
+    if (rs == 4) launch_yz_v<T, D, 4, 4>(ctx, B, in, variant);
+    else if (rs == 1) launch_yz_v<T, D, 4, 1>(ctx, B, in, variant);
+    else launch_yz_v<T, D, 4, 3>(ctx, B, in, variant);
+  }
+}
+
+// Autotuner of the y / z sweeps: on the context's current state (the sweeps only read the state and
+// accumulate into the dq scratch), time every variant for each block, direction and the active
+// precision with CUDA events on the library stream, and keep the fastest.  Runs once per precision,
+// outside any stream capture, before the step graph is built.
+template <typename T>
+int autotune_yz(ostc_ctx *ctx) {
+  const int pi = std::is_same_v<T, float> ? 1 : 0;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  for (auto &B : ctx->blk) {
+    const DevState in = state_of(B, 0);
+    for (int dir = 1; dir <= (B.db.mz > 1 ? 2 : 1); ++dir) {
+      float best = 1e30f;
+      int bv = 0;
+      for (int v = 0; v < kYzVariants; ++v) {
+        auto run = [&]() {
+          if (dir == 1) launch_yz<T, 1>(ctx, B, in, v);
+          else launch_yz<T, 2>(ctx, B, in, v);
+        };
+        run();  // warm-up
+        CK(cudaEventRecord(e0, ctx->stream));
+        for (int r = 0; r < 3; ++r) run();
+        CK(cudaEventRecord(e1, ctx->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+          best = ms;
+          bv = v;
+        }
+      }
+      B.yz_var[pi][dir - 1] = bv;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CK(cudaGetLastError());
+  return OSTC_OK;
+}
+
 // inviscid sweep of one block
 template <typename T>
 int launch_flux(ostc_ctx *ctx, BlockRes &B, DevState in) {
@@ -1333,36 +1523,12 @@ int launch_flux(ostc_ctx *ctx, BlockRes &B, DevState in) {
 #undef OSTC_FX
     end_t(ctx, tok);
   }
-  // y and z
+  // y and z: the variant the autotuner chose for this block and precision (column march by default)
   for (int dir = 1; dir <= (is3d ? 2 : 1); ++dir) {
-    const int n_dir = dir == 1 ? b.my : b.mz, n_o = dir == 1 ? b.mz : b.my;
-    // split columns into segments so that the grid fills the GPU at least ~4 waves deep
-    const long long cols = (long long)((b.mx + 31) / 32) * ((n_o + 1) / 2);
-    int nseg = (int)std::max<long long>(1, (ctx->sm_count * 12 + cols - 1) / cols);
-    int seg = std::max(2 * ng, (n_dir + nseg - 1) / nseg);
-    nseg = (n_dir + seg - 1) / seg;
-    dim3 grid((b.mx + 31) / 32, (n_o + 1) / 2, nseg);
-    dim3 block(32, 2, 1);
-    const size_t smem = march_smem_bytes<T>(ng);
+    const int v = B.yz_var[ctx->precision == OSTC_PREC_MIXED][dir - 1];
     long tok = begin_t(ctx, dir == 1 ? "flux_y" : "flux_z");
-#define OSTC_MARCH(D, N, R) k_flux_march<D, N, R, T><<<grid, block, smem, ctx->stream>>>(b, in, B.dq, seg)
-#define OSTC_MARCH_NR(D)                  \
-  if (ng == 3) {                           \
-    if (rs == 4) OSTC_MARCH(D, 3, 4);      \
-    else if (rs == 1) OSTC_MARCH(D, 3, 1); \
-    else OSTC_MARCH(D, 3, 3);              \
-  } else {                                 \
-    if (rs == 4) OSTC_MARCH(D, 4, 4);      \
-    else if (rs == 1) OSTC_MARCH(D, 4, 1); \
-    else OSTC_MARCH(D, 4, 3);              \
-  }
-    if (dir == 1) {
-      OSTC_MARCH_NR(1)
-    } else {
-      OSTC_MARCH_NR(2)
-    }
-#undef OSTC_MARCH_NR
-#undef OSTC_MARCH
+    if (dir == 1) launch_yz<T, 1>(ctx, B, in, v < 0 ? 0 : v);
+    else launch_yz<T, 2>(ctx, B, in, v < 0 ? 0 : v);
     end_t(ctx, tok);
   }
   return OSTC_OK;
@@ -1456,6 +1622,17 @@ bool set_march_attrs() {
   set((const void *)k_flux_march<2, 4, 1, T>, 4);
   set((const void *)k_flux_march<2, 4, 3, T>, 4);
   set((const void *)k_flux_march<2, 4, 4, T>, 4);
+  auto tset = [&](const void *fn, size_t bytes) {
+    ok = ok && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess;
+  };
+  using S = YzShapes<T>;
+#define OSTC_TSET(D, N, R)                                                                                      \
+  tset((const void *)k_flux_tile<D, N, R, T, S::X1, S::D1, S::F1>, tile_smem_bytes<N, S::X1, S::D1 * S::F1, T>()); \
+  tset((const void *)k_flux_tile<D, N, R, T, S::X2, S::D2, S::F2>, tile_smem_bytes<N, S::X2, S::D2 * S::F2, T>()); \
+  tset((const void *)k_flux_tile<D, N, R, T, S::X3, S::D3, S::F3>, tile_smem_bytes<N, S::X3, S::D3 * S::F3, T>());
+  OSTC_TSET(1, 3, 1) OSTC_TSET(1, 3, 3) OSTC_TSET(1, 3, 4) OSTC_TSET(1, 4, 1) OSTC_TSET(1, 4, 3) OSTC_TSET(1, 4, 4)
+  OSTC_TSET(2, 3, 1) OSTC_TSET(2, 3, 3) OSTC_TSET(2, 3, 4) OSTC_TSET(2, 4, 1) OSTC_TSET(2, 4, 3) OSTC_TSET(2, 4, 4)
+#undef OSTC_TSET
   ok = ok && cudaFuncSetAttribute((const void *)k_visc_update<T, true, 32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)visc_smem_bytes<T, true, 32, 4>()) == cudaSuccess;
   ok = ok && cudaFuncSetAttribute((const void *)k_visc_update<T, false, 32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1608,7 +1785,14 @@ int check_ready(ostc_ctx *ctx) {
     ctx->err = "upload of the species / reaction tables to constant memory failed";
     return OSTC_ECUDA;
   }
-  if (!ctx->initialised) return initialise(ctx);
+  if (!ctx->initialised) {
+    if (int r = initialise(ctx)) return r;
+  }
+  const int pi = ctx->precision == OSTC_PREC_MIXED ? 1 : 0;
+  if (ctx->der.inviscid_type == 1 && !ctx->tuned[pi]) {
+    if (int r = pi ? autotune_yz<float>(ctx) : autotune_yz<double>(ctx)) return r;
+    ctx->tuned[pi] = true;
+  }
   return OSTC_OK;
 }
 
