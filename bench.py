@@ -387,9 +387,13 @@ def run_extra(args, local, barrier, allmax, world):
     react = {"workload": "reacting H2/air mixing layer 384x192x96, 9 species / 19 reactions, WENO7-Z "
                          "characteristic flux splitting (inviscid_scheme 72), mixture-averaged transport, FP64",
              "nodes": rc.nodes}
-    for mode, key in ((ostc.CHEM_EXPLICIT, "explicit"), (ostc.CHEM_POINT_IMPLICIT, "point_implicit")):
+    ref_cv = None
+    for mode, prec, key in ((ostc.CHEM_EXPLICIT, ostc.PREC_FP64, "explicit"),
+                            (ostc.CHEM_POINT_IMPLICIT, ostc.PREC_FP64, "point_implicit"),
+                            (ostc.CHEM_EXPLICIT, ostc.PREC_MIXED, "explicit_mixed")):
         s = ostc.Solver(tmp, device=local)
         s.set_chem_mode(mode)
+        s.set_precision(prec)
         s.set_state(rc.bv, sv=rc.sv)
         s.step(2)
         barrier()
@@ -397,6 +401,19 @@ def run_extra(args, local, barrier, allmax, world):
         prof = s.profile(1)
         react[key] = {"value": world * rc.nodes * 5 / (ms / 1e3), "ms_per_step": ms / 5,
                       "kernels_ms_per_step": {k: v[1] for k, v in prof.items()}, "flags": s.error_flags()}
+        if key == "explicit":
+            ref_cv = s.get_state()[0]
+        elif key == "explicit_mixed":
+            # same 8 steps from the same state as the FP64 explicit run: error of the mixed mode
+            cv = s.get_state()[0]
+            names = ["rho", "rho_u", "rho_v", "rho_w", "rho_E"] + [f"rho_Y_{n}" for n in rc.mixture["tables"].names]
+            react[key]["dtype"] = "f32 split fluxes / viscous fluxes / transport, f64 state / Newton / chemistry"
+            # relative L2 per conserved variable; the momentum components against the momentum magnitude
+            err = oc.relative_errors(cv, ref_cv)
+            react[key]["rel_l2_vs_fp64"] = {names[l]: err[l][1] for l in range(cv.shape[0])}
+            react[key]["rel_max_vs_fp64"] = {names[l]: err[l][0] for l in range(cv.shape[0])}
+            react[key]["speedup_vs_fp64"] = react["explicit"]["ms_per_step"] / react[key]["ms_per_step"]
+            react[key]["after_steps"] = 8
         s.close()
     react["value"] = react["explicit"]["value"]
     out["reacting"] = react

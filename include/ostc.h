@@ -37,7 +37,8 @@ extern "C" {
 
 /* ostc_set_precision modes */
 #define OSTC_PREC_FP64 0   /* every operation in FP64, as the reference */
-#define OSTC_PREC_MIXED 1  /* reconstruction, Riemann, viscous flux in FP32; RK3 state, EOS in FP64 */
+#define OSTC_PREC_MIXED 1  /* reconstruction, Riemann / flux splitting, viscous flux and (mixtures)
+                              transport properties in FP32; RK3 state, EOS, chemistry in FP64 */
 
 /* ostc_rhs term mask (the order of evaluation follows RK.cuh:116-139) */
 #define OSTC_TERM_INVISCID 1u

@@ -20,6 +20,13 @@ template <int NS> struct Spec {
 };
 #define OSTC_NS (NS > 0 ? NS : c_mix.ns)
 
+template <typename T> __device__ __forceinline__ T tpow(T x, T y);
+template <> __device__ __forceinline__ double tpow<double>(double x, double y) { return pow(x, y); }
+template <> __device__ __forceinline__ float tpow<float>(float x, float y) { return powf(x, y); }
+}  // namespace ostc
+#include "dual.cuh"
+namespace ostc {
+
 struct MixTables {
   int ns, nr;
   int use_gibbs;  // some reaction takes kb from the equilibrium constant (backward_reaction_rate's n_gibbs)
@@ -39,32 +46,34 @@ __constant__ MixTables c_mix;
 
 // compute_enthalpy_and_cp (Thermo.cu:136-192): h_k and cp_k in J/kg, linear h extrapolation below
 // t_low.  Either output may be null (compute_enthalpy / compute_cp).
-template <int NS>
-__device__ __forceinline__ void mix_h_cp(double t, double *h, double *cp) {
-  const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t5 = t4 * t;
+template <int NS, typename T = double>
+__device__ __forceinline__ void mix_h_cp(T t, T *h, T *cp) {
+  const T t2 = t * t, t3 = t2 * t, t4 = t3 * t, t5 = t4 * t;
 #pragma unroll
   for (int i = 0; i < OSTC_NS; ++i) {
-    double hh, cc;
-    if (t < c_mix.t_low[i]) {
-      const double tt = c_mix.t_low[i], tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tt5 = tt4 * tt;
+    T hh, cc;
+    if (t < (T)c_mix.t_low[i]) {
+      const T tt = (T)c_mix.t_low[i], tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tt5 = tt4 * tt;
       const double *a = c_mix.low[i];
-      hh = a[0] * tt + 0.5 * a[1] * tt2 + a[2] * tt3 / 3 + 0.25 * a[3] * tt4 + 0.2 * a[4] * tt5 + a[5];
-      cc = a[0] + a[1] * tt + a[2] * tt2 + a[3] * tt3 + a[4] * tt4;
+      hh = (T)a[0] * tt + T(0.5) * (T)a[1] * tt2 + (T)a[2] * tt3 / T(3) + T(0.25) * (T)a[3] * tt4 +
+           T(0.2) * (T)a[4] * tt5 + (T)a[5];
+      cc = (T)a[0] + (T)a[1] * tt + (T)a[2] * tt2 + (T)a[3] * tt3 + (T)a[4] * tt4;
       hh += cc * (t - tt);
     } else {
-      const double *a = t < c_mix.t_mid[i] ? c_mix.low[i] : c_mix.high[i];
-      hh = a[0] * t + 0.5 * a[1] * t2 + a[2] * t3 / 3 + 0.25 * a[3] * t4 + 0.2 * a[4] * t5 + a[5];
-      cc = a[0] + a[1] * t + a[2] * t2 + a[3] * t3 + a[4] * t4;
+      const double *a = t < (T)c_mix.t_mid[i] ? c_mix.low[i] : c_mix.high[i];
+      hh = (T)a[0] * t + T(0.5) * (T)a[1] * t2 + (T)a[2] * t3 / T(3) + T(0.25) * (T)a[3] * t4 +
+           T(0.2) * (T)a[4] * t5 + (T)a[5];
+      cc = (T)a[0] + (T)a[1] * t + (T)a[2] * t2 + (T)a[3] * t3 + (T)a[4] * t4;
     }
-    if (h) h[i] = hh * c_mix.ru_mw[i];
-    if (cp) cp[i] = cc * c_mix.ru_mw[i];
+    if (h) h[i] = hh * (T)c_mix.ru_mw[i];
+    if (cp) cp[i] = cc * (T)c_mix.ru_mw[i];
   }
 }
 
 // compute_gibbs_div_rt (Thermo.cu:194-210)
-template <int NS>
-__device__ __forceinline__ void mix_gibbs_rt(double t, double *g) {
-  const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, ti = 1 / t, lt = log(t);
+template <int NS, typename T = double>
+__device__ __forceinline__ void mix_gibbs_rt(T t, T *g) {
+  const T t2 = t * t, t3 = t2 * t, t4 = t3 * t, ti = 1 / t, lt = log(t);
 #pragma unroll
   for (int i = 0; i < OSTC_NS; ++i) {
     if (t < c_mix.t_low[i]) {
@@ -83,62 +92,66 @@ __device__ __forceinline__ void mix_gibbs_rt(double t, double *g) {
 // Node properties of update_physical_properties<mixture> (FieldOperation.cuh:116-134) with
 // compute_transport_property (Transport.cu:43-136): cp, gamma, acoustic speed, Wilke viscosity,
 // Eucken-type conductivity and mixture-averaged rho*D_k (outputs written through the pointers).
-template <int NS>
-__device__ __forceinline__ void mix_properties(double rho, double p, double t, const double *y, double &gamma,
-                                               double &acoustic, double &mu, double &cond, double *rhod) {
+template <int NS, typename T = double>
+__device__ __forceinline__ void mix_properties(T rho, T p, T t, const T *y, T &gamma, T &acoustic, T &mu, T &cond,
+                                               T *rhod) {
   const int ns = OSTC_NS;
-  double cp[Spec<NS>::A];
-  mix_h_cp<NS>(t, nullptr, cp);
-  double mw = 0, cpt = 0, cvt = 0;
+  T cp[Spec<NS>::A];
+  mix_h_cp<NS, T>(t, nullptr, cp);
+  T mw = 0, cpt = 0, cvt = 0;
   for (int l = 0; l < ns; ++l) {
-    mw += y[l] * c_mix.imw[l];
+    mw += y[l] * (T)c_mix.imw[l];
     cpt += y[l] * cp[l];
-    cvt += y[l] * (cp[l] - c_mix.ru_mw[l]);
+    cvt += y[l] * (cp[l] - (T)c_mix.ru_mw[l]);
   }
   mw = 1 / mw;
   gamma = cpt / cvt;
-  acoustic = sqrt(gamma * kRuD * t / mw);
-  double X[Spec<NS>::A], vis[Spec<NS>::A];
-  const double st = sqrt(t);
+  acoustic = tsqrt(gamma * T(kRuD) * t / mw);
+  T X[Spec<NS>::A], vis[Spec<NS>::A];
+  const T st = tsqrt(t);
   for (int l = 0; l < ns; ++l) {
-    X[l] = y[l] * mw * c_mix.imw[l];
-    const double tdl = t * c_mix.lj_potent_inv[l];
-    const double ci = 1.147 * pow(tdl, -0.145) + pow(tdl + 0.5, -2);
-    vis[l] = c_mix.vis_coeff[l] * st / ci;
+    X[l] = y[l] * mw * (T)c_mix.imw[l];
+    const T tdl = t * (T)c_mix.lj_potent_inv[l];
+    const T ci = T(1.147) * tpow<T>(tdl, T(-0.145)) + tpow<T>(tdl + T(0.5), T(-2));
+    vis[l] = (T)c_mix.vis_coeff[l] * st / ci;
   }
-  double visc = 0, cd = 0;
+  T visc = 0, cd = 0;
   for (int m = 0; m < ns; ++m) {
-    double vt = 0;
+    T vt = 0;
     for (int n = 0; n < ns; ++n) {
-      double pf = 1.0;
+      T pf = 1;
       if (m != n) {
-        const double num = 1 + sqrt(vis[m] / vis[n]) * c_mix.wj_div_wi_1_4[m][n];
-        pf = num * num * c_mix.sqrt_wiwj_8[m][n];
+        const T num = T(1) + tsqrt(vis[m] / vis[n]) * (T)c_mix.wj_div_wi_1_4[m][n];
+        pf = num * num * (T)c_mix.sqrt_wiwj_8[m][n];
       }
       vt += pf * X[n];
     }
-    const double ct = 1.065 * vt - 0.065 * X[m];
+    const T ct = T(1.065) * vt - T(0.065) * X[m];
     visc += vis[m] * X[m] / vt;
-    const double lam = vis[m] * (cp[m] + 1.25 * c_mix.ru_mw[m]);
+    const T lam = vis[m] * (cp[m] + T(1.25) * (T)c_mix.ru_mw[m]);
     cd += lam * X[m] / ct;
   }
   mu = visc;
   cond = cd;
-  // mixture-averaged diffusion with the binary coefficients D_ln = coeff T^1.5 / (p Omega_D(T*))
-  const double t32p = t * st / p;
-  const double eps = 1e-12;
+  // mixture-averaged diffusion with the binary coefficients D_ln = coeff T^1.5 / (p Omega_D(T*)).
+  // D_ln is symmetric in (l, n) (both of its tables are), so each pair is evaluated once and added to
+  // both species' sums; every sum still runs over n in increasing order.
+  const T t32p = t * st / p;
+  const T eps = T(1e-12);
+  T num[Spec<NS>::A], den[Spec<NS>::A];
+  for (int l = 0; l < ns; ++l) num[l] = den[l] = 0;
   for (int l = 0; l < ns; ++l) {
-    double num = 0, den = 0;
-    for (int n = 0; n < ns; ++n) {
-      if (l == n) continue;
-      const double tr = t * c_mix.kb_over_eps[l][n];
-      const double om = 1.0 / pow(tr, 0.145) + 1.0 / ((tr + 0.5) * (tr + 0.5));
-      const double dln = c_mix.binary_diff[l][n] * t32p / om;
-      num += (X[n] + eps) * c_mix.mw[n];
-      den += (X[n] + eps) / dln;
+    for (int n = l + 1; n < ns; ++n) {
+      const T tr = t * (T)c_mix.kb_over_eps[l][n];
+      const T om = T(1) / tpow<T>(tr, T(0.145)) + T(1) / ((tr + T(0.5)) * (tr + T(0.5)));
+      const T dln = (T)c_mix.binary_diff[l][n] * t32p / om;
+      num[l] += (X[n] + eps) * (T)c_mix.mw[n];
+      den[l] += (X[n] + eps) / dln;
+      num[n] += (X[l] + eps) * (T)c_mix.mw[l];
+      den[n] += (X[l] + eps) / dln;
     }
-    rhod[l] = rho * num / (den * mw);
   }
+  for (int l = 0; l < ns; ++l) rhod[l] = rho * num[l] / (den[l] * mw);
 }
 
 // compute_temperature_and_pressure (FieldOperation.cu:3-40): Newton on e(T) starting from t, relative
@@ -168,47 +181,62 @@ __device__ __forceinline__ double mix_temperature(double rho, double e, double t
   return t;
 }
 
-__device__ __forceinline__ double arrhenius(double t, double A, double b, double Ea) {
-  // pow(t, 0) is exactly 1: temperature-independent prefactors skip the pow
-  return A * (b == 0.0 ? 1.0 : pow(t, b)) * exp(-Ea / t);
+// A T^b exp(-Ea/T) (arrhenius, FiniteRateChem.cu:104-106) as A exp(b ln T - Ea/T): one exp per
+// rate with ln T and 1/T formed once per node (the argument's rounding, ~1e-16 of |Ea/T| <= ~60,
+// is the only difference from pow * exp)
+__device__ __forceinline__ double arrhenius(double lt, double ti, double A, double b, double Ea) {
+  return A * exp(fma(b, lt, -Ea * ti));
+}
+
+// x^n for the small integer reaction orders of the equilibrium constant, pow beyond |n| = 2
+template <typename T>
+__device__ __forceinline__ T ipow(T x, int n) {
+  switch (n) {
+    case 0: return T(1.0);
+    case 1: return x;
+    case -1: return 1.0 / x;
+    case 2: return x * x;
+    case -2: return 1.0 / (x * x);
+    default: return pow(x, (double)n);
+  }
 }
 
 // finite_rate_chemistry (FiniteRateChem.cu:7-58, rates :60-195): omega_k in kg/(m^3 s) at one node.
 // With jac non-null also the chemical source Jacobian of compute_chem_src_jacobian
 // (FiniteRateChem.cu:197-217), [ns][ns] row-major, in 1/s.
-template <int NS>
-__device__ __forceinline__ void mix_chemistry(double rho, double t, const double *y, double *omega,
-                                              double *jac = nullptr) {
+template <int NS, typename T = double>
+__device__ __forceinline__ void mix_chemistry(T rho, T t, const T *y, T *omega, T *jac = nullptr) {
   const int ns = OSTC_NS, nr = c_mix.nr;
-  double c[Spec<NS>::A];
+  const T lt = log(t), ti = 1.0 / t;
+  T c[Spec<NS>::A];
   for (int l = 0; l < ns; ++l) c[l] = rho * y[l] * c_mix.imw[l] * 1e-3;
-  double g[Spec<NS>::A];
+  T g[Spec<NS>::A];
   bool gibbs = false;
   for (int l = 0; l < ns; ++l) omega[l] = 0;
-  double cre[Spec<NS>::A], des[Spec<NS>::A];
+  T cre[Spec<NS>::A], des[Spec<NS>::A];
   for (int l = 0; l < ns; ++l) cre[l] = des[l] = 0;
   for (int r = 0; r < nr; ++r) {
     const int ty = c_mix.label[r];
-    double cc = 0;
+    T cc = 0;
     if (ty >= 4)
       for (int l = 0; l < ns; ++l) cc += c[l] * c_mix.third_body[r][l];
-    double kf = arrhenius(t, c_mix.A[r], c_mix.b[r], c_mix.Ea[r]);
+    T kf = arrhenius(lt, ti, c_mix.A[r], c_mix.b[r], c_mix.Ea[r]);
     if (ty == 3) {
-      kf += arrhenius(t, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
+      kf += arrhenius(lt, ti, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
     } else if (ty == 4) {
       kf *= cc;
     } else if (ty > 4) {
-      const double klow = arrhenius(t, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
-      const double pr = klow * cc / kf;
-      double F = 1.0;
+      const T klow = arrhenius(lt, ti, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
+      const T pr = klow * cc / kf;
+      T F = 1.0;
       if (ty > 5) {
-        double fc = (1 - c_mix.troe_alpha[r]) * exp(-t / c_mix.troe_t3[r]) +
+        T fc = (1 - c_mix.troe_alpha[r]) * exp(-t / c_mix.troe_t3[r]) +
                     c_mix.troe_alpha[r] * exp(-t / c_mix.troe_t1[r]);
         if (ty == 7) fc += exp(-c_mix.troe_t2[r] / t);
-        const double lfc = log10(fc);
-        const double cq = -0.4 - 0.67 * lfc, nq = 0.75 - 1.27 * lfc;
-        const double lpr = log10(pr);
-        const double tmp = (lpr + cq) / (nq - 0.14 * (lpr + cq));
+        const T lfc = log10(fc);
+        const T cq = -0.4 - 0.67 * lfc, nq = 0.75 - 1.27 * lfc;
+        const T lpr = log10(pr);
+        const T tmp = (lpr + cq) / (nq - 0.14 * (lpr + cq));
         F = pow(10.0, lfc / (1.0 + tmp * tmp));
       }
       kf = kf * pr / (1.0 + pr) * F;
@@ -216,26 +244,26 @@ __device__ __forceinline__ void mix_chemistry(double rho, double t, const double
     // backward_reaction_rate (FiniteRateChem.cu:108-150): irreversible 0; the equilibrium constant
     // for every other type but 2 when any reaction needs it (it also overwrites REV coefficients);
     // else the REV Arrhenius coefficients (times the third-body sum for type 4)
-    double kb = 0;
+    T kb = 0;
     if (ty == 0) {
       kb = 0;
     } else if (ty != 2 && c_mix.use_gibbs) {
       if (!gibbs) {
-        mix_gibbs_rt<NS>(t, g);
+        mix_gibbs_rt<NS, T>(t, g);
         gibbs = true;
       }
-      double dg = 0;
+      T dg = 0;
       for (int l = 0; l < ns; ++l) dg += g[l] * (c_mix.stoi_b[r][l] - c_mix.stoi_f[r][l]);
-      const double temp_t = kPatmD / kRuD * 1e-3 / t;
-      const double kc = pow(temp_t, (double)c_mix.order[r]) * exp(-dg);
+      const T temp_t = kPatmD / kRuD * 1e-3 / t;
+      const T kc = ipow(temp_t, c_mix.order[r]) * exp(-dg);
       kb = kf / kc;
     } else if (c_mix.rev_type[r] == 1) {
-      kb = arrhenius(t, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
+      kb = arrhenius(lt, ti, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
       if (ty == 4) kb *= cc;
     }
     // concentration products: integer powers as products (pow(c, 1) = c, pow(c, 2) = c*c to within
     // the rounding of pow itself), pow only for higher orders
-    double q1 = 1.0, q2 = ty != 0 ? 1.0 : 0.0;
+    T q1 = 1.0, q2 = ty != 0 ? 1.0 : 0.0;
 #pragma unroll
     for (int l = 0; l < ns; ++l) {
       const int nf = c_mix.stoi_f[r][l];
@@ -275,7 +303,7 @@ __device__ __forceinline__ void mix_chemistry(double rho, double t, const double
 #pragma unroll
     for (int n = 0; n < ns; ++n) {
       const bool live = y[n] > 1e-25;
-      const double inv = live ? 1.0 / (rho * y[n]) : 0.0;
+      const T inv = live ? 1.0 / (rho * y[n]) : 0.0;
 #pragma unroll
       for (int m = 0; m < ns; ++m) jac[m * ns + n] = c_mix.mw[m] * (live ? jac[m * ns + n] * inv : 0.0) * 1e+3;
     }
@@ -324,39 +352,50 @@ __device__ __forceinline__ void mix_lu_solve(double *lhs, double *b) {
 
 // ---------------------------------------------------------------- flux-split WENO7 (71 / 72)
 
-__device__ __forceinline__ double fvs_beta7(double s1, double s2, double s3) {
-  return s1 * s1 + 13.0 / 12.0 * s2 * s2 + 1043.0 / 960 * s3 * s3 + 1.0 / 12 * s1 * s3;
+template <typename T>
+__device__ __forceinline__ T fvs_beta7(T s1, T s2, T s3) {
+  return s1 * s1 + T(13.0 / 12.0) * s2 * s2 + T(1043.0 / 960) * s3 * s3 + T(1.0 / 12) * s1 * s3;
+}
+
+// (eps + beta)^2 of the Z weights; in FP32 floored at 1e-30 so that a smooth stencil (beta = 0,
+// where the scaled eps underflows) gives the linear weights instead of 0/0
+template <typename T>
+__device__ __forceinline__ T fvs_den(T eps, T beta) {
+  const T d = (eps + beta) * (eps + beta);
+  if constexpr (sizeof(T) == 4) return fmaxf(d, 1e-30f);
+  return d;
 }
 
 // WENO7 of the flux-split path (WENO.cu:1619-1693): returns f+ + f-.
-__device__ __forceinline__ double fvs_weno7(const double *vp, const double *vm, double eps) {
-  const double one6th = 1.0 / 6, one12th = 1.0 / 12;
-  const double c0 = 1.0 / 35, c1 = 12.0 / 35, c2 = 18.0 / 35, c3 = 4.0 / 35;
-  double s1 = one6th * (-2 * vp[0] + 9 * vp[1] - 18 * vp[2] + 11 * vp[3]);
-  double s2 = -vp[0] + 4 * vp[1] - 5 * vp[2] + 2 * vp[3];
-  double s3 = -vp[0] + 3 * vp[1] - 3 * vp[2] + vp[3];
-  double b0 = fvs_beta7(s1, s2, s3);
+template <typename T>
+__device__ __forceinline__ T fvs_weno7_core(const T *vp, const T *vm, T eps) {
+  const T one6th = T(1.0 / 6), one12th = T(1.0 / 12);
+  const T c0 = T(1.0 / 35), c1 = T(12.0 / 35), c2 = T(18.0 / 35), c3 = T(4.0 / 35);
+  T s1 = one6th * (-2 * vp[0] + 9 * vp[1] - 18 * vp[2] + 11 * vp[3]);
+  T s2 = -vp[0] + 4 * vp[1] - 5 * vp[2] + 2 * vp[3];
+  T s3 = -vp[0] + 3 * vp[1] - 3 * vp[2] + vp[3];
+  T b0 = fvs_beta7(s1, s2, s3);
   s1 = one6th * (vp[1] - 6 * vp[2] + 3 * vp[3] + 2 * vp[4]);
   s2 = vp[2] - 2 * vp[3] + vp[4];
   s3 = -vp[1] + 3 * vp[2] - 3 * vp[3] + vp[4];
-  double b1 = fvs_beta7(s1, s2, s3);
+  T b1 = fvs_beta7(s1, s2, s3);
   s1 = one6th * (-2 * vp[2] - 3 * vp[3] + 6 * vp[4] - vp[5]);
   s3 = -vp[2] + 3 * vp[3] - 3 * vp[4] + vp[5];
-  double b2 = fvs_beta7(s1, s2, s3);
+  T b2 = fvs_beta7(s1, s2, s3);
   s1 = one6th * (-11 * vp[3] + 18 * vp[4] - 9 * vp[5] + 2 * vp[6]);
   s2 = 2 * vp[3] - 5 * vp[4] + 4 * vp[5] - vp[6];
   s3 = -vp[3] + 3 * vp[4] - 3 * vp[5] + vp[6];
-  double b3 = fvs_beta7(s1, s2, s3);
-  double tau = (b0 - b3) * (b0 - b3);
-  double a0 = c0 + c0 * tau / ((eps + b0) * (eps + b0));
-  double a1 = c1 + c1 * tau / ((eps + b1) * (eps + b1));
-  double a2 = c2 + c2 * tau / ((eps + b2) * (eps + b2));
-  double a3 = c3 + c3 * tau / ((eps + b3) * (eps + b3));
-  double v0 = one12th * (-3 * vp[0] + 13 * vp[1] - 23 * vp[2] + 25 * vp[3]);
-  double v1 = one12th * (vp[1] - 5 * vp[2] + 13 * vp[3] + 3 * vp[4]);
-  double v2 = one12th * (-vp[2] + 7 * vp[3] + 7 * vp[4] - vp[5]);
-  double v3 = one12th * (3 * vp[3] + 13 * vp[4] - 5 * vp[5] + vp[6]);
-  const double fp = (a0 * v0 + a1 * v1 + a2 * v2 + a3 * v3) / (a0 + a1 + a2 + a3);
+  T b3 = fvs_beta7(s1, s2, s3);
+  T tau = (b0 - b3) * (b0 - b3);
+  T a0 = c0 + c0 * tau / (fvs_den(eps, b0));
+  T a1 = c1 + c1 * tau / (fvs_den(eps, b1));
+  T a2 = c2 + c2 * tau / (fvs_den(eps, b2));
+  T a3 = c3 + c3 * tau / (fvs_den(eps, b3));
+  T v0 = one12th * (-3 * vp[0] + 13 * vp[1] - 23 * vp[2] + 25 * vp[3]);
+  T v1 = one12th * (vp[1] - 5 * vp[2] + 13 * vp[3] + 3 * vp[4]);
+  T v2 = one12th * (-vp[2] + 7 * vp[3] + 7 * vp[4] - vp[5]);
+  T v3 = one12th * (3 * vp[3] + 13 * vp[4] - 5 * vp[5] + vp[6]);
+  const T fp = (a0 * v0 + a1 * v1 + a2 * v2 + a3 * v3) / (a0 + a1 + a2 + a3);
   s1 = one6th * (-2 * vm[6] + 9 * vm[5] - 18 * vm[4] + 11 * vm[3]);
   s2 = -vm[6] + 4 * vm[5] - 5 * vm[4] + 2 * vm[3];
   s3 = -vm[6] + 3 * vm[5] - 3 * vm[4] + vm[3];
@@ -373,16 +412,49 @@ __device__ __forceinline__ double fvs_weno7(const double *vp, const double *vm, 
   s3 = -vm[3] + 3 * vm[2] - 3 * vm[1] + vm[0];
   b3 = fvs_beta7(s1, s2, s3);
   tau = (b0 - b3) * (b0 - b3);
-  a0 = c0 + c0 * tau / ((eps + b0) * (eps + b0));
-  a1 = c1 + c1 * tau / ((eps + b1) * (eps + b1));
-  a2 = c2 + c2 * tau / ((eps + b2) * (eps + b2));
-  a3 = c3 + c3 * tau / ((eps + b3) * (eps + b3));
+  a0 = c0 + c0 * tau / (fvs_den(eps, b0));
+  a1 = c1 + c1 * tau / (fvs_den(eps, b1));
+  a2 = c2 + c2 * tau / (fvs_den(eps, b2));
+  a3 = c3 + c3 * tau / (fvs_den(eps, b3));
   v0 = one12th * (-3 * vm[6] + 13 * vm[5] - 23 * vm[4] + 25 * vm[3]);
   v1 = one12th * (vm[5] - 5 * vm[4] + 13 * vm[3] + 3 * vm[2]);
   v2 = one12th * (-vm[4] + 7 * vm[3] + 7 * vm[2] - vm[1]);
   v3 = one12th * (3 * vm[3] + 13 * vm[2] - 5 * vm[1] + vm[0]);
-  const double fm = (a0 * v0 + a1 * v1 + a2 * v2 + a3 * v3) / (a0 + a1 + a2 + a3);
+  const T fm = (a0 * v0 + a1 * v1 + a2 * v2 + a3 * v3) / (a0 + a1 + a2 + a3);
   return fp + fm;
+}
+
+__device__ __forceinline__ double fvs_weno7(const double *vp, const double *vm, double eps) {
+  return fvs_weno7_core<double>(vp, vm, eps);
+}
+
+// FP32 form.  beta ~ v^2 and tau ~ v^4, so the split fluxes of a minor species (|v| ~ 1e-11) or the
+// energy flux of a coarse grid (|v| ~ 1e10) leave the FP32 range although the weights themselves
+// (tau / (eps + beta)^2, scale-free as eps -> 0) are O(1).  The stencil is therefore scaled by the
+// power of two 2^-E below its largest magnitude (exact), eps by 2^-2E, and the face value scaled back.
+__device__ __forceinline__ float fvs_weno7(const float *vp, const float *vm, double eps) {
+  float m = 0.f;
+#pragma unroll
+  for (int i = 0; i < 7; ++i) m = fmaxf(m, fmaxf(fabsf(vp[i]), fabsf(vm[i])));
+  if (!(m > 0.f)) {  // all zero: the face value is 0 (or NaN, carried through)
+    float z = 0.f;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) z += vp[i] + vm[i];
+    return z;
+  }
+  int ex = (__float_as_int(m) >> 23) & 0xff;  // biased exponent of m
+  ex = ex < 1 ? 1 : (ex > 253 ? 253 : ex);
+  const float inv = __int_as_float((254 - ex) << 23);  // 2^(127 - ex)
+  const float scale = __int_as_float(ex << 23);        // 2^(ex - 127)
+  float sp[7], sm[7];
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    sp[i] = vp[i] * inv;
+    sm[i] = vm[i] * inv;
+  }
+  const double id = (double)inv;
+  const float e = (float)(eps * id * id);
+  return fvs_weno7_core<float>(sp, sm, e) * scale;
 }
 
 }  // namespace ostc

@@ -1306,32 +1306,32 @@ void launch_flux_pv(ostc_ctx *ctx, BlockRes &B, DevState in) {
 }
 
 // flux-split WENO7 sweeps (inviscid_type 3, schemes 71 / 72), accumulating into dq
-template <int NS>
+template <int NS, typename T>
 void launch_fvs_t(ostc_ctx *ctx, BlockRes &B, DevState in) {
   const DevBlock &b = B.db;
   const int nv = ctx->nv, sch = ctx->der.inviscid_scheme;
   {
     long tok = begin_t(ctx, "flux_x");
     dim3 grid((b.mx + FvsTile<0>::TD - 2) / (FvsTile<0>::TD - 1), b.my, b.mz);
-    k_fvs<0, NS><<<grid, FvsTile<0>::TD, fvs_smem_bytes<0>(nv), ctx->stream>>>(b, in, B.dq, nv, sch);
+    k_fvs<0, NS, T><<<grid, FvsTile<0>::TD, fvs_smem_bytes<0, T>(nv), ctx->stream>>>(b, in, B.dq, nv, sch);
     end_t(ctx, tok);
   }
   {
     long tok = begin_t(ctx, "flux_y");
     dim3 grid((b.mx + FvsTile<1>::TXL - 1) / FvsTile<1>::TXL, (b.my + FvsTile<1>::TD - 2) / (FvsTile<1>::TD - 1), b.mz);
-    k_fvs<1, NS><<<grid, dim3(FvsTile<1>::TXL, FvsTile<1>::TD), fvs_smem_bytes<1>(nv), ctx->stream>>>(b, in, B.dq, nv, sch);
+    k_fvs<1, NS, T><<<grid, dim3(FvsTile<1>::TXL, FvsTile<1>::TD), fvs_smem_bytes<1, T>(nv), ctx->stream>>>(b, in, B.dq, nv, sch);
     end_t(ctx, tok);
   }
   if (b.mz > 1) {
     long tok = begin_t(ctx, "flux_z");
     dim3 grid((b.mx + FvsTile<2>::TXL - 1) / FvsTile<2>::TXL, (b.mz + FvsTile<2>::TD - 2) / (FvsTile<2>::TD - 1), b.my);
-    k_fvs<2, NS><<<grid, dim3(FvsTile<2>::TXL, FvsTile<2>::TD), fvs_smem_bytes<2>(nv), ctx->stream>>>(b, in, B.dq, nv, sch);
+    k_fvs<2, NS, T><<<grid, dim3(FvsTile<2>::TXL, FvsTile<2>::TD), fvs_smem_bytes<2, T>(nv), ctx->stream>>>(b, in, B.dq, nv, sch);
     end_t(ctx, tok);
   }
 }
 
 // mixture viscous sweeps, accumulating into dq
-template <int NS>
+template <int NS, typename T>
 void launch_mix_visc_t(ostc_ctx *ctx, BlockRes &B, DevState in) {
   const DevBlock &b = B.db;
   const int nv = ctx->nv;
@@ -1339,34 +1339,38 @@ void launch_mix_visc_t(ostc_ctx *ctx, BlockRes &B, DevState in) {
   long tok = begin_t(ctx, "visc");
   {
     dim3 grid((b.mx + FvsTile<0>::TD - 2) / (FvsTile<0>::TD - 1), b.my, b.mz);
-    const size_t sm = (size_t)FvsTile<0>::TD * nv * sizeof(double);
-    if (is3d) k_mix_visc<0, true, NS><<<grid, FvsTile<0>::TD, sm, ctx->stream>>>(b, in, B.dq, nv);
-    else k_mix_visc<0, false, NS><<<grid, FvsTile<0>::TD, sm, ctx->stream>>>(b, in, B.dq, nv);
+    const size_t sm = (size_t)FvsTile<0>::TD * nv * sizeof(T);
+    if (is3d) k_mix_visc<0, true, NS, T><<<grid, FvsTile<0>::TD, sm, ctx->stream>>>(b, in, B.dq, nv);
+    else k_mix_visc<0, false, NS, T><<<grid, FvsTile<0>::TD, sm, ctx->stream>>>(b, in, B.dq, nv);
   }
   {
     dim3 grid((b.mx + FvsTile<1>::TXL - 1) / FvsTile<1>::TXL, (b.my + FvsTile<1>::TD - 2) / (FvsTile<1>::TD - 1), b.mz);
-    const size_t sm = (size_t)FvsTile<1>::TD * FvsTile<1>::TXL * nv * sizeof(double);
+    const size_t sm = (size_t)FvsTile<1>::TD * FvsTile<1>::TXL * nv * sizeof(T);
     dim3 blk(FvsTile<1>::TXL, FvsTile<1>::TD);
-    if (is3d) k_mix_visc<1, true, NS><<<grid, blk, sm, ctx->stream>>>(b, in, B.dq, nv);
-    else k_mix_visc<1, false, NS><<<grid, blk, sm, ctx->stream>>>(b, in, B.dq, nv);
+    if (is3d) k_mix_visc<1, true, NS, T><<<grid, blk, sm, ctx->stream>>>(b, in, B.dq, nv);
+    else k_mix_visc<1, false, NS, T><<<grid, blk, sm, ctx->stream>>>(b, in, B.dq, nv);
   }
   if (is3d) {
     dim3 grid((b.mx + FvsTile<2>::TXL - 1) / FvsTile<2>::TXL, (b.mz + FvsTile<2>::TD - 2) / (FvsTile<2>::TD - 1), b.my);
-    const size_t sm = (size_t)FvsTile<2>::TD * FvsTile<2>::TXL * nv * sizeof(double);
-    k_mix_visc<2, true, NS><<<grid, dim3(FvsTile<2>::TXL, FvsTile<2>::TD), sm, ctx->stream>>>(b, in, B.dq, nv);
+    const size_t sm = (size_t)FvsTile<2>::TD * FvsTile<2>::TXL * nv * sizeof(T);
+    k_mix_visc<2, true, NS, T><<<grid, dim3(FvsTile<2>::TXL, FvsTile<2>::TD), sm, ctx->stream>>>(b, in, B.dq, nv);
   }
   end_t(ctx, tok);
 }
 
 // The H2/air mechanism's 9 species get a dedicated instantiation; other counts the generic one.
+// In the mixed precision mode the flux-split, viscous and property kernels run in FP32.
 constexpr int kFixedNS = 9;
 void launch_fvs(ostc_ctx *ctx, BlockRes &B, DevState in) {
-  if (ctx->der.n_spec == kFixedNS) launch_fvs_t<kFixedNS>(ctx, B, in);
-  else launch_fvs_t<0>(ctx, B, in);
+  const bool f32 = ctx->precision == OSTC_PREC_MIXED;
+  if (ctx->der.n_spec == kFixedNS) f32 ? launch_fvs_t<kFixedNS, float>(ctx, B, in) : launch_fvs_t<kFixedNS, double>(ctx, B, in);
+  else f32 ? launch_fvs_t<0, float>(ctx, B, in) : launch_fvs_t<0, double>(ctx, B, in);
 }
 void launch_mix_visc(ostc_ctx *ctx, BlockRes &B, DevState in) {
-  if (ctx->der.n_spec == kFixedNS) launch_mix_visc_t<kFixedNS>(ctx, B, in);
-  else launch_mix_visc_t<0>(ctx, B, in);
+  const bool f32 = ctx->precision == OSTC_PREC_MIXED;
+  if (ctx->der.n_spec == kFixedNS)
+    f32 ? launch_mix_visc_t<kFixedNS, float>(ctx, B, in) : launch_mix_visc_t<kFixedNS, double>(ctx, B, in);
+  else f32 ? launch_mix_visc_t<0, float>(ctx, B, in) : launch_mix_visc_t<0, double>(ctx, B, in);
 }
 template <int NS>
 void launch_mix_source_t(ostc_ctx *ctx, BlockRes &B, DevState in, bool chem) {
@@ -1386,10 +1390,15 @@ void launch_chem_epi(ostc_ctx *ctx, BlockRes &B, DevState in) {
 }
 
 void launch_mix_props(ostc_ctx *ctx, BlockRes &B, DevState st) {
-  if (ctx->der.n_spec == kFixedNS)
-    k_mix_props<kFixedNS><<<grid_for(ctx, B.db.plane, 128), 128, 0, ctx->stream>>>(B.db, st);
-  else
-    k_mix_props<0><<<grid_for(ctx, B.db.plane, 128), 128, 0, ctx->stream>>>(B.db, st);
+  const int g = grid_for(ctx, B.db.plane, 128);
+  const bool f32 = ctx->precision == OSTC_PREC_MIXED;
+  if (ctx->der.n_spec == kFixedNS) {
+    if (f32) k_mix_props<kFixedNS, float><<<g, 128, 0, ctx->stream>>>(B.db, st);
+    else k_mix_props<kFixedNS, double><<<g, 128, 0, ctx->stream>>>(B.db, st);
+  } else {
+    if (f32) k_mix_props<0, float><<<g, 128, 0, ctx->stream>>>(B.db, st);
+    else k_mix_props<0, double><<<g, 128, 0, ctx->stream>>>(B.db, st);
+  }
 }
 
 DevState state_of(BlockRes &B, int s);
@@ -1646,12 +1655,16 @@ bool set_mix_attrs(int nv) {
   auto set = [&](const void *fn, size_t bytes) {
     ok = ok && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess;
   };
-  set((const void *)k_fvs<0, 0>, fvs_smem_bytes<0>(nv));
-  set((const void *)k_fvs<1, 0>, fvs_smem_bytes<1>(nv));
-  set((const void *)k_fvs<2, 0>, fvs_smem_bytes<2>(nv));
-  set((const void *)k_fvs<0, kFixedNS>, fvs_smem_bytes<0>(nv));
-  set((const void *)k_fvs<1, kFixedNS>, fvs_smem_bytes<1>(nv));
-  set((const void *)k_fvs<2, kFixedNS>, fvs_smem_bytes<2>(nv));
+#define OSTC_FSET(T)                                                      \
+  set((const void *)k_fvs<0, 0, T>, fvs_smem_bytes<0, T>(nv));            \
+  set((const void *)k_fvs<1, 0, T>, fvs_smem_bytes<1, T>(nv));            \
+  set((const void *)k_fvs<2, 0, T>, fvs_smem_bytes<2, T>(nv));            \
+  set((const void *)k_fvs<0, kFixedNS, T>, fvs_smem_bytes<0, T>(nv));     \
+  set((const void *)k_fvs<1, kFixedNS, T>, fvs_smem_bytes<1, T>(nv));     \
+  set((const void *)k_fvs<2, kFixedNS, T>, fvs_smem_bytes<2, T>(nv));
+  OSTC_FSET(double)
+  OSTC_FSET(float)
+#undef OSTC_FSET
   return ok;
 }
 
@@ -2116,11 +2129,6 @@ int ostc_set_precision(ostc_ctx *ctx, int mode) {
   if (!ctx) return OSTC_EINVAL;
   if (mode != OSTC_PREC_FP64 && mode != OSTC_PREC_MIXED) {
     ctx->err = "unknown precision mode";
-    return OSTC_EINVAL;
-  }
-  if (mode == OSTC_PREC_MIXED && ctx->der.inviscid_type == 3) {
-    ctx->err = "the mixed-precision path covers the AWENO and primitive-reconstruction schemes; the flux-split "
-               "WENO7 path (inviscid_scheme 71/72, mixtures) runs in FP64";
     return OSTC_EINVAL;
   }
   ctx->precision = mode;

@@ -90,3 +90,30 @@ def test_point_implicit_chemistry_matches_oracle(built, tmp_path, dims, steps):
     err = oc.relative_errors(cg, co)
     assert all(m < TOL and l2 < TOL for m, l2 in err), err
     assert s.error_flags() == 0
+
+
+@pytest.mark.parametrize("kw", [dict(inviscid_scheme=72), dict(inviscid_scheme=71, finite_rate=False)],
+                         ids=["fr72", "mix71"])
+def test_mixture_mixed_precision(built, tmp_path, kw):
+    """Mixed precision on the multi-component path (FP32 split fluxes, viscous fluxes and transport
+    properties; FP64 state, Newton temperature and chemistry) against the FP64 path after 12 steps:
+    relative L2 error per conserved variable (momentum components against the momentum magnitude),
+    every species density rho*Y_k included, below 1e-5, and the species mass fractions within 1e-6
+    absolute."""
+    import ostc
+
+    case = oc.reacting_mixing_layer_3d(mx=40, my=32, mz=16, **kw)
+    d = oc.write_case(case, tmp_path / "case")
+    out = {}
+    for prec in (ostc.PREC_FP64, ostc.PREC_MIXED):
+        s = ostc.Solver(str(d))
+        s.set_precision(prec)
+        s.set_state(case.bv, sv=case.sv)
+        s.step(12)
+        cv, _ = s.get_state()
+        out[prec] = (cv, s.get_species(), s.error_flags())
+    (c64, y64, f64), (c32, y32, f32) = out[ostc.PREC_FP64], out[ostc.PREC_MIXED]
+    assert f64 == 0 and f32 == 0
+    l2 = [e[1] for e in oc.relative_errors(c32, c64)]
+    assert max(l2) < 1e-5, l2
+    assert np.max(np.abs(y32 - y64)) < 1e-6
