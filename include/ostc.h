@@ -110,6 +110,24 @@ int ostc_get_state(ostc_ctx *ctx, int block, double *cv, double *bv, double *sv,
  * SourceTerm.cuh:11-35).  dq has the reference's sign: d(cv)/dt = dq / jac. */
 int ostc_rhs(ostc_ctx *ctx, int block, unsigned term_mask, double *dq, int ptr_kind);
 
+/* Replace the interior conservative state of one block by cv[n_var][N] (the layout of dq): the
+ * primitive state follows by the equation of state (mixtures: the temperature Newton iteration
+ * started from each node's current T, FieldOperation.cu:3-40), then the boundary faces, interfaces
+ * and (mixtures) properties, as after an RK stage.  The physical time is unchanged.  No reference
+ * counterpart: it lets a caller perturb cv (finite differences, adjoint checks). */
+int ostc_set_conservative(ostc_ctx *ctx, int block, const double *cv, int ptr_kind);
+
+/* Vector-Jacobian product of ostc_rhs at the current state (no reference counterpart):
+ * cv_bar = (d dq / d cv)^T dq_bar for the terms in term_mask, with cv the block's interior
+ * conservative variables and every dependent quantity (primitive state by the equation of state,
+ * ghost nodes by the boundary faces, transport properties) following cv as ostc_set_conservative
+ * defines it.  dq_bar and cv_bar have the layout of dq.  The product is that of the FP64 right-hand
+ * side.  Covers the multi-component path (species = 1; inviscid_scheme 71 / 72, viscous, explicit
+ * finite-rate source) on a single block with periodic and outflow faces; anything else returns
+ * OSTC_EINVAL.  Accumulation uses atomics: results agree run to run to rounding. */
+int ostc_rhs_vjp(ostc_ctx *ctx, int block, unsigned term_mask, const double *dq_bar, double *cv_bar,
+                 int ptr_kind);
+
 /* Advance n_steps full SSP-RK3 steps (the loop body of RK3<mix,turb>, RK.cuh:85-185), all stream
  * ordered and replayed from a CUDA graph.  dt_last (nullable) receives the last step's dt (CFL
  * minimum over all blocks, TimeAdvanceFunc.cu:39-64, or the fixed dt); reading it synchronises. */

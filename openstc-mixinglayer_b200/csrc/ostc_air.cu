@@ -80,6 +80,7 @@ __device__ __forceinline__ void cv_from_bv_node(const DevBlock &b, DevState s, l
 }  // namespace ostc
 
 #include "ostc_mix.cuh"
+#include "ostc_adj.cuh"
 
 namespace ostc {
 
@@ -1043,6 +1044,44 @@ __global__ void __launch_bounds__(128) k_inner_carry(DevBlock b, DevState in, De
 
 // ------------------------------------------------------------------------------ set-up kernels
 
+// Interior primitive state from the conservative variables already in s.cv (update_cv_and_bv_rk's
+// closing part, RK.cuh:250-284): mixtures solve T by the Newton iteration from the node's current T
+// (compute_temperature_and_pressure, FieldOperation.cu:3-40); air closes p, T, mu directly.
+template <int NS>
+__global__ void __launch_bounds__(128) k_state_from_cv(DevBlock b, DevState s, int mixture, unsigned *flags) {
+  const long long P = b.plane;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % b.mx);
+    const long long r = n / b.mx;
+    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const long long p = b.id(i, j, k);
+    const double rho = s.cv[p], di = 1.0 / rho;
+    const double u = s.cv[P + p] * di, v = s.cv[2 * P + p] * di, w = s.cv[3 * P + p] * di;
+    double pr, t;
+    if (mixture) {
+      const int ns = OSTC_NS;
+      double y[Spec<NS>::A];
+      for (int l = 0; l < ns; ++l) {
+        y[l] = s.cv[(5 + l) * P + p] * di;
+        s.sv[l * P + p] = y[l];
+      }
+      const double e = s.cv[4 * P + p] * di - 0.5 * (u * u + v * v + w * w);
+      t = mix_temperature<NS>(rho, e, s.bv[5 * P + p], y, pr);
+    } else {
+      pr = (kGamma - 1) * (s.cv[4 * P + p] - 0.5 * rho * (u * u + v * v + w * w));
+      t = pr * kMwD * di / kRuD;
+      s.mul[p] = sutherland(t);
+    }
+    s.bv[p] = rho;
+    s.bv[P + p] = u;
+    s.bv[2 * P + p] = v;
+    s.bv[3 * P + p] = w;
+    s.bv[4 * P + p] = pr;
+    s.bv[5 * P + p] = t;
+    if (!(rho > 0) || !(pr > 0) || !(t > 0)) atomicOr(flags, (rho != rho || pr != pr || t != t) ? 2u : 1u);
+  }
+}
+
 // every padded node of planes dst[0..nv) set to val[l]
 __global__ void k_fill_planes(long long plane, double *__restrict__ dst, int nv, FillVals v) {
   const long long tot = plane * nv;
@@ -1157,6 +1196,8 @@ struct BlockRes {
   std::vector<DevInner> inner;  // interfaces of this block, file order
   int yz_var[2][2] = {{-1, -1}, {-1, -1}};  // autotuned y / z sweep variant [FP64, mixed][y, z]
   std::vector<int> inner_target;
+  double *adj = nullptr;  // node adjoint planes of ostc_rhs_vjp (allocated on first use)
+  double *dqb = nullptr;  // dq_bar on the device
 };
 
 struct ostc_ctx {
@@ -1402,6 +1443,44 @@ void launch_mix_props(ostc_ctx *ctx, BlockRes &B, DevState st) {
 }
 
 DevState state_of(BlockRes &B, int s);
+
+// ---- adjoint of the multi-component right-hand side (ostc_rhs_vjp)
+template <int NS>
+void launch_adjoint_t(ostc_ctx *ctx, BlockRes &B, DevState in, unsigned mask, const DevAdj &A) {
+  const DevBlock &b = B.db;
+  const int nv = ctx->nv, sch = ctx->der.inviscid_scheme;
+  const bool is3d = b.mz > 1;
+  if (mask & OSTC_TERM_INVISCID) {
+    dim3 g0((b.mx + FvsTile<0>::TD - 2) / (FvsTile<0>::TD - 1), b.my, b.mz);
+    k_adj_fvs<0, NS><<<g0, FvsTile<0>::TD, adj_fvs_smem_bytes<0>(nv), ctx->stream>>>(b, in, B.dqb, nv, sch, A);
+    dim3 g1((b.mx + FvsTile<1>::TXL - 1) / FvsTile<1>::TXL, (b.my + FvsTile<1>::TD - 2) / (FvsTile<1>::TD - 1), b.mz);
+    k_adj_fvs<1, NS><<<g1, dim3(FvsTile<1>::TXL, FvsTile<1>::TD), adj_fvs_smem_bytes<1>(nv), ctx->stream>>>(
+        b, in, B.dqb, nv, sch, A);
+    if (is3d) {
+      dim3 g2((b.mx + FvsTile<2>::TXL - 1) / FvsTile<2>::TXL, (b.mz + FvsTile<2>::TD - 2) / (FvsTile<2>::TD - 1), b.my);
+      k_adj_fvs<2, NS><<<g2, dim3(FvsTile<2>::TXL, FvsTile<2>::TD), adj_fvs_smem_bytes<2>(nv), ctx->stream>>>(
+          b, in, B.dqb, nv, sch, A);
+    }
+  }
+  if ((mask & OSTC_TERM_VISCOUS) && ctx->der.viscous_order != 0) {
+    dim3 g0((b.mx + FvsTile<0>::TD - 2) / (FvsTile<0>::TD - 1), b.my, b.mz);
+    dim3 g1((b.mx + FvsTile<1>::TXL - 1) / FvsTile<1>::TXL, (b.my + FvsTile<1>::TD - 2) / (FvsTile<1>::TD - 1), b.mz);
+    dim3 blk(FvsTile<1>::TXL, FvsTile<1>::TD);
+    if (is3d) {
+      k_adj_visc<0, true, NS><<<g0, FvsTile<0>::TD, 0, ctx->stream>>>(b, in, B.dqb, nv, A);
+      k_adj_visc<1, true, NS><<<g1, blk, 0, ctx->stream>>>(b, in, B.dqb, nv, A);
+      dim3 g2((b.mx + FvsTile<2>::TXL - 1) / FvsTile<2>::TXL, (b.mz + FvsTile<2>::TD - 2) / (FvsTile<2>::TD - 1), b.my);
+      k_adj_visc<2, true, NS><<<g2, dim3(FvsTile<2>::TXL, FvsTile<2>::TD), 0, ctx->stream>>>(b, in, B.dqb, nv, A);
+    } else {
+      k_adj_visc<0, false, NS><<<g0, FvsTile<0>::TD, 0, ctx->stream>>>(b, in, B.dqb, nv, A);
+      k_adj_visc<1, false, NS><<<g1, blk, 0, ctx->stream>>>(b, in, B.dqb, nv, A);
+    }
+  }
+  if ((mask & OSTC_TERM_SOURCE) && ctx->der.reaction == 1)
+    k_adj_source<NS><<<grid_for(ctx, b.n, 128), 128, 0, ctx->stream>>>(b, in, B.dqb, A);
+  k_adj_props<NS><<<grid_for(ctx, b.plane, 128), 128, 0, ctx->stream>>>(b, in, A);
+  k_adj_eos<NS><<<grid_for(ctx, b.plane, 128), 128, 0, ctx->stream>>>(b, in, A);
+}
 
 // y / z sweep variants: 0 = column march, 1..3 = tiles of the shapes below (per precision: rows
 // of 128 bytes, and a block small enough for the register budget of the FP64 face arithmetic).
@@ -1665,6 +1744,12 @@ bool set_mix_attrs(int nv) {
   OSTC_FSET(double)
   OSTC_FSET(float)
 #undef OSTC_FSET
+  set((const void *)k_adj_fvs<0, 0>, adj_fvs_smem_bytes<0>(nv));
+  set((const void *)k_adj_fvs<1, 0>, adj_fvs_smem_bytes<1>(nv));
+  set((const void *)k_adj_fvs<2, 0>, adj_fvs_smem_bytes<2>(nv));
+  set((const void *)k_adj_fvs<0, kFixedNS>, adj_fvs_smem_bytes<0>(nv));
+  set((const void *)k_adj_fvs<1, kFixedNS>, adj_fvs_smem_bytes<1>(nv));
+  set((const void *)k_adj_fvs<2, kFixedNS>, adj_fvs_smem_bytes<2>(nv));
   return ok;
 }
 
@@ -2066,6 +2151,8 @@ void ostc_destroy(ostc_ctx *ctx) {
     cudaFree(B.jac);
     cudaFree(B.dq);
     cudaFree(B.last);
+    cudaFree(B.adj);
+    cudaFree(B.dqb);
     for (int s = 0; s < 3; ++s) {
       cudaFree(B.cv[s]);
       cudaFree(B.bv[s]);
@@ -2265,6 +2352,91 @@ int ostc_rhs(ostc_ctx *ctx, int block, unsigned mask, double *dq, int ptr_kind) 
   }
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(dq, B.dq, 5 * B.db.n * sizeof(double),
+                     ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return OSTC_OK;
+}
+
+int ostc_set_conservative(ostc_ctx *ctx, int block, const double *cv, int ptr_kind) {
+  if (!ctx || !cv || block < 0 || block >= (int)ctx->blk.size()) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  BlockRes &B = ctx->blk[block];
+  const int nv = ctx->nv;
+  const auto kind = ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  CK(cudaMemcpyAsync(ctx->d_staging, cv, (size_t)nv * B.db.n * sizeof(double), kind, ctx->stream));
+  DevState st = state_of(B, 0);
+  k_scatter<<<grid_for(ctx, nv * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, ctx->d_staging, st.cv, nv);
+  const int g = grid_for(ctx, B.db.n, 128);
+  if (ctx->mixture && ctx->der.n_spec == kFixedNS)
+    k_state_from_cv<kFixedNS><<<g, 128, 0, ctx->stream>>>(B.db, st, 1, ctx->d_flags);
+  else
+    k_state_from_cv<0><<<g, 128, 0, ctx->stream>>>(B.db, st, ctx->mixture ? 1 : 0, ctx->d_flags);
+  launch_bcs(ctx, block, st);
+  launch_interfaces(ctx, 0);
+  if (ctx->mixture)
+    for (auto &Bk : ctx->blk) launch_mix_props(ctx, Bk, state_of(Bk, 0));
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  return OSTC_OK;
+}
+
+int ostc_rhs_vjp(ostc_ctx *ctx, int block, unsigned mask, const double *dq_bar, double *cv_bar, int ptr_kind) {
+  if (!ctx || !dq_bar || !cv_bar || block < 0 || block >= (int)ctx->blk.size()) return OSTC_EINVAL;
+  if (!ctx->mixture) {
+    ctx->err = "ostc_rhs_vjp covers the multi-component path (species = 1)";
+    return OSTC_EINVAL;
+  }
+  if ((mask & OSTC_TERM_SOURCE) && ctx->der.reaction == 1 && ctx->chem_mode == OSTC_CHEM_POINT_IMPLICIT) {
+    ctx->err = "ostc_rhs_vjp: the point-implicit chemistry mode has no adjoint; use the explicit source";
+    return OSTC_EINVAL;
+  }
+  BlockRes &B = ctx->blk[block];
+  if (ctx->blk.size() > 1 || !B.inner.empty()) {
+    ctx->err = "ostc_rhs_vjp: single-block cases only (interfaces couple the blocks' right-hand sides)";
+    return OSTC_EINVAL;
+  }
+  for (const auto &f : B.faces)
+    if (f.type != kPeriodic && f.type != kOutflow) {
+      ctx->err = "ostc_rhs_vjp: boundary faces must be periodic or outflow";
+      return OSTC_EINVAL;
+    }
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  const int nv = ctx->nv, ns = ctx->der.n_spec;
+  const long long P = B.db.plane;
+  const int planes = nv + 9 + 2 * ns;
+  if (!B.adj) {
+    CK(cudaMalloc(&B.adj, (size_t)planes * P * sizeof(double)));
+    CK(cudaMalloc(&B.dqb, (size_t)nv * B.db.n * sizeof(double)));
+  }
+  CK(cudaMemsetAsync(B.adj, 0, (size_t)planes * P * sizeof(double), ctx->stream));
+  CK(cudaMemcpyAsync(B.dqb, dq_bar, (size_t)nv * B.db.n * sizeof(double),
+                     ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+  DevAdj A;
+  A.cv = B.adj;
+  A.p = A.cv + nv * P;
+  A.c = A.p + P;
+  A.rho = A.c + P;
+  A.vel = A.rho + P;
+  A.T = A.vel + 3 * P;
+  A.Y = A.T + P;
+  A.mu = A.Y + ns * P;
+  A.lam = A.mu + P;
+  A.rhod = A.lam + P;
+  const DevState in = state_of(B, 0);
+  if (ns == kFixedNS) launch_adjoint_t<kFixedNS>(ctx, B, in, mask, A);
+  else launch_adjoint_t<0>(ctx, B, in, mask, A);
+  for (auto it = ctx->order.rbegin(); it != ctx->order.rend(); ++it) {
+    if (it->first != block) continue;
+    const DevFace &f = B.faces[it->second];
+    const int t0 = f.face == 0 ? 1 : 0, t1 = f.face == 2 ? 1 : 2;
+    const long long nn = (long long)(f.re[t0] - f.rs[t0] + 1) * (f.re[t1] - f.rs[t1] + 1);
+    k_adj_bc_face<<<grid_for(ctx, nn, 128), 128, 0, ctx->stream>>>(B.db, A.cv, nv, f);
+  }
+  k_adj_gather<<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, A.cv, nv, B.dq);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(cv_bar, B.dq, (size_t)nv * B.db.n * sizeof(double),
                      ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return OSTC_OK;

@@ -25,7 +25,8 @@ EXPORTS = [
     "ostc_set_precision", "ostc_set_state", "ostc_get_state", "ostc_rhs", "ostc_rk3_step",
     "ostc_physical_time", "ostc_store_residual_reference", "ostc_residual", "ostc_error_flags",
     "ostc_device_view", "ostc_profile_steps", "ostc_total_nodes", "ostc_probe_case", "ostc_timed_steps",
-    "ostc_step_kernel_count", "ostc_residual_noalloc", "ostc_set_chem_mode",
+    "ostc_step_kernel_count", "ostc_residual_noalloc", "ostc_set_chem_mode", "ostc_set_conservative",
+    "ostc_rhs_vjp",
 ]
 
 
@@ -68,6 +69,8 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.ostc_set_state.argtypes = [vp, ip, vp, vp, ip]
     lib.ostc_get_state.argtypes = [vp, ip, vp, vp, vp, ip]
     lib.ostc_rhs.argtypes = [vp, ip, ctypes.c_uint, vp, ip]
+    lib.ostc_set_conservative.argtypes = [vp, ip, vp, ip]
+    lib.ostc_rhs_vjp.argtypes = [vp, ip, ctypes.c_uint, vp, vp, ip]
     lib.ostc_rk3_step.argtypes = [vp, ip, dp]
     lib.ostc_physical_time.argtypes = [vp, dp]
     lib.ostc_store_residual_reference.argtypes = [vp]
@@ -195,6 +198,18 @@ class Solver:
         dq = np.empty((self.n_var,) + self.shape(block))
         self._check(self.lib.ostc_rhs(self.h, block, mask, _ptr(dq), OSTC_HOST))
         return dq
+
+    def set_conservative(self, cv: np.ndarray, block: int = 0):
+        """Interior conservative state [n_var][k][j][i]; primitive state, ghosts and properties follow."""
+        cv = np.ascontiguousarray(cv, dtype=np.float64)
+        self._check(self.lib.ostc_set_conservative(self.h, block, _ptr(cv), OSTC_HOST))
+
+    def rhs_vjp(self, dq_bar: np.ndarray, mask: int = TERM_ALL, block: int = 0) -> np.ndarray:
+        """(d rhs / d cv)^T dq_bar at the current state, same layout as rhs()."""
+        dq_bar = np.ascontiguousarray(dq_bar, dtype=np.float64)
+        cv_bar = np.empty((self.n_var,) + self.shape(block))
+        self._check(self.lib.ostc_rhs_vjp(self.h, block, mask, _ptr(dq_bar), _ptr(cv_bar), OSTC_HOST))
+        return cv_bar
 
     def step(self, n: int = 1) -> float:
         dt = ctypes.c_double()

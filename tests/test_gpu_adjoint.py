@@ -1,0 +1,163 @@
+"""Adjoint of the multi-component right-hand side (ostc_rhs_vjp, no reference counterpart) against
+central finite differences of ostc_rhs on the GPU, through the C ABI.
+
+The product is pinned by the dot-product identity <w, J v> = <J^T w, v>: J v is taken as the central
+difference (R(cv + eps v) - R(cv - eps v)) / (2 eps) with the perturbed states set through
+ostc_set_conservative (equation of state, ghost faces and properties follow cv), J^T w from
+ostc_rhs_vjp at cv.  v is seeded N(0,1) times |cv| per node and variable (a relative perturbation
+everywhere), w seeded N(0,1); the differences at 2 eps and eps (eps = 1e-8) are combined by
+Richardson extrapolation.  Tolerance, as numpy's isclose: |<w, J v> - <J^T w, v>| <= 1e-6 |<w, J v>|
++ 1e-9 sum |w * J v| (the second term covers directions whose inner product cancels to a small
+fraction of its terms, where the difference's own error is set by the terms).
+
+The WENO-Z weights of the flux-split path use eps ~ 1e-40 (scaled): where a characteristic field is
+locally constant (a field that does not vary along a sweep, e.g. the species fields of a layer that
+is uniform in x) the weights jump with any perturbation, the flux is only directionally
+differentiable there, and no linear adjoint can match a finite difference.  The seeded states
+therefore carry 5 % multiplicative noise on T, p and every Y besides the layer's velocity noise; on
+them a plain central difference converges to the adjoint as O(eps^2) down to ~1e-7 (eps = 1e-8).
+"""
+import numpy as np
+import pytest
+
+import ostc_cases as oc
+
+pytestmark = pytest.mark.gpu
+EPS = 1e-8
+RTOL = 1e-6
+ATOL = 1e-9  # times sum |w * J v|
+NOISE = 5e-2
+
+
+def _noisy(case, seed=5):
+    """5 % seeded noise on T, p and the mass fractions (renormalised), rho from the equation of state."""
+    rng = np.random.default_rng(seed)
+    case.bv[5] *= 1 + NOISE * rng.standard_normal(case.bv[5].shape)
+    case.bv[4] *= 1 + NOISE * rng.standard_normal(case.bv[4].shape)
+    sv = case.sv * (1 + NOISE * rng.standard_normal(case.sv.shape))
+    case.sv[:] = sv / sv.sum(axis=0)
+    mw = 1 / np.einsum("l...,l->...", case.sv, 1 / case.mixture["tables"].mw)
+    case.bv[0] = case.bv[4] * mw / (oc.R_U * case.bv[5])
+    return case
+
+
+def _solver(case, tmp_path):
+    import ostc
+
+    case = _noisy(case)
+    d = oc.write_case(case, tmp_path / "case")
+    s = ostc.Solver(str(d))
+    s.set_state(case.bv, sv=case.sv)
+    cv0, _ = s.get_state()
+    return s, cv0
+
+
+def _directions(cv0, rng, n):
+    return [rng.standard_normal(cv0.shape) * np.abs(cv0) for _ in range(n)]
+
+
+def _fd(s, cv0, v, mask):
+    """Central differences at 2 eps and eps combined by Richardson extrapolation (error O(eps^4))."""
+    d = []
+    for h in (2 * EPS, EPS):
+        s.set_conservative(cv0 + h * v)
+        rp = s.rhs(mask)
+        s.set_conservative(cv0 - h * v)
+        rm = s.rhs(mask)
+        d.append((rp - rm) / (2 * h))
+    s.set_conservative(cv0)
+    return (4 * d[1] - d[0]) / 3
+
+
+def _check(s, cv0, mask, rng, n_dir):
+    w = rng.standard_normal(cv0.shape)
+    s.set_conservative(cv0)
+    g = s.rhs_vjp(w, mask)
+    errs = []
+    for v in _directions(cv0, rng, n_dir):
+        jv = _fd(s, cv0, v, mask)
+        lhs, rhs = float(np.sum(w * jv)), float(np.sum(g * v))
+        # error in units of the tolerance (<= 1 passes)
+        errs.append(abs(lhs - rhs) / (RTOL * abs(lhs) + ATOL * float(np.sum(np.abs(w * jv)))))
+    return errs
+
+
+@pytest.mark.parametrize("kw", [dict(inviscid_scheme=72), dict(inviscid_scheme=71, finite_rate=False)],
+                         ids=["fr72", "mix71"])
+@pytest.mark.parametrize("mask,name", [(1, "inviscid"), (2, "viscous"), (4, "source"), (7, "all")])
+def test_vjp_matches_finite_differences(built, tmp_path, kw, mask, name):
+    case = oc.reacting_mixing_layer_3d(mx=24, my=18, mz=12, **kw)
+    s, cv0 = _solver(case, tmp_path)
+    if mask == 4 and not kw.get("finite_rate", True):
+        # no chemistry: the source term and its adjoint are zero
+        w = np.random.default_rng(1).standard_normal(cv0.shape)
+        assert not np.any(s.rhs_vjp(w, 4))
+        return
+    errs = _check(s, cv0, mask, np.random.default_rng(7 + mask), 4)
+    assert max(errs) <= 1.0, (name, errs)
+
+
+def test_vjp_64_directions_2d(built, tmp_path):
+    """64 seeded directions on a 2-D reacting layer (all terms)."""
+    case = oc.reacting_mixing_layer_3d(mx=40, my=24, mz=1)
+    s, cv0 = _solver(case, tmp_path)
+    errs = _check(s, cv0, 7, np.random.default_rng(64), 64)
+    assert max(errs) <= 1.0, sorted(errs)[-5:]
+
+
+def test_vjp_is_linear_and_additive(built, tmp_path):
+    case = oc.reacting_mixing_layer_3d(mx=20, my=16, mz=10)
+    s, cv0 = _solver(case, tmp_path)
+    rng = np.random.default_rng(3)
+    w1, w2 = rng.standard_normal(cv0.shape), rng.standard_normal(cv0.shape)
+    g = s.rhs_vjp(2.0 * w1 - w2)
+    g_lin = 2.0 * s.rhs_vjp(w1) - s.rhs_vjp(w2)
+    assert np.max(np.abs(g - g_lin)) <= 1e-10 * np.max(np.abs(g))
+    parts = s.rhs_vjp(w1, 1) + s.rhs_vjp(w1, 2) + s.rhs_vjp(w1, 4)
+    g1 = s.rhs_vjp(w1, 7)
+    assert np.max(np.abs(parts - g1)) <= 1e-10 * np.max(np.abs(g1))
+
+
+def test_torch_autograd_wrapper(built, tmp_path):
+    """ostc_rhs / ostc_rhs_vjp as a torch.autograd.Function (test harness only): the gradient of
+    L(cv) = <w, rhs(cv)> by backward() against a central difference along a seeded direction."""
+    torch = pytest.importorskip("torch")
+    case = oc.reacting_mixing_layer_3d(mx=20, my=16, mz=10)
+    s, cv0 = _solver(case, tmp_path)
+
+    class Rhs(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, cv):
+            s.set_conservative(cv.detach().numpy())
+            return torch.from_numpy(s.rhs())
+
+        @staticmethod
+        def backward(ctx, g):
+            return torch.from_numpy(s.rhs_vjp(g.detach().numpy()))
+
+    rng = np.random.default_rng(11)
+    w = torch.from_numpy(rng.standard_normal(cv0.shape))
+    x = torch.from_numpy(cv0.copy()).requires_grad_(True)
+    loss = (w * Rhs.apply(x)).sum()
+    loss.backward()
+    v = _directions(cv0, rng, 1)[0]
+    jv = _fd(s, cv0, v, 7)
+    fd = float(np.sum(w.numpy() * jv))
+    ad = float(np.sum(x.grad.numpy() * v))
+    assert abs(fd - ad) <= RTOL * abs(fd) + ATOL * float(np.sum(np.abs(w.numpy() * jv)))
+
+
+def test_vjp_rejects_uncovered_cases(built, tmp_path):
+    import ostc
+
+    air = oc.mixing_layer_3d(mx=24, my=16, mz=8)
+    d = oc.write_case(air, tmp_path / "air")
+    s = ostc.Solver(str(d))
+    s.set_state(air.bv)
+    with pytest.raises(ostc.OstcError, match="multi-component"):
+        s.rhs_vjp(np.zeros((5,) + s.shape(0)))
+    case = oc.reacting_mixing_layer_3d(mx=20, my=16, mz=10)
+    s2, cv0 = _solver(case, tmp_path)
+    s2.set_chem_mode(ostc.CHEM_POINT_IMPLICIT)
+    with pytest.raises(ostc.OstcError, match="point-implicit"):
+        s2.rhs_vjp(np.zeros_like(cv0))
