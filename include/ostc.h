@@ -128,6 +128,20 @@ int ostc_set_conservative(ostc_ctx *ctx, int block, const double *cv, int ptr_ki
 int ostc_rhs_vjp(ostc_ctx *ctx, int block, unsigned term_mask, const double *dq_bar, double *cv_bar,
                  int ptr_kind);
 
+/* Adjoint of one SSP-RK3 step (RK.cuh:85-185, stage coefficients :10-14) from the current state, with
+ * the step's dt (CFL of the current state, or the fixed dt) held constant: lam_in = (d q' / d q)^T
+ * lam_out, q the interior conservative state before the step and q' after it (layout of dq).  The
+ * state is left as it was.  Same coverage as ostc_rhs_vjp, FP64 precision mode only. */
+int ostc_rk3_step_vjp(ostc_ctx *ctx, const double *lam_out, double *lam_in, int ptr_kind);
+
+/* Checkpointed discrete adjoint of n_steps SSP-RK3 steps from the current state: runs the steps
+ * (the context ends at the final state, as after ostc_rk3_step(n_steps)), keeping a device
+ * checkpoint every `every` steps and each step's dt, then sweeps backwards segment by segment,
+ * recomputing a segment's states from its checkpoint: lam_initial = (d q_N / d q_0)^T lam_final.
+ * Device memory: (n_steps / every + every + 1) states of (n_var + 6 + n_spec) padded planes. */
+int ostc_adjoint_steps(ostc_ctx *ctx, int n_steps, int every, const double *lam_final, double *lam_initial,
+                       int ptr_kind);
+
 /* Advance n_steps full SSP-RK3 steps (the loop body of RK3<mix,turb>, RK.cuh:85-185), all stream
  * ordered and replayed from a CUDA graph.  dt_last (nullable) receives the last step's dt (CFL
  * minimum over all blocks, TimeAdvanceFunc.cu:39-64, or the fixed dt); reading it synchronises. */

@@ -55,6 +55,7 @@ __device__ inline Dual exp(const Dual &a) {
   return Dual(e, e * a.d);
 }
 __device__ inline Dual log(const Dual &a) { return Dual(::log(a.v), a.d / a.v); }
+__device__ inline Dual fabs(const Dual &a) { return a.v < 0 ? -a : a; }
 __device__ inline Dual log10(const Dual &a) { return Dual(::log10(a.v), a.d / (a.v * 2.302585092994045684)); }
 __device__ inline Dual sqrt(const Dual &a) {
   const double s = ::sqrt(a.v);

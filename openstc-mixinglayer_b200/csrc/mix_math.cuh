@@ -156,24 +156,24 @@ __device__ __forceinline__ void mix_properties(T rho, T p, T t, const T *y, T &g
 
 // compute_temperature_and_pressure (FieldOperation.cu:3-40): Newton on e(T) starting from t, relative
 // tolerance 1e-3, at most 1000 iterations.  Returns T; p = rho R T through pout.
-template <int NS>
-__device__ __forceinline__ double mix_temperature(double rho, double e, double t, const double *y, double &pout) {
+template <int NS, typename T = double>
+__device__ __forceinline__ T mix_temperature(T rho, T e, T t, const T *y, T &pout) {
   const int ns = OSTC_NS;
-  double mw = 0;
+  T mw = 0;
   for (int l = 0; l < ns; ++l) mw += y[l] * c_mix.imw[l];
   mw = 1 / mw;
-  const double gc = kRuD / mw;
-  double err = 1;
+  const T gc = kRuD / mw;
+  T err = 1.0;
   int iter = 0;
-  double h[Spec<NS>::A], cp[Spec<NS>::A];
+  T h[Spec<NS>::A], cp[Spec<NS>::A];
   while (err > 1e-3 && iter++ < 1000) {
-    mix_h_cp<NS>(t, h, cp);
-    double cpt = 0, hm = 0;
+    mix_h_cp<NS, T>(t, h, cp);
+    T cpt = 0.0, hm = 0.0;
     for (int l = 0; l < ns; ++l) {
       cpt += cp[l] * y[l];
       hm += h[l] * y[l];
     }
-    const double t1 = t - (hm - gc * t - e) / (cpt - gc);
+    const T t1 = t - (hm - gc * t - e) / (cpt - gc);
     err = fabs(1 - t1 / t);
     t = t1;
   }

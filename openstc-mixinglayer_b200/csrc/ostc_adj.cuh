@@ -883,21 +883,71 @@ __global__ void __launch_bounds__(128) k_adj_props(DevBlock b, DevState s, DevAd
   }
 }
 
-// Reverse of the equation of state at every padded node: rho = cv0, u = cv1 / rho (v, w alike),
-// Y_l = cv_{5+l} / rho, T from e = cv4 / rho - |V|^2 / 2 = sum Y h(T) - Ru T sum Y / W
-// (compute_temperature_and_pressure, FieldOperation.cu:3-40, through the implicit-function
-// derivative at the node's T), p = rho Ru T sum Y / W.  Leaves the total cv adjoint in A.cv.
+// Ghost nodes hold copies of their source node's primitive state (bv, sv) and recompute their cv from
+// it (compute_cv_from_bv_1_point<mixture>, FieldOperation.cuh:78-105): rho E = rho (sum h(T) Y +
+// |V|^2 / 2) - p.  This moves a ghost's cv adjoint onto its primitive adjoints (rho, u, v, w, p, T, Y).
 template <int NS>
-__global__ void __launch_bounds__(128) k_adj_eos(DevBlock b, DevState s, DevAdj A) {
+__global__ void __launch_bounds__(128) k_adj_ghost_cv(DevBlock b, DevState s, DevAdj A, int nv) {
+  if (NS > 0) nv = 5 + NS;
   const long long P = b.plane;
   const int ns = OSTC_NS;
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
-    const double rho = s.cv[p];
     if (!(s.bv[p] > 0)) continue;
+    const int i = (int)(p % b.pitch) - b.g;
+    const long long r = p / b.pitch;
+    const int j = (int)(r % b.sy) - b.g, k = (int)(r / b.sy) - b.gz;
+    if (i >= 0 && i < b.mx && j >= 0 && j < b.my && k >= 0 && k < b.mz) continue;
+    const double rho = s.bv[p], u = s.bv[P + p], v = s.bv[2 * P + p], w = s.bv[3 * P + p], t = s.bv[5 * P + p];
+    double a[Spec<NS>::A + 5];
+    bool any = false;
+    for (int l = 0; l < nv; ++l) {
+      a[l] = A.cv[l * P + p];
+      any = any || a[l] != 0.0;
+      A.cv[l * P + p] = 0.0;
+    }
+    if (!any) continue;
+    double h[Spec<NS>::A], cp[Spec<NS>::A];
+    mix_h_cp<NS, double>(t, h, cp);
+    double hy = 0, cpy = 0;
+    for (int l = 0; l < ns; ++l) {
+      const double y = s.sv[l * P + p];
+      hy += h[l] * y;
+      cpy += cp[l] * y;
+    }
+    const double ek = 0.5 * (u * u + v * v + w * w);
+    double arho = a[0] + a[1] * u + a[2] * v + a[3] * w + a[4] * (hy + ek);
+    for (int l = 0; l < ns; ++l) {
+      arho += a[5 + l] * s.sv[l * P + p];
+      A.Y[(long long)l * P + p] += a[4] * rho * h[l] + a[5 + l] * rho;
+    }
+    A.rho[p] += arho;
+    A.vel[p] += (a[1] + a[4] * u) * rho;
+    A.vel[P + p] += (a[2] + a[4] * v) * rho;
+    A.vel[2 * P + p] += (a[3] + a[4] * w) * rho;
+    A.T[p] += a[4] * rho * cpy;
+    A.p[p] -= a[4];
+  }
+}
+
+// Interior nodes: primitive adjoints -> cv (and T) adjoints.  rho = cv0, u = cv1 / rho (v, w
+// alike), Y_l = cv_{5+l} / rho, p = rho Ru T sum Y / W.  With exact_t the node's T is the root of
+// e = cv4 / rho - |V|^2 / 2 = sum Y h(T) - Ru T sum Y / W (compute_temperature_and_pressure,
+// FieldOperation.cu:3-40) and its adjoint goes to cv by the implicit-function derivative; otherwise
+// T is a state variable of its own and its adjoint is left in A.T.
+template <int NS>
+__global__ void __launch_bounds__(128) k_adj_eos(DevBlock b, DevState s, DevAdj A, int exact_t) {
+  const long long P = b.plane;
+  const int ns = OSTC_NS;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % b.mx);
+    const long long r = n / b.mx;
+    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const long long p = b.id(i, j, k);
+    const double rho = s.cv[p];
     const double t = s.bv[5 * P + p];
     const double irho = 1.0 / rho;
     const double u = s.cv[P + p] * irho, v = s.cv[2 * P + p] * irho, w = s.cv[3 * P + p] * irho;
-    double y[Spec<NS>::A], ay[Spec<NS>::A], h[Spec<NS>::A], cp[Spec<NS>::A];
+    double y[Spec<NS>::A], ay[Spec<NS>::A];
     double gsum = 0;  // sum Y / W
     for (int l = 0; l < ns; ++l) {
       y[l] = s.cv[(5 + l) * P + p] * irho;
@@ -911,19 +961,22 @@ __global__ void __launch_bounds__(128) k_adj_eos(DevBlock b, DevState s, DevAdj 
     arho += ap * kRuD * t * gsum;
     aT += ap * rho * kRuD * gsum;
     for (int l = 0; l < ns; ++l) ay[l] += ap * rho * kRuD * t * c_mix.imw[l];
-    // T(e, Y)
-    mix_h_cp<NS, double>(t, h, cp);
-    double cvm = 0;
-    for (int l = 0; l < ns; ++l) cvm += y[l] * (cp[l] - kRuD * c_mix.imw[l]);
-    const double ae = aT / cvm;
-    for (int l = 0; l < ns; ++l) ay[l] -= aT * (h[l] - kRuD * t * c_mix.imw[l]) / cvm;
-    // e = cv4 / rho - (u^2 + v^2 + w^2) / 2
-    double acv4 = A.cv[4 * P + p] + ae * irho;
-    arho -= ae * s.cv[4 * P + p] * irho * irho;
-    au -= ae * u;
-    av -= ae * v;
-    aw -= ae * w;
-    A.cv[4 * P + p] = acv4;
+    if (exact_t) {
+      double h[Spec<NS>::A], cp[Spec<NS>::A];
+      mix_h_cp<NS, double>(t, h, cp);
+      double cvm = 0;
+      for (int l = 0; l < ns; ++l) cvm += y[l] * (cp[l] - kRuD * c_mix.imw[l]);
+      const double ae = aT / cvm;
+      for (int l = 0; l < ns; ++l) ay[l] -= aT * (h[l] - kRuD * t * c_mix.imw[l]) / cvm;
+      // e = cv4 / rho - (u^2 + v^2 + w^2) / 2
+      A.cv[4 * P + p] += ae * irho;
+      arho -= ae * s.cv[4 * P + p] * irho * irho;
+      au -= ae * u;
+      av -= ae * v;
+      aw -= ae * w;
+      aT = 0.0;
+    }
+    A.T[p] = aT;
     A.cv[P + p] += au * irho;
     A.cv[2 * P + p] += av * irho;
     A.cv[3 * P + p] += aw * irho;
@@ -937,9 +990,10 @@ __global__ void __launch_bounds__(128) k_adj_eos(DevBlock b, DevState s, DevAdj 
 }
 
 // Ghost fills in reverse (apply_outflow / apply_periodic, BoundCond.cuh:205-233, 1443-1486): each
-// ghost node's cv adjoint moves to the node it was copied from.  Faces run in the reverse of the
-// forward order, so a ghost filled from another face's ghost passes its adjoint on in turn.
-__global__ void __launch_bounds__(128) k_adj_bc_face(DevBlock b, double *Acv, int nv, DevFace f) {
+// ghost node's primitive adjoints (rho, u, v, w, p, T, Y) move to the node it was copied from.  Faces
+// run in the reverse of the forward order, so a ghost filled from another face's ghost passes its
+// adjoint on in turn.
+__global__ void __launch_bounds__(128) k_adj_bc_face(DevBlock b, DevAdj A, int ns, DevFace f) {
   const int t0 = f.face == 0 ? 1 : 0;
   const int t1 = f.face == 2 ? 1 : 2;
   const int n0 = f.re[t0] - f.rs[t0] + 1, n1 = f.re[t1] - f.rs[t1] + 1;
@@ -949,6 +1003,7 @@ __global__ void __launch_bounds__(128) k_adj_bc_face(DevBlock b, double *Acv, in
   int dir[3] = {0, 0, 0};
   dir[f.face] = f.direction;
   const long long dstep = dir[0] * st[0] + dir[1] * st[1] + dir[2] * st[2];
+  double *planes[6] = {A.rho, A.vel, A.vel + P, A.vel + 2 * P, A.p, A.T};
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += (long long)gridDim.x * blockDim.x) {
     int idx[3];
     idx[f.face] = f.rs[f.face];
@@ -965,15 +1020,69 @@ __global__ void __launch_bounds__(128) k_adj_bc_face(DevBlock b, double *Acv, in
     for (int g = b.g; g >= 1; --g) {
       const long long pg = pb + g * dstep;
       const long long ps = f.type == kPeriodic ? po + g * dstep : pb;
-      for (int l = 0; l < nv; ++l) {
-        Acv[l * P + ps] += Acv[l * P + pg];
-        Acv[l * P + pg] = 0.0;
+      for (int q = 0; q < 6; ++q) {
+        planes[q][ps] += planes[q][pg];
+        planes[q][pg] = 0.0;
+      }
+      for (int l = 0; l < ns; ++l) {
+        A.Y[l * P + ps] += A.Y[l * P + pg];
+        A.Y[l * P + pg] = 0.0;
       }
     }
   }
 }
 
-// interior part of the cv adjoint, in the layout of dq
+// Reverse of the stage's temperature Newton iteration (update_cv_and_bv_rk + compute_temperature_and_
+// pressure, RK.cuh:230-284, FieldOperation.cu:3-40): T_out = N(T_start; e, Y) of the stage output's
+// cv, started from the stage input's T, iterated to the reference's relative tolerance 1e-3.  The
+// iterate (not the exact root) is differentiated, by Dual evaluations seeded on e, each Y and the
+// start T: lam_cv += (dT_out / d cv_out)^T lam_t, lam_t_start += dT_out / dT_start * lam_t.
+template <int NS>
+__global__ void __launch_bounds__(128) k_adj_newton(DevBlock b, DevState in, DevState out, const double *lam_t,
+                                                    double *lam_cv, double *lam_t_start) {
+  const long long P = b.plane;
+  const int ns = OSTC_NS;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    const double lt = lam_t[n];
+    if (lt == 0.0) continue;
+    const int i = (int)(n % b.mx);
+    const long long r = n / b.mx;
+    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const long long p = b.id(i, j, k);
+    const double rho = out.cv[p], irho = 1.0 / rho;
+    const double u = out.cv[P + p] * irho, v = out.cv[2 * P + p] * irho, w = out.cv[3 * P + p] * irho;
+    const double e = out.cv[4 * P + p] / rho - 0.5 * (u * u + v * v + w * w);
+    const double t0 = in.bv[5 * P + p];
+    double yv[Spec<NS>::A];
+    for (int l = 0; l < ns; ++l) yv[l] = out.cv[(5 + l) * P + p] * irho;
+    double de = 0, dts = 0, dy[Spec<NS>::A];
+    for (int in_ = 0; in_ < ns + 2; ++in_) {
+      Dual y[Spec<NS>::A], pr;
+      for (int l = 0; l < ns; ++l) y[l] = Dual(yv[l], in_ == 2 + l ? 1.0 : 0.0);
+      const Dual t = mix_temperature<NS, Dual>(Dual(rho), Dual(e, in_ == 0 ? 1.0 : 0.0), Dual(t0, in_ == 1 ? 1.0 : 0.0),
+                                               y, pr);
+      if (in_ == 0) de = t.d;
+      else if (in_ == 1) dts = t.d;
+      else dy[in_ - 2] = t.d;
+    }
+    lam_t_start[n] += dts * lt;
+    // e = cv4 / rho - |V|^2 / 2, Y = cv_{5+l} / rho
+    const double ae = de * lt;
+    double arho = -ae * out.cv[4 * P + p] * irho * irho + ae * (u * u + v * v + w * w) * irho;
+    lam_cv[4 * b.n + n] += ae * irho;
+    lam_cv[b.n + n] -= ae * u * irho;
+    lam_cv[2 * b.n + n] -= ae * v * irho;
+    lam_cv[3 * b.n + n] -= ae * w * irho;
+    for (int l = 0; l < ns; ++l) {
+      const double ay = dy[l] * lt;
+      lam_cv[(5 + l) * b.n + n] += ay * irho;
+      arho -= ay * yv[l] * irho;
+    }
+    lam_cv[n] += arho;
+  }
+}
+
+// interior part of nv adjoint planes, in the layout of dq
 __global__ void k_adj_gather(DevBlock b, const double *__restrict__ Acv, int nv, double *__restrict__ out) {
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(n % b.mx);
@@ -981,6 +1090,64 @@ __global__ void k_adj_gather(DevBlock b, const double *__restrict__ Acv, int nv,
     const int j = (int)(r % b.my), k = (int)(r / b.my);
     const long long p = b.id(i, j, k);
     for (int l = 0; l < nv; ++l) out[l * b.n + n] = Acv[l * b.plane + p];
+  }
+}
+
+// Seed of a stage's right-hand-side adjoint: dqb = c dt / J * lam (the stage adds c dt / J * dq to
+// cv, update_cv_and_bv_rk, RK.cuh:230-284).  2-D blocks zero component 3 of lam in place first: the
+// stage output's rho*w is set to 0, so its adjoint never reaches the stage's inputs.
+__global__ void k_adj_stage_seed(DevBlock b, double *lam, double c, const double *dtp, double *dqb, int nv) {
+  const double dt = *dtp;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % b.mx);
+    const long long r = n / b.mx;
+    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const double f = c * dt / b.jac[b.id(i, j, k)];
+    if (b.mz == 1) lam[3 * b.n + n] = 0.0;
+    for (int l = 0; l < nv; ++l) dqb[l * b.n + n] = f * lam[l * b.n + n];
+  }
+}
+
+// y = a x + c y over n values
+__global__ void k_axpby(long long n, double a, const double *__restrict__ x, double c, double *__restrict__ y) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = a * x[i] + c * y[i];
+}
+
+// lam_cv += (dT / dcv)^T lam_t for T the equation-of-state root of the node's cv (implicit-function
+// derivative of sum Y h(T) - Ru T sum Y / W = cv4 / rho - |V|^2 / 2), interior nodes
+template <int NS>
+__global__ void __launch_bounds__(128) k_adj_t_to_cv(DevBlock b, DevState s, const double *lam_t, double *lam_cv) {
+  const long long P = b.plane;
+  const int ns = OSTC_NS;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    const double lt = lam_t[n];
+    if (lt == 0.0) continue;
+    const int i = (int)(n % b.mx);
+    const long long r = n / b.mx;
+    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const long long p = b.id(i, j, k);
+    const double rho = s.cv[p], irho = 1.0 / rho, t = s.bv[5 * P + p];
+    const double u = s.cv[P + p] * irho, v = s.cv[2 * P + p] * irho, w = s.cv[3 * P + p] * irho;
+    double y[Spec<NS>::A], h[Spec<NS>::A], cp[Spec<NS>::A];
+    mix_h_cp<NS, double>(t, h, cp);
+    double cvm = 0;
+    for (int l = 0; l < ns; ++l) {
+      y[l] = s.cv[(5 + l) * P + p] * irho;
+      cvm += y[l] * (cp[l] - kRuD * c_mix.imw[l]);
+    }
+    const double ae = lt / cvm;
+    double arho = -ae * s.cv[4 * P + p] * irho * irho + ae * (u * u + v * v + w * w) * irho;
+    lam_cv[4 * b.n + n] += ae * irho;
+    lam_cv[b.n + n] -= ae * u * irho;
+    lam_cv[2 * b.n + n] -= ae * v * irho;
+    lam_cv[3 * b.n + n] -= ae * w * irho;
+    for (int l = 0; l < ns; ++l) {
+      const double ay = -lt * (h[l] - kRuD * t * c_mix.imw[l]) / cvm;
+      lam_cv[(5 + l) * b.n + n] += ay * irho;
+      arho -= ay * y[l] * irho;
+    }
+    lam_cv[n] += arho;
   }
 }
 

@@ -1188,8 +1188,9 @@ using namespace ostc;
 struct BlockRes {
   DevBlock db{};
   double *met = nullptr, *jac = nullptr;
-  double *cv[3]{}, *bv[3]{}, *mul[3]{};
-  double *sv[3]{}, *cond[3]{}, *rhod[3]{}, *gam[3]{}, *acs[3]{};  // mixtures only
+  // state slots: 0..2 the RK3 stage buffers, 3 the step adjoint's copy of a step's output
+  double *cv[4]{}, *bv[4]{}, *mul[4]{};
+  double *sv[4]{}, *cond[4]{}, *rhod[4]{}, *gam[4]{}, *acs[4]{};  // mixtures only
   double *dq = nullptr;
   double *last = nullptr;
   std::vector<DevFace> faces;  // file order
@@ -1198,6 +1199,8 @@ struct BlockRes {
   std::vector<int> inner_target;
   double *adj = nullptr;  // node adjoint planes of ostc_rhs_vjp (allocated on first use)
   double *dqb = nullptr;  // dq_bar on the device
+  // step adjoint: [lam_cv, x2_cv, x1_cv, g_cv] (n_var x N each) then [lam_T, x2_T, x1_T, g_T] (N each)
+  double *adj_work = nullptr;
 };
 
 struct ostc_ctx {
@@ -1479,7 +1482,7 @@ void launch_adjoint_t(ostc_ctx *ctx, BlockRes &B, DevState in, unsigned mask, co
   if ((mask & OSTC_TERM_SOURCE) && ctx->der.reaction == 1)
     k_adj_source<NS><<<grid_for(ctx, b.n, 128), 128, 0, ctx->stream>>>(b, in, B.dqb, A);
   k_adj_props<NS><<<grid_for(ctx, b.plane, 128), 128, 0, ctx->stream>>>(b, in, A);
-  k_adj_eos<NS><<<grid_for(ctx, b.plane, 128), 128, 0, ctx->stream>>>(b, in, A);
+  k_adj_ghost_cv<NS><<<grid_for(ctx, b.plane, 128), 128, 0, ctx->stream>>>(b, in, A, nv);
 }
 
 // y / z sweep variants: 0 = column march, 1..3 = tiles of the shapes below (per precision: rows
@@ -1811,56 +1814,220 @@ int enqueue_step(ostc_ctx *ctx) {
   return OSTC_OK;
 }
 
-// One SSP-RK3 step of a mixture (RK.cuh:85-185 with MixtureModel Mixture / FR): source, flux-split
-// WENO7, viscous, update + temperature Newton, boundary faces, properties.
-int enqueue_step_mix(ostc_ctx *ctx) {
+// CFL time step of the current state (slot 0) into d_dt (local_time_step + global_time_step)
+void enqueue_mix_dt(ostc_ctx *ctx) {
+  long tok = begin_t(ctx, "cfl_dt");
+  k_dt_reset<<<1, 1, 0, ctx->stream>>>(ctx->d_dtbits);
+  for (auto &B : ctx->blk)
+    k_cfl_dt<<<grid_for(ctx, B.db.n, 256), 256, 0, ctx->stream>>>(B.db, state_of(B, 0), ctx->der.cfl,
+                                                                 ctx->der.prandtl, B.db.mz > 1, ctx->d_dtbits);
+  k_dt_decode<<<1, 1, 0, ctx->stream>>>(ctx->d_dtbits, ctx->d_dt);
+  end_t(ctx, tok);
+}
+
+// Stage rk (0..2) of a mixture SSP-RK3 step: state slot rk -> slot (rk + 1) % 3, with slot 0 the
+// step's start state and d_dt the step's dt.
+void enqueue_mix_stage(ostc_ctx *ctx, int rk, int sout_override = -1) {
   static const double A[3] = {1.0, 0.75, 1.0 / 3.0}, Bc[3] = {0.0, 0.25, 2.0 / 3.0}, C[3] = {1.0, 0.25, 2.0 / 3.0};
-  const bool fixed = ctx->der.fixed_time_step;
   const int nv = ctx->nv;
-  for (int rk = 0; rk < 3; ++rk) {
-    const int sin = rk, sout = (rk + 1) % 3;
-    if (rk == 0 && !fixed) {
-      long tok = begin_t(ctx, "cfl_dt");
-      k_dt_reset<<<1, 1, 0, ctx->stream>>>(ctx->d_dtbits);
-      for (auto &B : ctx->blk)
-        k_cfl_dt<<<grid_for(ctx, B.db.n, 256), 256, 0, ctx->stream>>>(B.db, state_of(B, sin), ctx->der.cfl,
-                                                                     ctx->der.prandtl, B.db.mz > 1, ctx->d_dtbits);
-      k_dt_decode<<<1, 1, 0, ctx->stream>>>(ctx->d_dtbits, ctx->d_dt);
+  const int sin = rk, sout = sout_override >= 0 ? sout_override : (rk + 1) % 3;
+  for (size_t bi = 0; bi < ctx->blk.size(); ++bi) {
+    BlockRes &B = ctx->blk[bi];
+    const DevState in = state_of(B, sin);
+    const bool chem = ctx->der.reaction == 1, implicit = chem && ctx->chem_mode == OSTC_CHEM_POINT_IMPLICIT;
+    {
+      long tok = begin_t(ctx, "source");
+      launch_mix_source(ctx, B, in, chem && !implicit);
       end_t(ctx, tok);
     }
-    for (size_t bi = 0; bi < ctx->blk.size(); ++bi) {
-      BlockRes &B = ctx->blk[bi];
-      const DevState in = state_of(B, sin);
-      const bool chem = ctx->der.reaction == 1, implicit = chem && ctx->chem_mode == OSTC_CHEM_POINT_IMPLICIT;
-      {
-        long tok = begin_t(ctx, "source");
-        launch_mix_source(ctx, B, in, chem && !implicit);
-        end_t(ctx, tok);
-      }
-      launch_fvs(ctx, B, in);
-      if (ctx->der.viscous_order != 0) launch_mix_visc(ctx, B, in);
-      if (implicit) launch_chem_epi(ctx, B, in);
-      {
-        long tok = begin_t(ctx, "update");
-        if (ctx->der.n_spec == kFixedNS)
-          k_mix_update<kFixedNS><<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(
-              B.db, in, state_of(B, 0), state_of(B, sout), B.dq, ctx->d_dt, A[rk], Bc[rk], C[rk], nv, ctx->d_flags);
-        else
-          k_mix_update<0><<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(
-              B.db, in, state_of(B, 0), state_of(B, sout), B.dq, ctx->d_dt, A[rk], Bc[rk], C[rk], nv, ctx->d_flags);
-        end_t(ctx, tok);
-      }
-      launch_carry(ctx, B, in, state_of(B, sout));
-      launch_bcs(ctx, (int)bi, state_of(B, sout));
-    }
-    launch_interfaces(ctx, sout);
-    for (auto &B : ctx->blk) {
-      long tok = begin_t(ctx, "properties");
-      launch_mix_props(ctx, B, state_of(B, sout));
+    launch_fvs(ctx, B, in);
+    if (ctx->der.viscous_order != 0) launch_mix_visc(ctx, B, in);
+    if (implicit) launch_chem_epi(ctx, B, in);
+    {
+      long tok = begin_t(ctx, "update");
+      if (ctx->der.n_spec == kFixedNS)
+        k_mix_update<kFixedNS><<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(
+            B.db, in, state_of(B, 0), state_of(B, sout), B.dq, ctx->d_dt, A[rk], Bc[rk], C[rk], nv, ctx->d_flags);
+      else
+        k_mix_update<0><<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(
+            B.db, in, state_of(B, 0), state_of(B, sout), B.dq, ctx->d_dt, A[rk], Bc[rk], C[rk], nv, ctx->d_flags);
       end_t(ctx, tok);
     }
+    launch_carry(ctx, B, in, state_of(B, sout));
+    launch_bcs(ctx, (int)bi, state_of(B, sout));
   }
+  launch_interfaces(ctx, sout);
+  for (auto &B : ctx->blk) {
+    long tok = begin_t(ctx, "properties");
+    launch_mix_props(ctx, B, state_of(B, sout));
+    end_t(ctx, tok);
+  }
+}
+
+// One SSP-RK3 step of a mixture (RK.cuh:85-185 with MixtureModel Mixture / FR): source, flux-split
+// WENO7, viscous, update + temperature Newton, boundary faces, properties, per stage.
+int enqueue_step_mix(ostc_ctx *ctx) {
+  if (!ctx->der.fixed_time_step) enqueue_mix_dt(ctx);
+  for (int rk = 0; rk < 3; ++rk) enqueue_mix_stage(ctx, rk);
   k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->d_time, ctx->d_dt, ctx->d_step);
+  return OSTC_OK;
+}
+
+// ---- adjoint entry points' shared pieces
+
+// what the adjoint covers: the multi-component path, explicit chemistry, one block, periodic and
+// outflow faces
+int adjoint_check(ostc_ctx *ctx, unsigned mask) {
+  if (!ctx->mixture) {
+    ctx->err = "the adjoint covers the multi-component path (species = 1)";
+    return OSTC_EINVAL;
+  }
+  if ((mask & OSTC_TERM_SOURCE) && ctx->der.reaction == 1 && ctx->chem_mode == OSTC_CHEM_POINT_IMPLICIT) {
+    ctx->err = "the point-implicit chemistry mode has no adjoint; use the explicit source";
+    return OSTC_EINVAL;
+  }
+  if (ctx->blk.size() > 1 || !ctx->blk[0].inner.empty()) {
+    ctx->err = "the adjoint covers single-block cases (interfaces couple the blocks' right-hand sides)";
+    return OSTC_EINVAL;
+  }
+  for (const auto &f : ctx->blk[0].faces)
+    if (f.type != kPeriodic && f.type != kOutflow) {
+      ctx->err = "the adjoint covers periodic and outflow boundary faces";
+      return OSTC_EINVAL;
+    }
+  return OSTC_OK;
+}
+
+int adjoint_alloc(ostc_ctx *ctx, BlockRes &B) {
+  if (B.adj) return OSTC_OK;
+  const int nv = ctx->nv, ns = ctx->der.n_spec;
+  const long long P = B.db.plane;
+  CK(cudaMalloc(&B.adj, (size_t)(nv + 9 + 2 * ns) * P * sizeof(double)));
+  CK(cudaMalloc(&B.dqb, (size_t)nv * B.db.n * sizeof(double)));
+  CK(cudaMalloc(&B.adj_work, (size_t)4 * (nv + 1) * B.db.n * sizeof(double)));
+  // state slot 3 (zeroed: its padding columns must read as empty nodes)
+  auto alloc = [&](double **p, size_t n) -> int {
+    if (cudaMalloc(p, n * sizeof(double)) != cudaSuccess || cudaMemset(*p, 0, n * sizeof(double)) != cudaSuccess)
+      return OSTC_ENOMEM;
+    return OSTC_OK;
+  };
+  int r = alloc(&B.cv[3], (size_t)nv * P);
+  if (!r) r = alloc(&B.bv[3], 6 * P);
+  if (!r) r = alloc(&B.mul[3], P);
+  if (!r) r = alloc(&B.sv[3], (size_t)ns * P);
+  if (!r) r = alloc(&B.rhod[3], (size_t)ns * P);
+  if (!r) r = alloc(&B.cond[3], P);
+  if (!r) r = alloc(&B.gam[3], P);
+  if (!r) r = alloc(&B.acs[3], P);
+  if (r) ctx->err = "device allocation for the adjoint failed";
+  return r;
+}
+
+// out (device, n_var x N) = (d dq / d cv)^T B.dqb at the state in `slot` of block `block`.  With
+// out_t null the state's T is the equation-of-state root of its cv (its adjoint goes to cv); else T
+// is a state variable and out_t (device, N) receives (d dq / d T)^T B.dqb.
+int vjp_core(ostc_ctx *ctx, int block, int slot, unsigned mask, double *out, double *out_t = nullptr) {
+  BlockRes &B = ctx->blk[block];
+  const int nv = ctx->nv, ns = ctx->der.n_spec;
+  const long long P = B.db.plane;
+  CK(cudaMemsetAsync(B.adj, 0, (size_t)(nv + 9 + 2 * ns) * P * sizeof(double), ctx->stream));
+  DevAdj A;
+  A.cv = B.adj;
+  A.p = A.cv + nv * P;
+  A.c = A.p + P;
+  A.rho = A.c + P;
+  A.vel = A.rho + P;
+  A.T = A.vel + 3 * P;
+  A.Y = A.T + P;
+  A.mu = A.Y + ns * P;
+  A.lam = A.mu + P;
+  A.rhod = A.lam + P;
+  const DevState in = state_of(B, slot);
+  if (ns == kFixedNS) launch_adjoint_t<kFixedNS>(ctx, B, in, mask, A);
+  else launch_adjoint_t<0>(ctx, B, in, mask, A);
+  for (auto it = ctx->order.rbegin(); it != ctx->order.rend(); ++it) {
+    if (it->first != block) continue;
+    const DevFace &f = B.faces[it->second];
+    const int t0 = f.face == 0 ? 1 : 0, t1 = f.face == 2 ? 1 : 2;
+    const long long nn = (long long)(f.re[t0] - f.rs[t0] + 1) * (f.re[t1] - f.rs[t1] + 1);
+    k_adj_bc_face<<<grid_for(ctx, nn, 128), 128, 0, ctx->stream>>>(B.db, A, ns, f);
+  }
+  if (ns == kFixedNS)
+    k_adj_eos<kFixedNS><<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, in, A, out_t ? 0 : 1);
+  else
+    k_adj_eos<0><<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, in, A, out_t ? 0 : 1);
+  k_adj_gather<<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, A.cv, nv, out);
+  if (out_t) k_adj_gather<<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, A.T, 1, out_t);
+  CK(cudaGetLastError());
+  return OSTC_OK;
+}
+
+// Adjoint of one SSP-RK3 step from the state in slot 0 with the dt in d_dt.  The step's state is
+// (cv, T): every stage's T is the temperature Newton iterate started from the stage input's T
+// (k_mix_update), so T carries an adjoint of its own.  On entry the work buffers hold lam_cv' and
+// lam_T' of the step's output, on return lam_cv and lam_T of slot 0.  With
+// S1 = q + dt/J R(q), S2 = 3/4 q + 1/4 S1 + 1/4 dt/J R(S1), q' = 1/3 q + 2/3 S2 + 2/3 dt/J R(S2)
+// (RK.cuh:10-14) and T_s = N(T_{s-1}; cv_s):
+//   stage 3: lam_cv' += N'^T lam_T';  x2 = 2/3 lam_cv' + R'(S2)^T (2/3 dt/J lam_cv'),
+//            x2_T = R'_T(S2)^T (...) + dN/dT_start lam_T'
+//   stage 2: likewise from (x2, x2_T) to (x1, x1_T) with 1/4, stage 1 to q with 1;
+//   lam_cv = 1/3 lam_cv' + 3/4 x2 + x1 + R'(q)^T (dt/J x1),  lam_T = R'_T(q)^T (...) + dN/dT_start x1_T.
+int step_vjp(ostc_ctx *ctx) {
+  BlockRes &B = ctx->blk[0];
+  const int nv = ctx->nv;
+  const long long N = B.db.n, nt = (long long)nv * N;
+  double *Lc = B.adj_work, *X2c = Lc + nt, *X1c = X2c + nt, *Gc = X1c + nt;
+  double *LT = Gc + nt, *X2T = LT + N, *X1T = X2T + N, *GT = X1T + N;
+  const int g = grid_for(ctx, N, 128), gt = grid_for(ctx, nt, 256), g1 = grid_for(ctx, N, 256);
+  auto newton = [&](int sin, int sout, const double *lt, double *lc, double *lts) {
+    if (ctx->der.n_spec == kFixedNS)
+      k_adj_newton<kFixedNS><<<g, 128, 0, ctx->stream>>>(B.db, state_of(B, sin), state_of(B, sout), lt, lc, lts);
+    else
+      k_adj_newton<0><<<g, 128, 0, ctx->stream>>>(B.db, state_of(B, sin), state_of(B, sout), lt, lc, lts);
+  };
+  enqueue_mix_stage(ctx, 0);     // S1 -> slot 1
+  enqueue_mix_stage(ctx, 1);     // S2 -> slot 2
+  enqueue_mix_stage(ctx, 2, 3);  // q' -> slot 3 (slot 0 keeps q)
+  // stage 3
+  CK(cudaMemsetAsync(X2T, 0, N * sizeof(double), ctx->stream));
+  newton(2, 3, LT, Lc, X2T);
+  k_adj_stage_seed<<<g, 128, 0, ctx->stream>>>(B.db, Lc, 2.0 / 3.0, ctx->d_dt, B.dqb, nv);
+  if (int r = vjp_core(ctx, 0, 2, OSTC_TERM_ALL, X2c, GT)) return r;
+  k_axpby<<<gt, 256, 0, ctx->stream>>>(nt, 2.0 / 3.0, Lc, 1.0, X2c);
+  k_axpby<<<g1, 256, 0, ctx->stream>>>(N, 1.0, GT, 1.0, X2T);
+  // stage 2
+  CK(cudaMemsetAsync(X1T, 0, N * sizeof(double), ctx->stream));
+  newton(1, 2, X2T, X2c, X1T);
+  k_adj_stage_seed<<<g, 128, 0, ctx->stream>>>(B.db, X2c, 0.25, ctx->d_dt, B.dqb, nv);
+  if (int r = vjp_core(ctx, 0, 1, OSTC_TERM_ALL, X1c, GT)) return r;
+  k_axpby<<<gt, 256, 0, ctx->stream>>>(nt, 0.25, X2c, 1.0, X1c);
+  k_axpby<<<g1, 256, 0, ctx->stream>>>(N, 1.0, GT, 1.0, X1T);
+  // stage 1
+  CK(cudaMemsetAsync(LT, 0, N * sizeof(double), ctx->stream));
+  newton(0, 1, X1T, X1c, LT);
+  k_adj_stage_seed<<<g, 128, 0, ctx->stream>>>(B.db, X1c, 1.0, ctx->d_dt, B.dqb, nv);
+  if (int r = vjp_core(ctx, 0, 0, OSTC_TERM_ALL, Gc, GT)) return r;
+  k_axpby<<<gt, 256, 0, ctx->stream>>>(nt, 0.75, X2c, 1.0 / 3.0, Lc);
+  k_axpby<<<gt, 256, 0, ctx->stream>>>(nt, 1.0, X1c, 1.0, Lc);
+  k_axpby<<<gt, 256, 0, ctx->stream>>>(nt, 1.0, Gc, 1.0, Lc);
+  k_axpby<<<g1, 256, 0, ctx->stream>>>(N, 1.0, GT, 1.0, LT);
+  CK(cudaGetLastError());
+  return OSTC_OK;
+}
+
+// lam_cv += (dT / dcv)^T lam_T at slot 0, T the equation-of-state root of cv (the start of a
+// trajectory set by ostc_set_state or ostc_set_conservative), then lam_T = 0
+int adjoint_t_to_cv(ostc_ctx *ctx) {
+  BlockRes &B = ctx->blk[0];
+  const long long N = B.db.n, nt = (long long)ctx->nv * N;
+  double *Lc = B.adj_work, *LT = Lc + 4 * nt;
+  const int g = grid_for(ctx, N, 128);
+  if (ctx->der.n_spec == kFixedNS)
+    k_adj_t_to_cv<kFixedNS><<<g, 128, 0, ctx->stream>>>(B.db, state_of(B, 0), LT, Lc);
+  else
+    k_adj_t_to_cv<0><<<g, 128, 0, ctx->stream>>>(B.db, state_of(B, 0), LT, Lc);
+  CK(cudaMemsetAsync(LT, 0, N * sizeof(double), ctx->stream));
+  CK(cudaGetLastError());
   return OSTC_OK;
 }
 
@@ -2153,7 +2320,8 @@ void ostc_destroy(ostc_ctx *ctx) {
     cudaFree(B.last);
     cudaFree(B.adj);
     cudaFree(B.dqb);
-    for (int s = 0; s < 3; ++s) {
+    cudaFree(B.adj_work);
+    for (int s = 0; s < 4; ++s) {
       cudaFree(B.cv[s]);
       cudaFree(B.bv[s]);
       cudaFree(B.mul[s]);
@@ -2383,62 +2551,143 @@ int ostc_set_conservative(ostc_ctx *ctx, int block, const double *cv, int ptr_ki
 
 int ostc_rhs_vjp(ostc_ctx *ctx, int block, unsigned mask, const double *dq_bar, double *cv_bar, int ptr_kind) {
   if (!ctx || !dq_bar || !cv_bar || block < 0 || block >= (int)ctx->blk.size()) return OSTC_EINVAL;
-  if (!ctx->mixture) {
-    ctx->err = "ostc_rhs_vjp covers the multi-component path (species = 1)";
-    return OSTC_EINVAL;
-  }
-  if ((mask & OSTC_TERM_SOURCE) && ctx->der.reaction == 1 && ctx->chem_mode == OSTC_CHEM_POINT_IMPLICIT) {
-    ctx->err = "ostc_rhs_vjp: the point-implicit chemistry mode has no adjoint; use the explicit source";
-    return OSTC_EINVAL;
-  }
-  BlockRes &B = ctx->blk[block];
-  if (ctx->blk.size() > 1 || !B.inner.empty()) {
-    ctx->err = "ostc_rhs_vjp: single-block cases only (interfaces couple the blocks' right-hand sides)";
-    return OSTC_EINVAL;
-  }
-  for (const auto &f : B.faces)
-    if (f.type != kPeriodic && f.type != kOutflow) {
-      ctx->err = "ostc_rhs_vjp: boundary faces must be periodic or outflow";
-      return OSTC_EINVAL;
-    }
+  if (int r = adjoint_check(ctx, mask)) return r;
   cudaSetDevice(ctx->device);
   if (int r = check_ready(ctx)) return r;
-  const int nv = ctx->nv, ns = ctx->der.n_spec;
-  const long long P = B.db.plane;
-  const int planes = nv + 9 + 2 * ns;
-  if (!B.adj) {
-    CK(cudaMalloc(&B.adj, (size_t)planes * P * sizeof(double)));
-    CK(cudaMalloc(&B.dqb, (size_t)nv * B.db.n * sizeof(double)));
+  BlockRes &B = ctx->blk[block];
+  if (int r = adjoint_alloc(ctx, B)) return r;
+  const size_t bytes = (size_t)ctx->nv * B.db.n * sizeof(double);
+  CK(cudaMemcpyAsync(B.dqb, dq_bar, bytes, ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                     ctx->stream));
+  if (int r = vjp_core(ctx, block, 0, mask, B.dq)) return r;
+  CK(cudaMemcpyAsync(cv_bar, B.dq, bytes, ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return OSTC_OK;
+}
+
+int ostc_rk3_step_vjp(ostc_ctx *ctx, const double *lam_out, double *lam_in, int ptr_kind) {
+  if (!ctx || !lam_out || !lam_in) return OSTC_EINVAL;
+  if (int r = adjoint_check(ctx, OSTC_TERM_ALL)) return r;
+  if (ctx->precision != OSTC_PREC_FP64) {
+    ctx->err = "the step adjoint is that of the FP64 step: set OSTC_PREC_FP64";
+    return OSTC_EINVAL;
   }
-  CK(cudaMemsetAsync(B.adj, 0, (size_t)planes * P * sizeof(double), ctx->stream));
-  CK(cudaMemcpyAsync(B.dqb, dq_bar, (size_t)nv * B.db.n * sizeof(double),
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  BlockRes &B = ctx->blk[0];
+  if (int r = adjoint_alloc(ctx, B)) return r;
+  const size_t bytes = (size_t)ctx->nv * B.db.n * sizeof(double);
+  CK(cudaMemcpyAsync(B.adj_work, lam_out, bytes,
                      ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
-  DevAdj A;
-  A.cv = B.adj;
-  A.p = A.cv + nv * P;
-  A.c = A.p + P;
-  A.rho = A.c + P;
-  A.vel = A.rho + P;
-  A.T = A.vel + 3 * P;
-  A.Y = A.T + P;
-  A.mu = A.Y + ns * P;
-  A.lam = A.mu + P;
-  A.rhod = A.lam + P;
-  const DevState in = state_of(B, 0);
-  if (ns == kFixedNS) launch_adjoint_t<kFixedNS>(ctx, B, in, mask, A);
-  else launch_adjoint_t<0>(ctx, B, in, mask, A);
-  for (auto it = ctx->order.rbegin(); it != ctx->order.rend(); ++it) {
-    if (it->first != block) continue;
-    const DevFace &f = B.faces[it->second];
-    const int t0 = f.face == 0 ? 1 : 0, t1 = f.face == 2 ? 1 : 2;
-    const long long nn = (long long)(f.re[t0] - f.rs[t0] + 1) * (f.re[t1] - f.rs[t1] + 1);
-    k_adj_bc_face<<<grid_for(ctx, nn, 128), 128, 0, ctx->stream>>>(B.db, A.cv, nv, f);
-  }
-  k_adj_gather<<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, A.cv, nv, B.dq);
-  CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(cv_bar, B.dq, (size_t)nv * B.db.n * sizeof(double),
+  CK(cudaMemsetAsync(B.adj_work + 4 * (size_t)ctx->nv * B.db.n, 0, B.db.n * sizeof(double), ctx->stream));
+  if (!ctx->der.fixed_time_step) enqueue_mix_dt(ctx);
+  if (int r = step_vjp(ctx)) return r;
+  if (int r = adjoint_t_to_cv(ctx)) return r;
+  CK(cudaMemcpyAsync(lam_in, B.adj_work, bytes,
                      ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  return OSTC_OK;
+}
+
+int ostc_adjoint_steps(ostc_ctx *ctx, int n_steps, int every, const double *lam_final, double *lam_initial,
+                       int ptr_kind) {
+  if (!ctx || !lam_final || !lam_initial || n_steps < 1 || every < 1) return OSTC_EINVAL;
+  if (int r = adjoint_check(ctx, OSTC_TERM_ALL)) return r;
+  if (ctx->precision != OSTC_PREC_FP64) {
+    ctx->err = "the step adjoint is that of the FP64 step: set OSTC_PREC_FP64";
+    return OSTC_EINVAL;
+  }
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  BlockRes &B = ctx->blk[0];
+  if (int r = adjoint_alloc(ctx, B)) return r;
+  const int nv = ctx->nv, ns = ctx->der.n_spec;
+  const long long P = B.db.plane;
+  const size_t state_doubles = (size_t)(nv + 6 + ns) * P;
+  const int ncp = (n_steps + every - 1) / every;
+  // device checkpoints (every `every` steps), one segment of step-start states, the final state
+  double *cps = nullptr, *seg = nullptr, *fin = nullptr;
+  auto release = [&]() {
+    cudaFree(cps);
+    cudaFree(seg);
+    cudaFree(fin);
+  };
+  if (cudaMalloc(&cps, (size_t)ncp * state_doubles * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&seg, (size_t)every * state_doubles * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&fin, state_doubles * sizeof(double)) != cudaSuccess) {
+    release();
+    ctx->err = "ostc_adjoint_steps: device memory for the checkpoints";
+    return OSTC_ECUDA;
+  }
+  auto save = [&](double *dst) {
+    cudaMemcpyAsync(dst, B.cv[0], (size_t)nv * P * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+    cudaMemcpyAsync(dst + (size_t)nv * P, B.bv[0], 6 * P * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+    cudaMemcpyAsync(dst + (size_t)(nv + 6) * P, B.sv[0], (size_t)ns * P * sizeof(double), cudaMemcpyDeviceToDevice,
+                    ctx->stream);
+  };
+  auto restore = [&](const double *src) {
+    cudaMemcpyAsync(B.cv[0], src, (size_t)nv * P * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+    cudaMemcpyAsync(B.bv[0], src + (size_t)nv * P, 6 * P * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+    cudaMemcpyAsync(B.sv[0], src + (size_t)(nv + 6) * P, (size_t)ns * P * sizeof(double), cudaMemcpyDeviceToDevice,
+                    ctx->stream);
+    launch_mix_props(ctx, B, state_of(B, 0));
+  };
+  // forward sweep: checkpoints and the dt of every step
+  std::vector<double> dts(n_steps);
+  for (int n = 0; n < n_steps; ++n) {
+    if (n % every == 0) save(cps + (size_t)(n / every) * state_doubles);
+    if (!ctx->der.fixed_time_step) enqueue_mix_dt(ctx);
+    for (int rk = 0; rk < 3; ++rk) enqueue_mix_stage(ctx, rk);
+    k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->d_time, ctx->d_dt, ctx->d_step);
+    if (cudaMemcpyAsync(&dts[n], ctx->d_dt, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+      release();
+      ctx->err = "ostc_adjoint_steps: forward sweep failed";
+      return OSTC_ECUDA;
+    }
+  }
+  save(fin);
+  // reverse sweep, one segment at a time: recompute the segment's step-start states from its
+  // checkpoint, then run the step adjoints backwards through them
+  const size_t bytes = (size_t)nv * B.db.n * sizeof(double);
+  cudaMemcpyAsync(B.adj_work, lam_final, bytes, ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                  ctx->stream);
+  cudaMemsetAsync(B.adj_work + 4 * (size_t)nv * B.db.n, 0, B.db.n * sizeof(double), ctx->stream);
+  int rc = OSTC_OK;
+  for (int sgi = ncp - 1; sgi >= 0 && rc == OSTC_OK; --sgi) {
+    const int a = sgi * every, b = std::min(a + every, n_steps);
+    restore(cps + (size_t)sgi * state_doubles);
+    for (int n = a; n < b; ++n) {
+      save(seg + (size_t)(n - a) * state_doubles);
+      if (n + 1 < b) {
+        cudaMemcpyAsync(ctx->d_dt, &dts[n], sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+        for (int rk = 0; rk < 3; ++rk) enqueue_mix_stage(ctx, rk);
+      }
+    }
+    for (int n = b - 1; n >= a && rc == OSTC_OK; --n) {
+      restore(seg + (size_t)(n - a) * state_doubles);
+      cudaMemcpyAsync(ctx->d_dt, &dts[n], sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+      rc = step_vjp(ctx);
+    }
+  }
+  // the first checkpoint is the caller's state, whose T is the equation-of-state root of its cv
+  if (rc == OSTC_OK) {
+    restore(cps);
+    rc = adjoint_t_to_cv(ctx);
+  }
+  restore(fin);
+  cudaMemcpyAsync(ctx->d_dt, &dts[n_steps - 1], sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+  if (rc == OSTC_OK)
+    cudaMemcpyAsync(lam_initial, B.adj_work, bytes,
+                    ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream);
+  const bool ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(ctx->stream) == cudaSuccess;
+  release();
+  if (rc != OSTC_OK) return rc;
+  if (!ok) {
+    ctx->err = "ostc_adjoint_steps: CUDA error";
+    return OSTC_ECUDA;
+  }
   return OSTC_OK;
 }
 

@@ -26,7 +26,7 @@ EXPORTS = [
     "ostc_physical_time", "ostc_store_residual_reference", "ostc_residual", "ostc_error_flags",
     "ostc_device_view", "ostc_profile_steps", "ostc_total_nodes", "ostc_probe_case", "ostc_timed_steps",
     "ostc_step_kernel_count", "ostc_residual_noalloc", "ostc_set_chem_mode", "ostc_set_conservative",
-    "ostc_rhs_vjp",
+    "ostc_rhs_vjp", "ostc_rk3_step_vjp", "ostc_adjoint_steps",
 ]
 
 
@@ -71,6 +71,8 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.ostc_rhs.argtypes = [vp, ip, ctypes.c_uint, vp, ip]
     lib.ostc_set_conservative.argtypes = [vp, ip, vp, ip]
     lib.ostc_rhs_vjp.argtypes = [vp, ip, ctypes.c_uint, vp, vp, ip]
+    lib.ostc_rk3_step_vjp.argtypes = [vp, vp, vp, ip]
+    lib.ostc_adjoint_steps.argtypes = [vp, ip, ip, vp, vp, ip]
     lib.ostc_rk3_step.argtypes = [vp, ip, dp]
     lib.ostc_physical_time.argtypes = [vp, dp]
     lib.ostc_store_residual_reference.argtypes = [vp]
@@ -210,6 +212,20 @@ class Solver:
         cv_bar = np.empty((self.n_var,) + self.shape(block))
         self._check(self.lib.ostc_rhs_vjp(self.h, block, mask, _ptr(dq_bar), _ptr(cv_bar), OSTC_HOST))
         return cv_bar
+
+    def step_vjp(self, lam_out: np.ndarray) -> np.ndarray:
+        """(d q' / d q)^T lam_out for one RK3 step from the current state (dt held fixed)."""
+        lam_out = np.ascontiguousarray(lam_out, dtype=np.float64)
+        lam_in = np.empty_like(lam_out)
+        self._check(self.lib.ostc_rk3_step_vjp(self.h, _ptr(lam_out), _ptr(lam_in), OSTC_HOST))
+        return lam_in
+
+    def adjoint_steps(self, n_steps: int, lam_final: np.ndarray, every: int = 20) -> np.ndarray:
+        """Advance n_steps and return (d q_N / d q_0)^T lam_final (checkpoint every `every` steps)."""
+        lam_final = np.ascontiguousarray(lam_final, dtype=np.float64)
+        lam0 = np.empty_like(lam_final)
+        self._check(self.lib.ostc_adjoint_steps(self.h, n_steps, every, _ptr(lam_final), _ptr(lam0), OSTC_HOST))
+        return lam0
 
     def step(self, n: int = 1) -> float:
         dt = ctypes.c_double()

@@ -78,8 +78,8 @@ class Case:
             "bool steady = 0",
             "int temporal_scheme = 3",
             f"real cfl = {s['cfl']!r}",
-            "bool fixed_time_step = 0",
-            "real dt = 1e-8",
+            f"bool fixed_time_step = {int(bool(s.get('fixed_time_step', 0)))}",
+            f"real dt = {s.get('dt', 1e-8)!r}",
             f"int reconstruction = {s['reconstruction']}",
             f"int inviscid_scheme = {s['inviscid_scheme']}",
             f"int viscous_order = {s['viscous_order']}",

@@ -161,3 +161,80 @@ def test_vjp_rejects_uncovered_cases(built, tmp_path):
     s2.set_chem_mode(ostc.CHEM_POINT_IMPLICIT)
     with pytest.raises(ostc.OstcError, match="point-implicit"):
         s2.rhs_vjp(np.zeros_like(cv0))
+
+
+def _fixed_dt_solver(tmp_path, dims, steps_dt_from=None):
+    """Noisy reacting layer with a fixed dt (the CFL dt of its initial state): finite differences of
+    whole steps then see the same dt the adjoint holds fixed."""
+    import ostc
+
+    mx, my, mz = dims
+    case = _noisy(oc.reacting_mixing_layer_3d(mx=mx, my=my, mz=mz))
+    d = oc.write_case(case, tmp_path / "cfl")
+    s = ostc.Solver(str(d))
+    s.set_state(case.bv, sv=case.sv)
+    dt = s.step(1)
+    s.close()
+    case.scheme["fixed_time_step"] = 1
+    case.scheme["dt"] = dt
+    d = oc.write_case(case, tmp_path / "fixed")
+    s = ostc.Solver(str(d))
+    s.set_state(case.bv, sv=case.sv)
+    cv0, _ = s.get_state()
+    return s, cv0, case
+
+
+def _fd_steps(s, case, cv0, v, n):
+    """Richardson-extrapolated central difference of q_n(q_0) along v.  Every perturbed start is set
+    from the exact base state (set_state), so that its temperature Newton iteration starts from the
+    base T and ends O(eps^2) from the root."""
+    d = []
+    for h in (2 * EPS, EPS):
+        out = []
+        for sg in (1, -1):
+            s.set_state(case.bv, sv=case.sv)
+            s.set_conservative(cv0 + sg * h * v)
+            s.step(n)
+            out.append(s.get_state()[0])
+        d.append((out[0] - out[1]) / (2 * h))
+    s.set_state(case.bv, sv=case.sv)
+    return (4 * d[1] - d[0]) / 3
+
+
+@pytest.mark.parametrize("dims", [(24, 18, 12), (40, 24, 1)], ids=["3d", "2d"])
+def test_step_vjp_matches_finite_differences(built, tmp_path, dims):
+    """Adjoint of one SSP-RK3 step (dt fixed) against differences of whole steps."""
+    s, cv0, case = _fixed_dt_solver(tmp_path, dims)
+    rng = np.random.default_rng(21)
+    w = rng.standard_normal(cv0.shape)
+    g = s.step_vjp(w)
+    cv_after, _ = s.get_state()
+    assert np.array_equal(cv_after, cv0)  # the state is left as it was
+    for v in _directions(cv0, rng, 3):
+        jv = _fd_steps(s, case, cv0, v, 1)
+        lhs, rhs = float(np.sum(w * jv)), float(np.sum(g * v))
+        assert abs(lhs - rhs) <= RTOL * abs(lhs) + ATOL * float(np.sum(np.abs(w * jv))), (lhs, rhs)
+
+
+def test_checkpointed_trajectory_adjoint(built, tmp_path):
+    """ostc_adjoint_steps over 7 steps with a checkpoint every 3 (segments of 3, 3, 1 steps): the
+    gradient of <w, q_7> w.r.t. q_0 against differences of 7-step runs, and the context ends at q_7."""
+    s, cv0, case = _fixed_dt_solver(tmp_path, (24, 18, 12))
+    rng = np.random.default_rng(22)
+    w = rng.standard_normal(cv0.shape)
+    lam0 = s.adjoint_steps(7, w, every=3)
+    q7, _ = s.get_state()
+    t7 = s.time()
+    s.set_state(case.bv, sv=case.sv)
+    s.step(7)
+    q7_ref, _ = s.get_state()
+    assert np.array_equal(q7, q7_ref)
+    assert t7 == s.time()
+    for v in _directions(cv0, rng, 2):
+        jv = _fd_steps(s, case, cv0, v, 7)
+        lhs, rhs = float(np.sum(w * jv)), float(np.sum(lam0 * v))
+        assert abs(lhs - rhs) <= RTOL * abs(lhs) + ATOL * float(np.sum(np.abs(w * jv))), (lhs, rhs)
+    # the checkpoint spacing does not change the result
+    s.set_state(case.bv, sv=case.sv)
+    lam1 = s.adjoint_steps(7, w, every=7)
+    assert np.max(np.abs(lam1 - lam0)) <= 1e-10 * np.max(np.abs(lam0))
