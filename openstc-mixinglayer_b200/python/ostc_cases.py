@@ -57,6 +57,8 @@ class Case:
     sv: np.ndarray | None = None
     mixture: dict | None = None
     freestream: dict | None = None
+    # generator parameters a harness may need afterwards (e.g. the velocity difference du)
+    extra: dict | None = None
 
     @property
     def nodes(self) -> int:
@@ -539,7 +541,53 @@ def reacting_mixing_layer_3d(mx=384, my=192, mz=96, seed=0, steps=100, h=0.125, 
                    therm="therm.dat", tran="tran.dat")
     freestream = dict(mach=0.5, pressure=p0, temperature=to, Y=dict(oxidiser))
     return Case("reacting_mixing_layer_3d", mx, my, mz, X, Y, Z, delta0, faces, structs, scheme, bv, steps,
-                sv=sv, mixture=mixture, freestream=freestream)
+                sv=sv, mixture=mixture, freestream=freestream, extra=dict(du=du, h=h))
+
+
+# ---- sensitivity of the momentum thickness to inflow mode amplitudes (adjoint harness)
+
+def mode_shapes(case: Case, n_modes: int = 8, seed: int = 0, amp: float = 1e-3) -> np.ndarray:
+    """v' shapes phi_m = amp du cos(2 pi m x / Lx + phase_m) exp(-y^2) (x, y in grid units, Lx the
+    periodic length (mx - 1) h, the layer's own envelope), phases U[0, 2 pi) from the seed: the
+    perturbation sum_m a_m phi_m added to v.  Returns [n_modes, mz, my, mx]."""
+    rng = np.random.default_rng(seed)
+    phases = rng.uniform(0.0, 2 * np.pi, n_modes)
+    lx = (case.mx - 1) * case.extra["h"]
+    env = np.exp(-case.y ** 2)
+    return np.stack([amp * case.extra["du"] * np.cos(2 * np.pi * (m + 1) * case.x / lx + phases[m]) * env
+                     for m in range(n_modes)])
+
+
+def add_modes(case: Case, a, shapes: np.ndarray) -> Case:
+    """A copy of the case with v += sum_m a_m shapes[m]."""
+    c = dataclasses.replace(case, bv=case.bv.copy(), sv=None if case.sv is None else case.sv.copy())
+    c.bv[2] = c.bv[2] + np.tensordot(np.asarray(a, dtype=float), shapes, axes=1)
+    return c
+
+
+def dcv_dmodes(cv: np.ndarray, shapes: np.ndarray) -> np.ndarray:
+    """d cv / d a_m at the state cv (v enters rho v and rho E = ... + rho |V|^2 / 2):
+    [n_modes, n_var, mz, my, mx]."""
+    rho, v = cv[0], cv[2] / cv[0]
+    out = np.zeros((shapes.shape[0],) + cv.shape)
+    out[:, 2] = rho * shapes
+    out[:, 4] = rho * v * shapes
+    return out
+
+
+def momentum_thickness(cv: np.ndarray, du: float, rho0: float, dy: float):
+    """theta = 1 / (rho0 du^2) sum_y <rho> (du/2 - u~)(du/2 + u~) dy, <.> the (x, z) average and
+    u~ = <rho u> / <rho> the Favre average; returns theta and d theta / d cv (zero but in rho, rho u)."""
+    rm = cv[0].mean(axis=(0, 2))
+    ru = cv[1].mean(axis=(0, 2))
+    ut = ru / rm
+    c = dy / (rho0 * du * du)
+    theta = float(c * np.sum(0.25 * du * du * rm - ru * ut))
+    nxz = cv.shape[1] * cv.shape[3]
+    g = np.zeros_like(cv)
+    g[0] = (c * (0.25 * du * du + ut * ut) / nxz)[None, :, None]
+    g[1] = (c * (-2.0 * ut) / nxz)[None, :, None]
+    return theta, g
 
 
 def relative_errors(a: np.ndarray, b: np.ndarray, momentum_group: bool = True):

@@ -238,3 +238,54 @@ def test_checkpointed_trajectory_adjoint(built, tmp_path):
     s.set_state(case.bv, sv=case.sv)
     lam1 = s.adjoint_steps(7, w, every=7)
     assert np.max(np.abs(lam1 - lam0)) <= 1e-10 * np.max(np.abs(lam0))
+
+
+def test_momentum_thickness_gradient_wrt_mode_amplitudes(built, tmp_path):
+    """The sensitivity problem of the adjoint: d theta(q_N) / d a_m for the momentum thickness after
+    N = 10 steps and the amplitudes a_m of 8 seeded v' modes (a_m = 1/8 at the base), by one
+    checkpointed trajectory adjoint (every 4 steps), against Richardson differences of 10-step runs
+    in each a_m.  Noisy reacting layer (T, p, Y), fixed dt.
+
+    theta moves by only ~1e-11 per 1e-5 of an amplitude, and the 10-step runs are piecewise smooth
+    in a_m at that scale (a stage's temperature Newton iteration count, the |U| kink of the split
+    fluxes), so these difference quotients scatter by ~1e-5 of the gradient whatever the step; the
+    tolerance here is 1e-4 of the largest component.  The 1e-6 pin of the trajectory adjoint is
+    test_checkpointed_trajectory_adjoint."""
+    import ostc
+
+    base = _noisy(oc.reacting_mixing_layer_3d(mx=24, my=18, mz=12))
+    shapes = oc.mode_shapes(base)
+    a0 = np.full(8, 1.0 / 8)
+    c0 = oc.add_modes(base, a0, shapes)
+    d = oc.write_case(c0, tmp_path / "cfl")
+    s = ostc.Solver(str(d))
+    s.set_state(c0.bv, sv=c0.sv)
+    dt = s.step(1)
+    s.close()
+    c0.scheme["fixed_time_step"], c0.scheme["dt"] = 1, dt
+    d = oc.write_case(c0, tmp_path / "fixed")
+    s = ostc.Solver(str(d))
+    n, du, dy = 10, c0.extra["du"], c0.extra["h"]
+    s.set_state(c0.bv, sv=c0.sv)
+    cv0, _ = s.get_state()
+    rho0 = float(cv0[0].mean())
+
+    def theta(a):
+        c = oc.add_modes(base, a, shapes)
+        s.set_state(c.bv, sv=c.sv)
+        s.step(n)
+        return oc.momentum_thickness(s.get_state()[0], du, rho0, dy)
+
+    _, g_n = theta(a0)
+    s.set_state(c0.bv, sv=c0.sv)
+    lam0 = s.adjoint_steps(n, g_n, every=4)
+    grad_ad = np.array([np.sum(lam0 * dm) for dm in oc.dcv_dmodes(cv0, shapes)])
+    h = 1e-5
+    grad_fd = np.empty(8)
+    for m in range(8):
+        e = np.zeros(8)
+        e[m] = 1.0
+        d1 = (theta(a0 + h * e)[0] - theta(a0 - h * e)[0]) / (2 * h)
+        d2 = (theta(a0 + 2 * h * e)[0] - theta(a0 - 2 * h * e)[0]) / (4 * h)
+        grad_fd[m] = (4 * d1 - d2) / 3
+    assert np.max(np.abs(grad_ad - grad_fd)) <= 1e-4 * np.max(np.abs(grad_fd)), (grad_ad, grad_fd)
