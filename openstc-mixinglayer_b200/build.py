@@ -9,7 +9,6 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 SOURCES = ["csrc/host.cpp", "csrc/chem.cpp", "csrc/ostc_air.cu", "csrc/ostc_noalloc.cu"]
-HEADERS = ["csrc/host.h", "csrc/air_math.cuh"]
 OUT = PKG / "libostc_b200.so"
 
 
@@ -24,7 +23,8 @@ def needs_build() -> bool:
     if not OUT.exists():
         return True
     t = OUT.stat().st_mtime
-    deps = [PKG / s for s in SOURCES + HEADERS] + [ROOT / "include" / "ostc.h"]
+    headers = sorted((PKG / "csrc").glob("*.h")) + sorted((PKG / "csrc").glob("*.cuh"))
+    deps = [PKG / s for s in SOURCES] + headers + [ROOT / "include" / "ostc.h"]
     return any(d.stat().st_mtime > t for d in deps)
 
 

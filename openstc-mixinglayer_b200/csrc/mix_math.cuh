@@ -201,6 +201,53 @@ __device__ __forceinline__ T ipow(T x, int n) {
   }
 }
 
+// Forward and backward rate constants of reaction r (forward_reaction_rate, backward_reaction_rate,
+// FiniteRateChem.cu:60-150) at T (with ln T, 1/T), third-body concentration sum cc and, where the
+// equilibrium constant is used, g = g_k / (Ru T) of every species.  Irreversible: kb = 0; the
+// equilibrium constant for every other type but 2 when any reaction needs it (it also overwrites
+// REV coefficients); else the REV Arrhenius coefficients (times the third-body sum for type 4).
+template <int NS, typename T>
+__device__ __forceinline__ void reaction_rates(int r, T t, T lt, T ti, T cc, const T *g, T &kf_out, T &kb_out) {
+  const int ns = OSTC_NS;
+  const int ty = c_mix.label[r];
+  T kf = arrhenius(lt, ti, c_mix.A[r], c_mix.b[r], c_mix.Ea[r]);
+  if (ty == 3) {
+    kf += arrhenius(lt, ti, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
+  } else if (ty == 4) {
+    kf *= cc;
+  } else if (ty > 4) {
+    const T klow = arrhenius(lt, ti, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
+    const T pr = klow * cc / kf;
+    T F = 1.0;
+    if (ty > 5) {
+      T fc = (1 - c_mix.troe_alpha[r]) * exp(-t / c_mix.troe_t3[r]) +
+                  c_mix.troe_alpha[r] * exp(-t / c_mix.troe_t1[r]);
+      if (ty == 7) fc += exp(-c_mix.troe_t2[r] / t);
+      const T lfc = log10(fc);
+      const T cq = -0.4 - 0.67 * lfc, nq = 0.75 - 1.27 * lfc;
+      const T lpr = log10(pr);
+      const T tmp = (lpr + cq) / (nq - 0.14 * (lpr + cq));
+      F = pow(10.0, lfc / (1.0 + tmp * tmp));
+    }
+    kf = kf * pr / (1.0 + pr) * F;
+  }
+  T kb = 0;
+  if (ty == 0) {
+    kb = 0;
+  } else if (ty != 2 && c_mix.use_gibbs) {
+    T dg = 0;
+    for (int l = 0; l < ns; ++l) dg += g[l] * (c_mix.stoi_b[r][l] - c_mix.stoi_f[r][l]);
+    const T temp_t = kPatmD / kRuD * 1e-3 / t;
+    const T kc = ipow(temp_t, c_mix.order[r]) * exp(-dg);
+    kb = kf / kc;
+  } else if (c_mix.rev_type[r] == 1) {
+    kb = arrhenius(lt, ti, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
+    if (ty == 4) kb *= cc;
+  }
+  kf_out = kf;
+  kb_out = kb;
+}
+
 // finite_rate_chemistry (FiniteRateChem.cu:7-58, rates :60-195): omega_k in kg/(m^3 s) at one node.
 // With jac non-null also the chemical source Jacobian of compute_chem_src_jacobian
 // (FiniteRateChem.cu:197-217), [ns][ns] row-major, in 1/s.
@@ -211,7 +258,7 @@ __device__ __forceinline__ void mix_chemistry(T rho, T t, const T *y, T *omega, 
   T c[Spec<NS>::A];
   for (int l = 0; l < ns; ++l) c[l] = rho * y[l] * c_mix.imw[l] * 1e-3;
   T g[Spec<NS>::A];
-  bool gibbs = false;
+  if (c_mix.use_gibbs) mix_gibbs_rt<NS, T>(t, g);
   for (int l = 0; l < ns; ++l) omega[l] = 0;
   T cre[Spec<NS>::A], des[Spec<NS>::A];
   for (int l = 0; l < ns; ++l) cre[l] = des[l] = 0;
@@ -220,47 +267,8 @@ __device__ __forceinline__ void mix_chemistry(T rho, T t, const T *y, T *omega, 
     T cc = 0;
     if (ty >= 4)
       for (int l = 0; l < ns; ++l) cc += c[l] * c_mix.third_body[r][l];
-    T kf = arrhenius(lt, ti, c_mix.A[r], c_mix.b[r], c_mix.Ea[r]);
-    if (ty == 3) {
-      kf += arrhenius(lt, ti, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
-    } else if (ty == 4) {
-      kf *= cc;
-    } else if (ty > 4) {
-      const T klow = arrhenius(lt, ti, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
-      const T pr = klow * cc / kf;
-      T F = 1.0;
-      if (ty > 5) {
-        T fc = (1 - c_mix.troe_alpha[r]) * exp(-t / c_mix.troe_t3[r]) +
-                    c_mix.troe_alpha[r] * exp(-t / c_mix.troe_t1[r]);
-        if (ty == 7) fc += exp(-c_mix.troe_t2[r] / t);
-        const T lfc = log10(fc);
-        const T cq = -0.4 - 0.67 * lfc, nq = 0.75 - 1.27 * lfc;
-        const T lpr = log10(pr);
-        const T tmp = (lpr + cq) / (nq - 0.14 * (lpr + cq));
-        F = pow(10.0, lfc / (1.0 + tmp * tmp));
-      }
-      kf = kf * pr / (1.0 + pr) * F;
-    }
-    // backward_reaction_rate (FiniteRateChem.cu:108-150): irreversible 0; the equilibrium constant
-    // for every other type but 2 when any reaction needs it (it also overwrites REV coefficients);
-    // else the REV Arrhenius coefficients (times the third-body sum for type 4)
-    T kb = 0;
-    if (ty == 0) {
-      kb = 0;
-    } else if (ty != 2 && c_mix.use_gibbs) {
-      if (!gibbs) {
-        mix_gibbs_rt<NS, T>(t, g);
-        gibbs = true;
-      }
-      T dg = 0;
-      for (int l = 0; l < ns; ++l) dg += g[l] * (c_mix.stoi_b[r][l] - c_mix.stoi_f[r][l]);
-      const T temp_t = kPatmD / kRuD * 1e-3 / t;
-      const T kc = ipow(temp_t, c_mix.order[r]) * exp(-dg);
-      kb = kf / kc;
-    } else if (c_mix.rev_type[r] == 1) {
-      kb = arrhenius(lt, ti, c_mix.A2[r], c_mix.b2[r], c_mix.Ea2[r]);
-      if (ty == 4) kb *= cc;
-    }
+    T kf, kb;
+    reaction_rates<NS, T>(r, t, lt, ti, cc, g, kf, kb);
     // concentration products: integer powers as products (pow(c, 1) = c, pow(c, 2) = c*c to within
     // the rounding of pow itself), pow only for higher orders
     T q1 = 1.0, q2 = ty != 0 ? 1.0 : 0.0;

@@ -818,68 +818,258 @@ __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_adj_vi
   mix_visc_face_bwd<DIM3, NS>(b, s, p0, DIR, afv, A);
 }
 
-// Reverse of the chemical source dq[5+l] += J omega_l(rho, T, Y) (compute_source<FR>): one Dual
-// evaluation of the chemistry per input (rho, T, Y_0..Y_ns-1), each giving that input's adjoint.
+// Reverse of the chemical source dq[5+l] += J omega_l(rho, T, Y) (compute_source<FR>,
+// SourceTerm.cuh:11-35; finite_rate_chemistry, FiniteRateChem.cu:7-195), interior nodes.
+// omega_l = 1e3 W_l sum_r (nu_b - nu_f)_rl (q1_r - q2_r), q1 = kf prod c^nu_f, q2 = kb prod c^nu_b,
+// c_l = rho Y_l / W_l 1e-3: per reaction the adjoint of q1 - q2 goes to kf, kb and the
+// concentrations; kf, kb are differentiated in T (and in the third-body sum) by Dual evaluations of
+// the same rate-constant code.
 template <int NS>
 __global__ void __launch_bounds__(128) k_adj_source(DevBlock b, DevState s, const double *__restrict__ dqb, DevAdj A) {
   const long long P = b.plane;
-  const int ns = OSTC_NS;
+  const int ns = OSTC_NS, nr = c_mix.nr;
+  constexpr int SA = Spec<NS>::A;
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(n % b.mx);
-    const long long r = n / b.mx;
-    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const long long r0 = n / b.mx;
+    const int j = (int)(r0 % b.my), k = (int)(r0 / b.my);
     const long long p = b.id(i, j, k);
-    double aw[Spec<NS>::A];
+    double aw[SA];
     bool any = false;
     for (int l = 0; l < ns; ++l) {
-      aw[l] = b.jac[p] * dqb[(5 + l) * b.n + n];
+      aw[l] = b.jac[p] * dqb[(5 + l) * b.n + n] * c_mix.mw[l] * 1e+3;
       any = any || aw[l] != 0.0;
     }
     if (!any) continue;
     const double rho = s.bv[p], t = s.bv[5 * P + p];
-    for (int in = 0; in < ns + 2; ++in) {
-      Dual y[Spec<NS>::A], om[Spec<NS>::A];
-      for (int l = 0; l < ns; ++l) y[l] = Dual(s.sv[l * P + p], in == 2 + l ? 1.0 : 0.0);
-      mix_chemistry<NS, Dual>(Dual(rho, in == 0 ? 1.0 : 0.0), Dual(t, in == 1 ? 1.0 : 0.0), y, om);
-      double g = 0;
-      for (int l = 0; l < ns; ++l) g += aw[l] * om[l].d;
-      if (in == 0) A.rho[p] += g;
-      else if (in == 1) A.T[p] += g;
-      else A.Y[(long long)(in - 2) * P + p] += g;
+    double y[SA], c[SA], ac[SA];
+    for (int l = 0; l < ns; ++l) {
+      y[l] = s.sv[l * P + p];
+      c[l] = rho * y[l] * c_mix.imw[l] * 1e-3;
+      ac[l] = 0.0;
     }
+    const double lt = log(t), ti = 1.0 / t;
+    const Dual tT(t, 1.0), ltT = log(tT), tiT = 1.0 / tT;
+    Dual gT[SA], gC[SA];
+    if (c_mix.use_gibbs) {
+      mix_gibbs_rt<NS, Dual>(tT, gT);
+      for (int l = 0; l < ns; ++l) gC[l] = Dual(gT[l].v, 0.0);
+    }
+    double aT = 0;
+    for (int r = 0; r < nr; ++r) {
+      double aq = 0;
+      for (int l = 0; l < ns; ++l) aq += aw[l] * (c_mix.stoi_b[r][l] - c_mix.stoi_f[r][l]);
+      if (aq == 0.0) continue;
+      const int ty = c_mix.label[r];
+      double cc = 0;
+      if (ty >= 4)
+        for (int l = 0; l < ns; ++l) cc += c[l] * c_mix.third_body[r][l];
+      Dual kf, kb;
+      reaction_rates<NS, Dual>(r, tT, ltT, tiT, Dual(cc), gT, kf, kb);
+      double dkf_dcc = 0, dkb_dcc = 0;
+      if (ty >= 4) {
+        Dual kfc, kbc;
+        reaction_rates<NS, Dual>(r, Dual(t), Dual(lt), Dual(ti), Dual(cc, 1.0), gC, kfc, kbc);
+        dkf_dcc = kfc.d;
+        dkb_dcc = kbc.d;
+      }
+      // concentration products as the forward forms them, and their partial derivatives
+      auto fpow = [](double x, int nu) { return nu == 1 ? x : (nu == 2 ? x * x : pow(x, (double)nu)); };
+      auto dpow = [](double x, int nu) { return nu == 1 ? 1.0 : (nu == 2 ? 2 * x : nu * pow(x, (double)(nu - 1))); };
+      double p1 = 1.0, p2 = 1.0;
+      for (int l = 0; l < ns; ++l) {
+        if (c_mix.stoi_f[r][l]) p1 *= fpow(c[l], c_mix.stoi_f[r][l]);
+        if (c_mix.stoi_b[r][l]) p2 *= fpow(c[l], c_mix.stoi_b[r][l]);
+      }
+      const double akf = aq * p1, akb = ty != 0 ? -aq * p2 : 0.0;
+      aT += akf * kf.d + akb * kb.d;
+      if (ty >= 4) {
+        const double acc = akf * dkf_dcc + akb * dkb_dcc;
+        for (int l = 0; l < ns; ++l) ac[l] += acc * c_mix.third_body[r][l];
+      }
+      for (int l = 0; l < ns; ++l) {
+        const int nf = c_mix.stoi_f[r][l], nb = ty != 0 ? c_mix.stoi_b[r][l] : 0;
+        if (nf) {
+          double d = dpow(c[l], nf);
+          for (int m = 0; m < ns; ++m)
+            if (m != l && c_mix.stoi_f[r][m]) d *= fpow(c[m], c_mix.stoi_f[r][m]);
+          ac[l] += aq * kf.v * d;
+        }
+        if (nb) {
+          double d = dpow(c[l], nb);
+          for (int m = 0; m < ns; ++m)
+            if (m != l && c_mix.stoi_b[r][m]) d *= fpow(c[m], c_mix.stoi_b[r][m]);
+          ac[l] -= aq * kb.v * d;
+        }
+      }
+    }
+    double arho = 0;
+    for (int l = 0; l < ns; ++l) {
+      arho += ac[l] * y[l] * c_mix.imw[l] * 1e-3;
+      A.Y[(long long)l * P + p] += ac[l] * rho * c_mix.imw[l] * 1e-3;
+    }
+    A.rho[p] += arho;
+    A.T[p] += aT;
   }
 }
 
-// Reverse of the transport and acoustic properties (update_physical_properties<mixture>) at every
-// padded node: one Dual evaluation per input (rho, p, T, Y_0..Y_ns-1).
+// Reverse of the transport and acoustic properties (update_physical_properties<mixture>,
+// FieldOperation.cuh:107-134, compute_transport_property, Transport.cu:43-136) at every padded node:
+// adjoints of c, mu, lambda and rho*D_k -> adjoints of rho, p, T and Y.  Hand-written reverse of
+// mix_properties (one forward sweep keeping its intermediates, then the reverse sweep).
 template <int NS>
 __global__ void __launch_bounds__(128) k_adj_props(DevBlock b, DevState s, DevAdj A) {
   const long long P = b.plane;
   const int ns = OSTC_NS;
+  constexpr int SA = Spec<NS>::A;
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
     const double rho = s.bv[p];
     if (!(rho > 0)) continue;
     const double ac = A.c[p], amu = A.mu[p], alam = A.lam[p];
-    double ard[Spec<NS>::A];
+    double ard[SA];
     bool any = ac != 0.0 || amu != 0.0 || alam != 0.0;
     for (int l = 0; l < ns; ++l) {
       ard[l] = A.rhod[(long long)l * P + p];
       any = any || ard[l] != 0.0;
     }
     if (!any) continue;
-    for (int in = 0; in < ns + 3; ++in) {
-      Dual y[Spec<NS>::A], rd[Spec<NS>::A];
-      for (int l = 0; l < ns; ++l) y[l] = Dual(s.sv[l * P + p], in == 3 + l ? 1.0 : 0.0);
-      Dual g, a, mu, cd;
-      mix_properties<NS, Dual>(Dual(rho, in == 0 ? 1.0 : 0.0), Dual(s.bv[4 * P + p], in == 1 ? 1.0 : 0.0),
-                               Dual(s.bv[5 * P + p], in == 2 ? 1.0 : 0.0), y, g, a, mu, cd, rd);
-      double sum = ac * a.d + amu * mu.d + alam * cd.d;
-      for (int l = 0; l < ns; ++l) sum += ard[l] * rd[l].d;
-      if (in == 0) A.rho[p] += sum;
-      else if (in == 1) A.p[p] += sum;
-      else if (in == 2) A.T[p] += sum;
-      else A.Y[(long long)(in - 3) * P + p] += sum;
+    const double pr = s.bv[4 * P + p], t = s.bv[5 * P + p];
+    double y[SA], cp[SA], dcp[SA];
+    for (int l = 0; l < ns; ++l) y[l] = s.sv[l * P + p];
+    mix_h_cp<NS, double>(t, nullptr, cp);
+    mix_dcp_dt<NS>(t, dcp);
+    // ---- forward (as mix_properties)
+    double smw = 0, cpt = 0, cvt = 0;
+    for (int l = 0; l < ns; ++l) {
+      smw += y[l] * c_mix.imw[l];
+      cpt += y[l] * cp[l];
+      cvt += y[l] * (cp[l] - c_mix.ru_mw[l]);
     }
+    const double mw = 1 / smw;
+    const double gamma = cpt / cvt;
+    const double acoustic = sqrt(gamma * kRuD * t / mw);
+    double X[SA], vis[SA], dlvis[SA];  // dlvis = d ln(vis) / dT
+    const double st = sqrt(t);
+    for (int l = 0; l < ns; ++l) {
+      X[l] = y[l] * mw * c_mix.imw[l];
+      const double lj = c_mix.lj_potent_inv[l], tdl = t * lj;
+      const double a1 = pow(tdl, -0.145), a2 = pow(tdl + 0.5, -2.0);
+      const double ci = 1.147 * a1 + a2;
+      vis[l] = c_mix.vis_coeff[l] * st / ci;
+      const double dci = lj * (1.147 * -0.145 * a1 / tdl - 2.0 * a2 / (tdl + 0.5));
+      dlvis[l] = 0.5 / t - dci / ci;
+    }
+    double vt[SA], ct[SA];
+    for (int m = 0; m < ns; ++m) {
+      double v_ = 0;
+      for (int n = 0; n < ns; ++n) {
+        double pf = 1.0;
+        if (m != n) {
+          const double nm = 1 + sqrt(vis[m] / vis[n]) * c_mix.wj_div_wi_1_4[m][n];
+          pf = nm * nm * c_mix.sqrt_wiwj_8[m][n];
+        }
+        v_ += pf * X[n];
+      }
+      vt[m] = v_;
+      ct[m] = 1.065 * v_ - 0.065 * X[m];
+    }
+    const double t32p = t * st / pr;
+    const double eps = 1e-12;
+    double num[SA], den[SA];
+    for (int l = 0; l < ns; ++l) num[l] = den[l] = 0;
+    for (int l = 0; l < ns; ++l)
+      for (int n = l + 1; n < ns; ++n) {
+        const double tr = t * c_mix.kb_over_eps[l][n];
+        const double om = 1.0 / pow(tr, 0.145) + 1.0 / ((tr + 0.5) * (tr + 0.5));
+        const double dln = c_mix.binary_diff[l][n] * t32p / om;
+        num[l] += (X[n] + eps) * c_mix.mw[n];
+        den[l] += (X[n] + eps) / dln;
+        num[n] += (X[l] + eps) * c_mix.mw[l];
+        den[n] += (X[l] + eps) / dln;
+      }
+    // ---- reverse
+    double aX[SA], avis[SA], aY[SA], acp[SA], aden[SA], avt[SA];
+    for (int l = 0; l < ns; ++l) aX[l] = avis[l] = aY[l] = acp[l] = 0.0;
+    double arho = 0, aT = 0, ap = 0, amw = 0, at32p = 0;
+    // rho D_l = rho num_l / (den_l mw)
+    for (int l = 0; l < ns; ++l) {
+      const double rd = rho * num[l] / (den[l] * mw);
+      arho += ard[l] * rd / rho;
+      const double anum = ard[l] * rd / num[l];
+      aden[l] = -ard[l] * rd / den[l];
+      amw -= ard[l] * rd / mw;
+      for (int n = 0; n < ns; ++n)
+        if (n != l) aX[n] += anum * c_mix.mw[n];
+    }
+    for (int l = 0; l < ns; ++l)
+      for (int n = l + 1; n < ns; ++n) {
+        const double kbe = c_mix.kb_over_eps[l][n], tr = t * kbe;
+        const double a1 = pow(tr, 0.145), a2 = 1.0 / ((tr + 0.5) * (tr + 0.5));
+        const double om = 1.0 / a1 + a2;
+        const double bd = c_mix.binary_diff[l][n];
+        const double dln = bd * t32p / om;
+        const double idl = 1.0 / dln;
+        aX[n] += aden[l] * idl;
+        aX[l] += aden[n] * idl;
+        const double adln = -(aden[l] * (X[n] + eps) + aden[n] * (X[l] + eps)) * idl * idl;
+        at32p += adln * bd / om;
+        const double aom = -adln * dln / om;
+        // om = tr^-0.145 + (tr + 0.5)^-2
+        aT += aom * kbe * (-0.145 / (a1 * tr) - 2.0 * a2 / (tr + 0.5));
+      }
+    // t32p = T^1.5 / p
+    aT += at32p * 1.5 * t32p / t;
+    ap -= at32p * t32p / pr;
+    // lambda = sum lam_m X_m / ct_m, lam_m = vis_m (cp_m + 1.25 Ru / W_m); mu = sum vis_m X_m / vt_m
+    for (int m = 0; m < ns; ++m) {
+      const double lfac = cp[m] + 1.25 * c_mix.ru_mw[m];
+      const double lamm = vis[m] * lfac;
+      const double alm = alam * X[m] / ct[m];
+      aX[m] += alam * lamm / ct[m];
+      const double act = -alam * lamm * X[m] / (ct[m] * ct[m]);
+      avt[m] = 1.065 * act;
+      aX[m] -= 0.065 * act;
+      avis[m] += alm * lfac;
+      acp[m] += alm * vis[m];
+      avis[m] += amu * X[m] / vt[m];
+      aX[m] += amu * vis[m] / vt[m];
+      avt[m] -= amu * vis[m] * X[m] / (vt[m] * vt[m]);
+    }
+    // vt_m = sum_n pf_mn X_n, pf_mn = (1 + sqrt(vis_m / vis_n) w_mn)^2 s_mn
+    for (int m = 0; m < ns; ++m)
+      for (int n = 0; n < ns; ++n) {
+        if (m == n) {
+          aX[n] += avt[m];
+          continue;
+        }
+        const double r = sqrt(vis[m] / vis[n]), w = c_mix.wj_div_wi_1_4[m][n], sw = c_mix.sqrt_wiwj_8[m][n];
+        const double nm = 1 + r * w;
+        aX[n] += avt[m] * nm * nm * sw;
+        const double ar = avt[m] * X[n] * 2 * nm * sw * w;
+        avis[m] += ar * r / (2 * vis[m]);
+        avis[n] -= ar * r / (2 * vis[n]);
+      }
+    for (int l = 0; l < ns; ++l) aT += avis[l] * vis[l] * dlvis[l];
+    // c = sqrt(gamma Ru T / mw)
+    const double agamma = ac * acoustic / (2 * gamma);
+    aT += ac * acoustic / (2 * t);
+    amw -= ac * acoustic / (2 * mw);
+    // X_l = Y_l mw / W_l
+    for (int l = 0; l < ns; ++l) {
+      aY[l] += aX[l] * mw * c_mix.imw[l];
+      amw += aX[l] * y[l] * c_mix.imw[l];
+    }
+    // gamma = cpt / cvt; mw = 1 / sum Y / W; cp_l(T)
+    const double acpt = agamma / cvt, acvt = -agamma * gamma / cvt;
+    for (int l = 0; l < ns; ++l) {
+      aY[l] += acpt * cp[l] + acvt * (cp[l] - c_mix.ru_mw[l]) - amw * mw * mw * c_mix.imw[l];
+      acp[l] += (acpt + acvt) * y[l];
+      aT += acp[l] * dcp[l];
+    }
+    A.rho[p] += arho;
+    A.p[p] += ap;
+    A.T[p] += aT;
+    for (int l = 0; l < ns; ++l) A.Y[(long long)l * P + p] += aY[l];
   }
 }
 
