@@ -60,9 +60,11 @@ FALLBACK_HBM_GBS = 6650.0
 ALGO_BYTES_PER_NODE = {"flux_x": 152, "flux_y": 192, "flux_z": 192, "visc_update": 336, "cfl_dt": 120}
 # DRAM bytes per node measured by one ncu capture of the kernel (dram__bytes_read.sum +
 # dram__bytes_write.sum over the nodes of the launch, 256x128x64 case of the same workload; traffic
-# grows with the node count, so a full-size launch moves this figure times its nodes):
-# profiles/k_flux_march_fp64_awe7_256x128x64.md (y sweep) and profiles/k_flux_march_z_fp64_awe7_256x128x64.md.
-MEASURED_TRAFFIC_PER_NODE = {"flux_y": 209.8}
+# grows with the node count, so a full-size launch moves this figure times its nodes).  The y/z
+# sweeps have two designs picked by the library's autotuner; at 512x256x128 it keeps the column
+# march for y (profiles/k_flux_march_fp64_awe7_256x128x64.md) and the 32x4x4 tile for z
+# (profiles/k_flux_tile_fp64_awe7_256x128x64.md).
+MEASURED_TRAFFIC_PER_NODE = {"flux_y": 209.8, "flux_z": 203.3}
 # Whole fused stage (three state passes + metric): 8 (3 n_var + 10) bytes per cell-stage, n_var = 5
 STAGE_BYTES = 8 * (3 * 5 + 10)
 
