@@ -1218,6 +1218,11 @@ struct ostc_ctx {
   double init_bv[6]{};
   std::vector<double> init_sv;
   cudaStream_t stream = nullptr;
+  // multi-block cases: side streams on which the blocks' stage work runs concurrently (forked from
+  // and joined back into `stream`, inside the captured step graph as well)
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> side_ev;
+  cudaEvent_t fork_ev = nullptr;
   Setup setup;
   Derived der;
   HostMesh mesh;
@@ -1774,6 +1779,31 @@ int initialise(ostc_ctx *ctx) {
 }
 
 // One SSP-RK3 step over all blocks (RK.cuh:85-185).
+// Run f(b) for every block.  Multi-block steps fork the blocks onto the side streams (block b on
+// side[b % n]) and join them back before returning, so independent blocks' sweeps fill the GPU
+// together; with per-kernel timing on (ostc_profile_steps) the blocks run one after another.
+template <class F>
+void for_blocks(ostc_ctx *ctx, F f) {
+  const size_t nb = ctx->blk.size();
+  if (nb == 1 || ctx->timing || ctx->side.empty()) {
+    for (size_t b = 0; b < nb; ++b) f((int)b);
+    return;
+  }
+  cudaStream_t main = ctx->stream;
+  cudaEventRecord(ctx->fork_ev, main);
+  const size_t ns = ctx->side.size();
+  for (size_t k = 0; k < ns; ++k) cudaStreamWaitEvent(ctx->side[k], ctx->fork_ev, 0);
+  for (size_t b = 0; b < nb; ++b) {
+    ctx->stream = ctx->side[b % ns];
+    f((int)b);
+  }
+  ctx->stream = main;
+  for (size_t k = 0; k < ns; ++k) {
+    cudaEventRecord(ctx->side_ev[k], ctx->side[k]);
+    cudaStreamWaitEvent(main, ctx->side_ev[k], 0);
+  }
+}
+
 template <typename T>
 int enqueue_step(ostc_ctx *ctx) {
   static const double A[3] = {1.0, 0.75, 1.0 / 3.0}, Bc[3] = {0.0, 0.25, 2.0 / 3.0}, C[3] = {1.0, 0.25, 2.0 / 3.0};
@@ -1789,7 +1819,7 @@ int enqueue_step(ostc_ctx *ctx) {
       k_dt_decode<<<1, 1, 0, ctx->stream>>>(ctx->d_dtbits, ctx->d_dt);
       end_t(ctx, tok);
     }
-    for (size_t bi = 0; bi < ctx->blk.size(); ++bi) {
+    for_blocks(ctx, [&](int bi) {
       BlockRes &B = ctx->blk[bi];
       launch_flux<T>(ctx, B, state_of(B, sin));
       StageArgs a{};
@@ -1806,8 +1836,8 @@ int enqueue_step(ostc_ctx *ctx) {
       a.flags = ctx->d_flags;
       launch_visc<T>(ctx, B, a);
       launch_carry(ctx, B, state_of(B, sin), state_of(B, sout));
-      launch_bcs(ctx, (int)bi, state_of(B, sout));
-    }
+      launch_bcs(ctx, bi, state_of(B, sout));
+    });
     launch_interfaces(ctx, sout);
   }
   k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->d_time, ctx->d_dt, ctx->d_step);
@@ -1831,7 +1861,7 @@ void enqueue_mix_stage(ostc_ctx *ctx, int rk, int sout_override = -1) {
   static const double A[3] = {1.0, 0.75, 1.0 / 3.0}, Bc[3] = {0.0, 0.25, 2.0 / 3.0}, C[3] = {1.0, 0.25, 2.0 / 3.0};
   const int nv = ctx->nv;
   const int sin = rk, sout = sout_override >= 0 ? sout_override : (rk + 1) % 3;
-  for (size_t bi = 0; bi < ctx->blk.size(); ++bi) {
+  for_blocks(ctx, [&](int bi) {
     BlockRes &B = ctx->blk[bi];
     const DevState in = state_of(B, sin);
     const bool chem = ctx->der.reaction == 1, implicit = chem && ctx->chem_mode == OSTC_CHEM_POINT_IMPLICIT;
@@ -1854,14 +1884,14 @@ void enqueue_mix_stage(ostc_ctx *ctx, int rk, int sout_override = -1) {
       end_t(ctx, tok);
     }
     launch_carry(ctx, B, in, state_of(B, sout));
-    launch_bcs(ctx, (int)bi, state_of(B, sout));
-  }
+    launch_bcs(ctx, bi, state_of(B, sout));
+  });
   launch_interfaces(ctx, sout);
-  for (auto &B : ctx->blk) {
+  for_blocks(ctx, [&](int bi) {
     long tok = begin_t(ctx, "properties");
-    launch_mix_props(ctx, B, state_of(B, sout));
+    launch_mix_props(ctx, ctx->blk[bi], state_of(ctx->blk[bi], sout));
     end_t(ctx, tok);
-  }
+  });
 }
 
 // One SSP-RK3 step of a mixture (RK.cuh:85-185 with MixtureModel Mixture / FR): source, flux-split
@@ -2187,6 +2217,23 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
     g_create_error = "cudaStreamCreate failed";
     return OSTC_ECUDA;
   }
+  if (ctx->mesh.blocks.size() > 1) {
+    const size_t ns = std::min<size_t>(ctx->mesh.blocks.size(), 4);
+    bool ok = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming) == cudaSuccess;
+    for (size_t k = 0; k < ns && ok; ++k) {
+      cudaStream_t st;
+      cudaEvent_t ev;
+      ok = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess;
+      if (ok) ctx->side.push_back(st);
+      ok = ok && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
+      if (ok) ctx->side_ev.push_back(ev);
+    }
+    if (!ok) {
+      g_create_error = "cudaStreamCreate (block streams) failed";
+      ostc_destroy(ctx.release());
+      return OSTC_ECUDA;
+    }
+  }
   const bool is3d = ctx->mesh.dimension == 3;
   size_t max_n = 0;
   for (auto &HB : ctx->mesh.blocks) {
@@ -2344,6 +2391,9 @@ void ostc_destroy(ostc_ctx *ctx) {
     cudaEventDestroy(e.second);
   }
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  for (auto st : ctx->side) cudaStreamDestroy(st);
+  for (auto ev : ctx->side_ev) cudaEventDestroy(ev);
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   delete ctx;
 }
 
