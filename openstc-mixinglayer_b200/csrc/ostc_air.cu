@@ -699,7 +699,8 @@ constexpr size_t visc_smem_bytes() {
 }
 
 template <typename T, bool DIM3, int TX, int TY>
-__global__ void __launch_bounds__(TX *TY, 3) k_visc_update(DevBlock b, StageArgs a, double *__restrict__ dq,
+// FP64: the plane ring's shared memory admits two blocks per SM, so registers are not capped for three
+__global__ void __launch_bounds__(TX *TY, sizeof(T) == 8 ? 2 : 3) k_visc_update(DevBlock b, StageArgs a, double *__restrict__ dq,
                                                                       int kseg) {
   constexpr int NP = DIM3 ? 3 : 1;  // planes in the ring
   constexpr int SX = TX + 2, SY = TY + 2;
@@ -773,6 +774,23 @@ __global__ void __launch_bounds__(TX *TY, 3) k_visc_update(DevBlock b, StageArgs
   const double dt = a.update ? *a.dt : 0.0;
   for (int k = k0; k < k1; ++k) {
     T fz_next[4] = {T(0), T(0), T(0), T(0)};
+    // the node's update operands are loaded first, so that their latency overlaps the plane load
+    // and the face fluxes (only this thread reads or writes node (i, j, k) of these arrays)
+    double d[5], cq[5], cin[5], jk = 1.0;
+    if (inside) {
+      const long long qi = b.iq(i, j, k);
+#pragma unroll
+      for (int l = 0; l < 5; ++l) d[l] = dq[l * b.n + qi];
+      if (a.update) {
+        const long long p = b.id(i, j, k);
+        jk = b.jac[p];
+#pragma unroll
+        for (int l = 0; l < 5; ++l) {
+          cq[l] = a.qn.cv[l * P + p];
+          cin[l] = a.in.cv[l * P + p];
+        }
+      }
+    }
     if (a.viscous) {
       if (DIM3) load_plane(k + 1);
       else load_plane(k);
@@ -788,9 +806,6 @@ __global__ void __launch_bounds__(TX *TY, 3) k_visc_update(DevBlock b, StageArgs
     }
     if (inside) {
       const long long qi = b.iq(i, j, k);
-      double d[5];
-#pragma unroll
-      for (int l = 0; l < 5; ++l) d[l] = dq[l * b.n + qi];
       if (a.viscous) {
 #pragma unroll
         for (int l = 1; l < 5; ++l) d[l] += (double)(fxs[ty][tx + 1][l - 1] - fxs[ty][tx][l - 1]);
@@ -806,10 +821,10 @@ __global__ void __launch_bounds__(TX *TY, 3) k_visc_update(DevBlock b, StageArgs
         for (int l = 0; l < 5; ++l) dq[l * b.n + qi] = d[l];
       } else {
         const long long p = b.id(i, j, k);
-        const double dtj = dt / b.jac[p];
+        const double dtj = dt / jk;
         double cv[5];
 #pragma unroll
-        for (int l = 0; l < 5; ++l) cv[l] = a.a * a.qn.cv[l * P + p] + a.bcoef * a.in.cv[l * P + p] + a.c * dtj * d[l];
+        for (int l = 0; l < 5; ++l) cv[l] = a.a * cq[l] + a.bcoef * cin[l] + a.c * dtj * d[l];
         if (!DIM3) cv[3] = 0;
         const double rho = cv[0];
         const double di = 1.0 / cv[0];
