@@ -144,7 +144,8 @@ int ostc_adjoint_steps(ostc_ctx *ctx, int n_steps, int every, const double *lam_
 
 /* Advance n_steps full SSP-RK3 steps (the loop body of RK3<mix,turb>, RK.cuh:85-185), all stream
  * ordered and replayed from a CUDA graph.  dt_last (nullable) receives the last step's dt (CFL
- * minimum over all blocks, TimeAdvanceFunc.cu:39-64, or the fixed dt); reading it synchronises. */
+ * minimum over all blocks, TimeAdvanceFunc.cu:39-64, or the fixed dt); reading it synchronises, and
+ * then a raised device error flag (NaN, non-positive rho / p / T) returns OSTC_ENUMERIC. */
 int ostc_rk3_step(ostc_ctx *ctx, int n_steps, double *dt_last);
 
 /* Same as ostc_rk3_step without the dt read-back, bracketed by CUDA events recorded on the context

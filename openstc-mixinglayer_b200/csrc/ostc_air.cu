@@ -2790,8 +2790,16 @@ int ostc_rk3_step(ostc_ctx *ctx, int n_steps, double *dt_last) {
   if (int r = ensure_graph(ctx)) return r;
   for (int s = 0; s < n_steps; ++s) CK(cudaGraphLaunch(ctx->graph, ctx->stream));
   if (dt_last) {
+    unsigned flags = 0;
     CK(cudaMemcpyAsync(dt_last, ctx->d_dt, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&flags, ctx->d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    if (flags) {
+      ctx->err = (flags & OSTC_FLAG_NAN) ? "a NaN appeared in the conservative state (ostc_error_flags reads and clears it)"
+                                         : "non-positive density, pressure or temperature after an RK stage "
+                                           "(ostc_error_flags reads and clears it)";
+      return OSTC_ENUMERIC;
+    }
   }
   return OSTC_OK;
 }

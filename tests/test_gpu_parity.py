@@ -118,3 +118,26 @@ def test_device_flags_clean_and_residual(built, tmp_path):
                    np.mean((b1[5] - b0[5]) ** 2)])
     assert np.allclose(res, ref, rtol=1e-10, atol=0)
     assert s.error_flags() == 0
+
+
+@pytest.mark.parametrize("what", ["nan_temperature", "negative_pressure"])
+def test_bad_state_raises_device_flag(built, tmp_path, what):
+    """Fault detection without a GPU fault: a state seeded with a NaN temperature (or a negative
+    pressure) at one interior node is stepped; the update kernel raises its device flag, the step
+    returns OSTC_ENUMERIC, and ostc_error_flags reports and clears the flag."""
+    import ostc
+
+    case = oc.mixing_layer_3d(mx=24, my=16, mz=8)
+    if what == "nan_temperature":
+        case.bv[5, 4, 8, 12] = np.nan
+    else:
+        case.bv[4, 4, 8, 12] = -case.bv[4, 4, 8, 12]
+    d = oc.write_case(case, tmp_path / "case")
+    s = ostc.Solver(str(d))
+    s.set_state(case.bv)
+    with pytest.raises(ostc.OstcError) as e:
+        s.step(1)
+    assert e.value.code == -6  # OSTC_ENUMERIC
+    flags = s.error_flags()
+    assert flags & (ostc.FLAG_NAN | ostc.FLAG_NONPOSITIVE)
+    assert s.error_flags() == 0  # read and cleared
