@@ -10,9 +10,9 @@ inviscid + viscous RHS, update, boundaries).  One cell-step = one interior node 
   value    plain FP64 path, inputs resident in HBM, CUDA events on the library stream
   mixed    FP32 flux/viscous arithmetic with FP64 state, same workload; its rel-L2 distance to the
            FP64 path after warmup+steps steps is stated
-  e2e      the same metric through the C ABI with host buffers: each step copies the primitive state
-           from pinned host memory in (ostc_set_state), advances one step and copies it back
-           (ostc_get_state)
+  e2e      the same metric through the C ABI with host buffers (ostc_run_states): each step copies
+           its primitive input state from pinned host memory in, advances one step and copies the
+           state back; the copies of neighbouring steps run on two copy streams under the compute
   roofline dominant kernel (by device time), algorithmic bytes per launch / average launch time
   cpu_baseline  the serial C restatement of the same path (oracle/) on a sub-grid sample
   reacting the 9-species H2/air mixing layer, 384 x 192 x 96, flux-split characteristic WENO7,
@@ -76,7 +76,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--dims", type=int, nargs=3, default=[512, 256, 128])
-    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--e2e-steps", type=int, default=6)
     p.add_argument("--no-mixed", action="store_true")
     p.add_argument("--cpu-sample", type=int, nargs=3, default=[96, 64, 48])
     p.add_argument("--cpu-steps", type=int, default=3)
@@ -334,15 +334,12 @@ def run_ours(args):
         hin.copy_(_t.from_numpy(case.bv))
         hout = _t.empty((6,) + s.shape(), dtype=_t.float64, pin_memory=True)
         se = ostc.Solver(tmp, device=local)
-        se.set_state_ptr(hin.data_ptr())
-        se.step(1)
-        se.get_state_ptr(0, hout.data_ptr())
+        # ostc_run_states: every step takes its input state from pinned host memory and returns its
+        # result there; the copies of neighbouring steps overlap the computation on copy streams
+        se.run_states_ptr([hin.data_ptr()], [hout.data_ptr()], 1)  # allocations, graph capture
         barrier()
         t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            se.set_state_ptr(hin.data_ptr())
-            se.step_async(1)
-            se.get_state_ptr(0, hout.data_ptr())
+        se.run_states_ptr([hin.data_ptr()] * args.e2e_steps, [hout.data_ptr()] * args.e2e_steps, 1)
         t1 = time.perf_counter()
         barrier()
         el = allmax(t1 - t0)

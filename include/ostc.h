@@ -148,6 +148,16 @@ int ostc_adjoint_steps(ostc_ctx *ctx, int n_steps, int every, const double *lam_
  * then a raised device error flag (NaN, non-positive rho / p / T) returns OSTC_ENUMERIC. */
 int ostc_rk3_step(ostc_ctx *ctx, int n_steps, double *dt_last);
 
+/* Serving loop over independent states (ensemble members, parameter sweeps), single-block cases:
+ * for each i < n, state i is set from host arrays bv_in[i] (and sv_in[i] for mixtures) exactly as
+ * ostc_set_state does, advanced n_steps SSP-RK3 steps from t = 0, and its primitive state written
+ * to bv_out[i] (sv_out[i]).  The host->device copy of state i + 1 and the device->host copy of state
+ * i - 1 run on two copy streams while state i is computed (double-buffered device staging), so with
+ * pinned host buffers the transfers hide behind the steps.  Synchronises at the end.  No reference
+ * counterpart (the reference advances one case per process). */
+int ostc_run_states(ostc_ctx *ctx, int n, const double *const *bv_in, const double *const *sv_in,
+                    double *const *bv_out, double *const *sv_out, int n_steps);
+
 /* Same as ostc_rk3_step without the dt read-back, bracketed by CUDA events recorded on the context
  * stream: *ms receives the device time of the n_steps steps.  Synchronises. */
 int ostc_timed_steps(ostc_ctx *ctx, int n_steps, double *ms);

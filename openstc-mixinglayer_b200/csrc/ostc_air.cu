@@ -1238,6 +1238,10 @@ struct ostc_ctx {
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> side_ev;
   cudaEvent_t fork_ev = nullptr;
+  // ostc_run_states pipeline: copy streams, double-buffered device staging, hand-over events
+  cudaStream_t rs_h2d = nullptr, rs_d2h = nullptr;
+  double *rs_in[2]{}, *rs_out[2]{};
+  cudaEvent_t rs_in_ready[2]{}, rs_in_free[2]{}, rs_out_ready[2]{}, rs_out_free[2]{};
   Setup setup;
   Derived der;
   HostMesh mesh;
@@ -1793,7 +1797,6 @@ int initialise(ostc_ctx *ctx) {
   return OSTC_OK;
 }
 
-// One SSP-RK3 step over all blocks (RK.cuh:85-185).
 // Run f(b) for every block.  Multi-block steps fork the blocks onto the side streams (block b on
 // side[b % n]) and join them back before returning, so independent blocks' sweeps fill the GPU
 // together; with per-kernel timing on (ostc_profile_steps) the blocks run one after another.
@@ -1819,6 +1822,7 @@ void for_blocks(ostc_ctx *ctx, F f) {
   }
 }
 
+// One SSP-RK3 step over all blocks (RK.cuh:85-185).
 template <typename T>
 int enqueue_step(ostc_ctx *ctx) {
   static const double A[3] = {1.0, 0.75, 1.0 / 3.0}, Bc[3] = {0.0, 0.25, 2.0 / 3.0}, C[3] = {1.0, 0.25, 2.0 / 3.0};
@@ -2079,6 +2083,33 @@ int adjoint_t_to_cv(ostc_ctx *ctx) {
 int enqueue_step_any(ostc_ctx *ctx) {
   if (ctx->mixture) return enqueue_step_mix(ctx);
   return ctx->precision == OSTC_PREC_MIXED ? enqueue_step<float>(ctx) : enqueue_step<double>(ctx);
+}
+
+// The device part of ostc_set_state: buffer A of block B takes the primitive state from device
+// arrays bv[6][N] (and sv[n_spec][N]); ghost nodes start from the default initialisation (or zero)
+// and are rewritten by the boundary faces and interfaces when the context next initialises.
+void enqueue_set_state(ostc_ctx *ctx, BlockRes &B, const double *bv, const double *sv) {
+  if (ctx->has_init) {
+    FillVals fv{};
+    for (int l = 0; l < 6; ++l) fv.val[l] = ctx->init_bv[l];
+    k_fill_planes<<<grid_for(ctx, 6 * B.db.plane, 256), 256, 0, ctx->stream>>>(B.db.plane, B.bv[0], 6, fv);
+  } else {
+    cudaMemsetAsync(B.bv[0], 0, 6 * B.db.plane * sizeof(double), ctx->stream);
+  }
+  cudaMemsetAsync(B.cv[0], 0, (size_t)ctx->nv * B.db.plane * sizeof(double), ctx->stream);
+  cudaMemsetAsync(B.mul[0], 0, B.db.plane * sizeof(double), ctx->stream);
+  k_scatter<<<grid_for(ctx, 6 * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, bv, B.bv[0], 6);
+  if (ctx->mixture) {
+    const int ns = ctx->der.n_spec;
+    if (ctx->has_init && (int)ctx->init_sv.size() == ns && ns <= 16) {
+      FillVals fv{};
+      for (int l = 0; l < ns; ++l) fv.val[l] = ctx->init_sv[l];
+      k_fill_planes<<<grid_for(ctx, ns * B.db.plane, 256), 256, 0, ctx->stream>>>(B.db.plane, B.sv[0], ns, fv);
+    } else {
+      cudaMemsetAsync(B.sv[0], 0, (size_t)ns * B.db.plane * sizeof(double), ctx->stream);
+    }
+    k_scatter<<<grid_for(ctx, ns * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, sv, B.sv[0], ns);
+  }
 }
 
 int check_ready(ostc_ctx *ctx) {
@@ -2349,7 +2380,7 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
             cudaMalloc(&ctx->d_sums, 4 * sizeof(double)) == cudaSuccess &&
             cudaMalloc(&ctx->d_step, sizeof(long long)) == cudaSuccess &&
             cudaMalloc(&ctx->d_flags, sizeof(unsigned)) == cudaSuccess &&
-            cudaMalloc(&ctx->d_staging, (size_t)std::max(6, ctx->nv) * max_n * sizeof(double)) == cudaSuccess;
+            cudaMalloc(&ctx->d_staging, (size_t)std::max(6 + ctx->der.n_spec, ctx->nv) * max_n * sizeof(double)) == cudaSuccess;
   if (!ok) {
     g_create_error = "device allocation failed";
     ostc_destroy(ctx.release());
@@ -2407,6 +2438,14 @@ void ostc_destroy(ostc_ctx *ctx) {
   }
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   for (auto st : ctx->side) cudaStreamDestroy(st);
+  if (ctx->rs_h2d) cudaStreamDestroy(ctx->rs_h2d);
+  if (ctx->rs_d2h) cudaStreamDestroy(ctx->rs_d2h);
+  for (int b = 0; b < 2; ++b) {
+    cudaFree(ctx->rs_in[b]);
+    cudaFree(ctx->rs_out[b]);
+    for (cudaEvent_t e : {ctx->rs_in_ready[b], ctx->rs_in_free[b], ctx->rs_out_ready[b], ctx->rs_out_free[b]})
+      if (e) cudaEventDestroy(e);
+  }
   for (auto ev : ctx->side_ev) cudaEventDestroy(ev);
   if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   delete ctx;
@@ -2484,30 +2523,11 @@ int ostc_set_state(ostc_ctx *ctx, int block, const double *bv, const double *sv,
   const auto kind = ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   const size_t bytes = 6 * (size_t)B.db.n * sizeof(double);
   CK(cudaMemcpyAsync(ctx->d_staging, bv, bytes, kind, ctx->stream));
-  // buffer A holds the new state; ghost nodes start from the default initialisation (or zero) and
-  // are rewritten by the boundary faces and interfaces
-  if (ctx->has_init) {
-    FillVals fv{};
-    for (int l = 0; l < 6; ++l) fv.val[l] = ctx->init_bv[l];
-    k_fill_planes<<<grid_for(ctx, 6 * B.db.plane, 256), 256, 0, ctx->stream>>>(B.db.plane, B.bv[0], 6, fv);
-  } else {
-    CK(cudaMemsetAsync(B.bv[0], 0, 6 * B.db.plane * sizeof(double), ctx->stream));
-  }
-  CK(cudaMemsetAsync(B.cv[0], 0, (size_t)ctx->nv * B.db.plane * sizeof(double), ctx->stream));
-  CK(cudaMemsetAsync(B.mul[0], 0, B.db.plane * sizeof(double), ctx->stream));
-  k_scatter<<<grid_for(ctx, 6 * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, ctx->d_staging, B.bv[0], 6);
   if (ctx->mixture) {
-    const int ns = ctx->der.n_spec;
-    if (ctx->has_init && (int)ctx->init_sv.size() == ns && ns <= 16) {
-      FillVals fv{};
-      for (int l = 0; l < ns; ++l) fv.val[l] = ctx->init_sv[l];
-      k_fill_planes<<<grid_for(ctx, ns * B.db.plane, 256), 256, 0, ctx->stream>>>(B.db.plane, B.sv[0], ns, fv);
-    } else {
-      CK(cudaMemsetAsync(B.sv[0], 0, (size_t)ns * B.db.plane * sizeof(double), ctx->stream));
-    }
-    CK(cudaMemcpyAsync(ctx->d_staging, sv, (size_t)ns * B.db.n * sizeof(double), kind, ctx->stream));
-    k_scatter<<<grid_for(ctx, ns * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, ctx->d_staging, B.sv[0], ns);
+    CK(cudaMemcpyAsync(ctx->d_staging + 6 * B.db.n, sv, (size_t)ctx->der.n_spec * B.db.n * sizeof(double), kind,
+                       ctx->stream));
   }
+  enqueue_set_state(ctx, B, ctx->d_staging, ctx->d_staging + 6 * B.db.n);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->block_set[block] = 1;
@@ -2753,6 +2773,76 @@ int ostc_adjoint_steps(ostc_ctx *ctx, int n_steps, int every, const double *lam_
     ctx->err = "ostc_adjoint_steps: CUDA error";
     return OSTC_ECUDA;
   }
+  return OSTC_OK;
+}
+
+static int ensure_graph(ostc_ctx *ctx);
+
+int ostc_run_states(ostc_ctx *ctx, int n, const double *const *bv_in, const double *const *sv_in,
+                    double *const *bv_out, double *const *sv_out, int n_steps) {
+  if (!ctx || n < 0 || n_steps < 0 || (n > 0 && (!bv_in || !bv_out))) return OSTC_EINVAL;
+  if (ctx->blk.size() != 1) {
+    ctx->err = "ostc_run_states: single-block cases";
+    return OSTC_EINVAL;
+  }
+  if (ctx->mixture && n > 0 && (!sv_in || !sv_out)) {
+    ctx->err = "ostc_run_states: a mixture case needs sv_in and sv_out";
+    return OSTC_EINVAL;
+  }
+  cudaSetDevice(ctx->device);
+  BlockRes &B = ctx->blk[0];
+  const long long N = B.db.n;
+  const int ns = ctx->mixture ? ctx->der.n_spec : 0;
+  const size_t vals = (size_t)(6 + ns) * N;
+  if (!ctx->rs_h2d) {
+    CK(cudaStreamCreateWithFlags(&ctx->rs_h2d, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&ctx->rs_d2h, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+      CK(cudaMalloc(&ctx->rs_in[b], vals * sizeof(double)));
+      CK(cudaMalloc(&ctx->rs_out[b], vals * sizeof(double)));
+      for (cudaEvent_t *e : {&ctx->rs_in_ready[b], &ctx->rs_in_free[b], &ctx->rs_out_ready[b], &ctx->rs_out_free[b]})
+        CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+  }
+  // the step graph is captured once, from the first state
+  for (int i = 0; i < n; ++i) {
+    const int b = i & 1;
+    // host -> device of state i (overlaps the computation of state i - 1)
+    CK(cudaStreamWaitEvent(ctx->rs_h2d, ctx->rs_in_free[b], 0));
+    CK(cudaMemcpyAsync(ctx->rs_in[b], bv_in[i], 6 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->rs_h2d));
+    if (ns)
+      CK(cudaMemcpyAsync(ctx->rs_in[b] + 6 * N, sv_in[i], (size_t)ns * N * sizeof(double), cudaMemcpyHostToDevice,
+                         ctx->rs_h2d));
+    CK(cudaEventRecord(ctx->rs_in_ready[b], ctx->rs_h2d));
+    // compute state i: set, initialise, n_steps steps
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->rs_in_ready[b], 0));
+    enqueue_set_state(ctx, B, ctx->rs_in[b], ctx->rs_in[b] + 6 * N);
+    CK(cudaEventRecord(ctx->rs_in_free[b], ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_time, 0, sizeof(double), ctx->stream));
+    ctx->block_set[0] = 1;
+    ctx->state_set = true;
+    ctx->initialised = false;
+    if (int r = check_ready(ctx)) return r;
+    if (n_steps > 0) {
+      if (int r = ensure_graph(ctx)) return r;
+      for (int st = 0; st < n_steps; ++st) CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+    }
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->rs_out_free[b], 0));
+    k_gather<<<grid_for(ctx, 6 * N, 256), 256, 0, ctx->stream>>>(B.db, B.bv[0], ctx->rs_out[b], 6);
+    if (ns)
+      k_gather<<<grid_for(ctx, ns * N, 256), 256, 0, ctx->stream>>>(B.db, B.sv[0], ctx->rs_out[b] + 6 * N, ns);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->rs_out_ready[b], ctx->stream));
+    // device -> host of state i (overlaps the computation of state i + 1)
+    CK(cudaStreamWaitEvent(ctx->rs_d2h, ctx->rs_out_ready[b], 0));
+    CK(cudaMemcpyAsync(bv_out[i], ctx->rs_out[b], 6 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->rs_d2h));
+    if (ns)
+      CK(cudaMemcpyAsync(sv_out[i], ctx->rs_out[b] + 6 * N, (size_t)ns * N * sizeof(double), cudaMemcpyDeviceToHost,
+                         ctx->rs_d2h));
+    CK(cudaEventRecord(ctx->rs_out_free[b], ctx->rs_d2h));
+  }
+  CK(cudaStreamSynchronize(ctx->rs_d2h));
+  CK(cudaStreamSynchronize(ctx->stream));
   return OSTC_OK;
 }
 

@@ -26,7 +26,7 @@ EXPORTS = [
     "ostc_physical_time", "ostc_store_residual_reference", "ostc_residual", "ostc_error_flags",
     "ostc_device_view", "ostc_profile_steps", "ostc_total_nodes", "ostc_probe_case", "ostc_timed_steps",
     "ostc_step_kernel_count", "ostc_residual_noalloc", "ostc_set_chem_mode", "ostc_set_conservative",
-    "ostc_rhs_vjp", "ostc_rk3_step_vjp", "ostc_adjoint_steps",
+    "ostc_rhs_vjp", "ostc_rk3_step_vjp", "ostc_adjoint_steps", "ostc_run_states",
 ]
 
 
@@ -73,6 +73,7 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.ostc_rhs_vjp.argtypes = [vp, ip, ctypes.c_uint, vp, vp, ip]
     lib.ostc_rk3_step_vjp.argtypes = [vp, vp, vp, ip]
     lib.ostc_adjoint_steps.argtypes = [vp, ip, ip, vp, vp, ip]
+    lib.ostc_run_states.argtypes = [vp, ip, vp, vp, vp, vp, ip]
     lib.ostc_rk3_step.argtypes = [vp, ip, dp]
     lib.ostc_physical_time.argtypes = [vp, dp]
     lib.ostc_store_residual_reference.argtypes = [vp]
@@ -212,6 +213,24 @@ class Solver:
         cv_bar = np.empty((self.n_var,) + self.shape(block))
         self._check(self.lib.ostc_rhs_vjp(self.h, block, mask, _ptr(dq_bar), _ptr(cv_bar), OSTC_HOST))
         return cv_bar
+
+    def run_states_ptr(self, bv_in: list, bv_out: list, n_steps: int = 1, sv_in=None, sv_out=None):
+        """ostc_run_states over host pointers (ints, ideally pinned memory): state i from bv_in[i]
+        (sv_in[i]), advanced n_steps steps, written to bv_out[i] (sv_out[i])."""
+        n = len(bv_in)
+        arr = lambda ps: (ctypes.c_void_p * n)(*[ctypes.c_void_p(p) for p in ps]) if ps is not None else None
+        self._check(self.lib.ostc_run_states(self.h, n, arr(bv_in), arr(sv_in), arr(bv_out), arr(sv_out), n_steps))
+
+    def run_states(self, bv_in: list, n_steps: int = 1, sv_in=None):
+        """Advance each of the (bv, sv) host states n_steps steps; returns the list of (bv, sv) results."""
+        bvi = [np.ascontiguousarray(b, dtype=np.float64) for b in bv_in]
+        svi = None if sv_in is None else [np.ascontiguousarray(x, dtype=np.float64) for x in sv_in]
+        bvo = [np.empty_like(b) for b in bvi]
+        svo = None if svi is None else [np.empty_like(x) for x in svi]
+        self.run_states_ptr([b.ctypes.data for b in bvi], [b.ctypes.data for b in bvo], n_steps,
+                            None if svi is None else [x.ctypes.data for x in svi],
+                            None if svo is None else [x.ctypes.data for x in svo])
+        return list(zip(bvo, svo if svo is not None else [None] * len(bvo)))
 
     def step_vjp(self, lam_out: np.ndarray) -> np.ndarray:
         """(d q' / d q)^T lam_out for one RK3 step from the current state (dt held fixed)."""

@@ -141,3 +141,27 @@ def test_bad_state_raises_device_flag(built, tmp_path, what):
     flags = s.error_flags()
     assert flags & (ostc.FLAG_NAN | ostc.FLAG_NONPOSITIVE)
     assert s.error_flags() == 0  # read and cleared
+
+
+@pytest.mark.parametrize("mixture", [False, True], ids=["air", "mixture"])
+def test_run_states_matches_one_at_a_time(built, tmp_path, mixture):
+    """ostc_run_states (independent states, copies overlapped with the steps) gives bitwise the
+    states that set_state + step + get_state give one at a time."""
+    case = (oc.reacting_mixing_layer_3d(mx=24, my=18, mz=12) if mixture else oc.mixing_layer_3d(mx=32, my=24, mz=16))
+    d = oc.write_case(case, tmp_path / "case")
+    s = ostc.Solver(str(d))
+    rng = np.random.default_rng(5)
+    states = []
+    for m in range(3):
+        bv = case.bv.copy()
+        bv[2] *= 1 + 0.1 * m
+        bv[1] += 0.01 * rng.standard_normal(bv[1].shape)
+        states.append((bv, None if case.sv is None else case.sv.copy()))
+    got = s.run_states([b for b, _ in states], 2, None if not mixture else [x for _, x in states])
+    for (bv, sv), (gb, gs) in zip(states, got):
+        s.set_state(bv, sv=sv)
+        s.step(2)
+        _, rb = s.get_state()
+        assert np.array_equal(gb, rb)
+        if mixture:
+            assert np.array_equal(gs, s.get_species())
