@@ -63,7 +63,7 @@ __global__ void k_mix_init_cv(DevBlock b, DevState s) {
 // compute_source<FR> (SourceTerm.cuh:11-35) as the first contribution to dq: dq[5+l] = J omega_l
 // (finite rate) or 0, dq[0..4] = 0.
 template <int NS>
-__global__ void __launch_bounds__(128) k_mix_source(DevBlock b, DevState s, double *__restrict__ dq, int nv,
+__global__ void __launch_bounds__(128, 4) k_mix_source(DevBlock b, DevState s, double *__restrict__ dq, int nv,
                                                      int finite_rate) {
   if (NS > 0) nv = 5 + NS;
   const long long P = b.plane;
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(128) k_mix_source(DevBlock b, DevState s, doub
 // (I - dt J_chem) x = dq_species (EPI + solve_chem_system, FiniteRateChem.cu:233-254, 302-357, with the
 // stage's global dt), one cell per thread, every cell of the block in one launch.
 template <int NS>
-__global__ void __launch_bounds__(128) k_mix_chem_epi(DevBlock b, DevState s, double *__restrict__ dq,
+__global__ void __launch_bounds__(128, 4) k_mix_chem_epi(DevBlock b, DevState s, double *__restrict__ dq,
                                                        const double *dtp) {
   const long long P = b.plane;
   const int ns = OSTC_NS;
@@ -136,7 +136,7 @@ __host__ __device__ constexpr size_t fvs_smem_bytes(int nv) {
 // and after a barrier the node threads difference neighbouring faces into dq.  T is the arithmetic
 // type of the fluxes (FP32 in the mixed precision mode: state read in FP64, dq accumulated in FP64).
 template <int DIR, int NS, typename T>
-__global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_fvs(DevBlock b, DevState s,
+__global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL, 4) k_fvs(DevBlock b, DevState s,
                                                                                double *__restrict__ dq, int nv,
                                                                                int scheme) {
   constexpr int TXL = FvsTile<DIR>::TXL, TD = FvsTile<DIR>::TD, NST = FvsTile<DIR>::NST;
@@ -451,7 +451,7 @@ __device__ __forceinline__ void mix_visc_face(const DevBlock &b, const DevState 
 // viscous_flux_fv/gv/hv (SchemeSelector.cuh:69-154) for mixtures: one thread per face of the tile,
 // then dq += fv(i+1/2) - fv(i-1/2) through shared memory; tiles as the flux-split sweeps.
 template <int DIR, bool DIM3, int NS, typename T>
-__global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_mix_visc(DevBlock b, DevState s,
+__global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL, sizeof(T) == 8 ? 4 : 5) k_mix_visc(DevBlock b, DevState s,
                                                                                     double *__restrict__ dq, int nv) {
   if (NS > 0) nv = 5 + NS;
   constexpr int TXL = FvsTile<DIR>::TXL, TD = FvsTile<DIR>::TD;
@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_mix_vi
 // update_cv_and_bv_rk<mixture> (RK.cuh:230-284) with compute_temperature_and_pressure
 // (FieldOperation.cu:3-40): the Newton iteration starts from the stage-input temperature.
 template <int NS>
-__global__ void __launch_bounds__(128) k_mix_update(DevBlock b, DevState in, DevState qn, DevState out,
+__global__ void __launch_bounds__(128, 4) k_mix_update(DevBlock b, DevState in, DevState qn, DevState out,
                                                      const double *__restrict__ dq, const double *dtp, double ca,
                                                      double cb, double cc, int nv, unsigned *flags) {
   if (NS > 0) nv = 5 + NS;
