@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(256) k_cfl_dt(DevBlock b, DevState s, double c
 // ------------------------------------------------------------------------------ inviscid flux
 
 // Resident blocks per SM the x sweep is compiled for (register budget 65536 / (128 * this)).
-template <typename T> struct FluxXOcc { static constexpr int blocks = 2; };
+template <typename T> struct FluxXOcc { static constexpr int blocks = 3; };
 template <> struct FluxXOcc<float> { static constexpr int blocks = 4; };
 
 // x sweep.  A block of 128 threads stages 127 + 2*NG nodes of one (j,k) row in shared memory
@@ -391,8 +391,17 @@ constexpr size_t tile_smem_bytes() {
   return (size_t)(15 * (TF - 1 + 2 * NG) + 5 * TF) * TXL * sizeof(T);
 }
 
+// Resident blocks per SM a tile variant is compiled for: FP32 variants at 128 registers per thread;
+// FP64 16-lane variants (half the shared memory of the 32-lane ones) at three 128-thread or two
+// 256-thread blocks; the FP64 32-lane variant is shared-memory limited to two blocks anyway.
+template <typename T, int TXL, int NT>
+__host__ __device__ constexpr int tile_min_blocks() {
+  return sizeof(T) == 4 ? 65536 / (NT * 128) : (TXL == 16 ? (NT == 128 ? 3 : 2) : 2);
+}
+
 template <int DIR, int NG, int RS, typename T, int TXL, int TD, int FPT>
-__global__ void __launch_bounds__(TXL * TD) k_flux_tile(DevBlock b, DevState s, double *__restrict__ dq) {
+__global__ void __launch_bounds__(TXL * TD, tile_min_blocks<T, TXL, TXL * TD>())
+    k_flux_tile(DevBlock b, DevState s, double *__restrict__ dq) {
   constexpr int TF = TD * FPT;
   constexpr int L = TF - 1;
   constexpr int NP = L + 2 * NG;
