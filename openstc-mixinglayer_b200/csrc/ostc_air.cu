@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(256) k_cfl_dt(DevBlock b, DevState s, double c
 
 // Resident blocks per SM the x sweep is compiled for (register budget 65536 / (128 * this)).
 template <typename T> struct FluxXOcc { static constexpr int blocks = 3; };
-template <> struct FluxXOcc<float> { static constexpr int blocks = 4; };
+template <> struct FluxXOcc<float> { static constexpr int blocks = 5; };
 
 // x sweep.  A block of 128 threads stages 127 + 2*NG nodes of one (j,k) row in shared memory
 // (coalesced along i), computes the 128 faces i0-1/2 .. i0+126+1/2 (one per thread) and finalises
@@ -709,7 +709,7 @@ constexpr size_t visc_smem_bytes() {
 
 template <typename T, bool DIM3, int TX, int TY>
 // FP64: the plane ring's shared memory admits two blocks per SM, so registers are not capped for three
-__global__ void __launch_bounds__(TX *TY, sizeof(T) == 8 ? 2 : 3) k_visc_update(DevBlock b, StageArgs a, double *__restrict__ dq,
+__global__ void __launch_bounds__(TX *TY, sizeof(T) == 8 ? 2 : 4) k_visc_update(DevBlock b, StageArgs a, double *__restrict__ dq,
                                                                       int kseg) {
   constexpr int NP = DIM3 ? 3 : 1;  // planes in the ring
   constexpr int SX = TX + 2, SY = TY + 2;
