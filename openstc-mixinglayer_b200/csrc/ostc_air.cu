@@ -391,12 +391,13 @@ constexpr size_t tile_smem_bytes() {
   return (size_t)(15 * (TF - 1 + 2 * NG) + 5 * TF) * TXL * sizeof(T);
 }
 
-// Resident blocks per SM a tile variant is compiled for: FP32 variants at 128 registers per thread;
-// FP64 16-lane variants (half the shared memory of the 32-lane ones) at three 128-thread or two
-// 256-thread blocks; the FP64 32-lane variant is shared-memory limited to two blocks anyway.
+// Resident blocks per SM a tile variant is compiled for: FP32 variants at 128 registers per thread,
+// but three 256-thread blocks (80 registers, measured faster despite small spills); FP64 16-lane
+// variants (half the shared memory of the 32-lane ones) at three 128-thread or two 256-thread
+// blocks; the FP64 32-lane variant is shared-memory limited to two blocks anyway.
 template <typename T, int TXL, int NT>
 __host__ __device__ constexpr int tile_min_blocks() {
-  return sizeof(T) == 4 ? 65536 / (NT * 128) : (TXL == 16 ? (NT == 128 ? 3 : 2) : 2);
+  return sizeof(T) == 4 ? (NT == 256 ? 3 : 65536 / (NT * 128)) : (TXL == 16 ? (NT == 128 ? 3 : 2) : 2);
 }
 
 template <int DIR, int NG, int RS, typename T, int TXL, int TD, int FPT>
