@@ -782,7 +782,7 @@ __device__ __forceinline__ void mix_visc_face_bwd(const DevBlock &b, const DevSt
 // Reverse of k_mix_visc: one thread per face; the face adjoint is dq_bar(n) - dq_bar(n + 1) over the
 // nodes this tile owns (the forward adds fv(n + 1/2) to node n and subtracts it from node n + 1).
 template <int DIR, bool DIM3, int NS>
-__global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_adj_visc(DevBlock b, DevState s,
+__global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL, 3) k_adj_visc(DevBlock b, DevState s,
                                                                                     const double *__restrict__ dqb,
                                                                                     int nv, DevAdj A) {
   if (NS > 0) nv = 5 + NS;
@@ -825,7 +825,7 @@ __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL) k_adj_vi
 // concentrations; kf, kb are differentiated in T (and in the third-body sum) by Dual evaluations of
 // the same rate-constant code.
 template <int NS>
-__global__ void __launch_bounds__(128) k_adj_source(DevBlock b, DevState s, const double *__restrict__ dqb, DevAdj A) {
+__global__ void __launch_bounds__(128, 4) k_adj_source(DevBlock b, DevState s, const double *__restrict__ dqb, DevAdj A) {
   const long long P = b.plane;
   const int ns = OSTC_NS, nr = c_mix.nr;
   constexpr int SA = Spec<NS>::A;
@@ -918,7 +918,7 @@ __global__ void __launch_bounds__(128) k_adj_source(DevBlock b, DevState s, cons
 // adjoints of c, mu, lambda and rho*D_k -> adjoints of rho, p, T and Y.  Hand-written reverse of
 // mix_properties (one forward sweep keeping its intermediates, then the reverse sweep).
 template <int NS>
-__global__ void __launch_bounds__(128) k_adj_props(DevBlock b, DevState s, DevAdj A) {
+__global__ void __launch_bounds__(128, 4) k_adj_props(DevBlock b, DevState s, DevAdj A) {
   const long long P = b.plane;
   const int ns = OSTC_NS;
   constexpr int SA = Spec<NS>::A;
@@ -1077,7 +1077,7 @@ __global__ void __launch_bounds__(128) k_adj_props(DevBlock b, DevState s, DevAd
 // it (compute_cv_from_bv_1_point<mixture>, FieldOperation.cuh:78-105): rho E = rho (sum h(T) Y +
 // |V|^2 / 2) - p.  This moves a ghost's cv adjoint onto its primitive adjoints (rho, u, v, w, p, T, Y).
 template <int NS>
-__global__ void __launch_bounds__(128) k_adj_ghost_cv(DevBlock b, DevState s, DevAdj A, int nv) {
+__global__ void __launch_bounds__(128, 4) k_adj_ghost_cv(DevBlock b, DevState s, DevAdj A, int nv) {
   if (NS > 0) nv = 5 + NS;
   const long long P = b.plane;
   const int ns = OSTC_NS;
@@ -1125,7 +1125,7 @@ __global__ void __launch_bounds__(128) k_adj_ghost_cv(DevBlock b, DevState s, De
 // FieldOperation.cu:3-40) and its adjoint goes to cv by the implicit-function derivative; otherwise
 // T is a state variable of its own and its adjoint is left in A.T.
 template <int NS>
-__global__ void __launch_bounds__(128) k_adj_eos(DevBlock b, DevState s, DevAdj A, int exact_t) {
+__global__ void __launch_bounds__(128, 4) k_adj_eos(DevBlock b, DevState s, DevAdj A, int exact_t) {
   const long long P = b.plane;
   const int ns = OSTC_NS;
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
@@ -1228,7 +1228,7 @@ __global__ void __launch_bounds__(128) k_adj_bc_face(DevBlock b, DevAdj A, int n
 // iterate (not the exact root) is differentiated, by Dual evaluations seeded on e, each Y and the
 // start T: lam_cv += (dT_out / d cv_out)^T lam_t, lam_t_start += dT_out / dT_start * lam_t.
 template <int NS>
-__global__ void __launch_bounds__(128) k_adj_newton(DevBlock b, DevState in, DevState out, const double *lam_t,
+__global__ void __launch_bounds__(128, 4) k_adj_newton(DevBlock b, DevState in, DevState out, const double *lam_t,
                                                     double *lam_cv, double *lam_t_start) {
   const long long P = b.plane;
   const int ns = OSTC_NS;
