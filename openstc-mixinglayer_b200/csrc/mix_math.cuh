@@ -35,6 +35,9 @@ struct MixTables {
   double low[kMS][7], high[kMS][7];
   double lj_potent_inv[kMS], vis_coeff[kMS];
   double wj_div_wi_1_4[kMS][kMS], sqrt_wiwj_8[kMS][kMS], binary_diff[kMS][kMS], kb_over_eps[kMS][kMS];
+  // ln of lj_potent_inv and of kb_over_eps: the reduced temperatures' powers T*^a = exp(a (ln T + ln c))
+  // then take one log per node instead of one pow per species / species pair
+  double ln_lj[kMS], ln_kbe[kMS][kMS];
   int label[kMR], rev_type[kMR], order[kMR];
   signed char stoi_f[kMR][kMS], stoi_b[kMR][kMS];
   double A[kMR], b[kMR], Ea[kMR], A2[kMR], b2[kMR], Ea2[kMR], third_body[kMR][kMS];
@@ -107,13 +110,17 @@ __device__ __forceinline__ void mix_properties(T rho, T p, T t, const T *y, T &g
   mw = 1 / mw;
   gamma = cpt / cvt;
   acoustic = tsqrt(gamma * T(kRuD) * t / mw);
-  T X[Spec<NS>::A], vis[Spec<NS>::A];
-  const T st = tsqrt(t);
+  // (T*)^-0.145 = exp(-0.145 (ln T + ln c)) and (T* + 0.5)^-2 = 1 / (T* + 0.5)^2: the same values as
+  // pow to within a few ulp, at one log per node
+  T X[Spec<NS>::A], vis[Spec<NS>::A], svis[Spec<NS>::A], isvis[Spec<NS>::A];
+  const T st = tsqrt(t), lt = log(t);
   for (int l = 0; l < ns; ++l) {
     X[l] = y[l] * mw * (T)c_mix.imw[l];
     const T tdl = t * (T)c_mix.lj_potent_inv[l];
-    const T ci = T(1.147) * tpow<T>(tdl, T(-0.145)) + tpow<T>(tdl + T(0.5), T(-2));
+    const T ci = T(1.147) * exp(T(-0.145) * (lt + (T)c_mix.ln_lj[l])) + T(1) / ((tdl + T(0.5)) * (tdl + T(0.5)));
     vis[l] = (T)c_mix.vis_coeff[l] * st / ci;
+    svis[l] = tsqrt(vis[l]);
+    isvis[l] = T(1) / svis[l];
   }
   T visc = 0, cd = 0;
   for (int m = 0; m < ns; ++m) {
@@ -121,7 +128,7 @@ __device__ __forceinline__ void mix_properties(T rho, T p, T t, const T *y, T &g
     for (int n = 0; n < ns; ++n) {
       T pf = 1;
       if (m != n) {
-        const T num = T(1) + tsqrt(vis[m] / vis[n]) * (T)c_mix.wj_div_wi_1_4[m][n];
+        const T num = T(1) + svis[m] * isvis[n] * (T)c_mix.wj_div_wi_1_4[m][n];
         pf = num * num * (T)c_mix.sqrt_wiwj_8[m][n];
       }
       vt += pf * X[n];
@@ -143,7 +150,7 @@ __device__ __forceinline__ void mix_properties(T rho, T p, T t, const T *y, T &g
   for (int l = 0; l < ns; ++l) {
     for (int n = l + 1; n < ns; ++n) {
       const T tr = t * (T)c_mix.kb_over_eps[l][n];
-      const T om = T(1) / tpow<T>(tr, T(0.145)) + T(1) / ((tr + T(0.5)) * (tr + T(0.5)));
+      const T om = exp(T(-0.145) * (lt + (T)c_mix.ln_kbe[l][n])) + T(1) / ((tr + T(0.5)) * (tr + T(0.5)));
       const T dln = (T)c_mix.binary_diff[l][n] * t32p / om;
       num[l] += (X[n] + eps) * (T)c_mix.mw[n];
       den[l] += (X[n] + eps) / dln;

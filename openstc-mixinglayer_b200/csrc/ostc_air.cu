@@ -2197,12 +2197,15 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
         m.high[i][q] = c.high[i * 7 + q];
       }
       m.lj_potent_inv[i] = c.lj_potent_inv[i];
+      m.ln_lj[i] = std::log(c.lj_potent_inv[i]);
       m.vis_coeff[i] = c.vis_coeff[i];
       for (int j = 0; j < c.n_spec; ++j) {
         m.wj_div_wi_1_4[i][j] = c.wj_div_wi_1_4[i * c.n_spec + j];
         m.sqrt_wiwj_8[i][j] = c.sqrt_wiwj_8[i * c.n_spec + j];
         m.binary_diff[i][j] = c.binary_diff[i * c.n_spec + j];
         m.kb_over_eps[i][j] = c.kb_over_eps_jk[i * c.n_spec + j];
+        // the diagonal (0) is never used
+        m.ln_kbe[i][j] = m.kb_over_eps[i][j] > 0 ? std::log(m.kb_over_eps[i][j]) : 0.0;
       }
     }
     m.use_gibbs = 0;
