@@ -381,6 +381,28 @@ __device__ __forceinline__ T fvs_den(T eps, T beta) {
   return d;
 }
 
+// Unnormalised Z weights a_k = c_k (1 + tau / D_k), D_k = (eps + beta_k)^2.  FP64 forms the four
+// quotients from two divisions, 1 / D0 = D1 / (D0 D1) and alike (D_k >= eps^2 keeps the pair products
+// in range for any practical eps; if one underflows the four divisions are taken); FP32 divides each
+// (its scaled D_k may be as small as 1e-30).
+template <typename T>
+__device__ __forceinline__ void fvs_weights(T c0, T c1, T c2, T c3, T tau, T d0, T d1, T d2, T d3, T &a0, T &a1, T &a2,
+                                            T &a3) {
+  const T p01 = d0 * d1, p23 = d2 * d3;
+  if (sizeof(T) == 8 && p01 > T(0) && p23 > T(0)) {  // pair products representable (always, for eps > 1e-77)
+    const T r01 = tau / p01, r23 = tau / p23;
+    a0 = c0 + c0 * (d1 * r01);
+    a1 = c1 + c1 * (d0 * r01);
+    a2 = c2 + c2 * (d3 * r23);
+    a3 = c3 + c3 * (d2 * r23);
+  } else {
+    a0 = c0 + c0 * tau / d0;
+    a1 = c1 + c1 * tau / d1;
+    a2 = c2 + c2 * tau / d2;
+    a3 = c3 + c3 * tau / d3;
+  }
+}
+
 // WENO7 of the flux-split path (WENO.cu:1619-1693): returns f+ + f-.
 template <typename T>
 __device__ __forceinline__ T fvs_weno7_core(const T *vp, const T *vm, T eps) {
@@ -402,10 +424,9 @@ __device__ __forceinline__ T fvs_weno7_core(const T *vp, const T *vm, T eps) {
   s3 = -vp[3] + 3 * vp[4] - 3 * vp[5] + vp[6];
   T b3 = fvs_beta7(s1, s2, s3);
   T tau = (b0 - b3) * (b0 - b3);
-  T a0 = c0 + c0 * tau / (fvs_den(eps, b0));
-  T a1 = c1 + c1 * tau / (fvs_den(eps, b1));
-  T a2 = c2 + c2 * tau / (fvs_den(eps, b2));
-  T a3 = c3 + c3 * tau / (fvs_den(eps, b3));
+  T a0, a1, a2, a3;
+  fvs_weights(c0, c1, c2, c3, tau, fvs_den(eps, b0), fvs_den(eps, b1), fvs_den(eps, b2), fvs_den(eps, b3), a0, a1, a2,
+              a3);
   T v0 = one12th * (-3 * vp[0] + 13 * vp[1] - 23 * vp[2] + 25 * vp[3]);
   T v1 = one12th * (vp[1] - 5 * vp[2] + 13 * vp[3] + 3 * vp[4]);
   T v2 = one12th * (-vp[2] + 7 * vp[3] + 7 * vp[4] - vp[5]);
@@ -427,10 +448,8 @@ __device__ __forceinline__ T fvs_weno7_core(const T *vp, const T *vm, T eps) {
   s3 = -vm[3] + 3 * vm[2] - 3 * vm[1] + vm[0];
   b3 = fvs_beta7(s1, s2, s3);
   tau = (b0 - b3) * (b0 - b3);
-  a0 = c0 + c0 * tau / (fvs_den(eps, b0));
-  a1 = c1 + c1 * tau / (fvs_den(eps, b1));
-  a2 = c2 + c2 * tau / (fvs_den(eps, b2));
-  a3 = c3 + c3 * tau / (fvs_den(eps, b3));
+  fvs_weights(c0, c1, c2, c3, tau, fvs_den(eps, b0), fvs_den(eps, b1), fvs_den(eps, b2), fvs_den(eps, b3), a0, a1, a2,
+              a3);
   v0 = one12th * (-3 * vm[6] + 13 * vm[5] - 23 * vm[4] + 25 * vm[3]);
   v1 = one12th * (vm[5] - 5 * vm[4] + 13 * vm[3] + 3 * vm[2]);
   v2 = one12th * (-vm[4] + 7 * vm[3] + 7 * vm[2] - vm[1]);
