@@ -40,3 +40,29 @@ def test_point_implicit_reduces_to_explicit(built):
     de = oe.rhs(7)
     di = oi.rhs(7)
     assert np.allclose(di, de, rtol=1e-12, atol=1e-12 * np.max(np.abs(de)))
+
+
+def _element_matrix(names):
+    """Atoms of H, O, N per species from the formula names of the mechanism (H2O2 -> H 2, O 2)."""
+    import re
+
+    elems = ["H", "O", "N"]
+    m = np.zeros((len(elems), len(names)))
+    for k, n in enumerate(names):
+        for sym, cnt in re.findall(r"([A-Z][a-z]?)(\d*)", n):
+            m[elems.index(sym), k] += int(cnt) if cnt else 1
+    return m
+
+
+def test_chemical_source_conserves_elements(built):
+    """sum_k a_ek omega_k / W_k = 0 for the elements H, O, N: reactions rearrange atoms only."""
+    case = oc.reacting_mixing_layer_3d(mx=10, my=12, mz=6)
+    t = case.mixture["tables"]
+    o = Oracle(case)
+    o.set_state(case.bv)
+    w = o.rhs(4)[5:]  # J omega_k
+    a = _element_matrix(t.names) / np.asarray(t.mw)[None, :]
+    moles = np.einsum("ek,k...->e...", a, w)
+    scale = np.einsum("ek,k...->e...", a, np.abs(w))
+    assert np.all(np.abs(moles) <= 1e-12 * np.max(scale, axis=tuple(range(1, scale.ndim)), keepdims=True)), \
+        np.max(np.abs(moles))
