@@ -174,6 +174,14 @@ int ostc_store_residual_reference(ostc_ctx *ctx);
  * res[l] = sqrt(sum over all interior nodes of (change)^2 / total node count). Synchronises. */
 int ostc_residual(ostc_ctx *ctx, double res[4]);
 
+/* Bounds-checked build only (libostc_b200_checked.so, compiled with -DOSTC_BOUNDS_CHECK): bit 1 = a
+ * padded-plane index, bit 2 = an interior index fell outside its block since the last call (the
+ * index was clamped, no access left the arrays); the call clears the flag.  ostc_bounds_checked()
+ * tells whether the loaded library is that build (1) or the regular one (0, flags always 0).  No
+ * reference counterpart: a device-side substitute for a memory checker. */
+int ostc_bounds_flags(ostc_ctx *ctx, unsigned *flags);
+int ostc_bounds_checked(void);
+
 /* Device error flags (OSTC_FLAG_*) accumulated since the last call, then cleared.  Synchronises. */
 int ostc_error_flags(ostc_ctx *ctx, unsigned *flags);
 

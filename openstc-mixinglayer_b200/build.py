@@ -10,6 +10,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 SOURCES = ["csrc/host.cpp", "csrc/chem.cpp", "csrc/ostc_air.cu", "csrc/ostc_noalloc.cu"]
 OUT = PKG / "libostc_b200.so"
+OUT_CHECKED = PKG / "libostc_b200_checked.so"  # -DOSTC_BOUNDS_CHECK: index-checked accessors
 
 
 def nvcc() -> str:
@@ -19,28 +20,29 @@ def nvcc() -> str:
     return "nvcc"
 
 
-def needs_build() -> bool:
-    if not OUT.exists():
+def needs_build(out: Path = OUT) -> bool:
+    if not out.exists():
         return True
-    t = OUT.stat().st_mtime
+    t = out.stat().st_mtime
     headers = sorted((PKG / "csrc").glob("*.h")) + sorted((PKG / "csrc").glob("*.cuh"))
     deps = [PKG / s for s in SOURCES] + headers + [ROOT / "include" / "ostc.h"]
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    if not force and not needs_build():
-        return OUT
+def build(force: bool = False, verbose: bool = False, checked: bool = False) -> Path:
+    out = OUT_CHECKED if checked else OUT
+    if not force and not needs_build(out):
+        return out
     cmd = [nvcc(), "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
            "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-I", str(ROOT / "include"), "-shared",
-           *[str(PKG / s) for s in SOURCES], "-o", str(OUT)]
+           *(["-DOSTC_BOUNDS_CHECK"] if checked else []), *[str(PKG / s) for s in SOURCES], "-o", str(out)]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc build of libostc_b200.so failed")
+        raise RuntimeError(f"nvcc build of {out.name} failed")
     if verbose:
         sys.stdout.write(r.stdout + r.stderr)
-    return OUT
+    return out
 
 
 if __name__ == "__main__":

@@ -17,6 +17,7 @@
 #include "ostc.h"
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -29,14 +30,36 @@
 
 namespace ostc {
 
+// Bounds-checked build (-DOSTC_BOUNDS_CHECK, libostc_b200_checked.so; the sanitizer is not
+// available): every padded-plane index id() and interior index iq() is checked against the block's
+// extents; an index outside them sets bit 1 (padded) or 2 (interior) of this flag and is clamped into
+// range, so the access stays inside the arrays.  ostc_bounds_flags reads and clears it.
+__device__ unsigned g_ostc_bounds = 0;
+
 struct DevBlock {
   int mx, my, mz, g, gz, pitch, sy, sz;
   long long plane, off0, n;
   const double *met, *jac;
   __host__ __device__ __forceinline__ long long id(int i, int j, int k) const {
+#if defined(OSTC_BOUNDS_CHECK) && defined(__CUDA_ARCH__)
+    if (i < -g || i >= pitch - g || j < -g || j >= sy - g || k < -gz || k >= sz - gz) {
+      atomicOr(&g_ostc_bounds, 1u);
+      i = min(max(i, -g), pitch - g - 1);
+      j = min(max(j, -g), sy - g - 1);
+      k = min(max(k, -gz), sz - gz - 1);
+    }
+#endif
     return off0 + ((long long)k * sy + j) * pitch + i;
   }
   __host__ __device__ __forceinline__ long long iq(int i, int j, int k) const {
+#if defined(OSTC_BOUNDS_CHECK) && defined(__CUDA_ARCH__)
+    if (i < 0 || i >= mx || j < 0 || j >= my || k < 0 || k >= mz) {
+      atomicOr(&g_ostc_bounds, 2u);
+      i = min(max(i, 0), mx - 1);
+      j = min(max(j, 0), my - 1);
+      k = min(max(k, 0), mz - 1);
+    }
+#endif
     return ((long long)k * my + j) * mx + i;
   }
 };
@@ -1320,8 +1343,11 @@ int fam_index(ostc_ctx *ctx, const char *name) {
 }
 
 // Records a begin event for a kernel family when timing is on; returns a token for end_t.
+// Per-kernel-family timing of ostc_profile_steps: CUDA events on the context stream around each
+// launch group, and an NVTX range of the same name (visible to nsys / ncu range filters).
 long begin_t(ostc_ctx *ctx, const char *name) {
   if (!ctx->timing) return -1;
+  nvtxRangePushA(name);
   const size_t slot = ctx->ev_used.size();
   if (slot >= ctx->ev_pool.size()) {
     cudaEvent_t a, b;
@@ -1335,6 +1361,7 @@ long begin_t(ostc_ctx *ctx, const char *name) {
 }
 void end_t(ostc_ctx *ctx, long tok) {
   if (tok < 0) return;
+  nvtxRangePop();
   cudaEventRecord(ctx->ev_pool[tok].second, ctx->stream);
 }
 
@@ -2970,6 +2997,24 @@ int ostc_residual(ostc_ctx *ctx, double res[4]) {
   CK(cudaStreamSynchronize(ctx->stream));
   for (int l = 0; l < 4; ++l) res[l] = std::sqrt(h[l] / (double)tot);
   return OSTC_OK;
+}
+
+int ostc_bounds_flags(ostc_ctx *ctx, unsigned *flags) {
+  if (!ctx || !flags) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaMemcpyFromSymbol(flags, g_ostc_bounds, sizeof(unsigned)));
+  const unsigned zero = 0;
+  CK(cudaMemcpyToSymbol(g_ostc_bounds, &zero, sizeof(unsigned)));
+  return OSTC_OK;
+}
+
+int ostc_bounds_checked(void) {
+#ifdef OSTC_BOUNDS_CHECK
+  return 1;
+#else
+  return 0;
+#endif
 }
 
 int ostc_error_flags(ostc_ctx *ctx, unsigned *flags) {

@@ -26,7 +26,8 @@ EXPORTS = [
     "ostc_physical_time", "ostc_store_residual_reference", "ostc_residual", "ostc_error_flags",
     "ostc_device_view", "ostc_profile_steps", "ostc_total_nodes", "ostc_probe_case", "ostc_timed_steps",
     "ostc_step_kernel_count", "ostc_residual_noalloc", "ostc_set_chem_mode", "ostc_set_conservative",
-    "ostc_rhs_vjp", "ostc_rk3_step_vjp", "ostc_adjoint_steps", "ostc_run_states",
+    "ostc_rhs_vjp", "ostc_rk3_step_vjp", "ostc_adjoint_steps", "ostc_run_states", "ostc_bounds_flags",
+    "ostc_bounds_checked",
 ]
 
 
@@ -51,7 +52,8 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = Path(path) if path else LIB_PATH
+    # OSTC_LIBRARY selects another build of the same ABI (the bounds-checked one in tests)
+    p = Path(path) if path else Path(os.environ.get("OSTC_LIBRARY", LIB_PATH))
     if not p.exists():
         raise OstcError(-100, f"{p} not built: run __graft_entry__.build() (nvcc for sm_100a)")
     lib = ctypes.CDLL(str(p))
@@ -74,6 +76,8 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.ostc_rk3_step_vjp.argtypes = [vp, vp, vp, ip]
     lib.ostc_adjoint_steps.argtypes = [vp, ip, ip, vp, vp, ip]
     lib.ostc_run_states.argtypes = [vp, ip, vp, vp, vp, vp, ip]
+    lib.ostc_bounds_flags.argtypes = [vp, ctypes.POINTER(ctypes.c_uint)]
+    lib.ostc_bounds_checked.argtypes = []
     lib.ostc_rk3_step.argtypes = [vp, ip, dp]
     lib.ostc_physical_time.argtypes = [vp, dp]
     lib.ostc_store_residual_reference.argtypes = [vp]
@@ -231,6 +235,12 @@ class Solver:
                             None if svi is None else [x.ctypes.data for x in svi],
                             None if svo is None else [x.ctypes.data for x in svo])
         return list(zip(bvo, svo if svo is not None else [None] * len(bvo)))
+
+    def bounds_flags(self) -> int:
+        """Index-bounds flags of the bounds-checked build (read and cleared; 0 in the regular build)."""
+        f = ctypes.c_uint()
+        self._check(self.lib.ostc_bounds_flags(self.h, ctypes.byref(f)))
+        return f.value
 
     def step_vjp(self, lam_out: np.ndarray) -> np.ndarray:
         """(d q' / d q)^T lam_out for one RK3 step from the current state (dt held fixed)."""
