@@ -20,6 +20,9 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1603,7 +1606,13 @@ void launch_yz(ostc_ctx *ctx, BlockRes &B, DevState in, int variant) {
 // Autotuner of the y / z sweeps: on the context's current state (the sweeps only read the state and
 // accumulate into the dq scratch), time every variant for each block, direction and the active
 // precision with CUDA events on the library stream, and keep the fastest.  Runs once per precision,
-// outside any stream capture, before the step graph is built.
+// outside any stream capture, before the step graph is built.  Results are cached in the process by
+// (device, block extents, ngg, scheme, precision, direction), so further contexts of the same shape
+// (other blocks of the same extents, a second solver on the same case) reuse them.
+using TuneKey = std::tuple<int, int, int, int, int, int, int, int, int>;
+std::map<TuneKey, int> g_tune_cache;
+std::mutex g_tune_mutex;
+
 template <typename T>
 int autotune_yz(ostc_ctx *ctx) {
   const int pi = std::is_same_v<T, float> ? 1 : 0;
@@ -1613,6 +1622,15 @@ int autotune_yz(ostc_ctx *ctx) {
   for (auto &B : ctx->blk) {
     const DevState in = state_of(B, 0);
     for (int dir = 1; dir <= (B.db.mz > 1 ? 2 : 1); ++dir) {
+      const TuneKey key{ctx->device, B.db.mx, B.db.my, B.db.mz, B.db.g, ctx->der.riemann, ctx->der.inviscid_type, pi, dir};
+      {
+        std::lock_guard<std::mutex> lk(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+          B.yz_var[pi][dir - 1] = it->second;
+          continue;
+        }
+      }
       float best = 1e30f;
       int bv = 0;
       for (int v = 0; v < kYzVariants; ++v) {
@@ -1633,6 +1651,8 @@ int autotune_yz(ostc_ctx *ctx) {
         }
       }
       B.yz_var[pi][dir - 1] = bv;
+      std::lock_guard<std::mutex> lk(g_tune_mutex);
+      g_tune_cache[key] = bv;
     }
   }
   cudaEventDestroy(e0);
