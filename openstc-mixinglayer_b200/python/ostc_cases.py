@@ -15,6 +15,7 @@ from __future__ import annotations
 import dataclasses
 import math
 import os
+import re
 from pathlib import Path
 
 import numpy as np
@@ -50,8 +51,8 @@ class Case:
     scheme: dict      # reconstruction, inviscid_scheme, viscous_order, cfl, prandtl_number
     bv: np.ndarray    # [6, mz, my, mx] initial primitive state
     steps: int = 100
-    # multi-component mixtures: sv [n_spec, mz, my, mx] mass fractions; mixture = dict(tables (an
-    # object with names, mw, ... as oracle/chem.py builds), finite_rate, chem_dir (directory holding
+    # multi-component mixtures: sv [n_spec, mz, my, mx] mass fractions; mixture = dict(tables (a
+    # SpeciesThermo: names, molecular weights, NASA-7 polynomials), finite_rate, chem_dir (directory holding
     # the CHEMKIN files), mechanism, therm, tran); freestream = reference state (mach, pressure,
     # temperature, Y {name: value}) written as the inflow struct "freestream"
     sv: np.ndarray | None = None
@@ -196,6 +197,72 @@ class Case:
         for st in self.bc_structs.values():
             m[st["label"][1]] = types[st["type"][1]]
         return m
+
+
+# element weights (kg/kmol) the species molecular weights are summed from
+_ATOMIC_WEIGHT = {"H": 1.008, "HE": 4.002602, "C": 12.011, "N": 14.007, "O": 15.999, "AR": 39.95}
+
+
+class SpeciesThermo:
+    """Species names (mechanism order), molecular weights and NASA-7 polynomials: what a synthetic
+    initial state and its freestream need from the CHEMKIN files (the library itself reads the full
+    mechanism, thermodynamics and transport from the same files)."""
+    names: list
+    n_spec: int
+    mw: np.ndarray
+    t_low: np.ndarray
+    t_mid: np.ndarray
+    t_high: np.ndarray
+    low: np.ndarray   # [n_spec, 7] below t_mid
+    high: np.ndarray  # [n_spec, 7] above t_mid
+
+
+def read_species(chem_dir: os.PathLike, mechanism: str, therm: str) -> SpeciesThermo:
+    """Species of the mechanism's SPECIES block and their therm.dat entries (fixed-column CHEMKIN
+    layout: name in columns 1-18, up to four element/count pairs of 5 columns from column 25, the
+    temperature range in columns 46-75, then 5 + 5 + 4 coefficients of 15 columns on three lines)."""
+    text = Path(chem_dir, mechanism).read_text().upper()
+    text = "\n".join(line.split("!")[0] for line in text.split("\n"))
+    m = re.search(r"\bSPEC(?:IES)?\b(.*?)\bEND\b", text, re.S)
+    if m is None:
+        raise ValueError(f"{mechanism}: no SPECIES block")
+    names = list(dict.fromkeys(m.group(1).split()))
+    ns = len(names)
+    st = SpeciesThermo()
+    st.names, st.n_spec = names, ns
+    st.mw = np.zeros(ns)
+    st.t_low, st.t_mid, st.t_high = np.full(ns, 300.0), np.full(ns, 1000.0), np.full(ns, 5000.0)
+    st.low, st.high = np.zeros((ns, 7)), np.zeros((ns, 7))
+    lines = Path(chem_dir, therm).read_text().split("\n")
+    i = next(k for k, line in enumerate(lines) if line.upper().startswith("THERMO")) + 1
+    while not lines[i].strip() or lines[i].lstrip().startswith("!"):
+        i += 1
+    st.t_low[:], st.t_mid[:], st.t_high[:] = (float(v) for v in lines[i].split()[:3])
+    i += 1
+    found = set()
+    while i < len(lines) and len(found) < ns:
+        head = lines[i].upper()
+        word = head[:18].split()
+        if not word or head.lstrip().startswith("!") or word[0] == "END" or word[0] not in names or word[0] in found:
+            i += 1
+            continue
+        k = names.index(word[0])
+        for col, arr in ((45, st.t_low), (55, st.t_high), (65, st.t_mid)):
+            field = head[col:col + 10].split()
+            if field:
+                arr[k] = float(field[0])
+        for q in range(4):
+            pair = head[24 + 5 * q:29 + 5 * q].split()
+            if len(pair) == 2 and pair[0] in _ATOMIC_WEIGHT:
+                st.mw[k] += _ATOMIC_WEIGHT[pair[0]] * int(float(pair[1]))
+        c = [float(lines[i + 1 + r][15 * q:15 * q + 15]) for r, nq in enumerate((5, 5, 4)) for q in range(nq)]
+        st.high[k] = c[0:7]
+        st.low[k] = c[7:14]
+        found.add(word[0])
+        i += 4
+    if len(found) < ns:
+        raise ValueError(f"{therm}: no entry for {sorted(set(names) - found)}")
+    return st
 
 
 def species_cp(tb, t):
@@ -490,12 +557,8 @@ def reacting_mixing_layer_3d(mx=384, my=192, mz=96, seed=0, steps=100, h=0.125, 
     runs from the first step), N2 the rest; T and Y blended by (1 + tanh(2y/delta0))/2, uniform p0, u = dU/2 tanh(2y/delta0)
     with dU = 2 Mc (c_fuel + c_ox)/2 and 1e-2 dU N(0,1) exp(-(y/delta0)^2) seeded noise in u, v, w;
     periodic x and z, outflow y; flux-split characteristic WENO7-Z (inviscid_scheme 72)."""
-    import sys
-    sys.path.insert(0, str(Path(__file__).resolve().parents[2] / "oracle"))
-    import chem as chemreader
-
     chem_dir = Path(chem_dir) if chem_dir else CHEM_FIXTURE
-    tb = chemreader.read(chem_dir, "H2_mech.inp", "therm.dat", "tran.dat", reactions=finite_rate)
+    tb = read_species(chem_dir, "H2_mech.inp", "therm.dat")
     ns = tb.n_spec
     fuel = fuel or {"H2": 0.05, "N2": 0.95}
     oxidiser = oxidiser or {"O2": 0.20, "H2O": 0.10, "OH": 1e-3, "O": 1e-4, "H": 1e-5, "HO2": 1e-6, "H2O2": 1e-7,

@@ -166,9 +166,13 @@ class Oracle:
         self.n_spec = 0
         mix = getattr(case, "mixture", None)
         if mix is not None:
-            self._chem = chem_struct(mix["tables"])
+            import chem  # the full restated tables (thermo, transport, reactions) of the same files
+            tables = chem.read(mix["chem_dir"], mix["mechanism"], mix["therm"], mix["tran"],
+                               reactions=mix["finite_rate"])
+            self.tables = tables
+            self._chem = chem_struct(tables)
             c.chem = ctypes.pointer(self._chem)
-            c.n_spec = self.n_spec = mix["tables"].n_spec
+            c.n_spec = self.n_spec = tables.n_spec
             c.finite_rate = 1 if mix["finite_rate"] else 0
         c.weno_eps_scale, c.v_ref = case.reference_scales()
         _set_init(c, case)

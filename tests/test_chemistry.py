@@ -10,7 +10,10 @@ from oracle import Oracle
 
 def test_h2_mechanism_tables(built):
     case = oc.reacting_mixing_layer_3d(mx=8, my=8, mz=6)
-    t = case.mixture["tables"]
+    t = Oracle(case).tables
+    assert case.mixture["tables"].names == t.names
+    assert np.array_equal(case.mixture["tables"].mw, t.mw)
+    assert np.array_equal(case.mixture["tables"].low, t.low) and np.array_equal(case.mixture["tables"].high, t.high)
     assert t.n_spec == 9 and t.n_reac == 19  # 21 reactions, two DUPLICATE pairs merged
     assert t.names == ["H", "H2", "H2O", "H2O2", "HO2", "O", "O2", "OH", "N2"]
     # Troe fall-off reactions (label 6) and third-body reactions (label 4) of the mechanism
