@@ -326,6 +326,20 @@ def run_ours(args):
                                "bytes_per_cell_step": 3 * STAGE_BYTES},
                 "kernels_ms_per_step": {k: v[1] / 2 for k, v in prof.items()}}
 
+    # ---- single-point statistics (SinglePointStat): one collection over the block and its ghost layer,
+    # every optional variable on, after the timed region; HBM bound (reads the 6 primitive planes,
+    # read-modify-writes every accumulator plane once)
+    s.stat_enable(0, ostc.STAT_REY_U | ostc.STAT_REY_V | ostc.STAT_REY_W | ostc.STAT_REY_T | ostc.STAT_RHO_P)
+    sprof = s.profile(2)
+    n_stat = s.stat_info()[0]
+    points = (mx + 2) * (my + 2) * (mz + 2)
+    st_ms = sprof["statistics"][1] / sprof["statistics"][0]
+    st_bytes = (6 + 2 * sum(n_stat)) * 8 * points
+    statistics = {"ms_per_collection": st_ms, "bytes_per_point": st_bytes // points, "points": points,
+                  "achieved_gbs": st_bytes / (st_ms / 1e3) / 1e9, "frac": st_bytes / (st_ms / 1e3) / 1e9 / hbm,
+                  "n_var": n_stat, "share_of_step": st_ms / (ms_max / K)}
+    s.stat_disable()
+
     # ---- end to end through the C ABI with host buffers
     e2e = None
     if args.e2e_steps > 0:
@@ -367,6 +381,7 @@ def run_ours(args):
                 "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic (seeded tanh shear layer + white noise; no dataset)",
                 "config": config_dict(args), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "statistics": statistics,
                 "mixed": mixed, "clocks": clocks, "gpu_launches": launches_per_step * K,
                 "error_flags": flags, **extra}
         print(json.dumps(line), flush=True)

@@ -204,6 +204,48 @@ int ostc_total_nodes(const ostc_ctx *ctx, long long *n);
  * (Parameter::deduce_known_info / Mesh::Mesh checks, Parameter.cpp:187-437, Mesh.cpp:592-641). */
 int ostc_probe_case(const char *setup_txt, const char *input_dir, int out[16], char *msg, int msg_len);
 
+/* ---- single-point statistics (SinglePointStat, SinglePointStat.h / SinglePointStat.cu:515-706)
+ *
+ * Replaces the collector the reference runs after every time step past start_collect_statistics_iter
+ * (RK.cuh:200-203, collect_single_point_basic_statistics SinglePointStat.cu:641-706) and its export
+ * (export_statistical_data, SinglePointStat.cu:553-638).  Per block and per node, one ghost layer
+ * included, sums over the collected steps of:
+ *   group 0 Reynolds 1st: rho, p, then u / v / w / T as OSTC_STAT_REY_* select (stat_rey_1st)
+ *   group 1 Favre 1st:    rho u, rho v, rho w, rho T, then rho Y_k for every species
+ *   group 2 Reynolds 2nd: rho rho, p p, then rho p with OSTC_STAT_RHO_P (rho_p_correlation)
+ *   group 3 Favre 2nd:    rho u u, rho v v, rho w w, rho u v, rho u w, rho v w, rho T T, rho Y_k Y_k
+ * each group stored [n_var][mz+2][my+2][mx+2], i fastest.  With if_collect_statistics = 1 in the
+ * setup (and an unsteady case) ostc_create enables collection with start_collect_statistics_iter,
+ * stat_rey_1st and rho_p_correlation; steps are counted from ostc_create.  The TKE budget and the
+ * species correlation / dissipation collectors (stat_lib/) are not provided. */
+#define OSTC_STAT_REY_U 1u
+#define OSTC_STAT_REY_V 2u
+#define OSTC_STAT_REY_W 4u
+#define OSTC_STAT_REY_T 8u
+#define OSTC_STAT_RHO_P 16u
+
+/* Allocate and zero the accumulators of every block and collect after each later step (ostc_rk3_step,
+ * ostc_timed_steps, ostc_profile_steps) whose index, counted from this call starting at 1, exceeds
+ * start_step.  Calling it again restarts from zero with the new selection. */
+int ostc_stat_enable(ostc_ctx *ctx, int start_step, unsigned flags);
+/* Stop collecting and free the accumulators. */
+int ostc_stat_disable(ostc_ctx *ctx);
+/* Variables per group (n_var[4]), collections so far (the reference's per-variable counters, all
+ * equal here) and steps counted since enabling.  OSTC_ESTATE when collection is off. */
+int ostc_stat_info(ostc_ctx *ctx, int n_var[4], int *n_collected, long long *steps);
+/* Copy group g (0..3) of block b: n_var x (mx+2)(my+2)(mz+2) doubles, layout as above, to host or
+ * device memory (ptr_kind).  Synchronises. */
+int ostc_stat_get(ostc_ctx *ctx, int block, int group, double *out, int ptr_kind);
+/* Write coll_rey_1st.bin, coll_fav_1st.bin, coll_rey_2nd.bin, coll_fav_2nd.bin into dir in the
+ * reference's layout (SinglePointStat.cu:163-226, 553-638, one process): int32 n_block, n_var, ngg = 1;
+ * the variable names as int32 characters, each ended by an int32 0; int32 counters[n_var]; then per
+ * block int32 mx, my, mz and its n_var planes of doubles. */
+int ostc_stat_export(ostc_ctx *ctx, const char *dir);
+/* Read the four files back into the accumulators and counters (if_continue_collect_statistics,
+ * read_previous_statistical_data): the selection must match the enabled one and the block extents
+ * the case's, else OSTC_EIO with the reason.  Collection then continues from the next step. */
+int ostc_stat_import(ostc_ctx *ctx, const char *dir);
+
 /* Limits of ostc_residual_noalloc: its static scratch holds one partial sum set per block of
  * 256 threads x 64 nodes, for at most OSTC_NOALLOC_MAX_BLOCKS blocks (128 KB of device memory). */
 #define OSTC_NOALLOC_NODES_PER_THREAD 64

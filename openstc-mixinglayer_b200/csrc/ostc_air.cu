@@ -23,6 +23,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -107,6 +108,7 @@ __device__ __forceinline__ void cv_from_bv_node(const DevBlock &b, DevState s, l
 
 #include "ostc_mix.cuh"
 #include "ostc_adj.cuh"
+#include "ostc_stat.cuh"
 
 namespace ostc {
 
@@ -1252,6 +1254,7 @@ struct BlockRes {
   double *dqb = nullptr;  // dq_bar on the device
   // step adjoint: [lam_cv, x2_cv, x1_cv, g_cv] (n_var x N each) then [lam_T, x2_T, x1_T, g_T] (N each)
   double *adj_work = nullptr;
+  double *stat = nullptr;  // single-point statistics accumulators (ostc_stat.cuh layout)
 };
 
 struct ostc_ctx {
@@ -1306,6 +1309,14 @@ struct ostc_ctx {
   std::vector<Fam> fams;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
   std::vector<std::pair<int, size_t>> ev_used;
+  // single-point statistics: collected after every step whose index (from enabling, 1-based)
+  // exceeds stat_start
+  bool stat_on = false;
+  int stat_start = 0;
+  long long stat_steps = 0;
+  int stat_count = 0;
+  unsigned stat_flags = 0;
+  StatSpec stat_spec{};
 };
 
 static std::string g_create_error;
@@ -2198,6 +2209,8 @@ int check_ready(ostc_ctx *ctx) {
 
 extern "C" {
 
+static int stat_setup(ostc_ctx *ctx, int start_step, const std::vector<int> &rey_idx, bool rho_p);
+
 int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_ctx **out) {
   if (!out || !input_dir) {
     g_create_error = "ostc_create: null argument";
@@ -2456,6 +2469,27 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
     ostc_destroy(ctx.release());
     return OSTC_ECUDA;
   }
+  // statistics requested by the setup (Driver.cu:104: unsteady runs only; init_stat_name,
+  // SinglePointStat.cu:115-146, skips unknown stat_rey_1st entries with a message)
+  if (ctx->setup.get_bool("if_collect_statistics") && !ctx->der.steady) {
+    std::vector<int> idx;
+    auto it = ctx->setup.string_arrays.find("stat_rey_1st");
+    if (it != ctx->setup.string_arrays.end())
+      for (std::string v : it->second) {
+        for (auto &c : v) c = (char)std::toupper((unsigned char)c);
+        const int q = v == "U" ? 1 : v == "V" ? 2 : v == "W" ? 3 : v == "T" ? 5 : -1;
+        if (q < 0 || idx.size() >= 4)
+          std::fprintf(stderr, "ostc: variable %s for Reynolds average is not supported\n", v.c_str());
+        else
+          idx.push_back(q);
+      }
+    if (int r = stat_setup(ctx.get(), ctx->setup.get_int("start_collect_statistics_iter"), idx,
+                           ctx->setup.get_bool("rho_p_correlation"))) {
+      g_create_error = ctx->err;
+      ostc_destroy(ctx.release());
+      return r;
+    }
+  }
   *out = ctx.release();
   return OSTC_OK;
 }
@@ -2474,6 +2508,7 @@ void ostc_destroy(ostc_ctx *ctx) {
     cudaFree(B.adj);
     cudaFree(B.dqb);
     cudaFree(B.adj_work);
+    cudaFree(B.stat);
     for (int s = 0; s < 4; ++s) {
       cudaFree(B.cv[s]);
       cudaFree(B.bv[s]);
@@ -2906,6 +2941,101 @@ int ostc_run_states(ostc_ctx *ctx, int n, const double *const *bv_in, const doub
   return OSTC_OK;
 }
 
+// ---------------------------------------------------------------- single-point statistics
+
+// Variable names of the four groups as the reference writes them (SinglePointStat.h:30-38,
+// init_stat_name SinglePointStat.cu:98-147).
+static std::vector<std::string> stat_names(const ostc_ctx *ctx, int g) {
+  const StatSpec &sp = ctx->stat_spec;
+  std::vector<std::string> v;
+  if (g == 0) {
+    v = {"rho", "p"};
+    for (int l = 0; l < sp.n_rey; ++l) {
+      const int q = sp.rey_idx[l];
+      v.push_back(q == 1 ? "u" : q == 2 ? "v" : q == 3 ? "w" : "T");
+    }
+  } else if (g == 1) {
+    v = {"rhoU", "rhoV", "rhoW", "rhoT"};
+    for (int l = 0; l < sp.ns; ++l) v.push_back("rho" + ctx->chem.names[l]);
+  } else if (g == 2) {
+    v = {"RhoRho", "pp"};
+    if (sp.rho_p) v.push_back("rhoP");
+  } else {
+    v = {"rhoUU", "rhoVV", "rhoWW", "rhoUV", "rhoUW", "rhoVW", "rhoTT"};
+    for (int l = 0; l < sp.ns; ++l) v.push_back("rho" + ctx->chem.names[l] + ctx->chem.names[l]);
+  }
+  return v;
+}
+
+static long long stat_block_doubles(const ostc_ctx *ctx, const BlockRes &B) {
+  int nvar = 0;
+  for (int g = 0; g < 4; ++g) nvar += stat_group_vars(ctx->stat_spec, g);
+  return nvar * stat_points(B.db);
+}
+
+static void stat_free(ostc_ctx *ctx) {
+  for (auto &B : ctx->blk) {
+    cudaFree(B.stat);
+    B.stat = nullptr;
+  }
+  ctx->stat_on = false;
+}
+
+// (Re)allocate and zero the accumulators for the selection rey_idx (primitive indices of the extra
+// Reynolds averages, in the order given) and rho_p.
+static int stat_setup(ostc_ctx *ctx, int start_step, const std::vector<int> &rey_idx, bool rho_p) {
+  if (start_step < 0 || rey_idx.size() > 4) {
+    ctx->err = "ostc_stat_enable: start_step must be >= 0 and at most 4 extra Reynolds averages";
+    return OSTC_EINVAL;
+  }
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  stat_free(ctx);
+  StatSpec sp{};
+  sp.n_rey = (int)rey_idx.size();
+  for (int l = 0; l < sp.n_rey; ++l) sp.rey_idx[l] = rey_idx[l];
+  sp.rho_p = rho_p ? 1 : 0;
+  sp.ns = ctx->der.n_spec;
+  ctx->stat_spec = sp;
+  for (auto &B : ctx->blk)
+    if (stat_points(B.db) >= (1LL << 31)) {
+      ctx->err = "ostc_stat_enable: a block with 2^31 or more points (ghost layer included) is not supported";
+      return OSTC_EINVAL;
+    }
+  for (auto &B : ctx->blk) {
+    const size_t bytes = (size_t)stat_block_doubles(ctx, B) * sizeof(double);
+    if (cudaMalloc(&B.stat, bytes) != cudaSuccess) {
+      stat_free(ctx);
+      ctx->err = "ostc_stat_enable: device allocation of the statistics accumulators failed";
+      return OSTC_ENOMEM;
+    }
+    CK(cudaMemsetAsync(B.stat, 0, bytes, ctx->stream));
+  }
+  ctx->stat_on = true;
+  ctx->stat_start = start_step;
+  ctx->stat_steps = 0;
+  ctx->stat_count = 0;
+  return OSTC_OK;
+}
+
+// After one step on the context stream: count it and, past the start step, accumulate every block
+// (SinglePointStat::collect_data, SinglePointStat.cu:515-551).
+static int stat_after_step(ostc_ctx *ctx) {
+  if (!ctx->stat_on) return OSTC_OK;
+  if (++ctx->stat_steps <= ctx->stat_start) return OSTC_OK;
+  for (auto &B : ctx->blk) {
+    long tok = begin_t(ctx, "statistics");
+    k_stat_collect<<<grid_for(ctx, stat_points(B.db), 256), 256, 0, ctx->stream>>>(B.db, state_of(B, 0), B.stat,
+                                                                                   ctx->stat_spec);
+    end_t(ctx, tok);
+  }
+  CK(cudaGetLastError());
+  ++ctx->stat_count;
+  return OSTC_OK;
+}
+
+static const char *const kStatFiles[4] = {"coll_rey_1st.bin", "coll_fav_1st.bin", "coll_rey_2nd.bin",
+                                          "coll_fav_2nd.bin"};
+
 static int ensure_graph(ostc_ctx *ctx) {
   if (!ctx->graph || ctx->graph_precision != ctx->precision) {
     if (ctx->graph) {
@@ -2938,7 +3068,10 @@ int ostc_rk3_step(ostc_ctx *ctx, int n_steps, double *dt_last) {
   cudaSetDevice(ctx->device);
   if (int r = check_ready(ctx)) return r;
   if (int r = ensure_graph(ctx)) return r;
-  for (int s = 0; s < n_steps; ++s) CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+  for (int s = 0; s < n_steps; ++s) {
+    CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+    if (int r = stat_after_step(ctx)) return r;
+  }
   if (dt_last) {
     unsigned flags = 0;
     CK(cudaMemcpyAsync(dt_last, ctx->d_dt, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -2963,7 +3096,10 @@ int ostc_timed_steps(ostc_ctx *ctx, int n_steps, double *ms) {
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
   CK(cudaEventRecord(a, ctx->stream));
-  for (int s = 0; s < n_steps; ++s) CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+  for (int s = 0; s < n_steps; ++s) {
+    CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+    if (int r = stat_after_step(ctx)) return r;
+  }
   CK(cudaEventRecord(b, ctx->stream));
   CK(cudaEventSynchronize(b));
   float t = 0;
@@ -3035,6 +3171,183 @@ int ostc_bounds_checked(void) {
 #else
   return 0;
 #endif
+}
+
+int ostc_stat_enable(ostc_ctx *ctx, int start_step, unsigned flags) {
+  if (!ctx) return OSTC_EINVAL;
+  if (flags & ~31u) {
+    ctx->err = "ostc_stat_enable: unknown flag bits";
+    return OSTC_EINVAL;
+  }
+  cudaSetDevice(ctx->device);
+  std::vector<int> idx;
+  if (flags & OSTC_STAT_REY_U) idx.push_back(1);
+  if (flags & OSTC_STAT_REY_V) idx.push_back(2);
+  if (flags & OSTC_STAT_REY_W) idx.push_back(3);
+  if (flags & OSTC_STAT_REY_T) idx.push_back(5);
+  return stat_setup(ctx, start_step, idx, (flags & OSTC_STAT_RHO_P) != 0);
+}
+
+int ostc_stat_disable(ostc_ctx *ctx) {
+  if (!ctx) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  stat_free(ctx);
+  return OSTC_OK;
+}
+
+int ostc_stat_info(ostc_ctx *ctx, int n_var[4], int *n_collected, long long *steps) {
+  if (!ctx) return OSTC_EINVAL;
+  if (!ctx->stat_on) {
+    ctx->err = "statistics collection is off (ostc_stat_enable, or if_collect_statistics in the setup)";
+    return OSTC_ESTATE;
+  }
+  for (int g = 0; g < 4 && n_var; ++g) n_var[g] = stat_group_vars(ctx->stat_spec, g);
+  if (n_collected) *n_collected = ctx->stat_count;
+  if (steps) *steps = ctx->stat_steps;
+  return OSTC_OK;
+}
+
+int ostc_stat_get(ostc_ctx *ctx, int block, int group, double *out, int ptr_kind) {
+  if (!ctx || !out || block < 0 || block >= (int)ctx->blk.size() || group < 0 || group > 3) return OSTC_EINVAL;
+  if (!ctx->stat_on) {
+    ctx->err = "statistics collection is off (ostc_stat_enable, or if_collect_statistics in the setup)";
+    return OSTC_ESTATE;
+  }
+  cudaSetDevice(ctx->device);
+  const BlockRes &B = ctx->blk[block];
+  const long long np = stat_points(B.db);
+  long long off = 0;
+  for (int g = 0; g < group; ++g) off += stat_group_vars(ctx->stat_spec, g) * np;
+  const size_t bytes = (size_t)stat_group_vars(ctx->stat_spec, group) * np * sizeof(double);
+  CK(cudaMemcpyAsync(out, B.stat + off, bytes, ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return OSTC_OK;
+}
+
+int ostc_stat_export(ostc_ctx *ctx, const char *dir) {
+  if (!ctx || !dir) return OSTC_EINVAL;
+  if (!ctx->stat_on) {
+    ctx->err = "statistics collection is off (ostc_stat_enable, or if_collect_statistics in the setup)";
+    return OSTC_ESTATE;
+  }
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<double> host;
+  for (int g = 0; g < 4; ++g) {
+    const std::string path = std::string(dir) + "/" + kStatFiles[g];
+    FILE *f = std::fopen(path.c_str(), "wb");
+    if (!f) {
+      ctx->err = "ostc_stat_export: cannot open " + path + " for writing";
+      return OSTC_EIO;
+    }
+    const int nvar = stat_group_vars(ctx->stat_spec, g);
+    bool ok = true;
+    auto put_i = [&](int v) { ok = ok && std::fwrite(&v, 4, 1, f) == 1; };
+    put_i((int)ctx->blk.size());
+    put_i(nvar);
+    put_i(1);
+    for (const auto &name : stat_names(ctx, g)) {
+      for (char c : name) put_i((int)c);
+      put_i(0);
+    }
+    for (int v = 0; v < nvar; ++v) put_i(ctx->stat_count);
+    long long off = 0;
+    for (int g2 = 0; g2 < g; ++g2) off += stat_group_vars(ctx->stat_spec, g2);
+    for (const auto &B : ctx->blk) {
+      put_i(B.db.mx);
+      put_i(B.db.my);
+      put_i(B.db.mz);
+      const long long np = stat_points(B.db);
+      host.resize((size_t)nvar * np);
+      if (cudaMemcpy(host.data(), B.stat + off * np, host.size() * sizeof(double), cudaMemcpyDeviceToHost) !=
+          cudaSuccess) {
+        std::fclose(f);
+        ctx->err = "ostc_stat_export: device copy failed";
+        return OSTC_ECUDA;
+      }
+      ok = ok && std::fwrite(host.data(), sizeof(double), host.size(), f) == host.size();
+    }
+    if (std::fclose(f) != 0 || !ok) {
+      ctx->err = "ostc_stat_export: write to " + path + " failed";
+      return OSTC_EIO;
+    }
+  }
+  return OSTC_OK;
+}
+
+int ostc_stat_import(ostc_ctx *ctx, const char *dir) {
+  if (!ctx || !dir) return OSTC_EINVAL;
+  if (!ctx->stat_on) {
+    ctx->err = "statistics collection is off (ostc_stat_enable, or if_collect_statistics in the setup)";
+    return OSTC_ESTATE;
+  }
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->stream));
+  // read and check all four files before touching the accumulators
+  std::vector<std::vector<double>> data(4 * ctx->blk.size());
+  int count = -1;
+  for (int g = 0; g < 4; ++g) {
+    const std::string path = std::string(dir) + "/" + kStatFiles[g];
+    FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) {
+      ctx->err = "ostc_stat_import: cannot open " + path;
+      return OSTC_EIO;
+    }
+    std::string why;
+    auto get_i = [&](int &v) { return std::fread(&v, 4, 1, f) == 1; };
+    const int nvar = stat_group_vars(ctx->stat_spec, g);
+    int nb = 0, nv = 0, ngg = 0;
+    if (!get_i(nb) || !get_i(nv) || !get_i(ngg)) why = "truncated header";
+    else if (nb != (int)ctx->blk.size() || nv != nvar || ngg != 1)
+      why = "header (n_block " + std::to_string(nb) + ", n_var " + std::to_string(nv) + ", ngg " +
+            std::to_string(ngg) + ") does not match the case and the enabled selection";
+    for (const auto &name : stat_names(ctx, g)) {
+      if (!why.empty()) break;
+      std::string got;
+      int c = 0;
+      while (get_i(c) && c != 0 && got.size() < 256) got.push_back((char)c);
+      if (got != name) why = "variable '" + got + "' where '" + name + "' was expected";
+    }
+    for (int v = 0; v < nvar && why.empty(); ++v) {
+      int c = 0;
+      if (!get_i(c)) why = "truncated counters";
+      else if (c < 0 || (count >= 0 && c != count)) why = "counters differ between variables or files";
+      else count = c;
+    }
+    for (size_t b = 0; b < ctx->blk.size() && why.empty(); ++b) {
+      const DevBlock &db = ctx->blk[b].db;
+      int mx = 0, my = 0, mz = 0;
+      if (!get_i(mx) || !get_i(my) || !get_i(mz)) why = "truncated block header";
+      else if (mx != db.mx || my != db.my || mz != db.mz)
+        why = "block " + std::to_string(b) + " extents differ from the case";
+      else {
+        auto &d = data[g * ctx->blk.size() + b];
+        d.resize((size_t)nvar * stat_points(db));
+        if (std::fread(d.data(), sizeof(double), d.size(), f) != d.size()) why = "truncated data";
+      }
+    }
+    std::fclose(f);
+    if (!why.empty()) {
+      ctx->err = "ostc_stat_import: " + path + ": " + why;
+      return OSTC_EIO;
+    }
+  }
+  for (size_t b = 0; b < ctx->blk.size(); ++b) {
+    long long off = 0;
+    const long long np = stat_points(ctx->blk[b].db);
+    for (int g = 0; g < 4; ++g) {
+      const auto &d = data[g * ctx->blk.size() + b];
+      CK(cudaMemcpy(ctx->blk[b].stat + off * np, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice));
+      off += stat_group_vars(ctx->stat_spec, g);
+    }
+  }
+  ctx->stat_count = count < 0 ? 0 : count;
+  // a continued collection (the reference's step index runs on across the restart): collect from the
+  // next step on
+  ctx->stat_steps = std::max<long long>(ctx->stat_steps, ctx->stat_start);
+  return OSTC_OK;
 }
 
 int ostc_error_flags(ostc_ctx *ctx, unsigned *flags) {
@@ -3119,7 +3432,13 @@ int ostc_profile_steps(ostc_ctx *ctx, int n_steps, int max, const char **names, 
   ctx->fams.clear();
   ctx->ev_used.clear();
   ctx->timing = true;
-  for (int s = 0; s < n_steps; ++s) enqueue_step_any(ctx);
+  for (int s = 0; s < n_steps; ++s) {
+    enqueue_step_any(ctx);
+    if (int r = stat_after_step(ctx)) {
+      ctx->timing = false;
+      return r;
+    }
+  }
   ctx->timing = false;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));

@@ -272,6 +272,18 @@ __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL, 4) k_fvs
       al[l] = gamma * T(kRuD) / (T)c_mix.mw[l] * tm - (gamma - 1) * hi[l];
       al[l] *= c2i;
     }
+    // The species columns of the five flow rows of L are cs_l * al[q] (cs = 1/2, -kx, -ky, -kz, 1/2):
+    // their products with the split fluxes share one sum per stencil node, formed once for all rows.
+    T sp[7], sm[7];
+    for (int m = 0; m < 7; ++m) {
+      T a = 0, bq = 0;
+      for (int q = 0; q < ns; ++q) {
+        a += al[q] * FP(m, 5 + q);
+        bq += al[q] * FM(m + 1, 5 + q);
+      }
+      sp[m] = a;
+      sm[m] = bq;
+    }
     T fch[Spec<NS>::A + 5];
     for (int l = 0; l < 5; ++l) {
       T cs = half, L[5];
@@ -316,12 +328,8 @@ __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL, 4) k_fvs
           a += L[q] * FP(m, q);
           bq += L[q] * FM(m + 1, q);
         }
-        for (int q = 0; q < ns; ++q) {
-          a += cs * al[q] * FP(m, 5 + q);
-          bq += cs * al[q] * FM(m + 1, 5 + q);
-        }
-        vp[m] = a;
-        vmn[m] = bq;
+        vp[m] = a + cs * sp[m];
+        vmn[m] = bq + cs * sm[m];
       }
       fch[l] = fvs_weno7(vp, vmn, eps);
     }

@@ -19,6 +19,8 @@ PREC_FP64, PREC_MIXED = 0, 1
 TERM_INVISCID, TERM_VISCOUS, TERM_SOURCE, TERM_ALL = 1, 2, 4, 7
 FLAG_NONPOSITIVE, FLAG_NAN = 1, 2
 CHEM_EXPLICIT, CHEM_POINT_IMPLICIT = 0, 1
+STAT_REY_U, STAT_REY_V, STAT_REY_W, STAT_REY_T, STAT_RHO_P = 1, 2, 4, 8, 16
+STAT_GROUPS = ("reynolds_1st", "favre_1st", "reynolds_2nd", "favre_2nd")
 
 EXPORTS = [
     "ostc_create", "ostc_destroy", "ostc_last_error", "ostc_n_blocks", "ostc_block_dims", "ostc_n_var",
@@ -27,7 +29,8 @@ EXPORTS = [
     "ostc_device_view", "ostc_profile_steps", "ostc_total_nodes", "ostc_probe_case", "ostc_timed_steps",
     "ostc_step_kernel_count", "ostc_residual_noalloc", "ostc_set_chem_mode", "ostc_set_conservative",
     "ostc_rhs_vjp", "ostc_rk3_step_vjp", "ostc_adjoint_steps", "ostc_run_states", "ostc_bounds_flags",
-    "ostc_bounds_checked",
+    "ostc_bounds_checked", "ostc_stat_enable", "ostc_stat_disable", "ostc_stat_info", "ostc_stat_get",
+    "ostc_stat_export", "ostc_stat_import",
 ]
 
 
@@ -78,6 +81,12 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.ostc_run_states.argtypes = [vp, ip, vp, vp, vp, vp, ip]
     lib.ostc_bounds_flags.argtypes = [vp, ctypes.POINTER(ctypes.c_uint)]
     lib.ostc_bounds_checked.argtypes = []
+    lib.ostc_stat_enable.argtypes = [vp, ip, ctypes.c_uint]
+    lib.ostc_stat_disable.argtypes = [vp]
+    lib.ostc_stat_info.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ctypes.c_longlong)]
+    lib.ostc_stat_get.argtypes = [vp, ip, ip, vp, ip]
+    lib.ostc_stat_export.argtypes = [vp, ctypes.c_char_p]
+    lib.ostc_stat_import.argtypes = [vp, ctypes.c_char_p]
     lib.ostc_rk3_step.argtypes = [vp, ip, dp]
     lib.ostc_physical_time.argtypes = [vp, dp]
     lib.ostc_store_residual_reference.argtypes = [vp]
@@ -235,6 +244,38 @@ class Solver:
                             None if svi is None else [x.ctypes.data for x in svi],
                             None if svo is None else [x.ctypes.data for x in svo])
         return list(zip(bvo, svo if svo is not None else [None] * len(bvo)))
+
+    # ---- single-point statistics (SinglePointStat)
+    def stat_enable(self, start_step: int = 0, flags: int = 0):
+        """Zero the accumulators and collect after every later step whose index (from this call,
+        1-based) exceeds start_step; flags: STAT_REY_* extras and STAT_RHO_P."""
+        self._check(self.lib.ostc_stat_enable(self.h, start_step, flags))
+
+    def stat_disable(self):
+        self._check(self.lib.ostc_stat_disable(self.h))
+
+    def stat_info(self):
+        """(variables per group, collections, steps since enabling)."""
+        nv = (ctypes.c_int * 4)()
+        nc = ctypes.c_int()
+        st = ctypes.c_longlong()
+        self._check(self.lib.ostc_stat_info(self.h, nv, ctypes.byref(nc), ctypes.byref(st)))
+        return list(nv), nc.value, st.value
+
+    def stat_get(self, group: int, block: int = 0) -> np.ndarray:
+        """Sums of group (0 Reynolds 1st, 1 Favre 1st, 2 Reynolds 2nd, 3 Favre 2nd) of block:
+        [n_var, mz + 2, my + 2, mx + 2], one ghost layer on every side."""
+        nv = self.stat_info()[0][group]
+        mz, my, mx = self.shape(block)
+        out = np.empty((nv, mz + 2, my + 2, mx + 2))
+        self._check(self.lib.ostc_stat_get(self.h, block, group, out.ctypes.data, OSTC_HOST))
+        return out
+
+    def stat_export(self, directory: str):
+        self._check(self.lib.ostc_stat_export(self.h, str(directory).encode()))
+
+    def stat_import(self, directory: str):
+        self._check(self.lib.ostc_stat_import(self.h, str(directory).encode()))
 
     def bounds_flags(self) -> int:
         """Index-bounds flags of the bounds-checked build (read and cleared; 0 in the regular build)."""

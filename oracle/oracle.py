@@ -114,6 +114,7 @@ def load():
         lib.orc_rhs.argtypes = [vp, ctypes.c_uint, dp]
         lib.orc_step.argtypes = [vp, ctypes.c_int]
         lib.orc_step.restype = ctypes.c_double
+        lib.orc_stat_collect.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int, dp]
         lib.orc_time.argtypes = [vp]
         lib.orc_time.restype = ctypes.c_double
         lib.orc_dt.argtypes = [vp]
@@ -237,6 +238,13 @@ class Oracle:
     def step(self, n: int = 1) -> float:
         return self.lib.orc_step(self.h, n)
 
+    def stat_collect(self, acc: np.ndarray, rey_idx=(), rho_p: bool = False):
+        """Add one single-point statistics collection of the current state to acc (float64,
+        C-contiguous, the four groups [n_var][mz+2][my+2][mx+2] back to back; orc_stat_collect)."""
+        assert acc.dtype == np.float64 and acc.flags.c_contiguous
+        idx = (ctypes.c_int * max(1, len(rey_idx)))(*rey_idx)
+        self.lib.orc_stat_collect(self.h, len(rey_idx), idx, int(rho_p), _dp(acc))
+
     def time(self) -> float:
         return self.lib.orc_time(self.h)
 
@@ -251,6 +259,7 @@ class _BlockView:
         self.lib, self.h, self.shape, self.n_spec = lib, h, shape, n_spec
 
     get_state = Oracle.get_state
+    stat_collect = Oracle.stat_collect
     metric = Oracle.metric
     mixture = Oracle.mixture
     time = Oracle.time

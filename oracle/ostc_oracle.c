@@ -2045,6 +2045,49 @@ double orc_step(orc_ctx *o, int n) {
   return dt;
 }
 
+/* ---------------------------------------------------------------- single-point statistics */
+
+/* collect_single_point_basic_statistics (SinglePointStat.cu:641-706): one collection added to acc,
+ * laid out as four groups [n_var][mz+2][my+2][mx+2] back to back (Reynolds 1st: rho, p, extras by
+ * primitive index; Favre 1st: rho u, rho v, rho w, rho T, rho Y_k; Reynolds 2nd: rho rho, p p
+ * [, rho p]; Favre 2nd: rho u u, rho v v, rho w w, rho u v, rho u w, rho v w, rho T T, rho Y_k Y_k).
+ * Nodes i = -1..mx, j = -1..my, k = -1..mz, read from the ghost layers as they stand after the
+ * step (2-D blocks: the k layers eliminate_k copied from k = 0). */
+void orc_stat_collect(const orc_ctx *o, int n_rey, const int *rey_idx, int rho_p, double *acc) {
+  const long P = o->P;
+  const int nx = o->mx + 2, ny = o->my + 2, nz = o->mz + 2;
+  const long np = (long)nx * ny * nz;
+  double *rey1 = acc, *fav1 = rey1 + (2 + n_rey) * np, *rey2 = fav1 + (4 + o->ns) * np;
+  double *fav2 = rey2 + (2 + rho_p) * np;
+  for (int k = -1; k <= o->mz; ++k)
+    for (int j = -1; j <= o->my; ++j)
+      for (int i = -1; i <= o->mx; ++i) {
+        const long n = (((long)(k + 1) * ny) + (j + 1)) * nx + (i + 1);
+        const long p = ID(o, i, j, k);
+        const double rho = o->bv[p], u = o->bv[P + p], v = o->bv[2 * P + p], w = o->bv[3 * P + p];
+        const double pr = o->bv[4 * P + p], T = o->bv[5 * P + p];
+        rey1[n] += rho;
+        rey1[np + n] += pr;
+        for (int l = 0; l < n_rey; ++l) rey1[(2 + l) * np + n] += o->bv[rey_idx[l] * P + p];
+        fav1[n] += rho * u;
+        fav1[np + n] += rho * v;
+        fav1[2 * np + n] += rho * w;
+        fav1[3 * np + n] += rho * T;
+        for (int l = 0; l < o->ns; ++l) fav1[(4 + l) * np + n] += rho * o->sv[l * P + p];
+        rey2[n] += rho * rho;
+        rey2[np + n] += pr * pr;
+        if (rho_p) rey2[2 * np + n] += rho * pr;
+        fav2[n] += rho * u * u;
+        fav2[np + n] += rho * v * v;
+        fav2[2 * np + n] += rho * w * w;
+        fav2[3 * np + n] += rho * u * v;
+        fav2[4 * np + n] += rho * u * w;
+        fav2[5 * np + n] += rho * v * w;
+        fav2[6 * np + n] += rho * T * T;
+        for (int l = 0; l < o->ns; ++l) fav2[(7 + l) * np + n] += rho * o->sv[l * P + p] * o->sv[l * P + p];
+      }
+}
+
 /* ---------------------------------------------------------------- multi-block (interfaces) */
 
 typedef struct {

@@ -98,6 +98,8 @@ void orc_get_metric(const orc_ctx *o, double *metric9, double *jac);
 void orc_rhs(orc_ctx *o, unsigned mask, double *dq);
 /* n full SSP-RK3 steps (RK.cuh:85-185).  Returns the last dt. */
 double orc_step(orc_ctx *o, int n);
+/* one single-point statistics collection added to acc (collect_single_point_basic_statistics) */
+void orc_stat_collect(const orc_ctx *o, int n_rey, const int *rey_idx, int rho_p, double *acc);
 double orc_time(const orc_ctx *o);
 /* Local CFL time step of the current state and its minimum (TimeAdvanceFunc.cuh:28-83). */
 double orc_dt(orc_ctx *o);

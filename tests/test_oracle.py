@@ -111,3 +111,36 @@ def test_ssprk3_third_order(built):
     e = [np.abs(run(n) - ref)[2].max() for n in (8, 16)]
     rate = math.log2(e[0] / e[1])
     assert 2.6 < rate < 3.6, (e, rate)
+
+
+def test_stat_collect_interior_formula(built):
+    """orc_stat_collect (collect_single_point_basic_statistics, SinglePointStat.cu:641-706) on the
+    interior nodes: twice the per-node products of the current primitive state, in the documented
+    group layout, for a mixture with every optional variable."""
+    case = oc.reacting_mixing_layer_3d(mx=10, my=8, mz=6)
+    o = Oracle(case)
+    o.set_state(case.bv, case.sv)
+    o.step(1)
+    _, bv, _ = o.get_state()
+    sv = o.mixture()["sv"]
+    ns = sv.shape[0]
+    rey, rho_p = [1, 2, 3, 5], True
+    n_var = [2 + len(rey), 4 + ns, 3, 7 + ns]
+    shape = (case.mz + 2, case.my + 2, case.mx + 2)
+    acc = np.zeros(sum(n_var) * int(np.prod(shape)))
+    o.stat_collect(acc, rey, rho_p)
+    o.stat_collect(acc, rey, rho_p)
+    groups, off = [], 0
+    for nv in n_var:
+        groups.append(acc[off:off + nv * int(np.prod(shape))].reshape((nv,) + shape)[:, 1:-1, 1:-1, 1:-1])
+        off += nv * int(np.prod(shape))
+    rho, u, v, w, p, t = bv
+    want = [[rho, p] + [bv[q] for q in rey],
+            [rho * u, rho * v, rho * w, rho * t] + [rho * y for y in sv],
+            [rho * rho, p * p, rho * p],
+            [rho * u * u, rho * v * v, rho * w * w, rho * u * v, rho * u * w, rho * v * w, rho * t * t] +
+            [rho * y * y for y in sv]]
+    for g in range(4):
+        assert groups[g].shape[0] == len(want[g])
+        for l, x in enumerate(want[g]):
+            assert np.array_equal(groups[g][l], 2 * x), (g, l)
