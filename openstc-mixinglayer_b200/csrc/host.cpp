@@ -876,10 +876,37 @@ bool resolve_boundaries(const Setup &s, const Derived &d, HostMesh &mesh, std::s
     for (auto &f : B.faces) {
       auto it = lab.find(f.label);
       f.type = it != lab.end() ? it->second.first : f.label;
-      if (f.type != kSymmetry && f.type != kFarfield && f.type != kOutflow && f.type != kPeriodic) {
+      if (f.type != kSymmetry && f.type != kFarfield && f.type != kOutflow && f.type != kPeriodic &&
+          f.type != kWall) {
         err = "boundary label " + std::to_string(f.label) +
-              " maps to a type outside this path (supported: symmetry 3, farfield 4, outflow 6, periodic 8)";
+              " maps to a type outside this path (supported: wall 2, symmetry 3, farfield 4, outflow 6, periodic 8)";
         return false;
+      }
+      if (f.type == kWall) {
+        // Wall::Wall (BoundCond.cpp:497-560): isothermal (default, 300 K) or adiabatic; the radiative
+        // wall needs wall distances and the blowing / fluctuating walls their forcing, neither on
+        // this path
+        f.temperature = 300.0;
+        f.wall_adiabatic = 0;
+        if (it != lab.end()) {
+          const auto &st = s.structs.at(it->second.second);
+          auto tt = st.find("thermal_type");
+          const std::string th = tt == st.end() ? "isothermal" : std::get<std::string>(tt->second);
+          if (th == "adiabatic") {
+            f.wall_adiabatic = 1;
+          } else if (th == "equilibrium_radiation") {
+            err = "wall label " + std::to_string(f.label) +
+                  ": thermal_type equilibrium_radiation is not provided (isothermal and adiabatic are)";
+            return false;
+          }
+          f.temperature = struct_real(st, "temperature", 300.0);
+          auto fl = st.find("fluctuation_type");
+          if (fl != st.end() && std::holds_alternative<int>(fl->second) && std::get<int>(fl->second) != 0) {
+            err = "wall label " + std::to_string(f.label) + ": wall fluctuations (fluctuation_type) are not provided";
+            return false;
+          }
+        }
+        continue;
       }
       if (f.type == kFarfield && d.species != 0) {
         err = "far-field faces (label " + std::to_string(f.label) +

@@ -88,6 +88,7 @@ struct BcFace {
   // far-field state (FarField ctor, BoundCond.cpp:586-669), air only on this path
   double density = 0, u = 0, v = 0, w = 0, pressure = 0, temperature = 0;
   double acoustic_speed = 0, gamma = kGammaAir, entropy = 0, mw = kMwAir;
+  int wall_adiabatic = 0;  // walls: 1 adiabatic, 0 isothermal at `temperature` (Wall, BoundCond.h:87-112)
 };
 
 // One 1:1 block interface after InnerFace::register_boundary (Mesh.cpp:34-176): the node range of

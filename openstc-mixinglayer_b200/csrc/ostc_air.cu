@@ -77,6 +77,7 @@ struct DevState {
 struct DevFace {
   int type, face, direction, rs[3], re[3];
   double density, u, v, w, pressure, temperature, acoustic_speed, gamma, entropy;
+  int wall_adiabatic;  // walls: 1 adiabatic, 0 isothermal at `temperature`
 };
 
 struct FillVals {
@@ -966,6 +967,54 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
       for (int g = 1; g <= b.g; ++g) {
         const long long pg = pb + g * dstep;
         copy_bv(b, s, pg, pb);
+        finish_node(b, s, pg);
+      }
+    } else if (f.type == kWall) {
+      // apply_wall (BoundCond.cuh:1024-1270), no-slip, isothermal or adiabatic: the wall node takes
+      // the first interior node's pressure (and mass fractions) at the wall temperature; ghost g
+      // mirrors interior node g with reversed velocity and, isothermal, T_g = 2 T_w - T_in (T_w
+      // where that falls to 0.1 T_w or below)
+      const long long pin = pb - dstep;
+      const double tw = f.wall_adiabatic ? s.bv[5 * P + pin] : f.temperature;
+      const double pw = s.bv[4 * P + pin];
+      double mw = kMwD;
+      if (s.sv) {
+        double imw = 0;
+        for (int l = 0; l < c_mix.ns; ++l) {
+          s.sv[l * P + pb] = s.sv[l * P + pin];
+          imw += s.sv[l * P + pb] / c_mix.mw[l];
+        }
+        mw = 1 / imw;
+      }
+      s.bv[pb] = pw * mw / (tw * kRuD);
+      s.bv[P + pb] = 0;
+      s.bv[2 * P + pb] = 0;
+      s.bv[3 * P + pb] = 0;
+      s.bv[4 * P + pb] = pw;
+      s.bv[5 * P + pb] = tw;
+      finish_node(b, s, pb);
+      for (int g = 1; g <= b.g; ++g) {
+        const long long pi = pb - g * dstep, pg = pb + g * dstep;
+        const double p_i = s.bv[4 * P + pi], t_i = s.bv[5 * P + pi];
+        double t_g = t_i;
+        if (!f.wall_adiabatic) {
+          t_g = 2 * tw - t_i;
+          if (t_g <= 0.1 * tw) t_g = tw;
+        }
+        if (s.sv) {
+          double imw = 0;
+          for (int l = 0; l < c_mix.ns; ++l) {
+            s.sv[l * P + pg] = s.sv[l * P + pi];
+            imw += s.sv[l * P + pg] / c_mix.mw[l];
+          }
+          mw = 1 / imw;
+        }
+        s.bv[pg] = p_i * mw / (t_g * kRuD);
+        s.bv[P + pg] = -s.bv[P + pi];
+        s.bv[2 * P + pg] = -s.bv[2 * P + pi];
+        s.bv[3 * P + pg] = -s.bv[3 * P + pi];
+        s.bv[4 * P + pg] = p_i;
+        s.bv[5 * P + pg] = t_g;
         finish_node(b, s, pg);
       }
     } else if (f.type == kPeriodic) {
@@ -2426,6 +2475,7 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
       f.acoustic_speed = hf.acoustic_speed;
       f.gamma = hf.gamma;
       f.entropy = hf.entropy;
+      f.wall_adiabatic = hf.wall_adiabatic;
       R.faces.push_back(f);
     }
     for (auto &hi : HB.inner) {

@@ -191,8 +191,20 @@ class Case:
         v_inf = c if abs(vel) < 1 else vel
         return rho * vel * rho * vel if abs(vel) >= 1 else rho * c * rho * c, v_inf
 
+    def wall_states(self):
+        """Wall ctor (BoundCond.cpp:497-560): label -> isothermal wall temperature (300 K by default)
+        and the adiabatic flag."""
+        out = {}
+        for st in self.bc_structs.values():
+            if st.get("type", (None, None))[1] != "wall":
+                continue
+            g = {k: v for k, (t, v) in st.items()}
+            out[g["label"]] = dict(temperature=float(g.get("temperature", 300.0)),
+                                   wall_adiabatic=int(g.get("thermal_type", "isothermal") == "adiabatic"))
+        return out
+
     def label_types(self):
-        types = {"symmetry": 3, "farfield": 4, "outflow": 6, "periodic": 8}
+        types = {"wall": 2, "symmetry": 3, "farfield": 4, "outflow": 6, "periodic": 8}
         m = {}
         for st in self.bc_structs.values():
             m[st["label"][1]] = types[st["type"][1]]
@@ -330,6 +342,9 @@ class MultiCase:
     def label_types(self):
         return Case.label_types(self)
 
+    def wall_states(self):
+        return Case.wall_states(self)
+
     def reference_scales(self):
         return Case.reference_scales(self)
 
@@ -461,6 +476,14 @@ def multiblock_mixing_layer_3d(nb=12, lo=32, hi=256, my=None, mz=None, seed=0, s
                      freestream=dict(mach=mc, pressure=p0, temperature=t0))
 
 
+def _wall_struct(thermal, t_wall):
+    """No-slip wall struct (label 2): isothermal at t_wall, or adiabatic."""
+    st = {"type": ("string", "wall"), "label": ("int", 2), "thermal_type": ("string", thermal)}
+    if thermal == "isothermal":
+        st["temperature"] = ("real", float(t_wall))
+    return st
+
+
 def _box_faces(mx, my, mz, xlab, ylab_lo, ylab_hi, zlab):
     f = [Face((0, 0, 0, my - 1, 0, mz - 1), xlab), Face((mx - 1, mx - 1, 0, my - 1, 0, mz - 1), xlab),
          Face((0, mx - 1, 0, 0, 0, mz - 1), ylab_lo), Face((0, mx - 1, my - 1, my - 1, 0, mz - 1), ylab_hi)]
@@ -470,7 +493,8 @@ def _box_faces(mx, my, mz, xlab, ylab_lo, ylab_hi, zlab):
 
 
 def mixing_layer_2d(mx=257, my=129, seed=0, steps=100, mc=0.4, re=1000.0, t0=300.0, delta0=1e-3,
-                    reconstruction=4, inviscid_scheme=3, cfl=0.5, entropy_fix_factor=0.125) -> Case:
+                    reconstruction=4, inviscid_scheme=3, cfl=0.5, entropy_fix_factor=0.125, ybc="symmetry",
+                    wall_thermal="isothermal") -> Case:
     """2-D temporal mixing layer: 256 x 128 cells on 2*pi x pi (node-coincident periodic x, mx = 257),
     u = dU/2 tanh(2y/delta0), Mc = dU/(2c), Re = rho dU delta0 / mu(T) , T and p uniform, and
     v' = 1e-3 dU sum_{m=1..8} a_m cos(m x + phi_m) exp(-(y/delta0)^2), a_m = 1/8, phi_m ~ U[0,2pi)."""
@@ -496,9 +520,13 @@ def mixing_layer_2d(mx=257, my=129, seed=0, steps=100, mc=0.4, re=1000.0, t0=300
     bv[3] = 0.0
     bv[4] = p0
     bv[5] = t0
-    faces = _box_faces(mx, my, 1, 8, 3, 3, 8)
-    structs = {"slipwall": {"type": ("string", "symmetry"), "label": ("int", 3)},
-               "periodic": {"type": ("string", "periodic"), "label": ("int", 8)}}
+    if ybc == "wall":
+        faces = _box_faces(mx, my, 1, 8, 2, 2, 8)
+        structs = {"wall": _wall_struct(wall_thermal, t0), "periodic": {"type": ("string", "periodic"), "label": ("int", 8)}}
+    else:
+        faces = _box_faces(mx, my, 1, 8, 3, 3, 8)
+        structs = {"slipwall": {"type": ("string", "symmetry"), "label": ("int", 3)},
+                   "periodic": {"type": ("string", "periodic"), "label": ("int", 8)}}
     scheme = dict(reconstruction=reconstruction, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=cfl,
                   prandtl_number=0.72, limiter=0, entropy_fix_factor=entropy_fix_factor)
     return Case("mixing_layer_2d", mx, my, 1, x, y, z, delta0, faces, structs, scheme, bv, steps)
@@ -506,7 +534,7 @@ def mixing_layer_2d(mx=257, my=129, seed=0, steps=100, mc=0.4, re=1000.0, t0=300
 
 def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0, t0=300.0, delta0=1e-3,
                     h=0.125, reconstruction=5, inviscid_scheme=4, cfl=0.5, ybc="farfield",
-                    entropy_fix_factor=0.125) -> Case:
+                    entropy_fix_factor=0.125, wall_thermal="isothermal") -> Case:
     """3-D temporal mixing layer: uniform spacing h*delta0, periodic x and z (node-coincident),
     far-field (Riemann-invariant, label 4/41) or outflow (label 6) y faces; u = dU/2 tanh(2y/delta0),
     Mc = 0.7, plus 1e-2 dU N(0,1) exp(-(y/delta0)^2) seeded white noise in u, v, w."""
@@ -536,6 +564,10 @@ def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0
                    "farfield_lower": {"type": ("string", "farfield"), "label": ("int", 41), "mach": ("real", mc),
                                       "pressure": ("real", p0), "temperature": ("real", t0), "u": ("real", -1.0),
                                       "v": ("real", 0.0), "w": ("real", 0.0)}}
+    elif ybc == "wall":
+        faces = _box_faces(mx, my, mz, 8, 2, 2, 8)
+        structs = {"periodic": {"type": ("string", "periodic"), "label": ("int", 8)},
+                   "wall": _wall_struct(wall_thermal, t0)}
     else:
         faces = _box_faces(mx, my, mz, 8, 6, 6, 8)
         structs = {"periodic": {"type": ("string", "periodic"), "label": ("int", 8)},
@@ -550,7 +582,7 @@ CHEM_FIXTURE = Path(__file__).resolve().parents[2] / "tests" / "golden" / "chem"
 
 def reacting_mixing_layer_3d(mx=384, my=192, mz=96, seed=0, steps=100, h=0.125, delta0=1e-3, mc=0.4,
                              p0=101325.0, inviscid_scheme=72, finite_rate=True, ybc="outflow",
-                             chem_dir=None, fuel=None, oxidiser=None) -> Case:
+                             chem_dir=None, fuel=None, oxidiser=None, wall_thermal="isothermal") -> Case:
     """Reacting H2/air temporal mixing layer (9 species, 19 reactions after merging duplicates):
     fuel Y_H2 = 0.05 in N2 at 300 K (y > 0) over vitiated air at 1500 K (y < 0): Y_O2 = 0.20, Y_H2O = 0.10,
     radicals Y_OH = 1e-3, Y_O = 1e-4, Y_H = 1e-5, Y_HO2 = 1e-6, Y_H2O2 = 1e-7 (so that every reaction
@@ -593,11 +625,16 @@ def reacting_mixing_layer_3d(mx=384, my=192, mz=96, seed=0, steps=100, h=0.125, 
     bv[3] = 1e-2 * du * rng.standard_normal(X.shape) * env
     bv[4] = p0
     bv[5] = T
-    if ybc != "outflow":
-        raise ValueError("the reacting case uses outflow y faces")
-    faces = _box_faces(mx, my, mz, 8, 6, 6, 8)
-    structs = {"periodic": {"type": ("string", "periodic"), "label": ("int", 8)},
-               "outflow": {"type": ("string", "outflow"), "label": ("int", 6)}}
+    if ybc == "wall":
+        faces = _box_faces(mx, my, mz, 8, 2, 2, 8)
+        structs = {"periodic": {"type": ("string", "periodic"), "label": ("int", 8)},
+                   "wall": _wall_struct(wall_thermal, 300.0)}
+    elif ybc == "outflow":
+        faces = _box_faces(mx, my, mz, 8, 6, 6, 8)
+        structs = {"periodic": {"type": ("string", "periodic"), "label": ("int", 8)},
+                   "outflow": {"type": ("string", "outflow"), "label": ("int", 6)}}
+    else:
+        raise ValueError("the reacting case uses outflow or wall y faces")
     scheme = dict(reconstruction=2, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=0.5, prandtl_number=0.72,
                   limiter=0, entropy_fix_factor=0.125)
     mixture = dict(tables=tb, finite_rate=finite_rate, chem_dir=str(chem_dir), mechanism="H2_mech.inp",

@@ -27,6 +27,7 @@ typedef struct {
   int type, face, direction;
   int rs[3], re[3];
   double density, u, v, w, pressure, temperature, acoustic_speed, gamma, entropy, mw;
+  int wall_adiabatic;
 } face_t;
 
 struct orc_ctx {
@@ -264,6 +265,7 @@ static void register_face(orc_ctx *o, const orc_face_in *in, face_t *f) {
   f->density = in->density; f->u = in->u; f->v = in->v; f->w = in->w;
   f->pressure = in->pressure; f->temperature = in->temperature;
   f->acoustic_speed = in->acoustic_speed; f->gamma = in->gamma; f->entropy = in->entropy; f->mw = in->mw;
+  f->wall_adiabatic = in->wall_adiabatic;
 }
 
 /* ---------------------------------------------------------------- pointwise helpers */
@@ -1653,6 +1655,57 @@ static void bc_outflow(orc_ctx *o, const face_t *f) {
         }
 }
 
+/* mixture molecular weight of node p from its mass fractions */
+static double node_mw(const orc_ctx *o, long p) {
+  if (!o->ns) return MW_AIR;
+  double s = 0;
+  for (int l = 0; l < o->ns; ++l) s += o->sv[l * o->P + p] / o->c.chem->mw[l];
+  return 1 / s;
+}
+
+/* apply_wall (BoundCond.cuh:1024-1270) without blowing or fluctuations: the wall node gets the first
+ * interior node's p (and Y), T_w (isothermal) or that node's T (adiabatic), zero velocity; ghost g
+ * mirrors interior node g: p and Y copied, velocity reversed, T_g = 2 T_w - T_in (isothermal; T_w
+ * when that is <= 0.1 T_w) or T_in (adiabatic), rho from the equation of state. */
+static void bc_wall(orc_ctx *o, const face_t *f) {
+  const long P = o->P;
+  int dir[3] = {0, 0, 0};
+  dir[f->face] = f->direction;
+  for (int i = f->rs[0]; i <= f->re[0]; ++i)
+    for (int j = f->rs[1]; j <= f->re[1]; ++j)
+      for (int k = f->rs[2]; k <= f->re[2]; ++k) {
+        const long pb = ID(o, i, j, k), pin = ID(o, i - dir[0], j - dir[1], k - dir[2]);
+        const double tw = f->wall_adiabatic ? o->bv[5 * P + pin] : f->temperature;
+        const double pw = o->bv[4 * P + pin];
+        for (int l = 0; l < o->ns; ++l) o->sv[l * P + pb] = o->sv[l * P + pin];
+        o->bv[pb] = pw * node_mw(o, pb) / (tw * R_U);
+        o->bv[P + pb] = 0;
+        o->bv[2 * P + pb] = 0;
+        o->bv[3 * P + pb] = 0;
+        o->bv[4 * P + pb] = pw;
+        o->bv[5 * P + pb] = tw;
+        cv_from_bv(o, pb);
+        for (int g = 1; g <= o->g; ++g) {
+          const long pi = ID(o, i - g * dir[0], j - g * dir[1], k - g * dir[2]);
+          const long pg = ID(o, i + g * dir[0], j + g * dir[1], k + g * dir[2]);
+          const double p_i = o->bv[4 * P + pi], t_i = o->bv[5 * P + pi];
+          double t_g = t_i;
+          if (!f->wall_adiabatic) {
+            t_g = 2 * tw - t_i;
+            if (t_g <= 0.1 * tw) t_g = tw;
+          }
+          for (int l = 0; l < o->ns; ++l) o->sv[l * P + pg] = o->sv[l * P + pi];
+          o->bv[pg] = p_i * node_mw(o, pg) / (t_g * R_U);
+          o->bv[P + pg] = -o->bv[P + pi];
+          o->bv[2 * P + pg] = -o->bv[2 * P + pi];
+          o->bv[3 * P + pg] = -o->bv[3 * P + pi];
+          o->bv[4 * P + pg] = p_i;
+          o->bv[5 * P + pg] = t_g;
+          cv_from_bv(o, pg);
+        }
+      }
+}
+
 /* apply_periodic (BoundCond.cuh:1443-1486): node-coincident, ghost mx-1+g <- interior g. */
 static void bc_periodic(orc_ctx *o, const face_t *f) {
   int dir[3] = {0, 0, 0};
@@ -1739,8 +1792,9 @@ static void bc_farfield(orc_ctx *o, const face_t *f) {
 /* DBoundCond::apply_boundary_conditions priority order (BoundCond.cuh:1488-1679):
  * farfield, outflow, symmetry, periodic (other types are not on this path). */
 static void apply_bcs(orc_ctx *o) {
-  const int order[4] = {ORC_FARFIELD, ORC_OUTFLOW, ORC_SYMMETRY, ORC_PERIODIC};
-  for (int t = 0; t < 4; ++t)
+  /* priority order of DBoundCond::apply_boundary_conditions (BoundCond.cuh:1488-1679) */
+  const int order[5] = {ORC_FARFIELD, ORC_OUTFLOW, ORC_SYMMETRY, ORC_WALL, ORC_PERIODIC};
+  for (int t = 0; t < 5; ++t)
     for (int n = 0; n < o->nf; ++n) {
       const face_t *f = &o->f[n];
       if (f->type != order[t]) continue;
@@ -1749,6 +1803,7 @@ static void apply_bcs(orc_ctx *o) {
         case ORC_OUTFLOW: bc_outflow(o, f); break;
         case ORC_SYMMETRY: bc_symmetry(o, f); break;
         case ORC_PERIODIC: bc_periodic(o, f); break;
+        case ORC_WALL: bc_wall(o, f); break;
       }
     }
 }

@@ -16,13 +16,15 @@ extern "C" {
 #endif
 
 /* Boundary type codes follow the reference labels (BoundCond.cu:232-258). */
-enum { ORC_SYMMETRY = 3, ORC_FARFIELD = 4, ORC_OUTFLOW = 6, ORC_PERIODIC = 8 };
+enum { ORC_WALL = 2, ORC_SYMMETRY = 3, ORC_FARFIELD = 4, ORC_OUTFLOW = 6, ORC_PERIODIC = 8 };
 
 typedef struct {
   int type;          /* ORC_* */
   int raw[6];        /* x1 x2 y1 y2 z1 z2 exactly as in "boundary   0.txt" (0-based node indices) */
   /* farfield state (used when type == ORC_FARFIELD), FarField ctor BoundCond.cpp:586-669 */
   double density, u, v, w, pressure, temperature, acoustic_speed, gamma, entropy, mw;
+  /* walls (type == ORC_WALL, Wall ctor BoundCond.cpp:497-560): 1 adiabatic, 0 isothermal at temperature */
+  int wall_adiabatic;
 } orc_face_in;
 
 /* Mixture tables (Species / Reaction, ChemData.cpp; DParameter.cu:57-155), row-major [i][j]. */

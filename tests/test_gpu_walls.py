@@ -1,0 +1,71 @@
+"""No-slip walls (apply_wall, BoundCond.cuh:1024-1270: isothermal or adiabatic, no blowing or
+fluctuation) on the GPU against the oracle, through the C ABI: RK3 trajectories of air (3-D and 2-D)
+and of the 9-species mixture with both y faces walls, 1e-12 relative per conserved variable as the
+other trajectory tests.
+"""
+import numpy as np
+import pytest
+
+import ostc
+import ostc_cases as oc
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def _run(case, tmp_path, steps, mixture=False):
+    d = oc.write_case(case, tmp_path / case.name)
+    s = ostc.Solver(str(d))
+    o = Oracle(case)
+    if mixture:
+        s.set_state(case.bv, sv=case.sv)
+        o.set_state(case.bv, case.sv)
+    else:
+        s.set_state(case.bv)
+        o.set_state(case.bv)
+    s.step(steps)
+    o.step(steps)
+    cg, bg = s.get_state()
+    co, bo, _ = o.get_state()
+    err = oc.relative_errors(cg, co)
+    assert all(m < TOL and l2 < TOL for m, l2 in err), err
+    assert s.error_flags() == 0
+    return bg
+
+
+@pytest.mark.parametrize("thermal", ["isothermal", "adiabatic"])
+def test_wall_air_3d(built, tmp_path, thermal):
+    case = oc.mixing_layer_3d(mx=32, my=24, mz=16, ybc="wall", wall_thermal=thermal)
+    bg = _run(case, tmp_path, 10)
+    assert np.all(bg[1:4, :, 0, :] == 0) and np.all(bg[1:4, :, -1, :] == 0)
+    if thermal == "isothermal":
+        assert np.all(bg[5, :, 0, :] == 300.0)
+
+
+@pytest.mark.parametrize("thermal,recon,rs", [("isothermal", 4, 3), ("adiabatic", 5, 4)])
+def test_wall_air_2d(built, tmp_path, thermal, recon, rs):
+    case = oc.mixing_layer_2d(mx=65, my=33, reconstruction=recon, inviscid_scheme=rs, ybc="wall",
+                              wall_thermal=thermal)
+    _run(case, tmp_path, 20)
+
+
+def test_wall_mixture(built, tmp_path):
+    case = oc.reacting_mixing_layer_3d(mx=20, my=16, mz=10, ybc="wall")
+    bg = _run(case, tmp_path, 3, mixture=True)
+    assert np.all(bg[5, :, 0, :] == 300.0)
+
+
+def test_wall_rejections(built, tmp_path):
+    """The radiative wall and the fluctuating walls are refused with the reason."""
+    case = oc.mixing_layer_3d(mx=16, my=12, mz=8, ybc="wall")
+    case.bc_structs["wall"]["thermal_type"] = ("string", "equilibrium_radiation")
+    d = oc.write_case(case, tmp_path / "rad")
+    with pytest.raises(ostc.OstcError, match="equilibrium_radiation"):
+        ostc.Solver(str(d))
+    case.bc_structs["wall"]["thermal_type"] = ("string", "isothermal")
+    case.bc_structs["wall"]["fluctuation_type"] = ("int", 1)
+    d = oc.write_case(case, tmp_path / "fluct")
+    with pytest.raises(ostc.OstcError, match="fluctuation"):
+        ostc.Solver(str(d))

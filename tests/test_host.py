@@ -112,7 +112,7 @@ def test_setup_grammar(built, tmp_path):
 
 def test_unknown_boundary_type_rejected(built, tmp_path):
     case, _ = _case_dir(tmp_path)
-    case.faces[0] = oc.Face(case.faces[0].raw, 2)  # label 2 = wall, not on this path
+    case.faces[0] = oc.Face(case.faces[0].raw, 5)  # label 5 = supersonic inflow, not on this path
     d = oc.write_case(case, tmp_path / "bad")
-    with pytest.raises(ostc.OstcError, match="label 2"):
+    with pytest.raises(ostc.OstcError, match="label 5"):
         ostc.probe_case(str(d))

@@ -144,3 +144,21 @@ def test_stat_collect_interior_formula(built):
         assert groups[g].shape[0] == len(want[g])
         for l, x in enumerate(want[g]):
             assert np.array_equal(groups[g][l], 2 * x), (g, l)
+
+
+@pytest.mark.parametrize("thermal", ["isothermal", "adiabatic"])
+def test_wall_face_nodes(built, thermal):
+    """apply_wall (BoundCond.cuh:1024-1270): after a step the wall nodes carry zero velocity, the
+    pressure of their first interior neighbour, and the wall temperature (isothermal) or the
+    neighbour's temperature (adiabatic)."""
+    case = oc.mixing_layer_3d(mx=16, my=12, mz=8, ybc="wall", wall_thermal=thermal, t0=300.0)
+    o = Oracle(case)
+    o.set_state(case.bv)
+    o.step(2)
+    _, bv, _ = o.get_state()
+    for jw, jn in ((0, 1), (-1, -2)):
+        assert np.all(bv[1:4, :, jw, :] == 0)
+        assert np.array_equal(bv[4, :, jw, :], bv[4, :, jn, :])
+        want = np.full_like(bv[5, :, jw, :], 300.0) if thermal == "isothermal" else bv[5, :, jn, :]
+        assert np.array_equal(bv[5, :, jw, :], want)
+        assert np.allclose(bv[0, :, jw, :], bv[4, :, jw, :] * 28.9647 / (8314.462618 * bv[5, :, jw, :]), rtol=1e-14)
