@@ -877,10 +877,30 @@ bool resolve_boundaries(const Setup &s, const Derived &d, HostMesh &mesh, std::s
       auto it = lab.find(f.label);
       f.type = it != lab.end() ? it->second.first : f.label;
       if (f.type != kSymmetry && f.type != kFarfield && f.type != kOutflow && f.type != kPeriodic &&
-          f.type != kWall) {
+          f.type != kWall && f.type != kInflow) {
         err = "boundary label " + std::to_string(f.label) +
-              " maps to a type outside this path (supported: wall 2, symmetry 3, farfield 4, outflow 6, periodic 8)";
+              " maps to a type outside this path (supported: wall 2, symmetry 3, farfield 4, inflow 5, outflow 6, "
+              "periodic 8)";
         return false;
+      }
+      if (f.type == kInflow) {
+        // apply_inflow with a constant state (BoundCond.cuh:483-613, inflow_type 0, no fluctuation):
+        // profile, digital-filter and fluctuating inflows are not on this path
+        if (it == lab.end()) {
+          err = "inflow label " + std::to_string(f.label) + " needs a struct in boundary_conditions";
+          return false;
+        }
+        const auto &st = s.structs.at(it->second.second);
+        for (const char *k : {"inflow_type", "fluctuation_type"}) {
+          auto q = st.find(k);
+          if (q != st.end() && std::holds_alternative<int>(q->second) && std::get<int>(q->second) != 0) {
+            err = "inflow label " + std::to_string(f.label) + ": " + k +
+                  " != 0 (profile / fluctuating inflow) is not provided; constant inflow is";
+            return false;
+          }
+        }
+        f.struct_name = it->second.second;
+        continue;
       }
       if (f.type == kWall) {
         // Wall::Wall (BoundCond.cpp:497-560): isothermal (default, 300 K) or adiabatic; the radiative
@@ -949,6 +969,22 @@ bool resolve_boundaries(const Setup &s, const Derived &d, HostMesh &mesh, std::s
         f.entropy = pressure / std::pow(density, gamma);
         f.mw = mw;
       }
+    }
+  return true;
+}
+
+bool resolve_inflows(const Setup &s, const ChemTables *chem, HostMesh &mesh, std::string &err) {
+  for (auto &B : mesh.blocks)
+    for (auto &f : B.faces) {
+      if (f.type != kInflow) continue;
+      double bv[6], c;
+      if (!inflow_state(s, f.struct_name, chem, bv, f.y, c, err)) return false;
+      f.density = bv[0];
+      f.u = bv[1];
+      f.v = bv[2];
+      f.w = bv[3];
+      f.pressure = bv[4];
+      f.temperature = bv[5];
     }
   return true;
 }

@@ -89,7 +89,12 @@ struct BcFace {
   double density = 0, u = 0, v = 0, w = 0, pressure = 0, temperature = 0;
   double acoustic_speed = 0, gamma = kGammaAir, entropy = 0, mw = kMwAir;
   int wall_adiabatic = 0;  // walls: 1 adiabatic, 0 isothermal at `temperature` (Wall, BoundCond.h:87-112)
+  // constant supersonic inflow (Inflow ctor, BoundCond.cpp:157-214): the struct it reads and, for
+  // mixtures, its mass fractions (filled once the species tables are known)
+  std::string struct_name;
+  std::vector<double> y;
 };
+
 
 // One 1:1 block interface after InnerFace::register_boundary (Mesh.cpp:34-176): the node range of
 // this block it writes (the coincident face plus ngg ghost layers), the matching start in the target
@@ -133,6 +138,8 @@ bool read_mesh(const std::string &input_dir, const Derived &d, HostMesh &mesh, s
 // Attaches types and far-field states to the faces from the setup's boundary structs
 // (DBoundCond::initialize_bc_on_GPU, BoundCond.cu:162-258).
 bool resolve_boundaries(const Setup &s, const Derived &d, HostMesh &mesh, std::string &err);
+// Inflow face states from their structs, with the species tables of a mixture case (nullptr: air).
+bool resolve_inflows(const Setup &s, const ChemTables *chem, HostMesh &mesh, std::string &err);
 // rho_inf^2 v_inf^2 and v_inf of the struct named by reference_state (0, 0 without one): the scales of
 // the flux-split WENO epsilon (DParameter.cu:26-29, WENO.cu:1466-1473).
 bool reference_scales(const Setup &s, const ChemTables *chem, double &eps_scale, double &v_ref, std::string &err);

@@ -78,6 +78,7 @@ struct DevFace {
   int type, face, direction, rs[3], re[3];
   double density, u, v, w, pressure, temperature, acoustic_speed, gamma, entropy;
   int wall_adiabatic;  // walls: 1 adiabatic, 0 isothermal at `temperature`
+  double y[16];        // inflow mass fractions (mixtures)
 };
 
 struct FillVals {
@@ -110,6 +111,8 @@ __device__ __forceinline__ void cv_from_bv_node(const DevBlock &b, DevState s, l
 #include "ostc_mix.cuh"
 #include "ostc_adj.cuh"
 #include "ostc_stat.cuh"
+
+static_assert(ostc::kMS <= 16, "DevFace::y holds the inflow mass fractions of at most 16 species");
 
 namespace ostc {
 
@@ -967,6 +970,21 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
       for (int g = 1; g <= b.g; ++g) {
         const long long pg = pb + g * dstep;
         copy_bv(b, s, pg, pb);
+        finish_node(b, s, pg);
+      }
+    } else if (f.type == kInflow) {
+      // apply_inflow, constant state (BoundCond.cuh:483-613): the face node and every ghost layer
+      // take the inflow struct's state
+      for (int g = 0; g <= b.g; ++g) {
+        const long long pg = pb + g * dstep;
+        s.bv[pg] = f.density;
+        s.bv[P + pg] = f.u;
+        s.bv[2 * P + pg] = f.v;
+        s.bv[3 * P + pg] = f.w;
+        s.bv[4 * P + pg] = f.pressure;
+        s.bv[5 * P + pg] = f.temperature;
+        if (s.sv)
+          for (int l = 0; l < c_mix.ns; ++l) s.sv[l * P + pg] = f.y[l];
         finish_node(b, s, pg);
       }
     } else if (f.type == kWall) {
@@ -2345,6 +2363,10 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
     ctx->der.n_scalar = c.n_spec;
     ctx->der.n_var = ctx->nv;
   }
+  if (!resolve_inflows(ctx->setup, ctx->mixture ? &ctx->chem : nullptr, ctx->mesh, err)) {
+    g_create_error = err;
+    return OSTC_EINVAL;
+  }
   if (ctx->der.inviscid_type == 3) {
     if (!reference_scales(ctx->setup, ctx->mixture ? &ctx->chem : nullptr, ctx->mixtab.weno_eps_scale,
                           ctx->mixtab.v_ref, err)) {
@@ -2476,6 +2498,7 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
       f.gamma = hf.gamma;
       f.entropy = hf.entropy;
       f.wall_adiabatic = hf.wall_adiabatic;
+      for (size_t l = 0; l < hf.y.size() && l < 16; ++l) f.y[l] = hf.y[l];
       R.faces.push_back(f);
     }
     for (auto &hi : HB.inner) {

@@ -191,6 +191,36 @@ class Case:
         v_inf = c if abs(vel) < 1 else vel
         return rho * vel * rho * vel if abs(vel) >= 1 else rho * c * rho * c, v_inf
 
+    def inflow_states(self):
+        """Inflow ctor (BoundCond.cpp:157-214) of constant inflows: label -> density, velocity
+        (Mach times the speed of sound along (u, v, w)), pressure, temperature and mass fractions y."""
+        out = {}
+        for st in self.bc_structs.values():
+            if st.get("type", (None, None))[1] != "inflow":
+                continue
+            g = {k: v for k, (t, v) in st.items()}
+            t, p, mach = float(g["temperature"]), float(g["pressure"]), float(g["mach"])
+            y = [0.0] * 16
+            mw, gamma = MW_AIR, GAMMA
+            if self.mixture:
+                tb = self.mixture["tables"]
+                yk = [float(g.get(n, 0.0)) for n in tb.names]
+                mw = 0.0
+                for i in range(tb.n_spec):
+                    mw += yk[i] / tb.mw[i]
+                mw = 1 / mw
+                cpi = species_cp(tb, t)
+                cp = cv = 0.0
+                for i in range(tb.n_spec):
+                    cp += yk[i] * cpi[i]
+                    cv += yk[i] * (cpi[i] - R_U / tb.mw[i])
+                gamma = cp / cv
+                y[:tb.n_spec] = yk
+            vel = mach * math.sqrt(gamma * R_U / mw * t)
+            out[g["label"]] = dict(density=p * mw / (R_U * t), u=g.get("u", 1.0) * vel, v=g.get("v", 0.0) * vel,
+                                   w=g.get("w", 0.0) * vel, pressure=p, temperature=t, y=y)
+        return out
+
     def wall_states(self):
         """Wall ctor (BoundCond.cpp:497-560): label -> isothermal wall temperature (300 K by default)
         and the adiabatic flag."""
@@ -204,7 +234,7 @@ class Case:
         return out
 
     def label_types(self):
-        types = {"wall": 2, "symmetry": 3, "farfield": 4, "outflow": 6, "periodic": 8}
+        types = {"wall": 2, "symmetry": 3, "farfield": 4, "inflow": 5, "outflow": 6, "periodic": 8}
         m = {}
         for st in self.bc_structs.values():
             m[st["label"][1]] = types[st["type"][1]]
@@ -345,6 +375,9 @@ class MultiCase:
     def wall_states(self):
         return Case.wall_states(self)
 
+    def inflow_states(self):
+        return Case.inflow_states(self)
+
     def reference_scales(self):
         return Case.reference_scales(self)
 
@@ -476,6 +509,20 @@ def multiblock_mixing_layer_3d(nb=12, lo=32, hi=256, my=None, mz=None, seed=0, s
                      freestream=dict(mach=mc, pressure=p0, temperature=t0))
 
 
+def _inflow_x(faces, structs, mach, p, t, y=None):
+    """Turn the periodic x faces into a constant supersonic inflow at i = 0 (label 5) and an outflow at
+    i = mx - 1 (label 6); y: inflow mass fractions {name: value} of a mixture."""
+    faces[0] = Face(faces[0].raw, 5)
+    faces[1] = Face(faces[1].raw, 6)
+    st = {"type": ("string", "inflow"), "label": ("int", 5), "mach": ("real", float(mach)),
+          "pressure": ("real", float(p)), "temperature": ("real", float(t)), "u": ("real", 1.0), "v": ("real", 0.0),
+          "w": ("real", 0.0)}
+    for k, v in (y or {}).items():
+        st[k] = ("real", float(v))
+    structs["inflow"] = st
+    structs.setdefault("outflow", {"type": ("string", "outflow"), "label": ("int", 6)})
+
+
 def _wall_struct(thermal, t_wall):
     """No-slip wall struct (label 2): isothermal at t_wall, or adiabatic."""
     st = {"type": ("string", "wall"), "label": ("int", 2), "thermal_type": ("string", thermal)}
@@ -534,7 +581,7 @@ def mixing_layer_2d(mx=257, my=129, seed=0, steps=100, mc=0.4, re=1000.0, t0=300
 
 def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0, t0=300.0, delta0=1e-3,
                     h=0.125, reconstruction=5, inviscid_scheme=4, cfl=0.5, ybc="farfield",
-                    entropy_fix_factor=0.125, wall_thermal="isothermal") -> Case:
+                    entropy_fix_factor=0.125, wall_thermal="isothermal", xbc="periodic") -> Case:
     """3-D temporal mixing layer: uniform spacing h*delta0, periodic x and z (node-coincident),
     far-field (Riemann-invariant, label 4/41) or outflow (label 6) y faces; u = dU/2 tanh(2y/delta0),
     Mc = 0.7, plus 1e-2 dU N(0,1) exp(-(y/delta0)^2) seeded white noise in u, v, w."""
@@ -572,6 +619,8 @@ def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0
         faces = _box_faces(mx, my, mz, 8, 6, 6, 8)
         structs = {"periodic": {"type": ("string", "periodic"), "label": ("int", 8)},
                    "outflow": {"type": ("string", "outflow"), "label": ("int", 6)}}
+    if xbc == "inflow":
+        _inflow_x(faces, structs, 1.5, p0, t0)
     scheme = dict(reconstruction=reconstruction, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=cfl,
                   prandtl_number=0.72, limiter=0, entropy_fix_factor=entropy_fix_factor)
     return Case("mixing_layer_3d", mx, my, mz, X, Y, Z, delta0, faces, structs, scheme, bv, steps)
@@ -582,7 +631,8 @@ CHEM_FIXTURE = Path(__file__).resolve().parents[2] / "tests" / "golden" / "chem"
 
 def reacting_mixing_layer_3d(mx=384, my=192, mz=96, seed=0, steps=100, h=0.125, delta0=1e-3, mc=0.4,
                              p0=101325.0, inviscid_scheme=72, finite_rate=True, ybc="outflow",
-                             chem_dir=None, fuel=None, oxidiser=None, wall_thermal="isothermal") -> Case:
+                             chem_dir=None, fuel=None, oxidiser=None, wall_thermal="isothermal",
+                             xbc="periodic") -> Case:
     """Reacting H2/air temporal mixing layer (9 species, 19 reactions after merging duplicates):
     fuel Y_H2 = 0.05 in N2 at 300 K (y > 0) over vitiated air at 1500 K (y < 0): Y_O2 = 0.20, Y_H2O = 0.10,
     radicals Y_OH = 1e-3, Y_O = 1e-4, Y_H = 1e-5, Y_HO2 = 1e-6, Y_H2O2 = 1e-7 (so that every reaction
@@ -635,6 +685,8 @@ def reacting_mixing_layer_3d(mx=384, my=192, mz=96, seed=0, steps=100, h=0.125, 
                    "outflow": {"type": ("string", "outflow"), "label": ("int", 6)}}
     else:
         raise ValueError("the reacting case uses outflow or wall y faces")
+    if xbc == "inflow":
+        _inflow_x(faces, structs, 1.2, p0, to, oxidiser)
     scheme = dict(reconstruction=2, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=0.5, prandtl_number=0.72,
                   limiter=0, entropy_fix_factor=0.125)
     mixture = dict(tables=tb, finite_rate=finite_rate, chem_dir=str(chem_dir), mechanism="H2_mech.inp",

@@ -19,7 +19,7 @@ LIB = HERE / "_build" / "libostc_oracle.so"
 class OrcFace(ctypes.Structure):
     _fields_ = [("type", ctypes.c_int), ("raw", ctypes.c_int * 6)] + [
         (n, ctypes.c_double) for n in ("density", "u", "v", "w", "pressure", "temperature", "acoustic_speed",
-                                       "gamma", "entropy", "mw")] + [("wall_adiabatic", ctypes.c_int)]
+                                       "gamma", "entropy", "mw")] + [("wall_adiabatic", ctypes.c_int), ("y", ctypes.c_double * 16)]
 
 
 MAXS, MAXR = 16, 64
@@ -155,7 +155,7 @@ class Oracle:
         c.cfl, c.prandtl = s["cfl"], s["prandtl_number"]
         c.fixed_time_step, c.dt = 0, 1e-8
         types = case.label_types()
-        ff = {**case.farfield_states(), **case.wall_states()}
+        ff = {**case.farfield_states(), **case.wall_states(), **case.inflow_states()}
         c.n_face = len(case.faces)
         for n, f in enumerate(case.faces):
             c.face[n].type = types[f.label]
@@ -163,7 +163,7 @@ class Oracle:
                 c.face[n].raw[q] = f.raw[q]
             if f.label in ff:
                 for k, v in ff[f.label].items():
-                    setattr(c.face[n], k, v)
+                    setattr(c.face[n], k, (ctypes.c_double * 16)(*v) if k == "y" else v)
         self.n_spec = 0
         mix = getattr(case, "mixture", None)
         if mix is not None:
@@ -274,7 +274,7 @@ class MultiOracle:
         nb = len(case.blocks)
         cases = (OrcCase * nb)()
         types = case.label_types()
-        ff = {**case.farfield_states(), **case.wall_states()}
+        ff = {**case.farfield_states(), **case.wall_states(), **case.inflow_states()}
         self._keep = []
         xs, ys, zs = (dp_arr * nb)(), (dp_arr * nb)(), (dp_arr * nb)()
         for b, blk in enumerate(case.blocks):
@@ -293,7 +293,7 @@ class MultiOracle:
                     c.face[n].raw[q] = f.raw[q]
                 if f.label in ff:
                     for k, v in ff[f.label].items():
-                        setattr(c.face[n], k, v)
+                        setattr(c.face[n], k, (ctypes.c_double * 16)(*v) if k == "y" else v)
             c.weno_eps_scale, c.v_ref = case.reference_scales()
             _set_init(c, case)
             for arr, src in ((xs, blk.x), (ys, blk.y), (zs, blk.z)):

@@ -28,6 +28,7 @@ typedef struct {
   int rs[3], re[3];
   double density, u, v, w, pressure, temperature, acoustic_speed, gamma, entropy, mw;
   int wall_adiabatic;
+  double y[16];
 } face_t;
 
 struct orc_ctx {
@@ -266,6 +267,7 @@ static void register_face(orc_ctx *o, const orc_face_in *in, face_t *f) {
   f->pressure = in->pressure; f->temperature = in->temperature;
   f->acoustic_speed = in->acoustic_speed; f->gamma = in->gamma; f->entropy = in->entropy; f->mw = in->mw;
   f->wall_adiabatic = in->wall_adiabatic;
+  memcpy(f->y, in->y, sizeof(f->y));
 }
 
 /* ---------------------------------------------------------------- pointwise helpers */
@@ -1655,6 +1657,28 @@ static void bc_outflow(orc_ctx *o, const face_t *f) {
         }
 }
 
+/* apply_inflow with a constant state (BoundCond.cuh:483-613): the face node and its ghost layers
+ * take the inflow state and mass fractions. */
+static void bc_inflow(orc_ctx *o, const face_t *f) {
+  const long P = o->P;
+  int dir[3] = {0, 0, 0};
+  dir[f->face] = f->direction;
+  for (int i = f->rs[0]; i <= f->re[0]; ++i)
+    for (int j = f->rs[1]; j <= f->re[1]; ++j)
+      for (int k = f->rs[2]; k <= f->re[2]; ++k)
+        for (int g = 0; g <= o->g; ++g) {
+          const long pg = ID(o, i + g * dir[0], j + g * dir[1], k + g * dir[2]);
+          o->bv[pg] = f->density;
+          o->bv[P + pg] = f->u;
+          o->bv[2 * P + pg] = f->v;
+          o->bv[3 * P + pg] = f->w;
+          o->bv[4 * P + pg] = f->pressure;
+          o->bv[5 * P + pg] = f->temperature;
+          for (int l = 0; l < o->ns; ++l) o->sv[l * P + pg] = f->y[l];
+          cv_from_bv(o, pg);
+        }
+}
+
 /* mixture molecular weight of node p from its mass fractions */
 static double node_mw(const orc_ctx *o, long p) {
   if (!o->ns) return MW_AIR;
@@ -1793,8 +1817,8 @@ static void bc_farfield(orc_ctx *o, const face_t *f) {
  * farfield, outflow, symmetry, periodic (other types are not on this path). */
 static void apply_bcs(orc_ctx *o) {
   /* priority order of DBoundCond::apply_boundary_conditions (BoundCond.cuh:1488-1679) */
-  const int order[5] = {ORC_FARFIELD, ORC_OUTFLOW, ORC_SYMMETRY, ORC_WALL, ORC_PERIODIC};
-  for (int t = 0; t < 5; ++t)
+  const int order[6] = {ORC_FARFIELD, ORC_OUTFLOW, ORC_INFLOW, ORC_SYMMETRY, ORC_WALL, ORC_PERIODIC};
+  for (int t = 0; t < 6; ++t)
     for (int n = 0; n < o->nf; ++n) {
       const face_t *f = &o->f[n];
       if (f->type != order[t]) continue;
@@ -1804,6 +1828,7 @@ static void apply_bcs(orc_ctx *o) {
         case ORC_SYMMETRY: bc_symmetry(o, f); break;
         case ORC_PERIODIC: bc_periodic(o, f); break;
         case ORC_WALL: bc_wall(o, f); break;
+        case ORC_INFLOW: bc_inflow(o, f); break;
       }
     }
 }

@@ -16,7 +16,7 @@ extern "C" {
 #endif
 
 /* Boundary type codes follow the reference labels (BoundCond.cu:232-258). */
-enum { ORC_WALL = 2, ORC_SYMMETRY = 3, ORC_FARFIELD = 4, ORC_OUTFLOW = 6, ORC_PERIODIC = 8 };
+enum { ORC_WALL = 2, ORC_SYMMETRY = 3, ORC_FARFIELD = 4, ORC_INFLOW = 5, ORC_OUTFLOW = 6, ORC_PERIODIC = 8 };
 
 typedef struct {
   int type;          /* ORC_* */
@@ -25,6 +25,9 @@ typedef struct {
   double density, u, v, w, pressure, temperature, acoustic_speed, gamma, entropy, mw;
   /* walls (type == ORC_WALL, Wall ctor BoundCond.cpp:497-560): 1 adiabatic, 0 isothermal at temperature */
   int wall_adiabatic;
+  /* constant inflow (type == ORC_INFLOW, Inflow ctor BoundCond.cpp:157-214): the state above and the
+   * mass fractions of a mixture */
+  double y[16];
 } orc_face_in;
 
 /* Mixture tables (Species / Reaction, ChemData.cpp; DParameter.cu:57-155), row-major [i][j]. */

@@ -1,7 +1,8 @@
-"""No-slip walls (apply_wall, BoundCond.cuh:1024-1270: isothermal or adiabatic, no blowing or
-fluctuation) on the GPU against the oracle, through the C ABI: RK3 trajectories of air (3-D and 2-D)
-and of the 9-species mixture with both y faces walls, 1e-12 relative per conserved variable as the
-other trajectory tests.
+"""Wall and inflow faces on the GPU against the oracle, through the C ABI: no-slip walls (apply_wall,
+BoundCond.cuh:1024-1270: isothermal or adiabatic, no blowing or fluctuation) on both y faces, and a
+constant supersonic inflow (apply_inflow, BoundCond.cuh:483-613) at i = 0 with an outflow at
+i = mx - 1.  RK3 trajectories of air (3-D and 2-D) and of the 9-species mixture, 1e-12 relative per
+conserved variable as the other trajectory tests.
 """
 import numpy as np
 import pytest
@@ -68,4 +69,31 @@ def test_wall_rejections(built, tmp_path):
     case.bc_structs["wall"]["fluctuation_type"] = ("int", 1)
     d = oc.write_case(case, tmp_path / "fluct")
     with pytest.raises(ostc.OstcError, match="fluctuation"):
+        ostc.Solver(str(d))
+
+
+@pytest.mark.parametrize("ybc", ["farfield", "wall"])
+def test_inflow_air_3d(built, tmp_path, ybc):
+    case = oc.mixing_layer_3d(mx=32, my=24, mz=16, xbc="inflow", ybc=ybc)
+    bg = _run(case, tmp_path, 10)
+    st = case.inflow_states()[5]
+    # the inflow face nodes hold the inflow state; with walls, the wall (applied later, higher
+    # priority) owns the corner nodes j = 0 and j = my - 1
+    js = slice(1, -1) if ybc == "wall" else slice(None)
+    assert np.all(bg[1, :, js, 0] == st["u"]) and np.all(bg[4, :, js, 0] == st["pressure"])
+    if ybc == "wall":
+        assert np.all(bg[1, :, 0, 0] == 0)
+
+
+def test_inflow_mixture(built, tmp_path):
+    case = oc.reacting_mixing_layer_3d(mx=20, my=16, mz=10, xbc="inflow")
+    _run(case, tmp_path, 3, mixture=True)
+
+
+def test_inflow_rejections(built, tmp_path):
+    """Profile and fluctuating inflows are refused with the reason."""
+    case = oc.mixing_layer_3d(mx=16, my=12, mz=8, xbc="inflow")
+    case.bc_structs["inflow"]["fluctuation_type"] = ("int", 1)
+    d = oc.write_case(case, tmp_path / "fl")
+    with pytest.raises(ostc.OstcError, match="fluctuation_type"):
         ostc.Solver(str(d))

@@ -162,3 +162,17 @@ def test_wall_face_nodes(built, thermal):
         want = np.full_like(bv[5, :, jw, :], 300.0) if thermal == "isothermal" else bv[5, :, jn, :]
         assert np.array_equal(bv[5, :, jw, :], want)
         assert np.allclose(bv[0, :, jw, :], bv[4, :, jw, :] * 28.9647 / (8314.462618 * bv[5, :, jw, :]), rtol=1e-14)
+
+
+def test_inflow_face_nodes(built):
+    """apply_inflow with a constant state (BoundCond.cuh:483-613): after a step the inflow face nodes
+    hold the state of the Inflow struct (BoundCond.cpp:157-214)."""
+    case = oc.mixing_layer_3d(mx=16, my=12, mz=8, xbc="inflow")
+    st = case.inflow_states()[5]
+    o = Oracle(case)
+    o.set_state(case.bv)
+    o.step(2)
+    _, bv, _ = o.get_state()
+    for l, k in enumerate(("density", "u", "v", "w", "pressure", "temperature")):
+        assert np.all(bv[l, :, :, 0] == st[k]), k
+    assert st["u"] > 1.0 * math.sqrt(1.4 * oc.R_AIR * st["temperature"])  # supersonic (Mach 1.5)
