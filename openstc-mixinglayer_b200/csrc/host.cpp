@@ -877,11 +877,26 @@ bool resolve_boundaries(const Setup &s, const Derived &d, HostMesh &mesh, std::s
       auto it = lab.find(f.label);
       f.type = it != lab.end() ? it->second.first : f.label;
       if (f.type != kSymmetry && f.type != kFarfield && f.type != kOutflow && f.type != kPeriodic &&
-          f.type != kWall && f.type != kInflow) {
+          f.type != kWall && f.type != kInflow && f.type != kSubsonicInflow && f.type != kBackPressure) {
         err = "boundary label " + std::to_string(f.label) +
               " maps to a type outside this path (supported: wall 2, symmetry 3, farfield 4, inflow 5, outflow 6, "
-              "periodic 8)";
+              "subsonic_inflow 7, periodic 8, back_pressure 9)";
         return false;
+      }
+      if (f.type == kSubsonicInflow || f.type == kBackPressure) {
+        // SubsonicInflow / BackPressure ctors (BoundCond.cpp:704-768): air only, states resolved with
+        // the reference state in resolve_inflows
+        if (d.species != 0) {
+          err = std::string(f.type == kBackPressure ? "back pressure" : "subsonic inflow") +
+                " faces do not support multi-species cases (label " + std::to_string(f.label) + ")";
+          return false;
+        }
+        if (it == lab.end()) {
+          err = "label " + std::to_string(f.label) + " needs a struct in boundary_conditions";
+          return false;
+        }
+        f.struct_name = it->second.second;
+        continue;
       }
       if (f.type == kInflow) {
         // apply_inflow with a constant state (BoundCond.cuh:483-613, inflow_type 0, no fluctuation):
@@ -974,8 +989,43 @@ bool resolve_boundaries(const Setup &s, const Derived &d, HostMesh &mesh, std::s
 }
 
 bool resolve_inflows(const Setup &s, const ChemTables *chem, HostMesh &mesh, std::string &err) {
+  // p_inf, T_inf: the reference state's pressure and temperature (Inflow ctor, BoundCond.cpp:299-310)
+  auto ref_pt = [&](double &p_inf, double &t_inf) {
+    auto rs = s.strings.find("reference_state");
+    if (rs == s.strings.end()) {
+      err = "a pressure or temperature ratio needs the reference_state struct (p_inf, T_inf)";
+      return false;
+    }
+    double bv[6], c;
+    std::vector<double> y;
+    if (!inflow_state(s, rs->second, chem, bv, y, c, err)) return false;
+    p_inf = bv[4];
+    t_inf = bv[5];
+    return true;
+  };
   for (auto &B : mesh.blocks)
     for (auto &f : B.faces) {
+      if (f.type == kBackPressure) {
+        const auto &st = s.structs.at(f.struct_name);
+        f.pressure = struct_real(st, "pressure", -1);
+        if (f.pressure < 0) {
+          double p_inf, t_inf;
+          if (!ref_pt(p_inf, t_inf)) return false;
+          f.pressure = struct_real(st, "p_pRef_ratio", 1.0) * p_inf;
+        }
+        continue;
+      }
+      if (f.type == kSubsonicInflow) {
+        const auto &st = s.structs.at(f.struct_name);
+        double p_inf, t_inf;
+        if (!ref_pt(p_inf, t_inf)) return false;
+        f.pressure = struct_real(st, "pt_pRef_ratio", 1.0) * p_inf;     // total pressure
+        f.temperature = struct_real(st, "Tt_TRef_ratio", 1.0) * t_inf;  // total temperature
+        f.u = struct_real(st, "u", 1.0);
+        f.v = struct_real(st, "v", 0.0);
+        f.w = struct_real(st, "w", 0.0);
+        continue;
+      }
       if (f.type != kInflow) continue;
       double bv[6], c;
       if (!inflow_state(s, f.struct_name, chem, bv, f.y, c, err)) return false;

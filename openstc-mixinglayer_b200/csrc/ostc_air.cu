@@ -987,6 +987,89 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
           for (int l = 0; l < c_mix.ns; ++l) s.sv[l * P + pg] = f.y[l];
         finish_node(b, s, pg);
       }
+    } else if (f.type == kBackPressure || f.type == kSubsonicInflow) {
+      // apply_back_pressure / apply_subsonic_inflow (BoundCond.cuh:1272-1441), air: outward unit
+      // normal of the face, normal velocity and speed of sound of the face node (which keeps its
+      // values); ghosts from the characteristic relations
+      double nx = b.met[(f.face * 3 + 0) * P + pb], ny = b.met[(f.face * 3 + 1) * P + pb],
+             nz = b.met[(f.face * 3 + 2) * P + pb];
+      const double gni = f.direction / sqrt(nx * nx + ny * ny + nz * nz);
+      nx *= gni;
+      ny *= gni;
+      nz *= gni;
+      const double rb = s.bv[pb], ub = s.bv[P + pb], vb = s.bv[2 * P + pb], wb = s.bv[3 * P + pb];
+      const double pbv = s.bv[4 * P + pb];
+      const double u_face = nx * ub + ny * vb + nz * wb;
+      const double ab = sqrt(kGamma * pbv / rb);
+      if (f.type == kBackPressure) {
+        double rho_b = rb, u_b = ub, v_b = vb, w_b = wb, p_b = pbv;
+        const bool sub = fabs(u_face / ab) < 1;
+        if (sub) {
+          p_b = f.pressure;
+          const long long p1 = pb - dstep;
+          const double d1 = s.bv[p1], u1 = s.bv[P + p1], v1 = s.bv[2 * P + p1], w1 = s.bv[3 * P + p1],
+                       pr1 = s.bv[4 * P + p1];
+          const double c1 = sqrt(kGamma * pr1 / d1);
+          rho_b = d1 + (p_b - pr1) / (c1 * c1);
+          u_b = u1 + nx * (pr1 - p_b) / (d1 * c1);
+          v_b = v1 + ny * (pr1 - p_b) / (d1 * c1);
+          w_b = w1 + nz * (pr1 - p_b) / (d1 * c1);
+        }
+        for (int g = 1; g <= b.g; ++g) {
+          const long long pg = pb + g * dstep, pi = pb - g * dstep;
+          double r, u, v, w, pr;
+          if (sub) {
+            pr = 2 * p_b - s.bv[4 * P + pi];
+            r = 2 * rho_b - s.bv[pi];
+            u = 2 * u_b - s.bv[P + pi];
+            v = 2 * v_b - s.bv[2 * P + pi];
+            w = 2 * w_b - s.bv[3 * P + pi];
+          } else {
+            r = rho_b;
+            u = u_b;
+            v = v_b;
+            w = w_b;
+            pr = p_b;
+          }
+          s.bv[pg] = r;
+          s.bv[P + pg] = u;
+          s.bv[2 * P + pg] = v;
+          s.bv[3 * P + pg] = w;
+          s.bv[4 * P + pg] = pr;
+          s.bv[5 * P + pg] = pr / (r * kRuD / kMwD);
+          finish_node(b, s, pg);
+        }
+      } else {
+        // negative Riemann invariant and total enthalpy of the face node, then the speed of sound
+        // from the quadratic that keeps both with the inflow's total state
+        const double riemann_neg = fabs(u_face) - 2 * ab / (kGamma - 1);
+        const double hti = pbv / rb * kGamma / (kGamma - 1) + 0.5 * (ub * ub + vb * vb + wb * wb);
+        const double qa = 1 + 2.0 / (kGamma - 1);
+        const double qb = 2 * riemann_neg;
+        const double qc = (kGamma - 1) * (0.5 * riemann_neg * riemann_neg - hti);
+        const double delta = qb * qb - 4 * qa * qc;
+        double a_new = ab;
+        if (delta >= 0) {
+          const double a_plus = (-qb + sqrt(delta)) / (2 * qa);
+          const double a_minus = (-qb - sqrt(delta)) / (2 * qa);
+          a_new = a_plus > a_minus ? a_plus : a_minus;
+        }
+        const double u_new = riemann_neg + 2 * a_new / (kGamma - 1);
+        const double mach = u_new / a_new;
+        const double pr = f.pressure * pow(1 + 0.5 * (kGamma - 1) * mach * mach, -kGamma / (kGamma - 1));
+        const double tt = f.temperature * pow(pr / f.pressure, (kGamma - 1) / kGamma);
+        const double r = pr * kMwD / (tt * kRuD);
+        for (int g = 1; g <= b.g; ++g) {
+          const long long pg = pb + g * dstep;
+          s.bv[pg] = r;
+          s.bv[P + pg] = u_new * f.u;
+          s.bv[2 * P + pg] = u_new * f.v;
+          s.bv[3 * P + pg] = u_new * f.w;
+          s.bv[4 * P + pg] = pr;
+          s.bv[5 * P + pg] = tt;
+          finish_node(b, s, pg);
+        }
+      }
     } else if (f.type == kWall) {
       // apply_wall (BoundCond.cuh:1024-1270), no-slip, isothermal or adiabatic: the wall node takes
       // the first interior node's pressure (and mass fractions) at the wall temperature; ghost g

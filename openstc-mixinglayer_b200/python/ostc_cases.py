@@ -221,6 +221,28 @@ class Case:
                                    w=g.get("w", 0.0) * vel, pressure=p, temperature=t, y=y)
         return out
 
+    def characteristic_states(self):
+        """SubsonicInflow / BackPressure ctors (BoundCond.cpp:704-768), air: label -> total pressure and
+        temperature (ratios times the reference state's p and T) with the flow direction, or the back
+        pressure (given, or its ratio times the reference pressure)."""
+        out = {}
+        f = self.freestream or {}
+        for st in self.bc_structs.values():
+            kind = st.get("type", (None, None))[1]
+            if kind not in ("subsonic_inflow", "back_pressure"):
+                continue
+            g = {k: v for k, (t, v) in st.items()}
+            if kind == "back_pressure":
+                p = float(g.get("pressure", -1.0))
+                if p < 0:
+                    p = float(g.get("p_pRef_ratio", 1.0)) * f["pressure"]
+                out[g["label"]] = dict(pressure=p)
+            else:
+                out[g["label"]] = dict(pressure=float(g.get("pt_pRef_ratio", 1.0)) * f["pressure"],
+                                       temperature=float(g.get("Tt_TRef_ratio", 1.0)) * f["temperature"],
+                                       u=float(g.get("u", 1.0)), v=float(g.get("v", 0.0)), w=float(g.get("w", 0.0)))
+        return out
+
     def wall_states(self):
         """Wall ctor (BoundCond.cpp:497-560): label -> isothermal wall temperature (300 K by default)
         and the adiabatic flag."""
@@ -234,7 +256,8 @@ class Case:
         return out
 
     def label_types(self):
-        types = {"wall": 2, "symmetry": 3, "farfield": 4, "inflow": 5, "outflow": 6, "periodic": 8}
+        types = {"wall": 2, "symmetry": 3, "farfield": 4, "inflow": 5, "outflow": 6, "subsonic_inflow": 7,
+                 "periodic": 8, "back_pressure": 9}
         m = {}
         for st in self.bc_structs.values():
             m[st["label"][1]] = types[st["type"][1]]
@@ -377,6 +400,9 @@ class MultiCase:
 
     def inflow_states(self):
         return Case.inflow_states(self)
+
+    def characteristic_states(self):
+        return Case.characteristic_states(self)
 
     def reference_scales(self):
         return Case.reference_scales(self)
@@ -619,11 +645,24 @@ def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0
         faces = _box_faces(mx, my, mz, 8, 6, 6, 8)
         structs = {"periodic": {"type": ("string", "periodic"), "label": ("int", 8)},
                    "outflow": {"type": ("string", "outflow"), "label": ("int", 6)}}
+    freestream = None
     if xbc == "inflow":
         _inflow_x(faces, structs, 1.5, p0, t0)
+    elif xbc == "subsonic":
+        # subsonic inflow at i = 0 (total state 1.2 p0, 1.05 T0) and back pressure p0 at i = mx - 1,
+        # both relative to the reference state (Mach mc, p0, T0)
+        faces[0] = Face(faces[0].raw, 7)
+        faces[1] = Face(faces[1].raw, 9)
+        structs["subsonic_inflow"] = {"type": ("string", "subsonic_inflow"), "label": ("int", 7),
+                                      "pt_pRef_ratio": ("real", 1.2), "Tt_TRef_ratio": ("real", 1.05),
+                                      "u": ("real", 1.0), "v": ("real", 0.0), "w": ("real", 0.0)}
+        structs["back_pressure"] = {"type": ("string", "back_pressure"), "label": ("int", 9),
+                                    "p_pRef_ratio": ("real", 1.0)}
+        freestream = dict(mach=mc, pressure=p0, temperature=t0)
     scheme = dict(reconstruction=reconstruction, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=cfl,
                   prandtl_number=0.72, limiter=0, entropy_fix_factor=entropy_fix_factor)
-    return Case("mixing_layer_3d", mx, my, mz, X, Y, Z, delta0, faces, structs, scheme, bv, steps)
+    return Case("mixing_layer_3d", mx, my, mz, X, Y, Z, delta0, faces, structs, scheme, bv, steps,
+                freestream=freestream)
 
 
 CHEM_FIXTURE = Path(__file__).resolve().parents[2] / "tests" / "golden" / "chem"

@@ -155,7 +155,8 @@ class Oracle:
         c.cfl, c.prandtl = s["cfl"], s["prandtl_number"]
         c.fixed_time_step, c.dt = 0, 1e-8
         types = case.label_types()
-        ff = {**case.farfield_states(), **case.wall_states(), **case.inflow_states()}
+        ff = {**case.farfield_states(), **case.wall_states(), **case.inflow_states(),
+              **case.characteristic_states()}
         c.n_face = len(case.faces)
         for n, f in enumerate(case.faces):
             c.face[n].type = types[f.label]
@@ -274,7 +275,8 @@ class MultiOracle:
         nb = len(case.blocks)
         cases = (OrcCase * nb)()
         types = case.label_types()
-        ff = {**case.farfield_states(), **case.wall_states(), **case.inflow_states()}
+        ff = {**case.farfield_states(), **case.wall_states(), **case.inflow_states(),
+              **case.characteristic_states()}
         self._keep = []
         xs, ys, zs = (dp_arr * nb)(), (dp_arr * nb)(), (dp_arr * nb)()
         for b, blk in enumerate(case.blocks):

@@ -1679,6 +1679,92 @@ static void bc_inflow(orc_ctx *o, const face_t *f) {
         }
 }
 
+/* apply_back_pressure / apply_subsonic_inflow (BoundCond.cuh:1272-1441), air: the face node keeps its
+ * values; back pressure: subsonic normal flow takes p_b and the first interior node's characteristic
+ * state at the face, ghosts extrapolate through it (2 q_b - q_in), supersonic copies the face node;
+ * subsonic inflow: speed of sound from the quadratic that keeps the face node's negative Riemann
+ * invariant and total enthalpy, then p and T from the total state, the same in every ghost layer. */
+static void bc_characteristic(orc_ctx *o, const face_t *f) {
+  const long P = o->P;
+  const double g = GAMMA_AIR;
+  int dir[3] = {0, 0, 0};
+  dir[f->face] = f->direction;
+  for (int i = f->rs[0]; i <= f->re[0]; ++i)
+    for (int j = f->rs[1]; j <= f->re[1]; ++j)
+      for (int k = f->rs[2]; k <= f->re[2]; ++k) {
+        const long pb = ID(o, i, j, k);
+        double nx = o->met[(f->face * 3 + 0) * P + pb], ny = o->met[(f->face * 3 + 1) * P + pb],
+               nz = o->met[(f->face * 3 + 2) * P + pb];
+        const double gni = f->direction / sqrt(nx * nx + ny * ny + nz * nz);
+        nx *= gni;
+        ny *= gni;
+        nz *= gni;
+        const double rb = o->bv[pb], ub = o->bv[P + pb], vb = o->bv[2 * P + pb], wb = o->bv[3 * P + pb];
+        const double pbv = o->bv[4 * P + pb];
+        const double u_face = nx * ub + ny * vb + nz * wb;
+        const double ab = sqrt(g * pbv / rb);
+        if (f->type == ORC_BACK_PRESSURE) {
+          double rho_b = rb, u_b = ub, v_b = vb, w_b = wb, p_b = pbv;
+          const int sub = fabs(u_face / ab) < 1;
+          if (sub) {
+            p_b = f->pressure;
+            const long p1 = ID(o, i - dir[0], j - dir[1], k - dir[2]);
+            const double d1 = o->bv[p1], u1 = o->bv[P + p1], v1 = o->bv[2 * P + p1], w1 = o->bv[3 * P + p1];
+            const double pr1 = o->bv[4 * P + p1];
+            const double c1 = sqrt(g * pr1 / d1);
+            rho_b = d1 + (p_b - pr1) / (c1 * c1);
+            u_b = u1 + nx * (pr1 - p_b) / (d1 * c1);
+            v_b = v1 + ny * (pr1 - p_b) / (d1 * c1);
+            w_b = w1 + nz * (pr1 - p_b) / (d1 * c1);
+          }
+          for (int q = 1; q <= o->g; ++q) {
+            const long pg = ID(o, i + q * dir[0], j + q * dir[1], k + q * dir[2]);
+            const long pi = ID(o, i - q * dir[0], j - q * dir[1], k - q * dir[2]);
+            double r = rho_b, u = u_b, v = v_b, w = w_b, pr = p_b;
+            if (sub) {
+              pr = 2 * p_b - o->bv[4 * P + pi];
+              r = 2 * rho_b - o->bv[pi];
+              u = 2 * u_b - o->bv[P + pi];
+              v = 2 * v_b - o->bv[2 * P + pi];
+              w = 2 * w_b - o->bv[3 * P + pi];
+            }
+            o->bv[pg] = r;
+            o->bv[P + pg] = u;
+            o->bv[2 * P + pg] = v;
+            o->bv[3 * P + pg] = w;
+            o->bv[4 * P + pg] = pr;
+            o->bv[5 * P + pg] = pr / (r * R_U / MW_AIR);
+            cv_from_bv(o, pg);
+          }
+        } else {
+          const double rn = fabs(u_face) - 2 * ab / (g - 1);
+          const double hti = pbv / rb * g / (g - 1) + 0.5 * (ub * ub + vb * vb + wb * wb);
+          const double qa = 1 + 2.0 / (g - 1), qb = 2 * rn, qc = (g - 1) * (0.5 * rn * rn - hti);
+          const double delta = qb * qb - 4 * qa * qc;
+          double a_new = ab;
+          if (delta >= 0) {
+            const double ap = (-qb + sqrt(delta)) / (2 * qa), am = (-qb - sqrt(delta)) / (2 * qa);
+            a_new = ap > am ? ap : am;
+          }
+          const double u_new = rn + 2 * a_new / (g - 1);
+          const double mach = u_new / a_new;
+          const double pr = f->pressure * pow(1 + 0.5 * (g - 1) * mach * mach, -g / (g - 1));
+          const double tt = f->temperature * pow(pr / f->pressure, (g - 1) / g);
+          const double r = pr * MW_AIR / (tt * R_U);
+          for (int q = 1; q <= o->g; ++q) {
+            const long pg = ID(o, i + q * dir[0], j + q * dir[1], k + q * dir[2]);
+            o->bv[pg] = r;
+            o->bv[P + pg] = u_new * f->u;
+            o->bv[2 * P + pg] = u_new * f->v;
+            o->bv[3 * P + pg] = u_new * f->w;
+            o->bv[4 * P + pg] = pr;
+            o->bv[5 * P + pg] = tt;
+            cv_from_bv(o, pg);
+          }
+        }
+      }
+}
+
 /* mixture molecular weight of node p from its mass fractions */
 static double node_mw(const orc_ctx *o, long p) {
   if (!o->ns) return MW_AIR;
@@ -1817,8 +1903,9 @@ static void bc_farfield(orc_ctx *o, const face_t *f) {
  * farfield, outflow, symmetry, periodic (other types are not on this path). */
 static void apply_bcs(orc_ctx *o) {
   /* priority order of DBoundCond::apply_boundary_conditions (BoundCond.cuh:1488-1679) */
-  const int order[6] = {ORC_FARFIELD, ORC_OUTFLOW, ORC_INFLOW, ORC_SYMMETRY, ORC_WALL, ORC_PERIODIC};
-  for (int t = 0; t < 6; ++t)
+  const int order[8] = {ORC_FARFIELD, ORC_OUTFLOW, ORC_BACK_PRESSURE, ORC_INFLOW, ORC_SUBSONIC_INFLOW,
+                        ORC_SYMMETRY, ORC_WALL, ORC_PERIODIC};
+  for (int t = 0; t < 8; ++t)
     for (int n = 0; n < o->nf; ++n) {
       const face_t *f = &o->f[n];
       if (f->type != order[t]) continue;
@@ -1829,6 +1916,8 @@ static void apply_bcs(orc_ctx *o) {
         case ORC_PERIODIC: bc_periodic(o, f); break;
         case ORC_WALL: bc_wall(o, f); break;
         case ORC_INFLOW: bc_inflow(o, f); break;
+        case ORC_BACK_PRESSURE:
+        case ORC_SUBSONIC_INFLOW: bc_characteristic(o, f); break;
       }
     }
 }

@@ -16,7 +16,10 @@ extern "C" {
 #endif
 
 /* Boundary type codes follow the reference labels (BoundCond.cu:232-258). */
-enum { ORC_WALL = 2, ORC_SYMMETRY = 3, ORC_FARFIELD = 4, ORC_INFLOW = 5, ORC_OUTFLOW = 6, ORC_PERIODIC = 8 };
+enum { ORC_WALL = 2, ORC_SYMMETRY = 3, ORC_FARFIELD = 4, ORC_INFLOW = 5, ORC_OUTFLOW = 6, ORC_SUBSONIC_INFLOW = 7,
+       ORC_PERIODIC = 8, ORC_BACK_PRESSURE = 9 };
+/* subsonic inflow: pressure / temperature hold the total pressure / temperature and u, v, w the flow
+ * direction; back pressure: pressure holds the back pressure (BoundCond.cpp:704-768) */
 
 typedef struct {
   int type;          /* ORC_* */

@@ -1,9 +1,11 @@
 """Wall and inflow faces on the GPU against the oracle, through the C ABI: no-slip walls (apply_wall,
-BoundCond.cuh:1024-1270: isothermal or adiabatic, no blowing or fluctuation) on both y faces, and a
+BoundCond.cuh:1024-1270: isothermal or adiabatic, no blowing or fluctuation) on both y faces, a
 constant supersonic inflow (apply_inflow, BoundCond.cuh:483-613) at i = 0 with an outflow at
-i = mx - 1.  RK3 trajectories of air (3-D and 2-D) and of the 9-species mixture, 1e-12 relative per
+i = mx - 1, and (air) a subsonic inflow with a back-pressure outflow (BoundCond.cuh:1272-1441).  RK3 trajectories of air (3-D and 2-D) and of the 9-species mixture, 1e-12 relative per
 conserved variable as the other trajectory tests.
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -96,4 +98,22 @@ def test_inflow_rejections(built, tmp_path):
     case.bc_structs["inflow"]["fluctuation_type"] = ("int", 1)
     d = oc.write_case(case, tmp_path / "fl")
     with pytest.raises(ostc.OstcError, match="fluctuation_type"):
+        ostc.Solver(str(d))
+
+
+@pytest.mark.parametrize("ybc", ["outflow", "wall"])
+def test_subsonic_inflow_back_pressure_air(built, tmp_path, ybc):
+    case = oc.mixing_layer_3d(mx=32, my=24, mz=16, xbc="subsonic", ybc=ybc)
+    c0 = math.sqrt(1.4 * oc.R_AIR * 300.0)
+    case.bv[1] = np.abs(case.bv[1]) + 0.3 * c0  # streamwise flow into the domain everywhere, subsonic
+    _run(case, tmp_path, 10)
+
+
+def test_characteristic_faces_refuse_mixtures(built, tmp_path):
+    case = oc.reacting_mixing_layer_3d(mx=16, my=12, mz=8)
+    case.faces[1] = oc.Face(case.faces[1].raw, 9)
+    case.bc_structs["back_pressure"] = {"type": ("string", "back_pressure"), "label": ("int", 9),
+                                        "pressure": ("real", 101325.0)}
+    d = oc.write_case(case, tmp_path / "bp")
+    with pytest.raises(ostc.OstcError, match="multi-species"):
         ostc.Solver(str(d))
