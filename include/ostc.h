@@ -204,6 +204,20 @@ int ostc_total_nodes(const ostc_ctx *ctx, long long *n);
  * (Parameter::deduce_known_info / Mesh::Mesh checks, Parameter.cpp:187-437, Mesh.cpp:592-641). */
 int ostc_probe_case(const char *setup_txt, const char *input_dir, int out[16], char *msg, int msg_len);
 
+/* ---- Tecplot flow-field file (FieldIO, FieldIO.h:73-648; read_flowfield, Initialize.cuh:102-215)
+ *
+ * ostc_write_plt writes every block's current state as the reference's output/flowfield.plt: binary
+ * Tecplot V112, one ordered zone per block with ngg_out ghost layers on each side, node-located
+ * double variables x, y, z, density, u, v, w, pressure, temperature, mach, then the species mass
+ * fractions (a laminar case without user-defined output); solution_time goes into every zone header.
+ * ostc_read_plt restarts from such a file (written here or by the reference): the primitive
+ * variables and mass fractions are found by name, their interior values set as ostc_set_state does,
+ * and the physical time continues from the file's solution time (returned in *solution_time, may be
+ * NULL).  Zone count and extents must match the case's blocks; float data, passive or shared
+ * variables and auxiliary zone data are refused with OSTC_EIO and the reason. */
+int ostc_write_plt(ostc_ctx *ctx, const char *path, int ngg_out, double solution_time);
+int ostc_read_plt(ostc_ctx *ctx, const char *path, double *solution_time);
+
 /* ---- single-point statistics (SinglePointStat, SinglePointStat.h / SinglePointStat.cu:515-706)
  *
  * Replaces the collector the reference runs after every time step past start_collect_statistics_iter

@@ -3329,6 +3329,239 @@ int ostc_bounds_checked(void) {
 #endif
 }
 
+// ---------------------------------------------------------------- Tecplot flow-field file
+
+// Variable names of the flow-field file: FieldIO::acquire_variable_names (FieldIO.h:450-488) for a
+// laminar air or mixture case without user-defined output (UDIO.cu:9-33).
+static std::vector<std::string> plt_names(const ostc_ctx *ctx) {
+  std::vector<std::string> v{"x", "y", "z", "density", "u", "v", "w", "pressure", "temperature", "mach"};
+  for (int l = 0; l < ctx->der.n_spec; ++l) v.push_back(ctx->chem.names[l]);
+  return v;
+}
+
+int ostc_write_plt(ostc_ctx *ctx, const char *path, int ngg_out, double solution_time) {
+  if (!ctx || !path) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  if (ngg_out < 0 || ngg_out > ctx->der.ngg) {
+    ctx->err = "ostc_write_plt: ngg_out must lie in [0, ngg]";
+    return OSTC_EINVAL;
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  const std::vector<std::string> names = plt_names(ctx);
+  const int nvar = (int)names.size(), ns = ctx->der.n_spec;
+  std::vector<char> buf;
+  auto put = [&](const void *p, size_t n) { buf.insert(buf.end(), (const char *)p, (const char *)p + n); };
+  auto put_i = [&](int v) { put(&v, 4); };
+  auto put_f = [&](float v) { put(&v, 4); };
+  auto put_d = [&](double v) { put(&v, 8); };
+  auto put_s = [&](const std::string &s) {
+    for (char c : s) put_i((int)c);
+    put_i(0);
+  };
+  // header (FieldIO::write_header, FieldIO.h:73-200)
+  put("#!TDV112", 8);
+  put_i(1);
+  put_i(0);
+  put_s("Solution file");
+  put_i(nvar);
+  for (const auto &n : names) put_s(n);
+  const int g = ngg_out;
+  for (size_t b = 0; b < ctx->blk.size(); ++b) {
+    const DevBlock &db = ctx->blk[b].db;
+    put_f(299.0f);
+    put_s("zone " + std::to_string(b));
+    put_i(-1);
+    put_i(-2);
+    put_d(solution_time);
+    put_i(-1);
+    put_i(0);
+    put_i(0);
+    put_i(0);
+    put_i(0);
+    put_i(db.mx + 2 * g);
+    put_i(db.my + 2 * g);
+    put_i(db.mz + 2 * g);
+    put_i(0);
+  }
+  put_f(357.0f);
+  // data sections (write_common_data_section + print_field, FieldIO.h:222-648): per zone the
+  // formats, the min/max pairs and the node arrays of x, y, z, bv, mach, Y_k
+  std::vector<double> pl;
+  for (size_t b = 0; b < ctx->blk.size(); ++b) {
+    BlockRes &B = ctx->blk[b];
+    const DevBlock &db = B.db;
+    const HostBlock &hb = ctx->mesh.blocks[b];
+    const long long P = db.plane;
+    const int nl = 6 + ns + (ctx->mixture ? 1 : 0);
+    pl.resize((size_t)nl * P);
+    CK(cudaMemcpy(pl.data(), B.bv[0], 6 * P * sizeof(double), cudaMemcpyDeviceToHost));
+    if (ns) CK(cudaMemcpy(pl.data() + 6 * P, B.sv[0], (size_t)ns * P * sizeof(double), cudaMemcpyDeviceToHost));
+    if (ctx->mixture) CK(cudaMemcpy(pl.data() + (6 + ns) * P, B.acs[0], P * sizeof(double), cudaMemcpyDeviceToHost));
+    const int nx = db.mx + 2 * g, ny = db.my + 2 * g, nz = db.mz + 2 * g;
+    const long long npt = (long long)nx * ny * nz;
+    std::vector<double> a((size_t)nvar * npt);
+    for (int k = -g; k < db.mz + g; ++k)
+      for (int j = -g; j < db.my + g; ++j)
+        for (int i = -g; i < db.mx + g; ++i) {
+          const long long q = ((long long)(k + g) * ny + (j + g)) * nx + (i + g);
+          // 2-D blocks hold no k ghosts: the reference's k layers are copies of k = 0
+          const long long p = db.id(i, j, db.gz ? k : 0);
+          const long c = hb.cidx(i, j, k);
+          a[q] = hb.x[c];
+          a[npt + q] = hb.y[c];
+          a[2 * npt + q] = hb.z[c];
+          for (int l = 0; l < 6; ++l) a[(3 + l) * npt + q] = pl[l * P + p];
+          // Mach number as update_physical_properties stores it (FieldOperation.cuh:107-140)
+          const double u = pl[P + p], v = pl[2 * P + p], w = pl[3 * P + p];
+          const double vel = std::sqrt(u * u + v * v + w * w);
+          a[9 * npt + q] = ctx->mixture ? vel / pl[(6 + ns) * P + p]
+                                        : vel / std::sqrt(kGammaAir * kRu / kMwAir * pl[5 * P + p]);
+          for (int l = 0; l < ns; ++l) a[(10 + l) * npt + q] = pl[(6 + l) * P + p];
+        }
+    put_f(299.0f);
+    for (int l = 0; l < nvar; ++l) put_i(2);
+    put_i(0);
+    put_i(0);
+    put_i(-1);
+    for (int l = 0; l < nvar; ++l) {
+      const double *v = &a[(size_t)l * npt];
+      double mn = v[0], mxv = v[0];
+      for (long long q = 1; q < npt; ++q) {
+        mn = std::min(mn, v[q]);
+        mxv = std::max(mxv, v[q]);
+      }
+      put_d(mn);
+      put_d(mxv);
+    }
+    put(a.data(), a.size() * sizeof(double));
+  }
+  FILE *f = std::fopen(path, "wb");
+  if (!f) {
+    ctx->err = std::string("ostc_write_plt: cannot open ") + path + " for writing";
+    return OSTC_EIO;
+  }
+  const bool ok = std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+  if (std::fclose(f) != 0 || !ok) {
+    ctx->err = std::string("ostc_write_plt: write to ") + path + " failed";
+    return OSTC_EIO;
+  }
+  return OSTC_OK;
+}
+
+int ostc_read_plt(ostc_ctx *ctx, const char *path, double *solution_time) {
+  if (!ctx || !path) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  FILE *f = std::fopen(path, "rb");
+  if (!f) {
+    ctx->err = std::string("ostc_read_plt: cannot open ") + path;
+    return OSTC_EIO;
+  }
+  std::vector<char> buf;
+  char chunk[1 << 16];
+  size_t got;
+  while ((got = std::fread(chunk, 1, sizeof(chunk), f)) > 0) buf.insert(buf.end(), chunk, chunk + got);
+  std::fclose(f);
+  size_t pos = 0;
+  bool bad = false;
+  auto take = [&](void *dst, size_t n) {
+    if (pos + n > buf.size()) {
+      bad = true;
+      std::memset(dst, 0, n);
+      return;
+    }
+    std::memcpy(dst, buf.data() + pos, n);
+    pos += n;
+  };
+  auto get_i = [&]() { int v; take(&v, 4); return v; };
+  auto get_f = [&]() { float v; take(&v, 4); return v; };
+  auto get_d = [&]() { double v; take(&v, 8); return v; };
+  auto get_s = [&]() {
+    std::string s;
+    for (int c = get_i(); c != 0 && !bad && s.size() < 4096; c = get_i()) s.push_back((char)c);
+    return s;
+  };
+  auto fail = [&](const std::string &why) {
+    ctx->err = std::string("ostc_read_plt: ") + path + ": " + why;
+    return OSTC_EIO;
+  };
+  // header (read_flowfield, Initialize.cuh:102-215)
+  if (buf.size() < 8 || std::memcmp(buf.data(), "#!TDV", 5) != 0) return fail("not a Tecplot binary file");
+  pos = 8;
+  get_i();
+  get_i();
+  get_s();
+  const int nvar = get_i();
+  if (bad || nvar <= 0 || nvar > 4096) return fail("bad variable count");
+  std::vector<std::string> names(nvar);
+  for (auto &n : names) n = get_s();
+  std::vector<std::array<int, 3>> dims;
+  double t0 = 0;
+  float marker = get_f();
+  while (!bad && std::fabs(marker - 299.0f) < 1e-3f) {
+    get_s();
+    get_i();
+    get_i();
+    const double t = get_d();
+    if (dims.empty()) t0 = t;
+    get_i();
+    if (get_i() != 0) return fail("only ordered zones are read");
+    if (get_i() != 0) return fail("only node-located data is read");
+    get_i();
+    get_i();
+    const int d0 = get_i(), d1 = get_i(), d2 = get_i();
+    dims.push_back({d0, d1, d2});
+    if (get_i() != 0) return fail("zone auxiliary data is not read");
+    marker = get_f();
+  }
+  if (bad || std::fabs(marker - 357.0f) > 1e-3f) return fail("header does not end with the end-of-header marker");
+  if (dims.size() != ctx->blk.size()) return fail("zone count differs from the case's block count");
+  auto find = [&](const std::string &n) {
+    for (int l = 0; l < nvar; ++l)
+      if (names[l] == n) return l;
+    return -1;
+  };
+  static const char *const kPrim[6] = {"density", "u", "v", "w", "pressure", "temperature"};
+  int col[6 + kMS];
+  for (int l = 0; l < 6; ++l)
+    if ((col[l] = find(kPrim[l])) < 0) return fail(std::string("no variable '") + kPrim[l] + "'");
+  const int ns = ctx->der.n_spec;
+  for (int l = 0; l < ns; ++l)
+    if ((col[6 + l] = find(ctx->chem.names[l])) < 0) return fail("no variable for species " + ctx->chem.names[l]);
+  for (size_t b = 0; b < ctx->blk.size(); ++b) {
+    const DevBlock &db = ctx->blk[b].db;
+    const int nx = dims[b][0], ny = dims[b][1], nz = dims[b][2];
+    const int g = (nx - db.mx) / 2;
+    if (g < 0 || nx != db.mx + 2 * g || ny != db.my + 2 * g || nz != db.mz + 2 * g)
+      return fail("zone " + std::to_string(b) + " extents do not match block " + std::to_string(b));
+    if (std::fabs(get_f() - 299.0f) > 1e-3f) return fail("missing zone data marker");
+    for (int l = 0; l < nvar; ++l)
+      if (get_i() != 2) return fail("only double-precision variables are read");
+    if (get_i() != 0 || get_i() != 0) return fail("passive or shared variables are not read");
+    get_i();
+    for (int l = 0; l < 2 * nvar; ++l) get_d();
+    const long long npt = (long long)nx * ny * nz;
+    if (bad || pos + (size_t)nvar * npt * 8 > buf.size()) return fail("truncated zone data");
+    const char *a = buf.data() + pos;
+    pos += (size_t)nvar * npt * 8;
+    const long long N = db.n;
+    std::vector<double> bv(6 * N), sv((size_t)ns * N);
+    for (int k = 0; k < db.mz; ++k)
+      for (int j = 0; j < db.my; ++j)
+        for (int i = 0; i < db.mx; ++i) {
+          const long long q = ((long long)(k + g) * ny + (j + g)) * nx + (i + g), n = db.iq(i, j, k);
+          for (int l = 0; l < 6; ++l) std::memcpy(&bv[l * N + n], a + ((size_t)col[l] * npt + q) * 8, 8);
+          for (int l = 0; l < ns; ++l) std::memcpy(&sv[l * N + n], a + ((size_t)col[6 + l] * npt + q) * 8, 8);
+        }
+    if (int r = ostc_set_state(ctx, (int)b, bv.data(), ns ? sv.data() : nullptr, OSTC_HOST)) return r;
+  }
+  // the physical time continues from the file's solution time
+  CK(cudaMemcpyAsync(ctx->d_time, &t0, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (solution_time) *solution_time = t0;
+  return OSTC_OK;
+}
+
 int ostc_stat_enable(ostc_ctx *ctx, int start_step, unsigned flags) {
   if (!ctx) return OSTC_EINVAL;
   if (flags & ~31u) {

@@ -30,7 +30,7 @@ EXPORTS = [
     "ostc_step_kernel_count", "ostc_residual_noalloc", "ostc_set_chem_mode", "ostc_set_conservative",
     "ostc_rhs_vjp", "ostc_rk3_step_vjp", "ostc_adjoint_steps", "ostc_run_states", "ostc_bounds_flags",
     "ostc_bounds_checked", "ostc_stat_enable", "ostc_stat_disable", "ostc_stat_info", "ostc_stat_get",
-    "ostc_stat_export", "ostc_stat_import",
+    "ostc_stat_export", "ostc_stat_import", "ostc_write_plt", "ostc_read_plt",
 ]
 
 
@@ -87,6 +87,8 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.ostc_stat_get.argtypes = [vp, ip, ip, vp, ip]
     lib.ostc_stat_export.argtypes = [vp, ctypes.c_char_p]
     lib.ostc_stat_import.argtypes = [vp, ctypes.c_char_p]
+    lib.ostc_write_plt.argtypes = [vp, ctypes.c_char_p, ip, ctypes.c_double]
+    lib.ostc_read_plt.argtypes = [vp, ctypes.c_char_p, dp]
     lib.ostc_rk3_step.argtypes = [vp, ip, dp]
     lib.ostc_physical_time.argtypes = [vp, dp]
     lib.ostc_store_residual_reference.argtypes = [vp]
@@ -244,6 +246,18 @@ class Solver:
                             None if svi is None else [x.ctypes.data for x in svi],
                             None if svo is None else [x.ctypes.data for x in svo])
         return list(zip(bvo, svo if svo is not None else [None] * len(bvo)))
+
+    # ---- Tecplot flow-field file (FieldIO / read_flowfield)
+    def write_plt(self, path: str, ngg_out: int = 0, solution_time: float | None = None):
+        """Write the current state as the reference's flowfield.plt (binary Tecplot V112)."""
+        t = self.time() if solution_time is None else solution_time
+        self._check(self.lib.ostc_write_plt(self.h, str(path).encode(), ngg_out, t))
+
+    def read_plt(self, path: str) -> float:
+        """Restart every block from a flowfield.plt; returns the file's solution time."""
+        t = ctypes.c_double()
+        self._check(self.lib.ostc_read_plt(self.h, str(path).encode(), ctypes.byref(t)))
+        return t.value
 
     # ---- single-point statistics (SinglePointStat)
     def stat_enable(self, start_step: int = 0, flags: int = 0):
