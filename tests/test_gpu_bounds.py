@@ -1,8 +1,9 @@
 """Index-bounds checks without a memory checker: the bounds-checked build of the library
 (libostc_b200_checked.so, -DOSTC_BOUNDS_CHECK) checks every padded-plane and interior index its
 kernels form through the block accessors, clamps any index outside the block and raises a flag.
-Tiny grids of every path (air AWENO / primitive schemes with each face type, mixtures with the
-flux-split schemes, multi-block interfaces, the adjoint) run through it in a child process; the
+Tiny grids of every path (air AWENO / primitive schemes with each face type, walls, inflows and
+back pressure, mixtures with the flux-split schemes, multi-block interfaces with the statistics
+collector, the adjoint) run through it in a child process; the
 flags must stay 0 and the results must match the oracle as the regular build's do."""
 import json
 import os
@@ -43,10 +44,17 @@ run("muscl_roe_2d", oc.mixing_layer_2d(mx=33, my=17, reconstruction=2, inviscid_
 run("awe5_ausm_outflow_3d", oc.mixing_layer_3d(mx=12, my=10, mz=8, ybc="outflow", reconstruction=4, inviscid_scheme=3), 2)
 run("fr72_3d", oc.reacting_mixing_layer_3d(mx=12, my=10, mz=8), 2, mixture=True)
 run("mix71_3d", oc.reacting_mixing_layer_3d(mx=12, my=10, mz=8, inviscid_scheme=71, finite_rate=False), 2, mixture=True)
+run("wall_iso_3d", oc.mixing_layer_3d(mx=12, my=10, mz=8, ybc="wall"), 2)
+run("wall_adi_2d", oc.mixing_layer_2d(mx=33, my=17, ybc="wall", wall_thermal="adiabatic"), 2)
+run("inflow_3d", oc.mixing_layer_3d(mx=12, my=10, mz=8, xbc="inflow"), 2)
+sub = oc.mixing_layer_3d(mx=12, my=10, mz=8, xbc="subsonic", ybc="outflow")
+sub.bv[1] = np.abs(sub.bv[1]) + 100.0
+run("subsonic_back_pressure_3d", sub, 2)
 mc = oc.multiblock_mixing_layer_3d(nb=3, lo=10, hi=16, my=10, mz=8, seed=1)
 d = oc.write_case(mc, tempfile.mkdtemp())
 s = ostc.Solver(str(d))
 for b, blk in enumerate(mc.blocks): s.set_state(blk.bv, block=b)
+s.stat_enable(0, 31)  # the statistics collector reads every block's ghost layer
 s.step(2)
 out["multiblock_3"] = {"flags": s.bounds_flags(), "err": 0.0}
 print(json.dumps(out))
