@@ -116,3 +116,34 @@ def test_unknown_boundary_type_rejected(built, tmp_path):
     d = oc.write_case(case, tmp_path / "bad")
     with pytest.raises(ostc.OstcError, match="label 5"):
         ostc.probe_case(str(d))
+
+
+def test_boundary_faces_probe(built, tmp_path):
+    """Walls, inflows and back pressure parse on the host (BoundCond.cpp:157-214, 497-560, 704-768):
+    accepted for air, with the refusals the reference makes (subsonic inflow / back pressure with
+    species) or that this path makes (radiative walls, fluctuating inflow, an inflow without struct)."""
+    ok = [("wall", oc.mixing_layer_3d(mx=12, my=10, mz=8, ybc="wall")),
+          ("adiabatic", oc.mixing_layer_2d(mx=33, my=17, ybc="wall", wall_thermal="adiabatic")),
+          ("inflow", oc.mixing_layer_3d(mx=12, my=10, mz=8, xbc="inflow")),
+          ("subsonic", oc.mixing_layer_3d(mx=12, my=10, mz=8, xbc="subsonic", ybc="outflow"))]
+    for name, case in ok:
+        p = ostc.probe_case(str(oc.write_case(case, tmp_path / name)))
+        assert p["n_faces"] == len(case.faces), name
+    bad = oc.reacting_mixing_layer_3d(mx=12, my=10, mz=8)
+    bad.faces[1] = oc.Face(bad.faces[1].raw, 9)
+    bad.bc_structs["back_pressure"] = {"type": ("string", "back_pressure"), "label": ("int", 9),
+                                       "pressure": ("real", 101325.0)}
+    with pytest.raises(ostc.OstcError, match="multi-species"):
+        ostc.probe_case(str(oc.write_case(bad, tmp_path / "bp_mix")))
+    rad = oc.mixing_layer_3d(mx=12, my=10, mz=8, ybc="wall")
+    rad.bc_structs["wall"]["thermal_type"] = ("string", "equilibrium_radiation")
+    with pytest.raises(ostc.OstcError, match="equilibrium_radiation"):
+        ostc.probe_case(str(oc.write_case(rad, tmp_path / "rad")))
+    fl = oc.mixing_layer_3d(mx=12, my=10, mz=8, xbc="inflow")
+    fl.bc_structs["inflow"]["fluctuation_type"] = ("int", 1)
+    with pytest.raises(ostc.OstcError, match="fluctuation_type"):
+        ostc.probe_case(str(oc.write_case(fl, tmp_path / "fl")))
+    nostruct = oc.mixing_layer_3d(mx=12, my=10, mz=8, xbc="inflow")
+    del nostruct.bc_structs["inflow"]
+    with pytest.raises(ostc.OstcError, match="needs a struct"):
+        ostc.probe_case(str(oc.write_case(nostruct, tmp_path / "ns")))
