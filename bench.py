@@ -26,6 +26,10 @@ inviscid + viscous RHS, update, boundaries).  One cell-step = one interior node 
   statistics  one single-point statistics collection (Reynolds / Favre moments, every option on)
            over the default workload and its ghost layer: device time and HBM fraction
 
+--only air|reacting|multiblock runs one workload for a few steps and prints its device time per step
+(the short command to put under a profiler, where the whole benchmark would launch too much); it
+takes --dims, --steps, --precision and --chem.
+
 --impl reference times that C restatement on all host cores (independent sub-grid replicas, one
 process per core): the reference's own implementation of this path exists only as CUDA device code.
 Multi-GPU (torchrun): the path is replicated, one independent case per GPU ("scaling": "weak").
@@ -69,6 +73,8 @@ ALGO_BYTES_PER_NODE = {"flux_x": 152, "flux_y": 192, "flux_z": 192, "visc_update
 MEASURED_TRAFFIC_PER_NODE = {"flux_y": 209.8, "flux_z": 203.3}
 # Whole fused stage (three state passes + metric): 8 (3 n_var + 10) bytes per cell-stage, n_var = 5
 STAGE_BYTES = 8 * (3 * 5 + 10)
+# steps after which the reacting layer's mixed-precision state is compared with the FP64 one
+REACT_ERR_STEPS = 100
 
 
 def parse():
@@ -84,7 +90,43 @@ def parse():
     p.add_argument("--cpu-steps", type=int, default=3)
     p.add_argument("--no-extra", action="store_true",
                    help="skip the reacting (9-species) and uneven multi-block workloads")
-    return p.parse_args()
+    p.add_argument("--only", choices=["air", "reacting", "multiblock"], default=None,
+                   help="run one workload for --steps steps and print its device time per step")
+    p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64", help="with --only")
+    p.add_argument("--chem", choices=["explicit", "point_implicit"], default="explicit", help="with --only")
+    a = p.parse_args()
+    a.dims_given = "--dims" in sys.argv
+    return a
+
+
+def run_only(args):
+    """One workload for args.steps steps (no warm-up, no extras): the command profiled in profiles/."""
+    import ostc
+    import ostc_cases as oc
+
+    tmp = tempfile.mkdtemp(prefix=f"ostc_{args.only}_")
+    if args.only == "multiblock":
+        case = oc.multiblock_mixing_layer_3d(seed=0)
+    elif args.only == "reacting":
+        case = oc.reacting_mixing_layer_3d(*(args.dims if args.dims_given else (384, 192, 96)), seed=0)
+    else:
+        case = oc.mixing_layer_3d(*args.dims, seed=0)
+    oc.write_case(case, tmp)
+    s = ostc.Solver(tmp)
+    s.set_precision(ostc.PREC_MIXED if args.precision == "mixed" else ostc.PREC_FP64)
+    if args.only == "reacting":
+        s.set_chem_mode(ostc.CHEM_POINT_IMPLICIT if args.chem == "point_implicit" else ostc.CHEM_EXPLICIT)
+    if args.only == "multiblock":
+        for b, blk in enumerate(case.blocks):
+            s.set_state(blk.bv, block=b)
+    else:
+        s.set_state(case.bv, sv=getattr(case, "sv", None))
+    ms = s.timed_steps(args.steps)
+    flags = s.error_flags()
+    print(json.dumps({"only": args.only, "nodes": s.total_nodes(), "steps": args.steps, "precision": args.precision,
+                      "ms_per_step": ms / args.steps, "error_flags": flags}))
+    s.close()
+    raise SystemExit(1 if flags else 0)
 
 
 def dist_env():
@@ -379,8 +421,19 @@ def run_ours(args):
                          f"{args.cpu_steps} steps ({cwall:.1f} s)"}
 
     if rank == 0:
+        # compact figures first, so that a truncated copy of the line still carries them
+        summary = {"mixed_speedup": mixed and mixed["speedup_vs_fp64"],
+                   "mixed_rel_l2_rms": mixed and mixed["rel_l2_vs_fp64_rms"]}
+        if extra:
+            em = extra["reacting"]["explicit_mixed"]
+            summary["reacting_mixed_speedup"] = em["speedup_vs_fp64"]
+            summary["reacting_mixed_rel_l2_max"] = max(em["rel_l2_vs_fp64"].values())
+            summary["adjoint_max_rel_diff"] = extra["adjoint"]["theta"]["max_rel_diff"]
+            summary["adjoint_fd_spread"] = extra["adjoint"]["theta"]["max_fd_spread"]
+            summary["multiblock_ms_per_step"] = extra["multiblock"]["ms_per_step"]
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
                 "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                **summary,
                 "dtype": "f64", "data": "synthetic (seeded tanh shear layer + white noise; no dataset)",
                 "config": config_dict(args), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "statistics": stat_line,
@@ -420,10 +473,13 @@ def run_extra(args, local, barrier, allmax, world):
         prof = s.profile(1)
         react[key] = {"value": world * rc.nodes * 5 / (ms / 1e3), "ms_per_step": ms / 5,
                       "kernels_ms_per_step": {k: v[1] for k, v in prof.items()}, "flags": s.error_flags()}
+        if key != "point_implicit":
+            # on to 100 steps (2 warm-up + 5 timed + 1 profiled + 92) for the error of the mixed mode
+            s.step(REACT_ERR_STEPS - 8)
         if key == "explicit":
             ref_cv = s.get_state()[0]
         elif key == "explicit_mixed":
-            # same 8 steps from the same state as the FP64 explicit run: error of the mixed mode
+            # same 100 steps from the same state as the FP64 explicit run: error of the mixed mode
             cv = s.get_state()[0]
             names = ["rho", "rho_u", "rho_v", "rho_w", "rho_E"] + [f"rho_Y_{n}" for n in rc.mixture["tables"].names]
             react[key]["dtype"] = "f32 split fluxes / viscous fluxes / transport, f64 state / Newton / chemistry"
@@ -432,7 +488,8 @@ def run_extra(args, local, barrier, allmax, world):
             react[key]["rel_l2_vs_fp64"] = {names[l]: err[l][1] for l in range(cv.shape[0])}
             react[key]["rel_max_vs_fp64"] = {names[l]: err[l][0] for l in range(cv.shape[0])}
             react[key]["speedup_vs_fp64"] = react["explicit"]["ms_per_step"] / react[key]["ms_per_step"]
-            react[key]["after_steps"] = 8
+            react[key]["after_steps"] = REACT_ERR_STEPS
+            react[key]["flags_after"] = s.error_flags()
         s.close()
     react["value"] = react["explicit"]["value"]
     out["reacting"] = react
@@ -461,8 +518,8 @@ def run_adjoint(local, n_steps=200, every=20):
     """The sensitivity workload of the adjoint (192 x 96 x 48 reacting layer, 9 species, FP64):
     device time of one right-hand-side VJP against one right-hand side, and the gradient of the
     momentum thickness after 200 steps w.r.t. 8 seeded v' mode amplitudes by one checkpointed
-    trajectory adjoint (every 20 steps), checked against central differences for two modes.  dt fixed
-    at the CFL dt of the initial state."""
+    trajectory adjoint (every 20 steps), checked for all eight modes against Richardson-combined central
+    differences (steps 1e-5 and 2e-5).  dt fixed at the CFL dt of the initial state."""
     import ctypes
     import time
 
@@ -520,13 +577,21 @@ def run_adjoint(local, n_steps=200, every=20):
     lam0 = s.adjoint_steps(n_steps, g_n, every=every)
     t_adj = time.perf_counter() - t
     grad = [float(np.sum(lam0 * dm)) for dm in oc.dcv_dmodes(cv0, shapes)]
-    fd = {}
+    # every mode by central differences at two step sizes, h and 2h, Richardson-combined; the gap
+    # between the two plain differences shows how far the differences themselves resolve the gradient
+    # (the Newton iterate's count and the |U| kink of the split fluxes make the 200-step map only
+    # piecewise smooth)
+    fd, spread = {}, {}
     hstep = 1e-5
-    for m in (0, 4):
+    for m in range(8):
         e = np.zeros(8)
         e[m] = 1.0
-        fd[m] = (theta(a0 + hstep * e)[0] - theta(a0 - hstep * e)[0]) / (2 * hstep)
+        d1 = (theta(a0 + hstep * e)[0] - theta(a0 - hstep * e)[0]) / (2 * hstep)
+        d2 = (theta(a0 + 2 * hstep * e)[0] - theta(a0 - 2 * hstep * e)[0]) / (4 * hstep)
+        fd[m] = (4 * d1 - d2) / 3
+        spread[m] = abs(d1 - d2)
     s.close()
+    gmax = max(abs(g) for g in grad)
     return {"workload": "reacting H2/air mixing layer 192x96x48, 9 species, WENO7-Z flux splitting (72), FP64, "
                         f"fixed dt {dt:.3e}",
             "nodes": base.nodes, "rhs_ms": times["rhs"], "rhs_vjp_ms": times["rhs_vjp"],
@@ -534,8 +599,11 @@ def run_adjoint(local, n_steps=200, every=20):
             "theta": {"steps": n_steps, "checkpoint_every": every, "theta": th, "forward_s": t_fwd,
                       "adjoint_s": t_adj, "adjoint_over_forward": t_adj / t_fwd,
                       "dtheta_da": grad,
-                      "central_difference_h1e-5": {f"a{m}": fd[m] for m in fd},
-                      "rel_diff": {f"a{m}": abs(fd[m] - grad[m]) / max(abs(g) for g in grad) for m in fd}},
+                      "central_difference_richardson_h1e-5_2e-5": {f"a{m}": fd[m] for m in fd},
+                      "rel_diff": {f"a{m}": abs(fd[m] - grad[m]) / gmax for m in fd},
+                      "fd_spread_h_vs_2h": {f"a{m}": spread[m] / gmax for m in fd},
+                      "max_rel_diff": max(abs(fd[m] - grad[m]) for m in fd) / gmax,
+                      "max_fd_spread": max(spread.values()) / gmax},
             "timing": "host wall clock around synchronising library calls (device-resident buffers)"}
 
 
@@ -544,7 +612,9 @@ def main():
     world, _, _ = dist_env()
     if world > 1:
         args.gpus = world
-    if args.impl == "reference":
+    if args.only:
+        run_only(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -273,15 +273,20 @@ int ostc_stat_import(ostc_ctx *ctx, const char *dir);
  * bv_new, bv_old: caller-owned device arrays of interior primitive states, [6][n_nodes]
  * (rho,u,v,w,p,T), e.g. the output of ostc_get_state(..., OSTC_DEVICE).  res: host array that
  * receives the RMS changes of rho, |V|, p and T (the same quantities as ostc_residual).  stream:
- * cudaStream_t to run on (NULL = legacy default stream); the call synchronises it.
+ * cudaStream_t to run on (NULL = legacy default stream); the call synchronises it.  A caller that
+ * runs while another thread captures a graph must pass a stream created with cudaStreamNonBlocking:
+ * work on the legacy default stream during another thread's capture of a blocking stream
+ * invalidates that capture.
  * n_nodes above OSTC_NOALLOC_MAX_NODES (67,108,864) is rejected with OSTC_EINVAL; the message is
  * available from ostc_last_error(NULL).
  * Scratch lives in one file-scope __device__ array (per GPU, held until the process exits), shared
  * by every call: calls that overlap on the GPU (different streams, or host threads on the same
  * device) race on it and must be serialised by the caller.  Each call writes every partial it
  * reads, so nothing in the array has to start at zero.  The first call on a device resolves the
- * array's device address (cudaGetSymbolAddress) and caches it; make that first call before any
- * stream capture. */
+ * array's device address (cudaGetSymbolAddress) and caches it with the id of the current context;
+ * a later call in a new context (after cudaDeviceReset, or a primary context released and made
+ * again) resolves it anew.  Make the first call on a device, and the first after such a reset,
+ * before any stream capture. */
 int ostc_residual_noalloc(const double *bv_new, const double *bv_old, long long n_nodes, double res[4],
                           void *stream);
 

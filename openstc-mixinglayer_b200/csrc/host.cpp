@@ -896,6 +896,16 @@ bool resolve_boundaries(const Setup &s, const Derived &d, HostMesh &mesh, std::s
           return false;
         }
         f.struct_name = it->second.second;
+        if (f.type == kSubsonicInflow) {
+          // the total-state ratios have no default (SubsonicInflow::SubsonicInflow reads them with
+          // info.at, BoundCond.cpp:714-715)
+          const auto &st = s.structs.at(f.struct_name);
+          for (const char *key : {"pt_pRef_ratio", "Tt_TRef_ratio"})
+            if (!st.count(key)) {
+              err = "subsonic inflow struct '" + f.struct_name + "' has no " + key;
+              return false;
+            }
+        }
         continue;
       }
       if (f.type == kInflow) {

@@ -10,6 +10,7 @@
 // every GPU loading the library holds until the process exits.
 #include "ostc.h"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -74,7 +75,33 @@ __global__ void k_res_final(double *scratch, int nblocks, long long n) {
 
 std::mutex g_mu;
 constexpr int kMaxDevices = 64;
+// per device: the array's device address and the id of the context it was resolved in.  A context
+// made anew (after cudaDeviceReset, or a primary context released and retained again) loads the
+// module anew, so the address is looked up again whenever the current context's id differs.
 double *g_scratch_ptr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};
+
+// id of the current context (cuCtxGetId: unique over the process lifetime), through the driver entry
+// point the runtime hands out, so the library needs no link against the driver library
+bool current_context_id(unsigned long long *id) {
+  using GetCurrent = CUresult (*)(CUcontext *);
+  using GetId = CUresult (*)(CUcontext, unsigned long long *);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  if (!get_current || !get_id) {
+    void *a = nullptr, *b = nullptr;
+    cudaDriverEntryPointQueryResult qa, qb;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+        qa != cudaDriverEntryPointSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+        qb != cudaDriverEntryPointSuccess)
+      return false;
+    get_current = reinterpret_cast<GetCurrent>(a);
+    get_id = reinterpret_cast<GetId>(b);
+  }
+  CUcontext c = nullptr;
+  return get_current(&c) == CUDA_SUCCESS && c && get_id(c, id) == CUDA_SUCCESS;
+}
 
 }  // namespace
 
@@ -95,12 +122,16 @@ extern "C" int ostc_residual_noalloc(const double *bv_new, const double *bv_old,
     ostc::set_free_error("ostc_residual_noalloc: no current CUDA device");
     return OSTC_ECUDA;
   }
+  // no context may be current yet (cudaGetDevice does not make one); the symbol lookup below binds
+  // the device's primary context, after which its id is read
+  unsigned long long ctx_id = 0;
+  const bool have_ctx = current_context_id(&ctx_id);
   double *scratch = nullptr;
   {
-    // first call on each device: resolve the device address of the static array (host code may not
-    // use the symbol itself; it is only a host-side stand-in)
+    // first call on each device (and in each new context): resolve the device address of the static
+    // array (host code may not use the symbol itself; it is only a host-side stand-in)
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_ptr[dev]) {
+    if (!have_ctx || !g_scratch_ptr[dev] || g_scratch_ctx[dev] != ctx_id) {
       void *p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, g_residual_scratch);
       if (e != cudaSuccess || !p) {
@@ -108,7 +139,12 @@ extern "C" int ostc_residual_noalloc(const double *bv_new, const double *bv_old,
                              cudaGetErrorString(e));
         return OSTC_ECUDA;
       }
+      if (!have_ctx && !current_context_id(&ctx_id)) {
+        ostc::set_free_error("ostc_residual_noalloc: cannot identify the current CUDA context");
+        return OSTC_ECUDA;
+      }
       g_scratch_ptr[dev] = static_cast<double *>(p);
+      g_scratch_ctx[dev] = ctx_id;
     }
     scratch = g_scratch_ptr[dev];
   }

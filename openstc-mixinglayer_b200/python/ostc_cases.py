@@ -60,6 +60,9 @@ class Case:
     freestream: dict | None = None
     # generator parameters a harness may need afterwards (e.g. the velocity difference du)
     extra: dict | None = None
+    # struct names listed in boundary_conditions besides bc_structs (the freestream struct when a face
+    # applies it as an inflow)
+    extra_bc: tuple = ()
 
     @property
     def nodes(self) -> int:
@@ -94,7 +97,7 @@ class Case:
             "bool turbulence = 0",
             "bool limit_flow = 0",
             "array string boundary_conditions {",
-            "    " + " ".join(self.bc_structs.keys()),
+            "    " + " ".join(list(self.bc_structs.keys()) + list(getattr(self, "extra_bc", ()))),
             "}",
         ]
         if self.mixture:
@@ -607,10 +610,13 @@ def mixing_layer_2d(mx=257, my=129, seed=0, steps=100, mc=0.4, re=1000.0, t0=300
 
 def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0, t0=300.0, delta0=1e-3,
                     h=0.125, reconstruction=5, inviscid_scheme=4, cfl=0.5, ybc="farfield",
-                    entropy_fix_factor=0.125, wall_thermal="isothermal", xbc="periodic") -> Case:
+                    entropy_fix_factor=0.125, wall_thermal="isothermal", xbc="periodic", ref_face=False) -> Case:
     """3-D temporal mixing layer: uniform spacing h*delta0, periodic x and z (node-coincident),
     far-field (Riemann-invariant, label 4/41) or outflow (label 6) y faces; u = dU/2 tanh(2y/delta0),
-    Mc = 0.7, plus 1e-2 dU N(0,1) exp(-(y/delta0)^2) seeded white noise in u, v, w."""
+    Mc = 0.7, plus 1e-2 dU N(0,1) exp(-(y/delta0)^2) seeded white noise in u, v, w.
+    ref_face (with xbc="subsonic"): the j = 0 face applies the reference state as a constant inflow
+    (label 5), the configuration in which the reference sets its reference values before it builds a
+    subsonic inflow (its FarField and Inflow faces set them, BoundCond.cu:258-261, BoundCond.cpp:300-310)."""
     rng = np.random.default_rng(seed)
     xs = np.arange(mx) * h
     ys = (np.arange(my) - (my - 1) / 2) * h
@@ -646,6 +652,7 @@ def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0
         structs = {"periodic": {"type": ("string", "periodic"), "label": ("int", 8)},
                    "outflow": {"type": ("string", "outflow"), "label": ("int", 6)}}
     freestream = None
+    extra_bc = ()
     if xbc == "inflow":
         _inflow_x(faces, structs, 1.5, p0, t0)
     elif xbc == "subsonic":
@@ -659,10 +666,13 @@ def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0
         structs["back_pressure"] = {"type": ("string", "back_pressure"), "label": ("int", 9),
                                     "p_pRef_ratio": ("real", 1.0)}
         freestream = dict(mach=mc, pressure=p0, temperature=t0)
+        if ref_face:
+            faces[2] = Face(faces[2].raw, 5)
+            extra_bc = ("freestream",)
     scheme = dict(reconstruction=reconstruction, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=cfl,
                   prandtl_number=0.72, limiter=0, entropy_fix_factor=entropy_fix_factor)
     return Case("mixing_layer_3d", mx, my, mz, X, Y, Z, delta0, faces, structs, scheme, bv, steps,
-                freestream=freestream)
+                freestream=freestream, extra_bc=extra_bc)
 
 
 CHEM_FIXTURE = Path(__file__).resolve().parents[2] / "tests" / "golden" / "chem"

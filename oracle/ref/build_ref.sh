@@ -1,5 +1,6 @@
 #!/bin/bash
-# Builds the reference solver (OpenSTC-MixingLayer, read-only sources under $REF) for parity runs:
+# Builds the reference solver (OpenSTC-MixingLayer, read-only sources under $REF, which the caller
+# must set) for parity runs:
 # .cu files through nvcc for sm_100a with relocatable device code, .cpp files through the host
 # compiler (as the reference's CMake build does), FP64, fmt header-only, the single-rank MPI subset
 # in oracle/ref/mpi.h, MAX_SPEC_NUMBER=9 / MAX_REAC_NUMBER=19.  Outputs go to oracle/_ref/ only:
@@ -8,7 +9,7 @@
 # TEST INFRASTRUCTURE: these binaries are the checker for the oracle, never part of the product.
 set -e
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${REF:-/root/reference}"
+if [ -z "$REF" ]; then echo "REF must name the reference source tree (the directory holding src/)" >&2; exit 2; fi
 OUT="$HERE/../_ref"
 OBJ="$OUT/obj"
 NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"

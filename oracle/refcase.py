@@ -67,7 +67,8 @@ FREESTREAM = """struct freestream = {
 """
 
 
-def write_reference_case(case, steps: int, directory: os.PathLike) -> Path:
+def write_reference_case(case, steps: int, directory: os.PathLike, setup_extra: str = "") -> Path:
+    """setup_extra: setup.txt lines appended last (the reference keeps the last value of a key)."""
     import ostc_cases as oc
 
     d = Path(directory)
@@ -85,7 +86,8 @@ def write_reference_case(case, steps: int, directory: os.PathLike) -> Path:
     (inp / "setup.txt").write_text(setup)
     if not case.freestream:
         setup += "string reference_state = freestream\n"
-        (inp / "setup.txt").write_text(setup)
+    setup += setup_extra
+    (inp / "setup.txt").write_text(setup)
     with open(d / "state_in.bin", "wb") as f:
         for blk in (case.blocks if hasattr(case, "blocks") else [case]):
             np.ascontiguousarray(blk.bv, dtype=np.float64).tofile(f)
@@ -96,13 +98,15 @@ def write_reference_case(case, steps: int, directory: os.PathLike) -> Path:
 
 
 def run_reference(case, steps: int, workdir: os.PathLike | None = None, timeout: int = 1800,
-                  with_seconds: bool = False):
+                  with_seconds: bool = False, setup_extra: str = ""):
     """Returns (cv[n_var,mz,my,mx], bv[6,mz,my,mx], physical time[, sv[n_spec,...] for mixtures]) after
-    `steps` reference RK3 steps, and with_seconds the wall time of the reference's RK3 call."""
+    `steps` reference RK3 steps, and with_seconds the wall time of the reference's RK3 call.  The files
+    the reference writes at the end of its run (output/flowfield.plt, output/stat/coll_*.bin when the
+    setup collects statistics) stay in `workdir`."""
     if not HARNESS.exists():
         raise FileNotFoundError(f"{HARNESS} not built (oracle/ref/build_ref.sh)")
     d = Path(workdir) if workdir else Path(tempfile.mkdtemp(prefix="ostc_ref_"))
-    write_reference_case(case, steps, d)
+    write_reference_case(case, steps, d, setup_extra)
     r = subprocess.run([str(HARNESS), "state_in.bin", "state_out.bin"], cwd=d, capture_output=True, text=True,
                        timeout=timeout)
     if r.returncode != 0:

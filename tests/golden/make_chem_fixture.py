@@ -52,4 +52,6 @@ def main(src: Path):
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference/input"))
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_chem_fixture.py <the reference's input directory>")
+    main(Path(sys.argv[1]))

@@ -5,14 +5,22 @@ path, so its own FP64 CUDA build - compiled from its sources by oracle/ref/build
 oracle/ref/ref_harness.cu through the reference's Driver and RK3 - advances each seeded case, and the
 interior conservative state it reaches is stored here with the case description.
 
-    python tests/golden/make_golden.py [outdir]
+    python tests/golden/make_golden.py [outdir] [case names...]
 
-Each fixture golden_<name>.npz holds cv (5 x mz x my x mx, float64, reference after `steps` steps),
-t (physical time), steps, and the case-generator call; the initial state is regenerated from it
-(ostc_cases, seeded) and its sum is stored as bv0_sum to detect drift of the generator.
+Each fixture golden_<name>.npz holds the case-generator call, steps, t (physical time) and the sum of
+the regenerated initial state (bv0_sum, to detect drift of the generator), and either
+  * cv (n_var x mz x my x mx, float64: the reference state after `steps` steps; cv_<b> per block), or,
+    for the grids of the benchmark sizes (`sampled`), a summary that a test can compare node by node
+    without storing the whole field: 16384 seeded node indices `idx` with the reference's cv there
+    (`cv_s`), the per-variable error scales of the whole field (`smax`, `sl2`: max-abs and L2 norm,
+    the momentum components sharing the momentum vector's, as ostc_cases.relative_errors scales them),
+    and the k-plane and j-plane sums of cv and |cv| (`ksum`, `kabs`, `jsum`, `jabs`);
+  * file_<name>: the bytes of files the reference wrote at the end of its run (its flowfield.plt,
+    its statistics files coll_*.bin), for the cases that keep them.
 """
 import json
 import sys
+import tempfile
 from pathlib import Path
 
 import numpy as np
@@ -20,12 +28,18 @@ import numpy as np
 ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT / "openstc-mixinglayer_b200" / "python"))
 sys.path.insert(0, str(ROOT / "oracle"))
+sys.path.insert(0, str(ROOT / "tests"))
 
 import ostc_cases as oc  # noqa: E402
 import refcase  # noqa: E402
+from golden_util import STAT_SETUP  # noqa: E402
+
+STAT_FILES = ["output/stat/coll_rey_1st.bin", "output/stat/coll_fav_1st.bin", "output/stat/coll_rey_2nd.bin",
+              "output/stat/coll_fav_2nd.bin"]
+PLT = ["output/flowfield.plt"]
 
 CASES = [
-    # name, generator, kwargs, steps
+    # name, generator, kwargs, steps[, options: sampled / setup (extra setup.txt lines) / files (kept)]
     ("ml2d_weno5_ausm", "mixing_layer_2d", dict(mx=65, my=33, reconstruction=4, inviscid_scheme=3), 100),
     ("ml2d_weno7_hllc", "mixing_layer_2d", dict(mx=65, my=33, reconstruction=5, inviscid_scheme=4), 50),
     ("ml3d_weno7_hllc_farfield", "mixing_layer_3d",
@@ -50,31 +64,133 @@ CASES = [
     ("mb3d_awe7_hllc", "multiblock_mixing_layer_3d", dict(dims=[20, 17, 23], my=16, mz=10), 10),
     ("mb2d_awe5_ausm", "multiblock_mixing_layer_3d",
      dict(dims=[30, 21, 26, 18], my=24, mz=1, reconstruction=4, inviscid_scheme=3), 20),
+    # the benchmark configurations at their stated sizes (or a 3-D grid of the same shape family):
+    # the 2-D layer exactly (256 x 128 cells, node-coincident periodic x, 100 steps) ...
+    ("c1_ml2d_256x128_weno5_ausm", "mixing_layer_2d", dict(mx=257, my=129), 100),
+    # ... the 3-D air layer (WENO7-Z + HLLC, viscous, far-field y) at 1/64 of its nodes over 20 steps
+    # and at its full 512 x 256 x 128 over 3 steps ...
+    ("c2_ml3d_128x64x32_weno7_hllc", "mixing_layer_3d", dict(mx=128, my=64, mz=32), 20, dict(sampled=True)),
+    ("c2_ml3d_512x256x128_weno7_hllc", "mixing_layer_3d", dict(), 3, dict(sampled=True)),
+    # ... the reacting 9-species layer (flux-split WENO7, finite-rate chemistry) at 1/64 of its nodes
+    ("c3_rml3d_96x48x24_fr72", "reacting_mixing_layer_3d", dict(mx=96, my=48, mz=24), 20, dict(sampled=True)),
+    # ... and a twelve-block chain of uneven i extents
+    ("c4_mb3d_12_blocks", "multiblock_mixing_layer_3d", dict(dims=None, my=18, mz=8), 10),
+    # boundary faces beyond the mixing-layer set: no-slip walls, constant supersonic inflow, subsonic
+    # inflow with back pressure (air), walls and inflow for the mixture
+    ("ml3d_wall_isothermal", "mixing_layer_3d", dict(mx=32, my=24, mz=16, ybc="wall"), 10),
+    ("ml3d_wall_adiabatic", "mixing_layer_3d", dict(mx=32, my=24, mz=16, ybc="wall", wall_thermal="adiabatic"), 10),
+    ("ml2d_wall_isothermal_weno5", "mixing_layer_2d", dict(mx=65, my=33, ybc="wall"), 20),
+    ("ml2d_wall_adiabatic_weno7", "mixing_layer_2d",
+     dict(mx=65, my=33, reconstruction=5, inviscid_scheme=4, ybc="wall", wall_thermal="adiabatic"), 20),
+    ("ml3d_inflow_outflow", "mixing_layer_3d", dict(mx=32, my=20, mz=12, ybc="outflow", xbc="inflow"), 10),
+    # (the j = 0 face applies the reference state: the reference builds a subsonic inflow only after a
+    # far-field or inflow face has set its reference values)
+    ("ml3d_subsonic_backpressure", "mixing_layer_3d",
+     dict(mx=32, my=20, mz=12, ybc="outflow", xbc="subsonic", ref_face=True), 10),
+    ("rml3d_wall", "reacting_mixing_layer_3d", dict(mx=20, my=16, mz=10, ybc="wall"), 5),
+    ("rml3d_inflow", "reacting_mixing_layer_3d", dict(mx=24, my=16, mz=10, xbc="inflow"), 5),
+    # the files the reference writes at the end of a run: flow field and statistics
+    ("ml3d_stat_plt", "mixing_layer_3d", dict(mx=16, my=12, mz=8, ybc="outflow"), 6,
+     dict(setup=STAT_SETUP, files=PLT + STAT_FILES)),
+    ("rml3d_stat_plt", "reacting_mixing_layer_3d", dict(mx=12, my=10, mz=6), 5,
+     dict(setup=STAT_SETUP, files=PLT + STAT_FILES)),
+    ("ml2d_plt", "mixing_layer_2d", dict(mx=33, my=17, ybc="wall"), 5, dict(files=PLT)),
 ]
+
+N_SAMPLE = 16384
+
+
+def reference_dt_defined(nodes: int) -> bool:
+    """Whether the reference's CFL minimum is defined for a block of this many nodes.  Its min_of_arr /
+    block_reduce_min (TimeAdvanceFunc.cu:70-89, gxl_lib/MyAtomic.cuh:33-64) read the shared-memory slot
+    of a warp that never wrote it when the last 128-thread block of a pass holds 32, 64 or 96 entries:
+    the first pass over the nodes, and the second over the per-block minima (one per 128 nodes)."""
+    first = nodes % 128
+    second = -(-nodes // 128)
+    return first not in (32, 64, 96) and second not in (32, 64, 96)
+
+
+def c4_dims(nb=12, lo=12, hi=30, my=18, mz=8, seed=4):
+    """Seeded uneven i extents of a twelve-block chain, each a block size the reference's dt is defined for."""
+    rng = np.random.default_rng(seed)
+    dims = []
+    while len(dims) < nb:
+        mx = int(rng.integers(lo, hi + 1))
+        if reference_dt_defined(mx * my * mz):
+            dims.append(mx)
+    return dims
+
+
+for _e in CASES:
+    if _e[0] == "c4_mb3d_12_blocks":
+        _e[2]["dims"] = c4_dims()
 
 
 def make_case(gen, kw):
     return getattr(oc, gen)(**kw)
 
 
-def main(outdir: Path, only=None):
+def scales(cv):
+    """Per-variable (max-abs, L2) error scales as ostc_cases.relative_errors forms them."""
+    mom = slice(1, 4)
+    mom_max = float(np.max(np.sqrt(np.sum(cv[mom] ** 2, axis=0))))
+    mom_l2 = float(np.linalg.norm(cv[mom]))
+    smax, sl2 = [], []
+    for l in range(cv.shape[0]):
+        if 1 <= l <= 3:
+            smax.append(mom_max)
+            sl2.append(mom_l2)
+        else:
+            smax.append(float(np.max(np.abs(cv[l]))))
+            sl2.append(float(np.linalg.norm(cv[l])))
+    return np.array(smax), np.array(sl2)
+
+
+def summarize(cv, seed=2024):
+    nv = cv.shape[0]
+    flat = cv.reshape(nv, -1)
+    n = flat.shape[1]
+    idx = np.sort(np.random.default_rng(seed).choice(n, size=min(N_SAMPLE, n), replace=False))
+    smax, sl2 = scales(cv)
+    return dict(idx=idx, cv_s=flat[:, idx].copy(), smax=smax, sl2=sl2, ksum=cv.sum(axis=(2, 3)),
+                kabs=np.abs(cv).sum(axis=(2, 3)), jsum=cv.sum(axis=(1, 3)), jabs=np.abs(cv).sum(axis=(1, 3)))
+
+
+def main(outdir: Path, only=None) -> int:
     outdir.mkdir(parents=True, exist_ok=True)
-    for name, gen, kw, steps in CASES:
+    failed = []
+    for entry in CASES:
+        name, gen, kw, steps = entry[:4]
+        opts = entry[4] if len(entry) > 4 else {}
         if only and name not in only:
             continue
         case = make_case(gen, kw)
-        cv, bv, t = refcase.run_reference(case, steps)[:3]
         meta = json.dumps({"generator": gen, "kwargs": kw})
+        try:
+            with tempfile.TemporaryDirectory(prefix="ostc_ref_") as wd:
+                cv, bv, t = refcase.run_reference(case, steps, wd, setup_extra=opts.get("setup", ""))[:3]
+                files = {}
+                for rel in opts.get("files", []):
+                    files["file_" + Path(rel).name] = np.frombuffer((Path(wd) / rel).read_bytes(), dtype=np.uint8)
+        except (RuntimeError, OSError) as e:
+            print(name, "FAILED:", e, flush=True)
+            failed.append(name)
+            continue
+        common = dict(t=t, steps=steps, case=meta, **files)
         if hasattr(case, "blocks"):
             arrays = {f"cv_{b}": c for b, c in enumerate(cv)}
-            np.savez_compressed(outdir / f"golden_{name}.npz", t=t, steps=steps, case=meta, n_block=len(cv),
-                                bv0_sum=float(sum(np.sum(b.bv) for b in case.blocks)), **arrays)
+            np.savez_compressed(outdir / f"golden_{name}.npz", n_block=len(cv),
+                                bv0_sum=float(sum(np.sum(b.bv) for b in case.blocks)), **common, **arrays)
             print(name, "t =", t, "blocks", len(cv), flush=True)
             continue
-        np.savez_compressed(outdir / f"golden_{name}.npz", cv=cv, t=t, steps=steps, case=meta,
-                            bv0_sum=float(np.sum(case.bv)))
+        if opts.get("sampled"):
+            np.savez_compressed(outdir / f"golden_{name}.npz", sampled=True, bv0_sum=float(np.sum(case.bv)),
+                                **common, **summarize(cv))
+        else:
+            np.savez_compressed(outdir / f"golden_{name}.npz", cv=cv, bv0_sum=float(np.sum(case.bv)), **common)
         print(name, "t =", t, "rho range", float(bv[0].min()), float(bv[0].max()), flush=True)
+    return 1 if failed else 0
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path(__file__).resolve().parent, sys.argv[2:] or None)
+    sys.exit(main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path(__file__).resolve().parent, sys.argv[2:] or None))

@@ -1,0 +1,146 @@
+"""Loading and comparing the reference-build fixtures (tests/golden/golden_*.npz, written by
+tests/golden/make_golden.py from the reference's own FP64 CUDA build).  Test helpers only.
+
+Bar: 1e-12 relative per conserved variable (max norm and L2, ostc_cases.relative_errors), the physical
+time to 1e-13.  Fixtures of the benchmark-size grids hold a seeded sample of nodes plus k- and j-plane
+sums instead of the whole field; they are compared at the sampled nodes (same bar; max-abs against the
+whole field's scale) and on every plane sum (difference within 1e-12 of the plane's sum of |cv|, the
+momentum components against the momentum's).
+"""
+import glob
+import json
+from pathlib import Path
+
+import numpy as np
+
+import ostc_cases as oc
+
+HERE = Path(__file__).resolve().parent
+TOL = 1e-12
+TOL_T = 1e-13
+
+# statistics collection in the reference's own setup keys (SinglePointStat, RK.cuh:200-207): collected
+# after every step past step 2, exported with the flow field when the run ends
+STAT_SETUP = """
+bool if_collect_statistics = 1
+int start_collect_statistics_iter = 2
+bool rho_p_correlation = 1
+array string stat_rey_1st {
+    T u
+}
+"""
+# variables compared against one shared scale (velocity and momentum components, their products)
+SCALE_GROUPS = [{"u", "v", "w"}, {"rhoU", "rhoV", "rhoW"},
+                {"rhoUU", "rhoVV", "rhoWW", "rhoUV", "rhoUW", "rhoVW"}]
+
+
+def assert_fields(names, got, ref, tol=TOL):
+    """Per named plane: max |got - ref| within tol of the max |ref| of the plane (or of its group)."""
+    scale = {n: float(np.max(np.abs(r))) for n, r in zip(names, ref)}
+    for g in SCALE_GROUPS:
+        m = max((scale[n] for n in g if n in scale), default=0.0)
+        for n in g:
+            if n in scale:
+                scale[n] = m
+    for n, a, r in zip(names, got, ref):
+        d = float(np.max(np.abs(a - r)))
+        assert d <= tol * scale[n] or d == 0.0, (n, d, scale[n])
+
+
+def fixture_path(name: str) -> Path:
+    return HERE / "golden" / f"golden_{name}.npz"
+
+
+def all_fixtures():
+    return sorted(glob.glob(str(HERE / "golden" / "golden_*.npz")))
+
+
+def name_of(path) -> str:
+    return Path(path).stem[len("golden_"):]
+
+
+def load(path):
+    """(case, steps, npz, t_ref); checks that the seeded case generator still makes the same state."""
+    z = np.load(path)
+    meta = json.loads(str(z["case"]))
+    case = getattr(oc, meta["generator"])(**meta["kwargs"])
+    total = sum(np.sum(b.bv) for b in case.blocks) if "n_block" in z else np.sum(case.bv)
+    assert abs(total - float(z["bv0_sum"])) <= 1e-12 * abs(float(z["bv0_sum"])), "case generator drifted"
+    return case, int(z["steps"]), z, float(z["t"])
+
+
+def meta(path):
+    """(generator kwargs, steps, sampled, multi-block, mixture, node count) without building the case."""
+    z = np.load(path)
+    m = json.loads(str(z["case"]))
+    return m, int(z["steps"]), "sampled" in z.files, "n_block" in z.files
+
+
+def sampled_errors(cv, z):
+    nv = cv.shape[0]
+    got = cv.reshape(nv, -1)[:, z["idx"]]
+    ref = z["cv_s"]
+    errs = []
+    for l, (mx, l2) in enumerate(oc.relative_errors(got[:, None, None, :], ref[:, None, None, :])):
+        d = np.abs(got[l] - ref[l])
+        errs.append((max(mx, float(np.max(d)) / float(z["smax"][l])), l2))
+    return errs
+
+
+def plane_errors(cv, z):
+    """Largest relative difference of the k-plane and j-plane sums per variable."""
+    out = []
+    ksum, jsum = cv.sum(axis=(2, 3)), cv.sum(axis=(1, 3))
+    kabs, jabs = z["kabs"].copy(), z["jabs"].copy()
+    kabs[1:4] = kabs[1:4].sum(axis=0)
+    jabs[1:4] = jabs[1:4].sum(axis=0)
+    for l in range(cv.shape[0]):
+        ek = np.max(np.abs(ksum[l] - z["ksum"][l]) / kabs[l])
+        ej = np.max(np.abs(jsum[l] - z["jsum"][l]) / jabs[l])
+        out.append(float(max(ek, ej)))
+    return out
+
+
+def assert_state(cv, z, block=None):
+    if block is not None:
+        err = oc.relative_errors(cv, z[f"cv_{block}"])
+        assert all(m < TOL and l2 < TOL for m, l2 in err), (block, err)
+        return
+    if "sampled" in z.files:
+        err = sampled_errors(cv, z)
+        assert all(m < TOL and l2 < TOL for m, l2 in err), err
+        pe = plane_errors(cv, z)
+        assert all(e < TOL for e in pe), pe
+        return
+    err = oc.relative_errors(cv, z["cv"])
+    assert all(m < TOL and l2 < TOL for m, l2 in err), err
+
+
+def run_library(case, steps, directory, setup_extra=""):
+    """Advances the case `steps` SSP-RK3 steps through the C ABI; returns the open solver."""
+    import ostc
+
+    d = oc.write_case(case, directory)
+    if setup_extra:
+        (d / "setup.txt").write_text((d / "setup.txt").read_text() + setup_extra)
+    s = ostc.Solver(str(d))
+    if hasattr(case, "blocks"):
+        for b, blk in enumerate(case.blocks):
+            s.set_state(blk.bv, block=b)
+    else:
+        s.set_state(case.bv, sv=case.sv)
+    s.step(steps)
+    return s
+
+
+def check_library(case, steps, z, t_ref, directory, setup_extra=""):
+    """Runs the library and checks its state and time against the fixture; returns the solver."""
+    s = run_library(case, steps, directory, setup_extra)
+    if hasattr(case, "blocks"):
+        for b in range(int(z["n_block"])):
+            assert_state(s.get_state(block=b)[0], z, block=b)
+    else:
+        assert_state(s.get_state()[0], z)
+    assert abs(s.time() - t_ref) <= TOL_T * t_ref
+    assert s.error_flags() == 0
+    return s

@@ -14,59 +14,9 @@ import pytest
 
 import ostc
 import ostc_cases as oc
+from ref_files import read_plt
 
 pytestmark = pytest.mark.gpu
-
-
-def read_plt(path):
-    """Minimal reader of the V112 layout that ostc_write_plt and the reference's FieldIO write."""
-    raw = path.read_bytes()
-    pos = 8
-    assert raw[:8] == b"#!TDV112"
-
-    def take(fmt, n=1):
-        nonlocal pos
-        v = np.frombuffer(raw, dtype=fmt, count=n, offset=pos)
-        pos += v.nbytes
-        return v
-
-    def s():
-        out = ""
-        while True:
-            c = int(take(np.int32)[0])
-            if c == 0:
-                return out
-            out += chr(c)
-
-    byte_order, file_type = (int(x) for x in take(np.int32, 2))
-    assert (byte_order, file_type) == (1, 0)
-    assert s() == "Solution file"
-    nvar = int(take(np.int32)[0])
-    names = [s() for _ in range(nvar)]
-    zones = []
-    marker = float(take(np.float32)[0])
-    while marker == 299.0:
-        name = s()
-        parent, strand = (int(x) for x in take(np.int32, 2))
-        t = float(take(np.float64)[0])
-        color, ztype, loc, raw_nb, misc = (int(x) for x in take(np.int32, 5))
-        dims = tuple(int(x) for x in take(np.int32, 3))
-        aux = int(take(np.int32)[0])
-        assert (parent, strand, color, ztype, loc, raw_nb, misc, aux) == (-1, -2, -1, 0, 0, 0, 0, 0)
-        zones.append((name, t, dims))
-        marker = float(take(np.float32)[0])
-    assert marker == 357.0
-    data = []
-    for _, _, (nx, ny, nz) in zones:
-        assert float(take(np.float32)[0]) == 299.0
-        assert list(take(np.int32, nvar)) == [2] * nvar
-        assert [int(x) for x in take(np.int32, 3)] == [0, 0, -1]
-        mm = take(np.float64, 2 * nvar).reshape(nvar, 2)
-        arr = take(np.float64, nvar * nx * ny * nz).reshape(nvar, nz, ny, nx)
-        assert np.array_equal(mm[:, 0], arr.min(axis=(1, 2, 3))) and np.array_equal(mm[:, 1], arr.max(axis=(1, 2, 3)))
-        data.append(arr)
-    assert pos == len(raw)
-    return names, zones, data
 
 
 @pytest.mark.parametrize("kind", ["air3d", "air2d", "mixture"])
@@ -145,3 +95,24 @@ def test_plt_two_blocks_and_rejections(built, tmp_path):
     (tmp_path / "junk.plt").write_bytes(b"not a plot file")
     with pytest.raises(ostc.OstcError, match="not a Tecplot"):
         s1.read_plt(tmp_path / "junk.plt")
+
+
+# ---- against the flowfield.plt the reference itself wrote at the end of the same run (FieldIO.h:73-450,
+# ngg_out 0 as RK3 uses, RK.cuh:57,204); fixtures from tests/golden/make_golden.py
+
+@pytest.mark.parametrize("name", ["ml3d_stat_plt", "rml3d_stat_plt", "ml2d_plt"])
+def test_plt_matches_reference_file(built, tmp_path, name):
+    import golden_util as gu
+
+    case, steps, z, t_ref = gu.load(gu.fixture_path(name))
+    s = gu.check_library(case, steps, z, t_ref, tmp_path / name, gu.STAT_SETUP if "stat" in name else "")
+    s.write_plt(tmp_path / "flowfield.plt", ngg_out=0)
+    names, zones, data = read_plt(tmp_path / "flowfield.plt")
+    rnames, rzones, rdata = read_plt(z["file_flowfield.plt"].tobytes())
+    assert names == rnames
+    assert [(zn, dims) for zn, _, dims in zones] == [(zn, dims) for zn, _, dims in rzones]
+    for (_, t, _), (_, rt, _) in zip(zones, rzones):
+        assert abs(t - rt) <= gu.TOL_T * rt
+    for got, ref in zip(data, rdata):
+        gu.assert_fields(names, got, ref)
+    s.close()

@@ -11,6 +11,7 @@ import pytest
 import ostc
 import ostc_cases as oc
 from oracle import MultiOracle, Oracle
+from ref_files import read_stat_file
 
 pytestmark = pytest.mark.gpu
 
@@ -104,40 +105,6 @@ def test_stat_multiblock_matches_oracle(built, tmp_path):
     _run_and_compare(s, lambda: m.step(1), m.blocks, ALL, 4, 0)
 
 
-def _read_stat_file(path):
-    """The reference's coll_*.bin layout: int32 n_block, n_var, ngg; names as int32 characters each
-    ended by 0; int32 counters[n_var]; per block int32 mx, my, mz and n_var planes of doubles."""
-    raw = path.read_bytes()
-    pos = 0
-
-    def ints(n):
-        nonlocal pos
-        v = np.frombuffer(raw, dtype=np.int32, count=n, offset=pos)
-        pos += 4 * n
-        return [int(x) for x in v]
-
-    nb, nv, ngg = ints(3)
-    names = []
-    for _ in range(nv):
-        name = ""
-        while True:
-            (c,) = ints(1)
-            if c == 0:
-                break
-            name += chr(c)
-        names.append(name)
-    counters = ints(nv)
-    blocks = []
-    for _ in range(nb):
-        mx, my, mz = ints(3)
-        n = nv * (mx + 2 * ngg) * (my + 2 * ngg) * (mz + 2 * ngg)
-        data = np.frombuffer(raw, dtype=np.float64, count=n, offset=pos)
-        pos += 8 * n
-        blocks.append(((mx, my, mz), data.reshape(nv, mz + 2 * ngg, my + 2 * ngg, mx + 2 * ngg)))
-    assert pos == len(raw)
-    return nb, ngg, names, counters, blocks
-
-
 def test_stat_export_import_and_setup(built, tmp_path):
     """Setup-driven collection (if_collect_statistics, start_collect_statistics_iter, stat_rey_1st in the
     listed order, rho_p_correlation), the exported files, and a continued collection from them."""
@@ -159,7 +126,7 @@ def test_stat_export_import_and_setup(built, tmp_path):
                     ["RhoRho", "pp", "rhoP"],
                     ["rhoUU", "rhoVV", "rhoWW", "rhoUV", "rhoUW", "rhoVW", "rhoTT"] + ["rho" + n + n for n in names]]
     for g, fname in enumerate(["coll_rey_1st.bin", "coll_fav_1st.bin", "coll_rey_2nd.bin", "coll_fav_2nd.bin"]):
-        nb, ngg, fnames, counters, blocks = _read_stat_file(out / fname)
+        nb, ngg, fnames, counters, blocks = read_stat_file(out / fname)
         assert (nb, ngg) == (1, 1) and fnames == expect_names[g] and counters == [2] * n_var[g]
         assert blocks[0][0] == (16, 12, 8)
         assert np.array_equal(blocks[0][1], s.stat_get(g))
@@ -223,3 +190,25 @@ def test_stat_off_and_bad_flags(built, tmp_path):
     s.stat_disable()
     with pytest.raises(ostc.OstcError):
         s.stat_get(0)
+
+
+# ---- against the coll_*.bin files the reference itself exported at the end of the same run
+# (SinglePointStat.cu:515-706, RK.cuh:200-207); fixtures from tests/golden/make_golden.py
+
+@pytest.mark.parametrize("name", ["ml3d_stat_plt", "rml3d_stat_plt"])
+def test_stat_matches_reference_files(built, tmp_path, name):
+    import golden_util as gu
+
+    case, steps, z, t_ref = gu.load(gu.fixture_path(name))
+    s = gu.check_library(case, steps, z, t_ref, tmp_path / name, gu.STAT_SETUP)
+    out = tmp_path / "stat"
+    out.mkdir()
+    s.stat_export(out)
+    for fname in ["coll_rey_1st.bin", "coll_fav_1st.bin", "coll_rey_2nd.bin", "coll_fav_2nd.bin"]:
+        nb, ngg, names, counters, blocks = read_stat_file(out / fname)
+        rnb, rngg, rnames, rcounters, rblocks = read_stat_file(z["file_" + fname].tobytes())
+        assert (nb, ngg, names, counters) == (rnb, rngg, rnames, rcounters), fname
+        for (ext, got), (rext, ref) in zip(blocks, rblocks):
+            assert ext == rext
+            gu.assert_fields(names, got, ref)
+    s.close()

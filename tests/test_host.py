@@ -121,7 +121,8 @@ def test_unknown_boundary_type_rejected(built, tmp_path):
 def test_boundary_faces_probe(built, tmp_path):
     """Walls, inflows and back pressure parse on the host (BoundCond.cpp:157-214, 497-560, 704-768):
     accepted for air, with the refusals the reference makes (subsonic inflow / back pressure with
-    species) or that this path makes (radiative walls, fluctuating inflow, an inflow without struct)."""
+    species, a subsonic inflow without its total-state ratios) or that this path makes (radiative walls,
+    fluctuating inflow, an inflow without struct)."""
     ok = [("wall", oc.mixing_layer_3d(mx=12, my=10, mz=8, ybc="wall")),
           ("adiabatic", oc.mixing_layer_2d(mx=33, my=17, ybc="wall", wall_thermal="adiabatic")),
           ("inflow", oc.mixing_layer_3d(mx=12, my=10, mz=8, xbc="inflow")),
@@ -143,6 +144,11 @@ def test_boundary_faces_probe(built, tmp_path):
     fl.bc_structs["inflow"]["fluctuation_type"] = ("int", 1)
     with pytest.raises(ostc.OstcError, match="fluctuation_type"):
         ostc.probe_case(str(oc.write_case(fl, tmp_path / "fl")))
+    for key in ("pt_pRef_ratio", "Tt_TRef_ratio"):
+        sub = oc.mixing_layer_3d(mx=12, my=10, mz=8, xbc="subsonic", ybc="outflow")
+        del sub.bc_structs["subsonic_inflow"][key]
+        with pytest.raises(ostc.OstcError, match=key):
+            ostc.probe_case(str(oc.write_case(sub, tmp_path / ("sub_" + key))))
     nostruct = oc.mixing_layer_3d(mx=12, my=10, mz=8, xbc="inflow")
     del nostruct.bc_structs["inflow"]
     with pytest.raises(ostc.OstcError, match="needs a struct"):
