@@ -198,7 +198,7 @@ class Case:
         """Inflow ctor (BoundCond.cpp:157-214) of constant inflows: label -> density, velocity
         (Mach times the speed of sound along (u, v, w)), pressure, temperature and mass fractions y."""
         out = {}
-        for st in self.bc_structs.values():
+        for st in self.face_structs():
             if st.get("type", (None, None))[1] != "inflow":
                 continue
             g = {k: v for k, (t, v) in st.items()}
@@ -258,11 +258,25 @@ class Case:
                                    wall_adiabatic=int(g.get("thermal_type", "isothermal") == "adiabatic"))
         return out
 
+    def face_structs(self):
+        """The boundary structs faces may apply: bc_structs, plus the freestream struct when
+        boundary_conditions lists it (extra_bc)."""
+        out = list(self.bc_structs.values())
+        if "freestream" in getattr(self, "extra_bc", ()) and self.freestream:
+            f = self.freestream
+            st = {"type": ("string", "inflow"), "label": ("int", 5), "mach": ("real", f["mach"]),
+                  "pressure": ("real", f["pressure"]), "temperature": ("real", f["temperature"]),
+                  "u": ("real", 1.0), "v": ("real", 0.0), "w": ("real", 0.0)}
+            for k, v in f.get("Y", {}).items():
+                st[k] = ("real", v)
+            out.append(st)
+        return out
+
     def label_types(self):
         types = {"wall": 2, "symmetry": 3, "farfield": 4, "inflow": 5, "outflow": 6, "subsonic_inflow": 7,
                  "periodic": 8, "back_pressure": 9}
         m = {}
-        for st in self.bc_structs.values():
+        for st in self.face_structs():
             m[st["label"][1]] = types[st["type"][1]]
         return m
 
@@ -394,6 +408,9 @@ class MultiCase:
 
     def farfield_states(self):
         return Case.farfield_states(self)
+
+    def face_structs(self):
+        return Case.face_structs(self)
 
     def label_types(self):
         return Case.label_types(self)
