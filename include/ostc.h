@@ -194,6 +194,22 @@ int ostc_device_view(ostc_ctx *ctx, int block, ostc_zone_view *out);
  * families written (<= max). */
 int ostc_profile_steps(ostc_ctx *ctx, int n_steps, int max, const char **names, int *launches, double *ms);
 
+/* Pin the kernel shape of one inviscid sweep (AWENO path) instead of the autotuner's choice:
+ * precision 0 = FP64, 1 = mixed; dir 0/1/2 = x/y/z; variant 0.. (x: 0 only, one thread per face;
+ * y/z: 0 column march, 1-3 shared-memory tiles of three shapes), or
+ * -1 to return the direction to the autotuner (forgetting its cached result for these block shapes).
+ * Every variant computes the same face fluxes with the same expressions; the choice changes speed,
+ * not results.  Takes effect at the next step.  No reference counterpart (its sweep kernels have one
+ * fixed shape). */
+int ostc_set_sweep_variant(ostc_ctx *ctx, int precision, int dir, int variant);
+
+/* What the sweep autotuner measured for one block: precision 0 = FP64, 1 = mixed; dir 0/1/2 = x/y/z.
+ * chosen receives the variant the steps use (-1 before tuning); ms[v] the device milliseconds of
+ * one launch of variant v as timed by the tuner (0 where it was not timed in this context, e.g. a
+ * result reused from an earlier context of the same shape).  Returns the variant count of that
+ * direction.  No reference counterpart: the reference has one fixed kernel shape per sweep. */
+int ostc_tune_report(ostc_ctx *ctx, int block, int precision, int dir, int *chosen, float *ms, int max);
+
 /* Number of interior nodes over all blocks (the unit of cell-steps/s). */
 int ostc_total_nodes(const ostc_ctx *ctx, long long *n);
 
@@ -259,6 +275,20 @@ int ostc_stat_export(ostc_ctx *ctx, const char *dir);
  * read_previous_statistical_data): the selection must match the enabled one and the block extents
  * the case's, else OSTC_EIO with the reason.  Collection then continues from the next step. */
 int ostc_stat_import(ostc_ctx *ctx, const char *dir);
+
+/* The reference's steady driver (steady_simulation, SteadySim.cuh:15-140, as Simulate.cuh selects it for
+ * steady = 1): up to max_iter iterations, each over every block and in place: dq from the chemical
+ * source (with its Jacobian for chemSrcMethod 1 / 2) and the inviscid and viscous fluxes; local time
+ * steps (local_time_step, TimeAdvanceFunc.cuh:28-83); implicit_treatment (ImplicitTreatmentHPP.cuh:7-54):
+ * with implicit_method 0 the point-implicit chemistry (EPI / DA, FiniteRateChem.cu:233-254, 414-426),
+ * with 1 DPLUR with DPLUR_inner_step inner iterations (DPLUR.cuh:14-327); update_cv_and_bv
+ * (FieldOperation.cuh:189-232); boundary faces, interfaces, properties.  The settings come from the
+ * setup (implicit_method, DPLUR_inner_step, chemSrcMethod, convergence_criteria, output_screen).  As the
+ * reference, it computes the residual (RMS change of rho, |V|, p, T, scaled by that of the first
+ * iteration) after iteration 1 and every output_screen-th and stops once its largest component falls
+ * below convergence_criteria.  iters_done / err_max (nullable) receive the iterations run and the last
+ * scaled residual (-1 if none was computed).  The physical time does not advance.  Synchronises. */
+int ostc_steady_step(ostc_ctx *ctx, int max_iter, int *iters_done, double *err_max);
 
 /* Limits of ostc_residual_noalloc: its static scratch holds one partial sum set per block of
  * 256 threads x 64 nodes, for at most OSTC_NOALLOC_MAX_BLOCKS blocks (128 KB of device memory). */

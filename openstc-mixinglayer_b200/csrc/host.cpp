@@ -36,6 +36,8 @@ void Setup::set_defaults() {
   strings["therm_file"] = "chemistry/therm.dat";
   strings["transport_file"] = "chemistry/tran.dat";
   ints["chemSrcMethod"] = 0;
+  ints["DPLUR_inner_step"] = 3;         // Parameter.cpp:450
+  reals["convergence_criteria"] = 1e-8;  // Parameter.cpp:451
   bools["turbulence"] = false;
   ints["turbulence_method"] = 1;
   ints["RANS_model"] = 2;
@@ -244,8 +246,30 @@ bool derive(const Setup &s, Derived &d, std::string &err) {
     err = "turbulence models are outside this library's path (laminar/DNS only)";
     return false;
   }
-  if (d.steady || d.temporal_scheme != 3) {
-    err = "only unsteady SSP-RK3 (steady = 0, temporal_scheme = 3) is on this library's path";
+  if (!d.steady && d.temporal_scheme != 3) {
+    err = "temporal_scheme " + std::to_string(d.temporal_scheme) +
+          ": of the unsteady drivers this library runs SSP-RK3 (temporal_scheme = 3); steady = 1 runs the steady "
+          "driver";
+    return false;
+  }
+  // steady driver settings (Parameter.cpp:449-451, 280-283): the implicit operator, its inner
+  // iterations and the treatment of the chemical source; RK3 treats the source explicitly
+  d.implicit_method = s.get_int("implicit_method");
+  d.dplur_inner = s.get_int("DPLUR_inner_step");
+  d.chem_src_method = s.get_int("chemSrcMethod");
+  d.convergence_criteria = s.get_real("convergence_criteria");
+  d.output_screen = s.get_int("output_screen");
+  if (!d.steady && d.temporal_scheme == 3) d.chem_src_method = 0;
+  if (d.implicit_method != 0 && d.implicit_method != 1) {
+    err = "implicit_method must be 0 (explicit) or 1 (DPLUR); got " + std::to_string(d.implicit_method);
+    return false;
+  }
+  if (d.chem_src_method < 0 || d.chem_src_method > 2) {
+    err = "chemSrcMethod must be 0 (explicit), 1 (EPI) or 2 (DA); got " + std::to_string(d.chem_src_method);
+    return false;
+  }
+  if (d.dplur_inner < 0) {
+    err = "DPLUR_inner_step must not be negative";
     return false;
   }
   if (d.inviscid_type == 4) {

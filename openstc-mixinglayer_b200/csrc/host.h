@@ -65,6 +65,11 @@ struct Derived {
   double prandtl = 0.72;
   bool steady = true;
   int temporal_scheme = 3;
+  int implicit_method = 0;   // steady driver: 0 explicit, 1 DPLUR
+  int dplur_inner = 3;       // DPLUR inner iterations
+  int chem_src_method = 0;   // 0 explicit, 1 EPI, 2 DA (forced 0 under RK3)
+  double convergence_criteria = 1e-8;
+  int output_screen = 100;   // steady driver: residual check every output_screen iterations
   bool fixed_time_step = false;
   double dt = 1e-8;
   double grid_scale = 1.0;

@@ -257,9 +257,11 @@ __device__ __forceinline__ void reaction_rates(int r, T t, T lt, T ti, T cc, con
 
 // finite_rate_chemistry (FiniteRateChem.cu:7-58, rates :60-195): omega_k in kg/(m^3 s) at one node.
 // With jac non-null also the chemical source Jacobian of compute_chem_src_jacobian
-// (FiniteRateChem.cu:197-217), [ns][ns] row-major, in 1/s.
+// (FiniteRateChem.cu:197-217), [ns][ns] row-major, in 1/s; with omega_d non-null the destruction
+// rates omega_d,k of chemical_source (:179-195), kg/(m^3 s).
 template <int NS, typename T = double>
-__device__ __forceinline__ void mix_chemistry(T rho, T t, const T *y, T *omega, T *jac = nullptr) {
+__device__ __forceinline__ void mix_chemistry(T rho, T t, const T *y, T *omega, T *jac = nullptr,
+                                              T *omega_d = nullptr) {
   const int ns = OSTC_NS, nr = c_mix.nr;
   const T lt = log(t), ti = 1.0 / t;
   T c[Spec<NS>::A];
@@ -314,6 +316,8 @@ __device__ __forceinline__ void mix_chemistry(T rho, T t, const T *y, T *omega, 
     }
   }
   for (int l = 0; l < ns; ++l) omega[l] = cre[l] * (c_mix.mw[l] * 1e+3) - des[l] * (c_mix.mw[l] * 1e+3);
+  if (omega_d)
+    for (int l = 0; l < ns; ++l) omega_d[l] = des[l] * (c_mix.mw[l] * 1e+3);
   if (jac) {
 #pragma unroll
     for (int n = 0; n < ns; ++n) {

@@ -111,6 +111,7 @@ __device__ __forceinline__ void cv_from_bv_node(const DevBlock &b, DevState s, l
 #include "ostc_mix.cuh"
 #include "ostc_adj.cuh"
 #include "ostc_stat.cuh"
+#include "ostc_steady.cuh"
 
 static_assert(ostc::kMS <= 16, "DevFace::y holds the inflow mass fractions of at most 16 species");
 
@@ -1399,12 +1400,17 @@ struct BlockRes {
   std::vector<DevFace> faces;  // file order
   std::vector<DevInner> inner;  // interfaces of this block, file order
   int yz_var[2][2] = {{-1, -1}, {-1, -1}};  // autotuned y / z sweep variant [FP64, mixed][y, z]
+  int x_var[2] = {-1, -1};                   // autotuned x sweep variant [FP64, mixed]
+  float tune_ms[2][3][8] = {};               // autotuner's time per variant [precision][x, y, z][variant]
   std::vector<int> inner_target;
   double *adj = nullptr;  // node adjoint planes of ostc_rhs_vjp (allocated on first use)
   double *dqb = nullptr;  // dq_bar on the device
   // step adjoint: [lam_cv, x2_cv, x1_cv, g_cv] (n_var x N each) then [lam_T, x2_T, x1_T, g_T] (N each)
   double *adj_work = nullptr;
   double *stat = nullptr;  // single-point statistics accumulators (ostc_stat.cuh layout)
+  // steady driver (ostc_steady.cuh layout, allocated on first use): local time steps, inviscid
+  // spectral radii, chemical source Jacobian, DPLUR iterates
+  double *dtl = nullptr, *srad = nullptr, *cj = nullptr, *dq0 = nullptr, *dqk = nullptr;
 };
 
 struct ostc_ctx {
@@ -1445,8 +1451,13 @@ struct ostc_ctx {
   unsigned *d_flags = nullptr;
   cudaGraphExec_t graph = nullptr;
   int graph_precision = -1;
-  bool tuned[2] = {false, false};  // y / z sweep autotuning done [FP64, mixed]
+  bool tuned[2] = {false, false};  // x / y / z sweep autotuning done [FP64, mixed]
+  int forced[2][3] = {{-1, -1, -1}, {-1, -1, -1}};  // sweep variants pinned by ostc_set_sweep_variant
   int graph_kernels = 0;
+  // steady driver: iterations done (the reference's step counter) and the residual scales of its
+  // first iteration (compute_residual, Residual.cuh:128-136)
+  long long steady_iter = 0;
+  double res_scale[4] = {1, 1, 1, 1};
   std::string err;
   int sm_count = 148;
   // timing (ostc_profile_steps)
@@ -1750,6 +1761,32 @@ void launch_yz_v(ostc_ctx *ctx, BlockRes &B, DevState in, int variant) {
   k_flux_march<D, N, R, T><<<grid, dim3(32, 2, 1), march_smem_bytes<T>(N), ctx->stream>>>(b, in, B.dq, seg);
 }
 
+// x sweep variants: 0 = one thread per face (k_flux_x) is the only shape; splitting each face over
+// two warps (by side or by characteristic field) was measured 1.3-1.7x slower at 512x256x128 (more
+// shared-memory reads, repeated Roe averages, spills at the register budget of twice the warps).
+constexpr int kXVariants = 1;
+
+template <typename T, int N, int R>
+void launch_x_v(ostc_ctx *ctx, BlockRes &B, DevState in, int variant) {
+  (void)variant;
+  const DevBlock &b = B.db;
+  k_flux_x<N, R, T><<<dim3((b.mx + 126) / 127, b.my, b.mz), 128, 0, ctx->stream>>>(b, in, B.dq);
+}
+
+template <typename T>
+void launch_x(ostc_ctx *ctx, BlockRes &B, DevState in, int variant) {
+  const int ng = ctx->der.ngg, rs = ctx->der.riemann;
+  if (ng == 3) {
+    if (rs == 4) launch_x_v<T, 3, 4>(ctx, B, in, variant);
+    else if (rs == 1) launch_x_v<T, 3, 1>(ctx, B, in, variant);
+    else launch_x_v<T, 3, 3>(ctx, B, in, variant);
+  } else {
+    if (rs == 4) launch_x_v<T, 4, 4>(ctx, B, in, variant);
+    else if (rs == 1) launch_x_v<T, 4, 1>(ctx, B, in, variant);
+    else launch_x_v<T, 4, 3>(ctx, B, in, variant);
+  }
+}
+
 template <typename T, int D>
 void launch_yz(ostc_ctx *ctx, BlockRes &B, DevState in, int variant) {
   const int ng = ctx->der.ngg, rs = ctx->der.riemann;
@@ -1764,8 +1801,8 @@ void launch_yz(ostc_ctx *ctx, BlockRes &B, DevState in, int variant) {
   }
 }
 
-// Autotuner of the y / z sweeps: on the context's current state (the sweeps only read the state and
-// accumulate into the dq scratch), time every variant for each block, direction and the active
+// Autotuner of the x, y and z sweeps: on the context's current state (the sweeps only read the state
+// and write or accumulate into the dq scratch), time every variant for each block, direction and the active
 // precision with CUDA events on the library stream, and keep the fastest.  Runs once per precision,
 // outside any stream capture, before the step graph is built.  Results are cached in the process by
 // (device, block extents, ngg, scheme, precision, direction), so further contexts of the same shape
@@ -1782,21 +1819,27 @@ int autotune_yz(ostc_ctx *ctx) {
   CK(cudaEventCreate(&e1));
   for (auto &B : ctx->blk) {
     const DevState in = state_of(B, 0);
-    for (int dir = 1; dir <= (B.db.mz > 1 ? 2 : 1); ++dir) {
+    for (int dir = 0; dir <= (B.db.mz > 1 ? 2 : 1); ++dir) {
       const TuneKey key{ctx->device, B.db.mx, B.db.my, B.db.mz, B.db.g, ctx->der.riemann, ctx->der.inviscid_type, pi, dir};
+      int &slot = dir == 0 ? B.x_var[pi] : B.yz_var[pi][dir - 1];
+      if (ctx->forced[pi][dir] >= 0) {
+        slot = ctx->forced[pi][dir];
+        continue;
+      }
       {
         std::lock_guard<std::mutex> lk(g_tune_mutex);
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) {
-          B.yz_var[pi][dir - 1] = it->second;
+          slot = it->second;
           continue;
         }
       }
       float best = 1e30f;
       int bv = 0;
-      for (int v = 0; v < kYzVariants; ++v) {
+      for (int v = 0; v < (dir == 0 ? kXVariants : kYzVariants); ++v) {
         auto run = [&]() {
-          if (dir == 1) launch_yz<T, 1>(ctx, B, in, v);
+          if (dir == 0) launch_x<T>(ctx, B, in, v);
+          else if (dir == 1) launch_yz<T, 1>(ctx, B, in, v);
           else launch_yz<T, 2>(ctx, B, in, v);
         };
         run();  // warm-up
@@ -1806,12 +1849,13 @@ int autotune_yz(ostc_ctx *ctx) {
         CK(cudaEventSynchronize(e1));
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, e0, e1));
+        B.tune_ms[pi][dir][v] = ms / 3;
         if (ms < best) {
           best = ms;
           bv = v;
         }
       }
-      B.yz_var[pi][dir - 1] = bv;
+      slot = bv;
       std::lock_guard<std::mutex> lk(g_tune_mutex);
       g_tune_cache[key] = bv;
     }
@@ -1839,21 +1883,13 @@ int launch_flux(ostc_ctx *ctx, BlockRes &B, DevState in) {
   const DevBlock &b = B.db;
   const int ng = ctx->der.ngg, rs = ctx->der.riemann;
   const bool is3d = b.mz > 1;
-  // x
+  // x: the variant the autotuner chose for this block and precision
   {
-    dim3 grid((b.mx + 126) / 127, b.my, b.mz);
+    (void)ng;
+    (void)rs;
     long tok = begin_t(ctx, "flux_x");
-#define OSTC_FX(N, R) k_flux_x<N, R, T><<<grid, 128, 0, ctx->stream>>>(b, in, B.dq)
-    if (ng == 3) {
-      if (rs == 4) OSTC_FX(3, 4);
-      else if (rs == 1) OSTC_FX(3, 1);
-      else OSTC_FX(3, 3);
-    } else {
-      if (rs == 4) OSTC_FX(4, 4);
-      else if (rs == 1) OSTC_FX(4, 1);
-      else OSTC_FX(4, 3);
-    }
-#undef OSTC_FX
+    const int v = B.x_var[ctx->precision == OSTC_PREC_MIXED];
+    launch_x<T>(ctx, B, in, v < 0 ? 0 : v);
     end_t(ctx, tok);
   }
   // y and z: the variant the autotuner chose for this block and precision (column march by default)
@@ -2355,6 +2391,130 @@ int check_ready(ostc_ctx *ctx) {
   return OSTC_OK;
 }
 
+// ---- steady driver (steady_simulation, SteadySim.cuh:15-140)
+
+int steady_alloc(ostc_ctx *ctx) {
+  const bool fr = ctx->mixture && ctx->der.reaction == 1;
+  const int ns = ctx->der.n_spec, csm = fr ? ctx->der.chem_src_method : 0;
+  for (auto &B : ctx->blk) {
+    const size_t N = (size_t)B.db.n;
+    if (!B.dtl) CK(cudaMalloc(&B.dtl, N * sizeof(double)));
+    if (!B.srad) CK(cudaMalloc(&B.srad, 3 * N * sizeof(double)));
+    if (csm && !B.cj) CK(cudaMalloc(&B.cj, N * (size_t)(csm == 1 ? ns * ns : ns) * sizeof(double)));
+    if (ctx->der.implicit_method == 1 && !B.dq0) {
+      CK(cudaMalloc(&B.dq0, N * ctx->nv * sizeof(double)));
+      CK(cudaMalloc(&B.dqk, N * ctx->nv * sizeof(double)));
+    }
+  }
+  return OSTC_OK;
+}
+
+template <int NS>
+void launch_steady_chem(ostc_ctx *ctx, BlockRes &B, DevState st, int method) {
+  k_mix_source_jac<NS><<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, st, B.dq, method, B.cj);
+}
+
+template <int NS>
+void launch_steady_implicit(ostc_ctx *ctx, BlockRes &B, DevState st, int csm, bool fr) {
+  const DevBlock &b = B.db;
+  const int g = grid_for(ctx, b.n, 128);
+  if (ctx->der.implicit_method == 1) {
+    // DPLUR (DPLUR.cuh:282-322)
+    DplurArgs a{B.dtl, B.srad, B.cj, B.dq, B.dq0, B.dqk, ctx->nv, fr ? csm + 1 : 0};
+    k_dplur_dq0<NS><<<g, 128, 0, ctx->stream>>>(b, a);
+    const size_t bytes = (size_t)ctx->nv * b.n * sizeof(double);
+    cudaMemcpyAsync(B.dq0, B.dq, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+    for (int it = 0; it < ctx->der.dplur_inner; ++it) {
+      for (const DevFace &f : B.faces)
+        if (f.type == kWall)
+          k_wall_dq_zero<<<grid_for(ctx, (long long)b.mx * b.my * b.mz / 4 + 1, 128), 128, 0, ctx->stream>>>(
+              b, f, B.dq, ctx->nv);
+      k_dplur_inner<NS><<<g, 128, 0, ctx->stream>>>(b, st, a);
+      cudaMemcpyAsync(B.dq, B.dqk, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+    }
+    k_dplur_back<<<g, 128, 0, ctx->stream>>>(b, B.dq, B.dtl, ctx->nv);
+  } else if (fr && csm) {
+    k_point_implicit<NS><<<g, 128, 0, ctx->stream>>>(b, B.dq, B.dtl, B.cj, csm);
+  }
+}
+
+// One iteration of the steady driver over every block, in place on state slot 0: dq from zero, the
+// chemical source first (with its Jacobian for chemSrcMethod 1 / 2), inviscid and viscous fluxes,
+// local_time_step, implicit_treatment (ImplicitTreatmentHPP.cuh:7-54), update_cv_and_bv, the block's
+// boundary faces; then the interfaces and (mixtures) the properties.
+template <typename T>
+int enqueue_steady_iteration(ostc_ctx *ctx) {
+  const bool fr = ctx->mixture && ctx->der.reaction == 1;
+  const int csm = fr ? ctx->der.chem_src_method : 0;
+  const bool fixed = ctx->der.n_spec == kFixedNS;
+  for (size_t bi = 0; bi < ctx->blk.size(); ++bi) {
+    BlockRes &B = ctx->blk[bi];
+    const DevState st = state_of(B, 0);
+    const DevBlock &b = B.db;
+    {
+      long tok = begin_t(ctx, "rhs");
+      if (ctx->mixture) {
+        if (csm) {
+          if (fixed) launch_steady_chem<kFixedNS>(ctx, B, st, csm);
+          else launch_steady_chem<0>(ctx, B, st, csm);
+        } else {
+          launch_mix_source(ctx, B, st, fr);
+        }
+        launch_fvs(ctx, B, st);
+        if (ctx->der.viscous_order != 0) launch_mix_visc(ctx, B, st);
+      } else {
+        launch_flux<T>(ctx, B, st);
+        StageArgs a{};
+        a.in = st;
+        a.qn = st;
+        a.out = st;
+        a.prandtl = ctx->der.prandtl;
+        a.viscous = ctx->der.viscous_order != 0;
+        a.update = 0;
+        a.flags = ctx->d_flags;
+        launch_visc<T>(ctx, B, a);
+      }
+      end_t(ctx, tok);
+    }
+    {
+      long tok = begin_t(ctx, "local_dt");
+      k_local_dt<<<grid_for(ctx, b.n, 256), 256, 0, ctx->stream>>>(b, st, ctx->der.cfl, ctx->der.prandtl, b.mz > 1,
+                                                                   B.dtl, B.srad);
+      end_t(ctx, tok);
+    }
+    {
+      long tok = begin_t(ctx, "implicit");
+      if (fixed) launch_steady_implicit<kFixedNS>(ctx, B, st, csm, fr);
+      else launch_steady_implicit<0>(ctx, B, st, csm, fr);
+      end_t(ctx, tok);
+    }
+    {
+      long tok = begin_t(ctx, "update");
+      if (ctx->mixture) {
+        if (fixed)
+          k_mix_update<kFixedNS><<<grid_for(ctx, b.n, 128), 128, 0, ctx->stream>>>(
+              b, st, st, st, B.dq, ctx->d_dt, 0.0, 1.0, 1.0, ctx->nv, ctx->d_flags, B.dtl);
+        else
+          k_mix_update<0><<<grid_for(ctx, b.n, 128), 128, 0, ctx->stream>>>(b, st, st, st, B.dq, ctx->d_dt, 0.0, 1.0,
+                                                                            1.0, ctx->nv, ctx->d_flags, B.dtl);
+      } else {
+        k_steady_update_air<<<grid_for(ctx, b.n, 256), 256, 0, ctx->stream>>>(b, st, B.dq, B.dtl, ctx->d_flags);
+      }
+      end_t(ctx, tok);
+    }
+    launch_bcs(ctx, (int)bi, st);
+  }
+  launch_interfaces(ctx, 0);
+  if (ctx->mixture)
+    for (auto &B : ctx->blk) {
+      long tok = begin_t(ctx, "properties");
+      launch_mix_props(ctx, B, state_of(B, 0));
+      end_t(ctx, tok);
+    }
+  CK(cudaGetLastError());
+  return OSTC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2665,6 +2825,11 @@ void ostc_destroy(ostc_ctx *ctx) {
     cudaFree(B.dqb);
     cudaFree(B.adj_work);
     cudaFree(B.stat);
+    cudaFree(B.dtl);
+    cudaFree(B.srad);
+    cudaFree(B.cj);
+    cudaFree(B.dq0);
+    cudaFree(B.dqk);
     for (int s = 0; s < 4; ++s) {
       cudaFree(B.cv[s]);
       cudaFree(B.bv[s]);
@@ -3311,6 +3476,48 @@ int ostc_residual(ostc_ctx *ctx, double res[4]) {
   return OSTC_OK;
 }
 
+int ostc_steady_step(ostc_ctx *ctx, int max_iter, int *iters_done, double *err_max) {
+  if (!ctx || max_iter < 0) return OSTC_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  if (int r = steady_alloc(ctx)) return r;
+  const int screen = std::max(1, ctx->der.output_screen);
+  int done = 0;
+  double err = -1;
+  for (int it = 0; it < max_iter; ++it) {
+    const long long step = ctx->steady_iter + 1;
+    const bool check = step == 1 || step % screen == 0;
+    // store_last_step before the iteration whose change is measured (SteadySim.cuh:52-53, 72-76)
+    if (check)
+      for (auto &B : ctx->blk)
+        k_store_last<<<grid_for(ctx, B.db.n, 256), 256, 0, ctx->stream>>>(B.db, state_of(B, 0), B.last);
+    const int r = ctx->precision == OSTC_PREC_MIXED ? enqueue_steady_iteration<float>(ctx)
+                                                     : enqueue_steady_iteration<double>(ctx);
+    if (r) return r;
+    ctx->steady_iter = step;
+    ++done;
+    if (check) {
+      // compute_residual (Residual.cuh:74-190): RMS changes scaled by those of the first iteration
+      double res[4];
+      if (int rr = ostc_residual(ctx, res)) return rr;
+      if (step == 1)
+        for (int l = 0; l < 4; ++l) ctx->res_scale[l] = res[l] < 1e-20 ? 1e-20 : res[l];
+      err = res[0] / ctx->res_scale[0];
+      for (int l = 1; l < 4; ++l) err = std::max(err, res[l] / ctx->res_scale[l]);
+      if (std::isnan(err)) {
+        ctx->err = "the steady residual is NaN";
+        if (iters_done) *iters_done = done;
+        return OSTC_ENUMERIC;
+      }
+      if (err < ctx->der.convergence_criteria) break;
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (iters_done) *iters_done = done;
+  if (err_max) *err_max = err;
+  return OSTC_OK;
+}
+
 int ostc_bounds_flags(ostc_ctx *ctx, unsigned *flags) {
   if (!ctx || !flags) return OSTC_EINVAL;
   cudaSetDevice(ctx->device);
@@ -3812,6 +4019,45 @@ int ostc_probe_case(const char *setup_txt, const char *input_dir, int out[16], c
                         der.viscous_order, (int)order.size()};
   for (int i = 0; i < 14; ++i) out[i] = vals[i];
   return OSTC_OK;
+}
+
+int ostc_set_sweep_variant(ostc_ctx *ctx, int precision, int dir, int variant) {
+  if (!ctx) return OSTC_EINVAL;
+  if (precision < 0 || precision > 1 || dir < 0 || dir > 2) {
+    ctx->err = "ostc_set_sweep_variant: precision must be 0/1 and dir 0/1/2";
+    return OSTC_EINVAL;
+  }
+  if (variant < -1 || variant >= (dir == 0 ? kXVariants : kYzVariants)) {
+    ctx->err = "ostc_set_sweep_variant: variant " + std::to_string(variant) + " outside -1.." +
+               std::to_string((dir == 0 ? kXVariants : kYzVariants) - 1);
+    return OSTC_EINVAL;
+  }
+  ctx->forced[precision][dir] = variant;
+  // the next step tunes again (keeping pinned directions) and captures a new step graph
+  ctx->tuned[precision] = false;
+  if (ctx->graph) {
+    cudaGraphExecDestroy(ctx->graph);
+    ctx->graph = nullptr;
+  }
+  if (variant < 0) {
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    for (auto &B : ctx->blk) {
+      const TuneKey key{ctx->device, B.db.mx, B.db.my, B.db.mz, B.db.g, ctx->der.riemann, ctx->der.inviscid_type,
+                        precision, dir};
+      g_tune_cache.erase(key);
+    }
+  }
+  return OSTC_OK;
+}
+
+int ostc_tune_report(ostc_ctx *ctx, int block, int precision, int dir, int *chosen, float *ms, int max) {
+  if (!ctx || block < 0 || block >= (int)ctx->blk.size() || precision < 0 || precision > 1 || dir < 0 || dir > 2)
+    return OSTC_EINVAL;
+  const BlockRes &B = ctx->blk[block];
+  if (chosen) *chosen = dir == 0 ? B.x_var[precision] : B.yz_var[precision][dir - 1];
+  const int n = std::min(max, dir == 0 ? kXVariants : kYzVariants);
+  for (int v = 0; v < n && ms; ++v) ms[v] = B.tune_ms[precision][dir][v];
+  return dir == 0 ? kXVariants : kYzVariants;
 }
 
 int ostc_profile_steps(ostc_ctx *ctx, int n_steps, int max, const char **names, int *launches, double *ms) {

@@ -495,21 +495,25 @@ __global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL, sizeof(T
 }
 
 // update_cv_and_bv_rk<mixture> (RK.cuh:230-284) with compute_temperature_and_pressure
-// (FieldOperation.cu:3-40): the Newton iteration starts from the stage-input temperature.
+// (FieldOperation.cu:3-40): the Newton iteration starts from the stage-input temperature.  With dtl
+// (per-node local time steps, interior-indexed) the step of each node is dtl[n] instead of *dtp: the
+// steady driver's update_cv_and_bv (FieldOperation.cuh:189-232) with ca = 0, cb = cc = 1 and the state
+// updated in place (in = qn = out).
 template <int NS>
 __global__ void __launch_bounds__(128, 4) k_mix_update(DevBlock b, DevState in, DevState qn, DevState out,
                                                      const double *__restrict__ dq, const double *dtp, double ca,
-                                                     double cb, double cc, int nv, unsigned *flags) {
+                                                     double cb, double cc, int nv, unsigned *flags,
+                                                     const double *__restrict__ dtl = nullptr) {
   if (NS > 0) nv = 5 + NS;
   const long long P = b.plane;
   const int ns = OSTC_NS;
-  const double dt = *dtp;
+  const double dt = dtl ? 0.0 : *dtp;
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(n % b.mx);
     const long long r = n / b.mx;
     const int j = (int)(r % b.my), k = (int)(r / b.my);
     const long long p = b.id(i, j, k);
-    const double dtj = dt / b.jac[p];
+    const double dtj = (dtl ? dtl[n] : dt) / b.jac[p];
     double c[Spec<NS>::A + 5];
     for (int l = 0; l < nv; ++l) {
       c[l] = ca * qn.cv[l * P + p] + cb * in.cv[l * P + p] + cc * dtj * dq[l * b.n + n];

@@ -30,7 +30,8 @@ EXPORTS = [
     "ostc_step_kernel_count", "ostc_residual_noalloc", "ostc_set_chem_mode", "ostc_set_conservative",
     "ostc_rhs_vjp", "ostc_rk3_step_vjp", "ostc_adjoint_steps", "ostc_run_states", "ostc_bounds_flags",
     "ostc_bounds_checked", "ostc_stat_enable", "ostc_stat_disable", "ostc_stat_info", "ostc_stat_get",
-    "ostc_stat_export", "ostc_stat_import", "ostc_write_plt", "ostc_read_plt",
+    "ostc_stat_export", "ostc_stat_import", "ostc_write_plt", "ostc_read_plt", "ostc_tune_report",
+    "ostc_set_sweep_variant", "ostc_steady_step",
 ]
 
 
@@ -97,6 +98,9 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.ostc_device_view.argtypes = [vp, ip, ctypes.POINTER(ZoneView)]
     lib.ostc_profile_steps.argtypes = [vp, ip, ip, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ip), dp]
     lib.ostc_total_nodes.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    lib.ostc_tune_report.argtypes = [vp, ip, ip, ip, ctypes.POINTER(ip), ctypes.POINTER(ctypes.c_float), ip]
+    lib.ostc_set_sweep_variant.argtypes = [vp, ip, ip, ip]
+    lib.ostc_steady_step.argtypes = [vp, ip, ctypes.POINTER(ip), dp]
     lib.ostc_timed_steps.argtypes = [vp, ip, dp]
     lib.ostc_step_kernel_count.argtypes = [vp, ctypes.POINTER(ip)]
     lib.ostc_residual_noalloc.argtypes = [vp, vp, ctypes.c_longlong, dp, vp]
@@ -357,6 +361,25 @@ class Solver:
         n = ctypes.c_longlong()
         self._check(self.lib.ostc_total_nodes(self.h, ctypes.byref(n)))
         return n.value
+
+    def steady(self, n: int = 1):
+        """Up to n iterations of the steady driver (ostc_steady_step): (iterations run, last scaled
+        residual or -1)."""
+        done = ctypes.c_int()
+        err = ctypes.c_double()
+        self._check(self.lib.ostc_steady_step(self.h, n, ctypes.byref(done), ctypes.byref(err)))
+        return done.value, err.value
+
+    def set_sweep_variant(self, dir: int, variant: int, precision: int = 0):
+        """Pin sweep `dir` (0/1/2 = x/y/z) to kernel variant `variant` (-1: back to the autotuner)."""
+        self._check(self.lib.ostc_set_sweep_variant(self.h, precision, dir, variant))
+
+    def tune_report(self, dir: int, precision: int = 0, block: int = 0):
+        """(chosen variant, [ms per launch of each variant]) from the sweep autotuner (dir 0/1/2 = x/y/z)."""
+        chosen = ctypes.c_int()
+        ms = (ctypes.c_float * 8)()
+        n = self._check(self.lib.ostc_tune_report(self.h, block, precision, dir, ctypes.byref(chosen), ms, 8))
+        return chosen.value, list(ms[:n])
 
     def profile(self, n_steps: int) -> dict:
         mx = 32

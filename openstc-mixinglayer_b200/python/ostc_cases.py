@@ -81,8 +81,12 @@ class Case:
             f"int total_step = {self.steps}",
             "int output_file = 1000000",
             "int output_screen = 1000000",
-            "bool steady = 0",
+            f"bool steady = {int(bool(s.get('steady', 0)))}",
             "int temporal_scheme = 3",
+            f"int implicit_method = {s.get('implicit_method', 0)}",
+            f"int DPLUR_inner_step = {s.get('dplur_inner_step', 3)}",
+            f"int chemSrcMethod = {s.get('chem_src_method', 0)}",
+            f"real convergence_criteria = {s.get('convergence_criteria', 1e-8)!r}",
             f"real cfl = {s['cfl']!r}",
             f"bool fixed_time_step = {int(bool(s.get('fixed_time_step', 0)))}",
             f"real dt = {s.get('dt', 1e-8)!r}",
@@ -587,7 +591,7 @@ def _box_faces(mx, my, mz, xlab, ylab_lo, ylab_hi, zlab):
 
 def mixing_layer_2d(mx=257, my=129, seed=0, steps=100, mc=0.4, re=1000.0, t0=300.0, delta0=1e-3,
                     reconstruction=4, inviscid_scheme=3, cfl=0.5, entropy_fix_factor=0.125, ybc="symmetry",
-                    wall_thermal="isothermal") -> Case:
+                    wall_thermal="isothermal", steady=None) -> Case:
     """2-D temporal mixing layer: 256 x 128 cells on 2*pi x pi (node-coincident periodic x, mx = 257),
     u = dU/2 tanh(2y/delta0), Mc = dU/(2c), Re = rho dU delta0 / mu(T) , T and p uniform, and
     v' = 1e-3 dU sum_{m=1..8} a_m cos(m x + phi_m) exp(-(y/delta0)^2), a_m = 1/8, phi_m ~ U[0,2pi)."""
@@ -622,12 +626,14 @@ def mixing_layer_2d(mx=257, my=129, seed=0, steps=100, mc=0.4, re=1000.0, t0=300
                    "periodic": {"type": ("string", "periodic"), "label": ("int", 8)}}
     scheme = dict(reconstruction=reconstruction, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=cfl,
                   prandtl_number=0.72, limiter=0, entropy_fix_factor=entropy_fix_factor)
+    scheme.update(steady or {})
     return Case("mixing_layer_2d", mx, my, 1, x, y, z, delta0, faces, structs, scheme, bv, steps)
 
 
 def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0, t0=300.0, delta0=1e-3,
                     h=0.125, reconstruction=5, inviscid_scheme=4, cfl=0.5, ybc="farfield",
-                    entropy_fix_factor=0.125, wall_thermal="isothermal", xbc="periodic", ref_face=False) -> Case:
+                    entropy_fix_factor=0.125, wall_thermal="isothermal", xbc="periodic", ref_face=False,
+                    steady=None) -> Case:
     """3-D temporal mixing layer: uniform spacing h*delta0, periodic x and z (node-coincident),
     far-field (Riemann-invariant, label 4/41) or outflow (label 6) y faces; u = dU/2 tanh(2y/delta0),
     Mc = 0.7, plus 1e-2 dU N(0,1) exp(-(y/delta0)^2) seeded white noise in u, v, w.
@@ -688,6 +694,7 @@ def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0
             extra_bc = ("freestream",)
     scheme = dict(reconstruction=reconstruction, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=cfl,
                   prandtl_number=0.72, limiter=0, entropy_fix_factor=entropy_fix_factor)
+    scheme.update(steady or {})
     return Case("mixing_layer_3d", mx, my, mz, X, Y, Z, delta0, faces, structs, scheme, bv, steps,
                 freestream=freestream, extra_bc=extra_bc)
 
@@ -698,7 +705,7 @@ CHEM_FIXTURE = Path(__file__).resolve().parents[2] / "tests" / "golden" / "chem"
 def reacting_mixing_layer_3d(mx=384, my=192, mz=96, seed=0, steps=100, h=0.125, delta0=1e-3, mc=0.4,
                              p0=101325.0, inviscid_scheme=72, finite_rate=True, ybc="outflow",
                              chem_dir=None, fuel=None, oxidiser=None, wall_thermal="isothermal",
-                             xbc="periodic") -> Case:
+                             xbc="periodic", steady=None) -> Case:
     """Reacting H2/air temporal mixing layer (9 species, 19 reactions after merging duplicates):
     fuel Y_H2 = 0.05 in N2 at 300 K (y > 0) over vitiated air at 1500 K (y < 0): Y_O2 = 0.20, Y_H2O = 0.10,
     radicals Y_OH = 1e-3, Y_O = 1e-4, Y_H = 1e-5, Y_HO2 = 1e-6, Y_H2O2 = 1e-7 (so that every reaction
@@ -755,6 +762,7 @@ def reacting_mixing_layer_3d(mx=384, my=192, mz=96, seed=0, steps=100, h=0.125, 
         _inflow_x(faces, structs, 1.2, p0, to, oxidiser)
     scheme = dict(reconstruction=2, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=0.5, prandtl_number=0.72,
                   limiter=0, entropy_fix_factor=0.125)
+    scheme.update(steady or {})
     mixture = dict(tables=tb, finite_rate=finite_rate, chem_dir=str(chem_dir), mechanism="H2_mech.inp",
                    therm="therm.dat", tran="tran.dat")
     freestream = dict(mach=0.5, pressure=p0, temperature=to, Y=dict(oxidiser))

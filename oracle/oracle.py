@@ -64,7 +64,8 @@ class OrcCase(ctypes.Structure):
                 ("n_face", ctypes.c_int), ("face", OrcFace * 16), ("n_spec", ctypes.c_int),
                 ("finite_rate", ctypes.c_int), ("chem", ctypes.POINTER(OrcChem)), ("weno_eps_scale", ctypes.c_double),
                 ("v_ref", ctypes.c_double), ("has_init", ctypes.c_int), ("init_bv", ctypes.c_double * 6),
-                ("init_sv", ctypes.c_double * MAXS), ("chem_mode", ctypes.c_int)]
+                ("init_sv", ctypes.c_double * MAXS), ("chem_mode", ctypes.c_int), ("implicit_method", ctypes.c_int),
+                ("dplur_inner", ctypes.c_int), ("chem_src_method", ctypes.c_int)]
 
 
 def riemann_of(reconstruction: int, inviscid_scheme: int) -> int:
@@ -114,6 +115,8 @@ def load():
         lib.orc_rhs.argtypes = [vp, ctypes.c_uint, dp]
         lib.orc_step.argtypes = [vp, ctypes.c_int]
         lib.orc_step.restype = ctypes.c_double
+        lib.orc_steady.argtypes = [vp, ctypes.c_int]
+        lib.orc_steady.restype = None
         lib.orc_stat_collect.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int, dp]
         lib.orc_time.argtypes = [vp]
         lib.orc_time.restype = ctypes.c_double
@@ -154,6 +157,9 @@ class Oracle:
         c.entropy_fix_factor = s.get("entropy_fix_factor", 0.125)
         c.cfl, c.prandtl = s["cfl"], s["prandtl_number"]
         c.fixed_time_step, c.dt = 0, 1e-8
+        c.implicit_method, c.dplur_inner = s.get("implicit_method", 0), s.get("dplur_inner_step", 3)
+        c.chem_src_method = s.get("chem_src_method", 0)
+        self.steady_case = bool(s.get("steady", 0))
         types = case.label_types()
         ff = {**case.farfield_states(), **case.wall_states(), **case.inflow_states(),
               **case.characteristic_states()}
@@ -238,6 +244,14 @@ class Oracle:
 
     def step(self, n: int = 1) -> float:
         return self.lib.orc_step(self.h, n)
+
+    def steady(self, n: int = 1):
+        """n iterations of the steady driver (local time steps, explicit / EPI / DA / DPLUR)."""
+        self.lib.orc_steady(self.h, n)
+
+    def advance(self, n: int):
+        """n steps of the case's own time-advance driver: steady iterations or SSP-RK3 steps."""
+        return self.steady(n) if self.steady_case else self.step(n)
 
     def stat_collect(self, acc: np.ndarray, rey_idx=(), rho_p: bool = False):
         """Add one single-point statistics collection of the current state to acc (float64,

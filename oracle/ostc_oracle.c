@@ -46,6 +46,9 @@ struct orc_ctx {
   int ns, nv;
   double *sv, *cond, *rhod, *cpm, *gam, *acs;
   double dt_cur; /* dt of the current step (point-implicit chemistry) */
+  /* steady driver: inviscid spectral radii per interior node [N][3] (local_time_step), chemical
+   * source Jacobian per node (chem_src_jac: [N][ns][ns] for EPI, [N][ns] for DA), DPLUR iterates */
+  double *srad, *cj, *dq0, *dqk;
   face_t f[16];
   int nf;
   double t;
@@ -1059,7 +1062,9 @@ static void lu_solve(double *lhs, double *b, int dim) {
 }
 
 /* implicit = 1: also compute_chem_src_jacobian (FiniteRateChem.cu:197-217) and replace the species dq
- * by the EPI solution (FiniteRateChem.cu:233-254) with dt_cur. */
+ * by the EPI solution (FiniteRateChem.cu:233-254) with dt_cur.  implicit = 2: store that Jacobian in
+ * o->cj (chemSrcMethod 1 of the steady driver); implicit = 3: store the diagonal approximation
+ * -omega_d / (rho Y) (compute_chem_src_jacobian_diagonal, FiniteRateChem.cu:219-231; chemSrcMethod 2). */
 static void chemistry_node_jac(orc_ctx *o, int i, int j, int k, int implicit) {
   const orc_chem *ch = o->c.chem;
   const int ns = ch->n_spec, nr = ch->n_reac;
@@ -1150,8 +1155,28 @@ static void chemistry_node_jac(orc_ctx *o, int i, int j, int k, int implicit) {
     cre *= ch->mw[l] * 1e+3;
     des *= ch->mw[l] * 1e+3;
     o->dq[(5 + l) * N + q] += jac * (cre - des);
+    if (implicit == 3) {
+      const double yl = o->sv[l * P + p];
+      o->cj[q * ns + l] = 0;
+      if (yl > 1e-25) o->cj[q * ns + l] = -des / (yl * rho);
+    }
   }
-  if (!implicit) return;
+  if (!implicit || implicit == 3) return;
+  if (implicit == 2) {
+    for (int m = 0; m < ns; ++m)
+      for (int n = 0; n < ns; ++n) {
+        double zz = 0;
+        const double yn = o->sv[n * P + p];
+        if (yn > 1e-25) {
+          for (int r = 0; r < nr; ++r)
+            zz += (ch->stoi_b[r * ns + m] - ch->stoi_f[r * ns + m]) *
+                  (ch->stoi_f[r * ns + n] * q1[r] - ch->stoi_b[r * ns + n] * q2[r]);
+          zz /= rho * yn;
+        }
+        o->cj[(q * ns + m) * ns + n] = ch->mw[m] * zz * 1e+3;
+      }
+    return;
+  }
   double lhs[ORC_MAX_SPEC * ORC_MAX_SPEC], b[ORC_MAX_SPEC];
   for (int m = 0; m < ns; ++m)
     for (int n = 0; n < ns; ++n) {
@@ -1983,6 +2008,11 @@ double orc_dt(orc_ctx *o) {
         sv *= c1 * c2;
         const double d = o->c.cfl / (sinv + sv);
         o->dtl[IQ(o, i, j, k)] = d;
+        if (o->srad) {
+          o->srad[3 * IQ(o, i, j, k)] = s0;
+          o->srad[3 * IQ(o, i, j, k) + 1] = s1;
+          o->srad[3 * IQ(o, i, j, k) + 2] = s2;
+        }
         if (d < dt) dt = d;
       }
   return dt;
@@ -2093,6 +2123,7 @@ void orc_destroy(orc_ctx *o) {
   free(o->x); free(o->y); free(o->z); free(o->jac); free(o->met);
   free(o->cv); free(o->qn); free(o->bv); free(o->mul); free(o->dq); free(o->dtl);
   free(o->sv); free(o->rhod); free(o->cond); free(o->cpm); free(o->gam); free(o->acs);
+  free(o->srad); free(o->cj); free(o->dq0); free(o->dqk);
   free(o);
 }
 
@@ -2212,6 +2243,227 @@ double orc_step(orc_ctx *o, int n) {
     o->t += dt;
   }
   return dt;
+}
+
+/* ---------------------------------------------------------------- steady driver (SteadySim.cuh) */
+
+/* compute_jacobian_times_dq (DPLUR.cuh:96-154): the split convective Jacobian of direction dir at
+ * interior node (i, j, k), with eigenvalue shift lam, times that node's dq. */
+static void jac_times_dq(const orc_ctx *o, const double *dqv, int i, int j, int k, int dir, double lam,
+                         double *out) {
+  const long P = o->P, N = (long)o->mx * o->my * o->mz;
+  const long p = ID(o, i, j, k), q = IQ(o, i, j, k);
+  const double xi_x = M(o, dir + 1, 1, p), xi_y = M(o, dir + 1, 2, p), xi_z = M(o, dir + 1, 3, p);
+  const double u = o->bv[P + p], v = o->bv[2 * P + p], w = o->bv[3 * P + p];
+  const double U = xi_x * u + xi_y * v + xi_z * w;
+  const double lmd1 = U + lam;
+  const double e = 0.5 * (u * u + v * v + w * w);
+  double gamma = GAMMA_AIR, b3 = 0, b4 = 0, h = 0;
+  double d[FVS_MAXV];
+  for (int l = 0; l < o->nv; ++l) d[l] = dqv[l * N + q];
+  if (!o->ns) {
+    h = gamma / (gamma - 1) * o->bv[4 * P + p] / o->bv[p] + e;
+  } else {
+    const orc_chem *ch = o->c.chem;
+    double hs[ORC_MAX_SPEC], cps[ORC_MAX_SPEC];
+    const double t = o->bv[5 * P + p];
+    mix_h_cp(ch, t, hs, cps);
+    gamma = o->gam[p];
+    for (int l = 0; l < o->ns; ++l) {
+      b3 += R_U * t / ch->mw[l] * d[5 + l];
+      b4 += hs[l] * d[5 + l];
+      h += o->sv[l * P + p] * hs[l];
+    }
+    b3 *= gamma;
+    b4 *= gamma - 1;
+    h += e;
+  }
+  const double b1 = xi_x * d[1] + xi_y * d[2] + xi_z * d[3] - U * d[0];
+  const double b2 = (gamma - 1) * (e * d[0] - u * d[1] - v * d[2] - w * d[3] + d[4]);
+  out[0] = b1 + lmd1 * d[0];
+  out[1] = u * b1 + xi_x * b2 + lmd1 * d[1] + xi_x * (b3 - b4);
+  out[2] = v * b1 + xi_y * b2 + lmd1 * d[2] + xi_y * (b3 - b4);
+  out[3] = w * b1 + xi_z * b2 + lmd1 * d[3] + xi_z * (b3 - b4);
+  out[4] = h * b1 + U * b2 + lmd1 * d[4] + U * (b3 - b4);
+  for (int l = 0; l < o->ns; ++l) out[5 + l] = lmd1 * d[5 + l] + o->sv[l * P + p] * b1;
+}
+
+/* (diag I - dt J) x = b for the species of node q (EPI_for_dq0 / EPI_for_dqk / EPI, FiniteRateChem.cu:
+ * 233-300), b solved in place */
+static void epi_solve(const orc_ctx *o, long q, double diag, double dt, double *b) {
+  const int ns = o->ns;
+  double lhs[ORC_MAX_SPEC * ORC_MAX_SPEC];
+  for (int m = 0; m < ns; ++m)
+    for (int n = 0; n < ns; ++n) {
+      const double jm = o->cj[(q * ns + m) * ns + n];
+      lhs[m * ns + n] = m == n ? diag - dt * jm : -dt * jm;
+    }
+  lu_solve(lhs, b, ns);
+}
+
+/* DPLUR (DPLUR.cuh:282-322, DPLUR.cu:5-40) on o->dq of one block: compute_DQ_0, DPLUR_inner_step
+ * inner iterations (walls' dq zeroed first, set_wall_dq_to_0), convert_dq_back_to_dqDt.  The viscous
+ * spectral radius the reference adds to the diagonal is never computed there (its array keeps the
+ * zeros of its allocation, Field.cu:553-565), so those terms are zero. */
+static void dplur(orc_ctx *o) {
+  const long N = (long)o->mx * o->my * o->mz;
+  const int nv = o->nv, ns = o->ns;
+  const int fr = ns && o->c.finite_rate, csm = o->c.chem_src_method;
+  for (int k = 0; k < o->mz; ++k)
+    for (int j = 0; j < o->my; ++j)
+      for (int i = 0; i < o->mx; ++i) {
+        const long q = IQ(o, i, j, k);
+        const double dt = o->dtl[q];
+        for (int l = 0; l < nv; ++l) o->dq[l * N + q] *= dt;
+        const double diag = 1 + 0.0 * dt + dt * (o->srad[3 * q] + o->srad[3 * q + 1] + o->srad[3 * q + 2]);
+        if (!fr) {
+          for (int l = 0; l < nv; ++l) o->dq[l * N + q] /= diag;
+          continue;
+        }
+        for (int l = 0; l < 5; ++l) o->dq[l * N + q] /= diag;
+        if (csm == 1) {
+          double b[ORC_MAX_SPEC];
+          for (int l = 0; l < ns; ++l) b[l] = o->dq[(5 + l) * N + q];
+          epi_solve(o, q, diag, dt, b);
+          for (int l = 0; l < ns; ++l) o->dq[(5 + l) * N + q] = b[l];
+        } else if (csm == 2) {
+          for (int l = 0; l < ns; ++l) o->dq[(5 + l) * N + q] /= diag - dt * o->cj[q * ns + l];
+        } else {
+          for (int l = 0; l < ns; ++l) o->dq[(5 + l) * N + q] /= diag;
+        }
+      }
+  memcpy(o->dq0, o->dq, sizeof(double) * nv * N);
+  for (int it = 0; it < o->c.dplur_inner; ++it) {
+    for (int n = 0; n < o->nf; ++n) {
+      const face_t *f = &o->f[n];
+      if (f->type != ORC_WALL) continue;
+      int lo[3] = {0, 0, 0}, hi[3] = {o->mx - 1, o->my - 1, o->mz - 1};
+      const int fi = f->face, at = f->direction < 0 ? 0 : (fi == 0 ? o->mx - 1 : fi == 1 ? o->my - 1 : o->mz - 1);
+      lo[fi] = hi[fi] = at;
+      for (int k = lo[2]; k <= hi[2]; ++k)
+        for (int j = lo[1]; j <= hi[1]; ++j)
+          for (int i = lo[0]; i <= hi[0]; ++i)
+            for (int l = 0; l < nv; ++l) o->dq[l * N + IQ(o, i, j, k)] = 0;
+    }
+    for (int k = 0; k < o->mz; ++k)
+      for (int j = 0; j < o->my; ++j)
+        for (int i = 0; i < o->mx; ++i) {
+          const long q = IQ(o, i, j, k);
+          double conv[FVS_MAXV], tot[FVS_MAXV];
+          for (int l = 0; l < nv; ++l) tot[l] = 0;
+          const int nb[3][3] = {{i - 1, j, k}, {i, j - 1, k}, {i, j, k - 1}};
+          const int pb[3][3] = {{i + 1, j, k}, {i, j + 1, k}, {i, j, k + 1}};
+          const int ext[3] = {o->mx, o->my, o->mz}, at[3] = {i, j, k};
+          for (int d = 0; d < 3; ++d) {
+            if (at[d] > 0) {
+              const long qn = IQ(o, nb[d][0], nb[d][1], nb[d][2]);
+              jac_times_dq(o, o->dq, nb[d][0], nb[d][1], nb[d][2], d, o->srad[3 * qn + d], conv);
+              for (int l = 0; l < nv; ++l) tot[l] += 0.5 * conv[l];
+            }
+          }
+          for (int d = 0; d < 3; ++d) {
+            if (at[d] != ext[d] - 1) {
+              const long qn = IQ(o, pb[d][0], pb[d][1], pb[d][2]);
+              jac_times_dq(o, o->dq, pb[d][0], pb[d][1], pb[d][2], d, -o->srad[3 * qn + d], conv);
+              for (int l = 0; l < nv; ++l) tot[l] -= 0.5 * conv[l];
+            }
+          }
+          const double dt = o->dtl[q];
+          const double diag = 1 + 0.0 * dt + dt * (o->srad[3 * q] + o->srad[3 * q + 1] + o->srad[3 * q + 2]);
+          const int nflow = fr ? 5 : nv;
+          for (int l = 0; l < nflow; ++l) o->dqk[l * N + q] = o->dq0[l * N + q] + dt * tot[l] / diag;
+          if (!fr) continue;
+          if (csm == 1) {
+            double b[ORC_MAX_SPEC];
+            for (int l = 0; l < ns; ++l) b[l] = tot[5 + l] * dt;
+            epi_solve(o, q, diag, dt, b);
+            for (int l = 0; l < ns; ++l) o->dqk[(5 + l) * N + q] = o->dq0[(5 + l) * N + q] + b[l];
+          } else if (csm == 2) {
+            for (int l = 0; l < ns; ++l)
+              o->dqk[(5 + l) * N + q] = o->dq0[(5 + l) * N + q] + dt * tot[5 + l] / (diag - dt * o->cj[q * ns + l]);
+          } else {
+            for (int l = 0; l < ns; ++l) o->dqk[(5 + l) * N + q] = o->dq0[(5 + l) * N + q] + dt * tot[5 + l] / diag;
+          }
+        }
+    memcpy(o->dq, o->dqk, sizeof(double) * nv * N);
+  }
+  for (long q = 0; q < N; ++q)
+    for (int l = 0; l < nv; ++l) o->dq[l * N + q] /= o->dtl[q];
+}
+
+/* update_cv_and_bv (FieldOperation.cuh:189-232): cv += dt_local / jac * dq, then the primitive state */
+static void steady_update(orc_ctx *o) {
+  const long P = o->P, N = (long)o->mx * o->my * o->mz;
+  for (int k = 0; k < o->mz; ++k)
+    for (int j = 0; j < o->my; ++j)
+      for (int i = 0; i < o->mx; ++i) {
+        const long p = ID(o, i, j, k), q = IQ(o, i, j, k);
+        const double dtj = o->dtl[q] / o->jac[p];
+        for (int l = 0; l < o->nv; ++l) o->cv[l * P + p] += dtj * o->dq[l * N + q];
+        if (o->mz == 1) o->cv[3 * P + p] = 0;
+        o->bv[p] = o->cv[p];
+        const double di = 1.0 / o->cv[p];
+        o->bv[P + p] = o->cv[P + p] * di;
+        o->bv[2 * P + p] = o->cv[2 * P + p] * di;
+        o->bv[3 * P + p] = o->cv[3 * P + p] * di;
+        if (o->ns) {
+          for (int l = 0; l < o->ns; ++l) o->sv[l * P + p] = o->cv[(5 + l) * P + p] * di;
+          mix_t_and_p(o, p, o->cv[4 * P + p]);
+        } else {
+          const double V2 = o->bv[P + p] * o->bv[P + p] + o->bv[2 * P + p] * o->bv[2 * P + p] +
+                            o->bv[3 * P + p] * o->bv[3 * P + p];
+          o->bv[4 * P + p] = (GAMMA_AIR - 1) * (o->cv[4 * P + p] - 0.5 * o->bv[p] * V2);
+          o->bv[5 * P + p] = o->bv[4 * P + p] * MW_AIR * di / R_U;
+        }
+      }
+}
+
+/* steady_simulation<mixture model, Laminar> iteration body for one block (SteadySim.cuh:65-140): dq
+ * from zero; the chemical source first (with its Jacobian for chemSrcMethod 1 / 2), the inviscid and
+ * viscous fluxes; local_time_step; implicit_treatment (ImplicitTreatmentHPP.cuh:7-54: EPI or DA when
+ * explicit, else DPLUR); update_cv_and_bv; boundary faces, 2-D k copy, properties.  The physical time
+ * does not advance. */
+void orc_steady(orc_ctx *o, int n) {
+  const long N = (long)o->mx * o->my * o->mz;
+  const int ns = o->ns, fr = ns && o->c.finite_rate, csm = o->c.chem_src_method;
+  if (!o->srad) o->srad = (double *)calloc(3 * N, sizeof(double));
+  if (fr && csm && !o->cj) o->cj = (double *)calloc(N * (csm == 1 ? ns * ns : ns), sizeof(double));
+  if (o->c.implicit_method == 1 && !o->dq0) {
+    o->dq0 = (double *)calloc(o->nv * N, sizeof(double));
+    o->dqk = (double *)calloc(o->nv * N, sizeof(double));
+  }
+  for (int s = 0; s < n; ++s) {
+    memset(o->dq, 0, sizeof(double) * o->nv * N);
+    if (fr)
+      for (int k = 0; k < o->mz; ++k)
+        for (int j = 0; j < o->my; ++j)
+          for (int i = 0; i < o->mx; ++i) chemistry_node_jac(o, i, j, k, csm == 1 ? 2 : csm == 2 ? 3 : 0);
+    for (int d = 0; d < o->dim; ++d) {
+      const int is = o->c.inviscid_scheme;
+      if (is == 71 || is == 72) fvs_direction(o, d);
+      else if (o->c.reconstruction == 4 || o->c.reconstruction == 5) aweno_direction(o, d);
+      else pv_direction(o, d);
+    }
+    if (o->c.viscous_order != 0) viscous(o);
+    orc_dt(o);
+    if (o->c.implicit_method == 1) {
+      dplur(o);
+    } else if (fr && csm) {
+      for (long q = 0; q < N; ++q) {
+        const double dt = o->dtl[q];
+        if (csm == 1) {
+          double b[ORC_MAX_SPEC];
+          for (int l = 0; l < ns; ++l) b[l] = o->dq[(5 + l) * N + q];
+          epi_solve(o, q, 1.0, dt, b);
+          for (int l = 0; l < ns; ++l) o->dq[(5 + l) * N + q] = b[l];
+        } else {
+          for (int l = 0; l < ns; ++l) o->dq[(5 + l) * N + q] /= 1 - dt * o->cj[q * ns + l];
+        }
+      }
+    }
+    steady_update(o);
+    fill_ghosts(o);
+  }
 }
 
 /* ---------------------------------------------------------------- single-point statistics */

@@ -80,6 +80,10 @@ typedef struct {
    * part of dq is replaced by the solution of (I - dt J_chem) x = dq_s (EPI, solve_chem_system,
    * FiniteRateChem.cu:197-254, 302-357) with the step's dt */
   int chem_mode;
+  /* steady driver (steady_simulation, SteadySim.cuh:15-140): local time steps; implicit_method 0
+   * (explicit, plus the point-implicit chemistry of chem_src_method) or 1 (DPLUR with dplur_inner
+   * inner iterations, DPLUR.cuh:282-322); chem_src_method 0 explicit, 1 EPI, 2 diagonal (DA) */
+  int implicit_method, dplur_inner, chem_src_method;
 } orc_case;
 
 typedef struct orc_ctx orc_ctx;
@@ -106,6 +110,8 @@ void orc_get_metric(const orc_ctx *o, double *metric9, double *jac);
 void orc_rhs(orc_ctx *o, unsigned mask, double *dq);
 /* n full SSP-RK3 steps (RK.cuh:85-185).  Returns the last dt. */
 double orc_step(orc_ctx *o, int n);
+/* n iterations of the steady driver (steady_simulation, SteadySim.cuh:65-140) */
+void orc_steady(orc_ctx *o, int n);
 /* one single-point statistics collection added to acc (collect_single_point_basic_statistics) */
 void orc_stat_collect(const orc_ctx *o, int n_rey, const int *rey_idx, int rho_p, double *acc);
 double orc_time(const orc_ctx *o);

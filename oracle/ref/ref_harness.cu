@@ -7,7 +7,8 @@
 // (main.cu:8-136; model Air, Mixture or FR from the species/reaction keys), replaces the freshly
 // initialised interior primitive variables with the ones in state_in.bin ([block][6 + n_spec][mz][my][mx]
 // doubles: rho u v w p T, then the mass fractions), runs the reference's
-// Driver::initialize_computation() and RK3() (RK.cuh:19-228) for total_step steps, and writes the
+// Driver::initialize_computation() and RK3() (RK.cuh:19-228) for total_step steps - or, when the setup
+// has steady = 1, its steady_simulation() (SteadySim.cuh:15-140) for total_step iterations - and writes the
 // interior cv[n_var], bv[6] and sv[n_spec] of every block, then the physical time, to state_out.bin.  It prints the
 // wall time of the RK3 call (steps, per-step output checks and the final flow-field file included).
 #include <chrono>
@@ -76,10 +77,12 @@ int run_model(cfd::Parameter &parameter, cfd::Mesh &mesh, const char *fin, const
 
   g_stage = "initialize_computation";
   driver.initialize_computation();
-  g_stage = "RK3";
+  g_stage = parameter.get_bool("steady") ? "steady_simulation" : "RK3";
   cudaDeviceSynchronize();
   const auto t_begin = std::chrono::steady_clock::now();
-  cfd::RK3<M, cfd::Laminar>(driver);
+  // the time-advance driver Simulate.cuh picks: the steady local-time-step loop (SteadySim.cuh) or RK3
+  if (parameter.get_bool("steady")) cfd::steady_simulation<M, cfd::Laminar>(driver);
+  else cfd::RK3<M, cfd::Laminar>(driver);
   cudaDeviceSynchronize();
   const double rk3_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_begin).count();
   std::printf("ref_harness: rk3_seconds = %.6f\n", rk3_seconds);

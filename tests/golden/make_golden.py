@@ -37,6 +37,8 @@ from golden_util import STAT_SETUP  # noqa: E402
 STAT_FILES = ["output/stat/coll_rey_1st.bin", "output/stat/coll_fav_1st.bin", "output/stat/coll_rey_2nd.bin",
               "output/stat/coll_fav_2nd.bin"]
 PLT = ["output/flowfield.plt"]
+# steady driver settings (no early stop on convergence: the fixture runs a fixed iteration count)
+STEADY = dict(steady=1, implicit_method=0, dplur_inner_step=3, chem_src_method=0, convergence_criteria=1e-300)
 
 CASES = [
     # name, generator, kwargs, steps[, options: sampled / setup (extra setup.txt lines) / files (kept)]
@@ -89,6 +91,21 @@ CASES = [
      dict(mx=32, my=20, mz=12, ybc="outflow", xbc="subsonic", ref_face=True), 10),
     ("rml3d_wall", "reacting_mixing_layer_3d", dict(mx=20, my=16, mz=10, ybc="wall"), 5),
     ("rml3d_inflow", "reacting_mixing_layer_3d", dict(mx=24, my=16, mz=10, xbc="inflow"), 5),
+    # the reference's steady driver (SteadySim.cuh): local time steps, explicit or DPLUR implicit
+    # treatment (DPLUR.cuh), the chemical source explicit, point-implicit (EPI) or diagonal (DA).  No
+    # wall case with DPLUR: the reference zeroes dq over the wall's ngg-padded range in an array with
+    # one ghost layer (DPLUR.cu:22-40, Mesh.cpp:14-32, Field.cu:559-562), outside that array
+    ("st_ml3d_explicit", "mixing_layer_3d", dict(mx=24, my=20, mz=12, ybc="outflow", steady=STEADY), 10),
+    ("st_ml3d_dplur", "mixing_layer_3d", dict(mx=24, my=20, mz=12, steady=dict(STEADY, implicit_method=1)), 10),
+    ("st_ml2d_dplur", "mixing_layer_2d", dict(mx=49, my=33, steady=dict(STEADY, implicit_method=1)), 15),
+    ("st_rml3d_epi", "reacting_mixing_layer_3d", dict(mx=16, my=12, mz=8, steady=dict(STEADY, chem_src_method=1)), 5),
+    ("st_rml3d_da", "reacting_mixing_layer_3d", dict(mx=16, my=12, mz=8, steady=dict(STEADY, chem_src_method=2)), 5),
+    ("st_rml3d_dplur_epi", "reacting_mixing_layer_3d",
+     dict(mx=16, my=12, mz=8, steady=dict(STEADY, implicit_method=1, chem_src_method=1)), 5),
+    ("st_rml3d_dplur_explicit", "reacting_mixing_layer_3d",
+     dict(mx=16, my=12, mz=8, steady=dict(STEADY, implicit_method=1, dplur_inner_step=2)), 5),
+    ("st_rml3d_mix_dplur", "reacting_mixing_layer_3d",
+     dict(mx=16, my=12, mz=8, finite_rate=False, steady=dict(STEADY, implicit_method=1)), 5),
     # the files the reference writes at the end of a run: flow field and statistics
     ("ml3d_stat_plt", "mixing_layer_3d", dict(mx=16, my=12, mz=8, ybc="outflow"), 6,
      dict(setup=STAT_SETUP, files=PLT + STAT_FILES)),

@@ -117,7 +117,8 @@ def assert_state(cv, z, block=None):
 
 
 def run_library(case, steps, directory, setup_extra=""):
-    """Advances the case `steps` SSP-RK3 steps through the C ABI; returns the open solver."""
+    """Advances the case `steps` SSP-RK3 steps (or, for a steady case, steady-driver iterations) through
+    the C ABI; returns the open solver."""
     import ostc
 
     d = oc.write_case(case, directory)
@@ -129,7 +130,11 @@ def run_library(case, steps, directory, setup_extra=""):
             s.set_state(blk.bv, block=b)
     else:
         s.set_state(case.bv, sv=case.sv)
-    s.step(steps)
+    if case.scheme.get("steady"):
+        done, _ = s.steady(steps)
+        assert done == steps
+    else:
+        s.step(steps)
     return s
 
 

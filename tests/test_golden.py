@@ -64,7 +64,7 @@ def test_oracle_matches_reference(built, path):
         return
     o = Oracle(case)
     o.set_state(case.bv)
-    o.step(steps)
+    o.advance(steps)
     gu.assert_state(o.get_state()[0], z)
     assert abs(o.time() - t_ref) <= gu.TOL_T * t_ref
 
