@@ -290,6 +290,18 @@ int ostc_stat_import(ostc_ctx *ctx, const char *dir);
  * scaled residual (-1 if none was computed).  The physical time does not advance.  Synchronises. */
 int ostc_steady_step(ostc_ctx *ctx, int max_iter, int *iters_done, double *err_max);
 
+/* The reference's dual time stepping (dual_time_stepping, DualTimeStepping.cuh:32-252; temporal_scheme 2):
+ * n_steps physical steps of the setup's dt, each forming q* = jac / (2 dt) (4 cv^n - cv^(n-1)) and then
+ * up to inner_iteration pseudo-time iterations of the steady driver's form with dq += q* - 1.5 jac /
+ * dt cv and DPLUR (DPLUR_inner_step inner sweeps, diagonal factor 1.5 / dt).  Every
+ * iteration_adjust_step-th step the inner loop is monitored as the reference's inner_converged does
+ * (residual scaled by the first iteration's; stop below 1e-3, the count trimmed to it; raised by 5 up
+ * to max_inner_iteration when the last iteration is still above) - the monitored residual uses the
+ * ostc_residual reference, which it overwrites.  inner_iters (nullable) receives the count in force
+ * afterwards.  The physical time advances by dt per step; statistics collect as after an RK3 step.
+ * Synchronises. */
+int ostc_dual_time_step(ostc_ctx *ctx, int n_steps, int *inner_iters);
+
 /* Limits of ostc_residual_noalloc: its static scratch holds one partial sum set per block of
  * 256 threads x 64 nodes, for at most OSTC_NOALLOC_MAX_BLOCKS blocks (128 KB of device memory). */
 #define OSTC_NOALLOC_NODES_PER_THREAD 64

@@ -37,6 +37,9 @@ void Setup::set_defaults() {
   strings["transport_file"] = "chemistry/tran.dat";
   ints["chemSrcMethod"] = 0;
   ints["DPLUR_inner_step"] = 3;         // Parameter.cpp:450
+  ints["inner_iteration"] = 20;         // Parameter.cpp:466-468
+  ints["max_inner_iteration"] = 30;
+  ints["iteration_adjust_step"] = 20;
   reals["convergence_criteria"] = 1e-8;  // Parameter.cpp:451
   bools["turbulence"] = false;
   ints["turbulence_method"] = 1;
@@ -246,10 +249,10 @@ bool derive(const Setup &s, Derived &d, std::string &err) {
     err = "turbulence models are outside this library's path (laminar/DNS only)";
     return false;
   }
-  if (!d.steady && d.temporal_scheme != 3) {
+  if (!d.steady && d.temporal_scheme != 3 && d.temporal_scheme != 2) {
     err = "temporal_scheme " + std::to_string(d.temporal_scheme) +
-          ": of the unsteady drivers this library runs SSP-RK3 (temporal_scheme = 3); steady = 1 runs the steady "
-          "driver";
+          ": of the unsteady drivers this library runs SSP-RK3 (3) and dual time stepping (2); steady = 1 runs "
+          "the steady driver";
     return false;
   }
   // steady driver settings (Parameter.cpp:449-451, 280-283): the implicit operator, its inner
@@ -259,6 +262,9 @@ bool derive(const Setup &s, Derived &d, std::string &err) {
   d.chem_src_method = s.get_int("chemSrcMethod");
   d.convergence_criteria = s.get_real("convergence_criteria");
   d.output_screen = s.get_int("output_screen");
+  d.inner_iteration = s.get_int("inner_iteration");
+  d.max_inner_iteration = s.get_int("max_inner_iteration");
+  d.iteration_adjust_step = s.get_int("iteration_adjust_step");
   if (!d.steady && d.temporal_scheme == 3) d.chem_src_method = 0;
   if (d.implicit_method != 0 && d.implicit_method != 1) {
     err = "implicit_method must be 0 (explicit) or 1 (DPLUR); got " + std::to_string(d.implicit_method);

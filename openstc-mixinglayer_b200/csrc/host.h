@@ -70,6 +70,7 @@ struct Derived {
   int chem_src_method = 0;   // 0 explicit, 1 EPI, 2 DA (forced 0 under RK3)
   double convergence_criteria = 1e-8;
   int output_screen = 100;   // steady driver: residual check every output_screen iterations
+  int inner_iteration = 20, max_inner_iteration = 30, iteration_adjust_step = 20;  // dual time stepping
   bool fixed_time_step = false;
   double dt = 1e-8;
   double grid_scale = 1.0;

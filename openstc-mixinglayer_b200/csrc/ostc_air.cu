@@ -1411,6 +1411,8 @@ struct BlockRes {
   // steady driver (ostc_steady.cuh layout, allocated on first use): local time steps, inviscid
   // spectral radii, chemical source Jacobian, DPLUR iterates
   double *dtl = nullptr, *srad = nullptr, *cj = nullptr, *dq0 = nullptr, *dqk = nullptr;
+  // dual time stepping: the previous physical step's cv (padded planes) and the BDF2 source q* (interior)
+  double *qn1 = nullptr, *qstar = nullptr;
 };
 
 struct ostc_ctx {
@@ -1458,6 +1460,11 @@ struct ostc_ctx {
   // first iteration (compute_residual, Residual.cuh:128-136)
   long long steady_iter = 0;
   double res_scale[4] = {1, 1, 1, 1};
+  // dual time stepping: physical steps done, the inner-iteration count in force (adapted by
+  // inner_converged, DualTimeStepping.cu:32-135) and the inner residual scales
+  long long dual_step = 0;
+  int dual_inner = -1;
+  double res_scale_inner[4] = {1, 1, 1, 1};
   std::string err;
   int sm_count = 148;
   // timing (ostc_profile_steps)
@@ -2393,7 +2400,7 @@ int check_ready(ostc_ctx *ctx) {
 
 // ---- steady driver (steady_simulation, SteadySim.cuh:15-140)
 
-int steady_alloc(ostc_ctx *ctx) {
+int steady_alloc(ostc_ctx *ctx, bool dual = false) {
   const bool fr = ctx->mixture && ctx->der.reaction == 1;
   const int ns = ctx->der.n_spec, csm = fr ? ctx->der.chem_src_method : 0;
   for (auto &B : ctx->blk) {
@@ -2401,9 +2408,13 @@ int steady_alloc(ostc_ctx *ctx) {
     if (!B.dtl) CK(cudaMalloc(&B.dtl, N * sizeof(double)));
     if (!B.srad) CK(cudaMalloc(&B.srad, 3 * N * sizeof(double)));
     if (csm && !B.cj) CK(cudaMalloc(&B.cj, N * (size_t)(csm == 1 ? ns * ns : ns) * sizeof(double)));
-    if (ctx->der.implicit_method == 1 && !B.dq0) {
+    if ((ctx->der.implicit_method == 1 || dual) && !B.dq0) {
       CK(cudaMalloc(&B.dq0, N * ctx->nv * sizeof(double)));
       CK(cudaMalloc(&B.dqk, N * ctx->nv * sizeof(double)));
+    }
+    if (dual && !B.qn1) {
+      CK(cudaMalloc(&B.qn1, (size_t)ctx->nv * B.db.plane * sizeof(double)));
+      CK(cudaMalloc(&B.qstar, N * ctx->nv * sizeof(double)));
     }
   }
   return OSTC_OK;
@@ -2415,12 +2426,13 @@ void launch_steady_chem(ostc_ctx *ctx, BlockRes &B, DevState st, int method) {
 }
 
 template <int NS>
-void launch_steady_implicit(ostc_ctx *ctx, BlockRes &B, DevState st, int csm, bool fr) {
+void launch_steady_implicit(ostc_ctx *ctx, BlockRes &B, DevState st, int csm, bool fr, bool dplur,
+                            double diag_factor) {
   const DevBlock &b = B.db;
   const int g = grid_for(ctx, b.n, 128);
-  if (ctx->der.implicit_method == 1) {
+  if (dplur) {
     // DPLUR (DPLUR.cuh:282-322)
-    DplurArgs a{B.dtl, B.srad, B.cj, B.dq, B.dq0, B.dqk, ctx->nv, fr ? csm + 1 : 0};
+    DplurArgs a{B.dtl, B.srad, B.cj, B.dq, B.dq0, B.dqk, ctx->nv, fr ? csm + 1 : 0, diag_factor};
     k_dplur_dq0<NS><<<g, 128, 0, ctx->stream>>>(b, a);
     const size_t bytes = (size_t)ctx->nv * b.n * sizeof(double);
     cudaMemcpyAsync(B.dq0, B.dq, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
@@ -2441,9 +2453,12 @@ void launch_steady_implicit(ostc_ctx *ctx, BlockRes &B, DevState st, int csm, bo
 // One iteration of the steady driver over every block, in place on state slot 0: dq from zero, the
 // chemical source first (with its Jacobian for chemSrcMethod 1 / 2), inviscid and viscous fluxes,
 // local_time_step, implicit_treatment (ImplicitTreatmentHPP.cuh:7-54), update_cv_and_bv, the block's
-// boundary faces; then the interfaces and (mixtures) the properties.
+// boundary faces; then the interfaces and (mixtures) the properties.  With dt_phys > 0 it is one
+// pseudo-time iteration of dual time stepping (DualTimeStepping.cuh:126-165): the BDF2 terms join dq
+// (compute_modified_rhs) and DPLUR runs with diag_factor 1.5 / dt_phys.
 template <typename T>
-int enqueue_steady_iteration(ostc_ctx *ctx) {
+int enqueue_steady_iteration(ostc_ctx *ctx, double dt_phys = 0.0) {
+  const bool dual = dt_phys > 0.0;
   const bool fr = ctx->mixture && ctx->der.reaction == 1;
   const int csm = fr ? ctx->der.chem_src_method : 0;
   const bool fixed = ctx->der.n_spec == kFixedNS;
@@ -2482,10 +2497,14 @@ int enqueue_steady_iteration(ostc_ctx *ctx) {
                                                                    B.dtl, B.srad);
       end_t(ctx, tok);
     }
+    if (dual)
+      k_modified_rhs<<<grid_for(ctx, b.n, 128), 128, 0, ctx->stream>>>(b, st, B.qstar, B.dq, ctx->nv, dt_phys);
     {
       long tok = begin_t(ctx, "implicit");
-      if (fixed) launch_steady_implicit<kFixedNS>(ctx, B, st, csm, fr);
-      else launch_steady_implicit<0>(ctx, B, st, csm, fr);
+      const bool dplur = dual || ctx->der.implicit_method == 1;
+      const double df = dual ? 1.5 / dt_phys : 0.0;
+      if (fixed) launch_steady_implicit<kFixedNS>(ctx, B, st, csm, fr, dplur, df);
+      else launch_steady_implicit<0>(ctx, B, st, csm, fr, dplur, df);
       end_t(ctx, tok);
     }
     {
@@ -2830,6 +2849,8 @@ void ostc_destroy(ostc_ctx *ctx) {
     cudaFree(B.cj);
     cudaFree(B.dq0);
     cudaFree(B.dqk);
+    cudaFree(B.qn1);
+    cudaFree(B.qstar);
     for (int s = 0; s < 4; ++s) {
       cudaFree(B.cv[s]);
       cudaFree(B.bv[s]);
@@ -3515,6 +3536,69 @@ int ostc_steady_step(ostc_ctx *ctx, int max_iter, int *iters_done, double *err_m
   CK(cudaStreamSynchronize(ctx->stream));
   if (iters_done) *iters_done = done;
   if (err_max) *err_max = err;
+  return OSTC_OK;
+}
+
+int ostc_dual_time_step(ostc_ctx *ctx, int n_steps, int *inner_iters) {
+  if (!ctx || n_steps < 0) return OSTC_EINVAL;
+  if (!(ctx->der.dt > 0.0)) {
+    ctx->err = "dual time stepping needs a positive physical step dt in the setup";
+    return OSTC_EINVAL;
+  }
+  cudaSetDevice(ctx->device);
+  if (int r = check_ready(ctx)) return r;
+  if (int r = steady_alloc(ctx, true)) return r;
+  const double dt = ctx->der.dt;
+  const int nv = ctx->nv;
+  if (ctx->dual_inner < 0) {
+    // the previous physical step's state starts as the initial one (DualTimeStepping.cuh:64-72)
+    for (auto &B : ctx->blk)
+      CK(cudaMemcpyAsync(B.qn1, B.cv[0], (size_t)nv * B.db.plane * sizeof(double), cudaMemcpyDeviceToDevice,
+                         ctx->stream));
+    ctx->dual_inner = ctx->der.inner_iteration;
+  }
+  CK(cudaMemcpyAsync(ctx->d_dt, &dt, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  for (int s = 0; s < n_steps; ++s) {
+    const long long step = ++ctx->dual_step;
+    for (auto &B : ctx->blk) {
+      k_qn_star<<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, state_of(B, 0), B.qn1, B.qstar, nv, dt);
+      CK(cudaMemcpyAsync(B.qn1, B.cv[0], (size_t)nv * B.db.plane * sizeof(double), cudaMemcpyDeviceToDevice,
+                         ctx->stream));
+    }
+    const bool monitor = ctx->der.iteration_adjust_step > 0 && step % ctx->der.iteration_adjust_step == 0;
+    for (int iter = 1; iter <= ctx->dual_inner; ++iter) {
+      // store_last_iter: the residual reference of ostc_residual holds the inner iterate
+      if (monitor)
+        for (auto &B : ctx->blk)
+          k_store_last<<<grid_for(ctx, B.db.n, 256), 256, 0, ctx->stream>>>(B.db, state_of(B, 0), B.last);
+      const int r = ctx->precision == OSTC_PREC_MIXED ? enqueue_steady_iteration<float>(ctx, dt)
+                                                       : enqueue_steady_iteration<double>(ctx, dt);
+      if (r) return r;
+      if (monitor) {
+        // inner_converged (DualTimeStepping.cu:32-135)
+        double res[4];
+        if (int rr = ostc_residual(ctx, res)) return rr;
+        if (iter == 1)
+          for (int l = 0; l < 4; ++l) ctx->res_scale_inner[l] = res[l] < 1e-20 ? 1e-20 : res[l];
+        double err = res[0] / ctx->res_scale_inner[0];
+        for (int l = 1; l < 4; ++l) err = std::max(err, res[l] / ctx->res_scale_inner[l]);
+        if (std::isnan(err)) {
+          ctx->err = "NaN in the inner iterations of dual time stepping";
+          return OSTC_ENUMERIC;
+        }
+        if (iter == ctx->dual_inner && err > 1e-3 && ctx->dual_inner < ctx->der.max_inner_iteration)
+          ctx->dual_inner = std::min(ctx->dual_inner + 5, ctx->der.max_inner_iteration);
+        if (err < 1e-3) {
+          if (ctx->dual_inner - iter > 0) ctx->dual_inner = iter;
+          break;
+        }
+      }
+    }
+    k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->d_time, ctx->d_dt, ctx->d_step);
+    if (int r = stat_after_step(ctx)) return r;
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (inner_iters) *inner_iters = ctx->dual_inner;
   return OSTC_OK;
 }
 

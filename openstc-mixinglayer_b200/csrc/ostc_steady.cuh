@@ -119,10 +119,11 @@ struct DplurArgs {
   const double *dtl, *srad, *cj;
   double *dq, *dq0, *dqk;
   int nv, chem;
+  double diag_factor;  // 0 for the steady driver, 1.5 / dt for dual time stepping
 };
 
-// compute_DQ_0 (DPLUR.cuh:14-92): dq <- dt dq / diag, diag = 1 + dt (sum of the inviscid spectral
-// radii).  The reference adds 2 dt times a viscous spectral radius that it never computes (its array
+// compute_DQ_0 (DPLUR.cuh:14-92): dq <- dt dq / diag, diag = 1 + diag_factor dt + dt (sum of the
+// inviscid spectral radii).  The reference adds 2 dt times a viscous spectral radius that it never computes (its array
 // keeps the zeros of its allocation, Field.cu:553-565): that term is zero and left out.
 template <int NS>
 __global__ void __launch_bounds__(128) k_dplur_dq0(DevBlock b, DplurArgs a) {
@@ -131,7 +132,7 @@ __global__ void __launch_bounds__(128) k_dplur_dq0(DevBlock b, DplurArgs a) {
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
     const double dt = a.dtl[n];
     for (int l = 0; l < nv; ++l) a.dq[l * b.n + n] *= dt;
-    const double diag = 1 + dt * (a.srad[n] + a.srad[b.n + n] + a.srad[2 * b.n + n]);
+    const double diag = 1 + a.diag_factor * dt + dt * (a.srad[n] + a.srad[b.n + n] + a.srad[2 * b.n + n]);
     const int nflow = a.chem ? 5 : nv;
     for (int l = 0; l < nflow; ++l) a.dq[l * b.n + n] /= diag;
     if (!a.chem) continue;
@@ -222,7 +223,7 @@ __global__ void __launch_bounds__(128) k_dplur_inner(DevBlock b, DevState s, Dpl
       }
     }
     const double dt = a.dtl[n];
-    const double diag = 1 + dt * (a.srad[n] + a.srad[b.n + n] + a.srad[2 * b.n + n]);
+    const double diag = 1 + a.diag_factor * dt + dt * (a.srad[n] + a.srad[b.n + n] + a.srad[2 * b.n + n]);
     const int nflow = a.chem ? 5 : nv;
     for (int l = 0; l < nflow; ++l) a.dqk[l * b.n + n] = a.dq0[l * b.n + n] + dt * tot[l] / diag;
     if (!a.chem) continue;
@@ -261,6 +262,35 @@ __global__ void k_dplur_back(DevBlock b, double *__restrict__ dq, const double *
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
     const double dt = dtl[n];
     for (int l = 0; l < nv; ++l) dq[l * b.n + n] /= dt;
+  }
+}
+
+// compute_qn_star (DualTimeStepping.cu:3-14): q* = jac / (2 dt) (4 cv^n - cv^(n-1)) of every interior
+// node, from the current state and the previous physical step's conservative state qn1 (padded planes).
+__global__ void k_qn_star(DevBlock b, DevState s, const double *__restrict__ qn1, double *__restrict__ qstar,
+                          int nv, double dt) {
+  const long long P = b.plane;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % b.mx);
+    const long long r = n / b.mx;
+    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const long long p = b.id(i, j, k);
+    const double factor = 0.5 * b.jac[p] / dt;
+    for (int l = 0; l < nv; ++l) qstar[l * b.n + n] = factor * (4 * s.cv[l * P + p] - qn1[l * P + p]);
+  }
+}
+
+// compute_modified_rhs (DualTimeStepping.cu:16-30): dq += q* - 1.5 jac / dt cv.
+__global__ void k_modified_rhs(DevBlock b, DevState s, const double *__restrict__ qstar, double *__restrict__ dq,
+                               int nv, double dt) {
+  const long long P = b.plane;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % b.mx);
+    const long long r = n / b.mx;
+    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const long long p = b.id(i, j, k);
+    const double factor = 1.5 * b.jac[p] / dt;
+    for (int l = 0; l < nv; ++l) dq[l * b.n + n] += qstar[l * b.n + n] - factor * s.cv[l * P + p];
   }
 }
 

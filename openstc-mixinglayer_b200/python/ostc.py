@@ -31,7 +31,7 @@ EXPORTS = [
     "ostc_rhs_vjp", "ostc_rk3_step_vjp", "ostc_adjoint_steps", "ostc_run_states", "ostc_bounds_flags",
     "ostc_bounds_checked", "ostc_stat_enable", "ostc_stat_disable", "ostc_stat_info", "ostc_stat_get",
     "ostc_stat_export", "ostc_stat_import", "ostc_write_plt", "ostc_read_plt", "ostc_tune_report",
-    "ostc_set_sweep_variant", "ostc_steady_step",
+    "ostc_set_sweep_variant", "ostc_steady_step", "ostc_dual_time_step",
 ]
 
 
@@ -101,6 +101,7 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.ostc_tune_report.argtypes = [vp, ip, ip, ip, ctypes.POINTER(ip), ctypes.POINTER(ctypes.c_float), ip]
     lib.ostc_set_sweep_variant.argtypes = [vp, ip, ip, ip]
     lib.ostc_steady_step.argtypes = [vp, ip, ctypes.POINTER(ip), dp]
+    lib.ostc_dual_time_step.argtypes = [vp, ip, ctypes.POINTER(ip)]
     lib.ostc_timed_steps.argtypes = [vp, ip, dp]
     lib.ostc_step_kernel_count.argtypes = [vp, ctypes.POINTER(ip)]
     lib.ostc_residual_noalloc.argtypes = [vp, vp, ctypes.c_longlong, dp, vp]
@@ -369,6 +370,13 @@ class Solver:
         err = ctypes.c_double()
         self._check(self.lib.ostc_steady_step(self.h, n, ctypes.byref(done), ctypes.byref(err)))
         return done.value, err.value
+
+    def dual(self, n: int = 1) -> int:
+        """n physical steps of dual time stepping (ostc_dual_time_step); the inner-iteration count in
+        force afterwards."""
+        inner = ctypes.c_int()
+        self._check(self.lib.ostc_dual_time_step(self.h, n, ctypes.byref(inner)))
+        return inner.value
 
     def set_sweep_variant(self, dir: int, variant: int, precision: int = 0):
         """Pin sweep `dir` (0/1/2 = x/y/z) to kernel variant `variant` (-1: back to the autotuner)."""

@@ -82,7 +82,10 @@ class Case:
             "int output_file = 1000000",
             "int output_screen = 1000000",
             f"bool steady = {int(bool(s.get('steady', 0)))}",
-            "int temporal_scheme = 3",
+            f"int temporal_scheme = {s.get('temporal_scheme', 3)}",
+            f"int inner_iteration = {s.get('inner_iteration', 20)}",
+            f"int max_inner_iteration = {s.get('max_inner_iteration', 30)}",
+            f"int iteration_adjust_step = {s.get('iteration_adjust_step', 20)}",
             f"int implicit_method = {s.get('implicit_method', 0)}",
             f"int DPLUR_inner_step = {s.get('dplur_inner_step', 3)}",
             f"int chemSrcMethod = {s.get('chem_src_method', 0)}",

@@ -65,7 +65,8 @@ class OrcCase(ctypes.Structure):
                 ("finite_rate", ctypes.c_int), ("chem", ctypes.POINTER(OrcChem)), ("weno_eps_scale", ctypes.c_double),
                 ("v_ref", ctypes.c_double), ("has_init", ctypes.c_int), ("init_bv", ctypes.c_double * 6),
                 ("init_sv", ctypes.c_double * MAXS), ("chem_mode", ctypes.c_int), ("implicit_method", ctypes.c_int),
-                ("dplur_inner", ctypes.c_int), ("chem_src_method", ctypes.c_int)]
+                ("dplur_inner", ctypes.c_int), ("chem_src_method", ctypes.c_int), ("inner_iteration", ctypes.c_int),
+                ("max_inner_iteration", ctypes.c_int), ("iteration_adjust_step", ctypes.c_int)]
 
 
 def riemann_of(reconstruction: int, inviscid_scheme: int) -> int:
@@ -117,6 +118,8 @@ def load():
         lib.orc_step.restype = ctypes.c_double
         lib.orc_steady.argtypes = [vp, ctypes.c_int]
         lib.orc_steady.restype = None
+        lib.orc_dual.argtypes = [vp, ctypes.c_int]
+        lib.orc_dual.restype = ctypes.c_int
         lib.orc_stat_collect.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int, dp]
         lib.orc_time.argtypes = [vp]
         lib.orc_time.restype = ctypes.c_double
@@ -159,7 +162,12 @@ class Oracle:
         c.fixed_time_step, c.dt = 0, 1e-8
         c.implicit_method, c.dplur_inner = s.get("implicit_method", 0), s.get("dplur_inner_step", 3)
         c.chem_src_method = s.get("chem_src_method", 0)
+        c.inner_iteration, c.max_inner_iteration = s.get("inner_iteration", 20), s.get("max_inner_iteration", 30)
+        c.iteration_adjust_step = s.get("iteration_adjust_step", 20)
         self.steady_case = bool(s.get("steady", 0))
+        self.dual_case = not self.steady_case and s.get("temporal_scheme", 3) == 2
+        if self.dual_case:
+            c.fixed_time_step, c.dt = 1, s.get("dt", 1e-8)
         types = case.label_types()
         ff = {**case.farfield_states(), **case.wall_states(), **case.inflow_states(),
               **case.characteristic_states()}
@@ -249,9 +257,15 @@ class Oracle:
         """n iterations of the steady driver (local time steps, explicit / EPI / DA / DPLUR)."""
         self.lib.orc_steady(self.h, n)
 
+    def dual(self, n: int = 1) -> int:
+        """n physical steps of dual time stepping; the inner-iteration count in force afterwards."""
+        return self.lib.orc_dual(self.h, n)
+
     def advance(self, n: int):
-        """n steps of the case's own time-advance driver: steady iterations or SSP-RK3 steps."""
-        return self.steady(n) if self.steady_case else self.step(n)
+        """n steps of the case's own time-advance driver: steady iterations, dual-time or SSP-RK3 steps."""
+        if self.steady_case:
+            return self.steady(n)
+        return self.dual(n) if self.dual_case else self.step(n)
 
     def stat_collect(self, acc: np.ndarray, rey_idx=(), rho_p: bool = False):
         """Add one single-point statistics collection of the current state to acc (float64,

@@ -49,6 +49,11 @@ struct orc_ctx {
   /* steady driver: inviscid spectral radii per interior node [N][3] (local_time_step), chemical
    * source Jacobian per node (chem_src_jac: [N][ns][ns] for EPI, [N][ns] for DA), DPLUR iterates */
   double *srad, *cj, *dq0, *dqk;
+  /* dual time stepping: previous physical step's cv (qn1, padded), the BDF2 source q* (interior), the
+   * inner iteration's stored (rho, |V|, p, T), the physical step count and the inner-iteration count */
+  double *qn1, *qstar, *inlast;
+  int dual_step, inner, dual_init;
+  double res_scale_inner[4];
   face_t f[16];
   int nf;
   double t;
@@ -2123,7 +2128,7 @@ void orc_destroy(orc_ctx *o) {
   free(o->x); free(o->y); free(o->z); free(o->jac); free(o->met);
   free(o->cv); free(o->qn); free(o->bv); free(o->mul); free(o->dq); free(o->dtl);
   free(o->sv); free(o->rhod); free(o->cond); free(o->cpm); free(o->gam); free(o->acs);
-  free(o->srad); free(o->cj); free(o->dq0); free(o->dqk);
+  free(o->srad); free(o->cj); free(o->dq0); free(o->dqk); free(o->qn1); free(o->qstar); free(o->inlast);
   free(o);
 }
 
@@ -2305,7 +2310,7 @@ static void epi_solve(const orc_ctx *o, long q, double diag, double dt, double *
  * inner iterations (walls' dq zeroed first, set_wall_dq_to_0), convert_dq_back_to_dqDt.  The viscous
  * spectral radius the reference adds to the diagonal is never computed there (its array keeps the
  * zeros of its allocation, Field.cu:553-565), so those terms are zero. */
-static void dplur(orc_ctx *o) {
+static void dplur(orc_ctx *o, double diag_factor) {
   const long N = (long)o->mx * o->my * o->mz;
   const int nv = o->nv, ns = o->ns;
   const int fr = ns && o->c.finite_rate, csm = o->c.chem_src_method;
@@ -2315,7 +2320,7 @@ static void dplur(orc_ctx *o) {
         const long q = IQ(o, i, j, k);
         const double dt = o->dtl[q];
         for (int l = 0; l < nv; ++l) o->dq[l * N + q] *= dt;
-        const double diag = 1 + 0.0 * dt + dt * (o->srad[3 * q] + o->srad[3 * q + 1] + o->srad[3 * q + 2]);
+        const double diag = 1 + diag_factor * dt + dt * (o->srad[3 * q] + o->srad[3 * q + 1] + o->srad[3 * q + 2]);
         if (!fr) {
           for (int l = 0; l < nv; ++l) o->dq[l * N + q] /= diag;
           continue;
@@ -2369,7 +2374,7 @@ static void dplur(orc_ctx *o) {
             }
           }
           const double dt = o->dtl[q];
-          const double diag = 1 + 0.0 * dt + dt * (o->srad[3 * q] + o->srad[3 * q + 1] + o->srad[3 * q + 2]);
+          const double diag = 1 + diag_factor * dt + dt * (o->srad[3 * q] + o->srad[3 * q + 1] + o->srad[3 * q + 2]);
           const int nflow = fr ? 5 : nv;
           for (int l = 0; l < nflow; ++l) o->dqk[l * N + q] = o->dq0[l * N + q] + dt * tot[l] / diag;
           if (!fr) continue;
@@ -2418,6 +2423,36 @@ static void steady_update(orc_ctx *o) {
       }
 }
 
+/* dq of the steady and dual-time drivers: from zero, the chemical source first (with its Jacobian for
+ * chemSrcMethod 1 / 2), then the inviscid and viscous fluxes (SteadySim.cuh:78-88) */
+static void steady_rhs(orc_ctx *o) {
+  const long N = (long)o->mx * o->my * o->mz;
+  const int fr = o->ns && o->c.finite_rate, csm = o->c.chem_src_method;
+  memset(o->dq, 0, sizeof(double) * o->nv * N);
+  if (fr)
+    for (int k = 0; k < o->mz; ++k)
+      for (int j = 0; j < o->my; ++j)
+        for (int i = 0; i < o->mx; ++i) chemistry_node_jac(o, i, j, k, csm == 1 ? 2 : csm == 2 ? 3 : 0);
+  for (int d = 0; d < o->dim; ++d) {
+    const int is = o->c.inviscid_scheme;
+    if (is == 71 || is == 72) fvs_direction(o, d);
+    else if (o->c.reconstruction == 4 || o->c.reconstruction == 5) aweno_direction(o, d);
+    else pv_direction(o, d);
+  }
+  if (o->c.viscous_order != 0) viscous(o);
+}
+
+static void steady_buffers(orc_ctx *o, int dplur_needed) {
+  const long N = (long)o->mx * o->my * o->mz;
+  const int ns = o->ns, fr = ns && o->c.finite_rate, csm = o->c.chem_src_method;
+  if (!o->srad) o->srad = (double *)calloc(3 * N, sizeof(double));
+  if (fr && csm && !o->cj) o->cj = (double *)calloc(N * (csm == 1 ? ns * ns : ns), sizeof(double));
+  if (dplur_needed && !o->dq0) {
+    o->dq0 = (double *)calloc(o->nv * N, sizeof(double));
+    o->dqk = (double *)calloc(o->nv * N, sizeof(double));
+  }
+}
+
 /* steady_simulation<mixture model, Laminar> iteration body for one block (SteadySim.cuh:65-140): dq
  * from zero; the chemical source first (with its Jacobian for chemSrcMethod 1 / 2), the inviscid and
  * viscous fluxes; local_time_step; implicit_treatment (ImplicitTreatmentHPP.cuh:7-54: EPI or DA when
@@ -2426,28 +2461,12 @@ static void steady_update(orc_ctx *o) {
 void orc_steady(orc_ctx *o, int n) {
   const long N = (long)o->mx * o->my * o->mz;
   const int ns = o->ns, fr = ns && o->c.finite_rate, csm = o->c.chem_src_method;
-  if (!o->srad) o->srad = (double *)calloc(3 * N, sizeof(double));
-  if (fr && csm && !o->cj) o->cj = (double *)calloc(N * (csm == 1 ? ns * ns : ns), sizeof(double));
-  if (o->c.implicit_method == 1 && !o->dq0) {
-    o->dq0 = (double *)calloc(o->nv * N, sizeof(double));
-    o->dqk = (double *)calloc(o->nv * N, sizeof(double));
-  }
+  steady_buffers(o, o->c.implicit_method == 1);
   for (int s = 0; s < n; ++s) {
-    memset(o->dq, 0, sizeof(double) * o->nv * N);
-    if (fr)
-      for (int k = 0; k < o->mz; ++k)
-        for (int j = 0; j < o->my; ++j)
-          for (int i = 0; i < o->mx; ++i) chemistry_node_jac(o, i, j, k, csm == 1 ? 2 : csm == 2 ? 3 : 0);
-    for (int d = 0; d < o->dim; ++d) {
-      const int is = o->c.inviscid_scheme;
-      if (is == 71 || is == 72) fvs_direction(o, d);
-      else if (o->c.reconstruction == 4 || o->c.reconstruction == 5) aweno_direction(o, d);
-      else pv_direction(o, d);
-    }
-    if (o->c.viscous_order != 0) viscous(o);
+    steady_rhs(o);
     orc_dt(o);
     if (o->c.implicit_method == 1) {
-      dplur(o);
+      dplur(o, 0.0);
     } else if (fr && csm) {
       for (long q = 0; q < N; ++q) {
         const double dt = o->dtl[q];
@@ -2464,6 +2483,105 @@ void orc_steady(orc_ctx *o, int n) {
     steady_update(o);
     fill_ghosts(o);
   }
+}
+
+/* (rho, |V|, p, T) of every interior node (store_last_iter, DualTimeStepping.cu:154-167) */
+static void store_last_iter(orc_ctx *o) {
+  const long P = o->P;
+  for (int k = 0; k < o->mz; ++k)
+    for (int j = 0; j < o->my; ++j)
+      for (int i = 0; i < o->mx; ++i) {
+        const long p = ID(o, i, j, k), q = IQ(o, i, j, k);
+        o->inlast[4 * q] = o->bv[p];
+        o->inlast[4 * q + 1] = sqrt(o->bv[P + p] * o->bv[P + p] + o->bv[2 * P + p] * o->bv[2 * P + p] +
+                                    o->bv[3 * P + p] * o->bv[3 * P + p]);
+        o->inlast[4 * q + 2] = o->bv[4 * P + p];
+        o->inlast[4 * q + 3] = o->bv[5 * P + p];
+      }
+}
+
+/* inner_converged (DualTimeStepping.cu:32-135): RMS change since store_last_iter, scaled by that of the
+ * first inner iteration; adapts the inner-iteration count; returns 1 when the inner loop stops */
+static int inner_converged(orc_ctx *o, int iter) {
+  const long P = o->P, N = (long)o->mx * o->my * o->mz;
+  double res[4] = {0, 0, 0, 0};
+  for (int k = 0; k < o->mz; ++k)
+    for (int j = 0; j < o->my; ++j)
+      for (int i = 0; i < o->mx; ++i) {
+        const long p = ID(o, i, j, k), q = IQ(o, i, j, k);
+        const double vel = sqrt(o->bv[P + p] * o->bv[P + p] + o->bv[2 * P + p] * o->bv[2 * P + p] +
+                                o->bv[3 * P + p] * o->bv[3 * P + p]);
+        const double d[4] = {o->bv[p] - o->inlast[4 * q], vel - o->inlast[4 * q + 1],
+                             o->bv[4 * P + p] - o->inlast[4 * q + 2], o->bv[5 * P + p] - o->inlast[4 * q + 3]};
+        for (int l = 0; l < 4; ++l) res[l] += d[l] * d[l];
+      }
+  for (int l = 0; l < 4; ++l) res[l] = sqrt(res[l] / N);
+  if (iter == 1)
+    for (int l = 0; l < 4; ++l) o->res_scale_inner[l] = res[l] < 1e-20 ? 1e-20 : res[l];
+  double err = res[0] / o->res_scale_inner[0];
+  for (int l = 1; l < 4; ++l)
+    if (res[l] / o->res_scale_inner[l] > err) err = res[l] / o->res_scale_inner[l];
+  if (iter == o->inner && err > 1e-3 && o->inner < o->c.max_inner_iteration) {
+    o->inner += 5;
+    if (o->inner > o->c.max_inner_iteration) o->inner = o->c.max_inner_iteration;
+  }
+  if (err < 1e-3) {
+    if (o->inner - iter > 0) o->inner = iter;
+    return 1;
+  }
+  return 0;
+}
+
+/* dual_time_stepping<mixture model, Laminar> (DualTimeStepping.cuh:32-252) for one block: per physical
+ * step q* = jac / (2 dt) (4 cv - cv_prev) (compute_qn_star, DualTimeStepping.cu:3-14), then up to
+ * `inner` pseudo-time iterations: dq, local time steps, dq += q* - 1.5 jac / dt cv (compute_modified_rhs,
+ * :16-30), DPLUR with diag_factor 1.5 / dt, update_cv_and_bv, boundary faces, k copy, properties; every
+ * iteration_adjust_step-th step the inner loop is monitored and its count adapted. */
+int orc_dual(orc_ctx *o, int n) {
+  const long P = o->P, N = (long)o->mx * o->my * o->mz;
+  const int nv = o->nv;
+  const double dt = o->c.dt, diag_factor = 1.5 / dt;
+  steady_buffers(o, 1);
+  if (!o->qn1) {
+    o->qn1 = (double *)calloc((size_t)nv * P, sizeof(double));
+    o->qstar = (double *)calloc((size_t)nv * N, sizeof(double));
+    o->inlast = (double *)calloc(4 * N, sizeof(double));
+  }
+  if (!o->dual_init) {
+    memcpy(o->qn1, o->cv, sizeof(double) * nv * P);
+    o->inner = o->c.inner_iteration;
+    o->dual_init = 1;
+  }
+  for (int s = 0; s < n; ++s) {
+    const int step = ++o->dual_step;
+    for (int k = 0; k < o->mz; ++k)
+      for (int j = 0; j < o->my; ++j)
+        for (int i = 0; i < o->mx; ++i) {
+          const long p = ID(o, i, j, k), q = IQ(o, i, j, k);
+          const double factor = 0.5 * o->jac[p] / dt;
+          for (int l = 0; l < nv; ++l) o->qstar[l * N + q] = factor * (4 * o->cv[l * P + p] - o->qn1[l * P + p]);
+        }
+    memcpy(o->qn1, o->cv, sizeof(double) * nv * P);
+    const int monitor = step % o->c.iteration_adjust_step == 0;
+    for (int iter = 1; iter <= o->inner; ++iter) {
+      if (monitor) store_last_iter(o);
+      steady_rhs(o);
+      orc_dt(o);
+      for (int k = 0; k < o->mz; ++k)
+        for (int j = 0; j < o->my; ++j)
+          for (int i = 0; i < o->mx; ++i) {
+            const long p = ID(o, i, j, k), q = IQ(o, i, j, k);
+            const double factor = 1.5 * o->jac[p] / dt;
+            for (int l = 0; l < nv; ++l) o->dq[l * N + q] += o->qstar[l * N + q] - factor * o->cv[l * P + p];
+          }
+      dplur(o, diag_factor);
+      steady_update(o);
+      fill_ghosts(o);
+      if (monitor && inner_converged(o, iter)) break;
+    }
+    o->t += dt;
+  }
+  return o->inner;
 }
 
 /* ---------------------------------------------------------------- single-point statistics */

@@ -84,6 +84,10 @@ typedef struct {
    * (explicit, plus the point-implicit chemistry of chem_src_method) or 1 (DPLUR with dplur_inner
    * inner iterations, DPLUR.cuh:282-322); chem_src_method 0 explicit, 1 EPI, 2 diagonal (DA) */
   int implicit_method, dplur_inner, chem_src_method;
+  /* dual time stepping (dual_time_stepping, DualTimeStepping.cuh:32-252; temporal_scheme 2): physical
+   * step dt (the case's dt), inner iterations and their adaptation (inner_converged,
+   * DualTimeStepping.cu:32-135) */
+  int inner_iteration, max_inner_iteration, iteration_adjust_step;
 } orc_case;
 
 typedef struct orc_ctx orc_ctx;
@@ -112,6 +116,8 @@ void orc_rhs(orc_ctx *o, unsigned mask, double *dq);
 double orc_step(orc_ctx *o, int n);
 /* n iterations of the steady driver (steady_simulation, SteadySim.cuh:65-140) */
 void orc_steady(orc_ctx *o, int n);
+/* n physical steps of dual time stepping; returns the inner-iteration count in force after them */
+int orc_dual(orc_ctx *o, int n);
 /* one single-point statistics collection added to acc (collect_single_point_basic_statistics) */
 void orc_stat_collect(const orc_ctx *o, int n_rey, const int *rey_idx, int rho_p, double *acc);
 double orc_time(const orc_ctx *o);

@@ -8,7 +8,8 @@
 // initialised interior primitive variables with the ones in state_in.bin ([block][6 + n_spec][mz][my][mx]
 // doubles: rho u v w p T, then the mass fractions), runs the reference's
 // Driver::initialize_computation() and RK3() (RK.cuh:19-228) for total_step steps - or, when the setup
-// has steady = 1, its steady_simulation() (SteadySim.cuh:15-140) for total_step iterations - and writes the
+// has steady = 1, its steady_simulation() (SteadySim.cuh:15-140) for total_step iterations, or with
+// temporal_scheme = 2 its dual_time_stepping() (DualTimeStepping.cuh:32-252) for total_step steps - and writes the
 // interior cv[n_var], bv[6] and sv[n_spec] of every block, then the physical time, to state_out.bin.  It prints the
 // wall time of the RK3 call (steps, per-step output checks and the final flow-field file included).
 #include <chrono>
@@ -77,11 +78,14 @@ int run_model(cfd::Parameter &parameter, cfd::Mesh &mesh, const char *fin, const
 
   g_stage = "initialize_computation";
   driver.initialize_computation();
-  g_stage = parameter.get_bool("steady") ? "steady_simulation" : "RK3";
+  const bool steady = parameter.get_bool("steady"), dual = !steady && parameter.get_int("temporal_scheme") == 2;
+  g_stage = steady ? "steady_simulation" : dual ? "dual_time_stepping" : "RK3";
   cudaDeviceSynchronize();
   const auto t_begin = std::chrono::steady_clock::now();
-  // the time-advance driver Simulate.cuh picks: the steady local-time-step loop (SteadySim.cuh) or RK3
-  if (parameter.get_bool("steady")) cfd::steady_simulation<M, cfd::Laminar>(driver);
+  // the time-advance driver Simulate.cuh picks: the steady local-time-step loop (SteadySim.cuh), dual
+  // time stepping (DualTimeStepping.cuh, temporal_scheme 2) or RK3
+  if (steady) cfd::steady_simulation<M, cfd::Laminar>(driver);
+  else if (dual) cfd::dual_time_stepping<M, cfd::Laminar>(driver);
   else cfd::RK3<M, cfd::Laminar>(driver);
   cudaDeviceSynchronize();
   const double rk3_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_begin).count();

@@ -39,6 +39,10 @@ STAT_FILES = ["output/stat/coll_rey_1st.bin", "output/stat/coll_fav_1st.bin", "o
 PLT = ["output/flowfield.plt"]
 # steady driver settings (no early stop on convergence: the fixture runs a fixed iteration count)
 STEADY = dict(steady=1, implicit_method=0, dplur_inner_step=3, chem_src_method=0, convergence_criteria=1e-300)
+# dual time stepping settings (its DPLUR needs implicit_method 1 for the reference to allocate the iterates,
+# Field.cu:557-563)
+DUAL = dict(steady=0, temporal_scheme=2, implicit_method=1, dplur_inner_step=2, inner_iteration=4,
+            max_inner_iteration=8, iteration_adjust_step=2)
 
 CASES = [
     # name, generator, kwargs, steps[, options: sampled / setup (extra setup.txt lines) / files (kept)]
@@ -106,6 +110,12 @@ CASES = [
      dict(mx=16, my=12, mz=8, steady=dict(STEADY, implicit_method=1, dplur_inner_step=2)), 5),
     ("st_rml3d_mix_dplur", "reacting_mixing_layer_3d",
      dict(mx=16, my=12, mz=8, finite_rate=False, steady=dict(STEADY, implicit_method=1)), 5),
+    # dual time stepping (DualTimeStepping.cuh, temporal_scheme 2): BDF2 physical steps of fixed dt, DPLUR
+    # pseudo-time inner iterations whose count adapts every iteration_adjust_step-th step
+    ("dt_ml3d", "mixing_layer_3d", dict(mx=24, my=20, mz=12, ybc="outflow", steady=dict(DUAL, dt=2e-7)), 6),
+    ("dt_ml2d", "mixing_layer_2d", dict(mx=49, my=33, steady=dict(DUAL, dt=4e-7)), 6),
+    ("dt_rml3d_epi", "reacting_mixing_layer_3d",
+     dict(mx=16, my=12, mz=8, steady=dict(DUAL, dt=5e-8, chem_src_method=1)), 4),
     # the files the reference writes at the end of a run: flow field and statistics
     ("ml3d_stat_plt", "mixing_layer_3d", dict(mx=16, my=12, mz=8, ybc="outflow"), 6,
      dict(setup=STAT_SETUP, files=PLT + STAT_FILES)),

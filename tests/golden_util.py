@@ -117,8 +117,8 @@ def assert_state(cv, z, block=None):
 
 
 def run_library(case, steps, directory, setup_extra=""):
-    """Advances the case `steps` SSP-RK3 steps (or, for a steady case, steady-driver iterations) through
-    the C ABI; returns the open solver."""
+    """Advances the case `steps` SSP-RK3 steps (or, for a steady case, steady-driver iterations; for
+    temporal_scheme 2, dual-time steps) through the C ABI; returns the open solver."""
     import ostc
 
     d = oc.write_case(case, directory)
@@ -133,6 +133,8 @@ def run_library(case, steps, directory, setup_extra=""):
     if case.scheme.get("steady"):
         done, _ = s.steady(steps)
         assert done == steps
+    elif case.scheme.get("temporal_scheme", 3) == 2:
+        s.dual(steps)
     else:
         s.step(steps)
     return s
@@ -146,6 +148,10 @@ def check_library(case, steps, z, t_ref, directory, setup_extra=""):
             assert_state(s.get_state(block=b)[0], z, block=b)
     else:
         assert_state(s.get_state()[0], z)
+    if case.scheme.get("temporal_scheme", 3) == 2 and not case.scheme.get("steady"):
+        # the reference's dual-time driver advances its physical time without storing it in its
+        # solution_time parameter (DualTimeStepping.cuh:172), which the fixture records: it is steps dt
+        t_ref = steps * case.scheme["dt"]
     assert abs(s.time() - t_ref) <= TOL_T * t_ref
     assert s.error_flags() == 0
     return s

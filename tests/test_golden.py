@@ -66,6 +66,8 @@ def test_oracle_matches_reference(built, path):
     o.set_state(case.bv)
     o.advance(steps)
     gu.assert_state(o.get_state()[0], z)
+    if o.dual_case:
+        t_ref = steps * case.scheme["dt"]  # not stored by the reference's dual-time driver
     assert abs(o.time() - t_ref) <= gu.TOL_T * t_ref
 
 

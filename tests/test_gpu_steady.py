@@ -1,4 +1,5 @@
-"""The steady driver (ostc_steady_step: the reference's steady_simulation, SteadySim.cuh:15-140) on the GPU.
+"""The steady driver (ostc_steady_step: the reference's steady_simulation, SteadySim.cuh:15-140) and dual time
+stepping (ostc_dual_time_step: dual_time_stepping, DualTimeStepping.cuh:32-252) on the GPU.
 
 * Against the reference's own FP64 build: fixtures golden_st_*.npz (tests/golden/make_golden.py) hold
   the state the reference reached after its steady iterations - air 3-D explicit and DPLUR, air 2-D
@@ -8,6 +9,9 @@
 * Against the oracle's restatement (oracle/ostc_oracle.c orc_steady): DPLUR with no-slip walls (whose
   dq is zeroed on the wall nodes; the reference's own wall zeroing writes outside its array and defines
   no result to match) and DPLUR + DA.
+* Dual time stepping against the reference build (fixtures golden_dt_*.npz: air 3-D and 2-D, the
+  9-species layer with EPI chemistry; BDF2 physical steps, DPLUR pseudo-time iterations whose count
+  adapts every second step) and the adapted inner-iteration count against the oracle's.
 * The convergence stop of the reference (residual scaled by that of the first iteration, checked after
   iteration 1 and every output_screen-th) and the mixed-precision steady iteration against FP64.
 """
@@ -87,3 +91,26 @@ def test_steady_mixed_precision(built, tmp_path):
         s.close()
     err = oc.relative_errors(out[1], out[0])
     assert all(l2 < 1e-6 for _, l2 in err), err
+
+
+@pytest.mark.parametrize("name", ["dt_ml3d", "dt_ml2d", "dt_rml3d_epi"])
+def test_dual_time_matches_reference_build(built, tmp_path, name):
+    case, steps, z, t_ref = gu.load(gu.fixture_path(name))
+    gu.check_library(case, steps, z, t_ref, tmp_path / name).close()
+
+
+def test_dual_time_inner_adaptation_matches_oracle(built, tmp_path):
+    dual = dict(steady=0, temporal_scheme=2, implicit_method=1, dplur_inner_step=2, inner_iteration=3,
+                max_inner_iteration=9, iteration_adjust_step=1, dt=3e-7)
+    case = oc.mixing_layer_3d(mx=24, my=20, mz=12, ybc="outflow", steady=dual)
+    d = oc.write_case(case, tmp_path / "adapt")
+    s = ostc.Solver(str(d))
+    s.set_state(case.bv)
+    o = Oracle(case)
+    o.set_state(case.bv)
+    for _ in range(4):
+        assert s.dual(1) == o.dual(1)
+    err = oc.relative_errors(s.get_state()[0], o.get_state()[0])
+    assert all(m < gu.TOL and l2 < gu.TOL for m, l2 in err), err
+    assert abs(s.time() - o.time()) <= 1e-14 * o.time()
+    s.close()
