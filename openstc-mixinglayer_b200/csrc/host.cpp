@@ -809,7 +809,7 @@ double sutherland_host(double t) { return 1.7894e-5 * std::pow(t / 288.16, 1.5) 
 // mixture weight, velocity = Mach * c along (u, v, w).  Returns false with err set when the struct
 // lacks mach, pressure or temperature.
 bool inflow_state(const Setup &s, const std::string &name, const ChemTables *chem, double bv[6],
-                  std::vector<double> &y, double &c, std::string &err) {
+                  std::vector<double> &y, double &c, std::string &err, double *gamma_out) {
   auto it = s.structs.find(name);
   if (it == s.structs.end()) {
     err = "struct '" + name + "' is not defined in the setup";
@@ -851,6 +851,7 @@ bool inflow_state(const Setup &s, const std::string &name, const ChemTables *che
     gamma = cpt / cvt;
   }
   c = std::sqrt(gamma * kRu / mw * temperature);
+  if (gamma_out) *gamma_out = gamma;
   const double velocity = mach * c;
   bv[0] = pressure * mw / (kRu * temperature);
   bv[1] = struct_real(st, "u", 1.0) * velocity;
@@ -983,15 +984,15 @@ bool resolve_boundaries(const Setup &s, const Derived &d, HostMesh &mesh, std::s
         }
         continue;
       }
-      if (f.type == kFarfield && d.species != 0) {
-        err = "far-field faces (label " + std::to_string(f.label) +
-              ") are implemented for air; mixtures use symmetry, outflow or periodic faces";
-        return false;
-      }
       if (f.type == kFarfield) {
         if (it == lab.end()) {
           err = "farfield label " + std::to_string(f.label) + " needs a struct in boundary_conditions";
           return false;
+        }
+        if (d.species != 0) {
+          // mixtures: the state needs the species tables (resolve_inflows)
+          f.struct_name = it->second.second;
+          continue;
         }
         const auto &st = s.structs.at(it->second.second);
         // FarField::FarField (BoundCond.cpp:586-669), air
@@ -1064,6 +1065,32 @@ bool resolve_inflows(const Setup &s, const ChemTables *chem, HostMesh &mesh, std
         f.u = struct_real(st, "u", 1.0);
         f.v = struct_real(st, "v", 0.0);
         f.w = struct_real(st, "w", 0.0);
+        continue;
+      }
+      if (f.type == kFarfield && chem && chem->n_spec > 0) {
+        // FarField::FarField for mixtures (BoundCond.cpp:586-669): (mach, pressure, temperature) with the
+        // struct's mass fractions; gamma from cp and cv of the composition at the temperature
+        const auto &st = s.structs.at(f.struct_name);
+        if (struct_real(st, "pressure", -1) < 0 || struct_real(st, "temperature", -1) < 0 ||
+            struct_real(st, "mach", -1) < 0) {
+          err = "far-field struct '" + f.struct_name + "' of a mixture needs mach, pressure and temperature on this path";
+          return false;
+        }
+        double bv[6], c, gamma;
+        if (!inflow_state(s, f.struct_name, chem, bv, f.y, c, err, &gamma)) return false;
+        double mw = 0;
+        for (int i = 0; i < chem->n_spec; ++i) mw += f.y[i] / chem->mw[i];
+        mw = 1 / mw;
+        f.density = bv[0];
+        f.u = bv[1];
+        f.v = bv[2];
+        f.w = bv[3];
+        f.pressure = bv[4];
+        f.temperature = bv[5];
+        f.acoustic_speed = c;
+        f.gamma = gamma;
+        f.mw = mw;
+        f.entropy = bv[4] / std::pow(bv[0], f.gamma);
         continue;
       }
       if (f.type != kInflow) continue;

@@ -149,10 +149,11 @@ bool resolve_inflows(const Setup &s, const ChemTables *chem, HostMesh &mesh, std
 // rho_inf^2 v_inf^2 and v_inf of the struct named by reference_state (0, 0 without one): the scales of
 // the flux-split WENO epsilon (DParameter.cu:26-29, WENO.cu:1466-1473).
 bool reference_scales(const Setup &s, const ChemTables *chem, double &eps_scale, double &v_ref, std::string &err);
-// The state (rho, u, v, w, p, T; mass fractions y, acoustic speed c) of a plain inflow struct, as the
-// reference's default initialisation fills every node of a block with it (Field.cu:316-345).
+// The state (rho, u, v, w, p, T; mass fractions y, acoustic speed c; gamma through gamma_out) of a plain
+// inflow struct, as the reference's default initialisation fills every node of a block with it
+// (Field.cu:316-345).
 bool inflow_state(const Setup &s, const std::string &name, const ChemTables *chem, double bv[6],
-                  std::vector<double> &y, double &c, std::string &err);
+                  std::vector<double> &y, double &c, std::string &err, double *gamma_out = nullptr);
 // Order in which faces are applied each stage (BoundCond.cuh:1488-1679): a list of (block, face).
 std::vector<std::pair<int, int>> bc_order(const Setup &s, const HostMesh &mesh);
 

@@ -76,7 +76,7 @@ struct DevState {
 
 struct DevFace {
   int type, face, direction, rs[3], re[3];
-  double density, u, v, w, pressure, temperature, acoustic_speed, gamma, entropy;
+  double density, u, v, w, pressure, temperature, acoustic_speed, gamma, entropy, mw;
   int wall_adiabatic;  // walls: 1 adiabatic, 0 isothermal at `temperature`
   double y[16];        // inflow mass fractions (mixtures)
 };
@@ -913,10 +913,94 @@ __device__ __forceinline__ void finish_node(const DevBlock &b, DevState s, long 
   s.mul[p] = sutherland(s.bv[5 * b.plane + p]);
 }
 
+// apply_farfield for mixtures (BoundCond.cuh:755-1022) at face node pb: the node's gamma, its mixture
+// molecular weight from its mass fractions; supersonic inflow takes the far-field state and mass
+// fractions, supersonic outflow copies the node; subsonic faces take the Riemann invariants, the
+// velocity and composition of the far field (inflow, u_n < 0) or of the node, and a gamma iterated
+// with cp of the face temperature until it changes by less than 1e-4.  As in the reference, the
+// entropy of the inflow branch is chosen for u_n <= 0 but its velocity and composition for u_n < 0.
+__device__ void farfield_mixture(const DevBlock &b, DevState s, const DevFace &f, long long pb, long long dstep,
+                                 const double *gam_prev) {
+  const long long P = b.plane;
+  const int ns = c_mix.ns;
+  double nx = b.met[(f.face * 3 + 0) * P + pb], ny = b.met[(f.face * 3 + 1) * P + pb],
+         nz = b.met[(f.face * 3 + 2) * P + pb];
+  const double gni = f.direction / sqrt(nx * nx + ny * ny + nz * nz);
+  nx *= gni;
+  ny *= gni;
+  nz *= gni;
+  const double ub = s.bv[P + pb], vb = s.bv[2 * P + pb], wb = s.bv[3 * P + pb];
+  const double uf = nx * ub + ny * vb + nz * wb;
+  double svb[kMS];
+  for (int l = 0; l < ns; ++l) svb[l] = s.sv[l * P + pb];
+  const double gb = gam_prev[pb];
+  double mw_inv = 0;
+  for (int l = 0; l < ns; ++l) mw_inv += svb[l] / c_mix.mw[l];
+  double mw = 1.0 / mw_inv;
+  const double pbv = s.bv[4 * P + pb], rb = s.bv[pb];
+  const double ab = sqrt(gb * pbv / rb);
+  const double mb = uf / ab;
+  double vals[6];
+  if (mb <= -1) {
+    vals[0] = f.density; vals[1] = f.u; vals[2] = f.v; vals[3] = f.w; vals[4] = f.pressure; vals[5] = f.temperature;
+    for (int l = 0; l < ns; ++l) svb[l] = f.y[l];
+  } else if (mb >= 1) {
+    for (int g = 1; g <= b.g; ++g) {
+      const long long pg = pb + g * dstep;
+      for (int l = 0; l < 6; ++l) s.bv[l * P + pg] = s.bv[l * P + pb];
+      for (int l = 0; l < ns; ++l) s.sv[l * P + pg] = s.sv[l * P + pb];
+      mix_cv_from_bv_node<0>(b, s, pg);
+    }
+    return;
+  } else {
+    const double rpos = uf + 2 * ab / (gb - 1);
+    const double uinf = f.u * nx + f.v * ny + f.w * nz;
+    const double rneg = uinf - 2 * f.acoustic_speed / (f.gamma - 1);
+    const double Un = 0.5 * (rpos + rneg);
+    if (mb < 0) {
+      vals[1] = f.u + (Un - uinf) * nx;
+      vals[2] = f.v + (Un - uinf) * ny;
+      vals[3] = f.w + (Un - uinf) * nz;
+      for (int l = 0; l < ns; ++l) svb[l] = f.y[l];
+      mw = f.mw;
+    } else {
+      vals[1] = ub + (Un - uf) * nx;
+      vals[2] = vb + (Un - uf) * ny;
+      vals[3] = wb + (Un - uf) * nz;
+    }
+    double gamma = kGamma, err = 1, rho = 0, pr = 0, t = 0;
+    // the reference's loop has no bound; 100 iterations (far more than the few it takes) end it here
+    for (int it = 0; err > 1e-4 && it < 100; ++it) {
+      const double glast = gamma;
+      const double cb = 0.25 * (gamma - 1) * (rpos - rneg);
+      const double sb = mb <= 0 ? f.entropy : pbv / pow(rb, gamma);
+      rho = pow(cb * cb / (gamma * sb), 1 / (gamma - 1));
+      pr = rho * cb * cb / gamma;
+      t = pr * mw / (rho * kRuD);
+      double cp[kMS];
+      mix_h_cp<0>(t, (double *)nullptr, cp);
+      double cpt = 0;
+      for (int l = 0; l < ns; ++l) cpt += cp[l] * svb[l];
+      gamma = cpt / (cpt - kRuD / mw);
+      err = fabs(1 - gamma / glast);
+    }
+    vals[0] = rho;
+    vals[4] = pr;
+    vals[5] = t;
+  }
+  for (int g = 0; g <= b.g; ++g) {
+    const long long pg = pb + g * dstep;
+#pragma unroll
+    for (int l = 0; l < 6; ++l) s.bv[l * P + pg] = vals[l];
+    for (int l = 0; l < ns; ++l) s.sv[l * P + pg] = svb[l];
+    mix_cv_from_bv_node<0>(b, s, pg);
+  }
+}
+
 // One boundary face: apply_symmetry / apply_outflow / apply_periodic / apply_farfield<Air>
 // (BoundCond.cuh:137-233, 755-1022, 1443-1486).  Threads cover the two tangential index ranges,
 // which include ngg ghost layers on each side (Mesh.cpp:14-32).
-__global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace f) {
+__global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace f, const double *gam_prev) {
   const int t0 = f.face == 0 ? 1 : 0;
   const int t1 = f.face == 2 ? 1 : 2;
   const int n0 = f.re[t0] - f.rs[t0] + 1, n1 = f.re[t1] - f.rs[t1] + 1;
@@ -1129,6 +1213,8 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
         copy_bv(b, s, pg, ps);
         finish_node(b, s, pg);
       }
+    } else if (f.type == kFarfield && s.sv) {
+      farfield_mixture(b, s, f, pb, dstep, gam_prev);
     } else if (f.type == kFarfield) {
       double nx = b.met[(f.face * 3 + 0) * P + pb], ny = b.met[(f.face * 3 + 1) * P + pb],
              nz = b.met[(f.face * 3 + 2) * P + pb];
@@ -1939,7 +2025,9 @@ void launch_carry(ostc_ctx *ctx, BlockRes &B, DevState in, DevState out) {
   }
 }
 
-void launch_bcs(ostc_ctx *ctx, int block, DevState out) {
+// gam_prev: where a mixture far-field face reads the gamma of its face node - the properties of the
+// stage input (the reference's in-place state holds the last properties sweep there); null = out's.
+void launch_bcs(ostc_ctx *ctx, int block, DevState out, const double *gam_prev = nullptr) {
   for (const auto &bf : ctx->order) {
     if (bf.first != block) continue;
     BlockRes &B = ctx->blk[block];
@@ -1947,7 +2035,7 @@ void launch_bcs(ostc_ctx *ctx, int block, DevState out) {
     const int t0 = f.face == 0 ? 1 : 0, t1 = f.face == 2 ? 1 : 2;
     const long long nn = (long long)(f.re[t0] - f.rs[t0] + 1) * (f.re[t1] - f.rs[t1] + 1);
     long tok = begin_t(ctx, "bc_face");
-    k_bc_face<<<grid_for(ctx, nn, 128), 128, 0, ctx->stream>>>(B.db, out, f);
+    k_bc_face<<<grid_for(ctx, nn, 128), 128, 0, ctx->stream>>>(B.db, out, f, gam_prev ? gam_prev : out.gam);
     end_t(ctx, tok);
   }
 }
@@ -2116,7 +2204,7 @@ int enqueue_step(ostc_ctx *ctx) {
       a.flags = ctx->d_flags;
       launch_visc<T>(ctx, B, a);
       launch_carry(ctx, B, state_of(B, sin), state_of(B, sout));
-      launch_bcs(ctx, bi, state_of(B, sout));
+      launch_bcs(ctx, bi, state_of(B, sout), state_of(B, sin).gam);
     });
     launch_interfaces(ctx, sout);
   }
@@ -2164,7 +2252,7 @@ void enqueue_mix_stage(ostc_ctx *ctx, int rk, int sout_override = -1) {
       end_t(ctx, tok);
     }
     launch_carry(ctx, B, in, state_of(B, sout));
-    launch_bcs(ctx, bi, state_of(B, sout));
+    launch_bcs(ctx, bi, state_of(B, sout), in.gam);
   });
   launch_interfaces(ctx, sout);
   for_blocks(ctx, [&](int bi) {
@@ -2370,6 +2458,13 @@ void enqueue_set_state(ostc_ctx *ctx, BlockRes &B, const double *bv, const doubl
       cudaMemsetAsync(B.sv[0], 0, (size_t)ns * B.db.plane * sizeof(double), ctx->stream);
     }
     k_scatter<<<grid_for(ctx, ns * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, sv, B.sv[0], ns);
+    // the properties start from zero, as the reference's freshly allocated arrays do: its first
+    // boundary faces (initialize_computation, Driver.cu:145-147) run before any properties sweep, and
+    // a mixture far-field face reads gamma there (BoundCond.cuh:788)
+    cudaMemsetAsync(B.gam[0], 0, B.db.plane * sizeof(double), ctx->stream);
+    cudaMemsetAsync(B.acs[0], 0, B.db.plane * sizeof(double), ctx->stream);
+    cudaMemsetAsync(B.cond[0], 0, B.db.plane * sizeof(double), ctx->stream);
+    cudaMemsetAsync(B.rhod[0], 0, (size_t)ns * B.db.plane * sizeof(double), ctx->stream);
   }
 }
 
@@ -2759,6 +2854,7 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
       f.acoustic_speed = hf.acoustic_speed;
       f.gamma = hf.gamma;
       f.entropy = hf.entropy;
+      f.mw = hf.mw;
       f.wall_adiabatic = hf.wall_adiabatic;
       for (size_t l = 0; l < hf.y.size() && l < 16; ++l) f.y[l] = hf.y[l];
       R.faces.push_back(f);

@@ -128,7 +128,8 @@ class Case:
         return "\n".join(lines) + "\n"
 
     def farfield_states(self):
-        """FarField ctor for air (BoundCond.cpp:586-669): label -> state dict."""
+        """FarField ctor (BoundCond.cpp:586-669) from (mach, pressure, temperature): label -> state dict;
+        for mixtures with the struct's mass fractions y, their molecular weight and gamma = cp / cv."""
         out = {}
         for name, st in self.bc_structs.items():
             if st.get("type", (None, None))[1] != "farfield":
@@ -136,11 +137,26 @@ class Case:
             g = {k: v for k, (t, v) in st.items()}
             mach, p, t = g.get("mach", -1.0), g.get("pressure", -1.0), g.get("temperature", -1.0)
             u, v, w = g.get("u", 1.0), g.get("v", 0.0), g.get("w", 0.0)
-            c = math.sqrt(GAMMA * R_U / MW_AIR * t)
+            mw, gamma, y = MW_AIR, GAMMA, [0.0] * 16
+            if self.mixture:
+                tb = self.mixture["tables"]
+                yk = [float(g.get(n, 0.0)) for n in tb.names]
+                mw = 0.0
+                for i in range(tb.n_spec):
+                    mw += yk[i] / tb.mw[i]
+                mw = 1 / mw
+                cpi = species_cp(tb, t)
+                cp = cv = 0.0
+                for i in range(tb.n_spec):
+                    cp += yk[i] * cpi[i]
+                    cv += yk[i] * (cpi[i] - R_U / tb.mw[i])
+                gamma = cp / cv
+                y[:tb.n_spec] = yk
+            c = math.sqrt(gamma * R_U / mw * t)
             vel = mach * c
-            rho = p * MW_AIR / (R_U * t)
+            rho = p * mw / (R_U * t)
             out[g["label"]] = dict(density=rho, u=u * vel, v=v * vel, w=w * vel, pressure=p, temperature=t,
-                                   acoustic_speed=c, gamma=GAMMA, entropy=p / rho ** GAMMA, mw=MW_AIR)
+                                   acoustic_speed=c, gamma=gamma, entropy=p / rho ** gamma, mw=mw, y=y)
         return out
 
     def default_state(self):
@@ -759,8 +775,24 @@ def reacting_mixing_layer_3d(mx=384, my=192, mz=96, seed=0, steps=100, h=0.125, 
         faces = _box_faces(mx, my, mz, 8, 6, 6, 8)
         structs = {"periodic": {"type": ("string", "periodic"), "label": ("int", 8)},
                    "outflow": {"type": ("string", "outflow"), "label": ("int", 6)}}
+    elif ybc == "farfield":
+        # far-field (Riemann-invariant) y faces: the fuel stream above (u = +dU/2), the vitiated air below
+        # (u = -dU/2), each at its own temperature and composition and the uniform pressure
+        faces = _box_faces(mx, my, mz, 8, 41, 4, 8)
+        up = {"type": ("string", "farfield"), "label": ("int", 4), "mach": ("real", 0.5 * du / cf),
+              "pressure": ("real", p0), "temperature": ("real", tf), "u": ("real", 1.0), "v": ("real", 0.0),
+              "w": ("real", 0.0)}
+        lo = {"type": ("string", "farfield"), "label": ("int", 41), "mach": ("real", 0.5 * du / co),
+              "pressure": ("real", p0), "temperature": ("real", to), "u": ("real", -1.0), "v": ("real", 0.0),
+              "w": ("real", 0.0)}
+        for k, v in fuel.items():
+            up[k] = ("real", float(v))
+        for k, v in oxidiser.items():
+            lo[k] = ("real", float(v))
+        structs = {"periodic": {"type": ("string", "periodic"), "label": ("int", 8)},
+                   "farfield_upper": up, "farfield_lower": lo}
     else:
-        raise ValueError("the reacting case uses outflow or wall y faces")
+        raise ValueError("the reacting case uses outflow, wall or far-field y faces")
     if xbc == "inflow":
         _inflow_x(faces, structs, 1.2, p0, to, oxidiser)
     scheme = dict(reconstruction=2, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=0.5, prandtl_number=0.72,

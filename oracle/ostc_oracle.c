@@ -1866,10 +1866,98 @@ static void bc_periodic(orc_ctx *o, const face_t *f) {
 }
 
 /* apply_farfield<Air> (BoundCond.cuh:755-1022) */
+/* apply_farfield<mixture> (BoundCond.cuh:755-1022) at face node (i, j, k): gamma of the node, mixture
+ * molecular weight from its mass fractions; supersonic inflow / outflow as for air; subsonic: Riemann
+ * invariants, far-field (u_n < 0) or node velocity and composition, and a gamma iterated with cp of
+ * the face temperature until its relative change is below 1e-4 (entropy of the inflow branch for
+ * u_n <= 0, as the reference writes it). */
+static void farfield_mixture_node(orc_ctx *o, const face_t *f, int i, int j, int k, const int dir[3]) {
+  const long P = o->P;
+  const orc_chem *ch = o->c.chem;
+  const int ns = o->ns;
+  const long pb = ID(o, i, j, k);
+  double nx = o->met[(f->face * 3 + 0) * P + pb], ny = o->met[(f->face * 3 + 1) * P + pb],
+         nz = o->met[(f->face * 3 + 2) * P + pb];
+  const double gni = f->direction / sqrt(nx * nx + ny * ny + nz * nz);
+  nx *= gni;
+  ny *= gni;
+  nz *= gni;
+  const double ub = o->bv[P + pb], vb = o->bv[2 * P + pb], wb = o->bv[3 * P + pb];
+  const double uf = nx * ub + ny * vb + nz * wb;
+  double svb[ORC_MAX_SPEC];
+  for (int l = 0; l < ns; ++l) svb[l] = o->sv[l * P + pb];
+  const double gb = o->gam[pb];
+  double mw_inv = 0;
+  for (int l = 0; l < ns; ++l) mw_inv += svb[l] / ch->mw[l];
+  double mw = 1.0 / mw_inv;
+  const double pbv = o->bv[4 * P + pb], rb = o->bv[pb];
+  const double ab = sqrt(gb * pbv / rb);
+  const double mb = uf / ab;
+  double vals[6];
+  if (mb <= -1) {
+    vals[0] = f->density; vals[1] = f->u; vals[2] = f->v; vals[3] = f->w; vals[4] = f->pressure;
+    vals[5] = f->temperature;
+    for (int l = 0; l < ns; ++l) svb[l] = f->y[l];
+  } else if (mb >= 1) {
+    for (int g = 1; g <= o->g; ++g) {
+      const long pg = ID(o, i + g * dir[0], j + g * dir[1], k + g * dir[2]);
+      copy_node(o, pg, pb);
+      cv_from_bv(o, pg);
+    }
+    return;
+  } else {
+    const double rpos = uf + 2 * ab / (gb - 1);
+    const double uinf = f->u * nx + f->v * ny + f->w * nz;
+    const double rneg = uinf - 2 * f->acoustic_speed / (f->gamma - 1);
+    const double Un = 0.5 * (rpos + rneg);
+    if (mb < 0) {
+      vals[1] = f->u + (Un - uinf) * nx;
+      vals[2] = f->v + (Un - uinf) * ny;
+      vals[3] = f->w + (Un - uinf) * nz;
+      for (int l = 0; l < ns; ++l) svb[l] = f->y[l];
+      mw = f->mw;
+    } else {
+      vals[1] = ub + (Un - uf) * nx;
+      vals[2] = vb + (Un - uf) * ny;
+      vals[3] = wb + (Un - uf) * nz;
+    }
+    double gamma = GAMMA_AIR, err = 1, rho = 0, pr = 0, t = 0;
+    for (int it = 0; err > 1e-4 && it < 100; ++it) {
+      const double glast = gamma;
+      const double cb = 0.25 * (gamma - 1) * (rpos - rneg);
+      const double sb = mb <= 0 ? f->entropy : pbv / pow(rb, gamma);
+      rho = pow(cb * cb / (gamma * sb), 1 / (gamma - 1));
+      pr = rho * cb * cb / gamma;
+      t = pr * mw / (rho * R_U);
+      double h[ORC_MAX_SPEC], cp[ORC_MAX_SPEC];
+      mix_h_cp(ch, t, h, cp);
+      double cpt = 0;
+      for (int l = 0; l < ns; ++l) cpt += cp[l] * svb[l];
+      gamma = cpt / (cpt - R_U / mw);
+      err = fabs(1 - gamma / glast);
+    }
+    vals[0] = rho;
+    vals[4] = pr;
+    vals[5] = t;
+  }
+  for (int g = 0; g <= o->g; ++g) {
+    const long pg = ID(o, i + g * dir[0], j + g * dir[1], k + g * dir[2]);
+    for (int l = 0; l < 6; ++l) o->bv[l * P + pg] = vals[l];
+    for (int l = 0; l < ns; ++l) o->sv[l * P + pg] = svb[l];
+    cv_from_bv(o, pg);
+  }
+}
+
 static void bc_farfield(orc_ctx *o, const face_t *f) {
   const long P = o->P;
   int dir[3] = {0, 0, 0};
   dir[f->face] = f->direction;
+  if (o->ns) {
+    for (int i = f->rs[0]; i <= f->re[0]; ++i)
+      for (int j = f->rs[1]; j <= f->re[1]; ++j)
+        for (int k = f->rs[2]; k <= f->re[2]; ++k) farfield_mixture_node(o, f, i, j, k, dir);
+    return;
+  }
   for (int i = f->rs[0]; i <= f->re[0]; ++i)
     for (int j = f->rs[1]; j <= f->re[1]; ++j)
       for (int k = f->rs[2]; k <= f->re[2]; ++k) {

@@ -95,6 +95,10 @@ CASES = [
      dict(mx=32, my=20, mz=12, ybc="outflow", xbc="subsonic", ref_face=True), 10),
     ("rml3d_wall", "reacting_mixing_layer_3d", dict(mx=20, my=16, mz=10, ybc="wall"), 5),
     ("rml3d_inflow", "reacting_mixing_layer_3d", dict(mx=24, my=16, mz=10, xbc="inflow"), 5),
+    # far-field (Riemann-invariant) faces of a mixture: fuel stream above, vitiated air below
+    ("rml3d_farfield_fr72", "reacting_mixing_layer_3d", dict(mx=32, my=20, mz=16, ybc="farfield"), 10),
+    ("rml3d_farfield_mix71", "reacting_mixing_layer_3d",
+     dict(mx=32, my=20, mz=16, ybc="farfield", inviscid_scheme=71, finite_rate=False), 10),
     # the reference's steady driver (SteadySim.cuh): local time steps, explicit or DPLUR implicit
     # treatment (DPLUR.cuh), the chemical source explicit, point-implicit (EPI) or diagonal (DA).  No
     # wall case with DPLUR: the reference zeroes dq over the wall's ngg-padded range in an array with

@@ -18,6 +18,18 @@ import ostc_cases as oc
 HERE = Path(__file__).resolve().parent
 TOL = 1e-12
 TOL_T = 1e-13
+# Far-field faces of mixtures: the reference iterates the face gamma with cp of the face temperature
+# until its relative change is below 1e-4 (BoundCond.cuh:949-967), and the interior temperature by
+# Newton to a relative 1e-3 (FieldOperation.cu:3-40); where an iteration ends near its threshold, a
+# rounding-level difference changes the iteration count and moves the face state by up to ~1e-5.  The
+# oracle built with and without fused multiply-adds lands 2e-6 and 3e-6 (max) from the reference's
+# state on the same case, so these fixtures are compared at (max, L2, time) = (1e-5, 1e-6, 1e-9).
+LOOSE = {"rml3d_farfield_fr72": (1e-5, 1e-6, 1e-9), "rml3d_farfield_mix71": (1e-5, 1e-6, 1e-9)}
+
+
+def tolerances(name):
+    """(max, L2, physical time) relative bars of a fixture."""
+    return LOOSE.get(name, (TOL, TOL, TOL_T))
 
 # statistics collection in the reference's own setup keys (SinglePointStat, RK.cuh:200-207): collected
 # after every step past step 2, exported with the flow field when the run ends
@@ -101,19 +113,20 @@ def plane_errors(cv, z):
     return out
 
 
-def assert_state(cv, z, block=None):
+def assert_state(cv, z, block=None, tol=(TOL, TOL)):
+    tm, tl = tol[0], tol[1]
     if block is not None:
         err = oc.relative_errors(cv, z[f"cv_{block}"])
-        assert all(m < TOL and l2 < TOL for m, l2 in err), (block, err)
+        assert all(m < tm and l2 < tl for m, l2 in err), (block, err)
         return
     if "sampled" in z.files:
         err = sampled_errors(cv, z)
-        assert all(m < TOL and l2 < TOL for m, l2 in err), err
+        assert all(m < tm and l2 < tl for m, l2 in err), err
         pe = plane_errors(cv, z)
-        assert all(e < TOL for e in pe), pe
+        assert all(e < tm for e in pe), pe
         return
     err = oc.relative_errors(cv, z["cv"])
-    assert all(m < TOL and l2 < TOL for m, l2 in err), err
+    assert all(m < tm and l2 < tl for m, l2 in err), err
 
 
 def run_library(case, steps, directory, setup_extra=""):
@@ -140,18 +153,20 @@ def run_library(case, steps, directory, setup_extra=""):
     return s
 
 
-def check_library(case, steps, z, t_ref, directory, setup_extra=""):
-    """Runs the library and checks its state and time against the fixture; returns the solver."""
+def check_library(case, steps, z, t_ref, directory, setup_extra="", name=None):
+    """Runs the library and checks its state and time against the fixture (bars: tolerances(name));
+    returns the solver."""
+    tm, tl, tt = tolerances(name)
     s = run_library(case, steps, directory, setup_extra)
     if hasattr(case, "blocks"):
         for b in range(int(z["n_block"])):
-            assert_state(s.get_state(block=b)[0], z, block=b)
+            assert_state(s.get_state(block=b)[0], z, block=b, tol=(tm, tl))
     else:
-        assert_state(s.get_state()[0], z)
+        assert_state(s.get_state()[0], z, tol=(tm, tl))
     if case.scheme.get("temporal_scheme", 3) == 2 and not case.scheme.get("steady"):
         # the reference's dual-time driver advances its physical time without storing it in its
         # solution_time parameter (DualTimeStepping.cuh:172), which the fixture records: it is steps dt
         t_ref = steps * case.scheme["dt"]
-    assert abs(s.time() - t_ref) <= TOL_T * t_ref
+    assert abs(s.time() - t_ref) <= tt * t_ref
     assert s.error_flags() == 0
     return s

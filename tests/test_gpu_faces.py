@@ -121,11 +121,12 @@ def test_characteristic_faces_refuse_mixtures(built, tmp_path):
 
 # ---- the same faces against the reference's own FP64 build (fixtures from tests/golden/make_golden.py:
 # the reference's Driver + RK3 with its apply_wall / apply_inflow / apply_subsonic_inflow /
-# apply_back_pressure, BoundCond.cuh:235-613,1024-1441)
+# apply_back_pressure, BoundCond.cuh:235-613,1024-1441), and far-field faces of mixtures (apply_farfield,
+# BoundCond.cuh:755-1022)
 
 REFERENCE_FACE_CASES = ["ml3d_wall_isothermal", "ml3d_wall_adiabatic", "ml2d_wall_isothermal_weno5",
                         "ml2d_wall_adiabatic_weno7", "ml3d_inflow_outflow", "ml3d_subsonic_backpressure", "rml3d_wall",
-                        "rml3d_inflow"]
+                        "rml3d_inflow", "rml3d_farfield_fr72", "rml3d_farfield_mix71"]
 
 
 @pytest.mark.parametrize("name", REFERENCE_FACE_CASES)
@@ -133,4 +134,4 @@ def test_faces_match_reference_build(built, tmp_path, name):
     import golden_util as gu
 
     case, steps, z, t_ref = gu.load(gu.fixture_path(name))
-    gu.check_library(case, steps, z, t_ref, tmp_path / name).close()
+    gu.check_library(case, steps, z, t_ref, tmp_path / name, name=name).close()
