@@ -162,6 +162,21 @@ int ostc_run_states(ostc_ctx *ctx, int n, const double *const *bv_in, const doub
  * stream: *ms receives the device time of the n_steps steps.  Synchronises. */
 int ostc_timed_steps(ostc_ctx *ctx, int n_steps, double *ms);
 
+/* How ostc_rk3_step and ostc_timed_steps issue a step.  OSTC_LAUNCH_GRAPH (the default): one CUDA
+ * graph per step, captured on first use, with the blocks' stage work forked onto side streams inside
+ * it.  OSTC_LAUNCH_BLOCK_LOOP: the reference's per-block launch loop (RK.cuh:112-174) - every kernel
+ * launched from the host in turn, block after block, on the context stream - for comparison and
+ * debugging.  Both compute the same results bit for bit. */
+#define OSTC_LAUNCH_GRAPH 0
+#define OSTC_LAUNCH_BLOCK_LOOP 1
+int ostc_set_launch_mode(ostc_ctx *ctx, int mode);
+
+/* Seed of the white-noise inflow (an inflow struct with fluctuation_type 1): generator state i of the
+ * face plane restarts from curand_init(seed + i, i, 0), as the reference's initialize_rng does with the
+ * clock (BoundCond.cu:1384-1391, 1731-1735); ostc_create seeds it from the clock too.  A case run with
+ * the seed the reference drew reproduces its inflow noise.  No effect without such a face. */
+int ostc_set_inflow_seed(ostc_ctx *ctx, long long seed);
+
 /* Number of kernels one step launches (kernel nodes of the captured step graph). */
 int ostc_step_kernel_count(ostc_ctx *ctx, int *n_kernels);
 

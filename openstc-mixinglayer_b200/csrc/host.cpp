@@ -237,6 +237,15 @@ bool derive(const Setup &s, Derived &d, std::string &err) {
   d.n_scalar = 0;
   d.n_var = 5;
   d.reaction = s.get_int("reaction");
+  d.problem_type = s.get_int("problem_type");
+  if (d.problem_type != 0 && d.problem_type != 1) {
+    err = "problem_type must be 0 (general) or 1 (mixing layer); got " + std::to_string(d.problem_type);
+    return false;
+  }
+  if (d.problem_type == 1 && s.get_bool("compatible_mixing_layer")) {
+    err = "compatible_mixing_layer = 1 (inflow and initial field from a profile file) is not provided";
+    return false;
+  }
   if (d.species != 0 && d.species != 1) {
     err = "species = " + std::to_string(d.species) + " (mixture-fraction / flamelet models) is not on this library's path";
     return false;
@@ -290,8 +299,15 @@ bool derive(const Setup &s, Derived &d, std::string &err) {
           " is not supported (reference reads outside its stencil); use 71 or, for mixtures, 72";
     return false;
   }
-  if (d.species == 1 && d.inviscid_type != 3) {
-    err = "for mixtures this library implements the flux-split WENO7 path (inviscid_scheme 71 or 72)";
+  if (d.species == 1 && d.inviscid_type == 1) {
+    // the reference's mixture AWENO_interpolation and CDSPart1D are empty stubs (AWENO.cu:8-13, 282-285)
+    err = "AWENO (reconstruction 4 / 5) is not defined for mixtures in the reference; use the flux-split WENO "
+          "(inviscid_scheme 71 / 72) or a primitive reconstruction (1-3) with AUSM+, HLLC or Roe";
+    return false;
+  }
+  if (d.species == 1 && (d.inviscid_type == 0 || d.inviscid_type == 2) && is == 1) {
+    err = "Lax-Friedrichs (inviscid_scheme 1) has no mixture form in the reference (riemannSolver_laxFriedrich<mixture> "
+          "only prints, RiemannSolver.cuh:419-424); use AUSM+ (3), HLLC (4) or Roe (2)";
     return false;
   }
   if (d.inviscid_type == 0 || d.inviscid_type == 2) {
@@ -803,6 +819,23 @@ double struct_real(const std::map<std::string, Setup::StructVal> &st, const char
   return def;
 }
 double sutherland_host(double t) { return 1.7894e-5 * std::pow(t / 288.16, 1.5) * (288.16 + 110) / (t + 110); }
+
+// Species::compute_cp (ChemData.cpp:126-149): mass-specific cp of every species, frozen at t_low below it
+void species_cp(const ChemTables &chem, double t, double *cp) {
+  const double t2 = t * t, t3 = t2 * t, t4 = t3 * t;
+  for (int i = 0; i < chem.n_spec; ++i) {
+    double cc;
+    if (t < chem.t_low[i]) {
+      const double tt = chem.t_low[i], tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt;
+      const double *a = &chem.low[i * 7];
+      cc = a[0] + a[1] * tt + a[2] * tt2 + a[3] * tt3 + a[4] * tt4;
+    } else {
+      const double *a = t < chem.t_mid[i] ? &chem.low[i * 7] : &chem.high[i * 7];
+      cc = a[0] + a[1] * t + a[2] * t2 + a[3] * t3 + a[4] * t4;
+    }
+    cp[i] = cc * (kRu / chem.mw[i]);
+  }
+}
 }  // namespace
 
 // State of a plain inflow struct (Inflow::Inflow, BoundCond.cpp:157-214): density from p, T and the
@@ -831,22 +864,12 @@ bool inflow_state(const Setup &s, const std::string &name, const ChemTables *che
     mw = 0;
     for (int i = 0; i < chem->n_spec; ++i) mw += y[i] / chem->mw[i];
     mw = 1 / mw;
-    // Species::compute_cp (ChemData.cpp:148-171): cp frozen at t_low below it
-    const double t = temperature, t2 = t * t, t3 = t2 * t, t4 = t3 * t;
+    for (int i = 0; i < chem->n_spec; ++i) cp[i] = 0;
+    species_cp(*chem, temperature, cp.data());
     double cpt = 0, cvt = 0;
     for (int i = 0; i < chem->n_spec; ++i) {
-      double cc;
-      if (t < chem->t_low[i]) {
-        const double tt = chem->t_low[i], tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt;
-        const double *a = &chem->low[i * 7];
-        cc = a[0] + a[1] * tt + a[2] * tt2 + a[3] * tt3 + a[4] * tt4;
-      } else {
-        const double *a = t < chem->t_mid[i] ? &chem->low[i * 7] : &chem->high[i * 7];
-        cc = a[0] + a[1] * t + a[2] * t2 + a[3] * t3 + a[4] * t4;
-      }
-      cc *= kRu / chem->mw[i];
-      cpt += y[i] * cc;
-      cvt += y[i] * (cc - kRu / chem->mw[i]);
+      cpt += y[i] * cp[i];
+      cvt += y[i] * (cp[i] - kRu / chem->mw[i]);
     }
     gamma = cpt / cvt;
   }
@@ -862,9 +885,121 @@ bool inflow_state(const Setup &s, const std::string &name, const ChemTables *che
   return true;
 }
 
+bool mixing_layer_streams(const Setup &s, const ChemTables *chem, MixingLayerStreams &m, std::string &err) {
+  auto up = s.structs.find("upper_stream"), lo = s.structs.find("lower_stream");
+  if (up == s.structs.end() || lo == s.structs.end()) {
+    err = "a mixing-layer problem (problem_type = 1) needs the structs upper_stream and lower_stream";
+    return false;
+  }
+  for (const char *k : {"ma_c", "velocity_ratio", "delta_omega"})
+    if (!s.reals.count(k)) {
+      err = std::string("a mixing-layer problem (problem_type = 1) needs the real ") + k;
+      return false;
+    }
+  const auto &U = up->second, &L = lo->second;
+  for (const auto *st : {&U, &L})
+    for (const char *k : {"temperature", "pressure"})
+      if (!st->count(k)) {
+        err = std::string("upper_stream / lower_stream need ") + k;
+        return false;
+      }
+  const double ma_c = s.get_real("ma_c"), vel_ratio = s.get_real("velocity_ratio");
+  const bool upper_faster = s.get_bool("upper_faster");
+  double ma_upper = struct_real(U, "mach", -1), ma_lower = struct_real(L, "mach", -1);
+  const double t_upper = struct_real(U, "temperature", 0), t_lower = struct_real(L, "temperature", 0);
+  const double p_upper = struct_real(U, "pressure", 0), p_lower = struct_real(L, "pressure", 0);
+  double rho_upper, rho_lower, c_upper, c_lower;
+  const int ns = chem ? chem->n_spec : 0;
+  m.y_upper.assign(ns, 0.0);
+  m.y_lower.assign(ns, 0.0);
+  if (ns > 0) {
+    for (int i = 0; i < ns; ++i) {
+      m.y_upper[i] = struct_real(U, chem->names[i].c_str(), 0.0);
+      m.y_lower[i] = struct_real(L, chem->names[i].c_str(), 0.0);
+    }
+    std::vector<double> cpu(ns), cpl(ns);
+    species_cp(*chem, t_upper, cpu.data());
+    species_cp(*chem, t_lower, cpl.data());
+    double mwi_u = 0, mwi_l = 0, cp_u = 0, cp_l = 0;
+    for (int i = 0; i < ns; ++i) {
+      mwi_u += m.y_upper[i] / chem->mw[i];
+      mwi_l += m.y_lower[i] / chem->mw[i];
+      cp_u += cpu[i] * m.y_upper[i];
+      cp_l += cpl[i] * m.y_lower[i];
+    }
+    const double g_u = cp_u / (cp_u - kRu * mwi_u), g_l = cp_l / (cp_l - kRu * mwi_l);
+    c_upper = std::sqrt(g_u * kRu * mwi_u * t_upper);
+    c_lower = std::sqrt(g_l * kRu * mwi_l * t_lower);
+    rho_upper = p_upper / (kRu * mwi_u * t_upper);
+    rho_lower = p_lower / (kRu * mwi_l * t_lower);
+  } else {
+    c_upper = std::sqrt(kGammaAir * kRu / kMwAir * t_upper);
+    c_lower = std::sqrt(kGammaAir * kRu / kMwAir * t_lower);
+    rho_upper = p_upper * kMwAir / (kRu * t_upper);
+    rho_lower = p_lower * kMwAir / (kRu * t_lower);
+  }
+  // the stream Mach numbers from the velocity ratio, or from one given Mach number and Ma_c
+  if (vel_ratio > 0) {
+    double u_slow, u_fast;
+    if (vel_ratio > 1) {
+      u_slow = ma_c * (c_upper + c_lower) / (vel_ratio - 1);
+      u_fast = vel_ratio * u_slow;
+    } else {
+      u_fast = ma_c * (c_upper + c_lower) / (1 - vel_ratio);
+      u_slow = u_fast * vel_ratio;
+    }
+    ma_upper = (upper_faster ? u_fast : u_slow) / c_upper;
+    ma_lower = (upper_faster ? u_slow : u_fast) / c_lower;
+  } else if (ma_upper < 0 && ma_lower < 0) {
+    err = "a mixing-layer problem needs velocity_ratio > 0 or a stream Mach number";
+    return false;
+  } else if (ma_upper > 0 && ma_lower > 0) {
+    // both given: the given streams are used as they are
+  } else if (ma_upper > 0) {
+    ma_lower = upper_faster ? (ma_upper - ma_c) * c_upper / c_lower - ma_c : (ma_c + ma_upper) * c_upper / c_lower + ma_c;
+  } else {
+    ma_upper = upper_faster ? (ma_c + ma_lower) * c_lower / c_upper + ma_c : (ma_lower - ma_c) * c_lower / c_upper - ma_c;
+  }
+  const double u_upper = ma_upper * c_upper, u_lower = ma_lower * c_lower;
+  const double a[6] = {rho_upper, u_upper, 0, 0, p_upper, t_upper}, b[6] = {rho_lower, u_lower, 0, 0, p_lower, t_lower};
+  for (int l = 0; l < 6; ++l) {
+    m.upper[l] = a[l];
+    m.lower[l] = b[l];
+  }
+  m.delta_omega = s.get_real("delta_omega");
+  return true;
+}
+
 bool reference_scales(const Setup &s, const ChemTables *chem, double &eps_scale, double &v_ref, std::string &err) {
   eps_scale = 0;
   v_ref = 0;
+  if (s.get_int("problem_type") == 1) {
+    // a mixing-layer problem: the inflow struct named by reference_state carries the upper stream
+    // (Inflow ctor, BoundCond.cpp:28-62, 299-305)
+    MixingLayerStreams m;
+    if (!mixing_layer_streams(s, chem, m, err)) return false;
+    const double *u = m.upper;
+    double vel = std::sqrt(u[1] * u[1] + u[2] * u[2] + u[3] * u[3]);
+    if (std::abs(vel) < 1) {
+      double mw = kMwAir, gamma = kGammaAir;
+      if (chem && chem->n_spec > 0) {
+        std::vector<double> cp(chem->n_spec);
+        species_cp(*chem, u[5], cp.data());
+        double mwi = 0, cpt = 0, cvt = 0;
+        for (int i = 0; i < chem->n_spec; ++i) {
+          mwi += m.y_upper[i] / chem->mw[i];
+          cpt += m.y_upper[i] * cp[i];
+          cvt += m.y_upper[i] * (cp[i] - kRu / chem->mw[i]);
+        }
+        mw = 1 / mwi;
+        gamma = cpt / cvt;
+      }
+      vel = std::sqrt(gamma * kRu / mw * u[5]);
+    }
+    v_ref = vel;
+    eps_scale = u[0] * v_ref * u[0] * v_ref;
+    return true;
+  }
   auto rs = s.strings.find("reference_state");
   if (rs == s.strings.end()) return true;
   double bv[6], c;
@@ -940,21 +1075,37 @@ bool resolve_boundaries(const Setup &s, const Derived &d, HostMesh &mesh, std::s
         continue;
       }
       if (f.type == kInflow) {
-        // apply_inflow with a constant state (BoundCond.cuh:483-613, inflow_type 0, no fluctuation):
-        // profile, digital-filter and fluctuating inflows are not on this path
+        // apply_inflow (BoundCond.cuh:235-613): a constant state (inflow_type 0) or, in a mixing-layer
+        // problem, the two-stream tanh profile (inflow_type 2, forced by problem_type 1; Inflow ctor
+        // BoundCond.cpp:10-21), either with optional white noise on the velocity (fluctuation_type 1).
+        // Profile-file inflows (1), stability-mode and receptivity fluctuations (2, 3) and the digital
+        // filter (11) are not on this path.
         if (it == lab.end()) {
           err = "inflow label " + std::to_string(f.label) + " needs a struct in boundary_conditions";
           return false;
         }
         const auto &st = s.structs.at(it->second.second);
-        for (const char *k : {"inflow_type", "fluctuation_type"}) {
+        auto get_int = [&](const char *k) {
           auto q = st.find(k);
-          if (q != st.end() && std::holds_alternative<int>(q->second) && std::get<int>(q->second) != 0) {
-            err = "inflow label " + std::to_string(f.label) + ": " + k +
-                  " != 0 (profile / fluctuating inflow) is not provided; constant inflow is";
-            return false;
-          }
+          return q != st.end() && std::holds_alternative<int>(q->second) ? std::get<int>(q->second) : 0;
+        };
+        int itype = get_int("inflow_type"), ftype = get_int("fluctuation_type");
+        if (d.problem_type == 1) itype = 2;
+        if (d.problem_type == 0 && itype == 2) itype = 0;
+        if (itype != 2 && ftype == 11) ftype = 0;
+        if (itype != 0 && itype != 2) {
+          err = "inflow label " + std::to_string(f.label) + ": inflow_type " + std::to_string(itype) +
+                " (profile file) is not provided; constant (0) and mixing-layer (problem_type 1) inflows are";
+          return false;
         }
+        if (ftype != 0 && ftype != 1) {
+          err = "inflow label " + std::to_string(f.label) + ": fluctuation_type " + std::to_string(ftype) +
+                " is not provided (stability-mode, receptivity and digital-filter fluctuations); white noise (1) is";
+          return false;
+        }
+        f.inflow_type = itype;
+        f.fluctuation_type = ftype;
+        f.fluct_intensity = ftype == 1 ? struct_real(st, "fluctuation_intensity", 0.0) : 0.0;
         f.struct_name = it->second.second;
         continue;
       }
@@ -1094,6 +1245,24 @@ bool resolve_inflows(const Setup &s, const ChemTables *chem, HostMesh &mesh, std
         continue;
       }
       if (f.type != kInflow) continue;
+      if (f.inflow_type == 2) {
+        // the mixing-layer inflow (Inflow ctor, BoundCond.cpp:28-98): the upper stream in the face's
+        // constant-state members, the lower stream beside it
+        MixingLayerStreams m;
+        if (!mixing_layer_streams(s, chem, m, err)) return false;
+        f.density = m.upper[0];
+        f.u = m.upper[1];
+        f.v = m.upper[2];
+        f.w = m.upper[3];
+        f.pressure = m.upper[4];
+        f.temperature = m.upper[5];
+        f.velocity = std::sqrt(f.u * f.u + f.v * f.v + f.w * f.w);
+        f.y = m.y_upper;
+        for (int l = 0; l < 6; ++l) f.lower[l] = m.lower[l];
+        f.y_lower = m.y_lower;
+        f.delta_omega = m.delta_omega;
+        continue;
+      }
       double bv[6], c;
       if (!inflow_state(s, f.struct_name, chem, bv, f.y, c, err)) return false;
       f.density = bv[0];
@@ -1102,6 +1271,8 @@ bool resolve_inflows(const Setup &s, const ChemTables *chem, HostMesh &mesh, std
       f.w = bv[3];
       f.pressure = bv[4];
       f.temperature = bv[5];
+      // the Inflow's velocity member: Mach times the speed of sound (BoundCond.cpp:217-223)
+      f.velocity = struct_real(s.structs.at(f.struct_name), "mach", -1) * c;
     }
   return true;
 }

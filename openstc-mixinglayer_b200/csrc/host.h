@@ -76,6 +76,7 @@ struct Derived {
   double grid_scale = 1.0;
   int species = 0;
   int reaction = 0;
+  int problem_type = 0;  // 0 general, 1 mixing layer (inflows take the two-stream profile)
 };
 
 bool derive(const Setup &s, Derived &d, std::string &err);
@@ -99,7 +100,26 @@ struct BcFace {
   // mixtures, its mass fractions (filled once the species tables are known)
   std::string struct_name;
   std::vector<double> y;
+  // inflow kind (Inflow ctor, BoundCond.cpp:10-21): 0 constant, 2 mixing-layer profile (every inflow
+  // of a problem_type 1 case); fluctuation_type 1 adds white noise of relative intensity
+  // fluct_intensity to the velocity (apply_inflow, BoundCond.cuh:402-425, 500-521); velocity is the
+  // Inflow's `velocity` member (the constant inflow scales its noise by it)
+  int inflow_type = 0, fluctuation_type = 0;
+  double fluct_intensity = 0, velocity = 0, delta_omega = 0;
+  // mixing-layer profile: the lower stream (rho, u, v, w, p, T) and its mass fractions; the upper
+  // stream is density .. temperature and y above
+  double lower[6]{};
+  std::vector<double> y_lower;
 };
+
+// The two streams of a mixing-layer problem (get_mixing_layer_info, MixingLayer.cu:9-191): rho, u, v,
+// w, p, T of the upper and lower stream and their mass fractions (mixtures).
+struct MixingLayerStreams {
+  double upper[6]{}, lower[6]{};
+  std::vector<double> y_upper, y_lower;
+  double delta_omega = 0;
+};
+bool mixing_layer_streams(const Setup &s, const ChemTables *chem, MixingLayerStreams &m, std::string &err);
 
 
 // One 1:1 block interface after InnerFace::register_boundary (Mesh.cpp:34-176): the node range of

@@ -17,6 +17,7 @@
 #include "ostc.h"
 
 #include <cuda_runtime.h>
+#include <curand_kernel.h>
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
@@ -27,6 +28,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <ctime>
 #include <memory>
 #include <string>
 #include <type_traits>
@@ -79,11 +81,47 @@ struct DevFace {
   double density, u, v, w, pressure, temperature, acoustic_speed, gamma, entropy, mw;
   int wall_adiabatic;  // walls: 1 adiabatic, 0 isothermal at `temperature`
   double y[16];        // inflow mass fractions (mixtures)
+  // inflows: 0 constant / 2 mixing-layer profile (upper stream above, `lower` below, blended in u by
+  // tanh(2 y / delta_omega)); fluct 1 adds white noise of relative intensity fluct_rms, drawn from
+  // rng[] at the face node's index in a plane of rng_row nodes per row (apply_inflow's indexing)
+  int inflow_type, fluct, rng_row;
+  double fluct_rms, velocity, delta_omega;
+  double lower[6], y_lower[16];
+  const double *ycoord;  // mixing-layer inflow: y of every face node, in the kernel's enumeration
+  curandState *rng;
 };
 
 struct FillVals {
   double val[16];
 };
+
+// The two streams of a mixing-layer problem, for the initial profile.
+struct MlVals {
+  double upper[6], lower[6], y_upper[16], y_lower[16], delta_omega;
+};
+
+// initialize_mixing_layer_with_info (Initialize.cu:259-326), laminar: every padded node takes the upper
+// or the lower stream by the sign of its y, with u blended by tanh(2 y / delta_omega).
+__global__ void k_fill_mixing_layer(long long plane, const double *__restrict__ ycoord, double *__restrict__ bv,
+                                    double *__restrict__ sv, int ns, MlVals m) {
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < plane; p += (long long)gridDim.x * blockDim.x) {
+    const double y = ycoord[p];
+    const double *st = y >= 0 ? m.upper : m.lower, *ys = y >= 0 ? m.y_upper : m.y_lower;
+    bv[plane + p] = 0.5 * (m.upper[1] + m.lower[1]) + 0.5 * (m.upper[1] - m.lower[1]) * tanh(2 * y / m.delta_omega);
+    bv[p] = st[0];
+    bv[2 * plane + p] = st[2];
+    bv[3 * plane + p] = st[3];
+    bv[4 * plane + p] = st[4];
+    bv[5 * plane + p] = st[5];
+    for (int l = 0; l < ns; ++l) sv[l * plane + p] = ys[l];
+  }
+}
+
+// initialize_rng (BoundCond.cu:1384-1391): generator state i seeded with seed + i, subsequence i
+__global__ void k_rng_init(curandState *st, long long n, unsigned long long seed) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    curand_init(seed + (unsigned long long)i, (unsigned long long)i, 0, &st[i]);
+}
 
 // One block interface (InnerFace after register_boundary, Mesh.cpp:38-141).
 struct DevInner {
@@ -112,6 +150,7 @@ __device__ __forceinline__ void cv_from_bv_node(const DevBlock &b, DevState s, l
 #include "ostc_adj.cuh"
 #include "ostc_stat.cuh"
 #include "ostc_steady.cuh"
+#include "pv_mix.cuh"
 
 static_assert(ostc::kMS <= 16, "DevFace::y holds the inflow mass fractions of at most 16 species");
 
@@ -1058,18 +1097,47 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
         finish_node(b, s, pg);
       }
     } else if (f.type == kInflow) {
-      // apply_inflow, constant state (BoundCond.cuh:483-613): the face node and every ghost layer
-      // take the inflow struct's state
+      // apply_inflow (BoundCond.cuh:235-613): the face node and every ghost layer take one state -
+      // the constant one, or the mixing-layer profile at the face node's y - with the white noise of
+      // fluctuation_type 1 added to its velocity
+      double rho = f.density, u = f.u, v = f.v, w = f.w, pr = f.pressure, tt = f.temperature;
+      const double *ys = f.y;
+      double vel = f.velocity;
+      bool noisy = f.fluct == 1;
+      if (f.inflow_type == 2) {
+        const double yc = f.ycoord[n];
+        u = 0.5 * (f.u + f.lower[1]) + 0.5 * (f.u - f.lower[1]) * tanh(2 * yc / f.delta_omega);
+        if (yc < 0) {
+          rho = f.lower[0];
+          v = f.lower[2];
+          w = f.lower[3];
+          pr = f.lower[4];
+          tt = f.lower[5];
+          ys = f.y_lower;
+        }
+        vel = sqrt(u * u + v * v + w * w);
+        // the noise is confined to |y| < 4 delta_omega (BoundCond.cuh:406)
+        noisy = noisy && yc < 4 * f.delta_omega && yc > -4 * f.delta_omega;
+      }
+      if (noisy) {
+        // one generator state per node of the face plane, ghost-padded by ngg (BoundCond.cuh:406-420)
+        const int a = f.face == 0 ? idx[1] : idx[0], c2 = f.face == 2 ? idx[1] : idx[2];
+        curandState *st = f.rng + ((long long)(c2 + b.g) * f.rng_row + (a + b.g));
+        curandState local = *st;
+        u += curand_normal_double(&local) * f.fluct_rms * vel;
+        if (f.inflow_type == 2) v += curand_normal_double(&local) * f.fluct_rms * vel;
+        *st = local;
+      }
       for (int g = 0; g <= b.g; ++g) {
         const long long pg = pb + g * dstep;
-        s.bv[pg] = f.density;
-        s.bv[P + pg] = f.u;
-        s.bv[2 * P + pg] = f.v;
-        s.bv[3 * P + pg] = f.w;
-        s.bv[4 * P + pg] = f.pressure;
-        s.bv[5 * P + pg] = f.temperature;
+        s.bv[pg] = rho;
+        s.bv[P + pg] = u;
+        s.bv[2 * P + pg] = v;
+        s.bv[3 * P + pg] = w;
+        s.bv[4 * P + pg] = pr;
+        s.bv[5 * P + pg] = tt;
         if (s.sv)
-          for (int l = 0; l < c_mix.ns; ++l) s.sv[l * P + pg] = f.y[l];
+          for (int l = 0; l < c_mix.ns; ++l) s.sv[l * P + pg] = ys[l];
         finish_node(b, s, pg);
       }
     } else if (f.type == kBackPressure || f.type == kSubsonicInflow) {
@@ -1484,6 +1552,8 @@ struct BlockRes {
   double *dq = nullptr;
   double *last = nullptr;
   std::vector<DevFace> faces;  // file order
+  std::vector<double *> face_y;  // per face: y of its nodes (mixing-layer inflows), else null
+  double *ycoord = nullptr;      // problem_type 1: y of every padded node (the initial profile)
   std::vector<DevInner> inner;  // interfaces of this block, file order
   int yz_var[2][2] = {{-1, -1}, {-1, -1}};  // autotuned y / z sweep variant [FP64, mixed][y, z]
   int x_var[2] = {-1, -1};                   // autotuned x sweep variant [FP64, mixed]
@@ -1499,6 +1569,9 @@ struct BlockRes {
   double *dtl = nullptr, *srad = nullptr, *cj = nullptr, *dq0 = nullptr, *dqk = nullptr;
   // dual time stepping: the previous physical step's cv (padded planes) and the BDF2 source q* (interior)
   double *qn1 = nullptr, *qstar = nullptr;
+  // mixtures on the primitive-reconstruction path (pv_mix.cuh): face fluxes of one sweep, entropy-fix
+  // thresholds (padded)
+  double *fcb = nullptr, *efd = nullptr;
 };
 
 struct ostc_ctx {
@@ -1539,6 +1612,13 @@ struct ostc_ctx {
   unsigned *d_flags = nullptr;
   cudaGraphExec_t graph = nullptr;
   int graph_precision = -1;
+  int launch_mode = OSTC_LAUNCH_GRAPH;
+  // white-noise inflow: one generator state per node of the largest fluctuating face plane, shared by
+  // the faces as the reference shares one array (BoundCond.cu:1706-1735); seeded by ostc_set_inflow_seed
+  curandState *rng = nullptr;
+  long long rng_size = 0;
+  // problem_type 1: the two streams of the initial mixing-layer profile
+  MixingLayerStreams ml;
   bool tuned[2] = {false, false};  // x / y / z sweep autotuning done [FP64, mixed]
   int forced[2][3] = {{-1, -1, -1}, {-1, -1, -1}};  // sweep variants pinned by ostc_set_sweep_variant
   int graph_kernels = 0;
@@ -1744,6 +1824,40 @@ void launch_mix_visc(ostc_ctx *ctx, BlockRes &B, DevState in) {
   if (ctx->der.n_spec == kFixedNS)
     f32 ? launch_mix_visc_t<kFixedNS, float>(ctx, B, in) : launch_mix_visc_t<kFixedNS, double>(ctx, B, in);
   else f32 ? launch_mix_visc_t<0, float>(ctx, B, in) : launch_mix_visc_t<0, double>(ctx, B, in);
+}
+
+// Inviscid sweeps of a mixture: flux-split WENO (inviscid_scheme 71 / 72) or the primitive
+// reconstruction with AUSM+ / HLLC / Roe (pv_mix.cuh), accumulated into dq.
+template <int NS>
+void launch_pv_mix_t(ostc_ctx *ctx, BlockRes &B, DevState in) {
+  const DevBlock &b = B.db;
+  const int nv = ctx->nv, recon = ctx->der.reconstruction, rs = ctx->der.riemann;
+  if (rs == 2) {
+    const long long pts = (long long)(b.mx + 2) * (b.my + 2) * (b.mz > 1 ? b.mz + 2 : 1);
+    k_efix_mix<<<grid_for(ctx, pts, 128), 128, 0, ctx->stream>>>(b, in, ctx->der.entropy_fix_factor, B.efd);
+  }
+  const int gn = grid_for(ctx, b.n, 128);
+#define OSTC_PVM(D)                                                                                                 \
+  k_pv_mix_face<NS, D><<<grid_for(ctx, pv_face_count<D>(b), 128), 128, 0, ctx->stream>>>(b, in, nv, recon, rs, B.efd, \
+                                                                                        B.fcb);                     \
+  k_pv_mix_diff<D><<<gn, 128, 0, ctx->stream>>>(b, nv, B.fcb, B.dq);
+  OSTC_PVM(0)
+  OSTC_PVM(1)
+  if (b.mz > 1) {
+    OSTC_PVM(2)
+  }
+#undef OSTC_PVM
+}
+
+void launch_mix_inviscid(ostc_ctx *ctx, BlockRes &B, DevState in) {
+  if (ctx->der.inviscid_type == 3) {
+    launch_fvs(ctx, B, in);
+    return;
+  }
+  long tok = begin_t(ctx, "pv_mix");
+  if (ctx->der.n_spec == kFixedNS) launch_pv_mix_t<kFixedNS>(ctx, B, in);
+  else launch_pv_mix_t<0>(ctx, B, in);
+  end_t(ctx, tok);
 }
 template <int NS>
 void launch_mix_source_t(ostc_ctx *ctx, BlockRes &B, DevState in, bool chem) {
@@ -2152,7 +2266,7 @@ int initialise(ostc_ctx *ctx) {
 template <class F>
 void for_blocks(ostc_ctx *ctx, F f) {
   const size_t nb = ctx->blk.size();
-  if (nb == 1 || ctx->timing || ctx->side.empty()) {
+  if (nb == 1 || ctx->timing || ctx->side.empty() || ctx->launch_mode == OSTC_LAUNCH_BLOCK_LOOP) {
     for (size_t b = 0; b < nb; ++b) f((int)b);
     return;
   }
@@ -2238,7 +2352,7 @@ void enqueue_mix_stage(ostc_ctx *ctx, int rk, int sout_override = -1) {
       launch_mix_source(ctx, B, in, chem && !implicit);
       end_t(ctx, tok);
     }
-    launch_fvs(ctx, B, in);
+    launch_mix_inviscid(ctx, B, in);
     if (ctx->der.viscous_order != 0) launch_mix_visc(ctx, B, in);
     if (implicit) launch_chem_epi(ctx, B, in);
     {
@@ -2278,6 +2392,10 @@ int enqueue_step_mix(ostc_ctx *ctx) {
 int adjoint_check(ostc_ctx *ctx, unsigned mask) {
   if (!ctx->mixture) {
     ctx->err = "the adjoint covers the multi-component path (species = 1)";
+    return OSTC_EINVAL;
+  }
+  if ((mask & OSTC_TERM_INVISCID) && ctx->der.inviscid_type != 3) {
+    ctx->err = "the adjoint's inviscid term is the flux-split WENO (inviscid_scheme 71 / 72)";
     return OSTC_EINVAL;
   }
   if ((mask & OSTC_TERM_SOURCE) && ctx->der.reaction == 1 && ctx->chem_mode == OSTC_CHEM_POINT_IMPLICIT) {
@@ -2438,7 +2556,21 @@ int enqueue_step_any(ostc_ctx *ctx) {
 // arrays bv[6][N] (and sv[n_spec][N]); ghost nodes start from the default initialisation (or zero)
 // and are rewritten by the boundary faces and interfaces when the context next initialises.
 void enqueue_set_state(ostc_ctx *ctx, BlockRes &B, const double *bv, const double *sv) {
-  if (ctx->has_init) {
+  const bool ml = ctx->der.problem_type == 1 && B.ycoord;
+  if (ml) {
+    MlVals m{};
+    for (int l = 0; l < 6; ++l) {
+      m.upper[l] = ctx->ml.upper[l];
+      m.lower[l] = ctx->ml.lower[l];
+    }
+    for (size_t l = 0; l < ctx->ml.y_upper.size() && l < 16; ++l) {
+      m.y_upper[l] = ctx->ml.y_upper[l];
+      m.y_lower[l] = ctx->ml.y_lower[l];
+    }
+    m.delta_omega = ctx->ml.delta_omega;
+    k_fill_mixing_layer<<<grid_for(ctx, B.db.plane, 256), 256, 0, ctx->stream>>>(
+        B.db.plane, B.ycoord, B.bv[0], ctx->mixture ? B.sv[0] : nullptr, ctx->mixture ? ctx->der.n_spec : 0, m);
+  } else if (ctx->has_init) {
     FillVals fv{};
     for (int l = 0; l < 6; ++l) fv.val[l] = ctx->init_bv[l];
     k_fill_planes<<<grid_for(ctx, 6 * B.db.plane, 256), 256, 0, ctx->stream>>>(B.db.plane, B.bv[0], 6, fv);
@@ -2450,7 +2582,9 @@ void enqueue_set_state(ostc_ctx *ctx, BlockRes &B, const double *bv, const doubl
   k_scatter<<<grid_for(ctx, 6 * B.db.n, 256), 256, 0, ctx->stream>>>(B.db, bv, B.bv[0], 6);
   if (ctx->mixture) {
     const int ns = ctx->der.n_spec;
-    if (ctx->has_init && (int)ctx->init_sv.size() == ns && ns <= 16) {
+    if (ml) {
+      // filled with the profile above
+    } else if (ctx->has_init && (int)ctx->init_sv.size() == ns && ns <= 16) {
       FillVals fv{};
       for (int l = 0; l < ns; ++l) fv.val[l] = ctx->init_sv[l];
       k_fill_planes<<<grid_for(ctx, ns * B.db.plane, 256), 256, 0, ctx->stream>>>(B.db.plane, B.sv[0], ns, fv);
@@ -2570,7 +2704,7 @@ int enqueue_steady_iteration(ostc_ctx *ctx, double dt_phys = 0.0) {
         } else {
           launch_mix_source(ctx, B, st, fr);
         }
-        launch_fvs(ctx, B, st);
+        launch_mix_inviscid(ctx, B, st);
         if (ctx->der.viscous_order != 0) launch_mix_visc(ctx, B, st);
       } else {
         launch_flux<T>(ctx, B, st);
@@ -2805,6 +2939,8 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
     const int nv = ctx->nv, ns = ctx->der.n_spec;
     bool ok = alloc(&R.met, 9 * b.plane) && alloc(&R.jac, b.plane) && alloc(&R.dq, (size_t)nv * b.n) &&
               alloc(&R.last, 4 * b.n);
+    if (ok && ctx->mixture && ctx->der.inviscid_type != 3)
+      ok = alloc(&R.fcb, (size_t)nv * (HB.mx + 1) * (HB.my + 1) * (HB.mz + 1)) && alloc(&R.efd, b.plane);
     for (int s = 0; s < 3 && ok; ++s) {
       ok = alloc(&R.cv[s], (size_t)nv * b.plane) && alloc(&R.bv[s], 6 * b.plane) && alloc(&R.mul[s], b.plane);
       if (ok && ctx->mixture)
@@ -2857,6 +2993,37 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
       f.mw = hf.mw;
       f.wall_adiabatic = hf.wall_adiabatic;
       for (size_t l = 0; l < hf.y.size() && l < 16; ++l) f.y[l] = hf.y[l];
+      f.inflow_type = hf.inflow_type;
+      f.fluct = hf.fluctuation_type;
+      f.fluct_rms = hf.fluct_intensity;
+      f.velocity = hf.velocity;
+      f.delta_omega = hf.delta_omega;
+      for (int l = 0; l < 6; ++l) f.lower[l] = hf.lower[l];
+      for (size_t l = 0; l < hf.y_lower.size() && l < 16; ++l) f.y_lower[l] = hf.y_lower[l];
+      f.rng_row = (f.face == 0 ? HB.my : HB.mx) + 2 * HB.ngg;
+      double *fy = nullptr;
+      if (hf.type == kInflow && hf.inflow_type == 2) {
+        // y of every face node in k_bc_face's enumeration (tangential ranges padded by ngg)
+        const int t0 = f.face == 0 ? 1 : 0, t1 = f.face == 2 ? 1 : 2;
+        const int n0 = f.re[t0] - f.rs[t0] + 1, n1 = f.re[t1] - f.rs[t1] + 1;
+        std::vector<double> hy((size_t)n0 * n1);
+        for (int q = 0; q < n0 * n1; ++q) {
+          int id3[3];
+          id3[f.face] = f.rs[f.face];
+          id3[t0] = f.rs[t0] + q % n0;
+          id3[t1] = f.rs[t1] + q / n0;
+          hy[q] = HB.y[HB.cidx(id3[0], id3[1], id3[2])];
+        }
+        if (cudaMalloc(&fy, hy.size() * sizeof(double)) != cudaSuccess) {
+          g_create_error = "device allocation for the inflow coordinates failed";
+          ctx->blk.push_back(R);
+          ostc_destroy(ctx.release());
+          return OSTC_ENOMEM;
+        }
+        cudaMemcpy(fy, hy.data(), hy.size() * sizeof(double), cudaMemcpyHostToDevice);
+      }
+      f.ycoord = fy;
+      R.face_y.push_back(fy);
       R.faces.push_back(f);
     }
     for (auto &hi : HB.inner) {
@@ -2889,6 +3056,67 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
     g_create_error = "device allocation failed";
     ostc_destroy(ctx.release());
     return OSTC_ENOMEM;
+  }
+  if (ctx->der.problem_type == 1) {
+    // the initial field of a mixing-layer problem is the two-stream profile at every node, ghosts
+    // included (initialize_mixing_layer, Initialize.cu:228-326): y of every padded node
+    std::string e2;
+    if (!mixing_layer_streams(ctx->setup, ctx->mixture ? &ctx->chem : nullptr, ctx->ml, e2)) {
+      g_create_error = e2;
+      ostc_destroy(ctx.release());
+      return OSTC_EINVAL;
+    }
+    for (size_t bi = 0; bi < ctx->blk.size(); ++bi) {
+      BlockRes &R = ctx->blk[bi];
+      const HostBlock &HB = ctx->mesh.blocks[bi];
+      const DevBlock &b = R.db;
+      std::vector<double> hy(b.plane, 0.0);
+      for (int k = -b.gz; k < b.mz + b.gz; ++k)
+        for (int j = -b.g; j < b.my + b.g; ++j)
+          for (int i = -b.g; i < b.mx + b.g; ++i) hy[b.id(i, j, k)] = HB.y[HB.cidx(i, j, k)];
+      if (cudaMalloc(&R.ycoord, hy.size() * sizeof(double)) != cudaSuccess) {
+        g_create_error = "device allocation failed";
+        ostc_destroy(ctx.release());
+        return OSTC_ENOMEM;
+      }
+      cudaMemcpy(R.ycoord, hy.data(), hy.size() * sizeof(double), cudaMemcpyHostToDevice);
+    }
+  }
+  {
+    // white-noise inflows: generator states for the largest fluctuating face plane, ghost-padded by
+    // ngg (BoundCond.cu:1706-1735), seeded from the clock as the reference does until
+    // ostc_set_inflow_seed fixes the seed
+    long long size = 0;
+    int n_fluct = 0;
+    for (size_t bi = 0; bi < ctx->blk.size(); ++bi) {
+      const HostBlock &HB = ctx->mesh.blocks[bi];
+      for (const auto &f : ctx->blk[bi].faces) {
+        if (f.type != kInflow || f.fluct != 1) continue;
+        ++n_fluct;
+        const long long n1 = f.face == 0 ? HB.my : HB.mx, n2 = f.face == 2 ? HB.my : HB.mz;
+        size = std::max(size, (n1 + 2 * HB.ngg) * (n2 + 2 * HB.ngg));
+      }
+    }
+    if (n_fluct > 1) {
+      // the reference draws every such face from one shared array, in face order; this library runs
+      // one fluctuating face
+      g_create_error = "more than one inflow face with fluctuation_type 1 is not provided";
+      ostc_destroy(ctx.release());
+      return OSTC_EINVAL;
+    }
+    if (size > 0) {
+      if (cudaMalloc(&ctx->rng, size * sizeof(curandState)) != cudaSuccess) {
+        g_create_error = "device allocation for the inflow random-number states failed";
+        ostc_destroy(ctx.release());
+        return OSTC_ENOMEM;
+      }
+      ctx->rng_size = size;
+      for (auto &R : ctx->blk)
+        for (auto &f : R.faces)
+          if (f.type == kInflow && f.fluct == 1) f.rng = ctx->rng;
+      k_rng_init<<<grid_for(ctx.get(), size, 128), 128, 0, ctx->stream>>>(ctx->rng, size,
+                                                                     (unsigned long long)std::time(nullptr));
+    }
   }
   const double dt0 = ctx->der.fixed_time_step ? ctx->der.dt : 1e6;
   cudaMemcpy(ctx->d_dt, &dt0, sizeof(double), cudaMemcpyHostToDevice);
@@ -2947,6 +3175,10 @@ void ostc_destroy(ostc_ctx *ctx) {
     cudaFree(B.dqk);
     cudaFree(B.qn1);
     cudaFree(B.qstar);
+    cudaFree(B.fcb);
+    cudaFree(B.efd);
+    cudaFree(B.ycoord);
+    for (double *p : B.face_y) cudaFree(p);
     for (int s = 0; s < 4; ++s) {
       cudaFree(B.cv[s]);
       cudaFree(B.bv[s]);
@@ -2958,6 +3190,7 @@ void ostc_destroy(ostc_ctx *ctx) {
       cudaFree(B.acs[s]);
     }
   }
+  cudaFree(ctx->rng);
   cudaFree(ctx->d_dtbits);
   cudaFree(ctx->d_dt);
   cudaFree(ctx->d_time);
@@ -3109,7 +3342,7 @@ int ostc_rhs(ostc_ctx *ctx, int block, unsigned mask, double *dq, int ptr_kind) 
     const bool chem = (mask & OSTC_TERM_SOURCE) && ctx->der.reaction == 1;
     const bool implicit = chem && ctx->chem_mode == OSTC_CHEM_POINT_IMPLICIT;
     launch_mix_source(ctx, B, in, chem && !implicit);
-    if (mask & OSTC_TERM_INVISCID) launch_fvs(ctx, B, in);
+    if (mask & OSTC_TERM_INVISCID) launch_mix_inviscid(ctx, B, in);
     if ((mask & OSTC_TERM_VISCOUS) && ctx->der.viscous_order != 0) launch_mix_visc(ctx, B, in);
     if (implicit) launch_chem_epi(ctx, B, in);
     CK(cudaGetLastError());
@@ -3501,15 +3734,47 @@ static int ensure_graph(ostc_ctx *ctx) {
   return OSTC_OK;
 }
 
+// One step as ostc_set_launch_mode selects: the captured graph, or every kernel launched from the
+// host, block after block on the context stream.
+static int launch_step(ostc_ctx *ctx) {
+  if (ctx->launch_mode == OSTC_LAUNCH_BLOCK_LOOP) {
+    if (int r = enqueue_step_any(ctx)) return r;
+    CK(cudaGetLastError());
+  } else {
+    CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+  }
+  return stat_after_step(ctx);
+}
+
+int ostc_set_launch_mode(ostc_ctx *ctx, int mode) {
+  if (!ctx) return OSTC_EINVAL;
+  if (mode != OSTC_LAUNCH_GRAPH && mode != OSTC_LAUNCH_BLOCK_LOOP) {
+    ctx->err = "launch mode must be OSTC_LAUNCH_GRAPH (0) or OSTC_LAUNCH_BLOCK_LOOP (1)";
+    return OSTC_EINVAL;
+  }
+  ctx->launch_mode = mode;
+  return OSTC_OK;
+}
+
+int ostc_set_inflow_seed(ostc_ctx *ctx, long long seed) {
+  if (!ctx) return OSTC_EINVAL;
+  if (!ctx->rng) return OSTC_OK;
+  cudaSetDevice(ctx->device);
+  k_rng_init<<<grid_for(ctx, ctx->rng_size, 128), 128, 0, ctx->stream>>>(ctx->rng, ctx->rng_size,
+                                                                          (unsigned long long)seed);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  return OSTC_OK;
+}
+
 int ostc_rk3_step(ostc_ctx *ctx, int n_steps, double *dt_last) {
   if (!ctx || n_steps < 0) return OSTC_EINVAL;
   cudaSetDevice(ctx->device);
   if (int r = check_ready(ctx)) return r;
-  if (int r = ensure_graph(ctx)) return r;
-  for (int s = 0; s < n_steps; ++s) {
-    CK(cudaGraphLaunch(ctx->graph, ctx->stream));
-    if (int r = stat_after_step(ctx)) return r;
-  }
+  if (ctx->launch_mode == OSTC_LAUNCH_GRAPH)
+    if (int r = ensure_graph(ctx)) return r;
+  for (int s = 0; s < n_steps; ++s)
+    if (int r = launch_step(ctx)) return r;
   if (dt_last) {
     unsigned flags = 0;
     CK(cudaMemcpyAsync(dt_last, ctx->d_dt, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -3529,15 +3794,14 @@ int ostc_timed_steps(ostc_ctx *ctx, int n_steps, double *ms) {
   if (!ctx || n_steps < 0 || !ms) return OSTC_EINVAL;
   cudaSetDevice(ctx->device);
   if (int r = check_ready(ctx)) return r;
-  if (int r = ensure_graph(ctx)) return r;
+  if (ctx->launch_mode == OSTC_LAUNCH_GRAPH)
+    if (int r = ensure_graph(ctx)) return r;
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
   CK(cudaEventRecord(a, ctx->stream));
-  for (int s = 0; s < n_steps; ++s) {
-    CK(cudaGraphLaunch(ctx->graph, ctx->stream));
-    if (int r = stat_after_step(ctx)) return r;
-  }
+  for (int s = 0; s < n_steps; ++s)
+    if (int r = launch_step(ctx)) return r;
   CK(cudaEventRecord(b, ctx->stream));
   CK(cudaEventSynchronize(b));
   float t = 0;
@@ -4170,9 +4434,9 @@ int ostc_probe_case(const char *setup_txt, const char *input_dir, int out[16], c
   else if (!derive(setup, der, err)) rc = OSTC_EINVAL;
   else if (!read_mesh(dir, der, mesh, err)) rc = err.find("cannot open") != std::string::npos ? OSTC_EIO : OSTC_EINVAL;
   else if (!resolve_boundaries(setup, der, mesh, err)) rc = OSTC_EINVAL;
+  ChemTables chem;
   if (rc == OSTC_OK && der.species == 1) {
     // the species count comes from the mechanism (Species ctor, ChemData.cpp:11-75)
-    ChemTables chem;
     auto str = [&](const char *k) {
       auto it = setup.strings.find(k);
       return it == setup.strings.end() ? std::string() : it->second;
@@ -4185,6 +4449,8 @@ int ostc_probe_case(const char *setup_txt, const char *input_dir, int out[16], c
       der.n_var = 5 + chem.n_spec;
     }
   }
+  // the inflow states (mixing-layer streams included) resolve on the host too
+  if (rc == OSTC_OK && !resolve_inflows(setup, der.species == 1 ? &chem : nullptr, mesh, err)) rc = OSTC_EINVAL;
   if (rc != OSTC_OK) {
     if (msg && msg_len > 0) {
       std::strncpy(msg, err.c_str(), (size_t)msg_len - 1);

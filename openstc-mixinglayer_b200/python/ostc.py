@@ -19,6 +19,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 TERM_INVISCID, TERM_VISCOUS, TERM_SOURCE, TERM_ALL = 1, 2, 4, 7
 FLAG_NONPOSITIVE, FLAG_NAN = 1, 2
 CHEM_EXPLICIT, CHEM_POINT_IMPLICIT = 0, 1
+LAUNCH_GRAPH, LAUNCH_BLOCK_LOOP = 0, 1
 STAT_REY_U, STAT_REY_V, STAT_REY_W, STAT_REY_T, STAT_RHO_P = 1, 2, 4, 8, 16
 STAT_GROUPS = ("reynolds_1st", "favre_1st", "reynolds_2nd", "favre_2nd")
 
@@ -31,7 +32,8 @@ EXPORTS = [
     "ostc_rhs_vjp", "ostc_rk3_step_vjp", "ostc_adjoint_steps", "ostc_run_states", "ostc_bounds_flags",
     "ostc_bounds_checked", "ostc_stat_enable", "ostc_stat_disable", "ostc_stat_info", "ostc_stat_get",
     "ostc_stat_export", "ostc_stat_import", "ostc_write_plt", "ostc_read_plt", "ostc_tune_report",
-    "ostc_set_sweep_variant", "ostc_steady_step", "ostc_dual_time_step",
+    "ostc_set_sweep_variant", "ostc_steady_step", "ostc_dual_time_step", "ostc_set_launch_mode",
+    "ostc_set_inflow_seed",
 ]
 
 
@@ -100,6 +102,8 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.ostc_total_nodes.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     lib.ostc_tune_report.argtypes = [vp, ip, ip, ip, ctypes.POINTER(ip), ctypes.POINTER(ctypes.c_float), ip]
     lib.ostc_set_sweep_variant.argtypes = [vp, ip, ip, ip]
+    lib.ostc_set_launch_mode.argtypes = [vp, ip]
+    lib.ostc_set_inflow_seed.argtypes = [vp, ctypes.c_longlong]
     lib.ostc_steady_step.argtypes = [vp, ip, ctypes.POINTER(ip), dp]
     lib.ostc_dual_time_step.argtypes = [vp, ip, ctypes.POINTER(ip)]
     lib.ostc_timed_steps.argtypes = [vp, ip, dp]
@@ -377,6 +381,15 @@ class Solver:
         inner = ctypes.c_int()
         self._check(self.lib.ostc_dual_time_step(self.h, n, ctypes.byref(inner)))
         return inner.value
+
+    def set_inflow_seed(self, seed: int):
+        """Reseed the white-noise inflow generators (curand_init(seed + i, i, 0) per face-plane node)."""
+        self._check(self.lib.ostc_set_inflow_seed(self.h, seed))
+
+    def set_launch_mode(self, mode: int):
+        """LAUNCH_GRAPH (one CUDA graph per step) or LAUNCH_BLOCK_LOOP (every kernel launched from the host,
+        block after block, as the reference's per-block loop does)."""
+        self._check(self.lib.ostc_set_launch_mode(self.h, mode))
 
     def set_sweep_variant(self, dir: int, variant: int, precision: int = 0):
         """Pin sweep `dir` (0/1/2 = x/y/z) to kernel variant `variant` (-1: back to the autotuner)."""

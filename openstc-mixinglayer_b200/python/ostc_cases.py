@@ -63,6 +63,10 @@ class Case:
     # struct names listed in boundary_conditions besides bc_structs (the freestream struct when a face
     # applies it as an inflow)
     extra_bc: tuple = ()
+    # mixing-layer problem (problem_type 1): ma_c, delta_omega (m), velocity_ratio, upper_faster and the
+    # upper / lower stream structs {key: value} (temperature, pressure, mass fractions by species name,
+    # mixture_fraction); every inflow then takes the two-stream profile
+    mixing_layer: dict | None = None
 
     @property
     def nodes(self) -> int:
@@ -71,9 +75,9 @@ class Case:
     def setup_text(self) -> str:
         s = self.scheme
         lines = [
-            "// synthetic temporal mixing layer",
+            "// synthetic mixing layer",
             "bool parallel = 0",
-            "int problem_type = 0",
+            f"int problem_type = {1 if getattr(self, 'mixing_layer', None) else 0}",
             "int mesh_file_type = 0",
             "int gridIsBinary = 1",
             f"real gridScale = {self.grid_scale!r}",
@@ -125,7 +129,60 @@ class Case:
             for k, (t, v) in st.items():
                 lines.append(f"    {t} {k} = {v!r}" if t == "real" else f"    {t} {k} = {v}")
             lines.append("}")
+        if getattr(self, "mixing_layer", None):
+            m = self.mixing_layer
+            lines += [f"real ma_c = {m['ma_c']!r}", f"real delta_omega = {m['delta_omega']!r}",
+                      f"real velocity_ratio = {m['velocity_ratio']!r}", f"bool upper_faster = {int(m['upper_faster'])}",
+                      "bool compatible_mixing_layer = 0"]
+            if "freestream" in self.bc_structs and not self.freestream:
+                lines.append("string reference_state = freestream")
+            for side in ("upper", "lower"):
+                lines.append(f"struct {side}_stream = {{")
+                lines += [f"    real {k} = {v!r}" for k, v in m[side].items()]
+                lines.append("}")
         return "\n".join(lines) + "\n"
+
+    def mixing_layer_streams(self):
+        """get_mixing_layer_info (MixingLayer.cu:9-191), laminar: rho, u, v, w, p, T and the mass
+        fractions of the upper and lower streams of a problem_type 1 case."""
+        m = self.mixing_layer
+        up, lo = m["upper"], m["lower"]
+        tu, tl, pu, pl = up["temperature"], lo["temperature"], up["pressure"], lo["pressure"]
+        ma_u, ma_l = up.get("mach", -1.0), lo.get("mach", -1.0)
+        ns = self.mixture["tables"].n_spec if self.mixture else 0
+        yu, yl = [0.0] * ns, [0.0] * ns
+        if ns:
+            tb = self.mixture["tables"]
+            for i, name in enumerate(tb.names):
+                yu[i], yl[i] = float(up.get(name, 0.0)), float(lo.get(name, 0.0))
+            cpu, cpl = species_cp(tb, tu), species_cp(tb, tl)
+            mwu = mwl = cp_u = cp_l = 0.0
+            for i in range(ns):
+                mwu += yu[i] / tb.mw[i]
+                mwl += yl[i] / tb.mw[i]
+                cp_u += cpu[i] * yu[i]
+                cp_l += cpl[i] * yl[i]
+            gu, gl = cp_u / (cp_u - R_U * mwu), cp_l / (cp_l - R_U * mwl)
+            cu, cl = math.sqrt(gu * R_U * mwu * tu), math.sqrt(gl * R_U * mwl * tl)
+            rho_u, rho_l = pu / (R_U * mwu * tu), pl / (R_U * mwl * tl)
+        else:
+            cu, cl = math.sqrt(GAMMA * R_U / MW_AIR * tu), math.sqrt(GAMMA * R_U / MW_AIR * tl)
+            rho_u, rho_l = pu * MW_AIR / (R_U * tu), pl * MW_AIR / (R_U * tl)
+        ma_c, vr, uf = m["ma_c"], m["velocity_ratio"], bool(m["upper_faster"])
+        if vr > 0:
+            if vr > 1:
+                slow = ma_c * (cu + cl) / (vr - 1)
+                fast = vr * slow
+            else:
+                fast = ma_c * (cu + cl) / (1 - vr)
+                slow = fast * vr
+            ma_u, ma_l = (fast if uf else slow) / cu, (slow if uf else fast) / cl
+        elif ma_u > 0 and ma_l < 0:
+            ma_l = (ma_u - ma_c) * cu / cl - ma_c if uf else (ma_c + ma_u) * cu / cl + ma_c
+        elif ma_l > 0 and ma_u < 0:
+            ma_u = (ma_c + ma_l) * cl / cu + ma_c if uf else (ma_l - ma_c) * cl / cu - ma_c
+        return dict(upper=[rho_u, ma_u * cu, 0.0, 0.0, pu, tu], lower=[rho_l, ma_l * cl, 0.0, 0.0, pl, tl],
+                    y_upper=yu, y_lower=yl, delta_omega=m["delta_omega"])
 
     def farfield_states(self):
         """FarField ctor (BoundCond.cpp:586-669) from (mach, pressure, temperature): label -> state dict;
@@ -189,7 +246,25 @@ class Case:
 
     def reference_scales(self):
         """(rho_inf^2 v_inf^2, v_inf) of the reference state as the reference's Inflow ctor computes
-        them (BoundCond.cpp:157-214, 299-305); (0, 0) without one."""
+        them (BoundCond.cpp:157-214, 299-305); (0, 0) without one.  In a mixing-layer problem the
+        reference state is the upper stream of the inflow struct it names (BoundCond.cpp:28-62)."""
+        if getattr(self, "mixing_layer", None):
+            ml = self.mixing_layer_streams()
+            up = ml["upper"]
+            vel = math.sqrt(up[1] ** 2 + up[2] ** 2 + up[3] ** 2)
+            if abs(vel) < 1:
+                # the Inflow's speed of sound: gamma = cp / cv of the upper stream (BoundCond.cpp:56-66)
+                mw, gamma = MW_AIR, GAMMA
+                if self.mixture:
+                    tb = self.mixture["tables"]
+                    yk = ml["y_upper"]
+                    mw = 1 / sum(yk[i] / tb.mw[i] for i in range(tb.n_spec))
+                    cpi = species_cp(tb, up[5])
+                    cp = sum(yk[i] * cpi[i] for i in range(tb.n_spec))
+                    cv = sum(yk[i] * (cpi[i] - R_U / tb.mw[i]) for i in range(tb.n_spec))
+                    gamma = cp / cv
+                vel = math.sqrt(gamma * R_U / mw * up[5])
+            return up[0] * vel * up[0] * vel, vel
         f = self.freestream
         if not f:
             return 0.0, 0.0
@@ -221,10 +296,21 @@ class Case:
         """Inflow ctor (BoundCond.cpp:157-214) of constant inflows: label -> density, velocity
         (Mach times the speed of sound along (u, v, w)), pressure, temperature and mass fractions y."""
         out = {}
+        ml = self.mixing_layer_streams() if getattr(self, "mixing_layer", None) else None
         for st in self.face_structs():
             if st.get("type", (None, None))[1] != "inflow":
                 continue
             g = {k: v for k, (t, v) in st.items()}
+            if ml is not None:
+                # problem_type 1: the mixing-layer inflow (inflow_type 2) with the two streams
+                y, yl = [0.0] * 16, [0.0] * 16
+                y[:len(ml["y_upper"])] = ml["y_upper"]
+                yl[:len(ml["y_lower"])] = ml["y_lower"]
+                up = ml["upper"]
+                out[g["label"]] = dict(density=up[0], u=up[1], v=up[2], w=up[3], pressure=up[4], temperature=up[5],
+                                       y=y, inflow_type=2, delta_omega=ml["delta_omega"], lower=ml["lower"],
+                                       y_lower=yl)
+                continue
             t, p, mach = float(g["temperature"]), float(g["pressure"]), float(g["mach"])
             y = [0.0] * 16
             mw, gamma = MW_AIR, GAMMA
@@ -514,34 +600,64 @@ def _write_multi(case: MultiCase, directory: os.PathLike) -> Path:
 
 def multiblock_mixing_layer_3d(nb=12, lo=32, hi=256, my=None, mz=None, seed=0, steps=100, mc=0.5, re=1000.0,
                                t0=300.0, delta0=1e-3, h=0.125, reconstruction=5, inviscid_scheme=4, cfl=0.5,
-                               dims=None) -> MultiCase:
-    """nb blocks chained along x with seeded uneven i extents (uniform in [lo, hi]; `dims` overrides),
-    common j / k extents (drawn once in [lo, hi] unless given), joined by 1:1 interfaces (block b's i-max face on block b+1's i-min face,
-    coincident nodes).  Outflow at the two x ends, far-field y, periodic z within every block.  Shear
-    layer u = dU/2 tanh(2y/delta0), Mc = 0.5, with 1e-2 dU N(0,1) exp(-(y/delta0)^2) seeded noise in u, v, w."""
+                               dims=None, uneven_axes=False) -> MultiCase:
+    """nb blocks chained along x, joined by 1:1 interfaces (block b's i-max face on block b+1's i-min
+    face, coincident nodes).  Outflow at the two x ends, far-field y, periodic z within every block.
+    Shear layer u = dU/2 tanh(2y/delta0), Mc = 0.5, with 1e-2 dU N(0,1) exp(-(y/delta0)^2) seeded noise in
+    u, v, w.
+
+    Extents: seeded uneven i extents (uniform in [lo, hi]; `dims` overrides) with common j / k extents
+    (drawn once in [lo, hi] unless given); or, with uneven_axes, every block's three extents drawn
+    (uniform in [lo, hi]; `dims` may give (mx, my, mz) tuples).  Then neighbouring blocks share the
+    part of their x faces where both have nodes: block b's node j sits at y = (j - (my_b - 1) // 2) h
+    and node k at z = k h, the interface covers the overlapping j and k ranges, and the rest of each
+    x face is an outflow patch."""
     rng = np.random.default_rng(seed)
-    mxs = list(dims) if dims is not None else [int(v) for v in rng.integers(lo, hi + 1, nb)]
-    # the chain shares its j and k extents (1:1 faces); unless given they are drawn once from the seed
-    if my is None:
-        my = int(rng.integers(lo, hi + 1))
-    if mz is None:
-        mz = int(rng.integers(lo, hi + 1))
-    nb = len(mxs)
+    if uneven_axes:
+        ext = [tuple(int(v) for v in e) for e in dims] if dims is not None else \
+            [tuple(int(v) for v in rng.integers(lo, hi + 1, 3)) for _ in range(nb)]
+    else:
+        mxs = list(dims) if dims is not None else [int(v) for v in rng.integers(lo, hi + 1, nb)]
+        # the chain shares its j and k extents (1:1 faces); unless given they are drawn once from the seed
+        if my is None:
+            my = int(rng.integers(lo, hi + 1))
+        if mz is None:
+            mz = int(rng.integers(lo, hi + 1))
+        ext = [(m, my, mz) for m in mxs]
+    nb = len(ext)
     c0 = math.sqrt(GAMMA * R_AIR * t0)
     du = 2 * mc * c0
     rho0 = re * sutherland(t0) / (du * delta0)
     p0 = rho0 * R_AIR * t0
-    two_d = mz == 1
+    two_d = all(e[2] == 1 for e in ext)
+    cen = [(e[1] - 1) // 2 for e in ext]
+
+    def overlap(b):
+        """j range of block b and of block b + 1, and the shared k count, of their common x face."""
+        (_, myb, mzb), (_, myn, mzn) = ext[b], ext[b + 1]
+        d = cen[b] - cen[b + 1]  # j of block b = j of block b+1 + d
+        jlo, jhi = max(0, d), min(myb - 1, myn - 1 + d)
+        return jlo, jhi, jlo - d, jhi - d, min(mzb, mzn)
+
+    def x_face(i, myb, mzb, jlo, jhi, kn, label_open, faces):
+        """Outflow patches of an x face outside the interface's j [jlo, jhi] x k [0, kn) rectangle."""
+        if jlo > 0:
+            faces.append(Face((i, i, 0, jlo - 1, 0, mzb - 1), label_open))
+        if jhi < myb - 1:
+            faces.append(Face((i, i, jhi + 1, myb - 1, 0, mzb - 1), label_open))
+        if kn < mzb:
+            faces.append(Face((i, i, jlo, jhi, kn, mzb - 1), label_open))
+
     blocks = []
     x0 = 0.0
-    for b, mx in enumerate(mxs):
+    for b, (mx, myb, mzb) in enumerate(ext):
         xs = x0 + np.arange(mx) * h
-        ys = (np.arange(my) - (my - 1) / 2) * h
-        zs = np.arange(mz) * h
+        ys = (np.arange(myb) - (myb - 1) / 2) * h if not uneven_axes else (np.arange(myb) - cen[b]) * h
+        zs = np.arange(mzb) * h
         Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
         x0 = xs[-1]
         env = np.exp(-Y ** 2)
-        bv = np.empty((6, mz, my, mx))
+        bv = np.empty((6, mzb, myb, mx))
         bv[0] = rho0
         bv[1] = 0.5 * du * np.tanh(2 * Y) + 1e-2 * du * rng.standard_normal(X.shape) * env
         bv[2] = 1e-2 * du * rng.standard_normal(X.shape) * env
@@ -550,19 +666,24 @@ def multiblock_mixing_layer_3d(nb=12, lo=32, hi=256, my=None, mz=None, seed=0, s
         bv[5] = t0
         faces = []
         if b == 0:
-            faces.append(Face((0, 0, 0, my - 1, 0, mz - 1), 6))
+            faces.append(Face((0, 0, 0, myb - 1, 0, mzb - 1), 6))
         if b == nb - 1:
-            faces.append(Face((mx - 1, mx - 1, 0, my - 1, 0, mz - 1), 6))
-        faces += [Face((0, mx - 1, 0, 0, 0, mz - 1), 41), Face((0, mx - 1, my - 1, my - 1, 0, mz - 1), 4)]
-        if not two_d:
-            faces += [Face((0, mx - 1, 0, my - 1, 0, 0), 8), Face((0, mx - 1, 0, my - 1, mz - 1, mz - 1), 8)]
+            faces.append(Face((mx - 1, mx - 1, 0, myb - 1, 0, mzb - 1), 6))
         inner = []
         if b > 0:
-            pm = mxs[b - 1]
-            inner.append(([1, 1, -1, -my, 1, mz, b + 1], [pm, pm, -1, -my, 1, mz, b]))
+            _, _, jlo, jhi, kn = overlap(b - 1)
+            plo, phi, _, _, _ = overlap(b - 1)
+            x_face(0, myb, mzb, jlo, jhi, kn, 6, faces)
+            pm = ext[b - 1][0]
+            inner.append(([1, 1, -(jlo + 1), -(jhi + 1), 1, kn, b + 1], [pm, pm, -(plo + 1), -(phi + 1), 1, kn, b]))
         if b < nb - 1:
-            inner.append(([mx, mx, -1, -my, 1, mz, b + 1], [1, 1, -1, -my, 1, mz, b + 2]))
-        blocks.append(Block(mx, my, mz, X, Y, Z, faces, bv, inner))
+            jlo, jhi, nlo, nhi, kn = overlap(b)
+            x_face(mx - 1, myb, mzb, jlo, jhi, kn, 6, faces)
+            inner.append(([mx, mx, -(jlo + 1), -(jhi + 1), 1, kn, b + 1], [1, 1, -(nlo + 1), -(nhi + 1), 1, kn, b + 2]))
+        faces += [Face((0, mx - 1, 0, 0, 0, mzb - 1), 41), Face((0, mx - 1, myb - 1, myb - 1, 0, mzb - 1), 4)]
+        if not two_d:
+            faces += [Face((0, mx - 1, 0, myb - 1, 0, 0), 8), Face((0, mx - 1, 0, myb - 1, mzb - 1, mzb - 1), 8)]
+        blocks.append(Block(mx, myb, mzb, X, Y, Z, faces, bv, inner))
     structs = {"outflow": {"type": ("string", "outflow"), "label": ("int", 6)},
                "farfield_upper": {"type": ("string", "farfield"), "label": ("int", 4), "mach": ("real", mc),
                                   "pressure": ("real", p0), "temperature": ("real", t0), "u": ("real", 1.0),
@@ -578,14 +699,18 @@ def multiblock_mixing_layer_3d(nb=12, lo=32, hi=256, my=None, mz=None, seed=0, s
                      freestream=dict(mach=mc, pressure=p0, temperature=t0))
 
 
-def _inflow_x(faces, structs, mach, p, t, y=None):
+def _inflow_x(faces, structs, mach, p, t, y=None, noise=0.0):
     """Turn the periodic x faces into a constant supersonic inflow at i = 0 (label 5) and an outflow at
-    i = mx - 1 (label 6); y: inflow mass fractions {name: value} of a mixture."""
+    i = mx - 1 (label 6); y: inflow mass fractions {name: value} of a mixture; noise > 0: white noise of
+    that relative intensity on the inflow velocity (fluctuation_type 1)."""
     faces[0] = Face(faces[0].raw, 5)
     faces[1] = Face(faces[1].raw, 6)
     st = {"type": ("string", "inflow"), "label": ("int", 5), "mach": ("real", float(mach)),
           "pressure": ("real", float(p)), "temperature": ("real", float(t)), "u": ("real", 1.0), "v": ("real", 0.0),
           "w": ("real", 0.0)}
+    if noise > 0:
+        st["fluctuation_type"] = ("int", 1)
+        st["fluctuation_intensity"] = ("real", float(noise))
     for k, v in (y or {}).items():
         st[k] = ("real", float(v))
     structs["inflow"] = st
@@ -652,7 +777,7 @@ def mixing_layer_2d(mx=257, my=129, seed=0, steps=100, mc=0.4, re=1000.0, t0=300
 def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0, t0=300.0, delta0=1e-3,
                     h=0.125, reconstruction=5, inviscid_scheme=4, cfl=0.5, ybc="farfield",
                     entropy_fix_factor=0.125, wall_thermal="isothermal", xbc="periodic", ref_face=False,
-                    steady=None) -> Case:
+                    steady=None, inflow_noise=0.0) -> Case:
     """3-D temporal mixing layer: uniform spacing h*delta0, periodic x and z (node-coincident),
     far-field (Riemann-invariant, label 4/41) or outflow (label 6) y faces; u = dU/2 tanh(2y/delta0),
     Mc = 0.7, plus 1e-2 dU N(0,1) exp(-(y/delta0)^2) seeded white noise in u, v, w.
@@ -696,7 +821,7 @@ def mixing_layer_3d(mx=512, my=256, mz=128, seed=0, steps=200, mc=0.7, re=1000.0
     freestream = None
     extra_bc = ()
     if xbc == "inflow":
-        _inflow_x(faces, structs, 1.5, p0, t0)
+        _inflow_x(faces, structs, 1.5, p0, t0, noise=inflow_noise)
     elif xbc == "subsonic":
         # subsonic inflow at i = 0 (total state 1.2 p0, 1.05 T0) and back pressure p0 at i = mx - 1,
         # both relative to the reference state (Mach mc, p0, T0)
@@ -724,13 +849,15 @@ CHEM_FIXTURE = Path(__file__).resolve().parents[2] / "tests" / "golden" / "chem"
 def reacting_mixing_layer_3d(mx=384, my=192, mz=96, seed=0, steps=100, h=0.125, delta0=1e-3, mc=0.4,
                              p0=101325.0, inviscid_scheme=72, finite_rate=True, ybc="outflow",
                              chem_dir=None, fuel=None, oxidiser=None, wall_thermal="isothermal",
-                             xbc="periodic", steady=None) -> Case:
+                             xbc="periodic", steady=None, reconstruction=2) -> Case:
     """Reacting H2/air temporal mixing layer (9 species, 19 reactions after merging duplicates):
     fuel Y_H2 = 0.05 in N2 at 300 K (y > 0) over vitiated air at 1500 K (y < 0): Y_O2 = 0.20, Y_H2O = 0.10,
     radicals Y_OH = 1e-3, Y_O = 1e-4, Y_H = 1e-5, Y_HO2 = 1e-6, Y_H2O2 = 1e-7 (so that every reaction
     runs from the first step), N2 the rest; T and Y blended by (1 + tanh(2y/delta0))/2, uniform p0, u = dU/2 tanh(2y/delta0)
     with dU = 2 Mc (c_fuel + c_ox)/2 and 1e-2 dU N(0,1) exp(-(y/delta0)^2) seeded noise in u, v, w;
-    periodic x and z, outflow y; flux-split characteristic WENO7-Z (inviscid_scheme 72)."""
+    periodic x and z, outflow y; flux-split characteristic WENO7-Z (inviscid_scheme 72), or, with
+    inviscid_scheme 2 / 3 / 4, the primitive reconstruction `reconstruction` (1 first order, 2 MUSCL,
+    3 NND2) with Roe, AUSM+ or HLLC."""
     chem_dir = Path(chem_dir) if chem_dir else CHEM_FIXTURE
     tb = read_species(chem_dir, "H2_mech.inp", "therm.dat")
     ns = tb.n_spec
@@ -795,8 +922,8 @@ def reacting_mixing_layer_3d(mx=384, my=192, mz=96, seed=0, steps=100, h=0.125, 
         raise ValueError("the reacting case uses outflow, wall or far-field y faces")
     if xbc == "inflow":
         _inflow_x(faces, structs, 1.2, p0, to, oxidiser)
-    scheme = dict(reconstruction=2, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=0.5, prandtl_number=0.72,
-                  limiter=0, entropy_fix_factor=0.125)
+    scheme = dict(reconstruction=reconstruction, inviscid_scheme=inviscid_scheme, viscous_order=2, cfl=0.5,
+                  prandtl_number=0.72, limiter=0, entropy_fix_factor=0.125)
     scheme.update(steady or {})
     mixture = dict(tables=tb, finite_rate=finite_rate, chem_dir=str(chem_dir), mechanism="H2_mech.inp",
                    therm="therm.dat", tran="tran.dat")
@@ -804,6 +931,76 @@ def reacting_mixing_layer_3d(mx=384, my=192, mz=96, seed=0, steps=100, h=0.125, 
     return Case("reacting_mixing_layer_3d", mx, my, mz, X, Y, Z, delta0, faces, structs, scheme, bv, steps,
                 sv=sv, mixture=mixture, freestream=freestream, extra=dict(du=du, h=h))
 
+
+
+def spatial_mixing_layer_3d(mx=64, my=48, mz=12, seed=0, steps=20, h=0.125, delta_omega=1e-3, ma_c=0.3,
+                            velocity_ratio=1.5, upper_faster=False, species=False, fluctuation_type=0,
+                            intensity=0.01, inviscid_scheme=None, chem_dir=None, finite_rate=False) -> Case:
+    """Spatially developing mixing layer (problem_type 1, the layout of the reference's shipped input):
+    the two-stream inflow profile at i = 0 (u blended by tanh(2 y / delta_omega), upper / lower stream
+    state by the sign of y), optionally with white noise on its velocity (fluctuation_type 1, relative
+    intensity `intensity`, within |y| < 4 delta_omega); outflow at the other x face and both y faces;
+    periodic z (3-D).  Air: upper 300 K, lower 500 K at 1 bar; species: H2/N2 fuel above (300 K) over
+    air (600 K) with the 9-species mechanism, frozen unless finite_rate.  Stream Mach numbers from
+    ma_c and the velocity ratio (lower stream faster unless upper_faster).  Grid in units of
+    delta_omega (gridScale = delta_omega), y = (j - (my - 1) / 2) h.  The initial field is the profile
+    plus 1e-2 dU N(0,1) exp(-(y/delta_omega)^2) seeded noise in u, v, w."""
+    rng = np.random.default_rng(seed)
+    xs = np.arange(mx) * h
+    ys = (np.arange(my) - (my - 1) / 2) * h
+    zs = np.arange(mz) * h
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    if species:
+        chem_dir = Path(chem_dir) if chem_dir else CHEM_FIXTURE
+        tb = read_species(chem_dir, "H2_mech.inp", "therm.dat")
+        upper = {"temperature": 300.0, "pressure": 101325.0, "H2": 0.1, "N2": 0.9, "mixture_fraction": 1.0}
+        lower = {"temperature": 600.0, "pressure": 101325.0, "O2": 0.232, "N2": 0.768, "mixture_fraction": 0.0}
+        mixture = dict(tables=tb, finite_rate=finite_rate, chem_dir=str(chem_dir), mechanism="H2_mech.inp",
+                       therm="therm.dat", tran="tran.dat")
+        scheme_id = inviscid_scheme or 72
+    else:
+        upper = {"temperature": 300.0, "pressure": 101325.0}
+        lower = {"temperature": 500.0, "pressure": 101325.0}
+        mixture = None
+        scheme_id = inviscid_scheme or 4
+    ml = dict(ma_c=ma_c, delta_omega=delta_omega, velocity_ratio=velocity_ratio, upper_faster=upper_faster,
+              upper=upper, lower=lower)
+    faces = [Face((0, 0, 0, my - 1, 0, mz - 1), 5), Face((mx - 1, mx - 1, 0, my - 1, 0, mz - 1), 6),
+             Face((0, mx - 1, 0, 0, 0, mz - 1), 6), Face((0, mx - 1, my - 1, my - 1, 0, mz - 1), 6)]
+    if mz > 1:
+        faces += [Face((0, mx - 1, 0, my - 1, 0, 0), 8), Face((0, mx - 1, 0, my - 1, mz - 1, mz - 1), 8)]
+    # the inflow struct is also the reference state, as in the reference's shipped input
+    structs = {"freestream": {"type": ("string", "inflow"), "label": ("int", 5), "inflow_type": ("int", 1),
+                              "fluctuation_type": ("int", fluctuation_type),
+                              "fluctuation_intensity": ("real", float(intensity))},
+               "outflow": {"type": ("string", "outflow"), "label": ("int", 6)}}
+    if mz > 1:
+        structs["periodic"] = {"type": ("string", "periodic"), "label": ("int", 8)}
+    recon = 5 if scheme_id in (1, 3, 4) else 2
+    scheme = dict(reconstruction=recon, inviscid_scheme=scheme_id, viscous_order=2, cfl=0.5, prandtl_number=0.72,
+                  limiter=0, entropy_fix_factor=0.125)
+    case = Case("spatial_mixing_layer", mx, my, mz, X, Y, Z, delta_omega, faces, structs, scheme,
+                np.zeros((6,) + X.shape), steps, mixture=mixture, mixing_layer=ml)
+    st = case.mixing_layer_streams()
+    up, lo = st["upper"], st["lower"]
+    yphys = Y * delta_omega
+    above = yphys >= 0
+    du = abs(up[1] - lo[1])
+    env = np.exp(-Y ** 2)
+    bv = case.bv
+    for l in (0, 4, 5):
+        bv[l] = np.where(above, up[l], lo[l])
+    bv[1] = 0.5 * (up[1] + lo[1]) + 0.5 * (up[1] - lo[1]) * np.tanh(2 * yphys / delta_omega)
+    bv[1] += 1e-2 * du * rng.standard_normal(X.shape) * env
+    bv[2] = 1e-2 * du * rng.standard_normal(X.shape) * env
+    bv[3] = 0.0 if mz == 1 else 1e-2 * du * rng.standard_normal(X.shape) * env
+    if species:
+        ns = tb.n_spec
+        case.sv = np.empty((ns,) + X.shape)
+        for l in range(ns):
+            case.sv[l] = np.where(above, st["y_upper"][l], st["y_lower"][l])
+    case.extra = dict(du=du, h=h)
+    return case
 
 # ---- sensitivity of the momentum thickness to inflow mode amplitudes (adjoint harness)
 

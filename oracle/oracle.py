@@ -19,7 +19,11 @@ LIB = HERE / "_build" / "libostc_oracle.so"
 class OrcFace(ctypes.Structure):
     _fields_ = [("type", ctypes.c_int), ("raw", ctypes.c_int * 6)] + [
         (n, ctypes.c_double) for n in ("density", "u", "v", "w", "pressure", "temperature", "acoustic_speed",
-                                       "gamma", "entropy", "mw")] + [("wall_adiabatic", ctypes.c_int), ("y", ctypes.c_double * 16)]
+                                       "gamma", "entropy", "mw")] + [("wall_adiabatic", ctypes.c_int), ("y", ctypes.c_double * 16),
+                                                                     ("inflow_type", ctypes.c_int),
+                                                                     ("delta_omega", ctypes.c_double),
+                                                                     ("lower", ctypes.c_double * 6),
+                                                                     ("y_lower", ctypes.c_double * 16)]
 
 
 MAXS, MAXR = 16, 64
@@ -66,7 +70,10 @@ class OrcCase(ctypes.Structure):
                 ("v_ref", ctypes.c_double), ("has_init", ctypes.c_int), ("init_bv", ctypes.c_double * 6),
                 ("init_sv", ctypes.c_double * MAXS), ("chem_mode", ctypes.c_int), ("implicit_method", ctypes.c_int),
                 ("dplur_inner", ctypes.c_int), ("chem_src_method", ctypes.c_int), ("inner_iteration", ctypes.c_int),
-                ("max_inner_iteration", ctypes.c_int), ("iteration_adjust_step", ctypes.c_int)]
+                ("max_inner_iteration", ctypes.c_int), ("iteration_adjust_step", ctypes.c_int),
+                ("problem_type", ctypes.c_int), ("ml_upper", ctypes.c_double * 6), ("ml_lower", ctypes.c_double * 6),
+                ("ml_y_upper", ctypes.c_double * MAXS), ("ml_y_lower", ctypes.c_double * MAXS),
+                ("ml_delta_omega", ctypes.c_double)]
 
 
 def riemann_of(reconstruction: int, inviscid_scheme: int) -> int:
@@ -79,6 +86,15 @@ def riemann_of(reconstruction: int, inviscid_scheme: int) -> int:
 
 
 def _set_init(c, case):
+    ml = case.mixing_layer_streams() if getattr(case, "mixing_layer", None) else None
+    if ml is not None:
+        # problem_type 1: every node starts from the two-stream profile
+        c.problem_type = 1
+        for q in range(6):
+            c.ml_upper[q], c.ml_lower[q] = ml["upper"][q], ml["lower"][q]
+        for q, (a, b) in enumerate(zip(ml["y_upper"], ml["y_lower"])):
+            c.ml_y_upper[q], c.ml_y_lower[q] = a, b
+        c.ml_delta_omega = ml["delta_omega"]
     st = case.default_state() if hasattr(case, "default_state") else None
     if st is not None:
         bv, y = st
@@ -178,7 +194,11 @@ class Oracle:
                 c.face[n].raw[q] = f.raw[q]
             if f.label in ff:
                 for k, v in ff[f.label].items():
-                    setattr(c.face[n], k, (ctypes.c_double * 16)(*v) if k == "y" else v)
+                    if k in ("y", "y_lower"):
+                        v = (ctypes.c_double * 16)(*v)
+                    elif k == "lower":
+                        v = (ctypes.c_double * 6)(*v)
+                    setattr(c.face[n], k, v)
         self.n_spec = 0
         mix = getattr(case, "mixture", None)
         if mix is not None:

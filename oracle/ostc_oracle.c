@@ -29,6 +29,8 @@ typedef struct {
   double density, u, v, w, pressure, temperature, acoustic_speed, gamma, entropy, mw;
   int wall_adiabatic;
   double y[16];
+  int inflow_type;
+  double delta_omega, lower[6], y_lower[16];
 } face_t;
 
 struct orc_ctx {
@@ -276,12 +278,17 @@ static void register_face(orc_ctx *o, const orc_face_in *in, face_t *f) {
   f->acoustic_speed = in->acoustic_speed; f->gamma = in->gamma; f->entropy = in->entropy; f->mw = in->mw;
   f->wall_adiabatic = in->wall_adiabatic;
   memcpy(f->y, in->y, sizeof(f->y));
+  f->inflow_type = in->inflow_type;
+  f->delta_omega = in->delta_omega;
+  memcpy(f->lower, in->lower, sizeof(f->lower));
+  memcpy(f->y_lower, in->y_lower, sizeof(f->y_lower));
 }
 
 /* ---------------------------------------------------------------- pointwise helpers */
 
 /* compute_cv_from_bv_1_point + compute_total_energy<Air> (FieldOperation.cuh:17-38,78-105). */
 static void mix_h_cp(const orc_chem *ch, double t, double *h, double *cp);
+#define FVS_MAXV (5 + ORC_MAX_SPEC)
 
 static void cv_from_bv(orc_ctx *o, long p) {
   const long P = o->P;
@@ -636,7 +643,7 @@ static double entropy_fix_delta(const orc_ctx *o, long p) {
   const double kx = sqrt(M(o, 1, 1, p) * M(o, 1, 1, p) + M(o, 1, 2, p) * M(o, 1, 2, p) + M(o, 1, 3, p) * M(o, 1, 3, p));
   const double ky = sqrt(M(o, 2, 1, p) * M(o, 2, 1, p) + M(o, 2, 2, p) * M(o, 2, 2, p) + M(o, 2, 3, p) * M(o, 2, 3, p));
   const double kz = sqrt(M(o, 3, 1, p) * M(o, 3, 1, p) + M(o, 3, 2, p) * M(o, 3, 2, p) + M(o, 3, 3, p) * M(o, 3, 3, p));
-  const double c = sqrt(GAMMA_AIR * o->bv[4 * P + p] / o->bv[p]);
+  const double c = o->ns ? o->acs[p] : sqrt(GAMMA_AIR * o->bv[4 * P + p] / o->bv[p]);
   if (o->dim == 2) return o->c.entropy_fix_factor * (U + V + c * 0.5 * (kx + ky));
   return o->c.entropy_fix_factor * (U + V + W + c * (kx + ky + kz) / 3.0);
 }
@@ -752,6 +759,269 @@ static void pv_reconstruct(const double st[4][5], int recon, double pl[6], doubl
 
 /* compute_convective_term_pv_1D (InviscidScheme.cu:52-161) and Roe_compute_inviscid_flux_1D
  * (:459-548) for one direction: faces at idx+1/2, idx = -1 .. n-1, then dq -= fc(i+1/2) - fc(i-1/2). */
+/* ---- mixtures: the primitive-reconstruction path with the mixture branches of reconstruction()
+ * (InviscidScheme.cu:163-215) and of the Riemann solvers (RiemannSolver.cuh:9-417).  A reconstructed
+ * state holds rho, u, v, w, p, Y_1..Y_ns at [0, nv), then rho E at [nv] and gamma at [nv + 1]. */
+#define PVM_MAX (FVS_MAXV + 2)
+
+static void pv_reconstruct_mix(const orc_ctx *o, double st[4][FVS_MAXV], int recon, double *pl, double *pr) {
+  const orc_chem *ch = o->c.chem;
+  const int nv = o->nv, ns = o->ns;
+  const double kappa = 1.0 / 3.0;
+  for (int l = 0; l < nv; ++l) {
+    const double di = st[1][l] - st[0][l], di1 = st[2][l] - st[1][l], di2 = st[3][l] - st[2][l];
+    if (recon == 2) {
+      const double dnl = minmod(di, di1), dpl = minmod(di1, di);
+      const double dnr = minmod(di1, di2), dpr = minmod(di2, di1);
+      pl[l] = st[1][l] + 0.25 * ((1 - kappa) * dnl + (1 + kappa) * dpl);
+      pr[l] = st[2][l] - 0.25 * ((1 - kappa) * dpr + (1 + kappa) * dnr);
+    } else if (recon == 3) {
+      pl[l] = st[1][l] + 0.5 * minmod(di, di1);
+      pr[l] = st[2][l] - 0.5 * minmod(di1, di2);
+    } else {
+      pl[l] = st[1][l];
+      pr[l] = st[2][l];
+    }
+  }
+  double el = 0.5 * (pl[1] * pl[1] + pl[2] * pl[2] + pl[3] * pl[3]);
+  double er = 0.5 * (pr[1] * pr[1] + pr[2] * pr[2] + pr[3] * pr[3]);
+  double mw_inv_l = 0, mw_inv_r = 0;
+  for (int l = 0; l < ns; ++l) {
+    mw_inv_l += pl[5 + l] / ch->mw[l];
+    mw_inv_r += pr[5 + l] / ch->mw[l];
+  }
+  const double t_l = pl[4] / (pl[0] * R_U * mw_inv_l);
+  const double t_r = pr[4] / (pr[0] * R_U * mw_inv_r);
+  double hl[ORC_MAX_SPEC], hr[ORC_MAX_SPEC], cpl_i[ORC_MAX_SPEC], cpr_i[ORC_MAX_SPEC];
+  mix_h_cp(ch, t_l, hl, cpl_i);
+  mix_h_cp(ch, t_r, hr, cpr_i);
+  double cpl = 0, cpr = 0, cvl = 0, cvr = 0;
+  for (int l = 0; l < ns; ++l) {
+    cpl += cpl_i[l] * pl[l + 5];
+    cpr += cpr_i[l] * pr[l + 5];
+    cvl += pl[l + 5] * (cpl_i[l] - R_U / ch->mw[l]);
+    cvr += pr[l + 5] * (cpr_i[l] - R_U / ch->mw[l]);
+    el += hl[l] * pl[l + 5];
+    er += hr[l] * pr[l + 5];
+  }
+  pl[nv] = pl[0] * el - pl[4];
+  pr[nv] = pr[0] * er - pr[4];
+  pl[nv + 1] = cpl / cvl;
+  pr[nv + 1] = cpr / cvr;
+}
+
+/* riemannSolver_ausmPlus<mixture> (RiemannSolver.cuh:9-96) */
+static void ausm_mix(const orc_ctx *o, const double *pl, const double *pr, const double mt[2][3],
+                     const double jc[2], double *fc) {
+  const int nv = o->nv;
+  const double k1 = 0.5 * (jc[0] * mt[0][0] + jc[1] * mt[1][0]);
+  const double k2 = 0.5 * (jc[0] * mt[0][1] + jc[1] * mt[1][1]);
+  const double k3 = 0.5 * (jc[0] * mt[0][2] + jc[1] * mt[1][2]);
+  const double gkj = sqrt(k1 * k1 + k2 * k2 + k3 * k3);
+  const double ul = (k1 * pl[1] + k2 * pl[2] + k3 * pl[3]) / gkj;
+  const double ur = (k1 * pr[1] + k2 * pr[2] + k3 * pr[3]) / gkj;
+  const double p_l = pl[4], p_r = pr[4], rho_l = pl[0], rho_r = pr[0];
+  const double gam_l = pl[nv + 1], gam_r = pr[nv + 1];
+  const double c = 0.5 * (sqrt(gam_l * p_l / rho_l) + sqrt(gam_r * p_r / rho_r));
+  const double mach_l = ul / c, mach_r = ur / c;
+  double mlp, mrn, plp, prn;
+  const double alpha = 3 / 16.0;
+  if (fabs(mach_l) > 1) {
+    mlp = 0.5 * (mach_l + fabs(mach_l));
+    plp = mlp / mach_l;
+  } else {
+    const double a = (mach_l + 1) * (mach_l + 1) * 0.25;
+    const double b = (mach_l * mach_l - 1) * (mach_l * mach_l - 1);
+    mlp = a + 0.125 * b;
+    plp = a * (2 - mach_l) + alpha * mach_l * b;
+  }
+  if (fabs(mach_r) > 1) {
+    mrn = 0.5 * (mach_r - fabs(mach_r));
+    prn = mrn / mach_r;
+  } else {
+    const double a = (mach_r - 1) * (mach_r - 1) * 0.25;
+    const double b = (mach_r * mach_r - 1) * (mach_r * mach_r - 1);
+    mrn = -a - 0.125 * b;
+    prn = a * (2 + mach_r) - alpha * mach_r * b;
+  }
+  const double p_coeff = plp * p_l + prn * p_r;
+  const double m_half = mlp + mrn;
+  const double mach_pos = 0.5 * (m_half + fabs(m_half));
+  const double mach_neg = 0.5 * (m_half - fabs(m_half));
+  const double mass_flux = c * (rho_l * mach_pos + rho_r * mach_neg);
+  const double coeff = mass_flux * gkj;
+  const double *q = mass_flux >= 0 ? pl : pr;
+  fc[0] = coeff;
+  fc[1] = coeff * q[1] + p_coeff * k1;
+  fc[2] = coeff * q[2] + p_coeff * k2;
+  fc[3] = coeff * q[3] + p_coeff * k3;
+  fc[4] = coeff * (q[nv] + q[4]) / q[0];
+  for (int l = 5; l < nv; ++l) fc[l] = coeff * q[l];
+}
+
+/* gamma, speed of sound, mixture molecular weight and species enthalpies at the Roe-averaged state
+ * (the mixture branches of riemannSolver_hllc / riemannSolver_Roe, RiemannSolver.cuh:118-137, 316-336) */
+static void roe_mixture_sound(const orc_ctx *o, const double *svm, double tl, double tr, double wl, double wr,
+                              double wsum_inv, int hllc_form, double *gamma, double *c, double *mw, double *h_i) {
+  const orc_chem *ch = o->c.chem;
+  double mw_inv = 0;
+  for (int l = 0; l < o->ns; ++l) mw_inv += svm[l] / ch->mw[l];
+  const double t = hllc_form ? (wl * tl + wr * tr) / (R_U * mw_inv) : (wl * tl + wr * tr) * wsum_inv / (R_U * mw_inv);
+  double cp_i[ORC_MAX_SPEC];
+  mix_h_cp(ch, t, h_i, cp_i);
+  double cv = 0, cp = 0;
+  for (int l = 0; l < o->ns; ++l) {
+    cp += cp_i[l] * svm[l];
+    cv += svm[l] * (cp_i[l] - R_U / ch->mw[l]);
+  }
+  *gamma = cp / cv;
+  *c = sqrt(*gamma * R_U * mw_inv * t);
+  *mw = 1.0 / mw_inv;
+}
+
+/* riemannSolver_hllc<mixture> (RiemannSolver.cuh:98-230) */
+static void hllc_mix(const orc_ctx *o, const double *pl, const double *pr, const double mt[2][3], const double jc[2],
+                     double *fc) {
+  const int nv = o->nv;
+  const double rl_c = sqrt(pl[0]) / (sqrt(pl[0]) + sqrt(pr[0])), rr_c = sqrt(pr[0]) / (sqrt(pl[0]) + sqrt(pr[0]));
+  const double u_t = pl[1] * rl_c + pr[1] * rr_c, v_t = pl[2] * rl_c + pr[2] * rr_c, w_t = pl[3] * rl_c + pr[3] * rr_c;
+  double svm[FVS_MAXV];
+  for (int l = 0; l < nv - 5; ++l) svm[l] = rl_c * pl[l + 5] + rr_c * pr[l + 5];
+  double gamma, c_t, mw, h_i[ORC_MAX_SPEC];
+  roe_mixture_sound(o, svm, pl[4] / pl[0], pr[4] / pr[0], rl_c, rr_c, 0, 1, &gamma, &c_t, &mw, h_i);
+  const double kx = 0.5 * (mt[0][0] + mt[1][0]), ky = 0.5 * (mt[0][1] + mt[1][1]), kz = 0.5 * (mt[0][2] + mt[1][2]);
+  const double gradK = sqrt(kx * kx + ky * ky + kz * kz);
+  const double U_t = (kx * u_t + ky * v_t + kz * w_t) / gradK;
+  const double jac_ave = 0.5 * (jc[0] + jc[1]);
+  const double gamma_l = pl[nv + 1], gamma_r = pr[nv + 1];
+  const double Ul = kx * pl[1] + ky * pl[2] + kz * pl[3];
+  const double cl = sqrt(gamma_l * pl[4] / pl[0]);
+  const double sl = fmin(Ul / gradK - cl, U_t - c_t);
+  if (sl >= 0) {
+    const double rhoUk = pl[0] * Ul;
+    fc[0] = jac_ave * rhoUk;
+    fc[1] = jac_ave * (rhoUk * pl[1] + pl[4] * kx);
+    fc[2] = jac_ave * (rhoUk * pl[2] + pl[4] * ky);
+    fc[3] = jac_ave * (rhoUk * pl[3] + pl[4] * kz);
+    fc[4] = jac_ave * ((pl[nv] + pl[4]) * Ul);
+    for (int l = 5; l < nv; ++l) fc[l] = jac_ave * rhoUk * pl[l];
+    return;
+  }
+  const double Ur = kx * pr[1] + ky * pr[2] + kz * pr[3];
+  const double cr = sqrt(gamma_r * pr[4] / pr[0]);
+  const double sr = fmax(Ur / gradK + cr, U_t + c_t);
+  if (sr < 0) {
+    const double rhoUk = pr[0] * Ur;
+    fc[0] = jac_ave * rhoUk;
+    fc[1] = jac_ave * (rhoUk * pr[1] + pr[4] * kx);
+    fc[2] = jac_ave * (rhoUk * pr[2] + pr[4] * ky);
+    fc[3] = jac_ave * (rhoUk * pr[3] + pr[4] * kz);
+    fc[4] = jac_ave * ((pr[nv] + pr[4]) * Ur);
+    for (int l = 5; l < nv; ++l) fc[l] = jac_ave * rhoUk * pr[l];
+    return;
+  }
+  const double sm = ((pr[0] * Ur * (sr - Ur / gradK) - pl[0] * Ul * (sl - Ul / gradK)) / gradK + pl[4] - pr[4]) /
+                    (pr[0] * (sr - Ur / gradK) - pl[0] * (sl - Ul / gradK));
+  const double pm = pl[0] * (sl - Ul / gradK) * (sm - Ul / gradK) + pl[4];
+  const double *q = sm >= 0 ? pl : pr;
+  const double s = sm >= 0 ? sl : sr, Uq = sm >= 0 ? Ul : Ur;
+  const double pCoeff = 1.0 / (s - sm);
+  const double QCoeff = jac_ave * pCoeff * sm * (s * gradK - Uq) * q[0];
+  fc[0] = QCoeff;
+  const double dP = (s * pm - sm * q[4]) * pCoeff * jac_ave;
+  fc[1] = QCoeff * q[1] + dP * kx;
+  fc[2] = QCoeff * q[2] + dP * ky;
+  fc[3] = QCoeff * q[3] + dP * kz;
+  fc[4] = QCoeff * q[nv] / q[0] + pCoeff * jac_ave * (s * pm * sm * gradK - sm * q[4] * Uq);
+  for (int l = 5; l < nv; ++l) fc[l] = QCoeff * q[l];
+}
+
+/* compute_half_sum_left_right_flux + riemannSolver_Roe<mixture> (RiemannSolver.cuh:232-417) */
+static void roe_mix(const orc_ctx *o, const double *pl, const double *pr, const double mt[2][3], const double jc[2],
+                    double d0, double d1, double *fc) {
+  const orc_chem *ch = o->c.chem;
+  const int nv = o->nv, ns = o->ns;
+  double JacKx = jc[0] * mt[0][0], JacKy = jc[0] * mt[0][1], JacKz = jc[0] * mt[0][2];
+  double Uk = pl[1] * JacKx + pl[2] * JacKy + pl[3] * JacKz;
+  double coeff = Uk * pl[0];
+  fc[0] = 0.5 * coeff;
+  fc[1] = 0.5 * (coeff * pl[1] + pl[4] * JacKx);
+  fc[2] = 0.5 * (coeff * pl[2] + pl[4] * JacKy);
+  fc[3] = 0.5 * (coeff * pl[3] + pl[4] * JacKz);
+  fc[4] = 0.5 * Uk * (pl[4] + pl[nv]);
+  for (int l = 5; l < nv; ++l) fc[l] = 0.5 * coeff * pl[l];
+  JacKx = jc[1] * mt[1][0];
+  JacKy = jc[1] * mt[1][1];
+  JacKz = jc[1] * mt[1][2];
+  Uk = pr[1] * JacKx + pr[2] * JacKy + pr[3] * JacKz;
+  coeff = Uk * pr[0];
+  fc[0] += 0.5 * coeff;
+  fc[1] += 0.5 * (coeff * pr[1] + pr[4] * JacKx);
+  fc[2] += 0.5 * (coeff * pr[2] + pr[4] * JacKy);
+  fc[3] += 0.5 * (coeff * pr[3] + pr[4] * JacKz);
+  fc[4] += 0.5 * Uk * (pr[4] + pr[nv]);
+  for (int l = 5; l < nv; ++l) fc[l] += 0.5 * coeff * pr[l];
+
+  const double dl = sqrt(pl[0]), dr = sqrt(pr[0]);
+  const double inv_den = 1.0 / (dl + dr);
+  const double u = (dl * pl[1] + dr * pr[1]) * inv_den;
+  const double v = (dl * pl[2] + dr * pr[2]) * inv_den;
+  const double w = (dl * pl[3] + dr * pr[3]) * inv_den;
+  const double ek = 0.5 * (u * u + v * v + w * w);
+  const double hl = (pl[nv] + pl[4]) / pl[0];
+  const double hr = (pr[nv] + pr[4]) / pr[0];
+  const double h = (dl * hl + dr * hr) * inv_den;
+  double svm[FVS_MAXV];
+  for (int l = 0; l < nv - 5; ++l) svm[l] = (dl * pl[l + 5] + dr * pr[l + 5]) * inv_den;
+  double gamma, c, mw, h_i[ORC_MAX_SPEC];
+  roe_mixture_sound(o, svm, pl[4] / pl[0], pr[4] / pr[0], dl, dr, inv_den, 0, &gamma, &c, &mw, h_i);
+  double kx = 0.5 * (mt[0][0] + mt[1][0]), ky = 0.5 * (mt[0][1] + mt[1][1]), kz = 0.5 * (mt[0][2] + mt[1][2]);
+  const double gradK = sqrt(kx * kx + ky * ky + kz * kz);
+  double Ukk = kx * u + ky * v + kz * w;
+  double ch3[3] = {Ukk - gradK * c, Ukk, Ukk + gradK * c};
+  const double ed = 0.5 * (d0 + d1);
+  for (int q = 0; q < 3; ++q) {
+    ch3[q] = fabs(ch3[q]);
+    if (ch3[q] < ed) ch3[q] = 0.5 * (ch3[q] * ch3[q] / ed + ed);
+  }
+  kx /= gradK;
+  ky /= gradK;
+  kz /= gradK;
+  Ukk /= gradK;
+  const double jac_ave = 0.5 * (jc[0] + jc[1]);
+  double dq[FVS_MAXV];
+  dq[0] = jac_ave * (pr[0] - pl[0]);
+  for (int l = 1; l < nv; ++l) dq[l] = jac_ave * (pr[0] * pr[l] - pl[0] * pl[l]);
+  dq[4] = jac_ave * (pr[nv] - pl[nv]);
+  double c1 = (gamma - 1) * (ek * dq[0] - u * dq[1] - v * dq[2] - w * dq[3] + dq[4]) / (c * c);
+  double c2 = (kx * dq[1] + ky * dq[2] + kz * dq[3] - Ukk * dq[0]) / c;
+  for (int l = 0; l < ns; ++l) c1 += (mw / ch->mw[l] - h_i[l] * (gamma - 1) / (c * c)) * dq[l + 5];
+  double c3 = dq[0] - c1;
+  double LDq[FVS_MAXV];
+  LDq[0] = 0.5 * (c1 - c2);
+  LDq[1] = kx * c3 - ((kz * v - ky * w) * dq[0] - kz * dq[2] + ky * dq[3]) / c;
+  LDq[2] = ky * c3 - ((kx * w - kz * u) * dq[0] - kx * dq[3] + kz * dq[1]) / c;
+  LDq[3] = kz * c3 - ((ky * u - kx * v) * dq[0] - ky * dq[1] + kx * dq[2]) / c;
+  LDq[4] = 0.5 * (c1 + c2);
+  for (int l = 0; l < ns; ++l) LDq[l + 5] = dq[l + 5] - svm[l] * dq[0];
+  double *b = dq;
+  b[0] = -ch3[0] * LDq[0];
+  for (int l = 1; l < nv; ++l) b[l] = -ch3[1] * LDq[l];
+  b[4] = -ch3[2] * LDq[4];
+  const double c0 = kx * b[1] + ky * b[2] + kz * b[3];
+  c1 = c0 + b[0] + b[4];
+  c2 = c * (b[4] - b[0]);
+  c3 = 0;
+  for (int l = 0; l < ns; ++l) c3 += (h_i[l] - mw / ch->mw[l] * c * c / (gamma - 1)) * b[l + 5];
+  fc[0] += 0.5 * c1;
+  fc[1] += 0.5 * (u * c1 + kx * c2 - c * (kz * b[2] - ky * b[3]));
+  fc[2] += 0.5 * (v * c1 + ky * c2 - c * (kx * b[3] - kz * b[1]));
+  fc[3] += 0.5 * (w * c1 + kz * c2 - c * (ky * b[1] - kx * b[2]));
+  fc[4] += 0.5 * (h * c1 + Ukk * c2 - c * c * c0 / (gamma - 1) +
+                  c * ((kz * v - ky * w) * b[1] + (kx * w - kz * u) * b[2] + (ky * u - kx * v) * b[3]) + c3);
+  for (int l = 0; l < nv - 5; ++l) fc[5 + l] += 0.5 * (b[l + 5] + svm[l] * c1);
+}
+
 static void pv_direction(orc_ctx *o, int dir) {
   const int ext[3] = {o->mx, o->my, o->mz};
   const long P = o->P, N = (long)o->mx * o->my * o->mz;
@@ -760,15 +1030,17 @@ static void pv_direction(orc_ctx *o, int dir) {
   const int n = ext[dir];
   int hi[3] = {o->mx, o->my, o->mz};
   hi[dir] = 1;
-  double *fc = (double *)malloc(sizeof(double) * 5 * (n + 1));
+  const int nv = o->nv;
+  double *fc = (double *)malloc(sizeof(double) * nv * (n + 1));
   for (int a = 0; a < hi[0]; ++a)
     for (int b = 0; b < hi[1]; ++b)
       for (int cc = 0; cc < hi[2]; ++cc) {
         for (int idx = -1; idx < n; ++idx) {
-          double st[4][5], mt[2][3], jc[2], ed[2] = {0, 0};
+          double st[4][FVS_MAXV], mt[2][3], jc[2], ed[2] = {0, 0};
           for (int m = 0; m < 4; ++m) {
             const long p = ID(o, a + (idx - 1 + m) * e[0], b + (idx - 1 + m) * e[1], cc + (idx - 1 + m) * e[2]);
             for (int l = 0; l < 5; ++l) st[m][l] = o->bv[l * P + p];
+            for (int l = 0; l < o->ns; ++l) st[m][5 + l] = o->sv[l * P + p];
           }
           for (int s = 0; s < 2; ++s) {
             const long p = ID(o, a + (idx + s) * e[0], b + (idx + s) * e[1], cc + (idx + s) * e[2]);
@@ -776,9 +1048,22 @@ static void pv_direction(orc_ctx *o, int dir) {
             jc[s] = o->jac[p];
             if (o->c.riemann == 2) ed[s] = entropy_fix_delta(o, p);
           }
+          double *f = &fc[nv * (idx + 1)];
+          if (o->ns) {
+            double pl[PVM_MAX], pr[PVM_MAX];
+            pv_reconstruct_mix(o, st, o->c.reconstruction, pl, pr);
+            switch (o->c.riemann) {
+              case 2: roe_mix(o, pl, pr, mt, jc, ed[0], ed[1], f); break;
+              case 4: hllc_mix(o, pl, pr, mt, jc, f); break;
+              default: ausm_mix(o, pl, pr, mt, jc, f); break;
+            }
+            continue;
+          }
+          double st5[4][5];
+          for (int m = 0; m < 4; ++m)
+            for (int l = 0; l < 5; ++l) st5[m][l] = st[m][l];
           double pl[6], pr[6];
-          pv_reconstruct(st, o->c.reconstruction, pl, pr);
-          double *f = &fc[5 * (idx + 1)];
+          pv_reconstruct(st5, o->c.reconstruction, pl, pr);
           switch (o->c.riemann) {
             case 1: lax_friedrichs(pl, pr, mt, jc, f); break;
             case 2: roe(pl, pr, mt, jc, ed[0], ed[1], f); break;
@@ -788,7 +1073,7 @@ static void pv_direction(orc_ctx *o, int dir) {
         }
         for (int idx = 0; idx < n; ++idx) {
           const long q = IQ(o, a + idx * e[0], b + idx * e[1], cc + idx * e[2]);
-          for (int l = 0; l < 5; ++l) o->dq[l * N + q] -= fc[5 * (idx + 1) + l] - fc[5 * idx + l];
+          for (int l = 0; l < nv; ++l) o->dq[l * N + q] -= fc[nv * (idx + 1) + l] - fc[nv * idx + l];
         }
       }
   free(fc);
@@ -1288,7 +1573,6 @@ static void fvs_node_flux(const double *Q, int nv, const double *k, double jac, 
   }
 }
 
-#define FVS_MAXV (5 + ORC_MAX_SPEC)
 
 /* compute_weno_flux_ch<mixture> for inviscid_scheme 72 (WENO.cu:722-758, 899-965, 1119-1142):
  * Roe-averaged mixture eigensystem at the face, characteristic projection of the split fluxes of
@@ -1689,24 +1973,33 @@ static void bc_outflow(orc_ctx *o, const face_t *f) {
 
 /* apply_inflow with a constant state (BoundCond.cuh:483-613): the face node and its ghost layers
  * take the inflow state and mass fractions. */
+/* apply_inflow (BoundCond.cuh:235-613) without fluctuation: the face node and its ghost layers take
+ * the constant state, or (inflow_type 2) the upper / lower stream by the sign of the face node's y with
+ * u = (u1 + u2) / 2 + (u1 - u2) / 2 tanh(2 y / delta_omega) (BoundCond.cuh:384-400). */
 static void bc_inflow(orc_ctx *o, const face_t *f) {
   const long P = o->P;
   int dir[3] = {0, 0, 0};
   dir[f->face] = f->direction;
   for (int i = f->rs[0]; i <= f->re[0]; ++i)
     for (int j = f->rs[1]; j <= f->re[1]; ++j)
-      for (int k = f->rs[2]; k <= f->re[2]; ++k)
+      for (int k = f->rs[2]; k <= f->re[2]; ++k) {
+        double st[6] = {f->density, f->u, f->v, f->w, f->pressure, f->temperature};
+        const double *ys = f->y;
+        if (f->inflow_type == 2) {
+          const double yc = o->y[IC(o, i, j, k)];
+          if (yc < 0) {
+            for (int l = 0; l < 6; ++l) st[l] = f->lower[l];
+            ys = f->y_lower;
+          }
+          st[1] = 0.5 * (f->u + f->lower[1]) + 0.5 * (f->u - f->lower[1]) * tanh(2 * yc / f->delta_omega);
+        }
         for (int g = 0; g <= o->g; ++g) {
           const long pg = ID(o, i + g * dir[0], j + g * dir[1], k + g * dir[2]);
-          o->bv[pg] = f->density;
-          o->bv[P + pg] = f->u;
-          o->bv[2 * P + pg] = f->v;
-          o->bv[3 * P + pg] = f->w;
-          o->bv[4 * P + pg] = f->pressure;
-          o->bv[5 * P + pg] = f->temperature;
-          for (int l = 0; l < o->ns; ++l) o->sv[l * P + pg] = f->y[l];
+          for (int l = 0; l < 6; ++l) o->bv[l * P + pg] = st[l];
+          for (int l = 0; l < o->ns; ++l) o->sv[l * P + pg] = ys[l];
           cv_from_bv(o, pg);
         }
+      }
 }
 
 /* apply_back_pressure / apply_subsonic_inflow (BoundCond.cuh:1272-1441), air: the face node keeps its
@@ -2244,7 +2537,22 @@ static void load_state(orc_ctx *o, const double *bv, const double *sv) {
   memset(o->bv, 0, sizeof(double) * 6 * P);
   memset(o->cv, 0, sizeof(double) * o->nv * P);
   if (o->ns) memset(o->sv, 0, sizeof(double) * o->ns * P);
-  if (o->c.has_init) {
+  if (o->c.problem_type == 1) {
+    /* initialize_mixing_layer_with_info (Initialize.cu:259-326): the stream of each node's y */
+    const int gz = o->dim == 3 ? o->g : o->g;
+    for (int k = -gz; k < o->mz + gz; ++k)
+      for (int j = -o->g; j < o->my + o->g; ++j)
+        for (int i = -o->g; i < o->mx + o->g; ++i) {
+          const long p = ID(o, i, j, k);
+          const double yc = o->y[IC(o, i, j, k)];
+          const double *st = yc >= 0 ? o->c.ml_upper : o->c.ml_lower;
+          const double *ys = yc >= 0 ? o->c.ml_y_upper : o->c.ml_y_lower;
+          for (int l = 0; l < 6; ++l) o->bv[l * P + p] = st[l];
+          o->bv[P + p] = 0.5 * (o->c.ml_upper[1] + o->c.ml_lower[1]) +
+                         0.5 * (o->c.ml_upper[1] - o->c.ml_lower[1]) * tanh(2 * yc / o->c.ml_delta_omega);
+          for (int l = 0; l < o->ns; ++l) o->sv[l * P + p] = ys[l];
+        }
+  } else if (o->c.has_init) {
     for (int l = 0; l < 6; ++l)
       for (long p = 0; p < P; ++p) o->bv[l * P + p] = o->c.init_bv[l];
     for (int l = 0; l < o->ns; ++l)

@@ -31,6 +31,13 @@ typedef struct {
   /* constant inflow (type == ORC_INFLOW, Inflow ctor BoundCond.cpp:157-214): the state above and the
    * mass fractions of a mixture */
   double y[16];
+  /* inflow_type 2 (mixing-layer problems, BoundCond.cpp:10-98, apply_inflow BoundCond.cuh:384-430):
+   * the state above is the upper stream, `lower` (rho u v w p T) and y_lower the lower one, blended in
+   * u by tanh(2 y / delta_omega).  The white-noise fluctuation is not restated (curand). */
+  int inflow_type;
+  double delta_omega;
+  double lower[6];
+  double y_lower[16];
 } orc_face_in;
 
 /* Mixture tables (Species / Reaction, ChemData.cpp; DParameter.cu:57-155), row-major [i][j]. */
@@ -88,6 +95,10 @@ typedef struct {
    * step dt (the case's dt), inner iterations and their adaptation (inner_converged,
    * DualTimeStepping.cu:32-135) */
   int inner_iteration, max_inner_iteration, iteration_adjust_step;
+  /* problem_type 1: every node, ghosts included, starts from the two-stream profile
+   * (initialize_mixing_layer_with_info, Initialize.cu:259-326) instead of the default state */
+  int problem_type;
+  double ml_upper[6], ml_lower[6], ml_y_upper[ORC_MAX_SPEC], ml_y_lower[ORC_MAX_SPEC], ml_delta_omega;
 } orc_case;
 
 typedef struct orc_ctx orc_ctx;

@@ -32,5 +32,6 @@ $CXX $CXXFLAGS -c "$HERE/fmt_os_stub.cpp" -o "$OUT/fmt_os_stub.o"
 $NVCC $FLAGS -c "$HERE/ref_harness.cu" -o "$OUT/ref_harness.o"
 LINK="$NVCC -std=c++20 -gencode arch=compute_100a,code=sm_100a -rdc=true"
 $LINK "$OBJ"/*.o "$OUT/fmt_os_stub.o" -o "$OUT/openstc"
-$LINK $(ls "$OBJ"/*.o | grep -v '/main.cu.o$') "$OUT/fmt_os_stub.o" "$OUT/ref_harness.o" -o "$OUT/ref_harness"
+# the harness reads the clock through __wrap_time (OSTC_REF_TIME fixes the inflow noise seed)
+$LINK -Xlinker --wrap=time $(ls "$OBJ"/*.o | grep -v '/main.cu.o$') "$OUT/fmt_os_stub.o" "$OUT/ref_harness.o" -o "$OUT/ref_harness"
 echo "built $OUT/openstc $OUT/ref_harness"

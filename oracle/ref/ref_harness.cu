@@ -12,10 +12,25 @@
 // temporal_scheme = 2 its dual_time_stepping() (DualTimeStepping.cuh:32-252) for total_step steps - and writes the
 // interior cv[n_var], bv[6] and sv[n_spec] of every block, then the physical time, to state_out.bin.  It prints the
 // wall time of the RK3 call (steps, per-step output checks and the final flow-field file included).
+//
+// The reference seeds the generator states of a white-noise inflow with the clock (time(), in
+// DBoundCond::initialize_bc_on_GPU, BoundCond.cu:1731-1734).  build_ref.sh links this harness with
+// --wrap=time, so that with OSTC_REF_TIME set the clock reads that value and the run is repeatable.
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
+#include <ctime>
 #include <exception>
 #include <vector>
+
+extern "C" time_t __real_time(time_t *t);
+extern "C" time_t __wrap_time(time_t *t) {
+  const char *v = std::getenv("OSTC_REF_TIME");
+  if (!v) return __real_time(t);
+  const time_t r = (time_t)std::strtoll(v, nullptr, 10);
+  if (t) *t = r;
+  return r;
+}
 
 #include "Parameter.h"
 #include "Mesh.h"

@@ -20,6 +20,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 HARNESS = HERE / "_ref" / "ref_harness"
+# the clock value the harness reports to the reference (its inflow noise seed, BoundCond.cu:1731-1734);
+# a library run reproduces the noise with ostc_set_inflow_seed(REF_TIME)
+REF_TIME = 1700000000
 
 EXTRA = """
 // keys the reference reads without defaults (parity runs only)
@@ -80,11 +83,15 @@ def write_reference_case(case, steps: int, directory: os.PathLike, setup_extra: 
     bv0 = case.blocks[0].bv if hasattr(case, "blocks") else case.bv
     p0 = float(bv0[4].flat[0])
     t0 = float(bv0[5].flat[0])
-    setup += EXTRA
-    if not case.freestream:
+    ml = getattr(case, "mixing_layer", None)
+    # a mixing-layer case names its own delta_omega and its inflow struct `freestream` is the reference
+    # state (problem_type 1)
+    setup += EXTRA.replace("real delta_omega = 1e-3\n", "") if ml else EXTRA
+    own_fs = "freestream" in getattr(case, "bc_structs", {})
+    if not case.freestream and not own_fs:
         setup += FREESTREAM.replace("@MACH@", "0.5").replace("@P@", repr(p0)).replace("@T@", repr(t0))
     (inp / "setup.txt").write_text(setup)
-    if not case.freestream:
+    if not case.freestream and not own_fs:
         setup += "string reference_state = freestream\n"
     setup += setup_extra
     (inp / "setup.txt").write_text(setup)
@@ -108,7 +115,7 @@ def run_reference(case, steps: int, workdir: os.PathLike | None = None, timeout:
     d = Path(workdir) if workdir else Path(tempfile.mkdtemp(prefix="ostc_ref_"))
     write_reference_case(case, steps, d, setup_extra)
     r = subprocess.run([str(HARNESS), "state_in.bin", "state_out.bin"], cwd=d, capture_output=True, text=True,
-                       timeout=timeout)
+                       timeout=timeout, env=dict(os.environ, OSTC_REF_TIME=str(REF_TIME)))
     if r.returncode != 0:
         raise RuntimeError(f"reference harness failed ({r.returncode}):\n{r.stdout[-4000:]}\n{r.stderr[-3000:]}")
     raw = np.fromfile(d / "state_out.bin", dtype=np.float64)

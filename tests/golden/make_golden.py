@@ -81,6 +81,9 @@ CASES = [
     ("c3_rml3d_96x48x24_fr72", "reacting_mixing_layer_3d", dict(mx=96, my=48, mz=24), 20, dict(sampled=True)),
     # ... and a twelve-block chain of uneven i extents
     ("c4_mb3d_12_blocks", "multiblock_mixing_layer_3d", dict(dims=None, my=18, mz=8), 10),
+    # every block's three extents drawn; neighbours share the overlapping part of their x faces, the
+    # rest of each x face is an outflow patch
+    ("mb3d_uneven_axes", "multiblock_mixing_layer_3d", dict(nb=4, lo=8, hi=20, seed=3, uneven_axes=True), 10),
     # boundary faces beyond the mixing-layer set: no-slip walls, constant supersonic inflow, subsonic
     # inflow with back pressure (air), walls and inflow for the mixture
     ("ml3d_wall_isothermal", "mixing_layer_3d", dict(mx=32, my=24, mz=16, ybc="wall"), 10),
@@ -99,6 +102,26 @@ CASES = [
     ("rml3d_farfield_fr72", "reacting_mixing_layer_3d", dict(mx=32, my=20, mz=16, ybc="farfield"), 10),
     ("rml3d_farfield_mix71", "reacting_mixing_layer_3d",
      dict(mx=32, my=20, mz=16, ybc="farfield", inviscid_scheme=71, finite_rate=False), 10),
+    # mixtures on the primitive-reconstruction path (reconstruction<mixture> + AUSM+ / HLLC / Roe mixture
+    # branches), reacting and frozen, 3-D and 2-D, one with far-field faces
+    ("rml3d_muscl_ausm", "reacting_mixing_layer_3d", dict(mx=24, my=16, mz=10, inviscid_scheme=3), 5),
+    ("rml3d_nnd_hllc", "reacting_mixing_layer_3d",
+     dict(mx=24, my=16, mz=10, inviscid_scheme=4, reconstruction=3, finite_rate=False), 5),
+    ("rml3d_first_roe", "reacting_mixing_layer_3d", dict(mx=24, my=16, mz=10, inviscid_scheme=2, reconstruction=1), 5),
+    ("rml2d_muscl_roe", "reacting_mixing_layer_3d", dict(mx=40, my=24, mz=1, inviscid_scheme=2), 10),
+    ("rml3d_farfield_nnd_ausm", "reacting_mixing_layer_3d",
+     dict(mx=24, my=16, mz=10, ybc="farfield", inviscid_scheme=3, reconstruction=3), 5),
+    # spatial mixing layers (problem_type 1, the reference's shipped layout): the two-stream inflow
+    # profile, air and 9-species, 3-D and 2-D; with white noise on the inflow velocity (its generator
+    # seeded from the clock the harness fixes), also on a constant inflow
+    ("sml3d_air", "spatial_mixing_layer_3d", dict(mx=40, my=32, mz=8), 10),
+    ("sml2d_air", "spatial_mixing_layer_3d", dict(mx=48, my=40, mz=1), 15),
+    ("sml3d_species", "spatial_mixing_layer_3d", dict(mx=32, my=24, mz=6, species=True), 6),
+    ("sml3d_air_noise", "spatial_mixing_layer_3d", dict(mx=40, my=32, mz=8, fluctuation_type=1), 10),
+    ("sml2d_air_noise", "spatial_mixing_layer_3d", dict(mx=48, my=40, mz=1, fluctuation_type=1), 15),
+    ("sml3d_species_noise", "spatial_mixing_layer_3d",
+     dict(mx=32, my=24, mz=6, species=True, fluctuation_type=1, intensity=0.02), 6),
+    ("ml3d_inflow_noise", "mixing_layer_3d", dict(mx=32, my=20, mz=12, ybc="outflow", xbc="inflow", inflow_noise=0.01), 10),
     # the reference's steady driver (SteadySim.cuh): local time steps, explicit or DPLUR implicit
     # treatment (DPLUR.cuh), the chemical source explicit, point-implicit (EPI) or diagonal (DA).  No
     # wall case with DPLUR: the reference zeroes dq over the wall's ngg-padded range in an array with
@@ -114,6 +137,8 @@ CASES = [
      dict(mx=16, my=12, mz=8, steady=dict(STEADY, implicit_method=1, dplur_inner_step=2)), 5),
     ("st_rml3d_mix_dplur", "reacting_mixing_layer_3d",
      dict(mx=16, my=12, mz=8, finite_rate=False, steady=dict(STEADY, implicit_method=1)), 5),
+    ("st_rml3d_muscl_ausm_dplur_epi", "reacting_mixing_layer_3d",
+     dict(mx=16, my=12, mz=8, inviscid_scheme=3, steady=dict(STEADY, implicit_method=1, chem_src_method=1)), 5),
     # dual time stepping (DualTimeStepping.cuh, temporal_scheme 2): BDF2 physical steps of fixed dt, DPLUR
     # pseudo-time inner iterations whose count adapts every iteration_adjust_step-th step
     ("dt_ml3d", "mixing_layer_3d", dict(mx=24, my=20, mz=12, ybc="outflow", steady=dict(DUAL, dt=2e-7)), 6),
@@ -196,7 +221,8 @@ def main(outdir: Path, only=None) -> int:
         if only and name not in only:
             continue
         case = make_case(gen, kw)
-        meta = json.dumps({"generator": gen, "kwargs": kw})
+        # inflow_seed: the clock the harness reported to the reference (its white-noise inflow seed)
+        meta = json.dumps({"generator": gen, "kwargs": kw, "inflow_seed": refcase.REF_TIME})
         try:
             with tempfile.TemporaryDirectory(prefix="ostc_ref_") as wd:
                 cv, bv, t = refcase.run_reference(case, steps, wd, setup_extra=opts.get("setup", ""))[:3]

@@ -81,6 +81,11 @@ def load(path):
     return case, int(z["steps"]), z, float(z["t"])
 
 
+def noisy(kwargs) -> bool:
+    """Whether a fixture's case draws white inflow noise (the oracle does not restate the generator)."""
+    return kwargs.get("fluctuation_type", 0) == 1 or kwargs.get("inflow_noise", 0) > 0
+
+
 def meta(path):
     """(generator kwargs, steps, sampled, multi-block, mixture, node count) without building the case."""
     z = np.load(path)
@@ -129,9 +134,10 @@ def assert_state(cv, z, block=None, tol=(TOL, TOL)):
     assert all(m < tm and l2 < tl for m, l2 in err), err
 
 
-def run_library(case, steps, directory, setup_extra=""):
+def run_library(case, steps, directory, setup_extra="", inflow_seed=None):
     """Advances the case `steps` SSP-RK3 steps (or, for a steady case, steady-driver iterations; for
-    temporal_scheme 2, dual-time steps) through the C ABI; returns the open solver."""
+    temporal_scheme 2, dual-time steps) through the C ABI; returns the open solver.  inflow_seed: the
+    seed of a white-noise inflow (the clock value the reference read)."""
     import ostc
 
     d = oc.write_case(case, directory)
@@ -143,6 +149,8 @@ def run_library(case, steps, directory, setup_extra=""):
             s.set_state(blk.bv, block=b)
     else:
         s.set_state(case.bv, sv=case.sv)
+    if inflow_seed is not None:
+        s.set_inflow_seed(inflow_seed)
     if case.scheme.get("steady"):
         done, _ = s.steady(steps)
         assert done == steps
@@ -157,7 +165,8 @@ def check_library(case, steps, z, t_ref, directory, setup_extra="", name=None):
     """Runs the library and checks its state and time against the fixture (bars: tolerances(name));
     returns the solver."""
     tm, tl, tt = tolerances(name)
-    s = run_library(case, steps, directory, setup_extra)
+    seed = json.loads(str(z["case"])).get("inflow_seed")
+    s = run_library(case, steps, directory, setup_extra, inflow_seed=seed)
     if hasattr(case, "blocks"):
         for b in range(int(z["n_block"])):
             assert_state(s.get_state(block=b)[0], z, block=b, tol=(tm, tl))

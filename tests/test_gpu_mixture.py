@@ -1,7 +1,8 @@
 """The multi-component path (species = 1) on the GPU against the CPU oracle, through the C ABI: the
 9-species H2/air mechanism with finite-rate chemistry (MixtureModel FR) or without (Mixture), the
-flux-split characteristic WENO7-Z (inviscid_scheme 72) or component-wise WENO7-Z (71), mixture
-transport and the temperature Newton iteration.
+flux-split characteristic WENO7-Z (inviscid_scheme 72) or component-wise WENO7-Z (71), or the primitive
+reconstructions (1st order, MUSCL, NND2) with the mixture AUSM+, HLLC and Roe solvers, mixture transport
+and the temperature Newton iteration.
 
 Tolerance: 1e-12 relative per conserved variable (max norm; momentum against the momentum magnitude)
 for the RHS terms and for RK3 trajectories; the physical time to 1e-13.
@@ -32,8 +33,14 @@ def _rel(a, b, floor=0.0):
             float(np.max(np.abs(a[l] - b[l])) / max(np.max(np.abs(b[l])), floor)) for l in range(a.shape[0])]
 
 
+PV_SCHEMES = [dict(inviscid_scheme=3, reconstruction=2), dict(inviscid_scheme=4, reconstruction=3, finite_rate=False),
+              dict(inviscid_scheme=2, reconstruction=1), dict(inviscid_scheme=2, reconstruction=2),
+              dict(inviscid_scheme=4, reconstruction=1), dict(inviscid_scheme=3, reconstruction=3)]
+PV_IDS = ["muscl_ausm", "nnd_hllc_frozen", "first_roe", "muscl_roe", "first_hllc", "nnd_ausm"]
+
+
 @pytest.mark.parametrize("kw", [dict(inviscid_scheme=72), dict(inviscid_scheme=72, finite_rate=False),
-                                dict(inviscid_scheme=71)], ids=["fr72", "mix72", "fr71"])
+                                dict(inviscid_scheme=71)] + PV_SCHEMES, ids=["fr72", "mix72", "fr71"] + PV_IDS)
 def test_mixture_rhs_terms(built, tmp_path, kw):
     case = oc.reacting_mixing_layer_3d(mx=24, my=18, mz=12, **kw)
     s, o = _pair(case, tmp_path)
@@ -51,8 +58,12 @@ def test_mixture_rhs_terms(built, tmp_path, kw):
 
 @pytest.mark.parametrize("dims,kw,steps", [((24, 18, 12), dict(inviscid_scheme=72), 10),
                                            ((24, 18, 12), dict(inviscid_scheme=71, finite_rate=False), 10),
-                                           ((40, 24, 1), dict(inviscid_scheme=72), 20)],
-                         ids=["fr72_3d", "mix71_3d", "fr72_2d"])
+                                           ((40, 24, 1), dict(inviscid_scheme=72), 20),
+                                           ((24, 18, 12), PV_SCHEMES[0], 10), ((24, 18, 12), PV_SCHEMES[1], 10),
+                                           ((24, 18, 12), PV_SCHEMES[2], 10), ((40, 24, 1), PV_SCHEMES[3], 20),
+                                           ((40, 24, 1), PV_SCHEMES[1], 20)],
+                         ids=["fr72_3d", "mix71_3d", "fr72_2d", "muscl_ausm_3d", "nnd_hllc_3d", "first_roe_3d",
+                              "muscl_roe_2d", "nnd_hllc_2d"])
 def test_mixture_trajectory(built, tmp_path, dims, kw, steps):
     mx, my, mz = dims
     case = oc.reacting_mixing_layer_3d(mx=mx, my=my, mz=mz, **kw)

@@ -60,9 +60,9 @@ def test_unsupported_species_rejected(built, tmp_path):
     (d / "setup.txt").write_text(s.replace("int species = 0", "int species = 2"))
     with pytest.raises(ostc.OstcError, match="species = 2"):
         ostc.probe_case(str(d))
-    # species = 1 with an AWENO scheme: mixtures run the flux-split WENO7 path only
+    # species = 1 with an AWENO scheme: the reference's mixture AWENO is an empty stub
     (d / "setup.txt").write_text(s.replace("int species = 0", "int species = 1"))
-    with pytest.raises(ostc.OstcError, match="flux-split"):
+    with pytest.raises(ostc.OstcError, match="AWENO"):
         ostc.probe_case(str(d))
 
 
@@ -75,6 +75,15 @@ def test_mixture_probe_and_errors(built, tmp_path):
     # the reference's 52 reads outside its stencil: rejected with the reason
     (d / "setup.txt").write_text(setup.replace("int inviscid_scheme = 72", "int inviscid_scheme = 52"))
     with pytest.raises(ostc.OstcError, match="outside its stencil"):
+        ostc.probe_case(str(d))
+    # the primitive reconstructions with the mixture AUSM+ / HLLC / Roe: two ghost layers
+    for scheme, it in ((3, 0), (4, 0), (2, 2)):
+        (d / "setup.txt").write_text(setup.replace("int inviscid_scheme = 72", f"int inviscid_scheme = {scheme}"))
+        info = ostc.probe_case(str(d))
+        assert info["ngg"] == 2 and info["inviscid_type"] == it, scheme
+    # Lax-Friedrichs has no mixture form in the reference
+    (d / "setup.txt").write_text(setup.replace("int inviscid_scheme = 72", "int inviscid_scheme = 1"))
+    with pytest.raises(ostc.OstcError, match="Lax-Friedrichs"):
         ostc.probe_case(str(d))
     (d / "setup.txt").write_text(setup.replace("chemistry/H2_mech.inp", "chemistry/missing.inp"))
     with pytest.raises(ostc.OstcError, match="cannot open") as e:
@@ -140,10 +149,21 @@ def test_boundary_faces_probe(built, tmp_path):
     rad.bc_structs["wall"]["thermal_type"] = ("string", "equilibrium_radiation")
     with pytest.raises(ostc.OstcError, match="equilibrium_radiation"):
         ostc.probe_case(str(oc.write_case(rad, tmp_path / "rad")))
-    fl = oc.mixing_layer_3d(mx=12, my=10, mz=8, xbc="inflow")
-    fl.bc_structs["inflow"]["fluctuation_type"] = ("int", 1)
-    with pytest.raises(ostc.OstcError, match="fluctuation_type"):
-        ostc.probe_case(str(oc.write_case(fl, tmp_path / "fl")))
+    # white noise (1) is on the path; stability-mode (2), receptivity (3) fluctuations and profile-file
+    # inflows are refused
+    fl = oc.mixing_layer_3d(mx=12, my=10, mz=8, xbc="inflow", inflow_noise=0.01)
+    assert ostc.probe_case(str(oc.write_case(fl, tmp_path / "fl1")))["n_faces"] == len(fl.faces)
+    for key, val in (("fluctuation_type", 2), ("fluctuation_type", 3), ("inflow_type", 1)):
+        fl = oc.mixing_layer_3d(mx=12, my=10, mz=8, xbc="inflow")
+        fl.bc_structs["inflow"][key] = ("int", val)
+        with pytest.raises(ostc.OstcError, match=key):
+            ostc.probe_case(str(oc.write_case(fl, tmp_path / f"fl_{key}_{val}")))
+    # a mixing-layer problem (problem_type 1) parses its streams; without them it is refused
+    ml = oc.spatial_mixing_layer_3d(mx=12, my=10, mz=6, fluctuation_type=1)
+    assert ostc.probe_case(str(oc.write_case(ml, tmp_path / "ml")))["n_faces"] == len(ml.faces)
+    del ml.mixing_layer["lower"]["temperature"]
+    with pytest.raises(ostc.OstcError, match="temperature"):
+        ostc.probe_case(str(oc.write_case(ml, tmp_path / "ml_bad")))
     for key in ("pt_pRef_ratio", "Tt_TRef_ratio"):
         sub = oc.mixing_layer_3d(mx=12, my=10, mz=8, xbc="subsonic", ybc="outflow")
         del sub.bc_structs["subsonic_inflow"][key]

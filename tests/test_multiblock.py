@@ -68,3 +68,48 @@ def test_gpu_multiblock_matches_oracle(built, tmp_path, dims, my, mz, recon, rs,
         err = oc.relative_errors(cg, co)
         assert all(mx < TOL and l2 < TOL for mx, l2 in err), (b, err)
     assert s.error_flags() == 0
+
+
+def _solver(mc, path):
+    import ostc
+
+    s = ostc.Solver(str(oc.write_case(mc, path)))
+    for b, blk in enumerate(mc.blocks):
+        s.set_state(blk.bv, block=b)
+    return s
+
+
+@pytest.mark.gpu
+def test_gpu_uneven_axes_matches_oracle(built, tmp_path):
+    """Every block's three extents differ: interfaces cover the overlap of neighbouring x faces and the
+    rest of each x face is an outflow patch (faces and interfaces on sub-ranges of a side)."""
+    mc = oc.multiblock_mixing_layer_3d(nb=5, lo=10, hi=24, seed=11, uneven_axes=True)
+    assert len({(b.my, b.mz) for b in mc.blocks}) > 1
+    s = _solver(mc, tmp_path / "mb")
+    m = MultiOracle(mc)
+    m.set_state()
+    s.step(8)
+    m.step(8)
+    assert abs(s.time() - m.time()) <= 1e-13 * m.time()
+    for b in range(len(mc.blocks)):
+        err = oc.relative_errors(s.get_state(block=b)[0], m.blocks[b].get_state()[0])
+        assert all(mx < TOL and l2 < TOL for mx, l2 in err), (b, err)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("uneven", [False, True], ids=["chain", "uneven_axes"])
+def test_block_loop_equals_graph(built, tmp_path, uneven):
+    """The per-block launch loop (kernels launched from the host, block after block) and the captured
+    step graph (blocks forked onto side streams) give the same state bit for bit."""
+    import ostc
+
+    mc = (oc.multiblock_mixing_layer_3d(nb=4, lo=10, hi=22, seed=5, uneven_axes=True) if uneven else
+          oc.multiblock_mixing_layer_3d(dims=[20, 17, 23, 19], my=14, mz=9))
+    out = []
+    for mode in (ostc.LAUNCH_GRAPH, ostc.LAUNCH_BLOCK_LOOP):
+        s = _solver(mc, tmp_path / f"m{mode}")
+        s.set_launch_mode(mode)
+        s.step(6)
+        out.append([s.get_state(block=b)[0] for b in range(len(mc.blocks))] + [s.time()])
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
