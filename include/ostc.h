@@ -268,6 +268,16 @@ int ostc_read_plt(ostc_ctx *ctx, const char *path, double *solution_time);
 #define OSTC_STAT_REY_W 4u
 #define OSTC_STAT_REY_T 8u
 #define OSTC_STAT_RHO_P 16u
+/* The additional collectors (collect_single_point_additional_statistics, SinglePointStat.cu:707-722),
+ * over interior nodes, exported as tke_budget.bin, species_velocity_correlation.bin and
+ * species_dissipation_rate.bin (stat groups 4, 5, 6; ostc_stat_get reads them too):
+ *   group 4 TKE budget: tau11 tau12 tau13 tau22 tau23 tau33, tau_ij dU_i/dx_j (stat_tke_budget)
+ *   group 5 per species: rho u Y, rho v Y, rho w Y (stat_species_velocity_correlation)
+ *   group 6 per species: rho D |grad Y|^2, rho D dY/dx, dY/dy, dY/dz, rho D (stat_species_dissipation_rate)
+ * Through ostc_stat_enable the species groups cover every species; the setup's stat_species selects. */
+#define OSTC_STAT_TKE_BUDGET 32u
+#define OSTC_STAT_SPECIES_VELOCITY 64u
+#define OSTC_STAT_SPECIES_DISSIPATION 128u
 
 /* Allocate and zero the accumulators of every block and collect after each later step (ostc_rk3_step,
  * ostc_timed_steps, ostc_profile_steps) whose index, counted from this call starting at 1, exceeds
@@ -278,9 +288,12 @@ int ostc_stat_disable(ostc_ctx *ctx);
 /* Variables per group (n_var[4]), collections so far (the reference's per-variable counters, all
  * equal here) and steps counted since enabling.  OSTC_ESTATE when collection is off. */
 int ostc_stat_info(ostc_ctx *ctx, int n_var[4], int *n_collected, long long *steps);
-/* Copy group g (0..3) of block b: n_var x (mx+2)(my+2)(mz+2) doubles, layout as above, to host or
- * device memory (ptr_kind).  Synchronises. */
+/* Copy group g of block b to host or device memory (ptr_kind): groups 0..3 n_var x (mx+2)(my+2)(mz+2)
+ * doubles, groups 4..6 n_var x mx my mz (no ghost layer; n_var from ostc_stat_group_vars, 0 when the
+ * collector is off), layout as above.  Synchronises. */
 int ostc_stat_get(ostc_ctx *ctx, int block, int group, double *out, int ptr_kind);
+/* Number of variables of statistics group g (0..6) in the current selection. */
+int ostc_stat_group_vars(ostc_ctx *ctx, int group, int *n_var);
 /* Write coll_rey_1st.bin, coll_fav_1st.bin, coll_rey_2nd.bin, coll_fav_2nd.bin into dir in the
  * reference's layout (SinglePointStat.cu:163-226, 553-638, one process): int32 n_block, n_var, ngg = 1;
  * the variable names as int32 characters, each ended by an int32 0; int32 counters[n_var]; then per

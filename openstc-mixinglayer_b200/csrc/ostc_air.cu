@@ -1553,6 +1553,8 @@ struct BlockRes {
   double *last = nullptr;
   std::vector<DevFace> faces;  // file order
   std::vector<double *> face_y;  // per face: y of its nodes (mixing-layer inflows), else null
+  double *plt_xyz = nullptr;     // flow-field output: the zone's coordinates for output width plt_g
+  int plt_g = -1;
   double *ycoord = nullptr;      // problem_type 1: y of every padded node (the initial profile)
   std::vector<DevInner> inner;  // interfaces of this block, file order
   int yz_var[2][2] = {{-1, -1}, {-1, -1}};  // autotuned y / z sweep variant [FP64, mixed][y, z]
@@ -2767,7 +2769,14 @@ int enqueue_steady_iteration(ostc_ctx *ctx, double dt_phys = 0.0) {
 
 extern "C" {
 
-static int stat_setup(ostc_ctx *ctx, int start_step, const std::vector<int> &rey_idx, bool rho_p);
+// The additional collectors of a statistics selection: the TKE budget, and for the species ss_idx
+// (indices into the mechanism) their velocity correlation and dissipation rate.
+struct StatExtras {
+  bool tke = false, svc = false, sdr = false;
+  std::vector<int> ss_idx;
+};
+static int stat_setup(ostc_ctx *ctx, int start_step, const std::vector<int> &rey_idx, bool rho_p,
+                      const StatExtras &ex = StatExtras());
 
 int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_ctx **out) {
   if (!out || !input_dir) {
@@ -3142,8 +3151,30 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
         else
           idx.push_back(q);
       }
+    // the additional collectors (SinglePointStat.cu:27-96): stat_tke_budget, and for the species of
+    // stat_species ("all", or names; unknown names skipped with a message) their velocity correlation
+    // and dissipation rate
+    StatExtras ex;
+    ex.tke = ctx->setup.get_bool("stat_tke_budget");
+    ex.svc = ctx->setup.get_bool("stat_species_velocity_correlation");
+    ex.sdr = ctx->setup.get_bool("stat_species_dissipation_rate");
+    auto ss = ctx->setup.string_arrays.find("stat_species");
+    if (ctx->mixture && ss != ctx->setup.string_arrays.end()) {
+      if (std::find(ss->second.begin(), ss->second.end(), "all") != ss->second.end()) {
+        for (int l = 0; l < ctx->der.n_spec; ++l) ex.ss_idx.push_back(l);
+      } else {
+        for (const auto &name : ss->second) {
+          auto f = std::find(ctx->chem.names.begin(), ctx->chem.names.end(), name);
+          if (f == ctx->chem.names.end())
+            std::fprintf(stderr, "ostc: species %s is not in the mechanism; its statistics are not collected\n",
+                         name.c_str());
+          else
+            ex.ss_idx.push_back((int)(f - ctx->chem.names.begin()));
+        }
+      }
+    }
     if (int r = stat_setup(ctx.get(), ctx->setup.get_int("start_collect_statistics_iter"), idx,
-                           ctx->setup.get_bool("rho_p_correlation"))) {
+                           ctx->setup.get_bool("rho_p_correlation"), ex)) {
       g_create_error = ctx->err;
       ostc_destroy(ctx.release());
       return r;
@@ -3178,6 +3209,7 @@ void ostc_destroy(ostc_ctx *ctx) {
     cudaFree(B.fcb);
     cudaFree(B.efd);
     cudaFree(B.ycoord);
+    cudaFree(B.plt_xyz);
     for (double *p : B.face_y) cudaFree(p);
     for (int s = 0; s < 4; ++s) {
       cudaFree(B.cv[s]);
@@ -3631,17 +3663,27 @@ static std::vector<std::string> stat_names(const ostc_ctx *ctx, int g) {
   } else if (g == 2) {
     v = {"RhoRho", "pp"};
     if (sp.rho_p) v.push_back("rhoP");
-  } else {
+  } else if (g == 3) {
     v = {"rhoUU", "rhoVV", "rhoWW", "rhoUV", "rhoUW", "rhoVW", "rhoTT"};
     for (int l = 0; l < sp.ns; ++l) v.push_back("rho" + ctx->chem.names[l] + ctx->chem.names[l]);
+  } else if (g == 4) {
+    // TkeBudget::collect_name (TkeBudget.cuh:9-12)
+    if (sp.tke) v = {"Tau11", "Tau12", "Tau13", "Tau22", "Tau23", "Tau33", "TauIjDUiDXj"};
+  } else {
+    // SpeciesVelocityCorrelation / SpeciesDissipationRate::collect_name with the species name appended,
+    // species outer (create_species_collect_file, SpeciesStat.cuh:176-205)
+    static const char *const kSvc[3] = {"rhoUY", "rhoVY", "rhoWY"};
+    static const char *const kSdr[5] = {"rhoDdYDxdYDx", "rhoDdYDx", "rhoDdYDy", "rhoDdYDz", "rhoD"};
+    if (stat_group_vars(sp, g) > 0)
+      for (int q = 0; q < sp.nss; ++q)
+        for (int c = 0; c < (g == 5 ? 3 : 5); ++c)
+          v.push_back(std::string(g == 5 ? kSvc[c] : kSdr[c]) + ctx->chem.names[sp.ss_idx[q]]);
   }
   return v;
 }
 
 static long long stat_block_doubles(const ostc_ctx *ctx, const BlockRes &B) {
-  int nvar = 0;
-  for (int g = 0; g < 4; ++g) nvar += stat_group_vars(ctx->stat_spec, g);
-  return nvar * stat_points(B.db);
+  return stat_group_offset(ctx->stat_spec, B.db, kStatGroups);
 }
 
 static void stat_free(ostc_ctx *ctx) {
@@ -3653,10 +3695,15 @@ static void stat_free(ostc_ctx *ctx) {
 }
 
 // (Re)allocate and zero the accumulators for the selection rey_idx (primitive indices of the extra
-// Reynolds averages, in the order given) and rho_p.
-static int stat_setup(ostc_ctx *ctx, int start_step, const std::vector<int> &rey_idx, bool rho_p) {
+// Reynolds averages, in the order given), rho_p and the additional collectors.
+static int stat_setup(ostc_ctx *ctx, int start_step, const std::vector<int> &rey_idx, bool rho_p,
+                      const StatExtras &ex) {
   if (start_step < 0 || rey_idx.size() > 4) {
     ctx->err = "ostc_stat_enable: start_step must be >= 0 and at most 4 extra Reynolds averages";
+    return OSTC_EINVAL;
+  }
+  if (ex.ss_idx.size() > 16) {
+    ctx->err = "ostc_stat_enable: at most 16 species for the species statistics";
     return OSTC_EINVAL;
   }
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
@@ -3666,6 +3713,12 @@ static int stat_setup(ostc_ctx *ctx, int start_step, const std::vector<int> &rey
   for (int l = 0; l < sp.n_rey; ++l) sp.rey_idx[l] = rey_idx[l];
   sp.rho_p = rho_p ? 1 : 0;
   sp.ns = ctx->der.n_spec;
+  sp.tke = ex.tke ? 1 : 0;
+  // the species collectors need species to collect (SinglePointStat.cu:87-96)
+  sp.nss = (int)ex.ss_idx.size();
+  sp.svc = ex.svc && sp.nss > 0 ? 1 : 0;
+  sp.sdr = ex.sdr && sp.nss > 0 ? 1 : 0;
+  for (int q = 0; q < sp.nss; ++q) sp.ss_idx[q] = ex.ss_idx[q];
   ctx->stat_spec = sp;
   for (auto &B : ctx->blk)
     if (stat_points(B.db) >= (1LL << 31)) {
@@ -3693,10 +3746,13 @@ static int stat_setup(ostc_ctx *ctx, int start_step, const std::vector<int> &rey
 static int stat_after_step(ostc_ctx *ctx) {
   if (!ctx->stat_on) return OSTC_OK;
   if (++ctx->stat_steps <= ctx->stat_start) return OSTC_OK;
+  const StatSpec &sp = ctx->stat_spec;
   for (auto &B : ctx->blk) {
     long tok = begin_t(ctx, "statistics");
-    k_stat_collect<<<grid_for(ctx, stat_points(B.db), 256), 256, 0, ctx->stream>>>(B.db, state_of(B, 0), B.stat,
-                                                                                   ctx->stat_spec);
+    k_stat_collect<<<grid_for(ctx, stat_points(B.db), 256), 256, 0, ctx->stream>>>(B.db, state_of(B, 0), B.stat, sp);
+    if (sp.tke || sp.svc || sp.sdr)
+      k_stat_extra<<<grid_for(ctx, B.db.n, 128), 128, 0, ctx->stream>>>(B.db, state_of(B, 0),
+                                                                         B.stat + stat_group_offset(sp, B.db, 4), sp);
     end_t(ctx, tok);
   }
   CK(cudaGetLastError());
@@ -3704,8 +3760,10 @@ static int stat_after_step(ostc_ctx *ctx) {
   return OSTC_OK;
 }
 
-static const char *const kStatFiles[4] = {"coll_rey_1st.bin", "coll_fav_1st.bin", "coll_rey_2nd.bin",
-                                          "coll_fav_2nd.bin"};
+static const char *const kStatFiles[kStatGroups] = {"coll_rey_1st.bin", "coll_fav_1st.bin", "coll_rey_2nd.bin",
+                                                    "coll_fav_2nd.bin", "tke_budget.bin",
+                                                    "species_velocity_correlation.bin",
+                                                    "species_dissipation_rate.bin"};
 
 static int ensure_graph(ostc_ctx *ctx) {
   if (!ctx->graph || ctx->graph_precision != ctx->precision) {
@@ -3982,6 +4040,75 @@ int ostc_bounds_checked(void) {
 
 // ---------------------------------------------------------------- Tecplot flow-field file
 
+// The zone data of one block in the flow-field file's layout, packed on the device
+// (FieldIO::print_field, FieldIO.h:560-648): variable-major arrays over the (mx+2g)(my+2g)(mz+2g) output
+// nodes, i fastest; x, y, z from xyz (the same layout), then rho u v w p T, the Mach number as
+// update_physical_properties stores it (FieldOperation.cuh:107-140: |V| over the mixture speed of sound,
+// or over sqrt(gamma R T) for air) and the mass fractions.  2-D blocks hold no k ghosts: their output k
+// layers repeat k = 0, the copies eliminate_k_gradient makes in the reference.
+__global__ void k_plt_pack(DevBlock b, DevState s, const double *__restrict__ xyz, int g, int ns, int mixture,
+                           double *__restrict__ out) {
+  const int nx = b.mx + 2 * g, ny = b.my + 2 * g, nz = b.mz + 2 * g;
+  const long long npt = (long long)nx * ny * nz, P = b.plane;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < npt; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % nx) - g;
+    const long long r = q / nx;
+    const int j = (int)(r % ny) - g, k = (int)(r / ny) - g;
+    const long long p = b.id(i, j, b.gz ? k : 0);
+    out[q] = xyz[q];
+    out[npt + q] = xyz[npt + q];
+    out[2 * npt + q] = xyz[2 * npt + q];
+    for (int l = 0; l < 6; ++l) out[(3 + l) * npt + q] = s.bv[l * P + p];
+    const double u = s.bv[P + p], v = s.bv[2 * P + p], w = s.bv[3 * P + p];
+    const double vel = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v)), __dmul_rn(w, w)));
+    out[9 * npt + q] = mixture ? vel / s.acs[p] : vel / sqrt(kGammaAir * kRu / kMwAir * s.bv[5 * P + p]);
+    for (int l = 0; l < ns; ++l) out[(10 + l) * npt + q] = s.sv[l * P + p];
+  }
+}
+
+// Per-block partial minima and maxima of every packed variable (the file's min/max pairs): block x of
+// row y covers variable y; part[(y * gridDim.x + x) * 2 + 0/1].
+__global__ void __launch_bounds__(256) k_plt_minmax(const double *__restrict__ a, long long npt, double *__restrict__ part) {
+  __shared__ double smin[256], smax[256];
+  const double *v = a + (long long)blockIdx.y * npt;
+  double mn = v[0], mxv = v[0];
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < npt; q += (long long)gridDim.x * blockDim.x) {
+    mn = fmin(mn, v[q]);
+    mxv = fmax(mxv, v[q]);
+  }
+  smin[threadIdx.x] = mn;
+  smax[threadIdx.x] = mxv;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) {
+      smin[threadIdx.x] = fmin(smin[threadIdx.x], smin[threadIdx.x + h]);
+      smax[threadIdx.x] = fmax(smax[threadIdx.x], smax[threadIdx.x + h]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const long long o = ((long long)blockIdx.y * gridDim.x + blockIdx.x) * 2;
+    part[o] = smin[0];
+    part[o + 1] = smax[0];
+  }
+}
+
+// The interior primitive state and mass fractions of one zone read from a flow-field file (its
+// selected variable columns cols[6 + ns][npt] staged on the device) into [6][N] and [ns][N].
+__global__ void k_plt_gather(DevBlock b, int g, int ns, const double *__restrict__ cols, double *__restrict__ bv,
+                             double *__restrict__ sv) {
+  const int nx = b.mx + 2 * g, ny = b.my + 2 * g;
+  const long long npt = (long long)nx * ny * (b.mz + 2 * g);
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % b.mx);
+    const long long r = n / b.mx;
+    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const long long q = ((long long)(k + g) * ny + (j + g)) * nx + (i + g);
+    for (int l = 0; l < 6; ++l) bv[l * b.n + n] = cols[l * npt + q];
+    for (int l = 0; l < ns; ++l) sv[l * b.n + n] = cols[(6 + l) * npt + q];
+  }
+}
+
 // Variable names of the flow-field file: FieldIO::acquire_variable_names (FieldIO.h:450-488) for a
 // laminar air or mixture case without user-defined output (UDIO.cu:9-33).
 static std::vector<std::string> plt_names(const ostc_ctx *ctx) {
@@ -4037,55 +4164,71 @@ int ostc_write_plt(ostc_ctx *ctx, const char *path, int ngg_out, double solution
   }
   put_f(357.0f);
   // data sections (write_common_data_section + print_field, FieldIO.h:222-648): per zone the
-  // formats, the min/max pairs and the node arrays of x, y, z, bv, mach, Y_k
-  std::vector<double> pl;
+  // formats, the min/max pairs and the node arrays of x, y, z, bv, mach, Y_k - packed and reduced on
+  // the device, then one copy of the packed zone into the file image
   for (size_t b = 0; b < ctx->blk.size(); ++b) {
     BlockRes &B = ctx->blk[b];
     const DevBlock &db = B.db;
-    const HostBlock &hb = ctx->mesh.blocks[b];
-    const long long P = db.plane;
-    const int nl = 6 + ns + (ctx->mixture ? 1 : 0);
-    pl.resize((size_t)nl * P);
-    CK(cudaMemcpy(pl.data(), B.bv[0], 6 * P * sizeof(double), cudaMemcpyDeviceToHost));
-    if (ns) CK(cudaMemcpy(pl.data() + 6 * P, B.sv[0], (size_t)ns * P * sizeof(double), cudaMemcpyDeviceToHost));
-    if (ctx->mixture) CK(cudaMemcpy(pl.data() + (6 + ns) * P, B.acs[0], P * sizeof(double), cudaMemcpyDeviceToHost));
     const int nx = db.mx + 2 * g, ny = db.my + 2 * g, nz = db.mz + 2 * g;
     const long long npt = (long long)nx * ny * nz;
-    std::vector<double> a((size_t)nvar * npt);
-    for (int k = -g; k < db.mz + g; ++k)
-      for (int j = -g; j < db.my + g; ++j)
-        for (int i = -g; i < db.mx + g; ++i) {
-          const long long q = ((long long)(k + g) * ny + (j + g)) * nx + (i + g);
-          // 2-D blocks hold no k ghosts: the reference's k layers are copies of k = 0
-          const long long p = db.id(i, j, db.gz ? k : 0);
-          const long c = hb.cidx(i, j, k);
-          a[q] = hb.x[c];
-          a[npt + q] = hb.y[c];
-          a[2 * npt + q] = hb.z[c];
-          for (int l = 0; l < 6; ++l) a[(3 + l) * npt + q] = pl[l * P + p];
-          // Mach number as update_physical_properties stores it (FieldOperation.cuh:107-140)
-          const double u = pl[P + p], v = pl[2 * P + p], w = pl[3 * P + p];
-          const double vel = std::sqrt(u * u + v * v + w * w);
-          a[9 * npt + q] = ctx->mixture ? vel / pl[(6 + ns) * P + p]
-                                        : vel / std::sqrt(kGammaAir * kRu / kMwAir * pl[5 * P + p]);
-          for (int l = 0; l < ns; ++l) a[(10 + l) * npt + q] = pl[(6 + l) * P + p];
-        }
+    if (!B.plt_xyz || B.plt_g != g) {
+      // the zone's coordinates (ghost grid included) uploaded once per output width
+      const HostBlock &hb = ctx->mesh.blocks[b];
+      std::vector<double> xyz(3 * (size_t)npt);
+      for (int k = -g; k < db.mz + g; ++k)
+        for (int j = -g; j < db.my + g; ++j)
+          for (int i = -g; i < db.mx + g; ++i) {
+            const long long q = ((long long)(k + g) * ny + (j + g)) * nx + (i + g);
+            const long c = hb.cidx(i, j, k);
+            xyz[q] = hb.x[c];
+            xyz[npt + q] = hb.y[c];
+            xyz[2 * npt + q] = hb.z[c];
+          }
+      cudaFree(B.plt_xyz);
+      B.plt_xyz = nullptr;
+      CK(cudaMalloc(&B.plt_xyz, xyz.size() * sizeof(double)));
+      CK(cudaMemcpy(B.plt_xyz, xyz.data(), xyz.size() * sizeof(double), cudaMemcpyHostToDevice));
+      B.plt_g = g;
+    }
+    double *dev = nullptr, *part = nullptr;
+    const int nb = (int)std::min<long long>(256, (npt + 255) / 256);
+    if (cudaMalloc(&dev, (size_t)nvar * npt * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&part, (size_t)nvar * nb * 2 * sizeof(double)) != cudaSuccess) {
+      cudaFree(dev);
+      ctx->err = "ostc_write_plt: device allocation for the packed zone failed";
+      return OSTC_ENOMEM;
+    }
+    k_plt_pack<<<grid_for(ctx, npt, 256), 256, 0, ctx->stream>>>(db, state_of(B, 0), B.plt_xyz, g, ns,
+                                                                  ctx->mixture ? 1 : 0, dev);
+    k_plt_minmax<<<dim3(nb, nvar), 256, 0, ctx->stream>>>(dev, npt, part);
+    std::vector<double> hp((size_t)nvar * nb * 2);
+    const cudaError_t e1 = cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                           ctx->stream);
     put_f(299.0f);
     for (int l = 0; l < nvar; ++l) put_i(2);
     put_i(0);
     put_i(0);
     put_i(-1);
+    const cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
     for (int l = 0; l < nvar; ++l) {
-      const double *v = &a[(size_t)l * npt];
-      double mn = v[0], mxv = v[0];
-      for (long long q = 1; q < npt; ++q) {
-        mn = std::min(mn, v[q]);
-        mxv = std::max(mxv, v[q]);
+      double mn = hp[(size_t)l * nb * 2], mxv = hp[(size_t)l * nb * 2 + 1];
+      for (int x = 1; x < nb; ++x) {
+        mn = std::min(mn, hp[((size_t)l * nb + x) * 2]);
+        mxv = std::max(mxv, hp[((size_t)l * nb + x) * 2 + 1]);
       }
       put_d(mn);
       put_d(mxv);
     }
-    put(a.data(), a.size() * sizeof(double));
+    const size_t at = buf.size();
+    buf.resize(at + (size_t)nvar * npt * sizeof(double));
+    const cudaError_t e3 =
+        cudaMemcpy(buf.data() + at, dev, (size_t)nvar * npt * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(dev);
+    cudaFree(part);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+      ctx->err = "ostc_write_plt: device packing failed";
+      return OSTC_ECUDA;
+    }
   }
   FILE *f = std::fopen(path, "wb");
   if (!f) {
@@ -4195,16 +4338,25 @@ int ostc_read_plt(ostc_ctx *ctx, const char *path, double *solution_time) {
     if (bad || pos + (size_t)nvar * npt * 8 > buf.size()) return fail("truncated zone data");
     const char *a = buf.data() + pos;
     pos += (size_t)nvar * npt * 8;
+    // the zone's primitive and species columns go to the device as they lie in the file; the interior
+    // is gathered there and set as the block's state
     const long long N = db.n;
-    std::vector<double> bv(6 * N), sv((size_t)ns * N);
-    for (int k = 0; k < db.mz; ++k)
-      for (int j = 0; j < db.my; ++j)
-        for (int i = 0; i < db.mx; ++i) {
-          const long long q = ((long long)(k + g) * ny + (j + g)) * nx + (i + g), n = db.iq(i, j, k);
-          for (int l = 0; l < 6; ++l) std::memcpy(&bv[l * N + n], a + ((size_t)col[l] * npt + q) * 8, 8);
-          for (int l = 0; l < ns; ++l) std::memcpy(&sv[l * N + n], a + ((size_t)col[6 + l] * npt + q) * 8, 8);
-        }
-    if (int r = ostc_set_state(ctx, (int)b, bv.data(), ns ? sv.data() : nullptr, OSTC_HOST)) return r;
+    double *cols = nullptr, *st = nullptr;
+    if (cudaMalloc(&cols, (size_t)(6 + ns) * npt * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&st, (size_t)(6 + ns) * N * sizeof(double)) != cudaSuccess) {
+      cudaFree(cols);
+      ctx->err = "ostc_read_plt: device allocation for the zone failed";
+      return OSTC_ENOMEM;
+    }
+    bool okc = true;
+    for (int l = 0; l < 6 + ns && okc; ++l)
+      okc = cudaMemcpyAsync(cols + (size_t)l * npt, a + (size_t)col[l] * npt * 8, npt * sizeof(double),
+                            cudaMemcpyHostToDevice, ctx->stream) == cudaSuccess;
+    if (okc) k_plt_gather<<<grid_for(ctx, N, 256), 256, 0, ctx->stream>>>(db, g, ns, cols, st, st + 6 * N);
+    const int r = okc ? ostc_set_state(ctx, (int)b, st, ns ? st + 6 * N : nullptr, OSTC_DEVICE) : OSTC_ECUDA;
+    cudaFree(cols);
+    cudaFree(st);
+    if (r) return r;
   }
   // the physical time continues from the file's solution time
   CK(cudaMemcpyAsync(ctx->d_time, &t0, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
@@ -4215,7 +4367,7 @@ int ostc_read_plt(ostc_ctx *ctx, const char *path, double *solution_time) {
 
 int ostc_stat_enable(ostc_ctx *ctx, int start_step, unsigned flags) {
   if (!ctx) return OSTC_EINVAL;
-  if (flags & ~31u) {
+  if (flags & ~255u) {
     ctx->err = "ostc_stat_enable: unknown flag bits";
     return OSTC_EINVAL;
   }
@@ -4225,7 +4377,12 @@ int ostc_stat_enable(ostc_ctx *ctx, int start_step, unsigned flags) {
   if (flags & OSTC_STAT_REY_V) idx.push_back(2);
   if (flags & OSTC_STAT_REY_W) idx.push_back(3);
   if (flags & OSTC_STAT_REY_T) idx.push_back(5);
-  return stat_setup(ctx, start_step, idx, (flags & OSTC_STAT_RHO_P) != 0);
+  StatExtras ex;
+  ex.tke = (flags & OSTC_STAT_TKE_BUDGET) != 0;
+  ex.svc = (flags & OSTC_STAT_SPECIES_VELOCITY) != 0;
+  ex.sdr = (flags & OSTC_STAT_SPECIES_DISSIPATION) != 0;
+  for (int l = 0; l < ctx->der.n_spec; ++l) ex.ss_idx.push_back(l);  // every species ("all")
+  return stat_setup(ctx, start_step, idx, (flags & OSTC_STAT_RHO_P) != 0, ex);
 }
 
 int ostc_stat_disable(ostc_ctx *ctx) {
@@ -4248,18 +4405,28 @@ int ostc_stat_info(ostc_ctx *ctx, int n_var[4], int *n_collected, long long *ste
   return OSTC_OK;
 }
 
+int ostc_stat_group_vars(ostc_ctx *ctx, int group, int *n_var) {
+  if (!ctx || !n_var || group < 0 || group >= kStatGroups) return OSTC_EINVAL;
+  if (!ctx->stat_on) {
+    ctx->err = "statistics collection is off (ostc_stat_enable, or if_collect_statistics in the setup)";
+    return OSTC_ESTATE;
+  }
+  *n_var = stat_group_vars(ctx->stat_spec, group);
+  return OSTC_OK;
+}
+
 int ostc_stat_get(ostc_ctx *ctx, int block, int group, double *out, int ptr_kind) {
-  if (!ctx || !out || block < 0 || block >= (int)ctx->blk.size() || group < 0 || group > 3) return OSTC_EINVAL;
+  if (!ctx || !out || block < 0 || block >= (int)ctx->blk.size() || group < 0 || group >= kStatGroups)
+    return OSTC_EINVAL;
   if (!ctx->stat_on) {
     ctx->err = "statistics collection is off (ostc_stat_enable, or if_collect_statistics in the setup)";
     return OSTC_ESTATE;
   }
   cudaSetDevice(ctx->device);
   const BlockRes &B = ctx->blk[block];
-  const long long np = stat_points(B.db);
-  long long off = 0;
-  for (int g = 0; g < group; ++g) off += stat_group_vars(ctx->stat_spec, g) * np;
-  const size_t bytes = (size_t)stat_group_vars(ctx->stat_spec, group) * np * sizeof(double);
+  const long long off = stat_group_offset(ctx->stat_spec, B.db, group);
+  const size_t bytes = (size_t)stat_group_vars(ctx->stat_spec, group) * stat_group_points(B.db, group) * sizeof(double);
+  if (bytes == 0) return OSTC_OK;
   CK(cudaMemcpyAsync(out, B.stat + off, bytes, ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                      ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
@@ -4275,34 +4442,33 @@ int ostc_stat_export(ostc_ctx *ctx, const char *dir) {
   cudaSetDevice(ctx->device);
   CK(cudaStreamSynchronize(ctx->stream));
   std::vector<double> host;
-  for (int g = 0; g < 4; ++g) {
+  for (int g = 0; g < kStatGroups; ++g) {
+    const int nvar = stat_group_vars(ctx->stat_spec, g);
+    if (g >= 4 && nvar == 0) continue;  // an additional collector that is off writes no file
     const std::string path = std::string(dir) + "/" + kStatFiles[g];
     FILE *f = std::fopen(path.c_str(), "wb");
     if (!f) {
       ctx->err = "ostc_stat_export: cannot open " + path + " for writing";
       return OSTC_EIO;
     }
-    const int nvar = stat_group_vars(ctx->stat_spec, g);
     bool ok = true;
     auto put_i = [&](int v) { ok = ok && std::fwrite(&v, 4, 1, f) == 1; };
     put_i((int)ctx->blk.size());
     put_i(nvar);
-    put_i(1);
+    put_i(g < 4 ? 1 : 0);  // ghost layers of the group's arrays
     for (const auto &name : stat_names(ctx, g)) {
       for (char c : name) put_i((int)c);
       put_i(0);
     }
     for (int v = 0; v < nvar; ++v) put_i(ctx->stat_count);
-    long long off = 0;
-    for (int g2 = 0; g2 < g; ++g2) off += stat_group_vars(ctx->stat_spec, g2);
     for (const auto &B : ctx->blk) {
       put_i(B.db.mx);
       put_i(B.db.my);
       put_i(B.db.mz);
-      const long long np = stat_points(B.db);
+      const long long np = stat_group_points(B.db, g);
       host.resize((size_t)nvar * np);
-      if (cudaMemcpy(host.data(), B.stat + off * np, host.size() * sizeof(double), cudaMemcpyDeviceToHost) !=
-          cudaSuccess) {
+      if (cudaMemcpy(host.data(), B.stat + stat_group_offset(ctx->stat_spec, B.db, g), host.size() * sizeof(double),
+                     cudaMemcpyDeviceToHost) != cudaSuccess) {
         std::fclose(f);
         ctx->err = "ostc_stat_export: device copy failed";
         return OSTC_ECUDA;
@@ -4325,10 +4491,12 @@ int ostc_stat_import(ostc_ctx *ctx, const char *dir) {
   }
   cudaSetDevice(ctx->device);
   CK(cudaStreamSynchronize(ctx->stream));
-  // read and check all four files before touching the accumulators
-  std::vector<std::vector<double>> data(4 * ctx->blk.size());
+  // read and check every file of the selection before touching the accumulators
+  std::vector<std::vector<double>> data(kStatGroups * ctx->blk.size());
   int count = -1;
-  for (int g = 0; g < 4; ++g) {
+  for (int g = 0; g < kStatGroups; ++g) {
+    const int nvar = stat_group_vars(ctx->stat_spec, g);
+    if (g >= 4 && nvar == 0) continue;
     const std::string path = std::string(dir) + "/" + kStatFiles[g];
     FILE *f = std::fopen(path.c_str(), "rb");
     if (!f) {
@@ -4337,10 +4505,9 @@ int ostc_stat_import(ostc_ctx *ctx, const char *dir) {
     }
     std::string why;
     auto get_i = [&](int &v) { return std::fread(&v, 4, 1, f) == 1; };
-    const int nvar = stat_group_vars(ctx->stat_spec, g);
     int nb = 0, nv = 0, ngg = 0;
     if (!get_i(nb) || !get_i(nv) || !get_i(ngg)) why = "truncated header";
-    else if (nb != (int)ctx->blk.size() || nv != nvar || ngg != 1)
+    else if (nb != (int)ctx->blk.size() || nv != nvar || ngg != (g < 4 ? 1 : 0))
       why = "header (n_block " + std::to_string(nb) + ", n_var " + std::to_string(nv) + ", ngg " +
             std::to_string(ngg) + ") does not match the case and the enabled selection";
     for (const auto &name : stat_names(ctx, g)) {
@@ -4364,7 +4531,7 @@ int ostc_stat_import(ostc_ctx *ctx, const char *dir) {
         why = "block " + std::to_string(b) + " extents differ from the case";
       else {
         auto &d = data[g * ctx->blk.size() + b];
-        d.resize((size_t)nvar * stat_points(db));
+        d.resize((size_t)nvar * stat_group_points(db, g));
         if (std::fread(d.data(), sizeof(double), d.size(), f) != d.size()) why = "truncated data";
       }
     }
@@ -4374,15 +4541,13 @@ int ostc_stat_import(ostc_ctx *ctx, const char *dir) {
       return OSTC_EIO;
     }
   }
-  for (size_t b = 0; b < ctx->blk.size(); ++b) {
-    long long off = 0;
-    const long long np = stat_points(ctx->blk[b].db);
-    for (int g = 0; g < 4; ++g) {
+  for (size_t b = 0; b < ctx->blk.size(); ++b)
+    for (int g = 0; g < kStatGroups; ++g) {
       const auto &d = data[g * ctx->blk.size() + b];
-      CK(cudaMemcpy(ctx->blk[b].stat + off * np, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice));
-      off += stat_group_vars(ctx->stat_spec, g);
+      if (d.empty()) continue;
+      CK(cudaMemcpy(ctx->blk[b].stat + stat_group_offset(ctx->stat_spec, ctx->blk[b].db, g), d.data(),
+                    d.size() * sizeof(double), cudaMemcpyHostToDevice));
     }
-  }
   ctx->stat_count = count < 0 ? 0 : count;
   // a continued collection (the reference's step index runs on across the restart): collect from the
   // next step on

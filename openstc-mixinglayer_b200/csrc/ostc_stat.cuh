@@ -19,14 +19,43 @@ struct StatSpec {
   int rey_idx[4];  // their primitive indices
   int rho_p;       // 1: accumulate rho p
   int ns;          // species (mass fractions accumulated Favre-weighted)
+  // the additional collectors (stat_lib/, SinglePointStat.cu:707-722), interior nodes only:
+  // tke: the viscous stresses and their work (TkeBudget); svc: rho u Y, rho v Y, rho w Y
+  // (SpeciesVelocityCorrelation); sdr: rho D |grad Y|^2, rho D grad Y, rho D
+  // (SpeciesDissipationRate) of the nss species ss_idx (stat_species)
+  int tke, svc, sdr, nss;
+  int ss_idx[16];
 };
 
+// Groups 0-3: the basic collector (one ghost layer); 4 TKE budget, 5 species velocity correlation,
+// 6 species dissipation rate (no ghost layer); a group that is off has no variables.
+constexpr int kStatGroups = 7;
+
 __host__ __device__ inline int stat_group_vars(const StatSpec &sp, int g) {
-  return g == 0 ? 2 + sp.n_rey : g == 1 ? 4 + sp.ns : g == 2 ? 2 + sp.rho_p : 7 + sp.ns;
+  switch (g) {
+    case 0: return 2 + sp.n_rey;
+    case 1: return 4 + sp.ns;
+    case 2: return 2 + sp.rho_p;
+    case 3: return 7 + sp.ns;
+    case 4: return sp.tke ? 7 : 0;
+    case 5: return sp.svc ? 3 * sp.nss : 0;
+    default: return sp.sdr ? 5 * sp.nss : 0;
+  }
 }
 
 __host__ __device__ inline long long stat_points(const DevBlock &b) {
   return (long long)(b.mx + 2) * (b.my + 2) * (b.mz + 2);
+}
+
+__host__ __device__ inline long long stat_group_points(const DevBlock &b, int g) {
+  return g < 4 ? stat_points(b) : (long long)b.mx * b.my * b.mz;
+}
+
+// offset (doubles) of group g in a block's accumulator buffer
+__host__ __device__ inline long long stat_group_offset(const StatSpec &sp, const DevBlock &b, int g) {
+  long long o = 0;
+  for (int q = 0; q < g; ++q) o += stat_group_vars(sp, q) * stat_group_points(b, q);
+  return o;
 }
 
 // Products and sums are rounded one at a time (no fused multiply-add), in the reference's order:
@@ -112,6 +141,82 @@ __global__ void __launch_bounds__(256) k_stat_collect(DevBlock b, DevState s, do
           fav1[(long long)(4 + l) * np + n] = __dadd_rn(f1[q], ry);
           fav2[(long long)(7 + l) * np + n] = __dadd_rn(f2[q], __dmul_rn(ry, y[q]));
         }
+      }
+    }
+  }
+}
+
+// collect_single_point_additional_statistics (SinglePointStat.cu:707-722) over the interior nodes:
+// collect_tke_budget (TkeBudget.cu:123-170), collect_species_velocity_correlation and
+// collect_species_dissipation_rate (SpeciesStat.cu:5-85).  Velocity and mass-fraction gradients by
+// central differences in computational space times the metric; 2-D blocks hold no k ghosts and their
+// zeta differences (copies of k = 0 in the reference) are zero, so those terms are left out.
+// ext: the block's accumulators of group 4 onwards.
+__global__ void __launch_bounds__(128) k_stat_extra(DevBlock b, DevState s, double *__restrict__ ext, StatSpec sp) {
+  const long long P = b.plane, n_all = b.n;
+  double *tke = ext;
+  double *svc = tke + (long long)stat_group_vars(sp, 4) * n_all;
+  double *sdr = svc + (long long)stat_group_vars(sp, 5) * n_all;
+  const bool is3d = b.gz > 0;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < n_all; n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % b.mx);
+    const long long r = n / b.mx;
+    const int j = (int)(r % b.my), k = (int)(r / b.my);
+    const long long p = b.id(i, j, k);
+    const long long pi0 = b.id(i - 1, j, k), pi1 = b.id(i + 1, j, k), pj0 = b.id(i, j - 1, k), pj1 = b.id(i, j + 1, k);
+    const long long pk0 = is3d ? b.id(i, j, k - 1) : p, pk1 = is3d ? b.id(i, j, k + 1) : p;
+    double m[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) m[q] = b.met[q * P + p];
+    // d/dx, d/dy, d/dz of plane f at this node
+    auto grad = [&](const double *f, double g[3]) {
+      const double dxi = f[pi1] - f[pi0], deta = f[pj1] - f[pj0];
+      const double dzeta = is3d ? f[pk1] - f[pk0] : 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        g[c] = is3d ? 0.5 * (m[c] * dxi + m[3 + c] * deta + m[6 + c] * dzeta) : 0.5 * (m[c] * dxi + m[3 + c] * deta);
+    };
+    if (sp.tke) {
+      double gu[3], gv[3], gw[3];
+      grad(s.bv + P, gu);
+      grad(s.bv + 2 * P, gv);
+      grad(s.bv + 3 * P, gw);
+      const double mu = s.mul[p];
+      const double t11 = mu * (4.0 * gu[0] - 2 * gv[1] - 2 * gw[2]) / 3.0;
+      const double t12 = mu * (gu[1] + gv[0]);
+      const double t13 = mu * (gu[2] + gw[0]);
+      const double t22 = mu * (4.0 * gv[1] - 2 * gu[0] - 2 * gw[2]) / 3.0;
+      const double t23 = mu * (gv[2] + gw[1]);
+      const double t33 = mu * (4.0 * gw[2] - 2 * gu[0] - 2 * gv[1]) / 3.0;
+      tke[n] += t11;
+      tke[n_all + n] += t12;
+      tke[2 * n_all + n] += t13;
+      tke[3 * n_all + n] += t22;
+      tke[4 * n_all + n] += t23;
+      tke[5 * n_all + n] += t33;
+      tke[6 * n_all + n] += t11 * gu[0] + t12 * gu[1] + t13 * gu[2] + t12 * gv[0] + t22 * gv[1] + t23 * gv[2] +
+                            t13 * gw[0] + t23 * gw[1] + t33 * gw[2];
+    }
+    if (sp.svc) {
+      const double rho = s.bv[p], u = s.bv[P + p], v = s.bv[2 * P + p], w = s.bv[3 * P + p];
+      for (int q = 0; q < sp.nss; ++q) {
+        const double z = s.sv[sp.ss_idx[q] * P + p];
+        svc[(3 * q) * n_all + n] += rho * u * z;
+        svc[(3 * q + 1) * n_all + n] += rho * v * z;
+        svc[(3 * q + 2) * n_all + n] += rho * w * z;
+      }
+    }
+    if (sp.sdr) {
+      for (int q = 0; q < sp.nss; ++q) {
+        const int is = sp.ss_idx[q];
+        double gz[3];
+        grad(s.sv + is * P, gz);
+        const double rd = s.rhod[is * P + p];
+        sdr[(5 * q) * n_all + n] += rd * (gz[0] * gz[0] + gz[1] * gz[1] + gz[2] * gz[2]);
+        sdr[(5 * q + 1) * n_all + n] += rd * gz[0];
+        sdr[(5 * q + 2) * n_all + n] += rd * gz[1];
+        sdr[(5 * q + 3) * n_all + n] += rd * gz[2];
+        sdr[(5 * q + 4) * n_all + n] += rd;
       }
     }
   }

@@ -21,7 +21,9 @@ FLAG_NONPOSITIVE, FLAG_NAN = 1, 2
 CHEM_EXPLICIT, CHEM_POINT_IMPLICIT = 0, 1
 LAUNCH_GRAPH, LAUNCH_BLOCK_LOOP = 0, 1
 STAT_REY_U, STAT_REY_V, STAT_REY_W, STAT_REY_T, STAT_RHO_P = 1, 2, 4, 8, 16
-STAT_GROUPS = ("reynolds_1st", "favre_1st", "reynolds_2nd", "favre_2nd")
+STAT_TKE_BUDGET, STAT_SPECIES_VELOCITY, STAT_SPECIES_DISSIPATION = 32, 64, 128
+STAT_GROUPS = ("reynolds_1st", "favre_1st", "reynolds_2nd", "favre_2nd", "tke_budget", "species_velocity_correlation",
+               "species_dissipation_rate")
 
 EXPORTS = [
     "ostc_create", "ostc_destroy", "ostc_last_error", "ostc_n_blocks", "ostc_block_dims", "ostc_n_var",
@@ -33,7 +35,7 @@ EXPORTS = [
     "ostc_bounds_checked", "ostc_stat_enable", "ostc_stat_disable", "ostc_stat_info", "ostc_stat_get",
     "ostc_stat_export", "ostc_stat_import", "ostc_write_plt", "ostc_read_plt", "ostc_tune_report",
     "ostc_set_sweep_variant", "ostc_steady_step", "ostc_dual_time_step", "ostc_set_launch_mode",
-    "ostc_set_inflow_seed",
+    "ostc_set_inflow_seed", "ostc_stat_group_vars",
 ]
 
 
@@ -104,6 +106,7 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.ostc_set_sweep_variant.argtypes = [vp, ip, ip, ip]
     lib.ostc_set_launch_mode.argtypes = [vp, ip]
     lib.ostc_set_inflow_seed.argtypes = [vp, ctypes.c_longlong]
+    lib.ostc_stat_group_vars.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_int)]
     lib.ostc_steady_step.argtypes = [vp, ip, ctypes.POINTER(ip), dp]
     lib.ostc_dual_time_step.argtypes = [vp, ip, ctypes.POINTER(ip)]
     lib.ostc_timed_steps.argtypes = [vp, ip, dp]
@@ -285,12 +288,19 @@ class Solver:
         self._check(self.lib.ostc_stat_info(self.h, nv, ctypes.byref(nc), ctypes.byref(st)))
         return list(nv), nc.value, st.value
 
+    def stat_group_vars(self, group: int) -> int:
+        n = ctypes.c_int()
+        self._check(self.lib.ostc_stat_group_vars(self.h, group, ctypes.byref(n)))
+        return n.value
+
     def stat_get(self, group: int, block: int = 0) -> np.ndarray:
-        """Sums of group (0 Reynolds 1st, 1 Favre 1st, 2 Reynolds 2nd, 3 Favre 2nd) of block:
-        [n_var, mz + 2, my + 2, mx + 2], one ghost layer on every side."""
-        nv = self.stat_info()[0][group]
+        """Sums of group (0 Reynolds 1st, 1 Favre 1st, 2 Reynolds 2nd, 3 Favre 2nd: [n_var, mz + 2, my + 2,
+        mx + 2], one ghost layer on every side; 4 TKE budget, 5 species velocity correlation, 6 species
+        dissipation rate: [n_var, mz, my, mx]) of block."""
+        nv = self.stat_group_vars(group)
         mz, my, mx = self.shape(block)
-        out = np.empty((nv, mz + 2, my + 2, mx + 2))
+        g = 1 if group < 4 else 0
+        out = np.empty((nv, mz + 2 * g, my + 2 * g, mx + 2 * g))
         self._check(self.lib.ostc_stat_get(self.h, block, group, out.ctypes.data, OSTC_HOST))
         return out
 

@@ -137,6 +137,7 @@ def load():
         lib.orc_dual.argtypes = [vp, ctypes.c_int]
         lib.orc_dual.restype = ctypes.c_int
         lib.orc_stat_collect.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int, dp]
+        lib.orc_stat_extra.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), vp, vp]
         lib.orc_time.argtypes = [vp]
         lib.orc_time.restype = ctypes.c_double
         lib.orc_dt.argtypes = [vp]
@@ -294,6 +295,17 @@ class Oracle:
         idx = (ctypes.c_int * max(1, len(rey_idx)))(*rey_idx)
         self.lib.orc_stat_collect(self.h, len(rey_idx), idx, int(rho_p), _dp(acc))
 
+    def stat_extra(self, tke=None, svc=None, sdr=None, ss_idx=()):
+        """Add one collection of the additional statistics of the current state (orc_stat_extra): tke
+        [7, mz, my, mx], and for the species ss_idx svc [3 nss, ...] and sdr [5 nss, ...]; None skips."""
+        def ptr(a):
+            if a is None:
+                return None
+            assert a.dtype == np.float64 and a.flags.c_contiguous
+            return a.ctypes.data
+        idx = (ctypes.c_int * max(1, len(ss_idx)))(*ss_idx)
+        self.lib.orc_stat_extra(self.h, ptr(tke), len(ss_idx), idx, ptr(svc), ptr(sdr))
+
     def time(self) -> float:
         return self.lib.orc_time(self.h)
 
@@ -309,6 +321,7 @@ class _BlockView:
 
     get_state = Oracle.get_state
     stat_collect = Oracle.stat_collect
+    stat_extra = Oracle.stat_extra
     metric = Oracle.metric
     mixture = Oracle.mixture
     time = Oracle.time

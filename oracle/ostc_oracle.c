@@ -3023,6 +3023,73 @@ void orc_stat_collect(const orc_ctx *o, int n_rey, const int *rey_idx, int rho_p
       }
 }
 
+/* collect_single_point_additional_statistics (SinglePointStat.cu:707-722) on the interior nodes:
+ * collect_tke_budget (TkeBudget.cu:123-170) into tke[7][N] when tke != 0, and for the species
+ * ss_idx[0..nss) collect_species_velocity_correlation into svc[3 nss][N] and
+ * collect_species_dissipation_rate into sdr[5 nss][N] (SpeciesStat.cu:5-85); null arrays are skipped.
+ * Gradients as the reference forms them: half the central differences in computational space times
+ * the metric (in 2-D the k ghost layers are copies of k = 0, so their difference is zero). */
+static double stat_grad(const orc_ctx *o, const double *f, int i, int j, int k, int c) {
+  const long p = ID(o, i, j, k);
+  const double di = f[ID(o, i + 1, j, k)] - f[ID(o, i - 1, j, k)];
+  const double dj = f[ID(o, i, j + 1, k)] - f[ID(o, i, j - 1, k)];
+  if (o->dim == 2) return 0.5 * (M(o, 1, c, p) * di + M(o, 2, c, p) * dj);
+  const double dk = f[ID(o, i, j, k + 1)] - f[ID(o, i, j, k - 1)];
+  return 0.5 * (M(o, 1, c, p) * di + M(o, 2, c, p) * dj + M(o, 3, c, p) * dk);
+}
+
+void orc_stat_extra(const orc_ctx *o, double *tke, int nss, const int *ss_idx, double *svc, double *sdr) {
+  const long P = o->P, N = (long)o->mx * o->my * o->mz;
+  for (int k = 0; k < o->mz; ++k)
+    for (int j = 0; j < o->my; ++j)
+      for (int i = 0; i < o->mx; ++i) {
+        const long n = IQ(o, i, j, k), p = ID(o, i, j, k);
+        if (tke) {
+          double gu[3], gv[3], gw[3];
+          for (int c = 0; c < 3; ++c) {
+            gu[c] = stat_grad(o, o->bv + P, i, j, k, c + 1);
+            gv[c] = stat_grad(o, o->bv + 2 * P, i, j, k, c + 1);
+            gw[c] = stat_grad(o, o->bv + 3 * P, i, j, k, c + 1);
+          }
+          const double mu = o->mul[p];
+          const double t11 = mu * (4.0 * gu[0] - 2 * gv[1] - 2 * gw[2]) / 3.0;
+          const double t12 = mu * (gu[1] + gv[0]);
+          const double t13 = mu * (gu[2] + gw[0]);
+          const double t22 = mu * (4.0 * gv[1] - 2 * gu[0] - 2 * gw[2]) / 3.0;
+          const double t23 = mu * (gv[2] + gw[1]);
+          const double t33 = mu * (4.0 * gw[2] - 2 * gu[0] - 2 * gv[1]) / 3.0;
+          tke[n] += t11;
+          tke[N + n] += t12;
+          tke[2 * N + n] += t13;
+          tke[3 * N + n] += t22;
+          tke[4 * N + n] += t23;
+          tke[5 * N + n] += t33;
+          tke[6 * N + n] += t11 * gu[0] + t12 * gu[1] + t13 * gu[2] + t12 * gv[0] + t22 * gv[1] + t23 * gv[2] +
+                            t13 * gw[0] + t23 * gw[1] + t33 * gw[2];
+        }
+        for (int q = 0; q < nss; ++q) {
+          const int is = ss_idx[q];
+          if (svc) {
+            const double rho = o->bv[p], u = o->bv[P + p], v = o->bv[2 * P + p], w = o->bv[3 * P + p];
+            const double z = o->sv[is * P + p];
+            svc[(3 * q) * N + n] += rho * u * z;
+            svc[(3 * q + 1) * N + n] += rho * v * z;
+            svc[(3 * q + 2) * N + n] += rho * w * z;
+          }
+          if (sdr) {
+            const double zx = stat_grad(o, o->sv + is * P, i, j, k, 1), zy = stat_grad(o, o->sv + is * P, i, j, k, 2),
+                         zz = stat_grad(o, o->sv + is * P, i, j, k, 3);
+            const double rd = o->rhod[is * P + p];
+            sdr[(5 * q) * N + n] += rd * (zx * zx + zy * zy + zz * zz);
+            sdr[(5 * q + 1) * N + n] += rd * zx;
+            sdr[(5 * q + 2) * N + n] += rd * zy;
+            sdr[(5 * q + 3) * N + n] += rd * zz;
+            sdr[(5 * q + 4) * N + n] += rd;
+          }
+        }
+      }
+}
+
 /* ---------------------------------------------------------------- multi-block (interfaces) */
 
 typedef struct {

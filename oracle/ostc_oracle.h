@@ -131,6 +131,9 @@ void orc_steady(orc_ctx *o, int n);
 int orc_dual(orc_ctx *o, int n);
 /* one single-point statistics collection added to acc (collect_single_point_basic_statistics) */
 void orc_stat_collect(const orc_ctx *o, int n_rey, const int *rey_idx, int rho_p, double *acc);
+/* The additional collectors on the interior nodes (SinglePointStat.cu:707-722): tke[7][N] (null: off),
+ * and for the species ss_idx[0..nss) svc[3 nss][N] and sdr[5 nss][N] (null: off). */
+void orc_stat_extra(const orc_ctx *o, double *tke, int nss, const int *ss_idx, double *svc, double *sdr);
 double orc_time(const orc_ctx *o);
 /* Local CFL time step of the current state and its minimum (TimeAdvanceFunc.cuh:28-83). */
 double orc_dt(orc_ctx *o);

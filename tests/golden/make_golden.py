@@ -32,11 +32,13 @@ sys.path.insert(0, str(ROOT / "tests"))
 
 import ostc_cases as oc  # noqa: E402
 import refcase  # noqa: E402
-from golden_util import STAT_SETUP  # noqa: E402
+from golden_util import STAT_SETUP, STAT_SETUP_EXTRA  # noqa: E402
 
 STAT_FILES = ["output/stat/coll_rey_1st.bin", "output/stat/coll_fav_1st.bin", "output/stat/coll_rey_2nd.bin",
               "output/stat/coll_fav_2nd.bin"]
 PLT = ["output/flowfield.plt"]
+EXTRA_FILES = ["output/stat/tke_budget.bin", "output/stat/species_velocity_correlation.bin",
+               "output/stat/species_dissipation_rate.bin"]
 # steady driver settings (no early stop on convergence: the fixture runs a fixed iteration count)
 STEADY = dict(steady=1, implicit_method=0, dplur_inner_step=3, chem_src_method=0, convergence_criteria=1e-300)
 # dual time stepping settings (its DPLUR needs implicit_method 1 for the reference to allocate the iterates,
@@ -151,6 +153,14 @@ CASES = [
     ("rml3d_stat_plt", "reacting_mixing_layer_3d", dict(mx=12, my=10, mz=6), 5,
      dict(setup=STAT_SETUP, files=PLT + STAT_FILES)),
     ("ml2d_plt", "mixing_layer_2d", dict(mx=33, my=17, ybc="wall"), 5, dict(files=PLT)),
+    # the additional collectors' files: the TKE budget (air 3-D and 2-D), and for three species of the
+    # reacting layer their velocity correlation and dissipation rate
+    ("ml3d_stat_extra", "mixing_layer_3d", dict(mx=16, my=12, mz=8, ybc="outflow"), 6,
+     dict(setup=STAT_SETUP_EXTRA, files=STAT_FILES + EXTRA_FILES[:1])),
+    ("ml2d_stat_extra", "mixing_layer_2d", dict(mx=33, my=17), 5,
+     dict(setup=STAT_SETUP_EXTRA, files=STAT_FILES + EXTRA_FILES[:1])),
+    ("rml3d_stat_extra", "reacting_mixing_layer_3d", dict(mx=12, my=10, mz=6), 5,
+     dict(setup=STAT_SETUP_EXTRA, files=STAT_FILES + EXTRA_FILES)),
 ]
 
 N_SAMPLE = 16384

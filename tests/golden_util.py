@@ -41,6 +41,18 @@ array string stat_rey_1st {
     T u
 }
 """
+# statistics of gradients (the additional collectors: central differences of the state) carry the
+# state's ~1e-13 difference grown by the ratio of a value to its local difference
+TOL_GRAD = 1e-10
+# the additional collectors: TKE budget and, for the listed species, their velocity correlation and
+# dissipation rate (SinglePointStat.cu:27-96, 707-722)
+STAT_SETUP_EXTRA = STAT_SETUP + """bool stat_tke_budget = 1
+bool stat_species_velocity_correlation = 1
+bool stat_species_dissipation_rate = 1
+array string stat_species {
+    H2 OH O2
+}
+"""
 # variables compared against one shared scale (velocity and momentum components, their products)
 SCALE_GROUPS = [{"u", "v", "w"}, {"rhoU", "rhoV", "rhoW"},
                 {"rhoUU", "rhoVV", "rhoWW", "rhoUV", "rhoUW", "rhoVW"}]

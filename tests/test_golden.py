@@ -22,7 +22,8 @@ FIXTURES = gu.all_fixtures()
 FACE_FIXTURES = {"ml3d_wall_isothermal", "ml3d_wall_adiabatic", "ml2d_wall_isothermal_weno5",
                  "ml2d_wall_adiabatic_weno7", "ml3d_inflow_outflow", "ml3d_subsonic_backpressure", "rml3d_wall",
                  "rml3d_inflow", "rml3d_farfield_fr72", "rml3d_farfield_mix71"}
-FILE_FIXTURES = {"ml3d_stat_plt", "rml3d_stat_plt", "ml2d_plt"}
+FILE_FIXTURES = {"ml3d_stat_plt", "rml3d_stat_plt", "ml2d_plt", "ml3d_stat_extra", "ml2d_stat_extra",
+                 "rml3d_stat_extra"}
 # node-steps the serial oracle finishes in a few seconds (mixtures cost about ten times air)
 ORACLE_BUDGET = 4e6
 
@@ -84,7 +85,7 @@ def test_gpu_matches_reference(built, tmp_path, path):
     s.close()
 
 
-@pytest.mark.parametrize("name", sorted(n for n in FILE_FIXTURES if "stat" in n))
+@pytest.mark.parametrize("name", sorted(n for n in FILE_FIXTURES if "stat" in n and gu.fixture_path(n).exists()))
 def test_oracle_statistics_match_reference_files(built, name):
     """The oracle's restatement of the basic statistics collector (SinglePointStat.cu:641-706) summed over
     the same trajectory as the reference's exported coll_*.bin files: rho, p and the stat_rey_1st extras
@@ -110,3 +111,32 @@ def test_oracle_statistics_match_reference_files(built, name):
         got = acc[off:off + n].reshape((n_var[g],) + shape)
         off += n
         gu.assert_fields(names, got, blocks[0][1])
+
+
+@pytest.mark.parametrize("name", sorted(n for n in FILE_FIXTURES
+                                        if n.endswith("stat_extra") and gu.fixture_path(n).exists()))
+def test_oracle_additional_statistics_match_reference_files(built, name):
+    """The oracle's restatement of the additional collectors (SinglePointStat.cu:707-722; TkeBudget.cu,
+    SpeciesStat.cu) summed over the same trajectory as the reference's tke_budget.bin and species
+    files: the viscous stresses and their work, and for H2, OH, O2 rho u_i Y and the dissipation terms."""
+    from ref_files import read_stat_file
+
+    case, steps, z, _ = gu.load(gu.fixture_path(name))
+    o = Oracle(case)
+    o.set_state(case.bv)
+    shape = (case.mz, case.my, case.mx)
+    mix = case.mixture is not None
+    ss = [case.mixture["tables"].names.index(n) for n in ("H2", "OH", "O2")] if mix else []
+    tke = np.zeros((7,) + shape)
+    svc = np.zeros((3 * len(ss),) + shape) if mix else None
+    sdr = np.zeros((5 * len(ss),) + shape) if mix else None
+    for st in range(1, steps + 1):
+        o.step(1)
+        if st > 2:
+            o.stat_extra(tke, svc, sdr, ss)
+    pairs = [("tke_budget.bin", tke)] + ([("species_velocity_correlation.bin", svc),
+                                          ("species_dissipation_rate.bin", sdr)] if mix else [])
+    for fname, got in pairs:
+        nb, ngg, names, counters, blocks = read_stat_file(z["file_" + fname].tobytes())
+        assert (nb, ngg) == (1, 0) and counters == [steps - 2] * len(names), fname
+        gu.assert_fields(names, got, blocks[0][1], tol=gu.TOL_GRAD)

@@ -16,6 +16,9 @@ from ref_files import read_stat_file
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
+# statistics of gradients (central differences of the state): the state's 1e-13 difference from the
+# oracle grows by the ratio of a value to its local difference
+GRAD_TOL = 1e-10
 ALL = ostc.STAT_REY_U | ostc.STAT_REY_V | ostc.STAT_REY_W | ostc.STAT_REY_T | ostc.STAT_RHO_P
 IDX = {ostc.STAT_REY_U: 1, ostc.STAT_REY_V: 2, ostc.STAT_REY_W: 3, ostc.STAT_REY_T: 5}
 
@@ -182,7 +185,7 @@ def test_stat_off_and_bad_flags(built, tmp_path):
     with pytest.raises(ostc.OstcError, match="statistics collection is off"):
         s.stat_info()
     with pytest.raises(ostc.OstcError, match="unknown flag"):
-        s.stat_enable(0, 64)
+        s.stat_enable(0, 256)
     s.stat_enable(5, 0)
     s.step(2)
     assert s.stat_info()[1:] == (0, 2)
@@ -195,20 +198,75 @@ def test_stat_off_and_bad_flags(built, tmp_path):
 # ---- against the coll_*.bin files the reference itself exported at the end of the same run
 # (SinglePointStat.cu:515-706, RK.cuh:200-207); fixtures from tests/golden/make_golden.py
 
-@pytest.mark.parametrize("name", ["ml3d_stat_plt", "rml3d_stat_plt"])
+@pytest.mark.parametrize("name", ["ml3d_stat_plt", "rml3d_stat_plt", "ml3d_stat_extra", "ml2d_stat_extra",
+                                  "rml3d_stat_extra"])
 def test_stat_matches_reference_files(built, tmp_path, name):
     import golden_util as gu
 
     case, steps, z, t_ref = gu.load(gu.fixture_path(name))
-    s = gu.check_library(case, steps, z, t_ref, tmp_path / name, gu.STAT_SETUP)
+    extra = name.endswith("stat_extra")
+    s = gu.check_library(case, steps, z, t_ref, tmp_path / name, gu.STAT_SETUP_EXTRA if extra else gu.STAT_SETUP)
     out = tmp_path / "stat"
     out.mkdir()
     s.stat_export(out)
-    for fname in ["coll_rey_1st.bin", "coll_fav_1st.bin", "coll_rey_2nd.bin", "coll_fav_2nd.bin"]:
+    files = sorted(k[len("file_"):] for k in z.files if k.startswith("file_") and k.endswith(".bin"))
+    assert len(files) >= 4
+    for fname in files:
         nb, ngg, names, counters, blocks = read_stat_file(out / fname)
         rnb, rngg, rnames, rcounters, rblocks = read_stat_file(z["file_" + fname].tobytes())
         assert (nb, ngg, names, counters) == (rnb, rngg, rnames, rcounters), fname
         for (ext, got), (rext, ref) in zip(blocks, rblocks):
             assert ext == rext
-            gu.assert_fields(names, got, ref)
+            gu.assert_fields(names, got, ref, tol=gu.TOL if fname.startswith("coll_") else gu.TOL_GRAD)
     s.close()
+
+
+EXTRA = ostc.STAT_TKE_BUDGET | ostc.STAT_SPECIES_VELOCITY | ostc.STAT_SPECIES_DISSIPATION
+
+
+@pytest.mark.parametrize("kind", ["air_3d", "air_2d", "mixture_3d"])
+def test_additional_collectors_match_oracle(built, tmp_path, kind):
+    """The TKE budget and (mixtures, every species) the species velocity correlation and dissipation
+    rate through ostc_stat_enable, against the oracle's orc_stat_extra over the same steps."""
+    if kind == "air_3d":
+        case = oc.mixing_layer_3d(mx=32, my=24, mz=16)
+    elif kind == "air_2d":
+        case = oc.mixing_layer_2d(mx=49, my=33)
+    else:
+        case = oc.reacting_mixing_layer_3d(mx=24, my=18, mz=12)
+    d = oc.write_case(case, tmp_path / "c")
+    s = ostc.Solver(str(d))
+    s.set_state(case.bv, sv=case.sv)
+    o = Oracle(case)
+    o.set_state(case.bv)
+    s.stat_enable(1, EXTRA)
+    shape = s.shape(0)
+    ns = case.sv.shape[0] if case.sv is not None else 0
+    tke = np.zeros((7,) + shape)
+    svc = np.zeros((3 * ns,) + shape) if ns else None
+    sdr = np.zeros((5 * ns,) + shape) if ns else None
+    for st in range(1, 5):
+        s.step(1)
+        o.step(1)
+        if st > 1:
+            o.stat_extra(tke, svc, sdr, list(range(ns)))
+    assert [s.stat_group_vars(g) for g in (4, 5, 6)] == [7, 3 * ns, 5 * ns]
+    for g, want in ((4, tke), (5, svc), (6, sdr)):
+        if want is None:
+            continue
+        got = s.stat_get(g)
+        assert got.shape == want.shape
+        for l in range(got.shape[0]):
+            scale = np.max(np.abs(want[l]))
+            if scale == 0:
+                assert np.all(got[l] == 0), (g, l)
+                continue
+            assert np.max(np.abs(got[l] - want[l])) <= GRAD_TOL * scale, (ostc.STAT_GROUPS[g], l)
+    # the exported files carry them with their names and no ghost layer
+    out = tmp_path / "stat"
+    out.mkdir()
+    s.stat_export(out)
+    nb, ngg, names, counters, blocks = read_stat_file(out / "tke_budget.bin")
+    assert (nb, ngg, names[0], names[-1], counters) == (1, 0, "Tau11", "TauIjDUiDXj", [3] * 7)
+    assert blocks[0][1].shape == (7,) + shape
+    assert (out / "species_dissipation_rate.bin").exists() == bool(ns)
