@@ -110,7 +110,7 @@ CASES = [
     ("rml3d_nnd_hllc", "reacting_mixing_layer_3d",
      dict(mx=24, my=16, mz=10, inviscid_scheme=4, reconstruction=3, finite_rate=False), 5),
     ("rml3d_first_roe", "reacting_mixing_layer_3d", dict(mx=24, my=16, mz=10, inviscid_scheme=2, reconstruction=1), 5),
-    ("rml2d_muscl_roe", "reacting_mixing_layer_3d", dict(mx=40, my=24, mz=1, inviscid_scheme=2), 10),
+    ("rml2d_muscl_roe", "reacting_mixing_layer_3d", dict(mx=40, my=26, mz=1, inviscid_scheme=2), 10),
     ("rml3d_farfield_nnd_ausm", "reacting_mixing_layer_3d",
      dict(mx=24, my=16, mz=10, ybc="farfield", inviscid_scheme=3, reconstruction=3), 5),
     # spatial mixing layers (problem_type 1, the reference's shipped layout): the two-stream inflow
@@ -231,6 +231,12 @@ def main(outdir: Path, only=None) -> int:
         if only and name not in only:
             continue
         case = make_case(gen, kw)
+        sizes = [b.mx * b.my * b.mz for b in case.blocks] if hasattr(case, "blocks") else [case.nodes]
+        if not all(reference_dt_defined(n) for n in sizes):
+            # the reference's CFL minimum would read unwritten shared memory: no defined result to pin
+            print(name, "SKIPPED: a block size for which the reference's dt is undefined", sizes, flush=True)
+            failed.append(name)
+            continue
         # inflow_seed: the clock the harness reported to the reference (its white-noise inflow seed)
         meta = json.dumps({"generator": gen, "kwargs": kw, "inflow_seed": refcase.REF_TIME})
         try:

@@ -27,8 +27,18 @@ TOL_T = 1e-13
 LOOSE = {"rml3d_farfield_fr72": (1e-5, 1e-6, 1e-9), "rml3d_farfield_mix71": (1e-5, 1e-6, 1e-9)}
 
 
-def tolerances(name):
-    """(max, L2, physical time) relative bars of a fixture."""
+# The oracle on the spatial mixing layers (problem_type 1): the inflow profile and the initial field
+# take tanh(2 y / delta_omega) from the C library, the reference and the CUDA path from CUDA's tanh,
+# and the two may differ in the last bit.  Changing the oracle's tanh by one ulp alone moves its state
+# after the fixtures' step counts by 1.3e-10 (3-D) and 1.2e-11 (2-D) in the max norm, the size of its
+# distance from the reference; the CUDA path keeps the 1e-12 bar on these fixtures.
+ORACLE_LOOSE = {n: (5e-10, 1e-11, TOL_T) for n in ("sml3d_air", "sml2d_air", "sml3d_species")}
+
+
+def tolerances(name, oracle=False):
+    """(max, L2, physical time) relative bars of a fixture (oracle: the bars of the CPU oracle)."""
+    if oracle and name in ORACLE_LOOSE:
+        return ORACLE_LOOSE[name]
     return LOOSE.get(name, (TOL, TOL, TOL_T))
 
 # statistics collection in the reference's own setup keys (SinglePointStat, RK.cuh:200-207): collected
