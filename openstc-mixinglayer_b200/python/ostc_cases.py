@@ -935,7 +935,8 @@ def reacting_mixing_layer_3d(mx=384, my=192, mz=96, seed=0, steps=100, h=0.125, 
 
 def spatial_mixing_layer_3d(mx=64, my=48, mz=12, seed=0, steps=20, h=0.125, delta_omega=1e-3, ma_c=0.3,
                             velocity_ratio=1.5, upper_faster=False, species=False, fluctuation_type=0,
-                            intensity=0.01, inviscid_scheme=None, chem_dir=None, finite_rate=False) -> Case:
+                            intensity=0.01, inviscid_scheme=None, chem_dir=None, finite_rate=False,
+                            noise=0.0) -> Case:
     """Spatially developing mixing layer (problem_type 1, the layout of the reference's shipped input):
     the two-stream inflow profile at i = 0 (u blended by tanh(2 y / delta_omega), upper / lower stream
     state by the sign of y), optionally with white noise on its velocity (fluctuation_type 1, relative
@@ -944,7 +945,8 @@ def spatial_mixing_layer_3d(mx=64, my=48, mz=12, seed=0, steps=20, h=0.125, delt
     air (600 K) with the 9-species mechanism, frozen unless finite_rate.  Stream Mach numbers from
     ma_c and the velocity ratio (lower stream faster unless upper_faster).  Grid in units of
     delta_omega (gridScale = delta_omega), y = (j - (my - 1) / 2) h.  The initial field is the profile
-    plus 1e-2 dU N(0,1) exp(-(y/delta_omega)^2) seeded noise in u, v, w."""
+    plus `noise` dU N(0,1) exp(-(y/delta_omega)^2) seeded noise in u, v, w (noise = 0: the profile alone,
+    as the reference starts a mixing-layer problem)."""
     rng = np.random.default_rng(seed)
     xs = np.arange(mx) * h
     ys = (np.arange(my) - (my - 1) / 2) * h
@@ -991,9 +993,9 @@ def spatial_mixing_layer_3d(mx=64, my=48, mz=12, seed=0, steps=20, h=0.125, delt
     for l in (0, 4, 5):
         bv[l] = np.where(above, up[l], lo[l])
     bv[1] = 0.5 * (up[1] + lo[1]) + 0.5 * (up[1] - lo[1]) * np.tanh(2 * yphys / delta_omega)
-    bv[1] += 1e-2 * du * rng.standard_normal(X.shape) * env
-    bv[2] = 1e-2 * du * rng.standard_normal(X.shape) * env
-    bv[3] = 0.0 if mz == 1 else 1e-2 * du * rng.standard_normal(X.shape) * env
+    bv[1] += noise * du * rng.standard_normal(X.shape) * env
+    bv[2] = noise * du * rng.standard_normal(X.shape) * env
+    bv[3] = 0.0 if mz == 1 else noise * du * rng.standard_normal(X.shape) * env
     if species:
         ns = tb.n_spec
         case.sv = np.empty((ns,) + X.shape)

@@ -25,20 +25,16 @@ TOL_T = 1e-13
 # oracle built with and without fused multiply-adds lands 2e-6 and 3e-6 (max) from the reference's
 # state on the same case, so these fixtures are compared at (max, L2, time) = (1e-5, 1e-6, 1e-9).
 LOOSE = {"rml3d_farfield_fr72": (1e-5, 1e-6, 1e-9), "rml3d_farfield_mix71": (1e-5, 1e-6, 1e-9)}
+# White-noise inflows of air (AWENO7 + HLLC): the face injects grid-scale noise every stage, and in that
+# rough region the WENO-Z weights grow the rounding-level differences of two implementations; the
+# 3-D fixture lands 6.6e-12 (max) from the reference, its L2 error stays below 2e-13.
+LOOSE.update({n: (1e-10, 1e-12, TOL_T) for n in ("sml3d_air_noise", "sml2d_air_noise")})
 
 
-# The oracle on the spatial mixing layers (problem_type 1): the inflow profile and the initial field
-# take tanh(2 y / delta_omega) from the C library, the reference and the CUDA path from CUDA's tanh,
-# and the two may differ in the last bit.  Changing the oracle's tanh by one ulp alone moves its state
-# after the fixtures' step counts by 1.3e-10 (3-D) and 1.2e-11 (2-D) in the max norm, the size of its
-# distance from the reference; the CUDA path keeps the 1e-12 bar on these fixtures.
-ORACLE_LOOSE = {n: (5e-10, 1e-11, TOL_T) for n in ("sml3d_air", "sml2d_air", "sml3d_species")}
 
 
-def tolerances(name, oracle=False):
-    """(max, L2, physical time) relative bars of a fixture (oracle: the bars of the CPU oracle)."""
-    if oracle and name in ORACLE_LOOSE:
-        return ORACLE_LOOSE[name]
+def tolerances(name):
+    """(max, L2, physical time) relative bars of a fixture."""
     return LOOSE.get(name, (TOL, TOL, TOL_T))
 
 # statistics collection in the reference's own setup keys (SinglePointStat, RK.cuh:200-207): collected

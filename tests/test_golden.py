@@ -67,7 +67,7 @@ def test_oracle_matches_reference(built, path):
             gu.assert_state(m.blocks[b].get_state()[0], z, block=b)
         assert abs(m.time() - t_ref) <= gu.TOL_T * t_ref
         return
-    tm, tl, tt = gu.tolerances(gu.name_of(path), oracle=True)
+    tm, tl, tt = gu.tolerances(gu.name_of(path))
     o = Oracle(case)
     o.set_state(case.bv)
     o.advance(steps)

@@ -93,12 +93,14 @@ def test_inflow_mixture(built, tmp_path):
 
 
 def test_inflow_rejections(built, tmp_path):
-    """Profile and fluctuating inflows are refused with the reason."""
-    case = oc.mixing_layer_3d(mx=16, my=12, mz=8, xbc="inflow")
-    case.bc_structs["inflow"]["fluctuation_type"] = ("int", 1)
-    d = oc.write_case(case, tmp_path / "fl")
-    with pytest.raises(ostc.OstcError, match="fluctuation_type"):
-        ostc.Solver(str(d))
+    """Profile-file inflows and the stability-mode / receptivity fluctuations are refused with the
+    reason (white noise, fluctuation_type 1, is built: tests/test_gpu_inflow.py)."""
+    for key, val in (("fluctuation_type", 2), ("fluctuation_type", 3), ("inflow_type", 1)):
+        case = oc.mixing_layer_3d(mx=16, my=12, mz=8, xbc="inflow")
+        case.bc_structs["inflow"][key] = ("int", val)
+        d = oc.write_case(case, tmp_path / f"fl_{key}_{val}")
+        with pytest.raises(ostc.OstcError, match=key):
+            ostc.Solver(str(d))
 
 
 @pytest.mark.parametrize("ybc", ["outflow", "wall"])
