@@ -1098,10 +1098,37 @@ bool resolve_boundaries(const Setup &s, const Derived &d, HostMesh &mesh, std::s
                 " (profile file) is not provided; constant (0) and mixing-layer (problem_type 1) inflows are";
           return false;
         }
-        if (ftype != 0 && ftype != 1) {
+        if (ftype != 0 && ftype != 1 && ftype != 11) {
           err = "inflow label " + std::to_string(f.label) + ": fluctuation_type " + std::to_string(ftype) +
-                " is not provided (stability-mode, receptivity and digital-filter fluctuations); white noise (1) is";
+                " is not provided (stability-mode and receptivity fluctuations); white noise (1) and, for "
+                "mixing-layer inflows, the digital filter (11) are";
           return false;
+        }
+        if (ftype == 11) {
+          // DBoundCond::initialize_digital_filter (DigitalFilter.cu:8-120): the inflow plane i = 0 of a
+          // 3-D block, z periodic; the Gaussian Reynolds-stress supplier (reynolds_stress_supplier 2)
+          if (f.face != 0 || f.direction != -1 || mesh.dimension != 3) {
+            err = "inflow label " + std::to_string(f.label) +
+                  ": the digital filter needs the i = 0 face of a 3-D block (the reference supports no other)";
+            return false;
+          }
+          if (B.mz - 1 < 50 + B.ngg) {
+            // apply_periodic_in_spanwise copies k = 1..50+ngg from k = 0..mz-1; with fewer planes its
+            // parallel copies read ghosts other threads write (DigitalFilter.cu:539-554)
+            err = "the digital filter needs mz - 1 >= 50 + ngg spanwise nodes (its periodic extension is "
+                  "otherwise undefined in the reference)";
+            return false;
+          }
+          if (s.get_int("reynolds_stress_supplier") != 2) {
+            err = "the digital filter supports reynolds_stress_supplier = 2 (Gaussian Reynolds stresses) only";
+            return false;
+          }
+          auto rij = s.real_arrays.find("df_reynolds_gaussian_peak");
+          if (rij == s.real_arrays.end() || rij->second.size() < 6) {
+            err = "the digital filter needs the array df_reynolds_gaussian_peak (R11 R12 R22 R13 R23 R33)";
+            return false;
+          }
+          f.df_rij.assign(rij->second.begin(), rij->second.begin() + 6);
         }
         f.inflow_type = itype;
         f.fluctuation_type = ftype;

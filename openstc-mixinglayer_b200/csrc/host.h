@@ -110,6 +110,9 @@ struct BcFace {
   // stream is density .. temperature and y above
   double lower[6]{};
   std::vector<double> y_lower;
+  // digital-filter inflow (fluctuation_type 11 of a mixing-layer inflow): the peak Reynolds stresses
+  // R11 R12 R22 R13 R23 R33 of the assumed Gaussian profile (df_reynolds_gaussian_peak)
+  std::vector<double> df_rij;
 };
 
 // The two streams of a mixing-layer problem (get_mixing_layer_info, MixingLayer.cu:9-191): rho, u, v,

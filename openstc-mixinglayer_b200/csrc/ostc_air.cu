@@ -151,6 +151,7 @@ __device__ __forceinline__ void cv_from_bv_node(const DevBlock &b, DevState s, l
 #include "ostc_stat.cuh"
 #include "ostc_steady.cuh"
 #include "pv_mix.cuh"
+#include "ostc_df.cuh"
 
 static_assert(ostc::kMS <= 16, "DevFace::y holds the inflow mass fractions of at most 16 species");
 
@@ -1621,6 +1622,14 @@ struct ostc_ctx {
   long long rng_size = 0;
   // problem_type 1: the two streams of the initial mixing-layer profile
   MixingLayerStreams ml;
+  // digital-filter inflow (at most one face): its buffers, block / face, the stream molecular weights,
+  // a device zero (the reference's dt before the first step), and whether the boundary faces being
+  // enqueued are the initial application
+  DevDf df{};
+  int df_block = -1, df_face = -1;
+  double df_mw_up = kMwAir, df_mw_lo = kMwAir;
+  double *d_zero = nullptr;
+  bool bc_initial = false;
   bool tuned[2] = {false, false};  // x / y / z sweep autotuning done [FP64, mixed]
   int forced[2][3] = {{-1, -1, -1}, {-1, -1, -1}};  // sweep variants pinned by ostc_set_sweep_variant
   int graph_kernels = 0;
@@ -2141,6 +2150,84 @@ void launch_carry(ostc_ctx *ctx, BlockRes &B, DevState in, DevState out) {
   }
 }
 
+// apply_inflow_df (BoundCond.cuh:614-754): the i = 0 plane and its ngg ghost layers, over the face plane
+// padded by ngg, take the upper (y > 0) or lower stream with u from the tanh profile plus the filtered
+// fluctuation times DeltaU, v and w the fluctuations, and T / rho moved by the strong Reynolds analogy
+// (t' = -u' u / cp, scaled by 0.25; rho' = -t' rho / T), p from the equation of state.
+__global__ void k_df_apply(DevBlock b, DevState s, DevFace f, DevDf d, double mw_up, double mw_lo) {
+  const long long np = (long long)d.py * d.pz;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < np; t += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(t % d.py) - d.g, k = (int)(t / d.py) - d.g;
+    const double y = d.yface[t];
+    double u = 0.5 * (f.u + f.lower[1]) + 0.5 * (f.u - f.lower[1]) * tanh(2 * y / f.delta_omega);
+    const double uf = d.fluc[df_p(d, j, k, 0)] * d.delta_u;
+    const double vf = d.fluc[df_p(d, j, k, 1)] * d.delta_u;
+    const double wf = d.fluc[df_p(d, j, k, 2)] * d.delta_u;
+    const bool up = y > 0;
+    const double mw = up ? mw_up : mw_lo;
+    double T = up ? f.temperature : f.lower[5];
+    double rho = up ? f.density : f.lower[0];
+    const double *ys = up ? f.y : f.y_lower;
+    double cp = 0;
+    if (s.sv) {
+      double cpl[kMS];
+      mix_h_cp<0, double>(T, nullptr, cpl);
+      for (int l = 0; l < c_mix.ns; ++l) cp += cpl[l] * ys[l];
+    } else {
+      cp = kGamma * kRuD / kMwAir / (kGamma - 1);
+    }
+    double tf = -uf * u / cp;
+    tf *= 0.25;
+    const double rf = -tf * rho / T;
+    u += uf;
+    rho += rf;
+    T += tf;
+    const double p = rho * kRuD / mw * T;
+    const long long P = b.plane;
+    for (int ig = 0; ig <= b.g; ++ig) {
+      const long long pg = b.id(-ig, j, k);
+      s.bv[pg] = rho;
+      s.bv[P + pg] = u;
+      s.bv[2 * P + pg] = vf;
+      s.bv[3 * P + pg] = wf;
+      s.bv[4 * P + pg] = p;
+      s.bv[5 * P + pg] = T;
+      if (s.sv)
+        for (int l = 0; l < c_mix.ns; ++l) s.sv[l * P + pg] = ys[l];
+      finish_node(b, s, pg);
+    }
+  }
+}
+
+// generate_random_numbers + apply_convolution (DigitalFilter.cu:367-397) and compute_fluctuations
+// (:399-407) of the filter, dtp the device dt the time correlation uses.
+void enqueue_df_fluctuations(ostc_ctx *ctx, const double *dtp, const DevFace &f) {
+  const DevDf &d = ctx->df;
+  const cudaStream_t st = ctx->stream;
+  k_df_generate<<<grid_for(ctx, (long long)d.wy * d.wz * 3, 128), 128, 0, st>>>(d);
+  k_df_remove_mean<<<(d.wy + 127) / 128, 128, 0, st>>>(d);
+  k_df_periodic<<<grid_for(ctx, (long long)d.wy * (kDfN + d.g), 128), 128, 0, st>>>(d);
+  k_df_conv_y<<<grid_for(ctx, (long long)d.py * d.wz, 128), 128, 0, st>>>(d);
+  k_df_conv_z<<<grid_for(ctx, (long long)d.py * d.pz, 128), 128, 0, st>>>(d);
+  k_df_correlate<<<grid_for(ctx, (long long)d.py * d.pz, 128), 128, 0, st>>>(d, dtp, f.u, f.lower[1], f.delta_omega);
+}
+
+// The filter's start (DigitalFilter.cu:226-247): generator states from seed, one random field and its
+// convolutions taken as the previous field, and the first fluctuations from it.
+void df_start(ostc_ctx *ctx, unsigned long long seed) {
+  const DevDf &d = ctx->df;
+  const cudaStream_t st = ctx->stream;
+  const long long ns = (long long)d.wy * d.wz * 3, np = (long long)d.py * d.pz;
+  k_df_rng_init<<<grid_for(ctx, ns, 128), 128, 0, st>>>(d.rng, ns, seed);
+  k_df_generate<<<grid_for(ctx, ns, 128), 128, 0, st>>>(d);
+  k_df_remove_mean<<<(d.wy + 127) / 128, 128, 0, st>>>(d);
+  k_df_periodic<<<grid_for(ctx, (long long)d.wy * (kDfN + d.g), 128), 128, 0, st>>>(d);
+  k_df_conv_y<<<grid_for(ctx, (long long)d.py * d.wz, 128), 128, 0, st>>>(d);
+  k_df_conv_z<<<grid_for(ctx, np, 128), 128, 0, st>>>(d);
+  cudaMemcpyAsync(d.vold, d.vnew, 3 * np * sizeof(double), cudaMemcpyDeviceToDevice, st);
+  k_df_first<<<grid_for(ctx, np, 128), 128, 0, st>>>(d);
+}
+
 // gam_prev: where a mixture far-field face reads the gamma of its face node - the properties of the
 // stage input (the reference's in-place state holds the last properties sweep there); null = out's.
 void launch_bcs(ostc_ctx *ctx, int block, DevState out, const double *gam_prev = nullptr) {
@@ -2151,7 +2238,17 @@ void launch_bcs(ostc_ctx *ctx, int block, DevState out, const double *gam_prev =
     const int t0 = f.face == 0 ? 1 : 0, t1 = f.face == 2 ? 1 : 2;
     const long long nn = (long long)(f.re[t0] - f.rs[t0] + 1) * (f.re[t1] - f.rs[t1] + 1);
     long tok = begin_t(ctx, "bc_face");
-    k_bc_face<<<grid_for(ctx, nn, 128), 128, 0, ctx->stream>>>(B.db, out, f, gam_prev ? gam_prev : out.gam);
+    if (f.type == kInflow && f.fluct == 11) {
+      // the digital filter (BoundCond.cuh:1561-1573): new random field, its convolutions, the time
+      // correlation with the current dt (zero at the initial application unless dt is fixed), then the
+      // inflow plane
+      enqueue_df_fluctuations(ctx, ctx->bc_initial && !ctx->der.fixed_time_step ? ctx->d_zero : ctx->d_dt, f);
+      const long long np = (long long)ctx->df.py * ctx->df.pz;
+      k_df_apply<<<grid_for(ctx, np, 128), 128, 0, ctx->stream>>>(B.db, out, f, ctx->df, ctx->df_mw_up,
+                                                                   ctx->df_mw_lo);
+    } else {
+      k_bc_face<<<grid_for(ctx, nn, 128), 128, 0, ctx->stream>>>(B.db, out, f, gam_prev ? gam_prev : out.gam);
+    }
     end_t(ctx, tok);
   }
 }
@@ -2247,7 +2344,9 @@ bool set_mix_attrs(int nv) {
 
 int initialise(ostc_ctx *ctx) {
   // Driver::initialize_computation (Driver.cu:115-199): BCs, properties, then cv <- bv (RK.cuh:37-45)
+  ctx->bc_initial = true;
   for (size_t b = 0; b < ctx->blk.size(); ++b) launch_bcs(ctx, (int)b, state_of(ctx->blk[b], 0));
+  ctx->bc_initial = false;
   launch_interfaces(ctx, 0);
   for (auto &B : ctx->blk) {
     if (ctx->mixture) {
@@ -3106,12 +3205,93 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
         size = std::max(size, (n1 + 2 * HB.ngg) * (n2 + 2 * HB.ngg));
       }
     }
-    if (n_fluct > 1) {
-      // the reference draws every such face from one shared array, in face order; this library runs
-      // one fluctuating face
+    int n_df = 0;
+    for (size_t bi = 0; bi < ctx->blk.size(); ++bi)
+      for (size_t fi = 0; fi < ctx->blk[bi].faces.size(); ++fi)
+        if (ctx->blk[bi].faces[fi].type == kInflow && ctx->blk[bi].faces[fi].fluct == 11) {
+          ++n_df;
+          ctx->df_block = (int)bi;
+          ctx->df_face = (int)fi;
+        }
+    if (n_fluct > 1 || n_df > 1 || (n_fluct && n_df)) {
+      // the reference draws every white-noise face from one shared array, in face order, and supports
+      // one digital-filter face; this library runs one fluctuating inflow face
       g_create_error = "more than one inflow face with fluctuation_type 1 is not provided";
       ostc_destroy(ctx.release());
       return OSTC_EINVAL;
+    }
+    if (n_df) {
+      // DBoundCond::initialize_digital_filter (DigitalFilter.cu:8-247): buffers, the Lund matrix of the
+      // Gaussian Reynolds stresses, the filter coefficients from the scaled y spacing and the mean z
+      // spacing, then the first random field
+      const HostBlock &HB = ctx->mesh.blocks[ctx->df_block];
+      const BcFace &hf = HB.faces[ctx->df_face];
+      DevDf &d = ctx->df;
+      d.my = HB.my;
+      d.mz = HB.mz;
+      d.g = HB.ngg;
+      d.wy = d.my + 2 * (kDfN + d.g);
+      d.wz = d.mz + 2 * (kDfN + d.g);
+      d.py = d.my + 2 * d.g;
+      d.pz = d.mz + 2 * d.g;
+      // DeltaU of write_reference_state (Driver.cu:252-276): the difference of the streams' speeds
+      d.delta_u = std::fabs(std::sqrt(hf.u * hf.u + hf.v * hf.v + hf.w * hf.w) -
+                            std::sqrt(hf.lower[1] * hf.lower[1] + hf.lower[2] * hf.lower[2] + hf.lower[3] * hf.lower[3]));
+      if (ctx->mixture) {
+        double a = 0, b2 = 0;
+        for (int l = 0; l < ctx->der.n_spec; ++l) {
+          a += hf.y[l] / ctx->chem.mw[l];
+          b2 += hf.y_lower[l] / ctx->chem.mw[l];
+        }
+        ctx->df_mw_up = 1 / a;
+        ctx->df_mw_lo = 1 / b2;
+      }
+      const long long ns = (long long)d.wy * d.wz * 3, nf = (long long)d.py * d.wz * 3,
+                      np = (long long)d.py * d.pz;
+      std::vector<double> ysc(d.py), yface((size_t)np);
+      const double yref = hf.delta_omega;
+      for (int j = -d.g; j < d.my + d.g; ++j) ysc[j + d.g] = HB.y[HB.cidx(0, j, 0)] / yref;
+      for (int k = -d.g; k < d.mz + d.g; ++k)
+        for (int j = -d.g; j < d.my + d.g; ++j) yface[(size_t)(k + d.g) * d.py + (j + d.g)] = HB.y[HB.cidx(0, j, k)];
+      double dz = 0;
+      for (int k = 1; k < d.mz; ++k) dz += HB.z[HB.cidx(0, 0, k)] - HB.z[HB.cidx(0, 0, k - 1)];
+      dz /= d.mz - 1;
+      double *ysc_d = nullptr, *yface_d = nullptr;
+      bool okd = cudaMalloc(&d.rng, ns * sizeof(curandState)) == cudaSuccess &&
+                 cudaMalloc(&d.r, ns * sizeof(double)) == cudaSuccess &&
+                 cudaMalloc(&d.fy, nf * sizeof(double)) == cudaSuccess &&
+                 cudaMalloc(&d.vnew, 3 * np * sizeof(double)) == cudaSuccess &&
+                 cudaMalloc(&d.vold, 3 * np * sizeof(double)) == cudaSuccess &&
+                 cudaMalloc(&d.fluc, 3 * np * sizeof(double)) == cudaSuccess &&
+                 cudaMalloc(&d.lund, 6 * (size_t)d.py * sizeof(double)) == cudaSuccess &&
+                 cudaMalloc(&d.by, (2 * kDfN + 1) * (size_t)d.py * sizeof(double)) == cudaSuccess &&
+                 cudaMalloc(&d.bz, (2 * kDfN + 1) * (size_t)d.py * sizeof(double)) == cudaSuccess &&
+                 cudaMalloc(&yface_d, np * sizeof(double)) == cudaSuccess &&
+                 cudaMalloc(&ysc_d, d.py * sizeof(double)) == cudaSuccess &&
+                 cudaMalloc(&ctx->d_zero, sizeof(double)) == cudaSuccess;
+      d.yface = yface_d;
+      if (!okd) {
+        cudaFree(ysc_d);
+        g_create_error = "device allocation for the digital filter failed";
+        ostc_destroy(ctx.release());
+        return OSTC_ENOMEM;
+      }
+      cudaMemset(d.r, 0, ns * sizeof(double));
+      cudaMemset(d.fy, 0, nf * sizeof(double));
+      cudaMemset(ctx->d_zero, 0, sizeof(double));
+      cudaMemcpy(ysc_d, ysc.data(), ysc.size() * sizeof(double), cudaMemcpyHostToDevice);
+      cudaMemcpy(yface_d, yface.data(), yface.size() * sizeof(double), cudaMemcpyHostToDevice);
+      const auto &R = hf.df_rij;
+      k_df_lund<<<(d.py + 127) / 128, 128, 0, ctx->stream>>>(d, ysc_d, R[0], R[1], R[2], R[3], R[4], R[5]);
+      k_df_coeffs<<<(d.py + 127) / 128, 128, 0, ctx->stream>>>(d, ysc_d, dz / yref);
+      df_start(ctx.get(), (unsigned long long)std::time(nullptr));
+      cudaStreamSynchronize(ctx->stream);
+      cudaFree(ysc_d);
+      if (cudaGetLastError() != cudaSuccess) {
+        g_create_error = "digital filter set-up failed on the device";
+        ostc_destroy(ctx.release());
+        return OSTC_ECUDA;
+      }
     }
     if (size > 0) {
       if (cudaMalloc(&ctx->rng, size * sizeof(curandState)) != cudaSuccess) {
@@ -3223,6 +3403,10 @@ void ostc_destroy(ostc_ctx *ctx) {
     }
   }
   cudaFree(ctx->rng);
+  for (void *p : {(void *)ctx->df.rng, (void *)ctx->df.r, (void *)ctx->df.fy, (void *)ctx->df.vnew,
+                  (void *)ctx->df.vold, (void *)ctx->df.fluc, (void *)ctx->df.lund, (void *)ctx->df.by,
+                  (void *)ctx->df.bz, (void *)ctx->df.yface, (void *)ctx->d_zero})
+    cudaFree(p);
   cudaFree(ctx->d_dtbits);
   cudaFree(ctx->d_dt);
   cudaFree(ctx->d_time);
@@ -3816,10 +4000,12 @@ int ostc_set_launch_mode(ostc_ctx *ctx, int mode) {
 
 int ostc_set_inflow_seed(ostc_ctx *ctx, long long seed) {
   if (!ctx) return OSTC_EINVAL;
-  if (!ctx->rng) return OSTC_OK;
+  if (!ctx->rng && !ctx->df.rng) return OSTC_OK;
   cudaSetDevice(ctx->device);
-  k_rng_init<<<grid_for(ctx, ctx->rng_size, 128), 128, 0, ctx->stream>>>(ctx->rng, ctx->rng_size,
-                                                                          (unsigned long long)seed);
+  if (ctx->rng)
+    k_rng_init<<<grid_for(ctx, ctx->rng_size, 128), 128, 0, ctx->stream>>>(ctx->rng, ctx->rng_size,
+                                                                            (unsigned long long)seed);
+  if (ctx->df.rng) df_start(ctx, (unsigned long long)seed);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
   return OSTC_OK;

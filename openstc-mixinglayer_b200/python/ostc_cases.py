@@ -136,6 +136,10 @@ class Case:
                       "bool compatible_mixing_layer = 0"]
             if "freestream" in self.bc_structs and not self.freestream:
                 lines.append("string reference_state = freestream")
+            if "df_rij" in m:
+                # the digital filter's Gaussian Reynolds-stress supplier (DigitalFilter.cu:309-345)
+                lines += ["int reynolds_stress_supplier = 2", "array real df_reynolds_gaussian_peak {",
+                          "    " + " ".join(repr(float(v)) for v in m["df_rij"]), "}"]
             for side in ("upper", "lower"):
                 lines.append(f"struct {side}_stream = {{")
                 lines += [f"    real {k} = {v!r}" for k, v in m[side].items()]
@@ -940,7 +944,8 @@ def spatial_mixing_layer_3d(mx=64, my=48, mz=12, seed=0, steps=20, h=0.125, delt
     """Spatially developing mixing layer (problem_type 1, the layout of the reference's shipped input):
     the two-stream inflow profile at i = 0 (u blended by tanh(2 y / delta_omega), upper / lower stream
     state by the sign of y), optionally with white noise on its velocity (fluctuation_type 1, relative
-    intensity `intensity`, within |y| < 4 delta_omega); outflow at the other x face and both y faces;
+    intensity `intensity`, within |y| < 4 delta_omega) or the digital filter's turbulent fluctuations
+    (fluctuation_type 11, 3-D with mz - 1 >= 50 + ngg); outflow at the other x face and both y faces;
     periodic z (3-D).  Air: upper 300 K, lower 500 K at 1 bar; species: H2/N2 fuel above (300 K) over
     air (600 K) with the 9-species mechanism, frozen unless finite_rate.  Stream Mach numbers from
     ma_c and the velocity ratio (lower stream faster unless upper_faster).  Grid in units of
@@ -967,6 +972,9 @@ def spatial_mixing_layer_3d(mx=64, my=48, mz=12, seed=0, steps=20, h=0.125, delt
         scheme_id = inviscid_scheme or 4
     ml = dict(ma_c=ma_c, delta_omega=delta_omega, velocity_ratio=velocity_ratio, upper_faster=upper_faster,
               upper=upper, lower=lower)
+    if fluctuation_type == 11:
+        # the digital filter's peak Reynolds stresses R11 R12 R22 R13 R23 R33 (the reference's input values)
+        ml["df_rij"] = [0.15, 0.09, 0.12, 0.05, 0.05, 0.118]
     faces = [Face((0, 0, 0, my - 1, 0, mz - 1), 5), Face((mx - 1, mx - 1, 0, my - 1, 0, mz - 1), 6),
              Face((0, mx - 1, 0, 0, 0, mz - 1), 6), Face((0, mx - 1, my - 1, my - 1, 0, mz - 1), 6)]
     if mz > 1:

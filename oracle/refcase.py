@@ -86,7 +86,10 @@ def write_reference_case(case, steps: int, directory: os.PathLike, setup_extra: 
     ml = getattr(case, "mixing_layer", None)
     # a mixing-layer case names its own delta_omega and its inflow struct `freestream` is the reference
     # state (problem_type 1)
-    setup += EXTRA.replace("real delta_omega = 1e-3\n", "") if ml else EXTRA
+    extra = EXTRA.replace("real delta_omega = 1e-3\n", "") if ml else EXTRA
+    if ml and "df_rij" in ml:
+        extra = extra.replace("int reynolds_stress_supplier = 0\n", "")
+    setup += extra
     own_fs = "freestream" in getattr(case, "bc_structs", {})
     if not case.freestream and not own_fs:
         setup += FREESTREAM.replace("@MACH@", "0.5").replace("@P@", repr(p0)).replace("@T@", repr(t0))

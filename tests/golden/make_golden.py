@@ -123,6 +123,9 @@ CASES = [
     ("sml2d_air_noise", "spatial_mixing_layer_3d", dict(mx=48, my=40, mz=1, fluctuation_type=1), 15),
     ("sml3d_species_noise", "spatial_mixing_layer_3d",
      dict(mx=32, my=24, mz=6, species=True, fluctuation_type=1, intensity=0.02), 6),
+    # the digital filter's turbulent inflow (fluctuation_type 11), air and 9-species
+    ("sml3d_air_df", "spatial_mixing_layer_3d", dict(mx=24, my=32, mz=56, fluctuation_type=11), 6),
+    ("sml3d_species_df", "spatial_mixing_layer_3d", dict(mx=20, my=24, mz=56, species=True, fluctuation_type=11), 4),
     ("ml3d_inflow_noise", "mixing_layer_3d", dict(mx=32, my=20, mz=12, ybc="outflow", xbc="inflow", inflow_noise=0.01), 10),
     # the reference's steady driver (SteadySim.cuh): local time steps, explicit or DPLUR implicit
     # treatment (DPLUR.cuh), the chemical source explicit, point-implicit (EPI) or diagonal (DA).  No

@@ -100,8 +100,9 @@ def load(path):
 
 
 def noisy(kwargs) -> bool:
-    """Whether a fixture's case draws white inflow noise (the oracle does not restate the generator)."""
-    return kwargs.get("fluctuation_type", 0) == 1 or kwargs.get("inflow_noise", 0) > 0
+    """Whether a fixture's case draws inflow noise (white noise or the digital filter's random fields: the
+    oracle does not restate the generator)."""
+    return kwargs.get("fluctuation_type", 0) in (1, 11) or kwargs.get("inflow_noise", 0) > 0
 
 
 def meta(path):

@@ -12,6 +12,12 @@ ghost-padded face plane seeded as curand_init(seed + i, i, 0) (BoundCond.cu:1384
 pinned against the reference build's own fixtures (tests/golden, seed = the clock the harness fixed);
 here: the face values minus the profile, scaled by intensity times speed, are standard normal (mean and
 spread), zero outside the band, repeatable for one seed and different for another.
+
+With fluctuation_type 11 the digital filter (DigitalFilter.cu) replaces the noise: per application a new
+normal field over the face plane, made zero-mean and unit-rms along z, filtered in y and z, correlated
+in time with the previous field and scaled by the Cholesky factor of a Gaussian Reynolds-stress profile;
+the face velocity carries it times the streams' velocity difference.  Also pinned by reference-build
+fixtures; here: its spread at the layer centre and its seed behaviour.
 """
 import numpy as np
 import pytest
@@ -109,3 +115,27 @@ def test_more_than_one_noisy_face_refused(built, tmp_path):
     case.faces[1] = oc.Face(case.faces[1].raw, 5)  # the x-max face becomes a second noisy inflow
     with pytest.raises(ostc.OstcError, match="more than one inflow face"):
         _solver(case, tmp_path, "two")
+
+
+def test_digital_filter_spread_and_seed(built, tmp_path):
+    """v on the inflow plane over the velocity difference has the rms sqrt(R22 exp(-2 (y / delta_omega)^2))
+    of the Lund transform (R22 = 0.12) near the layer centre; one seed repeats, another does not."""
+    case = oc.spatial_mixing_layer_3d(mx=16, my=40, mz=64, fluctuation_type=11)
+    st = case.mixing_layer_streams()
+    du = abs(st["upper"][1] - st["lower"][1])
+    out = []
+    for n, seed in enumerate((21, 21, 22)):
+        s = _solver(case, tmp_path, f"df{n}")
+        s.set_inflow_seed(seed)
+        s.step(2)
+        out.append(s.get_state()[1])
+        s.close()
+    assert np.array_equal(out[0], out[1])
+    assert not np.array_equal(out[0], out[2])
+    ys = case.y[0, :, 0] * case.grid_scale / st["delta_omega"]
+    rows = np.abs(ys) < 0.5
+    v = out[0][2, :, :, 0][:, rows] / du
+    want = np.sqrt(0.12 * np.exp(-2 * ys[rows] ** 2))
+    ratio = float(np.sqrt(np.mean(v ** 2)) / np.sqrt(np.mean(want ** 2)))
+    assert 0.6 < ratio < 1.4, ratio
+    assert abs(float(np.mean(v))) < 0.2 * float(np.sqrt(np.mean(want ** 2)))

@@ -158,6 +158,15 @@ def test_boundary_faces_probe(built, tmp_path):
         fl.bc_structs["inflow"][key] = ("int", val)
         with pytest.raises(ostc.OstcError, match=key):
             ostc.probe_case(str(oc.write_case(fl, tmp_path / f"fl_{key}_{val}")))
+    # the digital filter: a 3-D block with enough spanwise planes and the Gaussian stress supplier
+    df = oc.spatial_mixing_layer_3d(mx=12, my=10, mz=56, fluctuation_type=11)
+    assert ostc.probe_case(str(oc.write_case(df, tmp_path / "df")))["n_faces"] == len(df.faces)
+    with pytest.raises(ostc.OstcError, match="mz - 1 >= 50"):
+        ostc.probe_case(str(oc.write_case(oc.spatial_mixing_layer_3d(mx=12, my=10, mz=20, fluctuation_type=11),
+                                          tmp_path / "df_thin")))
+    with pytest.raises(ostc.OstcError, match="3-D block"):
+        ostc.probe_case(str(oc.write_case(oc.spatial_mixing_layer_3d(mx=12, my=10, mz=1, fluctuation_type=11),
+                                          tmp_path / "df_2d")))
     # a mixing-layer problem (problem_type 1) parses its streams; without them it is refused
     ml = oc.spatial_mixing_layer_3d(mx=12, my=10, mz=6, fluctuation_type=1)
     assert ostc.probe_case(str(oc.write_case(ml, tmp_path / "ml")))["n_faces"] == len(ml.faces)
