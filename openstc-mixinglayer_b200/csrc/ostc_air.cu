@@ -1615,6 +1615,10 @@ struct ostc_ctx {
   unsigned *d_flags = nullptr;
   cudaGraphExec_t graph = nullptr;
   int graph_precision = -1;
+  // one steady / dual-time iteration captured as a graph: key = 2 x mixed + dual, with its physical dt
+  cudaGraphExec_t steady_graph = nullptr;
+  int steady_key = -1;
+  double steady_dt = 0;
   int launch_mode = OSTC_LAUNCH_GRAPH;
   // white-noise inflow: one generator state per node of the largest fluctuating face plane, shared by
   // the faces as the reference shares one array (BoundCond.cu:1706-1735); seeded by ostc_set_inflow_seed
@@ -3370,6 +3374,7 @@ void ostc_destroy(ostc_ctx *ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+  if (ctx->steady_graph) cudaGraphExecDestroy(ctx->steady_graph);
   for (auto &B : ctx->blk) {
     cudaFree(B.met);
     cudaFree(B.jac);
@@ -4101,6 +4106,35 @@ int ostc_residual(ostc_ctx *ctx, double res[4]) {
   return OSTC_OK;
 }
 
+// One steady (dt_phys = 0) or dual-time inner iteration: replayed from a captured graph (captured on
+// first use per precision and physical dt), or launched kernel by kernel while timing or in the
+// per-block launch mode.
+static int steady_iteration(ostc_ctx *ctx, double dt_phys) {
+  const bool mixed = ctx->precision == OSTC_PREC_MIXED;
+  if (ctx->timing || ctx->launch_mode == OSTC_LAUNCH_BLOCK_LOOP)
+    return mixed ? enqueue_steady_iteration<float>(ctx, dt_phys) : enqueue_steady_iteration<double>(ctx, dt_phys);
+  const int key = (mixed ? 2 : 0) + (dt_phys > 0.0 ? 1 : 0);
+  if (!ctx->steady_graph || ctx->steady_key != key || ctx->steady_dt != dt_phys) {
+    if (ctx->steady_graph) {
+      cudaGraphExecDestroy(ctx->steady_graph);
+      ctx->steady_graph = nullptr;
+    }
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const int r = mixed ? enqueue_steady_iteration<float>(ctx, dt_phys) : enqueue_steady_iteration<double>(ctx, dt_phys);
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (r) return r;
+    CK(e);
+    const cudaError_t ei = cudaGraphInstantiate(&ctx->steady_graph, g, 0);
+    cudaGraphDestroy(g);
+    CK(ei);
+    ctx->steady_key = key;
+    ctx->steady_dt = dt_phys;
+  }
+  CK(cudaGraphLaunch(ctx->steady_graph, ctx->stream));
+  return OSTC_OK;
+}
+
 int ostc_steady_step(ostc_ctx *ctx, int max_iter, int *iters_done, double *err_max) {
   if (!ctx || max_iter < 0) return OSTC_EINVAL;
   cudaSetDevice(ctx->device);
@@ -4116,9 +4150,7 @@ int ostc_steady_step(ostc_ctx *ctx, int max_iter, int *iters_done, double *err_m
     if (check)
       for (auto &B : ctx->blk)
         k_store_last<<<grid_for(ctx, B.db.n, 256), 256, 0, ctx->stream>>>(B.db, state_of(B, 0), B.last);
-    const int r = ctx->precision == OSTC_PREC_MIXED ? enqueue_steady_iteration<float>(ctx)
-                                                     : enqueue_steady_iteration<double>(ctx);
-    if (r) return r;
+    if (int r = steady_iteration(ctx, 0.0)) return r;
     ctx->steady_iter = step;
     ++done;
     if (check) {
@@ -4175,9 +4207,7 @@ int ostc_dual_time_step(ostc_ctx *ctx, int n_steps, int *inner_iters) {
       if (monitor)
         for (auto &B : ctx->blk)
           k_store_last<<<grid_for(ctx, B.db.n, 256), 256, 0, ctx->stream>>>(B.db, state_of(B, 0), B.last);
-      const int r = ctx->precision == OSTC_PREC_MIXED ? enqueue_steady_iteration<float>(ctx, dt)
-                                                       : enqueue_steady_iteration<double>(ctx, dt);
-      if (r) return r;
+      if (int r = steady_iteration(ctx, dt)) return r;
       if (monitor) {
         // inner_converged (DualTimeStepping.cu:32-135)
         double res[4];
@@ -4835,6 +4865,10 @@ int ostc_set_sweep_variant(ostc_ctx *ctx, int precision, int dir, int variant) {
   if (ctx->graph) {
     cudaGraphExecDestroy(ctx->graph);
     ctx->graph = nullptr;
+  }
+  if (ctx->steady_graph) {
+    cudaGraphExecDestroy(ctx->steady_graph);
+    ctx->steady_graph = nullptr;
   }
   if (variant < 0) {
     std::lock_guard<std::mutex> lk(g_tune_mutex);

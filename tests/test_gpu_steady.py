@@ -26,6 +26,8 @@ from oracle import Oracle
 pytestmark = pytest.mark.gpu
 
 STEADY = dict(steady=1, implicit_method=0, dplur_inner_step=3, chem_src_method=0, convergence_criteria=1e-300)
+DUAL = dict(steady=0, temporal_scheme=2, implicit_method=1, dplur_inner_step=2, inner_iteration=4,
+            max_inner_iteration=8, iteration_adjust_step=2)
 REFERENCE_STEADY = ["st_ml3d_explicit", "st_ml3d_dplur", "st_ml2d_dplur", "st_rml3d_epi", "st_rml3d_da",
                     "st_rml3d_dplur_epi", "st_rml3d_dplur_explicit", "st_rml3d_mix_dplur"]
 
@@ -114,3 +116,26 @@ def test_dual_time_inner_adaptation_matches_oracle(built, tmp_path):
     assert all(m < gu.TOL and l2 < gu.TOL for m, l2 in err), err
     assert abs(s.time() - o.time()) <= 1e-14 * o.time()
     s.close()
+
+
+@pytest.mark.parametrize("kind", ["steady_mixture_dplur_epi", "dual_air"])
+def test_iteration_graph_equals_kernel_loop(built, tmp_path, kind):
+    """A steady or dual-time iteration replayed from its captured graph gives the state the same
+    iteration launched kernel by kernel gives (OSTC_LAUNCH_BLOCK_LOOP), bit for bit."""
+    if kind == "dual_air":
+        case = oc.mixing_layer_3d(mx=24, my=20, mz=12, ybc="outflow", steady=dict(DUAL, dt=2e-7))
+    else:
+        case = oc.reacting_mixing_layer_3d(mx=16, my=12, mz=8,
+                                           steady=dict(STEADY, implicit_method=1, chem_src_method=1))
+    out = []
+    for mode in (ostc.LAUNCH_GRAPH, ostc.LAUNCH_BLOCK_LOOP):
+        s = ostc.Solver(str(oc.write_case(case, tmp_path / f"m{mode}")))
+        s.set_launch_mode(mode)
+        s.set_state(case.bv, sv=case.sv)
+        if kind == "dual_air":
+            s.dual(4)
+        else:
+            s.steady(6)
+        out.append(s.get_state()[0])
+        s.close()
+    assert np.array_equal(out[0], out[1])
