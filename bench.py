@@ -28,6 +28,8 @@ inviscid + viscous RHS, update, boundaries).  One cell-step = one interior node 
            over the default workload and its ghost layer: device time and HBM fraction
 
 --only air|reacting|multiblock runs one workload for a few steps and prints its device time per step
+(--only adjoint: that many right-hand-side VJPs of the 9-species layer, 192 x 96 x 48 unless --dims;
+--only adjoint_air: of the air layer with outflow y faces, 512 x 256 x 128 unless --dims)
 (the short command to put under a profiler, where the whole benchmark would launch too much); it
 takes --dims, --steps, --precision and --chem.
 
@@ -91,7 +93,7 @@ def parse():
     p.add_argument("--cpu-steps", type=int, default=3)
     p.add_argument("--no-extra", action="store_true",
                    help="skip the reacting (9-species) and uneven multi-block workloads")
-    p.add_argument("--only", choices=["air", "reacting", "multiblock"], default=None,
+    p.add_argument("--only", choices=["air", "reacting", "multiblock", "adjoint", "adjoint_air"], default=None,
                    help="run one workload for --steps steps and print its device time per step")
     p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64", help="with --only")
     p.add_argument("--chem", choices=["explicit", "point_implicit"], default="explicit", help="with --only")
@@ -106,6 +108,8 @@ def run_only(args):
     import ostc_cases as oc
 
     tmp = tempfile.mkdtemp(prefix=f"ostc_{args.only}_")
+    if args.only in ("adjoint", "adjoint_air"):
+        return run_only_vjp(args, tmp)
     if args.only == "multiblock":
         case = oc.multiblock_mixing_layer_3d(seed=0, uneven_axes=True)
     elif args.only == "reacting":
@@ -126,6 +130,45 @@ def run_only(args):
     flags = s.error_flags()
     print(json.dumps({"only": args.only, "nodes": s.total_nodes(), "steps": args.steps, "precision": args.precision,
                       "ms_per_step": ms / args.steps, "error_flags": flags}))
+    s.close()
+    raise SystemExit(1 if flags else 0)
+
+
+def run_only_vjp(args, tmp):
+    """args.steps right-hand-side VJPs (all terms) of the reacting or the air layer, device-resident
+    buffers; the time of one right-hand side beside it."""
+    import ctypes
+    import time
+
+    import ostc
+    import ostc_cases as oc
+    import torch
+
+    if args.only == "adjoint_air":
+        case = oc.mixing_layer_3d(*args.dims, seed=0, ybc="outflow")
+    else:
+        case = oc.reacting_mixing_layer_3d(*(args.dims if args.dims_given else (192, 96, 48)), seed=0)
+    oc.write_case(case, tmp)
+    s = ostc.Solver(tmp)
+    s.set_state(case.bv, sv=getattr(case, "sv", None))
+    shape = s.get_state()[0].shape
+    dev = torch.device("cuda", 0)
+    wb = torch.randn(shape, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(0))
+    gb = torch.empty_like(wb)
+    vjp = lambda: s.lib.ostc_rhs_vjp(s.h, 0, 7, ctypes.c_void_p(wb.data_ptr()), ctypes.c_void_p(gb.data_ptr()), 1)
+    rhs = lambda: s.lib.ostc_rhs(s.h, 0, 7, ctypes.c_void_p(gb.data_ptr()), 1)
+    times = {}
+    for name, call in (("rhs", rhs), ("vjp", vjp)):
+        assert call() == 0  # first call: scratch allocation, autotuning
+        torch.cuda.synchronize(dev)
+        t = time.perf_counter()  # the calls synchronise the library stream
+        for _ in range(args.steps):
+            assert call() == 0
+        times[name] = (time.perf_counter() - t) * 1e3 / args.steps
+    flags = s.error_flags()
+    print(json.dumps({"only": args.only, "nodes": s.total_nodes(), "vjps": args.steps, "ms_per_rhs": times["rhs"],
+                      "ms_per_vjp": times["vjp"], "vjp_over_rhs": times["vjp"] / times["rhs"],
+                      "error_flags": flags}))
     s.close()
     raise SystemExit(1 if flags else 0)
 

@@ -123,15 +123,17 @@ int ostc_set_conservative(ostc_ctx *ctx, int block, const double *cv, int ptr_ki
  * ghost nodes by the boundary faces, transport properties) following cv as ostc_set_conservative
  * defines it.  dq_bar and cv_bar have the layout of dq.  The product is that of the FP64 right-hand
  * side.  Covers the multi-component path (species = 1; inviscid_scheme 71 / 72, viscous, explicit
- * finite-rate source) on a single block with periodic and outflow faces; anything else returns
- * OSTC_EINVAL.  Accumulation uses atomics: results agree run to run to rounding. */
+ * finite-rate source) and the air path (AWENO: WENO5-Z / WENO7-Z reconstruction with AUSM+, HLLC or
+ * Lax-Friedrichs, and the viscous terms) on a single block with periodic and outflow faces; anything
+ * else returns OSTC_EINVAL.  Accumulation uses atomics: results agree run to run to rounding. */
 int ostc_rhs_vjp(ostc_ctx *ctx, int block, unsigned term_mask, const double *dq_bar, double *cv_bar,
                  int ptr_kind);
 
 /* Adjoint of one SSP-RK3 step (RK.cuh:85-185, stage coefficients :10-14) from the current state, with
  * the step's dt (CFL of the current state, or the fixed dt) held constant: lam_in = (d q' / d q)^T
  * lam_out, q the interior conservative state before the step and q' after it (layout of dq).  The
- * state is left as it was.  Same coverage as ostc_rhs_vjp, FP64 precision mode only. */
+ * state is left as it was.  The multi-component coverage of ostc_rhs_vjp (air returns OSTC_EINVAL),
+ * FP64 precision mode only. */
 int ostc_rk3_step_vjp(ostc_ctx *ctx, const double *lam_out, double *lam_in, int ptr_kind);
 
 /* Checkpointed discrete adjoint of n_steps SSP-RK3 steps from the current state: runs the steps

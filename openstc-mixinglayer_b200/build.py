@@ -8,7 +8,7 @@ from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
-SOURCES = ["csrc/host.cpp", "csrc/chem.cpp", "csrc/ostc_air.cu", "csrc/ostc_noalloc.cu"]
+SOURCES = ["csrc/host.cpp", "csrc/chem.cpp", "csrc/ostc_b200.cu", "csrc/ostc_noalloc.cu"]
 OUT = PKG / "libostc_b200.so"
 OUT_CHECKED = PKG / "libostc_b200_checked.so"  # -DOSTC_BOUNDS_CHECK: index-checked accessors
 

@@ -1,4 +1,4 @@
-// ostc_mix.cuh -- kernels of the multi-component path (species = 1; included by ostc_air.cu after
+// ostc_mix.cuh -- kernels of the multi-component path (species = 1; included by ostc_b200.cu after
 // DevBlock/DevState).  Per RK stage (RK.cuh:112-172): the chemical source initialises dq, the
 // flux-split WENO7 sweeps and the viscous sweeps accumulate into it, the update kernel combines the
 // stage and solves the temperature, the boundary faces fill the ghosts, and the properties kernel

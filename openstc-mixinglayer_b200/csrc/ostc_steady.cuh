@@ -1,7 +1,7 @@
 // ostc_steady.cuh -- the reference's steady driver (steady_simulation, SteadySim.cuh:15-140) on the
 // device: per-node local time steps, the point-implicit chemical source (EPI / diagonal approximation,
 // FiniteRateChem.cu:197-254, 414-426) and the DPLUR implicit operator (DPLUR.cuh:14-327, DPLUR.cu:5-40).
-// Included by ostc_air.cu after the air and mixture kernels; the host side is ostc_steady_step there.
+// Included by ostc_b200.cu after the air and mixture kernels; the host side is ostc_steady_step there.
 //
 // Layout: every per-node array of this driver is interior-indexed like dq (node n = (k*my + j)*mx + i):
 // dt_local[n], the inviscid spectral radii srad[d*N + n] (d = 0..2), the chemical source Jacobian

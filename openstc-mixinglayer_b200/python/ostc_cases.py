@@ -768,6 +768,10 @@ def mixing_layer_2d(mx=257, my=129, seed=0, steps=100, mc=0.4, re=1000.0, t0=300
     if ybc == "wall":
         faces = _box_faces(mx, my, 1, 8, 2, 2, 8)
         structs = {"wall": _wall_struct(wall_thermal, t0), "periodic": {"type": ("string", "periodic"), "label": ("int", 8)}}
+    elif ybc == "outflow":
+        faces = _box_faces(mx, my, 1, 8, 6, 6, 8)
+        structs = {"outflow": {"type": ("string", "outflow"), "label": ("int", 6)},
+                   "periodic": {"type": ("string", "periodic"), "label": ("int", 8)}}
     else:
         faces = _box_faces(mx, my, 1, 8, 3, 3, 8)
         structs = {"slipwall": {"type": ("string", "symmetry"), "label": ("int", 3)},

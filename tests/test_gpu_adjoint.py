@@ -67,10 +67,10 @@ def _directions(cv0, rng, n):
     return [rng.standard_normal(cv0.shape) * np.abs(cv0) for _ in range(n)]
 
 
-def _fd(s, cv0, v, mask):
+def _fd(s, cv0, v, mask, eps=EPS):
     """Central differences at 2 eps and eps combined by Richardson extrapolation (error O(eps^4))."""
     d = []
-    for h in (2 * EPS, EPS):
+    for h in (2 * eps, eps):
         s.set_conservative(cv0 + h * v)
         rp = s.rhs(mask)
         s.set_conservative(cv0 - h * v)
@@ -168,15 +168,90 @@ def test_torch_autograd_wrapper(built, tmp_path):
     assert abs(fd - ad) <= RTOL * abs(fd) + ATOL * float(np.sum(np.abs(w.numpy() * jv)))
 
 
+AIR = {"weno7_hllc_3d": lambda: oc.mixing_layer_3d(mx=24, my=20, mz=12, ybc="outflow"),
+       "weno5_ausm_3d": lambda: oc.mixing_layer_3d(mx=20, my=16, mz=12, ybc="outflow", reconstruction=4,
+                                                   inviscid_scheme=3),
+       # Lax-Friedrichs: |U| and the larger spectral radius put two kinks in every face flux, so a
+       # smaller grid keeps the differences off them
+       "weno7_lf_3d": lambda: oc.mixing_layer_3d(mx=14, my=12, mz=10, ybc="outflow", inviscid_scheme=1),
+       "weno5_ausm_2d": lambda: oc.mixing_layer_2d(mx=40, my=28, ybc="outflow")}
+
+
+def _check_air(s, cv0, mask, rng, n_dir):
+    """_check with the differences at steps 1e-7 and 1e-8, each direction judged by the better one.
+    The air right-hand side is only piecewise smooth: the HLLC contact switch (sign of the star speed),
+    AUSM+'s upwind switch (sign of the mass flux), the Lax-Friedrichs flux's |U| and larger spectral
+    radius have kinks, and a direction's difference crosses one at some face with a probability that grows
+    with the step and the number of faces (the crossing face's term then carries an O(1) error).  At
+    1e-8 the difference of nearly cancelling fluxes carries ~1e-6 of rounding, at 1e-7 ~1e-8, and at
+    1e-5 the WENO weights' curvature ~1e-3.  A wrong adjoint disagrees at both steps; a kink crossed
+    at one step leaves the other."""
+    w = rng.standard_normal(cv0.shape)
+    s.set_conservative(cv0)
+    g = s.rhs_vjp(w, mask)
+    errs = []
+    for v in _directions(cv0, rng, n_dir):
+        rhs = float(np.sum(g * v))
+        e = []
+        for eps in (1e-7, 1e-8):
+            jv = _fd(s, cv0, v, mask, eps)
+            lhs = float(np.sum(w * jv))
+            e.append(abs(lhs - rhs) / (RTOL * abs(lhs) + ATOL * float(np.sum(np.abs(w * jv)))))
+        errs.append(min(e))
+    return errs
+
+
+def _air_solver(case, tmp_path, seed=3):
+    """An air layer with 2 % seeded noise on T and p (rho from the equation of state), so that no
+    sweep sees a field that is constant along it."""
+    import ostc
+
+    rng = np.random.default_rng(seed)
+    case.bv[5] *= 1 + 2e-2 * rng.standard_normal(case.bv[5].shape)
+    case.bv[4] *= 1 + 2e-2 * rng.standard_normal(case.bv[4].shape)
+    case.bv[0] = case.bv[4] / (oc.R_AIR * case.bv[5])
+    s = ostc.Solver(str(oc.write_case(case, tmp_path / "air")))
+    s.set_state(case.bv)
+    return s, s.get_state()[0]
+
+
+@pytest.mark.parametrize("name", list(AIR))
+@pytest.mark.parametrize("mask,term", [(1, "inviscid"), (2, "viscous"), (3, "all")])
+def test_air_vjp_matches_finite_differences(built, tmp_path, name, mask, term):
+    """The air path (AWENO5/7-Z with AUSM+, HLLC or Lax-Friedrichs, Sutherland viscous terms, periodic and
+    outflow faces): ostc_rhs_vjp against Richardson central differences of ostc_rhs, 6 directions."""
+    s, cv0 = _air_solver(AIR[name](), tmp_path)
+    errs = _check_air(s, cv0, mask, np.random.default_rng(11 + mask), 6)
+    assert max(errs) <= 1.0, (name, term, errs)
+
+
+@pytest.mark.parametrize("name", ["weno7_hllc_3d", "weno5_ausm_2d"])
+def test_air_vjp_64_directions(built, tmp_path, name):
+    """64 seeded directions (all terms)."""
+    s, cv0 = _air_solver(AIR[name](), tmp_path)
+    errs = _check_air(s, cv0, 3, np.random.default_rng(64), 64)
+    assert max(errs) <= 1.0, sorted(errs)[-5:]
+
+
 def test_vjp_rejects_uncovered_cases(built, tmp_path):
     import ostc
 
-    air = oc.mixing_layer_3d(mx=24, my=16, mz=8)
+    air = oc.mixing_layer_3d(mx=24, my=16, mz=8)  # far-field y faces
     d = oc.write_case(air, tmp_path / "air")
     s = ostc.Solver(str(d))
     s.set_state(air.bv)
-    with pytest.raises(ostc.OstcError, match="multi-component"):
+    with pytest.raises(ostc.OstcError, match="periodic and outflow"):
         s.rhs_vjp(np.zeros((5,) + s.shape(0)))
+    air_out = oc.mixing_layer_3d(mx=24, my=16, mz=8, ybc="outflow")
+    s1 = ostc.Solver(str(oc.write_case(air_out, tmp_path / "air_out")))
+    s1.set_state(air_out.bv)
+    with pytest.raises(ostc.OstcError, match="step adjoint"):
+        s1.step_vjp(np.zeros((5,) + s1.shape(0)))
+    pv_air = oc.mixing_layer_3d(mx=24, my=16, mz=8, ybc="outflow", reconstruction=2)
+    s4 = ostc.Solver(str(oc.write_case(pv_air, tmp_path / "pv_air")))
+    s4.set_state(pv_air.bv)
+    with pytest.raises(ostc.OstcError, match="AWENO"):
+        s4.rhs_vjp(np.zeros((5,) + s4.shape(0)))
     case = oc.reacting_mixing_layer_3d(mx=20, my=16, mz=10)
     s2, cv0 = _solver(case, tmp_path)
     s2.set_chem_mode(ostc.CHEM_POINT_IMPLICIT)
