@@ -132,15 +132,15 @@ int ostc_rhs_vjp(ostc_ctx *ctx, int block, unsigned term_mask, const double *dq_
 /* Adjoint of one SSP-RK3 step (RK.cuh:85-185, stage coefficients :10-14) from the current state, with
  * the step's dt (CFL of the current state, or the fixed dt) held constant: lam_in = (d q' / d q)^T
  * lam_out, q the interior conservative state before the step and q' after it (layout of dq).  The
- * state is left as it was.  The multi-component coverage of ostc_rhs_vjp (air returns OSTC_EINVAL),
- * FP64 precision mode only. */
+ * state is left as it was.  Same coverage as ostc_rhs_vjp, FP64 precision mode only. */
 int ostc_rk3_step_vjp(ostc_ctx *ctx, const double *lam_out, double *lam_in, int ptr_kind);
 
 /* Checkpointed discrete adjoint of n_steps SSP-RK3 steps from the current state: runs the steps
  * (the context ends at the final state, as after ostc_rk3_step(n_steps)), keeping a device
  * checkpoint every `every` steps and each step's dt, then sweeps backwards segment by segment,
  * recomputing a segment's states from its checkpoint: lam_initial = (d q_N / d q_0)^T lam_final.
- * Device memory: (n_steps / every + every + 1) states of (n_var + 6 + n_spec) padded planes. */
+ * Device memory: (n_steps / every + every + 1) states of (n_var + 6 + n_spec) padded planes (air:
+ * n_var + 7). */
 int ostc_adjoint_steps(ostc_ctx *ctx, int n_steps, int every, const double *lam_final, double *lam_initial,
                        int ptr_kind);
 

@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(64, MarchOcc<T>::blocks) k_flux_march(DevBlock
   auto Raw = [&](int sl, int v) -> double & { return raw[(sl * NRAW + v) * nthr + tid]; };
   auto Mraw = [&](int sl, int v) -> double & { return mraw[(sl * 4 + v) * nthr + tid]; };
   auto prefetch_node = [&](int n, int sl) {
-    const long long p = base + (long long)n * stride;
+    const long long p = b.chk(base + (long long)n * stride);
 #pragma unroll
     for (int l = 0; l < 5; ++l) cp_async8(&Raw(sl, l), s.cv + l * P + p);
 #pragma unroll
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(64, MarchOcc<T>::blocks) k_flux_march(DevBlock
     cp_async8(&Raw(sl, 13), b.jac + p);
   };
   auto prefetch_metric = [&](int n, int sl) {
-    const long long p = base + (long long)n * stride;
+    const long long p = b.chk(base + (long long)n * stride);
 #pragma unroll
     for (int c = 0; c < 3; ++c) cp_async8(&Mraw(sl, c), mrow + c * P + p);
     cp_async8(&Mraw(sl, 3), b.jac + p);
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(64, MarchOcc<T>::blocks) k_flux_march(DevBlock
     for (int l = 0; l < 5; ++l) R(slot, 6 + l) = f[l];
   };
   auto load_direct = [&](int n) {
-    const long long p = base + (long long)n * stride;
+    const long long p = b.chk(base + (long long)n * stride);
     double cv[5], bv[5], km[3];
 #pragma unroll
     for (int l = 0; l < 5; ++l) {
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(64, MarchOcc<T>::blocks) k_flux_march(DevBlock
     cp_async_commit();
   }
   T fprev[5] = {T(0), T(0), T(0), T(0), T(0)};
-  long long pc = base + (long long)(s0 - 1) * stride;
+  long long pc = b.chk(base + (long long)(s0 - 1) * stride);
   T mt0[3] = {(T)mrow[pc], (T)mrow[P + pc], (T)mrow[2 * P + pc]};
   T j0 = (T)b.jac[pc];
   for (int c = s0 - 1; c < s1; ++c) {
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(64, MarchOcc<T>::blocks) k_flux_march(DevBlock
       }
     } else {
       load_direct(c + NG);
-      const long long pn = pc + stride;
+      const long long pn = b.chk(pc + stride);
 #pragma unroll
       for (int q3 = 0; q3 < 3; ++q3) mt1[q3] = (T)mrow[q3 * P + pn];
       j1 = (T)b.jac[pn];
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(TXL * TD, tile_min_blocks<T, TXL, TXL * TD>())
     for (int n = threadIdx.y; n < NP; n += TD) {
       const int d = d0 - NG + n;
       if (d >= nd + NG) continue;
-      const long long p = base + (long long)d * stride;
+      const long long p = b.chk(base + (long long)d * stride);
       T bb[5], kk[3];
 #pragma unroll
       for (int l = 0; l < 5; ++l) {
@@ -846,7 +846,7 @@ __device__ void farfield_mixture(const DevBlock &b, DevState s, const DevFace &f
     for (int l = 0; l < ns; ++l) svb[l] = f.y[l];
   } else if (mb >= 1) {
     for (int g = 1; g <= b.g; ++g) {
-      const long long pg = pb + g * dstep;
+      const long long pg = b.chk(pb + g * dstep);
       for (int l = 0; l < 6; ++l) s.bv[l * P + pg] = s.bv[l * P + pb];
       for (int l = 0; l < ns; ++l) s.sv[l * P + pg] = s.sv[l * P + pb];
       mix_cv_from_bv_node<0>(b, s, pg);
@@ -889,7 +889,7 @@ __device__ void farfield_mixture(const DevBlock &b, DevState s, const DevFace &f
     vals[5] = t;
   }
   for (int g = 0; g <= b.g; ++g) {
-    const long long pg = pb + g * dstep;
+    const long long pg = b.chk(pb + g * dstep);
 #pragma unroll
     for (int l = 0; l < 6; ++l) s.bv[l * P + pg] = vals[l];
     for (int l = 0; l < ns; ++l) s.sv[l * P + pg] = svb[l];
@@ -917,7 +917,7 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
     idx[t1] = f.rs[t1] + (int)(n / n0);
     const long long pb = b.id(idx[0], idx[1], idx[2]);
     if (f.type == kSymmetry) {
-      const long long pin = pb - dstep;
+      const long long pin = b.chk(pb - dstep);
       double kx = b.met[(f.face * 3 + 0) * P + pb], ky = b.met[(f.face * 3 + 1) * P + pb],
              kz = b.met[(f.face * 3 + 2) * P + pb];
       const double km = sqrt(kx * kx + ky * ky + kz * kz);
@@ -938,7 +938,7 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
         s.mul[pb] = sutherland(s.bv[5 * P + pb]);
       }
       for (int g = 1; g <= b.g; ++g) {
-        const long long pg = pb + g * dstep, pi = pb - g * dstep;
+        const long long pg = b.chk(pb + g * dstep), pi = b.chk(pb - g * dstep);
         s.bv[pg] = s.bv[pi];
         const double u = s.bv[P + pi], v = s.bv[2 * P + pi], w = s.bv[3 * P + pi];
         uk = kx * u + ky * v + kz * w;
@@ -953,7 +953,7 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
       }
     } else if (f.type == kOutflow) {
       for (int g = 1; g <= b.g; ++g) {
-        const long long pg = pb + g * dstep;
+        const long long pg = b.chk(pb + g * dstep);
         copy_bv(b, s, pg, pb);
         finish_node(b, s, pg);
       }
@@ -990,7 +990,7 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
         *st = local;
       }
       for (int g = 0; g <= b.g; ++g) {
-        const long long pg = pb + g * dstep;
+        const long long pg = b.chk(pb + g * dstep);
         s.bv[pg] = rho;
         s.bv[P + pg] = u;
         s.bv[2 * P + pg] = v;
@@ -1020,7 +1020,7 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
         const bool sub = fabs(u_face / ab) < 1;
         if (sub) {
           p_b = f.pressure;
-          const long long p1 = pb - dstep;
+          const long long p1 = b.chk(pb - dstep);
           const double d1 = s.bv[p1], u1 = s.bv[P + p1], v1 = s.bv[2 * P + p1], w1 = s.bv[3 * P + p1],
                        pr1 = s.bv[4 * P + p1];
           const double c1 = sqrt(kGamma * pr1 / d1);
@@ -1030,7 +1030,7 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
           w_b = w1 + nz * (pr1 - p_b) / (d1 * c1);
         }
         for (int g = 1; g <= b.g; ++g) {
-          const long long pg = pb + g * dstep, pi = pb - g * dstep;
+          const long long pg = b.chk(pb + g * dstep), pi = b.chk(pb - g * dstep);
           double r, u, v, w, pr;
           if (sub) {
             pr = 2 * p_b - s.bv[4 * P + pi];
@@ -1074,7 +1074,7 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
         const double tt = f.temperature * pow(pr / f.pressure, (kGamma - 1) / kGamma);
         const double r = pr * kMwD / (tt * kRuD);
         for (int g = 1; g <= b.g; ++g) {
-          const long long pg = pb + g * dstep;
+          const long long pg = b.chk(pb + g * dstep);
           s.bv[pg] = r;
           s.bv[P + pg] = u_new * f.u;
           s.bv[2 * P + pg] = u_new * f.v;
@@ -1089,7 +1089,7 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
       // the first interior node's pressure (and mass fractions) at the wall temperature; ghost g
       // mirrors interior node g with reversed velocity and, isothermal, T_g = 2 T_w - T_in (T_w
       // where that falls to 0.1 T_w or below)
-      const long long pin = pb - dstep;
+      const long long pin = b.chk(pb - dstep);
       const double tw = f.wall_adiabatic ? s.bv[5 * P + pin] : f.temperature;
       const double pw = s.bv[4 * P + pin];
       double mw = kMwD;
@@ -1109,7 +1109,7 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
       s.bv[5 * P + pb] = tw;
       finish_node(b, s, pb);
       for (int g = 1; g <= b.g; ++g) {
-        const long long pi = pb - g * dstep, pg = pb + g * dstep;
+        const long long pi = b.chk(pb - g * dstep), pg = b.chk(pb + g * dstep);
         const double p_i = s.bv[4 * P + pi], t_i = s.bv[5 * P + pi];
         double t_g = t_i;
         if (!f.wall_adiabatic) {
@@ -1138,7 +1138,7 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
       other[f.face] = f.direction < 0 ? ext[f.face] - 1 : 0;
       const long long po = b.id(other[0], other[1], other[2]);
       for (int g = 1; g <= b.g; ++g) {
-        const long long pg = pb + g * dstep, ps = po + g * dstep;
+        const long long pg = b.chk(pb + g * dstep), ps = b.chk(po + g * dstep);
         copy_bv(b, s, pg, ps);
         finish_node(b, s, pg);
       }
@@ -1161,7 +1161,7 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
         vals[0] = f.density; vals[1] = f.u; vals[2] = f.v; vals[3] = f.w; vals[4] = f.pressure; vals[5] = f.temperature;
       } else if (mb >= 1) {
         for (int g = 1; g <= b.g; ++g) {
-          const long long pg = pb + g * dstep;
+          const long long pg = b.chk(pb + g * dstep);
           copy_bv(b, s, pg, pb);
           finish_node(b, s, pg);
         }
@@ -1192,7 +1192,7 @@ __global__ void __launch_bounds__(128) k_bc_face(DevBlock b, DevState s, DevFace
       for (int l = 0; l < 6; ++l) s.bv[l * P + pb] = vals[l];
       finish_node(b, s, pb);
       for (int g = 1; g <= b.g; ++g) {
-        const long long pg = pb + g * dstep;
+        const long long pg = b.chk(pb + g * dstep);
 #pragma unroll
         for (int l = 0; l < 6; ++l) s.bv[l * P + pg] = vals[l];
         finish_node(b, s, pg);

@@ -786,9 +786,10 @@ int ostc_rk3_step_vjp(ostc_ctx *ctx, const double *lam_out, double *lam_in, int 
   CK(cudaMemcpyAsync(B.adj_work, lam_out, bytes,
                      ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemsetAsync(B.adj_work + 4 * (size_t)ctx->nv * B.db.n, 0, B.db.n * sizeof(double), ctx->stream));
-  if (!ctx->der.fixed_time_step) enqueue_mix_dt(ctx);
+  if (!ctx->der.fixed_time_step) enqueue_cfl_dt(ctx);
   if (int r = step_vjp(ctx)) return r;
-  if (int r = adjoint_t_to_cv(ctx)) return r;
+  if (ctx->mixture)
+    if (int r = adjoint_t_to_cv(ctx)) return r;
   CK(cudaMemcpyAsync(lam_in, B.adj_work, bytes,
                      ptr_kind == OSTC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
@@ -809,7 +810,10 @@ int ostc_adjoint_steps(ostc_ctx *ctx, int n_steps, int every, const double *lam_
   if (int r = adjoint_alloc(ctx, B)) return r;
   const int nv = ctx->nv, ns = ctx->der.n_spec;
   const long long P = B.db.plane;
-  const size_t state_doubles = (size_t)(nv + 6 + ns) * P;
+  // a saved state: cv, bv and (mixtures) the mass fractions or (air) the viscosity
+  const int nx = ctx->mixture ? ns : 1;
+  double *const xs = ctx->mixture ? B.sv[0] : B.mul[0];
+  const size_t state_doubles = (size_t)(nv + 6 + nx) * P;
   const int ncp = (n_steps + every - 1) / every;
   // device checkpoints (every `every` steps), one segment of step-start states, the final state
   double *cps = nullptr, *seg = nullptr, *fin = nullptr;
@@ -828,22 +832,28 @@ int ostc_adjoint_steps(ostc_ctx *ctx, int n_steps, int every, const double *lam_
   auto save = [&](double *dst) {
     cudaMemcpyAsync(dst, B.cv[0], (size_t)nv * P * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
     cudaMemcpyAsync(dst + (size_t)nv * P, B.bv[0], 6 * P * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
-    cudaMemcpyAsync(dst + (size_t)(nv + 6) * P, B.sv[0], (size_t)ns * P * sizeof(double), cudaMemcpyDeviceToDevice,
+    cudaMemcpyAsync(dst + (size_t)(nv + 6) * P, xs, (size_t)nx * P * sizeof(double), cudaMemcpyDeviceToDevice,
                     ctx->stream);
   };
   auto restore = [&](const double *src) {
     cudaMemcpyAsync(B.cv[0], src, (size_t)nv * P * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
     cudaMemcpyAsync(B.bv[0], src + (size_t)nv * P, 6 * P * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
-    cudaMemcpyAsync(B.sv[0], src + (size_t)(nv + 6) * P, (size_t)ns * P * sizeof(double), cudaMemcpyDeviceToDevice,
+    cudaMemcpyAsync(xs, src + (size_t)(nv + 6) * P, (size_t)nx * P * sizeof(double), cudaMemcpyDeviceToDevice,
                     ctx->stream);
-    launch_mix_props(ctx, B, state_of(B, 0));
+    if (ctx->mixture) launch_mix_props(ctx, B, state_of(B, 0));
+  };
+  auto stages = [&]() {
+    for (int rk = 0; rk < 3; ++rk) {
+      if (ctx->mixture) enqueue_mix_stage(ctx, rk);
+      else enqueue_air_stage<double>(ctx, rk);
+    }
   };
   // forward sweep: checkpoints and the dt of every step
   std::vector<double> dts(n_steps);
   for (int n = 0; n < n_steps; ++n) {
     if (n % every == 0) save(cps + (size_t)(n / every) * state_doubles);
-    if (!ctx->der.fixed_time_step) enqueue_mix_dt(ctx);
-    for (int rk = 0; rk < 3; ++rk) enqueue_mix_stage(ctx, rk);
+    if (!ctx->der.fixed_time_step) enqueue_cfl_dt(ctx);
+    stages();
     k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->d_time, ctx->d_dt, ctx->d_step);
     if (cudaMemcpyAsync(&dts[n], ctx->d_dt, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
         cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
@@ -867,7 +877,7 @@ int ostc_adjoint_steps(ostc_ctx *ctx, int n_steps, int every, const double *lam_
       save(seg + (size_t)(n - a) * state_doubles);
       if (n + 1 < b) {
         cudaMemcpyAsync(ctx->d_dt, &dts[n], sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
-        for (int rk = 0; rk < 3; ++rk) enqueue_mix_stage(ctx, rk);
+        stages();
       }
     }
     for (int n = b - 1; n >= a && rc == OSTC_OK; --n) {
@@ -877,7 +887,7 @@ int ostc_adjoint_steps(ostc_ctx *ctx, int n_steps, int every, const double *lam_
     }
   }
   // the first checkpoint is the caller's state, whose T is the equation-of-state root of its cv
-  if (rc == OSTC_OK) {
+  if (rc == OSTC_OK && ctx->mixture) {
     restore(cps);
     rc = adjoint_t_to_cv(ctx);
   }

@@ -27,6 +27,18 @@ struct DevBlock {
 #endif
     return off0 + ((long long)k * sy + j) * pitch + i;
   }
+  // A padded-plane index formed from an accessor's index plus neighbour strides (stencil offsets,
+  // ghost layers): checked in the bounds-checked build against the plane (bit 4, clamped), passed
+  // through otherwise.
+  __host__ __device__ __forceinline__ long long chk(long long p) const {
+#if defined(OSTC_BOUNDS_CHECK) && defined(__CUDA_ARCH__)
+    if (p < 0 || p >= plane) {
+      atomicOr(&g_ostc_bounds, 4u);
+      p = p < 0 ? 0 : plane - 1;
+    }
+#endif
+    return p;
+  }
   __host__ __device__ __forceinline__ long long iq(int i, int j, int k) const {
 #if defined(OSTC_BOUNDS_CHECK) && defined(__CUDA_ARCH__)
     if (i < 0 || i >= mx || j < 0 || j >= my || k < 0 || k >= mz) {

@@ -649,48 +649,8 @@ void for_blocks(ostc_ctx *ctx, F f) {
 }
 
 // One SSP-RK3 step over all blocks (RK.cuh:85-185).
-template <typename T>
-int enqueue_step(ostc_ctx *ctx) {
-  static const double A[3] = {1.0, 0.75, 1.0 / 3.0}, Bc[3] = {0.0, 0.25, 2.0 / 3.0}, C[3] = {1.0, 0.25, 2.0 / 3.0};
-  const bool fixed = ctx->der.fixed_time_step;
-  for (int rk = 0; rk < 3; ++rk) {
-    const int sin = rk, sout = (rk + 1) % 3;
-    if (rk == 0 && !fixed) {
-      long tok = begin_t(ctx, "cfl_dt");
-      k_dt_reset<<<1, 1, 0, ctx->stream>>>(ctx->d_dtbits);
-      for (auto &B : ctx->blk)
-        k_cfl_dt<<<grid_for(ctx, B.db.n, 256), 256, 0, ctx->stream>>>(B.db, state_of(B, sin), ctx->der.cfl,
-                                                                     ctx->der.prandtl, B.db.mz > 1, ctx->d_dtbits);
-      k_dt_decode<<<1, 1, 0, ctx->stream>>>(ctx->d_dtbits, ctx->d_dt);
-      end_t(ctx, tok);
-    }
-    for_blocks(ctx, [&](int bi) {
-      BlockRes &B = ctx->blk[bi];
-      launch_flux<T>(ctx, B, state_of(B, sin));
-      StageArgs a{};
-      a.in = state_of(B, sin);
-      a.qn = state_of(B, 0);
-      a.out = state_of(B, sout);
-      a.a = A[rk];
-      a.bcoef = Bc[rk];
-      a.c = C[rk];
-      a.dt = ctx->d_dt;
-      a.prandtl = ctx->der.prandtl;
-      a.viscous = ctx->der.viscous_order != 0;
-      a.update = 1;
-      a.flags = ctx->d_flags;
-      launch_visc<T>(ctx, B, a);
-      launch_carry(ctx, B, state_of(B, sin), state_of(B, sout));
-      launch_bcs(ctx, bi, state_of(B, sout), state_of(B, sin).gam);
-    });
-    launch_interfaces(ctx, sout);
-  }
-  k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->d_time, ctx->d_dt, ctx->d_step);
-  return OSTC_OK;
-}
-
 // CFL time step of the current state (slot 0) into d_dt (local_time_step + global_time_step)
-void enqueue_mix_dt(ostc_ctx *ctx) {
+void enqueue_cfl_dt(ostc_ctx *ctx) {
   long tok = begin_t(ctx, "cfl_dt");
   k_dt_reset<<<1, 1, 0, ctx->stream>>>(ctx->d_dtbits);
   for (auto &B : ctx->blk)
@@ -698,6 +658,43 @@ void enqueue_mix_dt(ostc_ctx *ctx) {
                                                                  ctx->der.prandtl, B.db.mz > 1, ctx->d_dtbits);
   k_dt_decode<<<1, 1, 0, ctx->stream>>>(ctx->d_dtbits, ctx->d_dt);
   end_t(ctx, tok);
+}
+
+// Stage rk (0..2) of an air SSP-RK3 step: state slot rk -> slot (rk + 1) % 3 (or sout_override), with
+// slot 0 the step's start state and d_dt the step's dt.
+template <typename T>
+void enqueue_air_stage(ostc_ctx *ctx, int rk, int sout_override = -1) {
+  static const double A[3] = {1.0, 0.75, 1.0 / 3.0}, Bc[3] = {0.0, 0.25, 2.0 / 3.0}, C[3] = {1.0, 0.25, 2.0 / 3.0};
+  const int sin = rk, sout = sout_override >= 0 ? sout_override : (rk + 1) % 3;
+  for_blocks(ctx, [&](int bi) {
+    BlockRes &B = ctx->blk[bi];
+    launch_flux<T>(ctx, B, state_of(B, sin));
+    StageArgs a{};
+    a.in = state_of(B, sin);
+    a.qn = state_of(B, 0);
+    a.out = state_of(B, sout);
+    a.a = A[rk];
+    a.bcoef = Bc[rk];
+    a.c = C[rk];
+    a.dt = ctx->d_dt;
+    a.prandtl = ctx->der.prandtl;
+    a.viscous = ctx->der.viscous_order != 0;
+    a.update = 1;
+    a.flags = ctx->d_flags;
+    launch_visc<T>(ctx, B, a);
+    launch_carry(ctx, B, state_of(B, sin), state_of(B, sout));
+    launch_bcs(ctx, bi, state_of(B, sout), state_of(B, sin).gam);
+  });
+  launch_interfaces(ctx, sout);
+}
+
+// One SSP-RK3 step of the air path: CFL dt from slot 0, then the three stages (A -> B -> C -> A).
+template <typename T>
+int enqueue_step(ostc_ctx *ctx) {
+  if (!ctx->der.fixed_time_step) enqueue_cfl_dt(ctx);
+  for (int rk = 0; rk < 3; ++rk) enqueue_air_stage<T>(ctx, rk);
+  k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->d_time, ctx->d_dt, ctx->d_step);
+  return OSTC_OK;
 }
 
 // Stage rk (0..2) of a mixture SSP-RK3 step: state slot rk -> slot (rk + 1) % 3, with slot 0 the
@@ -742,7 +739,7 @@ void enqueue_mix_stage(ostc_ctx *ctx, int rk, int sout_override = -1) {
 // One SSP-RK3 step of a mixture (RK.cuh:85-185 with MixtureModel Mixture / FR): source, flux-split
 // WENO7, viscous, update + temperature Newton, boundary faces, properties, per stage.
 int enqueue_step_mix(ostc_ctx *ctx) {
-  if (!ctx->der.fixed_time_step) enqueue_mix_dt(ctx);
+  if (!ctx->der.fixed_time_step) enqueue_cfl_dt(ctx);
   for (int rk = 0; rk < 3; ++rk) enqueue_mix_stage(ctx, rk);
   k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->d_time, ctx->d_dt, ctx->d_step);
   return OSTC_OK;
@@ -752,13 +749,11 @@ int enqueue_step_mix(ostc_ctx *ctx) {
 
 // what the adjoint covers: the multi-component path, explicit chemistry, one block, periodic and
 // outflow faces
-// step: the step adjoint (ostc_rk3_step_vjp, ostc_adjoint_steps) rather than ostc_rhs_vjp
+// step: the step adjoint (ostc_rk3_step_vjp, ostc_adjoint_steps) rather than ostc_rhs_vjp (the same
+// coverage today)
 int adjoint_check(ostc_ctx *ctx, unsigned mask, bool step = false) {
+  (void)step;
   if (!ctx->mixture) {
-    if (step) {
-      ctx->err = "the step adjoint covers the multi-component path (species = 1); air has ostc_rhs_vjp";
-      return OSTC_EINVAL;
-    }
     if ((mask & OSTC_TERM_INVISCID) && ctx->der.inviscid_type != 1) {
       ctx->err = "the air adjoint's inviscid term is the AWENO path (WENO5-Z / WENO7-Z with a Riemann solver)";
       return OSTC_EINVAL;
@@ -790,8 +785,8 @@ int adjoint_alloc(ostc_ctx *ctx, BlockRes &B) {
   const long long P = B.db.plane;
   CK(cudaMalloc(&B.adj, (size_t)(nv + 9 + 2 * ns) * P * sizeof(double)));
   CK(cudaMalloc(&B.dqb, (size_t)nv * B.db.n * sizeof(double)));
-  if (!ctx->mixture) return OSTC_OK;  // air: ostc_rhs_vjp only (cv adjoint planes, dq_bar)
   CK(cudaMalloc(&B.adj_work, (size_t)4 * (nv + 1) * B.db.n * sizeof(double)));
+  if (!ctx->mixture) return OSTC_OK;  // air: the step adjoint needs no fourth state slot
   // state slot 3 (zeroed: its padding columns must read as empty nodes)
   auto alloc = [&](double **p, size_t n) -> int {
     if (cudaMalloc(p, n * sizeof(double)) != cudaSuccess || cudaMemset(*p, 0, n * sizeof(double)) != cudaSuccess)
@@ -829,15 +824,16 @@ void launch_adjoint_air_inviscid(ostc_ctx *ctx, BlockRes &B, DevState in, double
   }
 }
 
-// ostc_rhs_vjp of the air path (ostc_adj_air.cuh): cv adjoint planes from the face, central-correction
-// and viscous terms, ghost folds in the reverse of the face order, interior gathered into out.
-int vjp_air(ostc_ctx *ctx, int block, unsigned mask, double *out) {
+// (d dq / d cv)^T B.dqb of the air path (ostc_adj_air.cuh) at the state in `slot`: cv adjoint planes
+// from the face, central-correction and viscous terms, ghost folds in the reverse of the face order,
+// interior gathered into out.
+int vjp_air(ostc_ctx *ctx, int block, int slot, unsigned mask, double *out) {
   BlockRes &B = ctx->blk[block];
   const DevBlock &b = B.db;
   const long long P = b.plane;
   double *acv = B.adj;
   CK(cudaMemsetAsync(acv, 0, (size_t)5 * P * sizeof(double), ctx->stream));
-  const DevState in = state_of(B, 0);
+  const DevState in = state_of(B, slot);
   if (mask & OSTC_TERM_INVISCID) {
     const int ng = ctx->der.ngg, rs = ctx->der.riemann;
     if (ng == 3) {
@@ -876,7 +872,7 @@ int vjp_air(ostc_ctx *ctx, int block, unsigned mask, double *out) {
 }
 
 int vjp_core(ostc_ctx *ctx, int block, int slot, unsigned mask, double *out, double *out_t = nullptr) {
-  if (!ctx->mixture) return vjp_air(ctx, block, mask, out);
+  if (!ctx->mixture) return vjp_air(ctx, block, slot, mask, out);
   BlockRes &B = ctx->blk[block];
   const int nv = ctx->nv, ns = ctx->der.n_spec;
   const long long P = B.db.plane;
@@ -922,7 +918,33 @@ int vjp_core(ostc_ctx *ctx, int block, int slot, unsigned mask, double *out, dou
 //            x2_T = R'_T(S2)^T (...) + dN/dT_start lam_T'
 //   stage 2: likewise from (x2, x2_T) to (x1, x1_T) with 1/4, stage 1 to q with 1;
 //   lam_cv = 1/3 lam_cv' + 3/4 x2 + x1 + R'(q)^T (dt/J x1),  lam_T = R'_T(q)^T (...) + dN/dT_start x1_T.
+// The air step: every stage's primitive state is the equation of state of its cv, so the state is cv
+// alone and the stage adjoints chain through the right-hand-side VJPs (stage 3's output is not needed).
+int step_vjp_air(ostc_ctx *ctx) {
+  BlockRes &B = ctx->blk[0];
+  const int nv = 5;
+  const long long N = B.db.n, nt = (long long)nv * N;
+  double *Lc = B.adj_work, *X2c = Lc + nt, *X1c = X2c + nt, *Gc = X1c + nt;
+  const int g = grid_for(ctx, N, 128), gt = grid_for(ctx, nt, 256);
+  enqueue_air_stage<double>(ctx, 0);  // S1 -> slot 1
+  enqueue_air_stage<double>(ctx, 1);  // S2 -> slot 2
+  k_adj_stage_seed<<<g, 128, 0, ctx->stream>>>(B.db, Lc, 2.0 / 3.0, ctx->d_dt, B.dqb, nv);
+  if (int r = vjp_air(ctx, 0, 2, OSTC_TERM_ALL, X2c)) return r;
+  k_axpby<<<gt, 256, 0, ctx->stream>>>(nt, 2.0 / 3.0, Lc, 1.0, X2c);
+  k_adj_stage_seed<<<g, 128, 0, ctx->stream>>>(B.db, X2c, 0.25, ctx->d_dt, B.dqb, nv);
+  if (int r = vjp_air(ctx, 0, 1, OSTC_TERM_ALL, X1c)) return r;
+  k_axpby<<<gt, 256, 0, ctx->stream>>>(nt, 0.25, X2c, 1.0, X1c);
+  k_adj_stage_seed<<<g, 128, 0, ctx->stream>>>(B.db, X1c, 1.0, ctx->d_dt, B.dqb, nv);
+  if (int r = vjp_air(ctx, 0, 0, OSTC_TERM_ALL, Gc)) return r;
+  k_axpby<<<gt, 256, 0, ctx->stream>>>(nt, 0.75, X2c, 1.0 / 3.0, Lc);
+  k_axpby<<<gt, 256, 0, ctx->stream>>>(nt, 1.0, X1c, 1.0, Lc);
+  k_axpby<<<gt, 256, 0, ctx->stream>>>(nt, 1.0, Gc, 1.0, Lc);
+  CK(cudaGetLastError());
+  return OSTC_OK;
+}
+
 int step_vjp(ostc_ctx *ctx) {
+  if (!ctx->mixture) return step_vjp_air(ctx);
   BlockRes &B = ctx->blk[0];
   const int nv = ctx->nv;
   const long long N = B.db.n, nt = (long long)nv * N;

@@ -623,7 +623,7 @@ __device__ __forceinline__ void mix_visc_face_bwd(const DevBlock &b, const DevSt
                                                   const double *afv, const DevAdj &A) {
   const long long P = b.plane;
   const long long st[3] = {1, b.pitch, (long long)b.pitch * b.sy};
-  const long long p1 = p0 + st[d];
+  const long long p1 = b.chk(p0 + st[d]);
   double m[9];
   for (int r = 0; r < 9; ++r) m[r] = 0.5 * (b.met[r * P + p0] + b.met[r * P + p1]);
   auto grad = [&](const double *B, double *out) {
@@ -1208,8 +1208,8 @@ __global__ void __launch_bounds__(128) k_adj_bc_face(DevBlock b, DevAdj A, int n
       po = b.id(other[0], other[1], other[2]);
     }
     for (int g = b.g; g >= 1; --g) {
-      const long long pg = pb + g * dstep;
-      const long long ps = f.type == kPeriodic ? po + g * dstep : pb;
+      const long long pg = b.chk(pb + g * dstep);
+      const long long ps = b.chk(f.type == kPeriodic ? po + g * dstep : pb);
       for (int q = 0; q < 6; ++q) {
         planes[q][ps] += planes[q][pg];
         planes[q][pg] = 0.0;

@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(128) k_adj_air_visc(DevBlock b, DevState s, co
     };
 #pragma unroll 1
     for (int sn = 0; sn < NN; ++sn) {
-      const long long ps = p0 + off[sn];
+      const long long ps = b.chk(p0 + off[sn]);
       double cv[5];
 #pragma unroll
       for (int l = 0; l < 5; ++l) cv[l] = s.cv[l * P + ps];
@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(128) k_adj_air_visc(DevBlock b, DevState s, co
         dq[3] = (dp[vv] - (vv == 0 ? pn * ir : 0.0)) * ir / rgas;
         dq[4] = dmu_dt * dq[3];
         auto V = [&](int q, int di, int dj, int dk) -> Dual {
-          const long long p = p0 + di * st3[0] + dj * st3[1] + dk * st3[2];
+          const long long p = b.chk(p0 + di * st3[0] + dj * st3[1] + dk * st3[2]);
           const double val = q == 0 ? s.bv[P + p] : q == 1 ? s.bv[2 * P + p] : q == 2 ? s.bv[3 * P + p]
                            : q == 3 ? s.bv[5 * P + p] : s.mul[p];
           return Dual(val, p == ps ? dq[q] : 0.0);
@@ -316,8 +316,8 @@ __global__ void __launch_bounds__(128) k_adj_air_bc_face(DevBlock b, double *acv
       po = b.id(oth[0], oth[1], oth[2]);
     }
     for (int g = b.g; g >= 1; --g) {
-      const long long pg = pb + g * dstep;
-      const long long ps = f.type == kPeriodic ? po + g * dstep : pb;
+      const long long pg = b.chk(pb + g * dstep);
+      const long long ps = b.chk(f.type == kPeriodic ? po + g * dstep : pb);
 #pragma unroll
       for (int l = 0; l < 5; ++l) {
         acv[l * P + ps] += acv[l * P + pg];

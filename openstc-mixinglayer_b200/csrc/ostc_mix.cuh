@@ -383,7 +383,7 @@ __device__ __forceinline__ void mix_visc_face(const DevBlock &b, const DevState 
                                               T *fv) {
   const long long P = b.plane;
   const long long st[3] = {1, b.pitch, (long long)b.pitch * b.sy};
-  const long long p1 = p0 + st[d];
+  const long long p1 = b.chk(p0 + st[d]);
   const T half = T(0.5);
   T m[9];
   for (int r = 0; r < 9; ++r) m[r] = (T)(0.5 * (b.met[r * P + p0] + b.met[r * P + p1]));

@@ -245,7 +245,8 @@ def test_vjp_rejects_uncovered_cases(built, tmp_path):
     air_out = oc.mixing_layer_3d(mx=24, my=16, mz=8, ybc="outflow")
     s1 = ostc.Solver(str(oc.write_case(air_out, tmp_path / "air_out")))
     s1.set_state(air_out.bv)
-    with pytest.raises(ostc.OstcError, match="step adjoint"):
+    s1.set_precision(ostc.PREC_MIXED)
+    with pytest.raises(ostc.OstcError, match="FP64 step"):
         s1.step_vjp(np.zeros((5,) + s1.shape(0)))
     pv_air = oc.mixing_layer_3d(mx=24, my=16, mz=8, ybc="outflow", reconstruction=2)
     s4 = ostc.Solver(str(oc.write_case(pv_air, tmp_path / "pv_air")))
@@ -286,12 +287,12 @@ def _fixed_dt_solver(tmp_path, dims, steps_dt_from=None):
     return s, cv0, case
 
 
-def _fd_steps(s, case, cv0, v, n):
+def _fd_steps(s, case, cv0, v, n, eps=EPS):
     """Richardson-extrapolated central difference of q_n(q_0) along v.  Every perturbed start is set
     from the exact base state (set_state), so that its temperature Newton iteration starts from the
     base T and ends O(eps^2) from the root."""
     d = []
-    for h in (2 * EPS, EPS):
+    for h in (2 * eps, eps):
         out = []
         for sg in (1, -1):
             s.set_state(case.bv, sv=case.sv)
@@ -391,3 +392,60 @@ def test_momentum_thickness_gradient_wrt_mode_amplitudes(built, tmp_path):
         d2 = (theta(a0 + 2 * h * e)[0] - theta(a0 - 2 * h * e)[0]) / (4 * h)
         grad_fd[m] = (4 * d1 - d2) / 3
     assert np.max(np.abs(grad_ad - grad_fd)) <= 1e-4 * np.max(np.abs(grad_fd)), (grad_ad, grad_fd)
+
+
+def _fixed_dt_air(tmp_path, make):
+    """A noisy air layer (see _air_solver) with a fixed dt, the CFL dt of its initial state."""
+    import ostc
+
+    case = make()
+    s, _ = _air_solver(case, tmp_path)
+    dt = s.step(1)
+    s.close()
+    case.scheme["fixed_time_step"] = 1
+    case.scheme["dt"] = dt
+    s = ostc.Solver(str(oc.write_case(case, tmp_path / "air_fixed")))
+    s.set_state(case.bv)
+    return s, s.get_state()[0], case
+
+
+def _air_steps_err(s, case, cv0, w, lam, v, n):
+    """Error of <lam, v> against differences of n-step runs along v, in units of the tolerance, judged
+    by the better of steps 1e-7 and 1e-8 (see _check_air)."""
+    rhs = float(np.sum(lam * v))
+    e = []
+    for eps in (1e-7, 1e-8):
+        jv = _fd_steps(s, case, cv0, v, n, eps)
+        lhs = float(np.sum(w * jv))
+        e.append(abs(lhs - rhs) / (RTOL * abs(lhs) + ATOL * float(np.sum(np.abs(w * jv)))))
+    return min(e)
+
+
+@pytest.mark.parametrize("name", ["weno7_hllc_3d", "weno5_ausm_2d"])
+def test_air_step_vjp_matches_finite_differences(built, tmp_path, name):
+    """Adjoint of one air SSP-RK3 step (dt fixed) against differences of whole steps."""
+    s, cv0, case = _fixed_dt_air(tmp_path, AIR[name])
+    rng = np.random.default_rng(23)
+    w = rng.standard_normal(cv0.shape)
+    g = s.step_vjp(w)
+    assert np.array_equal(s.get_state()[0], cv0)  # the state is left as it was
+    errs = [_air_steps_err(s, case, cv0, w, g, v, 1) for v in _directions(cv0, rng, 3)]
+    assert max(errs) <= 1.0, errs
+
+
+def test_air_checkpointed_trajectory_adjoint(built, tmp_path):
+    """ostc_adjoint_steps on the air layer: 5 steps with a checkpoint every 2, against differences of
+    5-step runs; the context ends at q_5; the checkpoint spacing does not change the result."""
+    s, cv0, case = _fixed_dt_air(tmp_path, AIR["weno7_hllc_3d"])
+    rng = np.random.default_rng(24)
+    w = rng.standard_normal(cv0.shape)
+    lam0 = s.adjoint_steps(5, w, every=2)
+    q5, _ = s.get_state()
+    s.set_state(case.bv)
+    s.step(5)
+    assert np.array_equal(q5, s.get_state()[0])
+    errs = [_air_steps_err(s, case, cv0, w, lam0, v, 5) for v in _directions(cv0, rng, 2)]
+    assert max(errs) <= 1.0, errs
+    s.set_state(case.bv)
+    lam1 = s.adjoint_steps(5, w, every=5)
+    assert np.max(np.abs(lam1 - lam0)) <= 1e-10 * np.max(np.abs(lam0))
