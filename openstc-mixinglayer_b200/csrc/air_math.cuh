@@ -15,6 +15,13 @@ constexpr double kMwD = 28.9647;
 template <typename T> __device__ __forceinline__ T tsqrt(T x);
 template <> __device__ __forceinline__ double tsqrt<double>(double x) { return sqrt(x); }
 template <> __device__ __forceinline__ float tsqrt<float>(float x) { return sqrtf(x); }
+// 1 / sqrt(x), from which the callers form sqrt(x) = x / sqrt(x) and 1 / x = (1 / sqrt(x))^2.  FP32:
+// one reciprocal square root stands in for a square root and a division.  FP64 keeps the correctly
+// rounded square root and division: with the reciprocal square root the FP64 sweeps ran 3 % faster,
+// but the multi-block reference fixtures moved from inside the 1e-12 parity bar to 1.1-1.8e-12.
+template <typename T> __device__ __forceinline__ T trsqrt(T x);
+template <> __device__ __forceinline__ double trsqrt<double>(double x) { return 1.0 / sqrt(x); }
+template <> __device__ __forceinline__ float trsqrt<float>(float x) { return rsqrtf(x); }
 template <typename T> __device__ __forceinline__ T tabs(T x);
 template <> __device__ __forceinline__ double tabs<double>(double x) { return fabs(x); }
 template <> __device__ __forceinline__ float tabs<float>(float x) { return fabsf(x); }
@@ -35,7 +42,8 @@ __device__ __forceinline__ double sutherland(double t) {
 // Convex WENO-Z combination sum_k a_k v_k / sum_k a_k with a_k = d_k (1 + tau / D_k) and
 // D_k = (eps + beta_k)^2 (AWENO.cu:193-197, 245-251).
 // FP64: multiplying numerator and denominator by prod_k D_k leaves one division per combination
-// instead of one per weight; products of three D_k stay far inside the FP64 range.
+// instead of one per weight (products of three D_k stay far inside the FP64 range), and the two sides
+// of a face share one division (finish).
 // FP32: products of three D_k can underflow, so each weight keeps its own fast division.  The
 // reference's WENO7 indicator beta2 (AWENO.cu:236-238, 263-265) is neither shift-invariant nor
 // positive semi-definite, so eps + beta2 can pass through zero; in FP32 its square can underflow to
@@ -43,32 +51,49 @@ __device__ __forceinline__ double sutherland(double t) {
 // selected, as in FP64).
 template <typename T> struct WenoComb;
 template <> struct WenoComb<double> {
-  static __device__ __forceinline__ double c3(double d0, double d1, double d2, double D0, double D1, double D2,
-                                              double tau, double v0, double v1, double v2) {
+  // numerator and denominator of the combination
+  static __device__ __forceinline__ void c3(double d0, double d1, double d2, double D0, double D1, double D2,
+                                            double tau, double v0, double v1, double v2, double &num, double &den) {
     const double w0 = d0 * (D0 + tau) * (D1 * D2), w1 = d1 * (D1 + tau) * (D0 * D2), w2 = d2 * (D2 + tau) * (D0 * D1);
-    return (w0 * v0 + w1 * v1 + w2 * v2) / (w0 + w1 + w2);
+    num = w0 * v0 + w1 * v1 + w2 * v2;
+    den = w0 + w1 + w2;
   }
-  static __device__ __forceinline__ double c4(double d0, double d1, double d2, double d3, double D0, double D1,
-                                              double D2, double D3, double tau, double v0, double v1, double v2,
-                                              double v3) {
+  static __device__ __forceinline__ void c4(double d0, double d1, double d2, double d3, double D0, double D1,
+                                            double D2, double D3, double tau, double v0, double v1, double v2,
+                                            double v3, double &num, double &den) {
     const double a = D0 * D1, b = D2 * D3;
     const double w0 = d0 * (D0 + tau) * (D1 * b), w1 = d1 * (D1 + tau) * (D0 * b);
     const double w2 = d2 * (D2 + tau) * (a * D3), w3 = d3 * (D3 + tau) * (a * D2);
-    return (w0 * v0 + w1 * v1 + w2 * v2 + w3 * v3) / (w0 + w1 + w2 + w3);
+    num = w0 * v0 + w1 * v1 + w2 * v2 + w3 * v3;
+    den = w0 + w1 + w2 + w3;
+  }
+  // the two sides' quotients from one division: a denominator is a sum of products of up to four
+  // (eps + beta)^2 factors, so the product of two stays inside the FP64 range
+  static __device__ __forceinline__ void finish(double nm, double dm, double np, double dp, double &vm, double &vp) {
+    const double q = 1.0 / (dm * dp);
+    vm = nm * dp * q;
+    vp = np * dm * q;
   }
 };
 template <> struct WenoComb<float> {
-  static __device__ __forceinline__ float c3(float d0, float d1, float d2, float D0, float D1, float D2, float tau,
-                                             float v0, float v1, float v2) {
+  static __device__ __forceinline__ void c3(float d0, float d1, float d2, float D0, float D1, float D2, float tau,
+                                            float v0, float v1, float v2, float &num, float &den) {
     const float a0 = d0 + d0 * __fdividef(tau, fmaxf(D0, 1e-30f)), a1 = d1 + d1 * __fdividef(tau, fmaxf(D1, 1e-30f));
     const float a2 = d2 + d2 * __fdividef(tau, fmaxf(D2, 1e-30f));
-    return __fdividef(a0 * v0 + a1 * v1 + a2 * v2, a0 + a1 + a2);
+    num = a0 * v0 + a1 * v1 + a2 * v2;
+    den = a0 + a1 + a2;
   }
-  static __device__ __forceinline__ float c4(float d0, float d1, float d2, float d3, float D0, float D1, float D2,
-                                             float D3, float tau, float v0, float v1, float v2, float v3) {
+  static __device__ __forceinline__ void c4(float d0, float d1, float d2, float d3, float D0, float D1, float D2,
+                                            float D3, float tau, float v0, float v1, float v2, float v3, float &num,
+                                            float &den) {
     const float a0 = d0 + d0 * __fdividef(tau, fmaxf(D0, 1e-30f)), a1 = d1 + d1 * __fdividef(tau, fmaxf(D1, 1e-30f));
     const float a2 = d2 + d2 * __fdividef(tau, fmaxf(D2, 1e-30f)), a3 = d3 + d3 * __fdividef(tau, fmaxf(D3, 1e-30f));
-    return __fdividef(a0 * v0 + a1 * v1 + a2 * v2 + a3 * v3, a0 + a1 + a2 + a3);
+    num = a0 * v0 + a1 * v1 + a2 * v2 + a3 * v3;
+    den = a0 + a1 + a2 + a3;
+  }
+  static __device__ __forceinline__ void finish(float nm, float dm, float np, float dp, float &vm, float &vp) {
+    vm = __fdividef(nm, dm);
+    vp = __fdividef(np, dp);
   }
 };
 
@@ -87,6 +112,7 @@ __device__ __forceinline__ void weno5_char(const T *Lr, const Q &q, T &vminus, T
     v[s] = acc;
   }
   const T th = T(13.0 / 12), eps = T(1e-6), o16 = T(1.0 / 16), f8 = T(5.0 / 8), f16 = T(5.0 / 16);
+  T nm, dm, np, dp;
   {
     const T v0 = T(0.125) * (T(3) * v[0] - T(10) * v[1] + T(15) * v[2]);
     const T v1 = T(0.125) * (-v[1] + T(6) * v[2] + T(3) * v[3]);
@@ -97,8 +123,8 @@ __device__ __forceinline__ void weno5_char(const T *Lr, const Q &q, T &vminus, T
     const T beta2 = th * (v[2] + v[4] - T(2) * v[3]) * (v[2] + v[4] - T(2) * v[3]) +
                     T(0.25) * (T(3) * v[2] + v[4] - T(4) * v[3]) * (T(3) * v[2] + v[4] - T(4) * v[3]);
     const T tau = (beta0 - beta2) * (beta0 - beta2);
-    vminus = WenoComb<T>::c3(o16, f8, f16, (eps + beta0) * (eps + beta0), (eps + beta1) * (eps + beta1),
-                             (eps + beta2) * (eps + beta2), tau, v0, v1, v2);
+    WenoComb<T>::c3(o16, f8, f16, (eps + beta0) * (eps + beta0), (eps + beta1) * (eps + beta1),
+                    (eps + beta2) * (eps + beta2), tau, v0, v1, v2, nm, dm);
   }
   {
     const T v0 = T(0.125) * (-v[1] + T(6) * v[2] + T(3) * v[3]);
@@ -110,9 +136,10 @@ __device__ __forceinline__ void weno5_char(const T *Lr, const Q &q, T &vminus, T
     const T beta2 = th * (v[3] + v[5] - T(2) * v[4]) * (v[3] + v[5] - T(2) * v[4]) +
                     T(0.25) * (T(3) * v[3] + v[5] - T(4) * v[4]) * (T(3) * v[3] + v[5] - T(4) * v[4]);
     const T tau = (beta0 - beta2) * (beta0 - beta2);
-    vplus = WenoComb<T>::c3(f16, f8, o16, (eps + beta0) * (eps + beta0), (eps + beta1) * (eps + beta1),
-                            (eps + beta2) * (eps + beta2), tau, v0, v1, v2);
+    WenoComb<T>::c3(f16, f8, o16, (eps + beta0) * (eps + beta0), (eps + beta1) * (eps + beta1),
+                    (eps + beta2) * (eps + beta2), tau, v0, v1, v2, np, dp);
   }
+  WenoComb<T>::finish(nm, dm, np, dp, vminus, vplus);
 }
 
 // Characteristic WENO7-Z interpolation from the 8 points i-3..i+4 (AWENO.cu:212-280).  beta2 keeps
@@ -145,6 +172,7 @@ __device__ __forceinline__ void weno7_char(const T *Lr, const Q &q, T &vminus, T
     v[s] = acc;
   }
   const T eps = T(1e-6), s7 = T(7.0 / 64), t5 = T(35.0 / 64), t1 = T(21.0 / 64), o1 = T(1.0 / 64);
+  T nm, dm, np, dp;
   {
     const T v0 = T(0.0625) * (T(5) * v[3] + T(15) * v[4] - T(5) * v[5] + v[6]);
     const T v1 = T(0.0625) * (-v[2] + T(9) * v[3] + T(9) * v[4] - v[5]);
@@ -153,8 +181,8 @@ __device__ __forceinline__ void weno7_char(const T *Lr, const Q &q, T &vminus, T
     T b0, b1, b2, b3;
     weno7_betas<T>(v, b0, b1, b2, b3);
     const T tau = (b3 + T(5) * b2 - T(5) * b1 - b0) * (b3 + T(5) * b2 - T(5) * b1 - b0);
-    vminus = WenoComb<T>::c4(s7, t5, t1, o1, (eps + b0) * (eps + b0), (eps + b1) * (eps + b1), (eps + b2) * (eps + b2),
-                             (eps + b3) * (eps + b3), tau, v0, v1, v2, v3);
+    WenoComb<T>::c4(s7, t5, t1, o1, (eps + b0) * (eps + b0), (eps + b1) * (eps + b1), (eps + b2) * (eps + b2),
+                    (eps + b3) * (eps + b3), tau, v0, v1, v2, v3, nm, dm);
   }
   {
     const T v1 = T(0.0625) * (T(5) * v[3] + T(15) * v[4] - T(5) * v[5] + v[6]);
@@ -164,9 +192,10 @@ __device__ __forceinline__ void weno7_char(const T *Lr, const Q &q, T &vminus, T
     T b0, b1, b2, b3;
     weno7_betas<T>(v + 1, b0, b1, b2, b3);
     const T tau = (b3 + T(5) * b2 - T(5) * b1 - b0) * (b3 + T(5) * b2 - T(5) * b1 - b0);
-    vplus = WenoComb<T>::c4(o1, t1, t5, s7, (eps + b0) * (eps + b0), (eps + b1) * (eps + b1), (eps + b2) * (eps + b2),
-                            (eps + b3) * (eps + b3), tau, v0, v1, v2, v3);
+    WenoComb<T>::c4(o1, t1, t5, s7, (eps + b0) * (eps + b0), (eps + b1) * (eps + b1), (eps + b2) * (eps + b2),
+                    (eps + b3) * (eps + b3), tau, v0, v1, v2, v3, np, dp);
   }
+  WenoComb<T>::finish(nm, dm, np, dp, vminus, vplus);
 }
 
 // AWENO_interpolation<Air> (AWENO.cu:15-154).  NG = 3 (WENO5) or 4 (WENO7); q(s, v) for
@@ -181,10 +210,11 @@ __device__ __forceinline__ void aweno_interp(const Q &q, const T *mt0, const T *
   constexpr int cl = NG - 1, cr = NG;
   const T gm1 = T(kGamma - 1), igm1 = T(1.0 / (kGamma - 1));
   const T l0 = q(cl, 0), r0 = q(cr, 0);
-  const T sl = tsqrt(l0), sr = tsqrt(r0);
+  const T rsl = trsqrt(l0), rsr = trsqrt(r0);
+  const T sl = l0 * rsl, sr = r0 * rsr;
   const T isum = T(1) / (sl + sr);
   const T rlc = sl * isum, rrc = sr * isum;
-  const T il0 = T(1) / l0, ir0 = T(1) / r0;
+  const T il0 = rsl * rsl, ir0 = rsr * rsr;
   const T um = rlc * q(cl, 1) * il0 + rrc * q(cr, 1) * ir0;
   const T vm = rlc * q(cl, 2) * il0 + rrc * q(cr, 2) * ir0;
   const T wm = rlc * q(cl, 3) * il0 + rrc * q(cr, 3) * ir0;
@@ -193,12 +223,12 @@ __device__ __forceinline__ void aweno_interp(const Q &q, const T *mt0, const T *
   const T hr = (q(cr, 4) + q(cr, 5)) * ir0;
   const T hm = rlc * hl + rrc * hr;
   const T cm2 = gm1 * (hm - ekm);
-  const T cm = tsqrt(cm2);
-  const T icm2 = T(1) / cm2, icm = cm * icm2;
+  const T icm = trsqrt(cm2);
+  const T cm = cm2 * icm, icm2 = icm * icm;
   T kx = T(0.5) * (mt0[0] + mt1[0]);
   T ky = T(0.5) * (mt0[1] + mt1[1]);
   T kz = T(0.5) * (mt0[2] + mt1[2]);
-  const T igk = T(1) / tsqrt(kx * kx + ky * ky + kz * kz);
+  const T igk = trsqrt(kx * kx + ky * ky + kz * kz);
   kx *= igk;
   ky *= igk;
   kz *= igk;
@@ -260,7 +290,8 @@ __device__ __forceinline__ void aweno_interp(const Q &q, const T *mt0, const T *
       qr[m] += Rc[m] * vpl;
     }
   }
-  const T iql = T(1) / ql[0], iqr = T(1) / qr[0];
+  const T iqq = T(1) / (ql[0] * qr[0]);
+  const T iql = qr[0] * iqq, iqr = ql[0] * iqq;
   pl[0] = ql[0];
   pl[1] = ql[1] * iql;
   pl[2] = ql[2] * iql;
@@ -284,8 +315,9 @@ __device__ __forceinline__ void ausm_plus(const T *pl, const T *pr, const T *mt0
   const T k1 = T(0.5) * (j0 * mt0[0] + j1 * mt1[0]);
   const T k2 = T(0.5) * (j0 * mt0[1] + j1 * mt1[1]);
   const T k3 = T(0.5) * (j0 * mt0[2] + j1 * mt1[2]);
-  const T gkj = tsqrt(k1 * k1 + k2 * k2 + k3 * k3);
-  const T igkj = T(1) / gkj;
+  const T k2s = k1 * k1 + k2 * k2 + k3 * k3;
+  const T igkj = trsqrt(k2s);
+  const T gkj = k2s * igkj;
   const T ul = (k1 * pl[1] + k2 * pl[2] + k3 * pl[3]) * igkj;
   const T ur = (k1 * pr[1] + k2 * pr[2] + k3 * pr[3]) * igkj;
   const T p_l = pl[4], p_r = pr[4], rho_l = pl[0], rho_r = pr[0];
@@ -333,14 +365,15 @@ __device__ __forceinline__ void ausm_plus(const T *pl, const T *pr, const T *mt0
 template <typename T>
 __device__ __forceinline__ void hllc(const T *pl, const T *pr, const T *mt0, const T *mt1, T j0, T j1, T *fc) {
   const T gam = T(kGamma);
-  const T sql = tsqrt(pl[0]), sqr = tsqrt(pr[0]);
+  const T rsl = trsqrt(pl[0]), rsr = trsqrt(pr[0]);
+  const T sql = pl[0] * rsl, sqr = pr[0] * rsr;
   const T isq = T(1) / (sql + sqr);
   const T rl_c = sql * isq;
   const T rr_c = sqr * isq;
   const T ut = pl[1] * rl_c + pr[1] * rr_c;
   const T vt = pl[2] * rl_c + pr[2] * rr_c;
   const T wt = pl[3] * rl_c + pr[3] * rr_c;
-  const T irl = T(1) / pl[0], irr = T(1) / pr[0];
+  const T irl = rsl * rsl, irr = rsr * rsr;
   const T hl = (pl[5] + pl[4]) * irl;
   const T hr = (pr[5] + pr[4]) * irr;
   const T ht = hl * rl_c + hr * rr_c;
@@ -349,8 +382,9 @@ __device__ __forceinline__ void hllc(const T *pl, const T *pr, const T *mt0, con
   const T kx = T(0.5) * (mt0[0] + mt1[0]);
   const T ky = T(0.5) * (mt0[1] + mt1[1]);
   const T kz = T(0.5) * (mt0[2] + mt1[2]);
-  const T gradK = tsqrt(kx * kx + ky * ky + kz * kz);
-  const T igk = T(1) / gradK;
+  const T k2s = kx * kx + ky * ky + kz * kz;
+  const T igk = trsqrt(k2s);
+  const T gradK = k2s * igk;
   const T Ubar = (kx * ut + ky * vt + kz * wt) * igk;
   const T jac = T(0.5) * (j0 + j1);
   const T Ul = kx * pl[1] + ky * pl[2] + kz * pl[3];

@@ -21,23 +21,30 @@
 
 namespace ostc {
 
+template <> __device__ __forceinline__ Dual trsqrt<Dual>(Dual x) { return 1.0 / ad::sqrt(x); }
 template <> __device__ __forceinline__ Dual tabs<Dual>(Dual x) { return ad::fabs(x); }
 template <> __device__ __forceinline__ Dual tmin<Dual>(Dual a, Dual b) { return b < a ? b : a; }
 template <> __device__ __forceinline__ Dual tmax<Dual>(Dual a, Dual b) { return b > a ? b : a; }
 
 // The FP64 weight combination (same products of the D_k) on dual numbers.
 template <> struct WenoComb<Dual> {
-  static __device__ __forceinline__ Dual c3(Dual d0, Dual d1, Dual d2, Dual D0, Dual D1, Dual D2, Dual tau, Dual v0,
-                                            Dual v1, Dual v2) {
+  static __device__ __forceinline__ void c3(Dual d0, Dual d1, Dual d2, Dual D0, Dual D1, Dual D2, Dual tau, Dual v0,
+                                            Dual v1, Dual v2, Dual &num, Dual &den) {
     const Dual w0 = d0 * (D0 + tau) * (D1 * D2), w1 = d1 * (D1 + tau) * (D0 * D2), w2 = d2 * (D2 + tau) * (D0 * D1);
-    return (w0 * v0 + w1 * v1 + w2 * v2) / (w0 + w1 + w2);
+    num = w0 * v0 + w1 * v1 + w2 * v2;
+    den = w0 + w1 + w2;
   }
-  static __device__ __forceinline__ Dual c4(Dual d0, Dual d1, Dual d2, Dual d3, Dual D0, Dual D1, Dual D2, Dual D3,
-                                            Dual tau, Dual v0, Dual v1, Dual v2, Dual v3) {
+  static __device__ __forceinline__ void c4(Dual d0, Dual d1, Dual d2, Dual d3, Dual D0, Dual D1, Dual D2, Dual D3,
+                                            Dual tau, Dual v0, Dual v1, Dual v2, Dual v3, Dual &num, Dual &den) {
     const Dual a = D0 * D1, b = D2 * D3;
     const Dual w0 = d0 * (D0 + tau) * (D1 * b), w1 = d1 * (D1 + tau) * (D0 * b);
     const Dual w2 = d2 * (D2 + tau) * (a * D3), w3 = d3 * (D3 + tau) * (a * D2);
-    return (w0 * v0 + w1 * v1 + w2 * v2 + w3 * v3) / (w0 + w1 + w2 + w3);
+    num = w0 * v0 + w1 * v1 + w2 * v2 + w3 * v3;
+    den = w0 + w1 + w2 + w3;
+  }
+  static __device__ __forceinline__ void finish(Dual nm, Dual dm, Dual np, Dual dp, Dual &vm, Dual &vp) {
+    vm = nm / dm;
+    vp = np / dp;
   }
 };
 
