@@ -685,9 +685,14 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 8 ? 2 : 4) k_visc_update(
       sv[slot][2][y][x] = (T)(a.in.bv[3 * P + p] - ref[2]);
       sv[slot][3][y][x] = (T)(a.in.bv[5 * P + p] - ref[3]);
       sv[slot][4][y][x] = (T)a.in.mul[p];
+      if constexpr (std::is_same_v<T, float>) {
 #pragma unroll
-      for (int r = 0; r < 9; ++r) sm[slot][r][y][x] = (T)b.met[r * P + p];
-      sm[slot][9][y][x] = (T)b.jac[p];
+        for (int r = 0; r < 10; ++r) sm[slot][r][y][x] = b.met32[r * P + p];
+      } else {
+#pragma unroll
+        for (int r = 0; r < 9; ++r) sm[slot][r][y][x] = (T)b.met[r * P + p];
+        sm[slot][9][y][x] = (T)b.jac[p];
+      }
     }
   };
   // face whose first node is tile node (x, y) of plane kk, direction d

@@ -213,6 +213,20 @@ int ostc_create(const char *setup_txt, const char *input_dir, int device, ostc_c
     cudaMemcpy(R.jac, hj.data(), hj.size() * sizeof(double), cudaMemcpyHostToDevice);
     b.met = R.met;
     b.jac = R.jac;
+    b.met32 = nullptr;
+    if (!ctx->mixture) {
+      std::vector<float> h32(10 * b.plane);
+      for (long long q = 0; q < 9 * b.plane; ++q) h32[q] = (float)hm[q];
+      for (long long q = 0; q < b.plane; ++q) h32[9 * b.plane + q] = (float)hj[q];
+      if (cudaMalloc(&R.met32, h32.size() * sizeof(float)) != cudaSuccess ||
+          cudaMemcpy(R.met32, h32.data(), h32.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+        g_create_error = "device allocation failed";
+        ctx->blk.push_back(R);
+        ostc_destroy(ctx.release());
+        return OSTC_ENOMEM;
+      }
+      b.met32 = R.met32;
+    }
     for (auto &hf : HB.faces) {
       DevFace f{};
       f.type = hf.type;
@@ -511,6 +525,7 @@ void ostc_destroy(ostc_ctx *ctx) {
   for (auto &B : ctx->blk) {
     cudaFree(B.met);
     cudaFree(B.jac);
+    cudaFree(B.met32);
     cudaFree(B.dq);
     cudaFree(B.last);
     cudaFree(B.adj);

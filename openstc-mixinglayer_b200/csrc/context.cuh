@@ -8,6 +8,7 @@ using namespace ostc;
 struct BlockRes {
   DevBlock db{};
   double *met = nullptr, *jac = nullptr;
+  float *met32 = nullptr;  // air: metric + Jacobian rounded to FP32 (DevBlock::met32)
   // state slots: 0..2 the RK3 stage buffers, 3 the step adjoint's copy of a step's output
   double *cv[4]{}, *bv[4]{}, *mul[4]{};
   double *sv[4]{}, *cond[4]{}, *rhod[4]{}, *gam[4]{}, *acs[4]{};  // mixtures only

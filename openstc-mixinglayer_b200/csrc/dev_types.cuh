@@ -16,6 +16,9 @@ struct DevBlock {
   int mx, my, mz, g, gz, pitch, sy, sz;
   long long plane, off0, n;
   const double *met, *jac;
+  // air: FP32 copies of the 9 metric planes and the Jacobian (plane 9), read by the mixed-precision
+  // viscous sweep (the values it would round from met / jac); null for mixtures
+  const float *met32;
   __host__ __device__ __forceinline__ long long id(int i, int j, int k) const {
 #if defined(OSTC_BOUNDS_CHECK) && defined(__CUDA_ARCH__)
     if (i < -g || i >= pitch - g || j < -g || j >= sy - g || k < -gz || k >= sz - gz) {
