@@ -633,25 +633,30 @@ struct StageArgs {
 // SSP-RK3 combine, EOS and Sutherland viscosity of the new state (update_cv_and_bv_rk, RK.cuh:230-284;
 // update_physical_properties<Air>, FieldOperation.cuh:107-140).
 // A block owns a TX x TY column of nodes and marches k through [k0, k1).  Shared memory keeps a ring
-// of three k planes (k-1, k, k+1) of u, v, w, T, mu and of the metric + Jacobian, each with a one-node
-// halo in i and j, loaded once (coalesced along i).  Every face flux is computed once: x and y faces
-// of plane k into shared memory, the z face k+1/2 in registers (carried to the next plane as k-1/2).
+// of three k planes (k-1, k, k+1) of u, v, w, T, mu and a ring of two (k, k+1) of the metric +
+// Jacobian (no face of plane k reads the metric of plane k-1), each with a one-node halo in i and j,
+// loaded once (coalesced along i).  Every face flux is computed once: x and y faces of plane k into
+// shared memory, the z face k+1/2 in registers (carried to the next plane as k-1/2).
 template <typename T, bool DIM3, int TX, int TY>
 constexpr size_t visc_smem_bytes() {
-  return sizeof(T) * ((DIM3 ? 3 : 1) * 15 * (TY + 2) * (TX + 2) + TY * (TX + 1) * 4 + (TY + 1) * TX * 4);
+  return sizeof(T) * ((DIM3 ? 3 * 5 + 2 * 10 : 15) * (TY + 2) * (TX + 2) + TY * (TX + 1) * 4 + (TY + 1) * TX * 4);
 }
 
 template <typename T, bool DIM3, int TX, int TY>
-// FP64: the plane ring's shared memory admits two blocks per SM, so registers are not capped for three
+// FP64: two blocks per SM at up to 255 registers; three fit in shared memory, but their 168-register
+// cap measured 5 % slower (40.1 against 38.05 ms per AWENO7 + HLLC step at 512 x 256 x 128)
 __global__ void __launch_bounds__(TX *TY, sizeof(T) == 8 ? 2 : 4) k_visc_update(DevBlock b, StageArgs a, double *__restrict__ dq,
                                                                       int kseg) {
-  constexpr int NP = DIM3 ? 3 : 1;  // planes in the ring
+  constexpr int NP = DIM3 ? 3 : 1;  // planes in the u, v, w, T, mu ring
+  constexpr int NM = DIM3 ? 2 : 1;  // planes in the metric ring
   constexpr int SX = TX + 2, SY = TY + 2;
+  constexpr int NS = (NP * 5 + NM * 10) * SY * SX;  // staged values
   extern __shared__ __align__(16) unsigned char vsm_raw[];
   auto sv = reinterpret_cast<T(*)[5][SY][SX]>(vsm_raw);
   auto sm = reinterpret_cast<T(*)[10][SY][SX]>(vsm_raw + sizeof(T) * NP * 5 * SY * SX);
-  auto fxs = reinterpret_cast<T(*)[TX + 1][4]>(vsm_raw + sizeof(T) * NP * 15 * SY * SX);
-  auto fys = reinterpret_cast<T(*)[TX][4]>(vsm_raw + sizeof(T) * (NP * 15 * SY * SX + TY * (TX + 1) * 4));
+  auto fxs = reinterpret_cast<T(*)[TX + 1][4]>(vsm_raw + sizeof(T) * NS);
+  auto fys = reinterpret_cast<T(*)[TX][4]>(vsm_raw + sizeof(T) * (NS + TY * (TX + 1) * 4));
+  auto mslot = [](int kk) { return DIM3 ? (kk & 1) : 0; };  // kk >= -1
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * TX + tx;
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
@@ -674,7 +679,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 8 ? 2 : 4) k_visc_update(
   }
   const T tref[3] = {(T)ref[0], (T)ref[1], (T)ref[2]};
   auto load_plane = [&](int kk) {
-    const int slot = DIM3 ? (kk + 3) % 3 : 0;
+    const int slot = DIM3 ? (kk + 3) % 3 : 0, ms = mslot(kk);
     for (int n = tid; n < SX * SY; n += TX * TY) {
       const int ii = i0 - 1 + n % SX, jj = j0 - 1 + n / SX;
       if (ii >= b.mx + b.g || jj >= b.my + b.g) continue;
@@ -687,26 +692,26 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 8 ? 2 : 4) k_visc_update(
       sv[slot][4][y][x] = (T)a.in.mul[p];
       if constexpr (std::is_same_v<T, float>) {
 #pragma unroll
-        for (int r = 0; r < 10; ++r) sm[slot][r][y][x] = b.met32[r * P + p];
+        for (int r = 0; r < 10; ++r) sm[ms][r][y][x] = b.met32[r * P + p];
       } else {
 #pragma unroll
-        for (int r = 0; r < 9; ++r) sm[slot][r][y][x] = (T)b.met[r * P + p];
-        sm[slot][9][y][x] = (T)b.jac[p];
+        for (int r = 0; r < 9; ++r) sm[ms][r][y][x] = (T)b.met[r * P + p];
+        sm[ms][9][y][x] = (T)b.jac[p];
       }
     }
   };
   // face whose first node is tile node (x, y) of plane kk, direction d
   auto face = [&](int d, int x, int y, int kk, T *fv) {
-    const int s0 = DIM3 ? (kk + 3) % 3 : 0;
+    const int s0 = DIM3 ? (kk + 3) % 3 : 0, m0 = mslot(kk);
     auto V = [&](int q, int di, int dj, int dk) -> T {
       const int sl = DIM3 ? (s0 + dk + 3) % 3 : 0;
       return sv[sl][q][y + dj][x + di];
     };
     auto Mt = [&](int r, int sd) -> T {
-      if (sd == 0) return sm[s0][r][y][x];
-      if (d == 0) return sm[s0][r][y][x + 1];
-      if (d == 1) return sm[s0][r][y + 1][x];
-      return sm[DIM3 ? (s0 + 1) % 3 : 0][r][y][x];
+      if (sd == 0) return sm[m0][r][y][x];
+      if (d == 0) return sm[m0][r][y][x + 1];
+      if (d == 1) return sm[m0][r][y + 1][x];
+      return sm[mslot(kk + 1)][r][y][x];
     };
     viscous_face<T, DIM3>(d, V, Mt, ipr, tref, fv);
   };
@@ -717,6 +722,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 8 ? 2 : 4) k_visc_update(
       load_plane(k0);
       __syncthreads();
       if (inside) face(2, tx + 1, ty + 1, k0 - 1, fz_prev);
+      __syncthreads();  // plane k0 + 1 takes the metric slot of plane k0 - 1
     }
   }
   const double dt = a.update ? *a.dt : 0.0;
