@@ -70,10 +70,16 @@ ALGO_BYTES_PER_NODE = {"flux_x": 152, "flux_y": 192, "flux_z": 192, "visc_update
 # DRAM bytes per node measured by one ncu capture of the kernel (dram__bytes_read.sum +
 # dram__bytes_write.sum over the nodes of the launch, 256x128x64 case of the same workload; traffic
 # grows with the node count, so a full-size launch moves this figure times its nodes).  The y/z
-# sweeps have two designs picked by the library's autotuner; at 512x256x128 it keeps the column
-# march for y (profiles/k_flux_march_fp64_awe7_256x128x64.md) and the 32x4x4 tile for z
-# (profiles/k_flux_tile_fp64_awe7_256x128x64.md).
-MEASURED_TRAFFIC_PER_NODE = {"flux_y": 209.8, "flux_z": 203.3}
+# sweeps have several designs picked by the library's autotuner; at 512x256x128 it keeps 16-lane
+# tiles, and the capture is of the 16 x 16 x 1 tile (the column march moved 209.8, the 32x4x4 tile
+# 194-203 B per node).
+MEASURED_TRAFFIC_PER_NODE = {"flux_y": 214.5, "flux_z": 214.5}
+# FP64 operations per face of the y/z sweep (AWENO7 + HLLC, central correction), from the same
+# capture's instruction counters: 2 x DFMA + DMUL + DADD thread-instructions over the launch's faces.
+# Against the FP64 FMA peak of the part (64 DFMA per cycle per SM) this is the roof the sweeps run
+# into; the HBM fraction above stays far from 1 because the sweeps are arithmetic bound.
+FP64_FLOP_PER_FACE = 3275
+FP64_DFMA_PER_CYCLE_PER_SM = 64
 # Whole fused stage (three state passes + metric): 8 (3 n_var + 10) bytes per cell-stage, n_var = 5
 STAGE_BYTES = 8 * (3 * 5 + 10)
 # steps after which the reacting layer's mixed-precision state is compared with the FP64 one
@@ -404,11 +410,21 @@ def run_ours(args):
     if dom in MEASURED_TRAFFIC_PER_NODE:
         traffic = MEASURED_TRAFFIC_PER_NODE[dom] * nodes
     step_ms = ms_max / K
+    fp64_roof = None
+    if dom in ("flux_y", "flux_z"):
+        mhz = float(clocks.get("sm_mhz") or 1965.0) if isinstance(clocks, dict) else 1965.0
+        n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+        peak_t = 2 * FP64_DFMA_PER_CYCLE_PER_SM * n_sm * mhz * 1e6 / 1e12
+        ach_t = FP64_FLOP_PER_FACE * nodes / (avg_ms / 1e3) / 1e12
+        fp64_roof = {"flop_per_face": FP64_FLOP_PER_FACE, "achieved_tflops": ach_t, "peak_tflops": peak_t,
+                     "frac": ach_t / peak_t, "peak": f"{2 * FP64_DFMA_PER_CYCLE_PER_SM} FP64 FLOP per cycle per SM x "
+                                                   f"{n_sm} SMs at the sampled {mhz:.0f} MHz"}
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": traffic, "algorithmic_bytes_per_launch": algo,
                 "avg_launch_ms": avg_ms, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "note": "flux kernels are FP64-ALU bound (characteristic WENO7 ~2.5 kFLOP per face); the HBM "
-                        "fraction is reported as the contract asks",
+                "note": "flux kernels are FP64-ALU bound (characteristic WENO7 + HLLC, 3.3 kFLOP per face); the "
+                        "HBM fraction is reported as the contract asks, the FP64 fraction in fp64",
+                "fp64": fp64_roof,
                 "whole_step": {"achieved": value / world * 3 * STAGE_BYTES / 1e9,
                                "frac": value / world * 3 * STAGE_BYTES / 1e9 / hbm,
                                "bytes_per_cell_step": 3 * STAGE_BYTES},
