@@ -33,9 +33,11 @@ __device__ __forceinline__ void mix_cv_from_bv_node(const DevBlock &b, const Dev
 }
 
 // update_physical_properties<mixture> over every padded node (FieldOperation.cuh:107-134), with the
-// node's state read in FP64 and the properties evaluated in T (FP32 in the mixed precision mode)
+// node's state read in FP64 and the properties evaluated in T (FP32 in the mixed precision mode).
+// FP32 at four resident blocks (128 registers) measured 1.4 ms per step faster than uncapped; FP64
+// is fastest uncapped.
 template <int NS, typename T>
-__global__ void __launch_bounds__(128) k_mix_props(DevBlock b, DevState s) {
+__global__ void __launch_bounds__(128, sizeof(T) == 8 ? 1 : 4) k_mix_props(DevBlock b, DevState s) {
   const long long P = b.plane;
   const int ns = OSTC_NS;
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
@@ -135,8 +137,10 @@ __host__ __device__ constexpr size_t fvs_smem_bytes(int nv) {
 // computed once into shared memory; each thread then forms one face flux from the 8-node stencil,
 // and after a barrier the node threads difference neighbouring faces into dq.  T is the arithmetic
 // type of the fluxes (FP32 in the mixed precision mode: state read in FP64, dq accumulated in FP64).
+// Resident blocks per SM (measured on the 384 x 192 x 96 layer): FP64 4; FP32 8 (64 registers, some
+// spills; 6, 7 and 8 blocks ran the mixed step in 79.5, 77.0 and 76.9 ms against 84.6 ms at 4).
 template <int DIR, int NS, typename T>
-__global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL, 4) k_fvs(DevBlock b, DevState s,
+__global__ void __launch_bounds__(FvsTile<DIR>::TD * FvsTile<DIR>::TXL, sizeof(T) == 8 ? 4 : 8) k_fvs(DevBlock b, DevState s,
                                                                                double *__restrict__ dq, int nv,
                                                                                int scheme) {
   constexpr int TXL = FvsTile<DIR>::TXL, TD = FvsTile<DIR>::TD, NST = FvsTile<DIR>::NST;
